@@ -1,0 +1,328 @@
+"""``delta._core`` re-created over the sm_100a C ABI (include/delta_gpu.h).
+
+Same function names, argument names / defaults, return types and error
+behaviour as the reference's nanobind module (src/bindings.cpp:902-1036,
+python/delta/_core.pyi). Arrays are coerced like nanobind's
+``ndarray<const T, ndim<N>, c_contig>`` casters (a C-contiguous copy in the
+declared dtype); the GIL is released inside every library call (ctypes).
+All image work runs on the GPU; nothing here computes pixels on the CPU.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, context, ptr
+
+__version__ = "1.1.1"
+
+
+def _img(a, name="array"):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if a.ndim != 2:
+        raise TypeError(f"{name}: expected a 2-D float32 array, got shape {a.shape}")
+    return a
+
+
+def _img_opt(a, name="array"):
+    return None if a is None else _img(a, name)
+
+
+def _mask_opt(a, name="mask"):
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=np.uint8)
+    if a.ndim != 2:
+        raise TypeError(f"{name}: expected a 2-D uint8 array, got shape {a.shape}")
+    return a
+
+
+def _mat(a, cols=None, name="matrix"):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.ndim == 1 and cols is not None:
+        a = a.reshape(-1, cols) if a.size % cols == 0 else a.reshape(1, -1)
+    if a.ndim != 2:
+        raise TypeError(f"{name}: expected a 2-D float64 array")
+    return a
+
+
+def _vec(a, name="vector"):
+    a = np.ascontiguousarray(a, dtype=np.float64).ravel()
+    return a
+
+
+def _knots(knots):
+    k = _mat(knots, name="knots")
+    if k.shape[1] != 2:
+        raise ValueError("knots must be (k, 2)")
+    if k.shape[0] < 3:
+        raise ValueError("need at least 3 knots")
+    return k
+
+
+def _points(points):
+    p = _mat(points, name="points")
+    if p.shape[1] != 2:
+        raise ValueError("points must be (m, 2)")
+    return p
+
+
+def _same_shape(a, ref, what):
+    if a is not None and a.shape != ref.shape:
+        raise RuntimeError(what)
+
+
+# ---- basis / convolve ---------------------------------------------------------
+
+
+def _resolve_radius(beta, n_max, radius):
+    return radius if radius > 0 else _lib.lib().dgpu_default_radius(ctypes.c_double(beta), int(n_max))
+
+
+def gauss_hermite_basis1d(beta: float, n_max: int, radius: int = 0) -> np.ndarray:
+    """1-D sampled Gauss-Hermite basis functions, shape (n_max+1, ksize)."""
+    if n_max < 0:
+        raise ValueError("n_max must be >= 0")
+    r = _resolve_radius(beta, n_max, radius)
+    out = np.zeros((n_max + 1, 2 * r + 1), np.float64)
+    ks = ctypes.c_int()
+    check(_lib.lib().dgpu_gauss_hermite_basis1d(ctypes.c_double(beta), int(n_max), int(radius), ptr(out),
+                                                ctypes.byref(ks)))
+    return out
+
+
+def gauss_hermite_kernels(beta: float, n_max: int, radius: int = 0):
+    """(orders int32 (ncomp, 2), kernels float32 (ncomp, ks, ks))."""
+    if n_max < 0:
+        raise ValueError("n_max must be >= 0")
+    r = _resolve_radius(beta, n_max, radius)
+    nc = (n_max + 1) * (n_max + 2) // 2
+    ks = 2 * r + 1
+    orders = np.zeros((nc, 2), np.int32)
+    kernels = np.zeros((nc, ks, ks), np.float32)
+    kso = ctypes.c_int()
+    check(_lib.lib().dgpu_gauss_hermite_kernels(ctypes.c_double(beta), int(n_max), int(radius), ptr(orders),
+                                                ptr(kernels), ctypes.byref(kso)))
+    return orders, kernels
+
+
+def basis_convolve(image, beta: float, n_max: int, radius: int = 0) -> np.ndarray:
+    """Convolve image with each basis component; returns (ncomp, H, W)."""
+    img = _img(image, "image")
+    h, w = img.shape
+    if n_max < 0:
+        raise ValueError("n_max must be >= 0")
+    nc = (n_max + 1) * (n_max + 2) // 2
+    out = np.empty((nc, h, w), np.float32)
+    ctx = context()
+    check(_lib.lib().dgpu_basis_convolve(ctx.handle, _lib.MEM_HOST, ptr(img), ctypes.c_int64(w),
+                                         ctypes.c_int64(h), ctypes.c_double(beta), int(n_max), int(radius),
+                                         ptr(out)), ctx.handle)
+    return out
+
+
+# ---- thin-plate spline ----------------------------------------------------------
+
+
+def grid_knots(x0: float, y0: float, x1: float, y1: float, nx: int, ny: int) -> np.ndarray:
+    """Regular nx*ny grid of knots over [x0,x1]x[y0,y1]."""
+    if nx < 1 or ny < 1:
+        raise ValueError("nx, ny must be >= 1")
+    out = np.zeros((nx * ny, 2), np.float64)
+    check(_lib.lib().dgpu_grid_knots(ctypes.c_double(x0), ctypes.c_double(y0), ctypes.c_double(x1),
+                                     ctypes.c_double(y1), int(nx), int(ny), ptr(out)))
+    return out
+
+
+def tps_design(knots, points) -> np.ndarray:
+    """Thin-plate regression-spline design matrix (m, n_basis)."""
+    k = _knots(knots)
+    p = _points(points)
+    out = np.zeros((p.shape[0], k.shape[0]), np.float64)
+    check(_lib.lib().dgpu_tps_design(ptr(k), k.shape[0], ptr(p), ctypes.c_int64(p.shape[0]), ptr(out)))
+    return out
+
+
+def tps_penalty(knots) -> np.ndarray:
+    """Thin-plate bending-energy penalty matrix (n_basis, n_basis)."""
+    k = _knots(knots)
+    out = np.zeros((k.shape[0], k.shape[0]), np.float64)
+    check(_lib.lib().dgpu_tps_penalty(ptr(k), k.shape[0], ptr(out)))
+    return out
+
+
+def tps_fit(knots, points, values, lam: float) -> np.ndarray:
+    """Unweighted penalised fit: (D^T D + lam P) theta = D^T values."""
+    k = _knots(knots)
+    p = _points(points)
+    v = _vec(values)
+    out = np.zeros(k.shape[0], np.float64)
+    check(_lib.lib().dgpu_tps_fit(ptr(k), k.shape[0], ptr(p), ctypes.c_int64(p.shape[0]), ptr(v),
+                                  ctypes.c_double(lam), ptr(out)))
+    return out
+
+
+def tps_evaluate(knots, points, coeffs) -> np.ndarray:
+    """Evaluate a fitted TPS field at points: design(points) @ coeffs."""
+    k = _knots(knots)
+    p = _points(points)
+    c = _vec(coeffs)
+    out = np.zeros(p.shape[0], np.float64)
+    check(_lib.lib().dgpu_tps_evaluate(ptr(k), k.shape[0], ptr(p), ctypes.c_int64(p.shape[0]), ptr(c), ptr(out)))
+    return out
+
+
+# ---- subtraction ---------------------------------------------------------------------
+
+
+def _model(knots, theta, beta, n_max, radius):
+    k = _knots(knots)
+    th = _vec(theta)
+    m = _lib.Model(k.ctypes.data, k.shape[0], th.ctypes.data, th.size, float(beta), int(n_max), int(radius))
+    return m, (k, th)
+
+
+def subtract(science, reference, knots, theta, beta: float, n_max: int, radius: int = 0,
+             saturation: float = 0.0, science_var=None, reference_var=None, science_mask=None,
+             reference_mask=None) -> dict:
+    """Full-frame spatially-varying subtraction with variance/mask propagation.
+
+    Returns {'difference','variance','mask','timing'} (src/bindings.cpp:603-638).
+    """
+    sci = _img(science, "science")
+    ref = _img(reference, "reference")
+    svar = _img_opt(science_var, "science_var")
+    rvar = _img_opt(reference_var, "reference_var")
+    smask = _mask_opt(science_mask, "science_mask")
+    rmask = _mask_opt(reference_mask, "reference_mask")
+    _same_shape(svar, sci, "variance shape does not match data")
+    _same_shape(smask, sci, "mask shape does not match data")
+    _same_shape(rvar, ref, "variance shape does not match data")
+    _same_shape(rmask, ref, "mask shape does not match data")
+    if sci.shape != ref.shape:
+        raise RuntimeError("subtract: science/reference shape mismatch")
+    if n_max < 0:
+        raise ValueError("n_max must be >= 0")
+    h, w = sci.shape
+    model, keep = _model(knots, theta, beta, n_max, radius)
+    diff = np.empty((h, w), np.float32)
+    var = np.empty((h, w), np.float32) if (svar is not None or rvar is not None) else None
+    mask = np.empty((h, w), np.uint8) if (smask is not None or rmask is not None or saturation > 0) else None
+    hv, hm = ctypes.c_int(), ctypes.c_int()
+    ctx = context()
+    check(_lib.lib().dgpu_subtract(ctx.handle, _lib.MEM_HOST, ctypes.c_int64(w), ctypes.c_int64(h), ptr(sci),
+                                   ptr(ref), ptr(svar), ptr(rvar), ptr(smask), ptr(rmask), ctypes.byref(model),
+                                   ctypes.c_double(saturation), ptr(diff), ptr(var), ptr(mask),
+                                   ctypes.byref(hv), ctypes.byref(hm)), ctx.handle)
+    return {"timing": _lib.drain_timing(ctx), "difference": diff, "variance": var if hv.value else None,
+            "mask": mask if hm.value else None}
+
+
+def photometric_scale(knots, theta, component_sums, height: int, width: int) -> np.ndarray:
+    """Per-pixel photometric scale field sum_n a_n(x,y) S_n, shape (H,W)."""
+    k = _knots(knots)
+    th = _vec(theta)
+    s = _vec(component_sums)
+    out = np.empty((height, width), np.float32)
+    ctx = context()
+    check(_lib.lib().dgpu_photometric_scale(ctx.handle, _lib.MEM_HOST, ptr(k), k.shape[0], ptr(th),
+                                            ctypes.c_int64(th.size), ptr(s), int(s.size), ctypes.c_int64(height),
+                                            ctypes.c_int64(width), ptr(out)), ctx.handle)
+    return out
+
+
+def photometric_scale_at(knots, theta, component_sums, points) -> np.ndarray:
+    """Photometric scale evaluated at points, shape (m,)."""
+    k = _knots(knots)
+    th = _vec(theta)
+    s = _vec(component_sums)
+    p = _points(points)
+    out = np.zeros(p.shape[0], np.float64)
+    check(_lib.lib().dgpu_photometric_scale_at(ptr(k), k.shape[0], ptr(th), ctypes.c_int64(th.size), ptr(s),
+                                               int(s.size), ptr(p), ctypes.c_int64(p.shape[0]), ptr(out)))
+    return out
+
+
+# ---- matched filter -------------------------------------------------------------------
+
+
+def matched_filter(image, psf, variance) -> np.ndarray:
+    """Match-filtered score image (per-pixel S/N map)."""
+    img = _img(image, "image")
+    p = _img(psf, "psf")
+    var = _img(variance, "variance")
+    if p.shape[0] != p.shape[1]:
+        raise RuntimeError("matched_filter: psf must be square")
+    if var.shape != img.shape:
+        raise RuntimeError("matched_filter: variance must match image shape")
+    h, w = img.shape
+    out = np.empty((h, w), np.float32)
+    ctx = context()
+    check(_lib.lib().dgpu_matched_filter(ctx.handle, _lib.MEM_HOST, ctypes.c_int64(w), ctypes.c_int64(h), ptr(img),
+                                         ptr(p), int(p.shape[0]), ptr(var), ptr(out)), ctx.handle)
+    return out
+
+
+# ---- catalog ------------------------------------------------------------------------------
+
+
+def build_catalog(score, difference, mask=None, threshold_sigma: float = 5.0,
+                  threshold_sigma_dipole: float = 3.0, expected_fwhm: float = 3.5,
+                  fwhm_tolerance_lo: float = 0.3, fwhm_tolerance_hi: float = 3.0, aperture_radius: int = 0,
+                  exclude_bad_pixels: bool = True, return_negative: bool = False, fit_psf_shape: bool = False,
+                  shape_chi2_tolerance: float = 3.0, variance=None, psf=None, bright_star_radius: float = 0.0,
+                  max_shape_fit: int = 5000, bright_x=None, bright_y=None) -> dict:
+    """Connected-component source catalog from a match-filtered score image."""
+    sc = _img(score, "score")
+    df = _img(difference, "difference")
+    mk = _mask_opt(mask)
+    var = _img_opt(variance, "variance")
+    p = _img_opt(psf, "psf")
+    if df.shape != sc.shape:
+        raise RuntimeError("build_catalog: difference shape must match score")
+    if var is not None and var.shape != sc.shape:
+        raise RuntimeError("build_catalog: variance shape must match score")
+    if p is not None and p.shape[0] != p.shape[1]:
+        raise RuntimeError("build_catalog: psf must be square")
+    if (bright_x is None) != (bright_y is None):
+        raise RuntimeError("build_catalog: supply both bright_x and bright_y, or neither")
+    bx = None if bright_x is None else np.ascontiguousarray(bright_x, np.float64).ravel()
+    by = None if bright_y is None else np.ascontiguousarray(bright_y, np.float64).ravel()
+    if bx is not None and bx.size != by.size:
+        raise RuntimeError("build_catalog: bright_x and bright_y must be the same length")
+    if mk is not None and mk.shape != sc.shape:
+        raise RuntimeError("mask shape does not match data")
+    h, w = sc.shape
+    prm = _lib.CatalogParams(float(threshold_sigma), float(threshold_sigma_dipole), float(expected_fwhm),
+                             float(fwhm_tolerance_lo), float(fwhm_tolerance_hi), int(aperture_radius),
+                             int(bool(exclude_bad_pixels)), int(bool(return_negative)), int(bool(fit_psf_shape)),
+                             float(shape_chi2_tolerance), float(bright_star_radius), int(max_shape_fit))
+    ctx = context()
+    L = _lib.lib()
+    n = ctypes.c_int()
+    check(L.dgpu_build_catalog(ctx.handle, _lib.MEM_HOST, ctypes.c_int64(w), ctypes.c_int64(h), ptr(sc), ptr(df),
+                               ptr(mk), ctypes.byref(prm), ptr(var), ptr(p), 0 if p is None else int(p.shape[0]),
+                               ptr(bx), ptr(by), 0 if bx is None else int(bx.size), ctypes.byref(n)), ctx.handle)
+    cols = {name: np.empty(n.value, dt) for name, dt in _lib.CATALOG_COLUMNS}
+    cc = _lib.CatalogColumns(*[cols[name].ctypes.data for name, _ in _lib.CATALOG_COLUMNS])
+    check(L.dgpu_catalog_fetch(ctx.handle, ctypes.byref(cc), n.value), ctx.handle)
+    cols["timing"] = _lib.drain_timing(ctx)
+    return cols
+
+
+def catalog_labels(shape) -> np.ndarray:
+    """Label image of the last build_catalog on this thread (not in the reference
+    binding; exposes the labels the reference keeps internal)."""
+    h, w = shape
+    out = np.empty((h, w), np.int32)
+    ctx = context()
+    check(_lib.lib().dgpu_catalog_labels(ctx.handle, _lib.MEM_HOST, ptr(out), ctypes.c_int64(h * w)), ctx.handle)
+    return out
+
+
+def drain_timing():
+    """Drain accumulated DELTA_TIMING sub-stage timers into a {label: seconds} dict."""
+    return _lib.drain_timing(context())

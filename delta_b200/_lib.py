@@ -1,0 +1,192 @@
+"""Loader for the in-tree CUDA library ``libdelta_gpu.so`` (include/delta_gpu.h).
+
+There is no CPU fallback: if the library or a CUDA device is missing, every
+device entry point raises :class:`DeviceUnavailableError`.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libdelta_gpu.so"
+
+DGPU_OK = 0
+DGPU_ERR_INVALID = 1
+DGPU_ERR_RUNTIME = 2
+DGPU_ERR_CUDA = 3
+DGPU_ERR_LIMIT = 4
+DGPU_ERR_CAPACITY = 5
+DGPU_ERR_NO_DEVICE = 6
+
+MEM_HOST = 0
+MEM_DEVICE = 1
+
+PREC_FP64 = 0
+PREC_FP32 = 1
+PREC_MIXED = 2
+
+
+class DeviceUnavailableError(RuntimeError):
+    """The CUDA library or a CUDA device is not available (no CPU fallback)."""
+
+
+class DeviceLoopLimitError(RuntimeError):
+    """A device loop hit its iteration cap and returned an error status."""
+
+
+_lib = None
+_lock = threading.Lock()
+_tls = threading.local()
+
+
+class Model(ctypes.Structure):
+    _fields_ = [
+        ("knots", ctypes.c_void_p),
+        ("n_knots", ctypes.c_int),
+        ("theta", ctypes.c_void_p),
+        ("n_theta", ctypes.c_int64),
+        ("beta", ctypes.c_double),
+        ("n_max", ctypes.c_int),
+        ("radius", ctypes.c_int),
+    ]
+
+
+class CatalogParams(ctypes.Structure):
+    _fields_ = [
+        ("threshold_sigma", ctypes.c_double),
+        ("threshold_sigma_dipole", ctypes.c_double),
+        ("expected_fwhm", ctypes.c_double),
+        ("fwhm_tolerance_lo", ctypes.c_double),
+        ("fwhm_tolerance_hi", ctypes.c_double),
+        ("aperture_radius", ctypes.c_int),
+        ("exclude_bad_pixels", ctypes.c_int),
+        ("return_negative", ctypes.c_int),
+        ("fit_psf_shape", ctypes.c_int),
+        ("shape_chi2_tolerance", ctypes.c_double),
+        ("bright_star_radius", ctypes.c_double),
+        ("max_shape_fit", ctypes.c_int),
+    ]
+
+
+CATALOG_COLUMNS = [
+    ("x", np.float64), ("y", np.float64), ("peak_x", np.int32), ("peak_y", np.int32),
+    ("peak_snr", np.float64), ("n_pix", np.int32), ("flux", np.float64),
+    ("expected_n_pix", np.float64), ("fwhm_ratio", np.float64), ("fwhm_consistent", np.uint8),
+    ("mask_flags", np.uint8), ("is_dipole", np.uint8), ("quality", np.uint8),
+    ("psf_chi2", np.float64), ("psf_chi2_dof", np.int32), ("psf_amplitude", np.float64),
+    ("psf_amplitude_err", np.float64), ("shape_consistent", np.uint8),
+    ("bright_star_dist", np.float64), ("near_bright_star", np.uint8),
+]
+
+
+class CatalogColumns(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_void_p) for name, _ in CATALOG_COLUMNS]
+
+
+def lib():
+    """The loaded C library (raises DeviceUnavailableError if it is missing)."""
+    global _lib
+    if _lib is None:
+        with _lock:
+            if _lib is None:
+                if not LIB_PATH.exists():
+                    raise DeviceUnavailableError(
+                        f"{LIB_PATH} is not built; run `python -c 'import __graft_entry__ as g; g.build()'`"
+                        " (or make -C delta_b200/csrc)"
+                    )
+                L = ctypes.CDLL(str(LIB_PATH))
+                L.dgpu_last_error.restype = ctypes.c_char_p
+                L.dgpu_last_error.argtypes = [ctypes.c_void_p]
+                L.dgpu_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+                L.dgpu_destroy.argtypes = [ctypes.c_void_p]
+                L.dgpu_default_radius.restype = ctypes.c_int
+                _lib = L
+    return _lib
+
+
+def ptr(a):
+    """Data pointer of a C-contiguous ndarray (None -> NULL)."""
+    if a is None:
+        return None
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def check(rc: int, ctx=None, what: str = "") -> None:
+    """Map a DGPU status code to the reference's Python exception types."""
+    if rc == DGPU_OK:
+        return
+    msg = lib().dgpu_last_error(ctx).decode(errors="replace")
+    if what and not msg.startswith(what):
+        msg = f"{what}: {msg}" if msg else what
+    if rc == DGPU_ERR_INVALID:
+        raise ValueError(msg)
+    if rc == DGPU_ERR_NO_DEVICE:
+        raise DeviceUnavailableError(msg)
+    if rc == DGPU_ERR_LIMIT:
+        raise DeviceLoopLimitError(msg)
+    raise RuntimeError(msg)
+
+
+class Context:
+    """One CUDA context handle (stream + workspace) of the library."""
+
+    def __init__(self, device: int = 0):
+        L = lib()
+        h = ctypes.c_void_p()
+        rc = L.dgpu_create(int(device), ctypes.byref(h))
+        if rc != DGPU_OK:
+            msg = L.dgpu_last_error(None).decode(errors="replace")
+            if rc == DGPU_ERR_NO_DEVICE:
+                raise DeviceUnavailableError(f"no CUDA device for delta_b200: {msg}")
+            raise RuntimeError(msg)
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            lib().dgpu_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle: int | None):
+        check(lib().dgpu_set_stream(self.handle, ctypes.c_void_p(stream_handle or 0)), self.handle)
+
+    def synchronize(self):
+        check(lib().dgpu_synchronize(self.handle), self.handle)
+
+
+def context() -> Context:
+    """The calling thread's default context on device ``DELTA_B200_DEVICE`` (default 0)."""
+    ctx = getattr(_tls, "ctx", None)
+    if ctx is None:
+        ctx = Context(int(os.environ.get("DELTA_B200_DEVICE", "0")))
+        _tls.ctx = ctx
+    return ctx
+
+
+def timing_enabled() -> bool:
+    v = os.environ.get("DELTA_TIMING", "")
+    return v not in ("", "0")
+
+
+def drain_timing(ctx: Context) -> dict | None:
+    if not timing_enabled():
+        return None
+    cap = 64
+    labels = (ctypes.c_char * 64 * cap)()
+    secs = (ctypes.c_double * cap)()
+    n = ctypes.c_int()
+    check(lib().dgpu_drain_timing(ctx.handle, labels, secs, cap, ctypes.byref(n)), ctx.handle)
+    return {bytes(labels[i]).split(b"\0", 1)[0].decode(): secs[i] for i in range(min(n.value, cap))}

@@ -1,0 +1,220 @@
+// Internal declarations shared by the host runtime (*.cpp) and the sm_100a
+// kernels (*.cu) of libdelta_gpu.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "delta_gpu.h"
+
+namespace dgpu {
+
+// ---------------------------------------------------------------------------
+// Errors
+// ---------------------------------------------------------------------------
+
+// Thrown inside the library only; every C entry point catches and converts.
+struct Failure : std::runtime_error {
+  int code;
+  Failure(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void fail(int code, const std::string& msg);
+void check_cuda(cudaError_t e, const char* what);
+#define DGPU_CUDA(call) ::dgpu::check_cuda((call), #call)
+#define DGPU_LAUNCH(what) ::dgpu::check_cuda(cudaGetLastError(), what)
+
+// ---------------------------------------------------------------------------
+// Device status word: kernels with a data-dependent loop bound record here
+// (never spin or trap). Bits are cleared at the start of each entry point.
+// ---------------------------------------------------------------------------
+enum StatusBit : unsigned {
+  kStatusLoopLimit = 1u << 0,  // union-find / search loop hit its cap
+  kStatusBounds = 1u << 1,     // an index check rejected an access
+};
+
+// ---------------------------------------------------------------------------
+// Workspace: named, growable device slots, so steady-state calls allocate
+// nothing. Slots never shrink; contents are not preserved across growth.
+// ---------------------------------------------------------------------------
+enum Slot : int {
+  kSlotInSci, kSlotInRef, kSlotInVarS, kSlotInVarR, kSlotInMaskS, kSlotInMaskR,
+  kSlotOutDiff, kSlotOutVar, kSlotOutMask, kSlotOutScore,
+  kSlotLattice, kSlotLatticeF, kSlotCellX, kSlotCellY, kSlotTaps, kSlotPhi, kSlotFullFields,
+  kSlotTheta, kSlotKnots, kSlotZ,
+  kSlotExactBad, kSlotSamples, kSlotSelect, kSlotPsf,
+  kSlotSeedPos, kSlotSeedNeg, kSlotLabels, kSlotLabelsNeg, kSlotRootRank, kSlotBlockCounts,
+  kSlotCompStats, kSlotCompOut, kSlotBright, kSlotScratch0, kSlotScratch1, kSlotScratch2,
+  kSlotFit0, kSlotFit1, kSlotFit2, kSlotFit3, kSlotFit4, kSlotFit5, kSlotFit6, kSlotFit7,
+  kSlotFit8, kSlotFit9, kSlotFit10, kSlotFit11, kSlotFit12, kSlotFit13, kSlotFit14, kSlotFit15,
+  kSlotFft0, kSlotFft1, kSlotFft2, kSlotFft3, kSlotFft4, kSlotFft5,
+  kSlotCount
+};
+
+struct Context {
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  unsigned* d_status = nullptr;  // device status word (see StatusBit)
+  void* slot_ptr[kSlotCount] = {};
+  size_t slot_size[kSlotCount] = {};
+  std::string last_error;
+  // Host-visible timing: label -> accumulated seconds (DELTA_TIMING).
+  std::vector<std::pair<std::string, double>> timing;
+  bool timing_enabled = false;
+  // Catalog results of the last dgpu_build_catalog (host copies).
+  std::vector<double> cat_d;    // 12 double columns x n
+  std::vector<int32_t> cat_i;   // 3 int32 columns x n
+  std::vector<uint8_t> cat_u8;  // 7 uint8 columns x n
+  int cat_count = 0;
+  int64_t cat_npix = 0;         // label image size of the last catalog
+
+  void* slot(Slot s, size_t bytes);
+};
+
+// RAII: clear the status word at entry, check it (after a sync) at exit.
+void reset_status(Context& c);
+void check_status(Context& c);  // synchronises the stream
+
+// Device-side timing scope keyed by a reference DELTA_TIMING label.
+struct StageTimer {
+  Context& c;
+  std::string label;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  StageTimer(Context& ctx, const char* l);
+  ~StageTimer();
+};
+
+// Copy a caller array into a device slot (mem == HOST) or return it in place.
+const void* stage_in(Context& c, int mem, const void* p, size_t bytes, Slot s);
+// Destination for an output: device slot (HOST) or the caller pointer (DEVICE).
+void* out_buf(Context& c, int mem, void* p, size_t bytes, Slot s);
+// Copy a device slot result back to the caller (HOST mode only).
+void stage_out(Context& c, int mem, void* host, const void* dev, size_t bytes);
+
+// ---------------------------------------------------------------------------
+// Host math: basis (basis.cpp) and thin-plate spline (tps.cpp)
+// ---------------------------------------------------------------------------
+struct Basis {
+  double beta = 0;
+  int n_max = 0, radius = 0, ks = 0, nc = 0;
+  std::vector<double> b1d;           // (n_max+1) x ks
+  std::vector<std::pair<int, int>> orders;  // (nx, ny) per component
+  Basis(double beta, int n_max, int radius);  // radius <= 0 -> default
+  std::vector<float> taps() const;   // float32 (n_max+1) x ks
+  std::vector<float> kernel2d(int c) const;
+  std::vector<double> component_sums() const;
+};
+int default_radius(double beta, int n_max);
+
+struct ThinPlate {
+  int k = 0;
+  double cx = 0, cy = 0, scale = 1;
+  std::vector<double> kn;       // k x 2 normalised knots
+  std::vector<double> z;        // k x (k-3) null space, row-major
+  std::vector<double> penalty;  // k x k
+  explicit ThinPlate(const double* knots, int k);
+  void design_row(double x, double y, double* out) const;  // k values
+  double min_knot_spacing() const;
+  // F (P x (nc+1)*r, row-major) with F F^T = blockdiag(penalty) (solve.cpp:47-65).
+  std::vector<double> pen_half(int nc, int* r_out) const;
+};
+
+// Symmetric eigendecomposition (cyclic Jacobi), ascending eigenvalues.
+void sym_eig(int n, const double* a, double* w, double* v);
+
+// Coarse field lattice geometry (subtract.cpp:107-316).
+struct FieldGeom {
+  bool exact = false;
+  int stride = 1, ncx = 0, ncy = 0;
+  std::vector<int> gx, gy, cellx, celly;
+  std::vector<float> wx, wy;
+};
+FieldGeom make_field_geom(const ThinPlate& tp, int w, int h);
+
+// ---------------------------------------------------------------------------
+// Device fields: lattice (coarse) or full-resolution arrays (exact).
+// ---------------------------------------------------------------------------
+struct DevFields {
+  int exact = 0;
+  int nf = 0, w = 0, h = 0;
+  const float* full = nullptr;   // exact: nf*h*w
+  const float* latf = nullptr;   // coarse: nf*ncy*ncx, float32 copies of the FP64 lattice
+  const double* lat = nullptr;   // coarse FP64 lattice
+  int ncx = 0, ncy = 0;
+  const int* cellx = nullptr;    // w
+  const float* wx = nullptr;     // w
+  const int* celly = nullptr;    // h
+  const float* wy = nullptr;     // h
+};
+
+// Evaluate the fields of `theta` (host) on the device.
+DevFields build_fields(Context& c, const ThinPlate& tp, const double* theta, int nf, int w, int h);
+// Same, with theta already on the device (FP64, nf*k).
+DevFields build_fields_dev(Context& c, const ThinPlate& tp, const double* d_theta, int nf, int w,
+                           int h);
+
+// ---------------------------------------------------------------------------
+// Kernel launchers (defined in the .cu files)
+// ---------------------------------------------------------------------------
+struct TpsDev {  // thin-plate constants for device evaluation
+  const double* kn = nullptr;  // k x 2
+  const double* z = nullptr;   // k x (k-3)
+  int k = 0;
+  double cx = 0, cy = 0, scale = 1;
+};
+TpsDev upload_tps(Context& c, const ThinPlate& tp);
+void launch_lattice(cudaStream_t s, const TpsDev& t, const double* theta, int nf, const int* gx,
+                    const int* gy, int ncx, int ncy, double* lat, float* latf);
+void launch_exact_fields(cudaStream_t s, const TpsDev& t, const double* theta, int nf, int w, int h,
+                         float* full);
+
+struct SubtractArgs {
+  int w, h;
+  const float* sci;
+  const float* ref;
+  const uint8_t* ref_mask;
+  DevFields F;
+  int n_max, ks, nc;
+  const float* taps;  // device (n_max+1)*ks
+  const int* ord;     // unused placeholder
+  const float* fill;  // device scalar (reference fill value)
+  float* diff;
+};
+void launch_model_convolve(cudaStream_t s, const SubtractArgs& a, const Basis& b);
+void launch_variance(cudaStream_t s, int w, int h, const DevFields& F, const float* phi, int rk,
+                     int nc, const float* var_s, const float* var_r, float* var_out);
+void launch_mask(cudaStream_t s, int w, int h, const float* sci, const float* ref,
+                 const uint8_t* sm, const uint8_t* rm, double saturation, int r, const float* diff,
+                 uint8_t* mask_out, uint8_t* exact_bad);
+void launch_mask_fill(cudaStream_t s, int64_t n, const uint8_t* mask, const uint8_t* exact_bad,
+                      const float* fill, float* diff, float* var);
+void launch_model_convolve_orders(cudaStream_t s, const SubtractArgs& a, const int2* orders, bool stack);
+void launch_photometric_scale(cudaStream_t s, const DevFields& F, const float* sums, int nc, float* out);
+
+// Upper median (element size/2 of the sorted sample) of values[7j] that pass a
+// predicate, via radix select. Result written to a device float.
+enum SampleKind { kSampleReference = 0, kSampleDifference = 1 };
+void launch_strided_median(Context& c, int kind, int64_t n, const float* values, const uint8_t* mask,
+                           float* d_result);
+
+void launch_matched_filter(cudaStream_t s, int w, int h, const float* img, const float* var,
+                           const float* psf_host, const float* psf_dev, int ps, float sumpsf2,
+                           float* out);
+
+void launch_basis_convolve(cudaStream_t s, int w, int h, const float* img, const Basis& b,
+                           const float* taps, float* out);
+
+// Catalog (k_ccl.cu)
+struct CatalogDevResult;
+int run_catalog(Context& c, int w, int h, const float* score, const float* diff,
+                const uint8_t* mask, const dgpu_catalog_params& p, const float* variance,
+                const float* psf, int psf_size, const double* bright_x, const double* bright_y,
+                int n_bright);
+
+}  // namespace dgpu

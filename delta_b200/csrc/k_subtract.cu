@@ -1,0 +1,689 @@
+// Full-frame subtraction kernels (sm_100a, FP32 SIMT):
+//   * thin-plate field lattice / exact fields (FP64),
+//   * fused tile model convolve D = S - b - sum_n a_n (g_ny *_y (g_nx *_x R~)),
+//   * block-effective variance K^2 (x) Var(R) + Var(S),
+//   * mask growth (separable OR dilation in shared memory) and exact-bad fill,
+//   * radix-select upper median of a stride-7 sample (fill values).
+// Reference: src/subtract.cpp:20-966.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "dev_common.cuh"
+
+namespace dgpu {
+
+// ---------------------------------------------------------------------------
+// Thin-plate fields
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ double tps_green_d(double r2) { return r2 <= 0.0 ? 0.0 : 0.5 * r2 * log(r2); }
+
+// fields(p, f) = design(p) . theta[f*k:(f+1)*k], design = [sigma Z | 1 | u | v]
+// (src/spatial.cpp:67-97, src/subtract.cpp:58-63).
+__device__ void eval_fields_at(const TpsDev t, const double* __restrict__ theta, int nf, double x,
+                               double y, double* out /* nf */) {
+  constexpr int kMaxK = 64;
+  double d[kMaxK];
+  const int k = t.k, nr = k - 3;
+  const double ux = (x - t.cx) / t.scale, uy = (y - t.cy) / t.scale;
+  for (int m = 0; m < nr; ++m) d[m] = 0.0;
+  for (int j = 0; j < k; ++j) {
+    const double dx = ux - t.kn[2 * j], dy = uy - t.kn[2 * j + 1];
+    const double s = tps_green_d(dx * dx + dy * dy);
+    for (int m = 0; m < nr; ++m) d[m] = fma(s, t.z[j * nr + m], d[m]);
+  }
+  d[nr] = 1.0;
+  d[nr + 1] = ux;
+  d[nr + 2] = uy;
+  for (int f = 0; f < nf; ++f) {
+    double acc = 0.0;
+    const double* th = theta + static_cast<size_t>(f) * k;
+    for (int m = 0; m < k; ++m) acc = fma(d[m], th[m], acc);
+    out[f] = acc;
+  }
+}
+
+__global__ void k_lattice(TpsDev t, const double* __restrict__ theta, int nf,
+                          const int* __restrict__ gx, const int* __restrict__ gy, int ncx, int ncy,
+                          double* __restrict__ lat, float* __restrict__ latf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ncx * ncy) return;
+  const int ix = i % ncx, iy = i / ncx;
+  double f[64];
+  eval_fields_at(t, theta, nf, static_cast<double>(gx[ix]), static_cast<double>(gy[iy]), f);
+  for (int q = 0; q < nf; ++q) {
+    const size_t o = (static_cast<size_t>(q) * ncy + iy) * ncx + ix;
+    lat[o] = f[q];
+    latf[o] = static_cast<float>(f[q]);
+  }
+}
+
+__global__ void k_exact_fields(TpsDev t, const double* __restrict__ theta, int nf, int w, int h,
+                               float* __restrict__ full) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= static_cast<int64_t>(w) * h) return;
+  const int x = static_cast<int>(i % w), y = static_cast<int>(i / w);
+  double f[64];
+  eval_fields_at(t, theta, nf, static_cast<double>(x), static_cast<double>(y), f);
+  for (int q = 0; q < nf; ++q) full[static_cast<size_t>(q) * w * h + i] = static_cast<float>(f[q]);
+}
+
+void launch_lattice(cudaStream_t s, const TpsDev& t, const double* theta, int nf, const int* gx,
+                    const int* gy, int ncx, int ncy, double* lat, float* latf) {
+  const int n = ncx * ncy;
+  k_lattice<<<ceil_div(n, 128), 128, 0, s>>>(t, theta, nf, gx, gy, ncx, ncy, lat, latf);
+  DGPU_LAUNCH("k_lattice");
+}
+
+void launch_exact_fields(cudaStream_t s, const TpsDev& t, const double* theta, int nf, int w, int h,
+                         float* full) {
+  const int64_t n = static_cast<int64_t>(w) * h;
+  k_exact_fields<<<ceil_div(n, 128), 128, 0, s>>>(t, theta, nf, w, h, full);
+  DGPU_LAUNCH("k_exact_fields");
+}
+
+// ---------------------------------------------------------------------------
+// Fused model convolve (src/subtract.cpp:466-639).
+//
+// One CTA per 64 x TH output tile. The sanitised reference window (tile + kh
+// halo, masked / non-finite -> fill, off-frame -> 0) is staged in shared
+// memory; the NX = n_max+1 shared x-passes are computed into shared memory for
+// the tile rows plus the y halo (each thread: 4 columns x all nx, sliding a
+// 4-wide register window so every staged value is loaded once per tap); the
+// y-pass of every component then runs out of shared memory with each thread
+// holding 8 output rows of one column in registers (again a sliding window),
+// and a_n / b are blended from the coarse lattice in registers. Per output
+// pixel the accumulation order is the reference's: x taps j = 0..ks-1, then
+// components in basis order, each y tap j ascending, d -= a_n * bn (FMA).
+// Off-frame rows of the x-pass buffer are exact zeros, which leaves every
+// clipped y sum bit-identical to the reference's jmin/jmax loop.
+// ---------------------------------------------------------------------------
+
+constexpr int kMcTW = 64;   // tile width (columns)
+constexpr int kMcRPT = 8;   // output rows per thread in the y pass
+constexpr int kMcXPT = 4;   // output columns per thread in the x pass
+
+struct McSmem {
+  int nrows, gbw_pad, lat_nx, lat_ny, cx0, cy0;
+};
+
+template <int NX, bool STACK>
+__global__ void __launch_bounds__(256)
+k_model_convolve(int w, int h, const float* __restrict__ sci, const float* __restrict__ ref,
+                 const uint8_t* __restrict__ rmask, DevFields F, const float* __restrict__ taps,
+                 const int2* __restrict__ orders, int ks, int nc, const float* __restrict__ fillp,
+                 float* __restrict__ diff, int TH) {
+  // STACK == true is delta::basis_convolve (src/convolve.cpp:90-113): the raw
+  // image (no sanitising), every component's B_n written to diff[n*h*w + ...].
+  extern __shared__ __align__(16) float smem[];
+  const int kh = (ks - 1) / 2;
+  const int nrows = TH + 2 * kh;
+  const int gbw = kMcTW + 2 * kh;
+  const int gbw_pad = (gbw + 3) & ~3;
+  float* rtile = smem;                                       // nrows x gbw_pad
+  float* txs = rtile + nrows * gbw_pad;                      // NX x nrows x 64
+  float* ktaps = txs + NX * nrows * kMcTW;                   // NX x ks
+  const int bx = blockIdx.x * kMcTW, by = blockIdx.y * TH;
+  const float fill = STACK ? 0.0f : *fillp;
+  const int tid = threadIdx.x;
+
+  for (int i = tid; i < NX * ks; i += blockDim.x) ktaps[i] = taps[i];
+  for (int i = tid; i < nrows * gbw; i += blockDim.x) {
+    const int r = i / gbw, c = i - r * gbw;
+    const int gy = by - kh + r, gx = bx - kh + c;
+    float v = 0.0f;
+    if (gy >= 0 && gy < h && gx >= 0 && gx < w) {
+      const size_t idx = static_cast<size_t>(gy) * w + gx;
+      v = __ldg(ref + idx);
+      if (!STACK) {
+        const bool bad = (rmask && __ldg(rmask + idx) != 0) || !isfinite(v);
+        if (bad) v = fill;
+      }
+    }
+    rtile[r * gbw_pad + c] = v;
+  }
+  __syncthreads();
+
+  // ---- x pass: txs[nx][r][lx] = sum_j k[nx][j] * R~[y][x + kh - j] ----
+  const int ngrp = kMcTW / kMcXPT;
+  for (int it = tid; it < nrows * ngrp; it += blockDim.x) {
+    const int r = it / ngrp, cg = it - r * ngrp;
+    const int gy = by - kh + r;
+    const int c0 = cg * kMcXPT;
+    float acc[NX][kMcXPT];
+#pragma unroll
+    for (int q = 0; q < NX; ++q)
+#pragma unroll
+      for (int i = 0; i < kMcXPT; ++i) acc[q][i] = 0.0f;
+    if (gy >= 0 && gy < h) {
+      const float* row = rtile + r * gbw_pad + c0 + 2 * kh;  // column of tap j=0, output 0
+      float win[kMcXPT];
+#pragma unroll
+      for (int i = 0; i < kMcXPT; ++i) win[i] = row[i];
+      for (int j = 0; j < ks; ++j) {
+        if (j > 0) {
+#pragma unroll
+          for (int i = kMcXPT - 1; i > 0; --i) win[i] = win[i - 1];
+          win[0] = row[-j];
+        }
+#pragma unroll
+        for (int q = 0; q < NX; ++q) {
+          const float kc = ktaps[q * ks + j];
+#pragma unroll
+          for (int i = 0; i < kMcXPT; ++i) acc[q][i] = __fmaf_rn(kc, win[i], acc[q][i]);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NX; ++q) {
+      float4 v = make_float4(acc[q][0], acc[q][1], acc[q][2], acc[q][3]);
+      *reinterpret_cast<float4*>(txs + (q * nrows + r) * kMcTW + c0) = v;
+    }
+  }
+  __syncthreads();
+
+  // ---- y pass + field blend, 8 rows of one column per thread ----
+  const int lx = tid % kMcTW;
+  const int ly0 = (tid / kMcTW) * kMcRPT;
+  if (ly0 >= TH) return;
+  const int x = bx + lx;
+  const bool xin = x < w;
+  const int xc = xin ? x : w - 1;
+  float d[kMcRPT];
+  // Coarse-cell coordinates of this column / these rows.
+  int jx = 0;
+  float wxv = 0.0f;
+  int jy[kMcRPT];
+  float fy[kMcRPT];
+  if (!STACK && !F.exact) {
+    jx = F.cellx[xc];
+    wxv = F.wx[xc];
+  }
+#pragma unroll
+  for (int i = 0; i < kMcRPT; ++i) {
+    const int y = min(by + ly0 + i, h - 1);
+    if (!STACK && !F.exact) {
+      jy[i] = F.celly[y];
+      fy[i] = F.wy[y];
+    } else {
+      jy[i] = 0;
+      fy[i] = 0.0f;
+    }
+  }
+  auto field = [&](int f, int i) -> float {
+    const int y = min(by + ly0 + i, h - 1);
+    if (F.exact) return __ldg(F.full + (static_cast<size_t>(f) * h + y) * w + xc);
+    const float* c0 = F.latf + (static_cast<size_t>(f) * F.ncy + jy[i]) * F.ncx + jx;
+    const float* c1 = c0 + F.ncx;
+    return cell_blend(__ldg(c0), __ldg(c0 + 1), __ldg(c1), __ldg(c1 + 1), fy[i], wxv);
+  };
+  if (!STACK) {
+#pragma unroll
+    for (int i = 0; i < kMcRPT; ++i) {
+      const int y = min(by + ly0 + i, h - 1);
+      d[i] = __ldg(sci + static_cast<size_t>(y) * w + xc) - field(nc, i);
+    }
+  }
+  for (int n = 0; n < nc; ++n) {
+    const int2 o = orders[n];
+    const float* col = txs + static_cast<size_t>(o.x) * nrows * kMcTW + lx;
+    const float* ky = ktaps + o.y * ks;
+    // output row ly0+i needs buffer row ly0 + i + 2kh - j.
+    const int base = ly0 + 2 * kh;
+    float win[kMcRPT];
+#pragma unroll
+    for (int i = 0; i < kMcRPT; ++i) win[i] = col[(base + i) * kMcTW];
+    float bn[kMcRPT];
+#pragma unroll
+    for (int i = 0; i < kMcRPT; ++i) bn[i] = 0.0f;
+    for (int j = 0; j < ks; ++j) {
+      if (j > 0) {
+#pragma unroll
+        for (int i = kMcRPT - 1; i > 0; --i) win[i] = win[i - 1];
+        win[0] = col[(base - j) * kMcTW];
+      }
+      const float c = ky[j];
+#pragma unroll
+      for (int i = 0; i < kMcRPT; ++i) bn[i] = __fmaf_rn(c, win[i], bn[i]);
+    }
+    if (STACK) {
+      if (xin) {
+#pragma unroll
+        for (int i = 0; i < kMcRPT; ++i) {
+          const int y = by + ly0 + i;
+          if (y < h) diff[(static_cast<size_t>(n) * h + y) * w + x] = bn[i];
+        }
+      }
+      continue;
+    }
+#pragma unroll
+    for (int i = 0; i < kMcRPT; ++i) d[i] = __fmaf_rn(-field(n, i), bn[i], d[i]);
+  }
+  if (STACK) return;
+  if (xin) {
+#pragma unroll
+    for (int i = 0; i < kMcRPT; ++i) {
+      const int y = by + ly0 + i;
+      if (y < h) diff[static_cast<size_t>(y) * w + x] = d[i];
+    }
+  }
+}
+
+template <int NX, bool STACK>
+static void launch_mc(cudaStream_t s, const SubtractArgs& a, const int2* orders, int TH, size_t smem) {
+  auto kern = k_model_convolve<NX, STACK>;
+  DGPU_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  dim3 grid(ceil_div(a.w, kMcTW), ceil_div(a.h, TH));
+  const int threads = kMcTW * (TH / kMcRPT);
+  kern<<<grid, threads, smem, s>>>(a.w, a.h, a.sci, a.ref, a.ref_mask, a.F, a.taps, orders, a.ks,
+                                   a.nc, a.fill, a.diff, TH);
+  DGPU_LAUNCH("k_model_convolve");
+}
+
+size_t model_convolve_smem(int nx, int ks, int TH) {
+  const int kh = (ks - 1) / 2;
+  const int nrows = TH + 2 * kh;
+  const int gbw_pad = ((kMcTW + 2 * kh) + 3) & ~3;
+  return sizeof(float) * (static_cast<size_t>(nrows) * gbw_pad + static_cast<size_t>(nx) * nrows * kMcTW +
+                          static_cast<size_t>(nx) * ks);
+}
+
+void launch_model_convolve_orders(cudaStream_t s, const SubtractArgs& a, const int2* orders, bool stack) {
+  const int nx = a.n_max + 1;
+  int TH = 32;
+  const size_t kMaxSmem = 200 * 1024;
+  while (TH > 8 && model_convolve_smem(nx, a.ks, TH) > kMaxSmem) TH /= 2;
+  const size_t smem = model_convolve_smem(nx, a.ks, TH);
+  if (smem > kMaxSmem) fail(DGPU_ERR_INVALID, "subtract: kernel footprint too large for the tile engine");
+  switch (nx) {
+    case 1: stack ? launch_mc<1, true>(s, a, orders, TH, smem) : launch_mc<1, false>(s, a, orders, TH, smem); break;
+    case 2: stack ? launch_mc<2, true>(s, a, orders, TH, smem) : launch_mc<2, false>(s, a, orders, TH, smem); break;
+    case 3: stack ? launch_mc<3, true>(s, a, orders, TH, smem) : launch_mc<3, false>(s, a, orders, TH, smem); break;
+    case 4: stack ? launch_mc<4, true>(s, a, orders, TH, smem) : launch_mc<4, false>(s, a, orders, TH, smem); break;
+    case 5: stack ? launch_mc<5, true>(s, a, orders, TH, smem) : launch_mc<5, false>(s, a, orders, TH, smem); break;
+    case 6: stack ? launch_mc<6, true>(s, a, orders, TH, smem) : launch_mc<6, false>(s, a, orders, TH, smem); break;
+    case 7: stack ? launch_mc<7, true>(s, a, orders, TH, smem) : launch_mc<7, false>(s, a, orders, TH, smem); break;
+    case 8: stack ? launch_mc<8, true>(s, a, orders, TH, smem) : launch_mc<8, false>(s, a, orders, TH, smem); break;
+    case 9: stack ? launch_mc<9, true>(s, a, orders, TH, smem) : launch_mc<9, false>(s, a, orders, TH, smem); break;
+    case 10: stack ? launch_mc<10, true>(s, a, orders, TH, smem) : launch_mc<10, false>(s, a, orders, TH, smem); break;
+    case 11: stack ? launch_mc<11, true>(s, a, orders, TH, smem) : launch_mc<11, false>(s, a, orders, TH, smem); break;
+    default: fail(DGPU_ERR_INVALID, "subtract: n_max above 10 is not supported by the tile engine");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Variance propagation (src/subtract.cpp:641-824): per 64x64 block, K frozen at
+// the block centre, squared and mirrored, footprint shrunk to the centred box
+// holding (1 - 1e-4f) of sum K^2, flat-window shortcut Q * Var(R) when the
+// window's (max - min) <= 1e-3f * max, otherwise the dense correlation in
+// (ly, lx) tap order; then + Var(S).
+// ---------------------------------------------------------------------------
+
+constexpr int kVarB = 64;
+
+__global__ void __launch_bounds__(256)
+k_variance(int w, int h, DevFields F, const float* __restrict__ phi, int rk, int nc,
+           const float* __restrict__ var_s, const float* __restrict__ var_r,
+           float* __restrict__ var_out) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int ks = 2 * rk + 1;
+  const int kk = ks * ks;
+  const int iw = kVarB + 2 * rk;
+  float* kf = reinterpret_cast<float*>(smraw);        // kk, mirrored K^2
+  float* k1 = kf + kk;                                // kk, K (unsquared)
+  float* win = k1 + kk;                               // iw * iw
+  float* an = win + iw * iw;                          // nc
+  __shared__ double s_qsum;
+  __shared__ int s_hw;
+  __shared__ float s_min[8], s_max[8];
+  const int tid = threadIdx.x;
+  const int bx = blockIdx.x * kVarB, by = blockIdx.y * kVarB;
+  const int bw = min(kVarB, w - bx), bh = min(kVarB, h - by);
+
+  if (var_r != nullptr) {
+    const int cpx = min(bx + bw / 2, w - 1), cpy = min(by + bh / 2, h - 1);
+    for (int n = tid; n < nc; n += blockDim.x) an[n] = field_point(F, n, cpx, cpy);
+    __syncthreads();
+    // K at the block centre, squared, mirrored: kf[kk-1-i] = K[i]^2.
+    for (int i = tid; i < kk; i += blockDim.x) {
+      float k2 = 0.0f;
+      for (int n = 0; n < nc; ++n) k2 = __fmaf_rn(an[n], __ldg(phi + static_cast<size_t>(n) * kk + i), k2);
+      k1[i] = k2;
+      kf[kk - 1 - i] = k2 * k2;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      // qsum = sum_i double(K_i) * double(K_i) in index order (exact squares).
+      double q = 0.0;
+      for (int i = 0; i < kk; ++i) q = fma(static_cast<double>(k1[i]), static_cast<double>(k1[i]), q);
+      s_qsum = q;
+    }
+    __syncthreads();
+    // Box shrink: lane L of warp 0 tests half-width L; the first box that
+    // reaches the target wins. Each box is summed in the reference's row-major
+    // order.
+    if (tid < 32) {
+      const double target = (1.0 - static_cast<double>(1e-4f)) * s_qsum;
+      int found = rk;
+      for (int base = 0; base < rk; base += 32) {
+        const int hw = base + tid;
+        bool ok = false;
+        if (hw < rk) {
+          double box = 0.0;
+          const int lo = rk - hw, hi = rk + hw;
+          for (int yy = lo; yy <= hi; ++yy)
+            for (int xx = lo; xx <= hi; ++xx) box += static_cast<double>(kf[yy * ks + xx]);
+          ok = box >= target;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, ok);
+        if (bal) {
+          found = base + __ffs(bal) - 1;
+          break;
+        }
+      }
+      if (tid == 0) s_hw = found;
+    }
+    // Gather the zero-padded window and its min / max.
+    float lmin = INFINITY, lmax = -INFINITY;
+    const int iwh = bh + 2 * rk, iww = bw + 2 * rk;
+    for (int i = tid; i < iwh * iww; i += blockDim.x) {
+      const int r = i / iww, c = i - r * iww;
+      const int gy = by - rk + r, gx = bx - rk + c;
+      const float v = (gy < 0 || gy >= h || gx < 0 || gx >= w) ? 0.0f : __ldg(var_r + static_cast<size_t>(gy) * w + gx);
+      win[r * iw + c] = v;
+      lmin = fminf(lmin, v);
+      lmax = fmaxf(lmax, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      lmin = fminf(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
+      lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    }
+    if ((tid & 31) == 0) {
+      s_min[tid >> 5] = lmin;
+      s_max[tid >> 5] = lmax;
+    }
+    __syncthreads();
+    float wmin = s_min[0], wmax = s_max[0];
+    for (int i = 1; i < (int)(blockDim.x >> 5); ++i) {
+      wmin = fminf(wmin, s_min[i]);
+      wmax = fmaxf(wmax, s_max[i]);
+    }
+    const int hw = s_hw;
+    const bool flat = wmax > 0.0f && (wmax - wmin) <= 1e-3f * wmax;
+    const float q = static_cast<float>(s_qsum);
+    const int lo = rk - hw, hi = rk + hw;
+    for (int p = tid; p < bw * bh; p += blockDim.x) {
+      const int oy = p / bw, ox = p - oy * bw;
+      float v;
+      if (flat) {
+        v = q * win[(oy + rk) * iw + ox + rk];
+      } else {
+        float acc = 0.0f;
+        for (int ly = lo; ly <= hi; ++ly) {
+          const float* wr = win + (oy + ly) * iw + ox;
+          const float* kr = kf + ly * ks;
+          for (int lx2 = lo; lx2 <= hi; ++lx2) {
+            const float c = kr[lx2];
+            if (c == 0.0f) continue;
+            acc = __fmaf_rn(c, wr[lx2], acc);
+          }
+        }
+        v = 0.0f + acc;
+      }
+      const size_t o = static_cast<size_t>(by + oy) * w + bx + ox;
+      if (var_s) v = v + __ldg(var_s + o);
+      var_out[o] = v;
+    }
+  } else {
+    for (int p = tid; p < bw * bh; p += blockDim.x) {
+      const int oy = p / bw, ox = p - oy * bw;
+      const size_t o = static_cast<size_t>(by + oy) * w + bx + ox;
+      var_out[o] = 0.0f + __ldg(var_s + o);
+    }
+  }
+}
+
+void launch_variance(cudaStream_t s, int w, int h, const DevFields& F, const float* phi, int rk,
+                     int nc, const float* var_s, const float* var_r, float* var_out) {
+  const int ks = 2 * rk + 1;
+  const int iw = kVarB + 2 * rk;
+  const size_t smem = sizeof(float) * (2 * static_cast<size_t>(ks) * ks + static_cast<size_t>(iw) * iw + nc + 4);
+  if (smem > 200 * 1024) fail(DGPU_ERR_INVALID, "subtract: kernel radius too large for the variance engine");
+  DGPU_CUDA(cudaFuncSetAttribute(k_variance, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  dim3 grid(ceil_div(w, kVarB), ceil_div(h, kVarB));
+  k_variance<<<grid, 256, smem, s>>>(w, h, F, phi, rk, nc, var_s, var_r, var_out);
+  DGPU_LAUNCH("k_variance");
+}
+
+// ---------------------------------------------------------------------------
+// Mask growth (src/subtract.cpp:826-914): science-side flags 1:1, reference
+// flags and saturated reference pixels OR-dilated by r (box), edge border r,
+// non-finite difference. One CTA per 32x32 tile with the (32+2r)^2 grow window
+// built on the fly in shared memory (x-dilate, then y-dilate).
+// exact_bad records the undilated garbage pixels for the fill pass.
+// ---------------------------------------------------------------------------
+
+constexpr int kMkT = 32;
+
+__global__ void __launch_bounds__(256)
+k_mask(int w, int h, const float* __restrict__ sci, const float* __restrict__ ref,
+       const uint8_t* __restrict__ sm, const uint8_t* __restrict__ rm, int has_sat, float sat, int r,
+       const float* __restrict__ diff, uint8_t* __restrict__ mask_out, uint8_t* __restrict__ exact_bad) {
+  extern __shared__ uint8_t msm[];
+  const int gw = kMkT + 2 * r;
+  uint8_t* g = msm;              // gw x gw grow sources
+  uint8_t* gxr = g + gw * gw;    // gw rows x 32 cols after the x dilation
+  const int bx = blockIdx.x * kMkT, by = blockIdx.y * kMkT;
+  const int tid = threadIdx.x;
+  const bool need_grow = (rm != nullptr) || has_sat;
+  if (need_grow) {
+    for (int i = tid; i < gw * gw; i += blockDim.x) {
+      const int yy = i / gw, xx = i - yy * gw;
+      const int gy = by - r + yy, gx = bx - r + xx;
+      uint8_t v = 0;
+      if (gy >= 0 && gy < h && gx >= 0 && gx < w) {
+        const size_t idx = static_cast<size_t>(gy) * w + gx;
+        if (rm) v |= rm[idx];
+        if (has_sat && ref[idx] >= sat) v |= 2;
+      }
+      g[i] = v;
+    }
+    __syncthreads();
+    for (int i = tid; i < gw * kMkT; i += blockDim.x) {
+      const int yy = i / kMkT, xx = i - yy * kMkT;
+      uint8_t acc = 0;
+      for (int d = 0; d <= 2 * r; ++d) acc |= g[yy * gw + xx + d];
+      gxr[i] = acc;
+    }
+    __syncthreads();
+  }
+  for (int i = tid; i < kMkT * kMkT; i += blockDim.x) {
+    const int ly = i / kMkT, lx = i - ly * kMkT;
+    const int x = bx + lx, y = by + ly;
+    if (x >= w || y >= h) continue;
+    const size_t idx = static_cast<size_t>(y) * w + x;
+    uint8_t m = 0;
+    uint8_t eb = 0;
+    if (sm && sm[idx]) {
+      m |= sm[idx];
+      eb = 1;
+    }
+    if (rm && rm[idx]) eb = 1;
+    if (has_sat) {
+      if (ref[idx] >= sat) eb = 1;
+      if (sci[idx] >= sat) {
+        m |= 2;
+        eb = 1;
+      }
+    }
+    if (need_grow) {
+      uint8_t acc = 0;
+      for (int d = 0; d <= 2 * r; ++d) acc |= gxr[(ly + d) * kMkT + lx];
+      m |= acc;
+    }
+    if (x < r || x >= w - r || y < r || y >= h - r) m |= 16;
+    if (!isfinite(diff[idx])) {
+      m |= 8;
+      eb = 1;
+    }
+    mask_out[idx] = m;
+    exact_bad[idx] = eb;
+  }
+}
+
+void launch_mask(cudaStream_t s, int w, int h, const float* sci, const float* ref,
+                 const uint8_t* sm, const uint8_t* rm, double saturation, int r, const float* diff,
+                 uint8_t* mask_out, uint8_t* exact_bad) {
+  const int gw = kMkT + 2 * r;
+  const size_t smem = static_cast<size_t>(gw) * gw + static_cast<size_t>(gw) * kMkT;
+  if (smem > 200 * 1024) fail(DGPU_ERR_INVALID, "subtract: kernel radius too large for mask growth");
+  DGPU_CUDA(cudaFuncSetAttribute(k_mask, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  dim3 grid(ceil_div(w, kMkT), ceil_div(h, kMkT));
+  const int has_sat = saturation > 0.0 ? 1 : 0;
+  k_mask<<<grid, 256, smem, s>>>(w, h, sci, ref, sm, rm, has_sat, static_cast<float>(saturation), r,
+                                 diff, mask_out, exact_bad);
+  DGPU_LAUNCH("k_mask");
+}
+
+__global__ void k_mask_fill(int64_t n, const uint8_t* __restrict__ mask,
+                            const uint8_t* __restrict__ exact_bad, const float* __restrict__ fillp,
+                            float* __restrict__ diff, float* __restrict__ var) {
+  const float fill = *fillp;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    if (mask[i] != 0 && exact_bad[i]) {
+      diff[i] = fill;
+      if (var) var[i] = 0.0f;
+    }
+  }
+}
+
+void launch_mask_fill(cudaStream_t s, int64_t n, const uint8_t* mask, const uint8_t* exact_bad,
+                      const float* fill, float* diff, float* var) {
+  const int blocks = static_cast<int>(std::min<int64_t>(ceil_div(n, 256), 148 * 16));
+  k_mask_fill<<<blocks, 256, 0, s>>>(n, mask, exact_bad, fill, diff, var);
+  DGPU_LAUNCH("k_mask_fill");
+}
+
+// ---------------------------------------------------------------------------
+// Upper median of a stride-7 sample by exact radix select (8 bits per pass over
+// the monotone uint32 key). Matches std::nth_element(size/2) on the sample
+// (src/subtract.cpp:20-51 for the reference fill, 915-945 for the difference
+// fill). An empty sample yields 0.
+// ---------------------------------------------------------------------------
+
+struct SelectState {
+  unsigned int count;   // sample size
+  unsigned int rank;    // remaining rank within the current prefix bucket
+  unsigned int prefix;  // key bits fixed so far
+  unsigned int hist[256];
+};
+
+__global__ void k_compact_samples(int kind, int64_t n, const float* __restrict__ v,
+                                  const uint8_t* __restrict__ mask, uint32_t* __restrict__ keys,
+                                  SelectState* st) {
+  const int64_t nsamp = (n + 6) / 7;
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < nsamp;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = 7 * j;
+    const float x = v[i];
+    const bool ok = isfinite(x) && (mask == nullptr || mask[i] == 0);
+    // kind 0 (reference): good finite reference pixels; kind 1 (difference):
+    // unmasked finite difference pixels (mask is the grown output mask).
+    (void)kind;
+    const unsigned bal = __ballot_sync(__activemask(), ok);
+    if (bal == 0) continue;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(bal) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(&st->count, __popc(bal));
+    base = __shfl_sync(__activemask(), base, leader);
+    if (ok) keys[base + __popc(bal & ((1u << lane) - 1))] = float_key(x);
+  }
+}
+
+__global__ void k_select_init(SelectState* st) {
+  st->rank = st->count / 2;
+  st->prefix = 0;
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) st->hist[i] = 0;
+}
+
+__global__ void k_select_hist(const uint32_t* __restrict__ keys, SelectState* st, int shift) {
+  __shared__ unsigned hist[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+  __syncthreads();
+  const unsigned count = st->count;
+  const unsigned prefix = st->prefix;
+  const unsigned himask = shift >= 24 ? 0u : (0xffffffffu << (shift + 8));
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const uint32_t k = keys[i];
+    if ((k & himask) == (prefix & himask)) atomicAdd(&hist[(k >> shift) & 0xffu], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 256; i += blockDim.x)
+    if (hist[i]) atomicAdd(&st->hist[i], hist[i]);
+}
+
+__global__ void k_select_pick(SelectState* st, int shift, float* result, int last) {
+  if (threadIdx.x != 0) return;
+  unsigned rank = st->rank, cum = 0;
+  int digit = 255;
+  for (int d = 0; d < 256; ++d) {
+    if (rank < cum + st->hist[d]) {
+      digit = d;
+      break;
+    }
+    cum += st->hist[d];
+  }
+  st->rank = rank - cum;
+  st->prefix |= static_cast<unsigned>(digit) << shift;
+  for (int d = 0; d < 256; ++d) st->hist[d] = 0;
+  if (last) *result = st->count ? key_float(st->prefix) : 0.0f;
+}
+
+void launch_strided_median(Context& c, int kind, int64_t n, const float* values, const uint8_t* mask,
+                           float* d_result) {
+  cudaStream_t s = c.stream;
+  const int64_t nsamp = (n + 6) / 7;
+  auto* st = static_cast<SelectState*>(c.slot(kSlotSelect, sizeof(SelectState)));
+  auto* keys = static_cast<uint32_t*>(c.slot(kSlotSamples, sizeof(uint32_t) * std::max<int64_t>(nsamp, 1)));
+  DGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(SelectState), s));
+  const int blocks = static_cast<int>(std::min<int64_t>(ceil_div(std::max<int64_t>(nsamp, 1), 256), 148 * 8));
+  k_compact_samples<<<blocks, 256, 0, s>>>(kind, n, values, mask, keys, st);
+  DGPU_LAUNCH("k_compact_samples");
+  k_select_init<<<1, 256, 0, s>>>(st);
+  DGPU_LAUNCH("k_select_init");
+  const int hb = static_cast<int>(std::min<int64_t>(ceil_div(std::max<int64_t>(nsamp, 1), 1024), 148 * 2));
+  for (int pass = 0; pass < 4; ++pass) {
+    const int shift = 24 - 8 * pass;
+    k_select_hist<<<hb, 256, 0, s>>>(keys, st, shift);
+    DGPU_LAUNCH("k_select_hist");
+    k_select_pick<<<1, 32, 0, s>>>(st, shift, d_result, pass == 3);
+    DGPU_LAUNCH("k_select_pick");
+  }
+}
+
+// photometric_scale (src/fit.cpp:513-530): out = sum_c float(S_c) * a_c in
+// component order, fused.
+__global__ void k_photometric_scale(DevFields F, const float* __restrict__ sums, int nc,
+                                    float* __restrict__ out) {
+  const int64_t n = static_cast<int64_t>(F.w) * F.h;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int x = static_cast<int>(i % F.w), y = static_cast<int>(i / F.w);
+    float acc = 0.0f;
+    for (int q = 0; q < nc; ++q) acc = __fmaf_rn(sums[q], field_point(F, q, x, y), acc);
+    out[i] = acc;
+  }
+}
+
+void launch_photometric_scale(cudaStream_t s, const DevFields& F, const float* sums, int nc, float* out) {
+  const int64_t n = static_cast<int64_t>(F.w) * F.h;
+  const int blocks = static_cast<int>(std::min<int64_t>(ceil_div(n, 256), 148 * 16));
+  k_photometric_scale<<<blocks, 256, 0, s>>>(F, sums, nc, out);
+  DGPU_LAUNCH("k_photometric_scale");
+}
+
+}  // namespace dgpu

@@ -1,0 +1,157 @@
+// Host runtime of libdelta_gpu.so: errors, context, workspace slots, staging,
+// device-event stage timers, device field set-up.
+#include <cuda_runtime.h>
+
+#include <cstdlib>
+#include <stdexcept>
+
+#include "internal.h"
+
+namespace dgpu {
+
+
+void fail(int code, const std::string& msg) { throw Failure(code, msg); }
+
+void check_cuda(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) fail(DGPU_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void* Context::slot(Slot s, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (slot_size[s] >= bytes) return slot_ptr[s];
+  // Growing: the stream may still read the old buffer.
+  if (slot_ptr[s]) {
+    DGPU_CUDA(cudaStreamSynchronize(stream));
+    DGPU_CUDA(cudaFree(slot_ptr[s]));
+    slot_ptr[s] = nullptr;
+    slot_size[s] = 0;
+  }
+  const size_t want = bytes + bytes / 8 + 256;
+  DGPU_CUDA(cudaMalloc(&slot_ptr[s], want));
+  slot_size[s] = want;
+  return slot_ptr[s];
+}
+
+void reset_status(Context& c) { DGPU_CUDA(cudaMemsetAsync(c.d_status, 0, sizeof(unsigned), c.stream)); }
+
+void check_status(Context& c) {
+  unsigned st = 0;
+  DGPU_CUDA(cudaMemcpyAsync(&st, c.d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, c.stream));
+  DGPU_CUDA(cudaStreamSynchronize(c.stream));
+  if (st & kStatusLoopLimit) fail(DGPU_ERR_LIMIT, "a device loop hit its iteration cap");
+  if (st & kStatusBounds) fail(DGPU_ERR_LIMIT, "a device bounds check rejected an access");
+}
+
+StageTimer::StageTimer(Context& ctx, const char* l) : c(ctx), label(l) {
+  if (!c.timing_enabled) return;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, c.stream);
+}
+
+StageTimer::~StageTimer() {
+  if (!c.timing_enabled || !e0) return;
+  cudaEventRecord(e1, c.stream);
+  cudaEventSynchronize(e1);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (auto& kv : c.timing)
+    if (kv.first == label) {
+      kv.second += ms * 1e-3;
+      return;
+    }
+  c.timing.emplace_back(label, ms * 1e-3);
+}
+
+const void* stage_in(Context& c, int mem, const void* p, size_t bytes, Slot s) {
+  if (p == nullptr) return nullptr;
+  if (mem == DGPU_MEM_DEVICE) return p;
+  void* d = c.slot(s, bytes);
+  DGPU_CUDA(cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, c.stream));
+  return d;
+}
+
+void* out_buf(Context& c, int mem, void* p, size_t bytes, Slot s) {
+  if (mem == DGPU_MEM_DEVICE) {
+    if (p == nullptr) fail(DGPU_ERR_INVALID, "missing output buffer");
+    return p;
+  }
+  return c.slot(s, bytes);
+}
+
+void stage_out(Context& c, int mem, void* host, const void* dev, size_t bytes) {
+  if (mem == DGPU_MEM_DEVICE || host == nullptr) return;
+  DGPU_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, c.stream));
+}
+
+TpsDev upload_tps(Context& c, const ThinPlate& tp) {
+  const int k = tp.k, nr = k - 3;
+  std::vector<double> buf(2 * static_cast<size_t>(k) + static_cast<size_t>(k) * std::max(nr, 0));
+  std::copy(tp.kn.begin(), tp.kn.end(), buf.begin());
+  std::copy(tp.z.begin(), tp.z.end(), buf.begin() + 2 * k);
+  double* d = static_cast<double*>(c.slot(kSlotZ, sizeof(double) * buf.size()));
+  DGPU_CUDA(cudaMemcpyAsync(d, buf.data(), sizeof(double) * buf.size(), cudaMemcpyHostToDevice, c.stream));
+  TpsDev t;
+  t.kn = d;
+  t.z = d + 2 * k;
+  t.k = k;
+  t.cx = tp.cx;
+  t.cy = tp.cy;
+  t.scale = tp.scale;
+  return t;
+}
+
+DevFields build_fields_dev(Context& c, const ThinPlate& tp, const double* d_theta, int nf, int w, int h) {
+  if (tp.k > 64) fail(DGPU_ERR_INVALID, "at most 64 knots are supported");
+  if (nf > 64) fail(DGPU_ERR_INVALID, "at most 63 kernel components are supported");
+  const FieldGeom g = make_field_geom(tp, w, h);
+  const TpsDev t = upload_tps(c, tp);
+  DevFields F;
+  F.nf = nf;
+  F.w = w;
+  F.h = h;
+  if (g.exact) {
+    F.exact = 1;
+    float* full = static_cast<float*>(c.slot(kSlotFullFields, sizeof(float) * static_cast<size_t>(nf) * w * h));
+    launch_exact_fields(c.stream, t, d_theta, nf, w, h, full);
+    F.full = full;
+    return F;
+  }
+  F.exact = 0;
+  F.ncx = g.ncx;
+  F.ncy = g.ncy;
+  std::vector<int> ib;
+  ib.insert(ib.end(), g.gx.begin(), g.gx.end());
+  ib.insert(ib.end(), g.gy.begin(), g.gy.end());
+  ib.insert(ib.end(), g.cellx.begin(), g.cellx.end());
+  ib.insert(ib.end(), g.celly.begin(), g.celly.end());
+  std::vector<float> fb;
+  fb.insert(fb.end(), g.wx.begin(), g.wx.end());
+  fb.insert(fb.end(), g.wy.begin(), g.wy.end());
+  int* di = static_cast<int*>(c.slot(kSlotCellX, sizeof(int) * ib.size()));
+  float* df = static_cast<float*>(c.slot(kSlotCellY, sizeof(float) * fb.size()));
+  DGPU_CUDA(cudaMemcpyAsync(di, ib.data(), sizeof(int) * ib.size(), cudaMemcpyHostToDevice, c.stream));
+  DGPU_CUDA(cudaMemcpyAsync(df, fb.data(), sizeof(float) * fb.size(), cudaMemcpyHostToDevice, c.stream));
+  const size_t nl = static_cast<size_t>(nf) * g.ncx * g.ncy;
+  double* lat = static_cast<double*>(c.slot(kSlotLattice, sizeof(double) * nl));
+  float* latf = static_cast<float*>(c.slot(kSlotLatticeF, sizeof(float) * nl));
+  launch_lattice(c.stream, t, d_theta, nf, di, di + g.ncx, g.ncx, g.ncy, lat, latf);
+  F.lat = lat;
+  F.latf = latf;
+  F.cellx = di + g.ncx + g.ncy;
+  F.celly = di + g.ncx + g.ncy + w;
+  F.wx = df;
+  F.wy = df + w;
+  return F;
+}
+
+DevFields build_fields(Context& c, const ThinPlate& tp, const double* theta, int nf, int w, int h) {
+  const size_t n = static_cast<size_t>(nf) * tp.k;
+  double* d = static_cast<double*>(c.slot(kSlotTheta, sizeof(double) * n));
+  DGPU_CUDA(cudaMemcpyAsync(d, theta, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
+  return build_fields_dev(c, tp, d, nf, w, h);
+}
+
+}  // namespace dgpu

@@ -1,0 +1,200 @@
+/* delta_gpu.h -- C ABI of the B200 (sm_100a) difference-imaging hot path.
+ *
+ * Drop-in boundary for tkillestein/delta 1.1.1: every entry point below
+ * replaces one function of the reference's nanobind module `delta._core`
+ * (src/bindings.cpp) and the C++ core function it wraps; the citation on each
+ * declaration names both. Plain pointers and sizes only; no exceptions cross
+ * this boundary. All functions return an int status (DGPU_OK == 0); the text of
+ * the last failure on a context is available from dgpu_last_error().
+ *
+ * Memory: image arguments are either host or device pointers, chosen per call
+ * by `mem` (DGPU_MEM_HOST: the library stages copies on its stream and
+ * synchronises before returning; DGPU_MEM_DEVICE: pointers are used in place,
+ * work is stream-ordered on the context's stream and the call returns without
+ * a final synchronisation unless the algorithm itself needs a host decision).
+ * Images are row-major float32 (index y*width + x), masks uint8 bit flags
+ * (src/../include/delta/image.hpp:14-22), optional layers are NULL.
+ *
+ * Threading: one context per host thread; calls on a context are serialised on
+ * its stream.
+ */
+#ifndef DELTA_GPU_H_
+#define DELTA_GPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define DGPU_OK 0
+#define DGPU_ERR_INVALID 1   /* bad argument / shape: the reference's invalid_argument, shape runtime_error */
+#define DGPU_ERR_RUNTIME 2   /* algorithmic failure the reference reports as runtime_error */
+#define DGPU_ERR_CUDA 3      /* CUDA runtime error */
+#define DGPU_ERR_LIMIT 4     /* a device loop hit its iteration cap (no spin, no trap) */
+#define DGPU_ERR_CAPACITY 5  /* caller buffer too small; the needed size was written back */
+#define DGPU_ERR_NO_DEVICE 6 /* no CUDA device / library built without one */
+
+#define DGPU_MEM_HOST 0
+#define DGPU_MEM_DEVICE 1
+
+/* Arithmetic of the normal-equation build in dgpu_fit_kernel / dgpu_solve_*. */
+#define DGPU_PREC_FP64 0  /* FP64 SIMT (accuracy reference) */
+#define DGPU_PREC_FP32 1  /* "plain": FP32 SIMT products and accumulation */
+#define DGPU_PREC_MIXED 2 /* "mixed": BF16x3 split tcgen05 products, FP32 accumulate,
+                             FP64 cross-CTA reduce, Cholesky and one refinement step */
+
+typedef struct dgpu_context dgpu_context;
+
+/* ---- context ------------------------------------------------------------ */
+int dgpu_device_count(int* count);
+int dgpu_create(int device, dgpu_context** out);
+void dgpu_destroy(dgpu_context* ctx);
+/* Run subsequent work on a caller stream (a cudaStream_t); NULL restores the
+ * context's own stream. */
+int dgpu_set_stream(dgpu_context* ctx, void* stream);
+int dgpu_synchronize(dgpu_context* ctx);
+const char* dgpu_last_error(const dgpu_context* ctx);
+/* Per-label device time of the last instrumented call (the reference's
+ * DELTA_TIMING labels, src/timing.cpp:19-46); fills up to `cap` entries and
+ * returns the count through *n. Enabled by DELTA_TIMING=1. */
+int dgpu_drain_timing(dgpu_context* ctx, char (*labels)[64], double* seconds, int cap, int* n);
+
+/* ---- basis (host math) ---------------------------------------------------- */
+/* GaussHermiteBasis::default_radius, src/basis.cpp:9-12. */
+int dgpu_default_radius(double beta, int n_max);
+/* gauss_hermite_basis1d, src/bindings.cpp:171-184 -> src/basis.cpp:14-59.
+ * out: (n_max+1) x (2r+1) float64; radius 0 resolves the default. */
+int dgpu_gauss_hermite_basis1d(double beta, int n_max, int radius, double* out, int* ksize);
+/* gauss_hermite_kernels, src/bindings.cpp:187-206 -> src/basis.cpp:66-79.
+ * orders: nc x 2 int32 (nx, ny); kernels: nc x ks x ks float32. */
+int dgpu_gauss_hermite_kernels(double beta, int n_max, int radius, int32_t* orders,
+                               float* kernels, int* ksize);
+/* component_sums, src/basis.cpp:81-93; out: nc float64. */
+int dgpu_component_sums(double beta, int n_max, int radius, double* out);
+
+/* ---- thin-plate spline (host math) ---------------------------------------- */
+/* grid_knots, src/spatial.cpp:113-129; out: (nx*ny) x 2 float64. */
+int dgpu_grid_knots(double x0, double y0, double x1, double y1, int nx, int ny, double* out);
+/* tps_design, src/bindings.cpp:487-490 -> src/spatial.cpp:67-97. out: m x k. */
+int dgpu_tps_design(const double* knots, int k, const double* points, int64_t m, double* out);
+/* tps_penalty, src/bindings.cpp:492-494 -> src/spatial.cpp:20-65. out: k x k. */
+int dgpu_tps_penalty(const double* knots, int k, double* out);
+/* tps_fit, src/bindings.cpp:496-500 -> src/spatial.cpp:131-140. out: k. */
+int dgpu_tps_fit(const double* knots, int k, const double* points, int64_t m,
+                 const double* values, double lam, double* out);
+/* tps_evaluate, src/bindings.cpp:502-506. out: m. */
+int dgpu_tps_evaluate(const double* knots, int k, const double* points, int64_t m,
+                      const double* coeffs, double* out);
+
+/* ---- kernel model ---------------------------------------------------------- */
+/* A fitted solution: knots (k x 2), theta ((nc+1)*k, ordered
+ * [c_0 | ... | c_{nc-1} | b], src/../include/delta/solve.hpp:12-15), basis. */
+typedef struct {
+  const double* knots; /* host, k x 2 */
+  int n_knots;
+  const double* theta; /* host, n_theta */
+  int64_t n_theta;
+  double beta;
+  int n_max;
+  int radius; /* 0 -> default_radius */
+} dgpu_model;
+
+/* ---- convolution ------------------------------------------------------------ */
+/* basis_convolve, src/bindings.cpp:209-227 -> src/convolve.cpp:90-113.
+ * out: nc x h x w float32. */
+int dgpu_basis_convolve(dgpu_context* ctx, int mem, const float* image, int64_t width,
+                        int64_t height, double beta, int n_max, int radius, float* out);
+
+/* ---- full-frame subtraction -------------------------------------------------- */
+/* subtract, src/bindings.cpp:603-638 -> delta::subtract, src/subtract.cpp:429-966
+ * (include/delta/subtract.hpp:75-78).
+ * out_variance is written when either variance layer is given, out_mask when
+ * either mask is given or saturation > 0 (pass NULL to skip otherwise). The
+ * flags *has_variance / *has_mask report which outputs were produced. */
+int dgpu_subtract(dgpu_context* ctx, int mem, int64_t width, int64_t height,
+                  const float* science, const float* reference, const float* science_var,
+                  const float* reference_var, const uint8_t* science_mask,
+                  const uint8_t* reference_mask, const dgpu_model* model, double saturation,
+                  float* out_difference, float* out_variance, uint8_t* out_mask,
+                  int* has_variance, int* has_mask);
+
+/* photometric_scale, src/bindings.cpp:696-708 -> src/fit.cpp:513-530. out: h x w. */
+int dgpu_photometric_scale(dgpu_context* ctx, int mem, const double* knots, int n_knots,
+                           const double* theta, int64_t n_theta, const double* component_sums,
+                           int nc, int64_t height, int64_t width, float* out);
+/* photometric_scale_at, src/bindings.cpp:711-719 -> src/fit.cpp:532-544. out: m. */
+int dgpu_photometric_scale_at(const double* knots, int n_knots, const double* theta,
+                              int64_t n_theta, const double* component_sums, int nc,
+                              const double* points, int64_t m, double* out);
+
+/* ---- matched filter ---------------------------------------------------------- */
+/* matched_filter, src/bindings.cpp:878-898 -> src/noise.cpp:535-632
+ * (include/delta/noise.hpp:88-93). out: h x w float32. */
+int dgpu_matched_filter(dgpu_context* ctx, int mem, int64_t width, int64_t height,
+                        const float* image, const float* psf, int psf_size,
+                        const float* variance, float* out);
+
+/* ---- catalog ----------------------------------------------------------------- */
+typedef struct {
+  double threshold_sigma;        /* 5.0 */
+  double threshold_sigma_dipole; /* 3.0 */
+  double expected_fwhm;          /* 3.5 */
+  double fwhm_tolerance_lo;      /* 0.3 */
+  double fwhm_tolerance_hi;      /* 3.0 */
+  int aperture_radius;           /* 0 */
+  int exclude_bad_pixels;        /* 1 */
+  int return_negative;           /* 0 */
+  int fit_psf_shape;             /* 0 */
+  double shape_chi2_tolerance;   /* 3.0 */
+  double bright_star_radius;     /* 0.0 */
+  int max_shape_fit;             /* 5000 */
+} dgpu_catalog_params;
+
+/* Column pointers for dgpu_catalog_fetch (host memory, `count` entries each). */
+typedef struct {
+  double* x;
+  double* y;
+  int32_t* peak_x;
+  int32_t* peak_y;
+  double* peak_snr;
+  int32_t* n_pix;
+  double* flux;
+  double* expected_n_pix;
+  double* fwhm_ratio;
+  uint8_t* fwhm_consistent;
+  uint8_t* mask_flags;
+  uint8_t* is_dipole;
+  uint8_t* quality;
+  double* psf_chi2;
+  int32_t* psf_chi2_dof;
+  double* psf_amplitude;
+  double* psf_amplitude_err;
+  uint8_t* shape_consistent;
+  double* bright_star_dist;
+  uint8_t* near_bright_star;
+} dgpu_catalog_columns;
+
+/* build_catalog, src/bindings.cpp:348-483 -> delta::build_catalog,
+ * src/catalog.cpp:600-697 (include/delta/catalog.hpp:117-121).
+ * Labels, reduces and (optionally) enriches on the device; the entries stay in
+ * the context until dgpu_catalog_fetch copies them out. *count receives the
+ * number of entries. variance / psf / bright_* are optional (NULL). */
+int dgpu_build_catalog(dgpu_context* ctx, int mem, int64_t width, int64_t height,
+                       const float* score, const float* difference, const uint8_t* mask,
+                       const dgpu_catalog_params* params, const float* variance,
+                       const float* psf, int psf_size, const double* bright_x,
+                       const double* bright_y, int n_bright, int* count);
+int dgpu_catalog_fetch(dgpu_context* ctx, const dgpu_catalog_columns* cols, int count);
+/* Label image of the last dgpu_build_catalog (polarity it returned), int32 h x w,
+ * 0 = background, 1..n numbered by each component's first pixel in raster order
+ * (the numbering of src/catalog.cpp:105-261). */
+int dgpu_catalog_labels(dgpu_context* ctx, int mem, int32_t* labels, int64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DELTA_GPU_H_ */
