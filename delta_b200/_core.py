@@ -246,6 +246,239 @@ def photometric_scale_at(knots, theta, component_sums, points) -> np.ndarray:
     return out
 
 
+# ---- penalised GLS + stamp fit ----------------------------------------------------------
+
+# Normal-equation arithmetic of fit_kernel / solve_gls* (the solve itself is
+# FP64 in every mode): "fp64" (default, accuracy reference), "fp32" (plain
+# FP32 SIMT), "mixed" (tensor-core split products + one FP64 refinement step).
+PRECISIONS = {"fp64": _lib.PREC_FP64, "fp32": _lib.PREC_FP32, "mixed": _lib.PREC_MIXED}
+_default_precision = "fp64"
+
+
+def set_default_precision(name: str) -> None:
+    """Select the normal-equation arithmetic used when a call does not pass one."""
+    global _default_precision
+    if name not in PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+    _default_precision = name
+
+
+def _prec(precision):
+    return PRECISIONS[precision or _default_precision]
+
+
+def _gls_struct(P, n_lambda, nc, n_stamps=0):
+    bufs = {
+        "theta": np.zeros(P, np.float64),
+        "lambda_grid": np.zeros(max(n_lambda, 1), np.float64),
+        "gcv_curve": np.zeros(max(n_lambda, 1), np.float64),
+        "component_sums": np.zeros(max(nc, 1), np.float64),
+        "stamp_x": np.zeros(max(n_stamps, 1), np.int32),
+        "stamp_y": np.zeros(max(n_stamps, 1), np.int32),
+        "stamp_chi2": np.zeros(max(n_stamps, 1), np.float64),
+        "stamp_accepted": np.zeros(max(n_stamps, 1), np.uint8),
+    }
+    res = _lib.GlsResult()
+    for name, arr in bufs.items():
+        setattr(res, name, arr.ctypes.data)
+    return res, bufs
+
+
+def _gls_dict(res, bufs) -> dict:
+    nl = res.n_lambda_out
+    return {
+        "theta": bufs["theta"],
+        "n_components": int(res.n_components),
+        "n_spatial": int(res.n_spatial),
+        "lambda": float(res.__getattribute__("lambda")),
+        "gcv": float(res.gcv),
+        "effective_dof": float(res.effective_dof),
+        "rss": float(res.rss),
+        "lambda_grid": bufs["lambda_grid"][:nl].copy(),
+        "gcv_curve": bufs["gcv_curve"][:nl].copy(),
+    }
+
+
+def _solve_inputs(knots, points, target, weights, bn):
+    k = _knots(knots)
+    p = _points(points)
+    t = _vec(target)
+    w = _vec(weights)
+    b = np.ascontiguousarray(bn, dtype=np.float64)
+    if b.ndim == 1:
+        b = b.reshape(-1, 1)
+    m = p.shape[0]
+    if t.size != m or w.size != m or b.shape[0] != m:
+        raise RuntimeError("solve_gls: row counts of design/target/weights/bn disagree")
+    return k, p, t, w, b
+
+
+def solve_gls(knots, points, target, weights, bn, lam: float, precision: str | None = None) -> dict:
+    """Penalised GLS at fixed lambda over the factorized A&L model."""
+    k, p, t, w, b = _solve_inputs(knots, points, target, weights, bn)
+    nc = b.shape[1]
+    res, bufs = _gls_struct((nc + 1) * k.shape[0], 0, nc)
+    ctx = context()
+    check(_lib.lib().dgpu_solve_gls(ctx.handle, ptr(k), k.shape[0], ptr(p), ctypes.c_int64(p.shape[0]), ptr(t),
+                                    ptr(w), ptr(b), int(nc), ctypes.c_double(lam), _prec(precision),
+                                    ctypes.byref(res)), ctx.handle)
+    return _gls_dict(res, bufs)
+
+
+def solve_gls_gcv(knots, points, target, weights, bn, lambda_grid, precision: str | None = None) -> dict:
+    """Penalised GLS selecting lambda by GCV over lambda_grid."""
+    k, p, t, w, b = _solve_inputs(knots, points, target, weights, bn)
+    grid = _vec(lambda_grid)
+    nc = b.shape[1]
+    res, bufs = _gls_struct((nc + 1) * k.shape[0], grid.size, nc)
+    ctx = context()
+    check(_lib.lib().dgpu_solve_gls_gcv(ctx.handle, ptr(k), k.shape[0], ptr(p), ctypes.c_int64(p.shape[0]), ptr(t),
+                                        ptr(w), ptr(b), int(nc), ptr(grid), int(grid.size), _prec(precision),
+                                        ctypes.byref(res)), ctx.handle)
+    return _gls_dict(res, bufs)
+
+
+def solve_gls_cv(knots, points, target, weights, bn, lambda_grid, group, n_groups: int,
+                 precision: str | None = None) -> dict:
+    """Penalised GLS selecting lambda by k-fold group cross-validation."""
+    k, p, t, w, b = _solve_inputs(knots, points, target, weights, bn)
+    grid = _vec(lambda_grid)
+    g = np.ascontiguousarray(group, dtype=np.int32).ravel()
+    if g.size != p.shape[0]:
+        raise RuntimeError("solve_gls_cv: group.size() must match points.rows()")
+    nc = b.shape[1]
+    res, bufs = _gls_struct((nc + 1) * k.shape[0], grid.size, nc)
+    ctx = context()
+    check(_lib.lib().dgpu_solve_gls_cv(ctx.handle, ptr(k), k.shape[0], ptr(p), ctypes.c_int64(p.shape[0]), ptr(t),
+                                       ptr(w), ptr(b), int(nc), ptr(grid), int(grid.size), ptr(g), int(n_groups),
+                                       _prec(precision), ctypes.byref(res)), ctx.handle)
+    return _gls_dict(res, bufs)
+
+
+def fit_kernel(science, reference, knots, stamp_x, stamp_y, stamp_radius: int, beta: float, n_max: int,
+               lambda_grid, radius: int = 0, clip_sigma: float = 4.0, clip_iterations: int = 5,
+               min_stamps: int = 5, cv_folds: int = 0, science_var=None, reference_var=None, science_mask=None,
+               reference_mask=None, precision: str | None = None) -> dict:
+    """Fit the matching kernel + background from stamp pixels via penalised GLS
+    with iterative per-stamp sigma clipping (src/bindings.cpp:643-693)."""
+    sci = _img(science, "science")
+    ref = _img(reference, "reference")
+    svar = _img_opt(science_var, "science_var")
+    rvar = _img_opt(reference_var, "reference_var")
+    smask = _mask_opt(science_mask, "science_mask")
+    rmask = _mask_opt(reference_mask, "reference_mask")
+    _same_shape(svar, sci, "variance shape does not match data")
+    _same_shape(smask, sci, "mask shape does not match data")
+    _same_shape(rvar, ref, "variance shape does not match data")
+    _same_shape(rmask, ref, "mask shape does not match data")
+    if sci.shape != ref.shape:
+        raise RuntimeError("fit_kernel: science/reference shape mismatch")
+    sx = np.ascontiguousarray(stamp_x, dtype=np.int32).ravel()
+    sy = np.ascontiguousarray(stamp_y, dtype=np.int32).ravel()
+    if sx.size != sy.size:
+        raise RuntimeError("fit_kernel: stamp_x/stamp_y length mismatch")
+    k = _knots(knots)
+    grid = _vec(lambda_grid)
+    if n_max < 0:
+        raise ValueError("n_max must be >= 0")
+    nc = (n_max + 1) * (n_max + 2) // 2
+    h, w = sci.shape
+    res, bufs = _gls_struct((nc + 1) * k.shape[0], grid.size, nc, sx.size)
+    ctx = context()
+    check(_lib.lib().dgpu_fit_kernel(
+        ctx.handle, _lib.MEM_HOST, ctypes.c_int64(w), ctypes.c_int64(h), ptr(sci), ptr(ref), ptr(svar), ptr(rvar),
+        ptr(smask), ptr(rmask), ptr(k), k.shape[0], ptr(sx), ptr(sy), int(sx.size), int(stamp_radius),
+        ctypes.c_double(beta), int(n_max), int(radius), ptr(grid), int(grid.size), ctypes.c_double(clip_sigma),
+        int(clip_iterations), int(min_stamps), int(cv_folds), _prec(precision), ctypes.byref(res)), ctx.handle)
+    out = _gls_dict(res, bufs)
+    nt = int(res.n_stamps_total)
+    out["timing"] = _lib.drain_timing(ctx)
+    out["component_sums"] = bufs["component_sums"][:nc].copy()
+    out["n_pixels"] = int(res.n_pixels)
+    out["n_stamps_used"] = int(res.n_stamps_used)
+    out["n_stamps_total"] = nt
+    out["n_stamps_rejected"] = int(res.n_stamps_rejected)
+    out["reduced_chi2"] = float(res.reduced_chi2)
+    out["cv_exact_design_bytes"] = int(res.cv_exact_design_bytes)
+    out["stamp_x"] = bufs["stamp_x"][:nt].copy()
+    out["stamp_y"] = bufs["stamp_y"][:nt].copy()
+    out["stamp_chi2"] = bufs["stamp_chi2"][:nt].copy()
+    out["stamp_accepted"] = bufs["stamp_accepted"][:nt].copy()
+    return out
+
+
+# ---- noise decorrelation -------------------------------------------------------------
+
+
+def decorrelate(difference, knots, theta, beta: float, n_max: int, var_science, var_reference, block: int = 256,
+                radius: int = 0, kernel_cell_blocks: int = 0) -> dict:
+    """Spatially-varying noise decorrelation via apodized FFT blocks.
+
+    Returns {'difference', 'variance', 'timing'} (src/bindings.cpp:766-792).
+    """
+    d = _img(difference, "difference")
+    vs = _img(var_science, "var_science")
+    vr = _img(var_reference, "var_reference")
+    h, w = d.shape
+    model, keep = _model(knots, theta, beta, n_max, radius)
+    out_d = np.empty((h, w), np.float32)
+    out_v = np.empty((h, w), np.float32)
+    ctx = context()
+    check(_lib.lib().dgpu_decorrelate(ctx.handle, _lib.MEM_HOST, ctypes.c_int64(w), ctypes.c_int64(h), ptr(d),
+                                      ctypes.byref(model), ptr(vs), ptr(vr), int(block), int(kernel_cell_blocks),
+                                      ptr(out_d), ptr(out_v)), ctx.handle)
+    return {"difference": out_d, "variance": out_v, "timing": _lib.drain_timing(ctx)}
+
+
+def whiten_score_psf(psf, knots, theta, beta: float, n_max: int, var_science, var_reference, block: int,
+                     radius: int = 0) -> np.ndarray:
+    """Apply the ZOGY decorrelation filter to a PSF stamp (frame-centre kernel/noise)."""
+    p = _img(psf, "psf")
+    if p.shape[0] != p.shape[1]:
+        raise RuntimeError("whiten_score_psf: psf must be square")
+    if block < p.shape[0]:
+        raise RuntimeError("whiten_score_psf: block must be >= psf side")
+    vs = _img(var_science, "var_science")
+    vr = _img(var_reference, "var_reference")
+    if vs.shape != vr.shape:
+        raise RuntimeError("whiten_score_psf: variance shapes disagree")
+    h, w = vs.shape
+    model, keep = _model(knots, theta, beta, n_max, radius)
+    out = np.empty_like(p)
+    ctx = context()
+    check(_lib.lib().dgpu_whiten_score_psf(ctx.handle, _lib.MEM_HOST, ptr(p), int(p.shape[0]), ctypes.byref(model),
+                                           ctypes.c_int64(w), ctypes.c_int64(h), ptr(vs), ptr(vr), int(block),
+                                           ptr(out)), ctx.handle)
+    return out
+
+
+def decorrelate_block(image, kernel, var_science: float, var_reference: float) -> np.ndarray:
+    """Whiten one square block with a constant kernel/noise (FFT core)."""
+    img = _img(image, "image")
+    n = img.shape[0]
+    if img.shape[1] != n:
+        raise RuntimeError("decorrelate_block: image must be square")
+    k = _img(kernel, "kernel")
+    if k.shape[0] != k.shape[1]:
+        raise RuntimeError("decorrelate_block: kernel must be square")
+    out = np.empty((n, n), np.float32)
+    ctx = context()
+    check(_lib.lib().dgpu_decorrelate_block(ctx.handle, ptr(img), int(n), ptr(k), int(k.shape[0]),
+                                            ctypes.c_double(var_science), ctypes.c_double(var_reference), ptr(out)),
+          ctx.handle)
+    return out
+
+
+def decorrelation_kernel(kernel, var_science: float, var_reference: float, n: int) -> np.ndarray:
+    """Real-space decorrelation kernel (centred, n x n) for QA."""
+    k = _img(kernel, "kernel")
+    out = np.empty((n, n), np.float32)
+    ctx = context()
+    check(_lib.lib().dgpu_decorrelation_kernel(ctx.handle, ptr(k), int(k.shape[0]), ctypes.c_double(var_science),
+                                               ctypes.c_double(var_reference), int(n), ptr(out)), ctx.handle)
+    return out
+
+
 # ---- matched filter -------------------------------------------------------------------
 
 

@@ -73,6 +73,32 @@ class CatalogParams(ctypes.Structure):
     ]
 
 
+class GlsResult(ctypes.Structure):
+    _fields_ = [
+        ("theta", ctypes.c_void_p),
+        ("lambda_grid", ctypes.c_void_p),
+        ("gcv_curve", ctypes.c_void_p),
+        ("component_sums", ctypes.c_void_p),
+        ("stamp_x", ctypes.c_void_p),
+        ("stamp_y", ctypes.c_void_p),
+        ("stamp_chi2", ctypes.c_void_p),
+        ("stamp_accepted", ctypes.c_void_p),
+        ("n_components", ctypes.c_int),
+        ("n_spatial", ctypes.c_int),
+        ("lambda", ctypes.c_double),
+        ("gcv", ctypes.c_double),
+        ("effective_dof", ctypes.c_double),
+        ("rss", ctypes.c_double),
+        ("reduced_chi2", ctypes.c_double),
+        ("n_pixels", ctypes.c_int64),
+        ("n_stamps_used", ctypes.c_int),
+        ("n_stamps_total", ctypes.c_int),
+        ("n_stamps_rejected", ctypes.c_int),
+        ("cv_exact_design_bytes", ctypes.c_int64),
+        ("n_lambda_out", ctypes.c_int),
+    ]
+
+
 CATALOG_COLUMNS = [
     ("x", np.float64), ("y", np.float64), ("peak_x", np.int32), ("peak_y", np.int32),
     ("peak_snr", np.float64), ("n_pix", np.int32), ("flux", np.float64),

@@ -1,0 +1,687 @@
+// Host driver of the stamp fit and the penalised-GLS entry points.
+//
+// The per-pixel / per-row / per-system arithmetic runs on the device
+// (k_fit.cu, k_solve.cu, k_gls.cu); this file sequences it and takes the
+// reference's small scalar decisions on the host: the lambda argmin, the CV
+// coarse-to-fine / warm-start search order (src/solve.cpp:344-402) and the
+// per-stamp median/MAD clip (src/fit.cpp:456-491), which read a few hundred
+// numbers per IRLS pass.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <numeric>
+
+#include "fit_internal.h"
+#include "gls_internal.h"
+
+using namespace dgpu;
+
+namespace {
+
+constexpr double kInf = std::numeric_limits<double>::infinity();
+constexpr double kNaN = std::numeric_limits<double>::quiet_NaN();
+
+template <class T>
+T* up(Context& c, Slot s, const T* host, size_t n) {
+  T* d = static_cast<T*>(c.slot(s, sizeof(T) * std::max<size_t>(n, 1)));
+  if (n) DGPU_CUDA(cudaMemcpyAsync(d, host, sizeof(T) * n, cudaMemcpyHostToDevice, c.stream));
+  return d;
+}
+
+template <class T>
+std::vector<T> down(Context& c, const T* dev, size_t n) {
+  std::vector<T> h(n);
+  if (n) DGPU_CUDA(cudaMemcpyAsync(h.data(), dev, sizeof(T) * n, cudaMemcpyDeviceToHost, c.stream));
+  DGPU_CUDA(cudaStreamSynchronize(c.stream));
+  return h;
+}
+
+double median_copy(std::vector<double> v) {
+  if (v.empty()) return kNaN;
+  const size_t mid = v.size() / 2;
+  std::nth_element(v.begin(), v.begin() + mid, v.end());
+  return v[mid];
+}
+
+struct GlsOut {
+  std::vector<double> theta;
+  double lambda = 0, gcv = 0, edf = 0, rss = 0;
+  std::vector<double> grid, curve;
+  const double* d_theta = nullptr;  // device copy of theta
+};
+
+// Rows + normal-equation machinery shared by fit_kernel and solve_gls*.
+struct Engine {
+  Context& c;
+  int prec;
+  const ThinPlate& tp;
+  int nc, nf, k, P;
+  int64_t N;
+  int SS;
+  int n_units;  // stamps (fit) or rows (direct solve)
+  FitRows R;
+  std::vector<double> pen_host, fk_host;
+  int rk = 0;
+  double* d_pen = nullptr;
+  double* d_fk = nullptr;
+
+  Engine(Context& ctx, int precision, const ThinPlate& t, int nc_, int64_t N_, int SS_, int units)
+      : c(ctx), prec(precision), tp(t), nc(nc_), nf(nc_ + 1), k(t.k), P((nc_ + 1) * t.k), N(N_), SS(SS_),
+        n_units(units) {
+    if (P > 1024) fail(DGPU_ERR_INVALID, "fit: (nc+1)*k above 1024 unknowns is not supported");
+    pen_host = tp.penalty;
+    fk_host = tp.pen_half(0, &rk);  // one k x r block (nc = 0)
+    std::vector<double> pf(pen_host);
+    pf.insert(pf.end(), fk_host.begin(), fk_host.end());
+    d_pen = up(c, kSlotFit14, pf.data(), pf.size());
+    d_fk = d_pen + static_cast<size_t>(k) * k;
+  }
+
+  void alloc_rows() {
+    const size_t n = static_cast<size_t>(N);
+    R.valid = static_cast<uint8_t*>(c.slot(kSlotFit0, n));
+    R.t = static_cast<double*>(c.slot(kSlotFit1, 8 * n));
+    R.vt = static_cast<double*>(c.slot(kSlotFit2, 8 * n));
+    R.vc = static_cast<double*>(c.slot(kSlotFit3, 8 * n));
+    R.bn = static_cast<double*>(c.slot(kSlotFit4, 8 * n * nc));
+    R.px = static_cast<int*>(c.slot(kSlotFit5, 4 * n));
+    R.py = static_cast<int*>(c.slot(kSlotFit6, 4 * n));
+    R.d = static_cast<double*>(c.slot(kSlotFit7, 8 * n * k));
+    R.w = static_cast<double*>(c.slot(kSlotFit8, 8 * n));
+    R.stamp_used = static_cast<int*>(c.slot(kSlotFit9, 4 * std::max(n_units, 1)));
+  }
+
+  // Workspace for up to `nsys` systems sharing the solver batch.
+  struct Work {
+    double *A, *Linv, *theta, *edf, *raw, *rss, *gcv, *lam;
+    int *ok, *midx, *ridx;
+    unsigned* barrier;
+  };
+  Work work(int nsys) {
+    const int Pp = solve_pp(P);
+    const size_t mat = static_cast<size_t>(Pp) * Pp;
+    Work w{};
+    char* big = static_cast<char*>(c.slot(kSlotFft0, sizeof(double) * 2 * mat * nsys));
+    w.A = reinterpret_cast<double*>(big);
+    w.Linv = w.A + mat * nsys;
+    const size_t small = sizeof(double) * (static_cast<size_t>(nsys) * P + 6 * nsys) + sizeof(int) * 3 * nsys + 64;
+    char* sm = static_cast<char*>(c.slot(kSlotFft1, small));
+    w.theta = reinterpret_cast<double*>(sm);
+    w.edf = w.theta + static_cast<size_t>(nsys) * P;
+    w.raw = w.edf + nsys;
+    w.rss = w.raw + nsys;
+    w.gcv = w.rss + nsys;
+    w.lam = w.gcv + nsys;
+    w.ok = reinterpret_cast<int*>(w.lam + nsys);
+    w.midx = w.ok + nsys;
+    w.ridx = w.midx + nsys;
+    w.barrier = static_cast<unsigned*>(c.slot(kSlotFft2, 64));
+    return w;
+  }
+
+  void solve(const Work& w, int nsys, const double* M, const int* midx, const double* rhs, const int* ridx) {
+    SolveBatch b;
+    b.P = P;
+    b.k = k;
+    b.nf = nf;
+    b.r = rk;
+    b.nsys = nsys;
+    b.M = M;
+    b.m_index = midx;
+    b.rhs = rhs;
+    b.r_index = ridx;
+    b.lam = w.lam;
+    b.pen = d_pen;
+    b.fk = d_fk;
+    b.A = w.A;
+    b.Linv = w.Linv;
+    b.theta = w.theta;
+    b.edf = w.edf;
+    b.ok = w.ok;
+    b.status = c.d_status;
+    b.barrier = w.barrier;
+    launch_solve_batch(c, b);
+  }
+
+  SolveBatch batch_of(const Work& w) const {
+    SolveBatch b;
+    b.P = P;
+    b.k = k;
+    b.nf = nf;
+    b.r = rk;
+    b.Linv = w.Linv;
+    return b;
+  }
+
+  // M, rhs, ywy, n over the rows whose unit mask is set.
+  void assemble(const uint8_t* mask, double* M, double* rhs, double* ywy, long long* n) {
+    launch_rhs(c, N, nc, k, SS, R, mask, nullptr, rhs, ywy, n);
+    launch_normal_equations(c, prec == DGPU_PREC_MIXED ? DGPU_PREC_FP32 : prec, N, nc, k, SS, R, mask, M);
+  }
+
+  // One FP64 refinement step of system s at lambda (theta updated in place).
+  void refine(const Work& w, int s, double lam, const uint8_t* mask, double* theta) {
+    double* r = static_cast<double*>(c.slot(kSlotFit15, sizeof(double) * 2 * P));
+    launch_rhs(c, N, nc, k, SS, R, mask, theta, r, nullptr, nullptr);
+    launch_refine_update(c.stream, P, k, d_pen, lam, theta, r);
+    launch_apply_inverse(c.stream, batch_of(w), s, r, r + P);
+    launch_axpy(c.stream, P, r + P, theta);
+  }
+
+  GlsOut gcv(const std::vector<double>& grid, const uint8_t* mask) {
+    if (grid.empty()) fail(DGPU_ERR_RUNTIME, "solve_gls_gcv: lambda_grid is empty");
+    const int nl = static_cast<int>(grid.size());
+    double* M = static_cast<double*>(c.slot(kSlotScratch1,
+                                            sizeof(double) * (static_cast<size_t>(P) * P + P + 2)));
+    double* rhs = M + static_cast<size_t>(P) * P;
+    double* ywy = rhs + P;
+    long long* n = reinterpret_cast<long long*>(ywy + 1);
+    assemble(mask, M, rhs, ywy, n);
+    Work w = work(nl);
+    DGPU_CUDA(cudaMemcpyAsync(w.lam, grid.data(), sizeof(double) * nl, cudaMemcpyHostToDevice, c.stream));
+    solve(w, nl, M, nullptr, rhs, nullptr);
+    launch_quad_err(c.stream, nl, P, w.theta, M, nullptr, rhs, nullptr, ywy, w.raw);
+    launch_gcv_finish(c.stream, nl, w.raw, w.edf, w.ok, n, w.rss, w.gcv);
+    GlsOut o;
+    o.grid = grid;
+    o.curve = down(c, w.gcv, nl);
+    int best = 0;
+    double bg = kInf;
+    for (int i = 0; i < nl; ++i)
+      if (o.curve[i] < bg) {
+        bg = o.curve[i];
+        best = i;
+      }
+    finish_single(w, best, grid[best], M, rhs, ywy, n, mask, o);
+    return o;
+  }
+
+  // Fill theta / scalars of system `s` (optionally refined) into o.
+  void finish_single(const Work& w, int s, double lam, const double* M, const double* rhs, const double* ywy,
+                     const long long* n, const uint8_t* mask, GlsOut& o) {
+    double* th = w.theta + static_cast<size_t>(s) * P;
+    if (prec == DGPU_PREC_MIXED) {
+      refine(w, s, lam, mask, th);
+      launch_quad_err(c.stream, 1, P, th, M, nullptr, rhs, nullptr, ywy, w.raw + s);
+      launch_gcv_finish(c.stream, 1, w.raw + s, w.edf + s, w.ok + s, n, w.rss + s, w.gcv + s);
+    }
+    o.theta = down(c, th, P);
+    o.d_theta = th;
+    o.lambda = lam;
+    o.edf = down(c, w.edf + s, 1)[0];
+    o.rss = down(c, w.rss + s, 1)[0];
+    o.gcv = down(c, w.gcv + s, 1)[0];
+  }
+
+  // Fixed-lambda solve (src/solve.cpp:208-215).
+  GlsOut fixed(double lam, const uint8_t* mask) {
+    double* M = static_cast<double*>(c.slot(kSlotScratch1, sizeof(double) * (static_cast<size_t>(P) * P + P + 2)));
+    double* rhs = M + static_cast<size_t>(P) * P;
+    double* ywy = rhs + P;
+    long long* n = reinterpret_cast<long long*>(ywy + 1);
+    assemble(mask, M, rhs, ywy, n);
+    Work w = work(1);
+    DGPU_CUDA(cudaMemcpyAsync(w.lam, &lam, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    solve(w, 1, M, nullptr, rhs, nullptr);
+    launch_quad_err(c.stream, 1, P, w.theta, M, nullptr, rhs, nullptr, ywy, w.raw);
+    launch_gcv_finish(c.stream, 1, w.raw, w.edf, w.ok, n, w.rss, w.gcv);
+    GlsOut o;
+    finish_single(w, 0, lam, M, rhs, ywy, n, mask, o);
+    return o;
+  }
+
+  // Group CV over per-unit folds (fold[u] in [0, G), -1 = excluded).
+  // stamped: per-stamp Kronecker build with stamp designs at pixel centroids.
+  GlsOut cv(const std::vector<double>& grid, const uint8_t* mask, const std::vector<int>& fold, int G,
+            int warm_start, bool stamped) {
+    if (grid.empty()) fail(DGPU_ERR_RUNTIME, "solve_gls_cv: lambda_grid is empty");
+    const int nl = static_cast<int>(grid.size());
+    const size_t PP = static_cast<size_t>(P) * P;
+    // fold parts: Mg[G], rg[G], yg[G]; all: Mall, rall, yall; train: Mt[G], rt[G]
+    double* base = static_cast<double*>(c.slot(kSlotScratch1,
+                                               sizeof(double) * ((2 * G + 1) * (PP + P) + G + 8)));
+    double* Mg = base;
+    double* Mt = Mg + G * PP;
+    double* Mall = Mt + G * PP;
+    double* rg = Mall + PP;
+    double* rt = rg + static_cast<size_t>(G) * P;
+    double* rall = rt + static_cast<size_t>(G) * P;
+    double* yg = rall + P;
+    double* yall = yg + G;
+    long long* nall = reinterpret_cast<long long*>(yall + 1);
+    // Active-row count (and per-row ywy) over all folds.
+    {
+      double* scratch = static_cast<double*>(c.slot(kSlotFit15, sizeof(double) * 2 * P));
+      launch_rhs(c, N, nc, k, SS, R, mask, nullptr, scratch, yall, nall);
+    }
+    if (stamped) {
+      // Per-stamp moments + centroids, stamp design on the host (S x k small).
+      double* As = static_cast<double*>(c.slot(kSlotFit10, sizeof(double) * static_cast<size_t>(n_units) * (nf * nf + nf + 4)));
+      double* rs = As + static_cast<size_t>(n_units) * nf * nf;
+      double* ds2 = rs + static_cast<size_t>(n_units) * nf;
+      double* cen = ds2 + n_units;
+      launch_stamp_moments(c.stream, n_units, nc, SS, R, mask, As, rs, ds2, cen);
+      const auto hc = down(c, cen, static_cast<size_t>(n_units) * 3);
+      std::vector<double> dsd(static_cast<size_t>(n_units) * k, 0.0);
+      std::vector<int> f2(n_units, -1);
+      for (int u = 0; u < n_units; ++u) {
+        const double cnt = hc[3 * u + 2];
+        if (cnt <= 0.0 || fold[u] < 0) continue;
+        tp.design_row(hc[3 * u] / cnt, hc[3 * u + 1] / cnt, dsd.data() + static_cast<size_t>(u) * k);
+        f2[u] = fold[u];
+      }
+      double* d_dsd = up(c, kSlotFit13, dsd.data(), dsd.size());
+      int* d_fold = static_cast<int*>(c.slot(kSlotBlockCounts, sizeof(int) * std::max(n_units, 1)));
+      DGPU_CUDA(cudaMemcpyAsync(d_fold, f2.data(), sizeof(int) * n_units, cudaMemcpyHostToDevice, c.stream));
+      launch_stamped_assemble(c.stream, G, n_units, nf, k, d_fold, As, rs, ds2, d_dsd, Mg, rg, yg);
+      DGPU_CUDA(cudaStreamSynchronize(c.stream));
+    } else {
+      uint8_t* fm = static_cast<uint8_t*>(c.slot(kSlotSeedNeg, std::max(n_units, 1)));
+      const auto hm = down(c, mask, n_units);
+      for (int g = 0; g < G; ++g) {
+        std::vector<uint8_t> m(n_units);
+        for (int u = 0; u < n_units; ++u) m[u] = (hm[u] && fold[u] == g) ? 1 : 0;
+        DGPU_CUDA(cudaMemcpyAsync(fm, m.data(), n_units, cudaMemcpyHostToDevice, c.stream));
+        long long* dummy = nall + 1;
+        launch_rhs(c, N, nc, k, SS, R, fm, nullptr, rg + static_cast<size_t>(g) * P, yg + g, dummy);
+        launch_normal_equations(c, prec == DGPU_PREC_MIXED ? DGPU_PREC_FP32 : prec, N, nc, k, SS, R, fm,
+                                Mg + g * PP);
+        DGPU_CUDA(cudaStreamSynchronize(c.stream));
+      }
+    }
+    launch_fold_train(c.stream, G, PP, Mg, Mall, Mt);
+    launch_fold_train(c.stream, G, P, rg, rall, rt);
+    {
+      // yall from the folds (matches cv_finish's sum of ysq[g]).
+      std::vector<double> y = down(c, yg, G);
+      double ys = 0.0;
+      for (double v : y) ys += v;
+      DGPU_CUDA(cudaMemcpyAsync(yall, &ys, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+      DGPU_CUDA(cudaStreamSynchronize(c.stream));
+    }
+    std::vector<double> curve(nl, kInf);
+    std::vector<char> done(nl, 0);
+    Work w = work(std::max(nl * G, 1));
+    auto evaluate = [&](const std::vector<int>& idx) {
+      const int m = static_cast<int>(idx.size());
+      const int ns = m * G;
+      std::vector<double> lam(ns);
+      std::vector<int> mi(ns);
+      for (int ii = 0; ii < m; ++ii)
+        for (int g = 0; g < G; ++g) {
+          lam[ii * G + g] = grid[idx[ii]];
+          mi[ii * G + g] = g;
+        }
+      DGPU_CUDA(cudaMemcpyAsync(w.lam, lam.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, c.stream));
+      DGPU_CUDA(cudaMemcpyAsync(w.midx, mi.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, c.stream));
+      solve(w, ns, Mt, w.midx, rt, w.midx);
+      launch_quad_err(c.stream, ns, P, w.theta, Mg, w.midx, rg, w.midx, yg, w.raw);
+      const auto err = down(c, w.raw, ns);
+      const auto ok = down(c, w.ok, ns);
+      for (int ii = 0; ii < m; ++ii) {
+        double tot = 0.0;
+        for (int g = 0; g < G; ++g) {
+          const double e = err[ii * G + g];
+          tot += ok[ii * G + g] ? (e > 0.0 ? e : 0.0) : kInf;
+        }
+        curve[idx[ii]] = tot;
+        done[idx[ii]] = 1;
+      }
+    };
+    auto argmin_done = [&]() {
+      int b = -1;
+      double bc = kInf;
+      for (int li = 0; li < nl; ++li)
+        if (done[li] && curve[li] < bc) {
+          bc = curve[li];
+          b = li;
+        }
+      return b;
+    };
+    if (warm_start >= 0 && warm_start < nl) {
+      std::vector<int> seed;
+      for (int li = std::max(0, warm_start - 1); li <= std::min(nl - 1, warm_start + 1); ++li) seed.push_back(li);
+      evaluate(seed);
+      for (int guard = 0; guard < nl + 2; ++guard) {
+        const int b = argmin_done();
+        std::vector<int> step;
+        if (b > 0 && !done[b - 1]) step.push_back(b - 1);
+        if (b >= 0 && b < nl - 1 && !done[b + 1]) step.push_back(b + 1);
+        if (step.empty()) break;
+        evaluate(step);
+      }
+    } else {
+      std::vector<int> coarse;
+      for (int li = 0; li < nl; li += 2) coarse.push_back(li);
+      if (coarse.empty() || coarse.back() != nl - 1) coarse.push_back(nl - 1);
+      evaluate(coarse);
+      int cb = coarse.front();
+      for (int li : coarse)
+        if (curve[li] < curve[cb]) cb = li;
+      std::vector<int> refine_idx;
+      for (int li = std::max(0, cb - 2); li <= std::min(nl - 1, cb + 2); ++li)
+        if (!done[li]) refine_idx.push_back(li);
+      if (!refine_idx.empty()) evaluate(refine_idx);
+    }
+    int best = 0;
+    double bc = kInf;
+    for (int li = 0; li < nl; ++li)
+      if (done[li] && curve[li] < bc) {
+        bc = curve[li];
+        best = li;
+      }
+    // Final all-data fit at the selected lambda.
+    Work w1 = work(1);
+    DGPU_CUDA(cudaMemcpyAsync(w1.lam, &grid[best], sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    solve(w1, 1, Mall, nullptr, rall, nullptr);
+    launch_quad_err(c.stream, 1, P, w1.theta, Mall, nullptr, rall, nullptr, yall, w1.raw);
+    launch_gcv_finish(c.stream, 1, w1.raw, w1.edf, w1.ok, nall, w1.rss, w1.gcv);
+    GlsOut o;
+    finish_single(w1, 0, grid[best], Mall, rall, yall, nall, mask, o);
+    o.grid = grid;
+    o.curve = curve;
+    return o;
+  }
+};
+
+void write_gls(const GlsOut& o, int nc, int k, dgpu_gls_result* out) {
+  std::memcpy(out->theta, o.theta.data(), sizeof(double) * o.theta.size());
+  out->n_components = nc;
+  out->n_spatial = k;
+  out->lambda = o.lambda;
+  out->gcv = o.gcv;
+  out->effective_dof = o.edf;
+  out->rss = o.rss;
+  out->n_lambda_out = static_cast<int>(o.grid.size());
+  if (out->lambda_grid && !o.grid.empty()) std::memcpy(out->lambda_grid, o.grid.data(), sizeof(double) * o.grid.size());
+  if (out->gcv_curve && !o.curve.empty()) std::memcpy(out->gcv_curve, o.curve.data(), sizeof(double) * o.curve.size());
+}
+
+template <class F>
+int guarded(dgpu_context* ctx, F&& f) {
+  auto* c = reinterpret_cast<Context*>(ctx);
+  try {
+    if (!ctx) fail(DGPU_ERR_INVALID, "null context");
+    DGPU_CUDA(cudaSetDevice(c->device));
+    reset_status(*c);
+    f(*c);
+    check_status(*c);
+    return DGPU_OK;
+  } catch (const Failure& e) {
+    if (c) c->last_error = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    if (c) c->last_error = e.what();
+    return DGPU_ERR_RUNTIME;
+  }
+}
+
+// Rows for the direct solver entry points: one unit per row.
+void direct_rows(Engine& E, const double* points, const double* target, const double* weights, const double* bn) {
+  const int64_t m = E.N;
+  std::vector<uint8_t> valid(m, 1);
+  std::vector<double> d(static_cast<size_t>(m) * E.k);
+  for (int64_t i = 0; i < m; ++i) E.tp.design_row(points[2 * i], points[2 * i + 1], d.data() + i * E.k);
+  E.alloc_rows();
+  Context& c = E.c;
+  DGPU_CUDA(cudaMemcpyAsync(E.R.valid, valid.data(), m, cudaMemcpyHostToDevice, c.stream));
+  DGPU_CUDA(cudaMemcpyAsync(E.R.t, target, 8 * m, cudaMemcpyHostToDevice, c.stream));
+  DGPU_CUDA(cudaMemcpyAsync(E.R.w, weights, 8 * m, cudaMemcpyHostToDevice, c.stream));
+  if (E.nc) DGPU_CUDA(cudaMemcpyAsync(E.R.bn, bn, 8 * m * E.nc, cudaMemcpyHostToDevice, c.stream));
+  DGPU_CUDA(cudaMemcpyAsync(E.R.d, d.data(), 8 * d.size(), cudaMemcpyHostToDevice, c.stream));
+  DGPU_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+}  // namespace
+
+extern "C" {
+
+int dgpu_solve_gls(dgpu_context* ctx, const double* knots, int n_knots, const double* points, int64_t m,
+                   const double* target, const double* weights, const double* bn, int nc, double lam,
+                   int precision, dgpu_gls_result* out) {
+  return guarded(ctx, [&](Context& c) {
+    const ThinPlate tp(knots, n_knots);
+    if (m <= 0) fail(DGPU_ERR_RUNTIME, "solve_gls: no rows");
+    Engine E(c, precision, tp, nc, m, 1, static_cast<int>(m));
+    direct_rows(E, points, target, weights, bn);
+    std::vector<uint8_t> ones(m, 1);
+    uint8_t* mask = up(c, kSlotSeedPos, ones.data(), ones.size());
+    GlsOut o = E.fixed(lam, mask);
+    o.grid.clear();
+    o.curve.clear();
+    write_gls(o, nc, tp.k, out);
+  });
+}
+
+int dgpu_solve_gls_gcv(dgpu_context* ctx, const double* knots, int n_knots, const double* points, int64_t m,
+                       const double* target, const double* weights, const double* bn, int nc,
+                       const double* lambda_grid, int n_lambda, int precision, dgpu_gls_result* out) {
+  return guarded(ctx, [&](Context& c) {
+    const ThinPlate tp(knots, n_knots);
+    if (n_lambda <= 0) fail(DGPU_ERR_RUNTIME, "solve_gls_gcv: lambda_grid is empty");
+    if (m <= 0) fail(DGPU_ERR_RUNTIME, "solve_gls: no rows");
+    Engine E(c, precision, tp, nc, m, 1, static_cast<int>(m));
+    direct_rows(E, points, target, weights, bn);
+    std::vector<uint8_t> ones(m, 1);
+    uint8_t* mask = up(c, kSlotSeedPos, ones.data(), ones.size());
+    const GlsOut o = E.gcv(std::vector<double>(lambda_grid, lambda_grid + n_lambda), mask);
+    write_gls(o, nc, tp.k, out);
+  });
+}
+
+int dgpu_solve_gls_cv(dgpu_context* ctx, const double* knots, int n_knots, const double* points, int64_t m,
+                      const double* target, const double* weights, const double* bn, int nc,
+                      const double* lambda_grid, int n_lambda, const int32_t* group, int n_groups, int precision,
+                      dgpu_gls_result* out) {
+  return guarded(ctx, [&](Context& c) {
+    const ThinPlate tp(knots, n_knots);
+    if (n_lambda <= 0) fail(DGPU_ERR_RUNTIME, "solve_gls_cv: lambda_grid is empty");
+    if (m <= 0) fail(DGPU_ERR_RUNTIME, "solve_gls: no rows");
+    Engine E(c, precision, tp, nc, m, 1, static_cast<int>(m));
+    direct_rows(E, points, target, weights, bn);
+    std::vector<uint8_t> ones(m, 1);
+    uint8_t* mask = up(c, kSlotSeedPos, ones.data(), ones.size());
+    const std::vector<double> grid(lambda_grid, lambda_grid + n_lambda);
+    GlsOut o;
+    if (n_groups < 2) {
+      o = E.gcv(grid, mask);
+    } else {
+      std::vector<int> fold(m);
+      for (int64_t i = 0; i < m; ++i) {
+        if (group[i] < 0 || group[i] >= n_groups) fail(DGPU_ERR_RUNTIME, "solve_gls_cv: group id out of range");
+        fold[i] = group[i];
+      }
+      o = E.cv(grid, mask, fold, n_groups, -1, false);
+    }
+    write_gls(o, nc, tp.k, out);
+  });
+}
+
+int dgpu_fit_kernel(dgpu_context* ctx, int mem, int64_t width, int64_t height, const float* science,
+                    const float* reference, const float* science_var, const float* reference_var,
+                    const uint8_t* science_mask, const uint8_t* reference_mask, const double* knots, int n_knots,
+                    const int32_t* stamp_x, const int32_t* stamp_y, int n_stamps, int stamp_radius, double beta,
+                    int n_max, int radius, const double* lambda_grid, int n_lambda, double clip_sigma,
+                    int clip_iterations, int min_stamps, int cv_folds, int precision, dgpu_gls_result* out) {
+  return guarded(ctx, [&](Context& c) {
+    if (width <= 0 || height <= 0) fail(DGPU_ERR_INVALID, "image must be non-empty");
+    if (width * height >= (int64_t(1) << 31)) fail(DGPU_ERR_INVALID, "image too large");
+    if (n_lambda <= 0) fail(DGPU_ERR_RUNTIME, "solve_gls_gcv: lambda_grid is empty");
+    if (stamp_radius < 0) fail(DGPU_ERR_INVALID, "stamp_radius must be >= 0");
+    const int w = static_cast<int>(width), h = static_cast<int>(height);
+    const size_t npx = static_cast<size_t>(w) * h;
+    const Basis b(beta, n_max, radius);
+    const ThinPlate tp(knots, n_knots);
+    const int nc = b.nc, k = tp.k;
+    cudaStream_t st = c.stream;
+    const auto* sci = static_cast<const float*>(stage_in(c, mem, science, 4 * npx, kSlotInSci));
+    const auto* ref = static_cast<const float*>(stage_in(c, mem, reference, 4 * npx, kSlotInRef));
+    const auto* vs = static_cast<const float*>(stage_in(c, mem, science_var, 4 * npx, kSlotInVarS));
+    const auto* vr = static_cast<const float*>(stage_in(c, mem, reference_var, 4 * npx, kSlotInVarR));
+    const auto* sm = static_cast<const uint8_t*>(stage_in(c, mem, science_mask, npx, kSlotInMaskS));
+    const auto* rm = static_cast<const uint8_t*>(stage_in(c, mem, reference_mask, npx, kSlotInMaskR));
+    const bool have_var = vs != nullptr || vr != nullptr;
+    const bool have_cvar = vr != nullptr;
+
+    StampGeom g;
+    g.w = w;
+    g.h = h;
+    g.sr = stamp_radius;
+    g.S = 2 * stamp_radius + 1;
+    g.SS = g.S * g.S;
+    g.r = b.radius;
+    g.ks = b.ks;
+    g.n_max = n_max;
+    g.nc = nc;
+    g.pmax = g.S + 2 * b.radius;
+    g.have_var = have_var ? 1 : 0;
+    g.have_cvar = have_cvar ? 1 : 0;
+    const int64_t N = static_cast<int64_t>(n_stamps) * g.SS;
+    if (N == 0) fail(DGPU_ERR_RUNTIME, "fit_kernel: no usable stamp pixels");
+
+    Engine E(c, precision, tp, nc, N, g.SS, n_stamps);
+    E.alloc_rows();
+    float* fill = static_cast<float*>(c.slot(kSlotScratch2, 64));
+    {
+      StageTimer t(c, "fit: stamp B_n convolve");
+      launch_strided_median(c, kSampleReference, static_cast<int64_t>(npx), ref, rm, fill);
+      int* dsx = up(c, kSlotBright, reinterpret_cast<const int*>(stamp_x), static_cast<size_t>(n_stamps));
+      int* dsy = static_cast<int*>(c.slot(kSlotCompOut, sizeof(int) * std::max(n_stamps, 1)));
+      DGPU_CUDA(cudaMemcpyAsync(dsy, stamp_y, sizeof(int) * n_stamps, cudaMemcpyHostToDevice, st));
+      const auto taps = b.taps();
+      float* dt = up(c, kSlotTaps, taps.data(), taps.size());
+      std::vector<int2> ord(nc);
+      for (int i = 0; i < nc; ++i) ord[i] = make_int2(b.orders[i].first, b.orders[i].second);
+      int2* dord = up(c, kSlotRootRank, ord.data(), ord.size());
+      launch_stamp_gather(st, g, n_stamps, dsx, dsy, sci, ref, vs, vr, sm, rm, dt, dord, fill, E.R);
+      const TpsDev t2 = upload_tps(c, tp);
+      launch_design_weights(st, N, t2, E.R, have_var ? 1 : 0);
+    }
+    StageTimer solve_timer(c, "fit: GLS solve");
+    const auto used = down(c, E.R.stamp_used, n_stamps);
+    // Contributing stamps in supplied order (src/fit.cpp:196-229).
+    std::vector<int> comp_of(n_stamps, -1), contrib;
+    for (int s = 0; s < n_stamps; ++s)
+      if (used[s]) {
+        comp_of[s] = static_cast<int>(contrib.size());
+        contrib.push_back(s);
+      }
+    const int nct = static_cast<int>(contrib.size());
+    if (nct == 0) fail(DGPU_ERR_RUNTIME, "fit_kernel: no usable stamp pixels");
+    std::vector<uint8_t> accepted(n_stamps, 0);
+    for (int s : contrib) accepted[s] = 1;
+    uint8_t* d_acc = static_cast<uint8_t*>(c.slot(kSlotSeedPos, std::max(n_stamps, 1)));
+    // Reweight inputs.
+    float* phi = nullptr;
+    if (have_cvar) {
+      std::vector<float> ph(static_cast<size_t>(nc) * b.ks * b.ks);
+      for (int q = 0; q < nc; ++q) {
+        const auto k2 = b.kernel2d(q);
+        std::copy(k2.begin(), k2.end(), ph.begin() + static_cast<size_t>(q) * b.ks * b.ks);
+      }
+      phi = up(c, kSlotPhi, ph.data(), ph.size());
+    }
+    const TpsDev tdev = upload_tps(c, tp);
+    int* dsx = static_cast<int*>(c.slot(kSlotBright, sizeof(int) * std::max(n_stamps, 1)));
+    int* dsy = static_cast<int*>(c.slot(kSlotCompOut, sizeof(int) * std::max(n_stamps, 1)));
+    double* chi2_d = static_cast<double*>(c.slot(kSlotCompStats, sizeof(double) * std::max(n_stamps, 1) + 4 * std::max(n_stamps, 1) + 64));
+    int* cnt_d = reinterpret_cast<int*>(chi2_d + std::max(n_stamps, 1));
+
+    const int clip_passes = (clip_sigma > 0.0 && clip_iterations > 0) ? clip_iterations : 0;
+    const int do_iterate = clip_iterations > 0 ? 1 : 0;
+    const int min_pass = (do_iterate && have_var) ? 1 : 0;
+    const int hard_max = std::max(clip_passes, min_pass);
+    const int floor_stamps = std::max(1, std::min(min_stamps, nct));
+    const std::vector<double> grid(lambda_grid, lambda_grid + n_lambda);
+    int warm_start = -1;
+    size_t cv_exact_bytes = 0;
+    GlsOut gls;
+    std::vector<double> stamp_chi2(n_stamps, kNaN);
+    std::vector<int> cnt(n_stamps, 0);
+    long long npix = 0;
+    double reduced = kNaN;
+    const double knot_spacing = tp.min_knot_spacing();
+    bool use_stamped = knot_spacing > 0.0 && knot_spacing >= 16.0 * (2.0 * stamp_radius + 1.0);
+    if (const char* e = std::getenv("DELTA_STAMP_APPROX")) use_stamped = std::atoi(e) != 0;
+
+    for (int iter = 0;; ++iter) {
+      DGPU_CUDA(cudaMemcpyAsync(d_acc, accepted.data(), n_stamps, cudaMemcpyHostToDevice, st));
+      {
+        double* scratch = static_cast<double*>(c.slot(kSlotFit15, sizeof(double) * (2 * E.P + 4)));
+        long long* nn = reinterpret_cast<long long*>(scratch + 2 * E.P + 1);
+        launch_rhs(c, N, nc, k, g.SS, E.R, d_acc, nullptr, scratch, scratch + 2 * E.P, nn);
+        npix = down(c, nn, 1)[0];
+      }
+      if (npix == 0) fail(DGPU_ERR_RUNTIME, "fit_kernel: all stamp pixels clipped");
+      if (cv_folds > 1) {
+        std::vector<int> fold(n_stamps, -1);
+        for (int s = 0; s < n_stamps; ++s)
+          if (comp_of[s] >= 0) fold[s] = comp_of[s] % cv_folds;
+        gls = E.cv(grid, d_acc, fold, cv_folds, warm_start, use_stamped);
+        if (!use_stamped) cv_exact_bytes = static_cast<size_t>(npix) * E.P * sizeof(double);
+        warm_start = static_cast<int>(std::min_element(gls.curve.begin(), gls.curve.end()) - gls.curve.begin());
+      } else {
+        gls = E.gcv(grid, d_acc);
+      }
+      launch_stamp_chi2(st, n_stamps, nc, k, g.SS, E.R, d_acc, gls.d_theta, chi2_d, cnt_d);
+      stamp_chi2 = down(c, chi2_d, n_stamps);
+      cnt = down(c, cnt_d, n_stamps);
+      const double denom = static_cast<double>(npix) - gls.edf;
+      reduced = denom > 0.0 ? gls.rss / denom : kNaN;
+      if (have_var) {
+        DGPU_CUDA(cudaMemcpyAsync(dsx, stamp_x, sizeof(int) * n_stamps, cudaMemcpyHostToDevice, st));
+        DGPU_CUDA(cudaMemcpyAsync(dsy, stamp_y, sizeof(int) * n_stamps, cudaMemcpyHostToDevice, st));
+        launch_reweight(st, g, n_stamps, tdev, dsx, dsy, E.R, d_acc, cnt_d, gls.d_theta, phi, vr, rm);
+      }
+      std::vector<int> to_reject;
+      if (clip_passes > 0 && iter < clip_passes) {
+        std::vector<double> act;
+        for (int s : contrib)
+          if (accepted[s] && cnt[s] > 0) act.push_back(stamp_chi2[s]);
+        const int n_active = static_cast<int>(act.size());
+        if (n_active > floor_stamps) {
+          const double med = median_copy(act);
+          std::vector<double> dev;
+          for (double v : act) dev.push_back(std::fabs(v - med));
+          const double thr = med + clip_sigma * 1.4826 * median_copy(dev);
+          std::vector<int> cand;
+          for (int s : contrib)
+            if (accepted[s] && cnt[s] > 0 && stamp_chi2[s] > thr) cand.push_back(s);
+          std::stable_sort(cand.begin(), cand.end(), [&](int a2, int b2) { return stamp_chi2[a2] > stamp_chi2[b2]; });
+          for (int s : cand) {
+            if (n_active - static_cast<int>(to_reject.size()) <= floor_stamps) break;
+            to_reject.push_back(s);
+          }
+        }
+      }
+      if (to_reject.empty() && iter >= min_pass) break;
+      if (iter >= hard_max) break;
+      for (int s : to_reject) accepted[s] = 0;
+    }
+    int n_used = 0;
+    for (int s : contrib)
+      if (accepted[s] && std::isfinite(stamp_chi2[s])) ++n_used;
+    write_gls(gls, nc, k, out);
+    const auto sums = b.component_sums();
+    if (out->component_sums) std::memcpy(out->component_sums, sums.data(), sizeof(double) * nc);
+    out->n_pixels = npix;
+    out->n_stamps_total = nct;
+    out->n_stamps_used = n_used;
+    out->n_stamps_rejected = nct - n_used;
+    out->reduced_chi2 = reduced;
+    out->cv_exact_design_bytes = static_cast<int64_t>(cv_exact_bytes);
+    for (int i = 0; i < nct; ++i) {
+      const int s = contrib[i];
+      if (out->stamp_x) out->stamp_x[i] = stamp_x[s];
+      if (out->stamp_y) out->stamp_y[i] = stamp_y[s];
+      if (out->stamp_chi2) out->stamp_chi2[i] = stamp_chi2[s];
+      if (out->stamp_accepted) out->stamp_accepted[i] = accepted[s];
+    }
+  });
+}
+
+}  // extern "C"

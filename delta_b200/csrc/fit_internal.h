@@ -1,0 +1,75 @@
+// Internal types of the stamp fit and the batched penalised-GLS solver.
+#pragma once
+
+#include "internal.h"
+
+namespace dgpu {
+
+struct StampGeom {
+  int w = 0, h = 0;
+  int sr = 0, S = 0, SS = 0;  // stamp radius, side 2sr+1, S*S
+  int r = 0, ks = 0;          // kernel radius, side 2r+1
+  int n_max = 0, nc = 0;
+  int pmax = 0;               // max patch side S + 2r
+  int have_var = 0, have_cvar = 0;
+};
+
+// Per-row buffers; N = n_stamps * SS rows in fixed per-stamp slots.
+struct FitRows {
+  uint8_t* valid = nullptr;
+  double* t = nullptr;
+  double* vt = nullptr;
+  double* vc = nullptr;
+  double* bn = nullptr;  // N x nc (float32 values from the stamp gather)
+  int* px = nullptr;
+  int* py = nullptr;
+  double* d = nullptr;   // N x k design rows
+  double* w = nullptr;   // IRLS weights
+  int* stamp_used = nullptr;
+};
+
+void launch_stamp_gather(cudaStream_t st, const StampGeom& g, int n_stamps, const int* sx, const int* sy,
+                         const float* sci, const float* ref, const float* vs, const float* vr,
+                         const uint8_t* sm, const uint8_t* rm, const float* taps, const int2* orders,
+                         const float* fill, const FitRows& R);
+void launch_design_weights(cudaStream_t st, int64_t N, const TpsDev& t, const FitRows& R, int have_var);
+void launch_normal_equations(Context& c, int prec, int64_t N, int nc, int k, int SS, const FitRows& R,
+                             const uint8_t* accepted, double* M);
+void launch_rhs(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, const uint8_t* accepted,
+                const double* theta, double* rhs, double* ywy, long long* n);
+void launch_stamp_chi2(cudaStream_t st, int n_stamps, int nc, int k, int SS, const FitRows& R,
+                       const uint8_t* accepted, const double* theta, double* chi2, int* cnt);
+void launch_reweight(cudaStream_t st, const StampGeom& g, int n_stamps, const TpsDev& t, const int* sx,
+                     const int* sy, const FitRows& R, const uint8_t* accepted, const int* cnt,
+                     const double* theta, const float* phi, const float* vr, const uint8_t* rm);
+
+// ---------------------------------------------------------------------------
+// Batched penalised GLS: for each system s of a batch, A_s = M_s + lam_s P0
+// (P0 = blockdiag of the k x k penalty), Cholesky A_s = L L^T, L^{-1},
+// theta_s = A_s^{-1} rhs_s, edf_s = P - lam_s ||L^{-1} F||_F^2 and, when
+// requested, the held-out error of a CV fold. One cooperative launch.
+// ---------------------------------------------------------------------------
+struct SolveBatch {
+  int P = 0, k = 0, nf = 0, r = 0;  // unknowns, knots, fields, rank of the penalty
+  int nsys = 0;
+  const double* M = nullptr;        // nsys_m x P x P (system s uses M + m_index[s]*P*P)
+  const int* m_index = nullptr;     // per system (nullptr -> 0)
+  const double* rhs = nullptr;      // per system rhs (rhs + r_index[s]*P)
+  const int* r_index = nullptr;
+  const double* lam = nullptr;      // nsys
+  const double* pen = nullptr;      // k x k
+  const double* fk = nullptr;       // k x r half factor of the penalty
+  double* A = nullptr;              // nsys x Pp x Pp workspace (L in the lower tiles)
+  double* Linv = nullptr;           // nsys x Pp x Pp
+  double* theta = nullptr;          // nsys x P
+  double* edf = nullptr;            // nsys
+  int* ok = nullptr;                // nsys: 1 if the Cholesky succeeded
+  unsigned* status = nullptr;
+  unsigned* barrier = nullptr;      // 2 words, zeroed before launch
+};
+int solve_pp(int P);  // padded size
+void launch_solve_batch(Context& c, const SolveBatch& b);
+// Apply a system's inverse: out = A_s^{-1} v (uses the Linv of system s).
+void launch_apply_inverse(cudaStream_t st, const SolveBatch& b, int s, const double* v, double* out);
+
+}  // namespace dgpu

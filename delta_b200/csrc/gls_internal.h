@@ -1,0 +1,22 @@
+// GCV / CV helper launchers (k_gls.cu).
+#pragma once
+
+#include "fit_internal.h"
+
+namespace dgpu {
+
+void launch_quad_err(cudaStream_t st, int nsys, int P, const double* theta, const double* M, const int* m_index,
+                     const double* r, const int* r_index, const double* y, double* out);
+void launch_gcv_finish(cudaStream_t st, int nsys, const double* raw, const double* edf, const int* ok,
+                       const long long* n, double* rss, double* gcv);
+void launch_fold_train(cudaStream_t st, int groups, size_t len, const double* part, double* all, double* train);
+void launch_stamp_moments(cudaStream_t st, int n_stamps, int nc, int SS, const FitRows& R, const uint8_t* accepted,
+                          double* As, double* rs, double* ds2, double* cen);
+void launch_stamped_assemble(cudaStream_t st, int groups, int nstamp, int nf, int k, const int* fold,
+                             const double* As, const double* rs, const double* ds2, const double* dsd, double* Mg,
+                             double* rg, double* yg);
+void launch_refine_update(cudaStream_t st, int P, int k, const double* pen, double lam, const double* theta,
+                          double* r);
+void launch_axpy(cudaStream_t st, int n, const double* d, double* x);
+
+}  // namespace dgpu

@@ -1,0 +1,469 @@
+// ZOGY noise decorrelation (reference src/noise.cpp:65-533), sm_100a.
+//
+// Per overlap-add block (n x n, n a power of two, stride n/2, reflect padded):
+//   row pass    : n real rows -> n/2-point complex FFT of the even/odd packing
+//                 -> Hermitian split -> n/2+1 bins per row (r2c), to scratch;
+//   column pass : n-point complex FFT down each of the n/2+1 columns, the
+//                 decorrelation filter Phi = sqrt(vs + vr sum K^2) /
+//                 sqrt(vs + vr |Khat|^2) applied in place (|Khat|^2 from the
+//                 per-cell cache, vs / vr the block's subsampled medians), then
+//                 the inverse column FFT -- filter fused between the passes;
+//   row inverse : Hermitian merge -> n/2-point inverse FFT -> n real samples,
+//                 scaled by 1/n^2 and Hann-weighted into the frame accumulators.
+// The overlap-add runs colour by colour in the reference's 9-colour order
+// (ix % 3, iy % 3), so every pixel accumulates its blocks in the same order on
+// every run and no two blocks of one launch touch the same pixel.
+// FFTs are unnormalised radix-2 in shared memory with FP64-derived twiddles.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "dev_common.cuh"
+#include "fft_internal.h"
+
+namespace dgpu {
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+
+// tw[k] = exp(sign 2 pi i k / m), k < m/2.
+__device__ void make_twiddles(float2* tw, int m, int sign) {
+  for (int k = threadIdx.x; k < m / 2; k += blockDim.x) {
+    double s, c;
+    sincospi(2.0 * k / m, &s, &c);
+    tw[k] = make_float2(static_cast<float>(c), static_cast<float>(sign * s));
+  }
+}
+
+// In-place radix-2 DIT FFT of L lines of length m (line-major) in shared memory.
+__device__ void smem_fft(float2* x, int L, int m, int logm, const float2* tw) {
+  for (int e = threadIdx.x; e < L * m; e += blockDim.x) {
+    const int line = e / m, j = e - line * m;
+    const int rj = static_cast<int>(__brev(static_cast<unsigned>(j)) >> (32 - logm));
+    if (j < rj) {
+      const float2 t = x[line * m + j];
+      x[line * m + j] = x[line * m + rj];
+      x[line * m + rj] = t;
+    }
+  }
+  __syncthreads();
+  for (int half = 1; half < m; half <<= 1) {
+    const int tstep = m / (2 * half);
+    for (int b = threadIdx.x; b < L * (m / 2); b += blockDim.x) {
+      const int line = b / (m / 2), j = b - line * (m / 2);
+      const int pos = j & (half - 1);
+      const int i0 = ((j - pos) << 1) + pos, i1 = i0 + half;
+      float2* xl = x + line * m;
+      const float2 a = xl[i0];
+      const float2 c = cmul(xl[i1], tw[pos * tstep]);
+      xl[i0] = cadd(a, c);
+      xl[i1] = csub(a, c);
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ int reflect_clamp(int s, int len) {
+  if (s < 0) s = -s - 1;
+  if (s >= len) s = 2 * len - s - 1;
+  return min(max(s, 0), len - 1);
+}
+
+// ---------------------------------------------------------------------------
+// Row pass (r2c). mode 0: block rows of the frame, reflect padded
+// (src/noise.cpp:392-406); mode 1: rows of a dense n x n real image per item.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_rows_fwd(FftGeom G, int mode, const float* __restrict__ src, int w, int h, const int* __restrict__ oxs,
+           const int* __restrict__ oys, int nox, float2* __restrict__ spec) {
+  extern __shared__ __align__(16) float2 fsm2[];
+  const int n = G.n, hn = n / 2, nb = hn + 1;
+  const int rows = G.rows_per_cta;
+  float2* z = fsm2;                 // rows x hn
+  float2* tw = z + rows * hn;       // hn/2 (length-hn FFT)
+  float2* twn = tw + hn / 2 + 1;    // hn (W^k, k < hn + 1) for the split
+  const int item = blockIdx.x, r0 = blockIdx.y * rows;
+  make_twiddles(tw, hn, -1);
+  for (int k = threadIdx.x; k <= hn; k += blockDim.x) {
+    double s, c;
+    sincospi(2.0 * k / n, &s, &c);
+    twn[k] = make_float2(static_cast<float>(c), static_cast<float>(-s));
+  }
+  int bx = 0, by = 0;
+  if (mode == 0) {
+    bx = oxs[item % nox];
+    by = oys[item / nox];
+  }
+  for (int e = threadIdx.x; e < rows * hn; e += blockDim.x) {
+    const int rr = e / hn, j = e - rr * hn;
+    const int row = r0 + rr;
+    float a, b;
+    if (mode == 0) {
+      const int sy = reflect_clamp(by + row, h);
+      const float* srow = src + static_cast<size_t>(sy) * w;
+      a = srow[reflect_clamp(bx + 2 * j, w)];
+      b = srow[reflect_clamp(bx + 2 * j + 1, w)];
+    } else {
+      const float* srow = src + (static_cast<size_t>(item) * n + row) * n;
+      a = srow[2 * j];
+      b = srow[2 * j + 1];
+    }
+    z[e] = make_float2(a, b);
+  }
+  __syncthreads();
+  smem_fft(z, rows, hn, G.logn - 1, tw);
+  for (int e = threadIdx.x; e < rows * nb; e += blockDim.x) {
+    const int rr = e / nb, k = e - rr * nb;
+    const float2 zk = z[rr * hn + (k % hn)];
+    const float2 zc = cconj(z[rr * hn + ((hn - k) % hn)]);
+    const float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
+    const float2 d = csub(zk, zc);                         // 2i O
+    const float2 od = make_float2(0.5f * d.y, -0.5f * d.x);  // O = d / (2i)
+    spec[(static_cast<size_t>(item) * n + r0 + rr) * nb + k] = cadd(ev, cmul(twn[k], od));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Column pass. mode 0: forward, multiply by the block filter, inverse (in
+// place); mode 1: forward and write |X|^2 in FP64 (kernel-power cache).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_cols(FftGeom G, int mode, float2* __restrict__ spec, const double* __restrict__ cell_power,
+       const double* __restrict__ cell_sumk2, const int* __restrict__ block_cell, const double* __restrict__ vsr,
+       double* __restrict__ power_out) {
+  extern __shared__ __align__(16) float2 fsm2[];
+  const int n = G.n, nb = n / 2 + 1;
+  const int C = G.cols_per_cta;
+  float2* x = fsm2;            // C x n
+  float2* tw = x + C * n;      // n/2
+  const int item = blockIdx.x, c0 = blockIdx.y * C;
+  const int ncol = min(C, nb - c0);
+  make_twiddles(tw, n, -1);
+  float2* sp = spec + static_cast<size_t>(item) * n * nb;
+  if (mode == 2) {
+    // Spectrum = the real filter itself (decorrelation_kernel_image, src/noise.cpp:139-146).
+    for (int e = threadIdx.x; e < C * n; e += blockDim.x) x[e] = make_float2(0.f, 0.f);
+  } else {
+    for (int e = threadIdx.x; e < C * n; e += blockDim.x) {
+      const int row = e / C, cc = e - row * C;
+      x[cc * n + row] = cc < ncol ? sp[static_cast<size_t>(row) * nb + c0 + cc] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    smem_fft(x, C, n, G.logn, tw);
+  }
+  if (mode == 1) {
+    for (int e = threadIdx.x; e < C * n; e += blockDim.x) {
+      const int row = e / C, cc = e - row * C;
+      if (cc >= ncol) continue;
+      const float2 v = x[cc * n + row];
+      const double re = v.x, im = v.y;
+      power_out[(static_cast<size_t>(item) * n + row) * nb + c0 + cc] = re * re + im * im;
+    }
+    return;
+  }
+  // Filter (src/noise.cpp:414-422), then the inverse column FFT.
+  const int cell = block_cell[item];
+  const double vs = vsr[2 * item], vr = vsr[2 * item + 1];
+  const double cnum = sqrt(fmax(vs + vr * cell_sumk2[cell], 0.0));
+  const double* pw = cell_power + static_cast<size_t>(cell) * n * nb;
+  for (int e = threadIdx.x; e < C * n; e += blockDim.x) {
+    const int cc = e / n, row = e - cc * n;
+    if (cc >= ncol) continue;
+    const double denom = vs + vr * pw[static_cast<size_t>(row) * nb + c0 + cc];
+    const float f = denom > 0.0 ? static_cast<float>(cnum / sqrt(denom)) : 0.0f;
+    x[cc * n + row] = mode == 2 ? make_float2(f, 0.0f) : make_float2(x[cc * n + row].x * f, x[cc * n + row].y * f);
+  }
+  __syncthreads();
+  make_twiddles(tw, n, +1);
+  __syncthreads();
+  smem_fft(x, C, n, G.logn, tw);
+  for (int e = threadIdx.x; e < C * n; e += blockDim.x) {
+    const int row = e / C, cc = e - row * C;
+    if (cc < ncol) sp[static_cast<size_t>(row) * nb + c0 + cc] = x[cc * n + row];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Row inverse (c2r). mode 0: Hann overlap-add of the blocks of one colour into
+// acc / var_acc (src/noise.cpp:430-452); mode 1: plain store x 1/n^2 into a
+// dense n x n real output per item.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_rows_inv(FftGeom G, int mode, const float2* __restrict__ spec, const int* __restrict__ items, int w, int h,
+           const int* __restrict__ oxs, const int* __restrict__ oys, int nox, const double* __restrict__ hwin,
+           const double* __restrict__ vsr, const double* __restrict__ cell_sumk2, const int* __restrict__ block_cell,
+           float* __restrict__ acc, float* __restrict__ var_acc, float* __restrict__ dense_out) {
+  extern __shared__ __align__(16) float2 fsm2[];
+  const int n = G.n, hn = n / 2, nb = hn + 1;
+  const int rows = G.rows_per_cta;
+  float2* z = fsm2;
+  float2* tw = z + rows * hn;
+  float2* twn = tw + hn / 2 + 1;
+  const int item = mode == 0 ? items[blockIdx.x] : blockIdx.x;
+  const int r0 = blockIdx.y * rows;
+  make_twiddles(tw, hn, +1);
+  for (int k = threadIdx.x; k <= hn; k += blockDim.x) {
+    double s, c;
+    sincospi(2.0 * k / n, &s, &c);
+    twn[k] = make_float2(static_cast<float>(c), static_cast<float>(s));  // W^-k
+  }
+  __syncthreads();
+  const float2* sp = spec + static_cast<size_t>(item) * n * nb;
+  for (int e = threadIdx.x; e < rows * hn; e += blockDim.x) {
+    const int rr = e / hn, k = e - rr * hn;
+    const float2* xr = sp + static_cast<size_t>(r0 + rr) * nb;
+    float2 xk = xr[k];
+    float2 xc = cconj(xr[hn - k]);
+    if (k == 0) {  // c2r ignores the imaginary parts of the DC and Nyquist bins
+      xk.y = 0.0f;
+      xc.y = 0.0f;
+    }
+    const float2 e2 = cadd(xk, xc);
+    const float2 o2 = cmul(csub(xk, xc), twn[k]);
+    z[e] = make_float2(e2.x - o2.y, e2.y + o2.x);  // 2E + i 2O
+  }
+  __syncthreads();
+  smem_fft(z, rows, hn, G.logn - 1, tw);
+  const float inv_n2 = 1.0f / static_cast<float>(static_cast<size_t>(n) * n);
+  if (mode == 1) {
+    for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
+      const int rr = e / n, m = e - rr * n;
+      const float2 v = z[rr * hn + (m >> 1)];
+      dense_out[(static_cast<size_t>(item) * n + r0 + rr) * n + m] = ((m & 1) ? v.y : v.x) * inv_n2;
+    }
+    return;
+  }
+  const int bx = oxs[item % nox], by = oys[item / nox];
+  const int cell = block_cell[item];
+  const double vs = vsr[2 * item], vr = vsr[2 * item + 1];
+  const double cnum = sqrt(fmax(vs + vr * cell_sumk2[cell], 0.0));
+  const double num = cnum * cnum;
+  for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
+    const int rr = e / n, m = e - rr * n;
+    const int iy = r0 + rr;
+    const int y = by + iy, x = bx + m;
+    if (y < 0 || y >= h || x < 0 || x >= w) continue;
+    const float2 v = z[rr * hn + (m >> 1)];
+    const float f = (m & 1) ? v.y : v.x;
+    const double wy_sig = hwin[iy] * static_cast<double>(inv_n2);
+    const double wy_var = hwin[iy];
+    const double wx = hwin[m];
+    const size_t o = static_cast<size_t>(y) * w + x;
+    acc[o] = static_cast<float>(static_cast<double>(acc[o]) + wy_sig * wx * static_cast<double>(f));
+    var_acc[o] = static_cast<float>(static_cast<double>(var_acc[o]) + wy_var * wx * num);
+  }
+}
+
+// Subsampled block noise: upper median of finite positive var[y][x] over the
+// block's step-(n/64) grid (src/noise.cpp:200-224). One CTA per (block, layer).
+__global__ void __launch_bounds__(512)
+k_block_var(FftGeom G, const float* __restrict__ vs, const float* __restrict__ vr, int w, int h,
+            const int* __restrict__ oxs, const int* __restrict__ oys, int nox, int nitem, double* __restrict__ vsr) {
+  extern __shared__ float vals[];
+  __shared__ int cnt;
+  const int item = blockIdx.x, layer = blockIdx.y;
+  const float* var = layer == 0 ? vs : vr;
+  const int n = G.n;
+  const int step = max(1, n / 64);
+  const int ns = (n + step - 1) / step;
+  int bx, by;
+  if (item < nitem) {
+    bx = oxs[item % nox];
+    by = oys[item / nox];
+  } else {  // the whiten_score_psf window
+    bx = G.extra_bx;
+    by = G.extra_by;
+  }
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  int cap = 1;
+  while (cap < ns * ns) cap <<= 1;
+  for (int e = threadIdx.x; e < cap; e += blockDim.x) vals[e] = INFINITY;
+  __syncthreads();
+  for (int e = threadIdx.x; e < ns * ns; e += blockDim.x) {
+    const int yy = by + (e / ns) * step, xx = bx + (e % ns) * step;
+    if (yy < 0 || yy >= h || xx < 0 || xx >= w) continue;
+    const float v = var[static_cast<size_t>(yy) * w + xx];
+    if (isfinite(v) && v > 0.0f) vals[atomicAdd(&cnt, 1)] = v;
+  }
+  __syncthreads();
+  // bitonic sort ascending of `cap` values (padding +inf)
+  for (int size = 2; size <= cap; size <<= 1)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < cap; i += blockDim.x) {
+        const int j = i ^ stride;
+        if (j > i) {
+          const bool up = (i & size) == 0;
+          const float a = vals[i], b = vals[j];
+          if ((a > b) == up) {
+            vals[i] = b;
+            vals[j] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  if (threadIdx.x == 0) vsr[2 * item + layer] = cnt ? static_cast<double>(vals[cnt / 2]) : 0.0;
+}
+
+// Local kernel per cell: K = sum_n float(a_n(cx,cy)) phi_n (exact thin-plate
+// fields at the cell's representative block centre), sum K^2 in FP64, and its
+// zero-phase embedding into an n x n real image (src/noise.cpp:65-84, 167-189,
+// 329-343). `dense` must be zeroed beforehand.
+__global__ void __launch_bounds__(256)
+k_local_kernels(FftGeom G, TpsDev t, const double* __restrict__ theta, int nc, const float* __restrict__ phi,
+                int ks, const double* __restrict__ centres, double* __restrict__ sumk2, float* __restrict__ dense,
+                float* __restrict__ kern_out) {
+  extern __shared__ float kk[];
+  __shared__ float an[64];
+  __shared__ double red[256];
+  const int cell = blockIdx.x, n = G.n;
+  if (threadIdx.x == 0) {
+    double d[64];
+    const double cx = centres[2 * cell], cy = centres[2 * cell + 1];
+    const int k = t.k, nr = k - 3;
+    const double ux = (cx - t.cx) / t.scale, uy = (cy - t.cy) / t.scale;
+    for (int m = 0; m < nr; ++m) d[m] = 0.0;
+    for (int j = 0; j < k; ++j) {
+      const double dx = ux - t.kn[2 * j], dy = uy - t.kn[2 * j + 1];
+      const double r2 = dx * dx + dy * dy;
+      const double s = r2 <= 0.0 ? 0.0 : 0.5 * r2 * log(r2);
+      for (int m = 0; m < nr; ++m) d[m] = fma(s, t.z[j * nr + m], d[m]);
+    }
+    d[nr] = 1.0;
+    d[nr + 1] = ux;
+    d[nr + 2] = uy;
+    for (int q = 0; q < nc; ++q) {
+      double f = 0.0;
+      for (int m = 0; m < k; ++m) f = fma(d[m], theta[q * k + m], f);
+      an[q] = static_cast<float>(f);
+    }
+  }
+  __syncthreads();
+  const int r = ks / 2;
+  double part = 0.0;
+  for (int i = threadIdx.x; i < ks * ks; i += blockDim.x) {
+    float v = 0.0f;
+    for (int q = 0; q < nc; ++q) v = __fmaf_rn(an[q], phi[static_cast<size_t>(q) * ks * ks + i], v);
+    kk[i] = v;
+    part = fma(static_cast<double>(v), static_cast<double>(v), part);
+    const int ky = i / ks, kx = i - ky * ks;
+    const int gy = ((ky - r) % n + n) % n, gx = ((kx - r) % n + n) % n;
+    if (dense) dense[(static_cast<size_t>(cell) * n + gy) * n + gx] = v;
+    if (kern_out) kern_out[static_cast<size_t>(cell) * ks * ks + i] = v;
+  }
+  red[threadIdx.x] = part;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < static_cast<unsigned>(o)) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && sumk2) sumk2[cell] = red[0];
+}
+
+// Normalise by the separable Hann weight sum (src/noise.cpp:458-479).
+__global__ void k_ola_normalise(int w, int h, const double* __restrict__ wx_total, const double* __restrict__ wy_total,
+                                float* __restrict__ acc, float* __restrict__ var_acc) {
+  const int64_t n = static_cast<int64_t>(w) * h;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int x = static_cast<int>(i % w), y = static_cast<int>(i / w);
+    const double ws = wy_total[y] * wx_total[x];
+    if (ws > 0.0) {
+      acc[i] = static_cast<float>(static_cast<double>(acc[i]) / ws);
+      var_acc[i] = static_cast<float>(static_cast<double>(var_acc[i]) / ws);
+    } else {
+      acc[i] = 0.0f;
+      var_acc[i] = 0.0f;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+static size_t rows_smem(const FftGeom& g) {
+  const int hn = g.n / 2;
+  return sizeof(float2) * (static_cast<size_t>(g.rows_per_cta) * hn + hn / 2 + 1 + hn + 1);
+}
+static size_t cols_smem(const FftGeom& g) {
+  return sizeof(float2) * (static_cast<size_t>(g.cols_per_cta) * g.n + g.n / 2 + 1);
+}
+
+FftGeom make_fft_geom(int n) {
+  FftGeom g;
+  g.n = n;
+  g.logn = 0;
+  while ((1 << g.logn) < n) ++g.logn;
+  g.rows_per_cta = std::max(1, std::min(n, 16384 / std::max(n / 2, 1)));  // <= 128 KB of spectrum
+  g.rows_per_cta = std::min(g.rows_per_cta, 64);
+  g.cols_per_cta = std::max(1, std::min(n / 2 + 1, 8192 / n));
+  return g;
+}
+
+void launch_rows_fwd(cudaStream_t s, const FftGeom& g, int mode, int nitems, const float* src, int w, int h,
+                     const int* oxs, const int* oys, int nox, float2* spec) {
+  const size_t smem = rows_smem(g);
+  DGPU_CUDA(cudaFuncSetAttribute(k_rows_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  dim3 grid(nitems, (g.n + g.rows_per_cta - 1) / g.rows_per_cta);
+  k_rows_fwd<<<grid, 256, smem, s>>>(g, mode, src, w, h, oxs, oys, nox, spec);
+  DGPU_LAUNCH("k_rows_fwd");
+}
+
+void launch_cols(cudaStream_t s, const FftGeom& g, int mode, int nitems, float2* spec, const double* cell_power,
+                 const double* cell_sumk2, const int* block_cell, const double* vsr, double* power_out) {
+  const size_t smem = cols_smem(g);
+  DGPU_CUDA(cudaFuncSetAttribute(k_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  dim3 grid(nitems, (g.n / 2 + 1 + g.cols_per_cta - 1) / g.cols_per_cta);
+  k_cols<<<grid, 256, smem, s>>>(g, mode, spec, cell_power, cell_sumk2, block_cell, vsr, power_out);
+  DGPU_LAUNCH("k_cols");
+}
+
+void launch_rows_inv(cudaStream_t s, const FftGeom& g, int mode, int nitems, const float2* spec, const int* items,
+                     int w, int h, const int* oxs, const int* oys, int nox, const double* hwin, const double* vsr,
+                     const double* cell_sumk2, const int* block_cell, float* acc, float* var_acc, float* dense_out) {
+  if (nitems == 0) return;
+  const size_t smem = rows_smem(g);
+  DGPU_CUDA(cudaFuncSetAttribute(k_rows_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  dim3 grid(nitems, (g.n + g.rows_per_cta - 1) / g.rows_per_cta);
+  k_rows_inv<<<grid, 256, smem, s>>>(g, mode, spec, items, w, h, oxs, oys, nox, hwin, vsr, cell_sumk2, block_cell,
+                                     acc, var_acc, dense_out);
+  DGPU_LAUNCH("k_rows_inv");
+}
+
+void launch_block_var(cudaStream_t s, const FftGeom& g, int nitems, int nextra, const float* vs, const float* vr,
+                      int w, int h, const int* oxs, const int* oys, int nox, double* vsr) {
+  const int step = std::max(1, g.n / 64);
+  const int ns = (g.n + step - 1) / step;
+  int cap = 1;
+  while (cap < ns * ns) cap <<= 1;
+  const size_t smem = sizeof(float) * cap;
+  DGPU_CUDA(cudaFuncSetAttribute(k_block_var, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  dim3 grid(nitems + nextra, 2);
+  k_block_var<<<grid, 512, smem, s>>>(g, vs, vr, w, h, oxs, oys, nox, nitems, vsr);
+  DGPU_LAUNCH("k_block_var");
+}
+
+void launch_local_kernels(cudaStream_t s, const FftGeom& g, int ncell, const TpsDev& t, const double* theta, int nc,
+                          const float* phi, int ks, const double* centres, double* sumk2, float* dense,
+                          float* kern_out) {
+  const size_t smem = sizeof(float) * static_cast<size_t>(ks) * ks;
+  DGPU_CUDA(cudaFuncSetAttribute(k_local_kernels, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  k_local_kernels<<<ncell, 256, smem, s>>>(g, t, theta, nc, phi, ks, centres, sumk2, dense, kern_out);
+  DGPU_LAUNCH("k_local_kernels");
+}
+
+void launch_ola_normalise(cudaStream_t s, int w, int h, const double* wx_total, const double* wy_total, float* acc,
+                          float* var_acc) {
+  const int64_t n = static_cast<int64_t>(w) * h;
+  const int blocks = static_cast<int>(std::min<int64_t>((n + 255) / 256, 148 * 16));
+  k_ola_normalise<<<blocks, 256, 0, s>>>(w, h, wx_total, wy_total, acc, var_acc);
+  DGPU_LAUNCH("k_ola_normalise");
+}
+
+}  // namespace dgpu

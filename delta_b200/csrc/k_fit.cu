@@ -1,0 +1,593 @@
+// Stamp fit kernels (reference src/fit.cpp:63-511, src/solve.cpp:70-145):
+//   * per-stamp gather: sanitised reference patch (stamp + kernel halo, clipped
+//     to the frame), per-stamp separable B_n in shared memory, pixel validity,
+//     row emission into fixed per-stamp slots (stamp-major, then y, then x --
+//     the reference's merged row order);
+//   * thin-plate design rows (FP64);
+//   * normal equations in the Kronecker-packed form
+//       M[(c,m),(c',m')] = G[{c,c'}][{m,m'}],
+//       G = sum_i w_i vec(b_i b_i^T)_sym vec(d_i d_i^T)_sym^T,  b_i = [bn_i, 1],
+//     a (nf(nf+1)/2) x N x (k(k+1)/2) contraction -- 1.8x fewer products than
+//     the P x P rank update -- in FP64 or FP32 SIMT with FP64 split-K reduction;
+//   * rhs / ywy / active-row count, and the FP64 residual right-hand side
+//     X^T W (t - X theta) used by the refinement step;
+//   * per-stamp chi^2 and the K^2 (x) Var_c reweight with K frozen at each stamp
+//     centre (src/fit.cpp:38-59, 389-454).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "dev_common.cuh"
+#include "fit_internal.h"
+
+namespace dgpu {
+
+__device__ __forceinline__ double tps_green_dev(double r2) { return r2 <= 0.0 ? 0.0 : 0.5 * r2 * log(r2); }
+
+// design(p) = [sigma Z | 1 | u | v] (src/spatial.cpp:67-97).
+__device__ void design_row_dev(const TpsDev& t, double x, double y, double* out) {
+  const int k = t.k, nr = k - 3;
+  const double ux = (x - t.cx) / t.scale, uy = (y - t.cy) / t.scale;
+  for (int m = 0; m < nr; ++m) out[m] = 0.0;
+  for (int j = 0; j < k; ++j) {
+    const double dx = ux - t.kn[2 * j], dy = uy - t.kn[2 * j + 1];
+    const double s = tps_green_dev(dx * dx + dy * dy);
+    for (int m = 0; m < nr; ++m) out[m] = fma(s, t.z[j * nr + m], out[m]);
+  }
+  out[nr] = 1.0;
+  out[nr + 1] = ux;
+  out[nr + 2] = uy;
+}
+
+// ---------------------------------------------------------------------------
+// Stamp gather (src/fit.cpp:117-194).
+// ---------------------------------------------------------------------------
+template <int NX>
+__global__ void __launch_bounds__(256)
+k_stamp_gather(StampGeom g, const int* __restrict__ stamp_x, const int* __restrict__ stamp_y,
+               const float* __restrict__ sci, const float* __restrict__ ref,
+               const float* __restrict__ vs, const float* __restrict__ vr,
+               const uint8_t* __restrict__ sm, const uint8_t* __restrict__ rm,
+               const float* __restrict__ taps, const int2* __restrict__ orders,
+               const float* __restrict__ fillp, FitRows R) {
+  extern __shared__ __align__(16) float fsm[];
+  const int s = blockIdx.x;
+  const int tid = threadIdx.x;
+  const size_t base = static_cast<size_t>(s) * g.SS;
+  const int nc = g.nc, ks = g.ks, kh = g.r;
+  for (int i = tid; i < g.SS; i += blockDim.x) {
+    R.valid[base + i] = 0;
+    R.t[base + i] = 0.0;
+    R.vt[base + i] = 0.0;
+    R.vc[base + i] = 0.0;
+    R.px[base + i] = 0;
+    R.py[base + i] = 0;
+  }
+  for (int i = tid; i < g.SS * nc; i += blockDim.x) R.bn[base * nc + i] = 0.0;
+  const int cx = stamp_x[s], cy = stamp_y[s];
+  const int x0 = max(0, cx - g.sr), x1 = min(g.w - 1, cx + g.sr);
+  const int y0 = max(0, cy - g.sr), y1 = min(g.h - 1, cy + g.sr);
+  __shared__ int s_used;
+  if (tid == 0) s_used = 0;
+  if (x1 < x0 || y1 < y0) {
+    if (tid == 0) R.stamp_used[s] = 0;
+    return;
+  }
+  const int ex0 = max(0, x0 - g.r), ex1 = min(g.w - 1, x1 + g.r);
+  const int ey0 = max(0, y0 - g.r), ey1 = min(g.h - 1, y1 + g.r);
+  const int pw = ex1 - ex0 + 1, ph = ey1 - ey0 + 1;
+  const int sw = x1 - x0 + 1, shh = y1 - y0 + 1;
+  float* patch = fsm;                           // ph x pw
+  float* tx = patch + g.pmax * g.pmax;          // NX x ph x sw
+  float* kt = tx + NX * g.pmax * g.S;           // NX x ks
+  const float fill = *fillp;
+  for (int i = tid; i < NX * ks; i += blockDim.x) kt[i] = taps[i];
+  for (int i = tid; i < ph * pw; i += blockDim.x) {
+    const int yy = i / pw, xx = i - yy * pw;
+    const size_t idx = static_cast<size_t>(ey0 + yy) * g.w + ex0 + xx;
+    const float v = ref[idx];
+    const bool bad = (rm && rm[idx] != 0) || !isfinite(v);
+    patch[i] = bad ? fill : v;
+  }
+  __syncthreads();
+  // x-pass over every patch row, stamp columns only (out-of-patch taps skipped).
+  for (int i = tid; i < ph * sw; i += blockDim.x) {
+    const int yy = i / sw, lx = i - yy * sw;
+    const int pc = x0 - ex0 + lx;
+    float acc[NX];
+#pragma unroll
+    for (int q = 0; q < NX; ++q) acc[q] = 0.0f;
+    for (int j = 0; j < ks; ++j) {
+      const int sc = pc + kh - j;
+      if (sc < 0 || sc >= pw) continue;
+      const float v = patch[yy * pw + sc];
+#pragma unroll
+      for (int q = 0; q < NX; ++q) acc[q] = __fmaf_rn(kt[q * ks + j], v, acc[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < NX; ++q) tx[(q * ph + yy) * sw + lx] = acc[q];
+  }
+  __syncthreads();
+  int used = 0;
+  for (int i = tid; i < shh * sw; i += blockDim.x) {
+    const int ly = i / sw, lx = i - ly * sw;
+    const int y = y0 + ly, x = x0 + lx;
+    const size_t idx = static_cast<size_t>(y) * g.w + x;
+    if (sm && sm[idx] != 0) continue;
+    if (rm && rm[idx] != 0) continue;
+    const float sv = sci[idx];
+    if (!isfinite(sv)) continue;
+    const double vtv = vs ? static_cast<double>(vs[idx]) : 0.0;
+    const double vcv = (g.have_cvar && vr) ? static_cast<double>(vr[idx]) : 0.0;
+    if (g.have_var && !(vtv + vcv > 0.0)) continue;
+    const int prow = y - ey0;
+    const size_t ri = base + static_cast<size_t>(y - (cy - g.sr)) * g.S + (x - (cx - g.sr));
+    bool fin = true;
+    for (int n = 0; n < nc; ++n) {
+      const int2 o = orders[n];
+      const float* ky = kt + o.y * ks;
+      const float* col = tx + static_cast<size_t>(o.x) * ph * sw + lx;
+      float acc = 0.0f;
+      for (int j = 0; j < ks; ++j) {
+        const int sr2 = prow + kh - j;
+        if (sr2 < 0 || sr2 >= ph) continue;
+        acc = __fmaf_rn(ky[j], col[sr2 * sw], acc);
+      }
+      if (!isfinite(acc)) fin = false;
+      R.bn[ri * nc + n] = static_cast<double>(acc);
+    }
+    if (!fin) {
+      for (int n = 0; n < nc; ++n) R.bn[ri * nc + n] = 0.0;
+      continue;
+    }
+    R.valid[ri] = 1;
+    R.t[ri] = static_cast<double>(sv);
+    R.vt[ri] = vtv;
+    R.vc[ri] = vcv;
+    R.px[ri] = x;
+    R.py[ri] = y;
+    used = 1;
+  }
+  if (used) atomicOr(&s_used, 1);
+  __syncthreads();
+  if (tid == 0) R.stamp_used[s] = s_used;
+}
+
+template <int NX>
+static void launch_gather_t(cudaStream_t st, const StampGeom& g, size_t smem, int n_stamps,
+                            const int* sx, const int* sy, const float* sci, const float* ref,
+                            const float* vs, const float* vr, const uint8_t* sm, const uint8_t* rm,
+                            const float* taps, const int2* orders, const float* fill, const FitRows& R) {
+  auto kern = k_stamp_gather<NX>;
+  DGPU_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  kern<<<n_stamps, 256, smem, st>>>(g, sx, sy, sci, ref, vs, vr, sm, rm, taps, orders, fill, R);
+  DGPU_LAUNCH("k_stamp_gather");
+}
+
+void launch_stamp_gather(cudaStream_t st, const StampGeom& g, int n_stamps, const int* sx, const int* sy,
+                         const float* sci, const float* ref, const float* vs, const float* vr,
+                         const uint8_t* sm, const uint8_t* rm, const float* taps, const int2* orders,
+                         const float* fill, const FitRows& R) {
+  if (n_stamps == 0) return;
+  const int nx = g.n_max + 1;
+  const size_t smem = sizeof(float) * (static_cast<size_t>(g.pmax) * g.pmax +
+                                       static_cast<size_t>(nx) * g.pmax * g.S + static_cast<size_t>(nx) * g.ks);
+  if (smem > 200 * 1024) fail(DGPU_ERR_INVALID, "fit_kernel: stamp + kernel footprint too large");
+  switch (nx) {
+#define DGPU_G(N) case N: launch_gather_t<N>(st, g, smem, n_stamps, sx, sy, sci, ref, vs, vr, sm, rm, taps, orders, fill, R); break;
+    DGPU_G(1) DGPU_G(2) DGPU_G(3) DGPU_G(4) DGPU_G(5) DGPU_G(6) DGPU_G(7) DGPU_G(8) DGPU_G(9) DGPU_G(10) DGPU_G(11)
+#undef DGPU_G
+    default: fail(DGPU_ERR_INVALID, "fit_kernel: n_max above 10 is not supported");
+  }
+}
+
+// Design rows + first-pass weights 1/(Var_t + Var_c) (src/fit.cpp:248-250, 282-287).
+__global__ void k_design_weights(int64_t N, TpsDev t, FitRows R, int have_var) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < N;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double* d = R.d + i * t.k;
+    if (!R.valid[i]) {
+      for (int m = 0; m < t.k; ++m) d[m] = 0.0;
+      R.w[i] = 0.0;
+      continue;
+    }
+    design_row_dev(t, static_cast<double>(R.px[i]), static_cast<double>(R.py[i]), d);
+    R.w[i] = have_var ? 1.0 / (R.vt[i] + R.vc[i]) : 1.0;
+  }
+}
+
+void launch_design_weights(cudaStream_t st, int64_t N, const TpsDev& t, const FitRows& R, int have_var) {
+  const int blocks = static_cast<int>(std::min<int64_t>((N + 255) / 256, 148 * 8));
+  k_design_weights<<<std::max(blocks, 1), 256, 0, st>>>(N, t, R, have_var);
+  DGPU_LAUNCH("k_design_weights");
+}
+
+// ---------------------------------------------------------------------------
+// Kronecker-packed normal equations, SIMT (FP64 or FP32 products/accumulation).
+// ---------------------------------------------------------------------------
+constexpr int kNeT = 64;  // u and v tile
+constexpr int kNeR = 32;  // rows per shared-memory chunk
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_normal_kron(int64_t N, int nc, int k, int SS, FitRows R, const uint8_t* __restrict__ accepted,
+              const int2* __restrict__ upairs, int Mu, const int2* __restrict__ vpairs, int Nv,
+              int64_t rows_per_split, double* __restrict__ gpart) {
+  __shared__ T Us[kNeR][kNeT + 1];
+  __shared__ T Vs[kNeR][kNeT + 1];
+  const int u0 = blockIdx.x * kNeT, v0 = blockIdx.y * kNeT;
+  const int64_t rbeg = static_cast<int64_t>(blockIdx.z) * rows_per_split;
+  const int64_t rend = min(N, rbeg + rows_per_split);
+  const int tid = threadIdx.x;
+  const int tu = tid % 16, tv = tid / 16;
+  T acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
+  for (int64_t r0 = rbeg; r0 < rend; r0 += kNeR) {
+    for (int e = tid; e < kNeR * kNeT; e += blockDim.x) {
+      const int rr = e / kNeT, cc = e - rr * kNeT;
+      const int64_t row = r0 + rr;
+      const bool act = row < rend && R.valid[row] && accepted[row / SS];
+      T uval = T(0), vval = T(0);
+      if (act) {
+        const int u = u0 + cc;
+        if (u < Mu) {
+          const int2 p = upairs[u];
+          const T b1 = p.x < nc ? static_cast<T>(R.bn[row * nc + p.x]) : T(1);
+          const T b2 = p.y < nc ? static_cast<T>(R.bn[row * nc + p.y]) : T(1);
+          uval = b1 * b2;
+        }
+        const int v = v0 + cc;
+        if (v < Nv) {
+          const int2 q = vpairs[v];
+          const T wv = static_cast<T>(R.w[row]);
+          vval = (wv * static_cast<T>(R.d[row * k + q.x])) * static_cast<T>(R.d[row * k + q.y]);
+        }
+      }
+      Us[rr][cc] = uval;
+      Vs[rr][cc] = vval;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int rr = 0; rr < kNeR; ++rr) {
+      T a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = Us[rr][tu * 4 + i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Vs[rr][tv * 4 + j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+  double* out = gpart + static_cast<size_t>(blockIdx.z) * Mu * Nv;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int u = u0 + tu * 4 + i;
+    if (u >= Mu) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int v = v0 + tv * 4 + j;
+      if (v < Nv) out[static_cast<size_t>(u) * Nv + v] = static_cast<double>(acc[i][j]);
+    }
+  }
+}
+
+// G = sum_z gpart[z] (fixed order), then M[p][q] = G[{c,c'}][{m,m'}].
+__global__ void k_reduce_g(int nsplit, int MuNv, const double* __restrict__ gpart, double* __restrict__ g) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < MuNv; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int z = 0; z < nsplit; ++z) s += gpart[static_cast<size_t>(z) * MuNv + i];
+    g[i] = s;
+  }
+}
+
+__device__ __forceinline__ int sym_pair(int a, int b, int n) {
+  if (a > b) {
+    const int t = a;
+    a = b;
+    b = t;
+  }
+  return a * n - a * (a - 1) / 2 + (b - a);
+}
+
+__global__ void k_expand_m(int nf, int k, int Nv, const double* __restrict__ g, double* __restrict__ M) {
+  const int P = nf * k;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P * P; i += gridDim.x * blockDim.x) {
+    const int p = i / P, q = i - p * P;
+    const int c = p / k, m = p - c * k, c2 = q / k, m2 = q - c2 * k;
+    M[i] = g[static_cast<size_t>(sym_pair(c, c2, nf)) * Nv + sym_pair(m, m2, k)];
+  }
+}
+
+void launch_normal_equations(Context& c, int prec, int64_t N, int nc, int k, int SS, const FitRows& R,
+                             const uint8_t* accepted, double* M) {
+  cudaStream_t st = c.stream;
+  const int nf = nc + 1;
+  const int Mu = nf * (nf + 1) / 2, Nv = k * (k + 1) / 2;
+  std::vector<int2> up, vp;
+  for (int a = 0; a < nf; ++a)
+    for (int b = a; b < nf; ++b) up.push_back(make_int2(a, b));
+  for (int a = 0; a < k; ++a)
+    for (int b = a; b < k; ++b) vp.push_back(make_int2(a, b));
+  int2* dpairs = static_cast<int2*>(c.slot(kSlotFit10, sizeof(int2) * (Mu + Nv)));
+  DGPU_CUDA(cudaMemcpyAsync(dpairs, up.data(), sizeof(int2) * Mu, cudaMemcpyHostToDevice, st));
+  DGPU_CUDA(cudaMemcpyAsync(dpairs + Mu, vp.data(), sizeof(int2) * Nv, cudaMemcpyHostToDevice, st));
+  const int gx = (Mu + kNeT - 1) / kNeT, gy = (Nv + kNeT - 1) / kNeT;
+  // Split K (rows) so the grid covers the GPU a few times over.
+  const int64_t target_splits = std::max<int64_t>(1, (148 * 6) / (gx * gy));
+  int64_t rps = std::max<int64_t>(kNeR * 8, (N + target_splits - 1) / target_splits);
+  rps = (rps + kNeR - 1) / kNeR * kNeR;
+  const int nsplit = static_cast<int>((N + rps - 1) / rps);
+  double* gpart = static_cast<double*>(c.slot(kSlotFit11, sizeof(double) * static_cast<size_t>(nsplit) * Mu * Nv));
+  double* g = static_cast<double*>(c.slot(kSlotFit12, sizeof(double) * static_cast<size_t>(Mu) * Nv));
+  dim3 grid(gx, gy, nsplit);
+  if (prec == DGPU_PREC_FP32)
+    k_normal_kron<float><<<grid, 256, 0, st>>>(N, nc, k, SS, R, accepted, dpairs, Mu, dpairs + Mu, Nv, rps, gpart);
+  else
+    k_normal_kron<double><<<grid, 256, 0, st>>>(N, nc, k, SS, R, accepted, dpairs, Mu, dpairs + Mu, Nv, rps, gpart);
+  DGPU_LAUNCH("k_normal_kron");
+  k_reduce_g<<<std::min(148 * 4, (Mu * Nv + 255) / 256), 256, 0, st>>>(nsplit, Mu * Nv, gpart, g);
+  DGPU_LAUNCH("k_reduce_g");
+  const int P = nf * k;
+  k_expand_m<<<std::min(148 * 8, (P * P + 255) / 256), 256, 0, st>>>(nf, k, Nv, g, M);
+  DGPU_LAUNCH("k_expand_m");
+}
+
+// ---------------------------------------------------------------------------
+// rhs = sum_i w_i e_i (b_i (x) d_i) with e_i = t_i (plain rhs) or
+// e_i = t_i - x_i . theta (FP64 refinement residual), plus ywy = sum w t^2
+// and the active-row count. One CTA per row chunk, rows staged in shared memory.
+// ---------------------------------------------------------------------------
+constexpr int kRhsRows = 32;
+
+__global__ void __launch_bounds__(256)
+k_rhs(int64_t N, int nc, int k, int SS, FitRows R, const uint8_t* __restrict__ accepted,
+      const double* __restrict__ theta, int64_t rows_per_split, double* __restrict__ rpart,
+      double* __restrict__ ypart, long long* __restrict__ npart) {
+  extern __shared__ double rsm[];
+  const int nf = nc + 1, P = nf * k;
+  double* sb = rsm;                       // kRhsRows x nf
+  double* sd = sb + kRhsRows * nf;        // kRhsRows x k
+  double* se = sd + kRhsRows * k;         // kRhsRows : w * e
+  double* sy = se + kRhsRows;             // kRhsRows : w * t * t
+  int* sa = reinterpret_cast<int*>(sy + kRhsRows);  // active flags
+  const int64_t rbeg = static_cast<int64_t>(blockIdx.x) * rows_per_split;
+  const int64_t rend = min(N, rbeg + rows_per_split);
+  const int tid = threadIdx.x;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};  // p = tid + 256*j
+  double yacc = 0.0;
+  long long nacc = 0;
+  for (int64_t r0 = rbeg; r0 < rend; r0 += kRhsRows) {
+    for (int e = tid; e < kRhsRows; e += blockDim.x) {
+      const int64_t row = r0 + e;
+      const bool act = row < rend && R.valid[row] && accepted[row / SS];
+      sa[e] = act ? 1 : 0;
+      double we = 0.0, wtt = 0.0;
+      if (act) {
+        double t = R.t[row];
+        const double wv = R.w[row];
+        wtt = wv * t * t;
+        if (theta) {
+          double model = 0.0;
+          for (int c2 = 0; c2 < nf; ++c2) {
+            double f = 0.0;
+            for (int m = 0; m < k; ++m) f = fma(R.d[row * k + m], theta[c2 * k + m], f);
+            const double b = c2 < nc ? R.bn[row * nc + c2] : 1.0;
+            model = fma(f, b, model);
+          }
+          t = t - model;
+        }
+        we = wv * t;
+      }
+      se[e] = we;
+      sy[e] = wtt;
+    }
+    for (int e = tid; e < kRhsRows * nf; e += blockDim.x) {
+      const int rr = e / nf, c2 = e - rr * nf;
+      const int64_t row = r0 + rr;
+      double b = 0.0;
+      if (row < rend) b = c2 < nc ? R.bn[row * nc + c2] : 1.0;
+      sb[e] = b;
+    }
+    for (int e = tid; e < kRhsRows * k; e += blockDim.x) {
+      const int rr = e / k, m = e - rr * k;
+      const int64_t row = r0 + rr;
+      sd[e] = row < rend ? R.d[row * k + m] : 0.0;
+    }
+    __syncthreads();
+    for (int j = 0; j < 4; ++j) {
+      const int p = tid + 256 * j;
+      if (p >= P) break;
+      const int c2 = p / k, m = p - c2 * k;
+      double a = acc[j];
+      for (int rr = 0; rr < kRhsRows; ++rr) a = fma(se[rr] * sb[rr * nf + c2], sd[rr * k + m], a);
+      acc[j] = a;
+    }
+    if (tid == 0)
+      for (int rr = 0; rr < kRhsRows; ++rr) {
+        yacc += sy[rr];
+        nacc += sa[rr];
+      }
+    __syncthreads();
+  }
+  for (int j = 0; j < 4; ++j) {
+    const int p = tid + 256 * j;
+    if (p < P) rpart[static_cast<size_t>(blockIdx.x) * P + p] = acc[j];
+  }
+  if (tid == 0) {
+    ypart[blockIdx.x] = yacc;
+    npart[blockIdx.x] = nacc;
+  }
+}
+
+__global__ void k_reduce_rhs(int nsplit, int P, const double* __restrict__ rpart, const double* __restrict__ ypart,
+                             const long long* __restrict__ npart, double* __restrict__ rhs, double* ywy,
+                             long long* n) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int z = 0; z < nsplit; ++z) s += rpart[static_cast<size_t>(z) * P + p];
+    rhs[p] = s;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    double y = 0.0;
+    long long c = 0;
+    for (int z = 0; z < nsplit; ++z) {
+      y += ypart[z];
+      c += npart[z];
+    }
+    if (ywy) *ywy = y;
+    if (n) *n = c;
+  }
+}
+
+void launch_rhs(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, const uint8_t* accepted,
+                const double* theta, double* rhs, double* ywy, long long* n) {
+  cudaStream_t st = c.stream;
+  const int P = (nc + 1) * k;
+  if (P > 1024) fail(DGPU_ERR_INVALID, "fit: more than 1024 unknowns is not supported");
+  int64_t rps = std::max<int64_t>(kRhsRows * 16, (N + 148 * 2 - 1) / (148 * 2));
+  rps = (rps + kRhsRows - 1) / kRhsRows * kRhsRows;
+  const int nsplit = static_cast<int>(std::max<int64_t>(1, (N + rps - 1) / rps));
+  char* buf = static_cast<char*>(c.slot(kSlotFit13, (sizeof(double) * (P + 1) + sizeof(long long)) * nsplit + 64));
+  double* rpart = reinterpret_cast<double*>(buf);
+  double* ypart = rpart + static_cast<size_t>(nsplit) * P;
+  long long* npart = reinterpret_cast<long long*>(ypart + nsplit);
+  const size_t smem = sizeof(double) * (kRhsRows * (nc + 1) + kRhsRows * k + 2 * kRhsRows) + sizeof(int) * kRhsRows;
+  k_rhs<<<nsplit, 256, smem, st>>>(N, nc, k, SS, R, accepted, theta, rps, rpart, ypart, npart);
+  DGPU_LAUNCH("k_rhs");
+  k_reduce_rhs<<<(P + 255) / 256, 256, 0, st>>>(nsplit, P, rpart, ypart, npart, rhs, ywy, n);
+  DGPU_LAUNCH("k_reduce_rhs");
+}
+
+// ---------------------------------------------------------------------------
+// Per-stamp chi^2 (src/fit.cpp:389-406): sum of w r^2 over the stamp's active
+// rows / count; NaN for stamps without active rows.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_stamp_chi2(int nc, int k, int SS, FitRows R, const uint8_t* __restrict__ accepted,
+             const double* __restrict__ theta, double* __restrict__ chi2, int* __restrict__ cnt) {
+  __shared__ double ssum[256];
+  __shared__ int scnt[256];
+  const int s = blockIdx.x;
+  const int nf = nc + 1;
+  double acc = 0.0;
+  int n = 0;
+  if (accepted[s]) {
+    for (int i = threadIdx.x; i < SS; i += blockDim.x) {
+      const size_t row = static_cast<size_t>(s) * SS + i;
+      if (!R.valid[row]) continue;
+      double model = 0.0;
+      for (int c2 = 0; c2 < nf; ++c2) {
+        double f = 0.0;
+        for (int m = 0; m < k; ++m) f = fma(R.d[row * k + m], theta[c2 * k + m], f);
+        const double b = c2 < nc ? R.bn[row * nc + c2] : 1.0;
+        model = fma(f, b, model);
+      }
+      const double res = R.t[row] - model;
+      acc += R.w[row] * res * res;
+      ++n;
+    }
+  }
+  ssum[threadIdx.x] = acc;
+  scnt[threadIdx.x] = n;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < static_cast<unsigned>(o)) {
+      ssum[threadIdx.x] += ssum[threadIdx.x + o];
+      scnt[threadIdx.x] += scnt[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    cnt[s] = scnt[0];
+    chi2[s] = scnt[0] > 0 ? ssum[0] / scnt[0] : __longlong_as_double(0x7ff8000000000000ll);
+  }
+}
+
+void launch_stamp_chi2(cudaStream_t st, int n_stamps, int nc, int k, int SS, const FitRows& R,
+                       const uint8_t* accepted, const double* theta, double* chi2, int* cnt) {
+  if (n_stamps == 0) return;
+  k_stamp_chi2<<<n_stamps, 256, 0, st>>>(nc, k, SS, R, accepted, theta, chi2, cnt);
+  DGPU_LAUNCH("k_stamp_chi2");
+}
+
+// ---------------------------------------------------------------------------
+// IRLS reweight (src/fit.cpp:411-454): K = sum_n float(a_n(stamp centre)) phi_n
+// squared elementwise; w = 1 / (Var_t + (K^2 (x) Var_c)) over each active row,
+// masked / non-positive / non-finite reference variance skipped, FP64 sum in
+// (dv, du) order. Science-variance only: w = 1 / Var_t.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_reweight(StampGeom g, TpsDev t, const int* __restrict__ stamp_x, const int* __restrict__ stamp_y,
+           FitRows R, const uint8_t* __restrict__ accepted, const int* __restrict__ cnt,
+           const double* __restrict__ theta, const float* __restrict__ phi, const float* __restrict__ vr,
+           const uint8_t* __restrict__ rm) {
+  extern __shared__ __align__(16) float wsm[];
+  const int s = blockIdx.x;
+  if (!accepted[s] || cnt[s] == 0) return;
+  const int ks = g.ks, kk = ks * ks, r = g.r;
+  const int nc = g.nc;
+  float* k2 = wsm;                      // kk
+  __shared__ float an[64];
+  __shared__ double dsh[64];
+  if (g.have_cvar) {
+    if (threadIdx.x == 0) {
+      design_row_dev(t, static_cast<double>(stamp_x[s]), static_cast<double>(stamp_y[s]), dsh);
+      for (int n = 0; n < nc; ++n) {
+        double f = 0.0;
+        for (int m = 0; m < t.k; ++m) f = fma(dsh[m], theta[n * t.k + m], f);
+        an[n] = static_cast<float>(f);
+      }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kk; i += blockDim.x) {
+      float v = 0.0f;
+      for (int n = 0; n < nc; ++n) v = __fmaf_rn(an[n], phi[static_cast<size_t>(n) * kk + i], v);
+      k2[i] = v * v;
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < g.SS; i += blockDim.x) {
+    const size_t row = static_cast<size_t>(s) * g.SS + i;
+    if (!R.valid[row]) continue;
+    if (g.have_cvar) {
+      const int x = R.px[row], y = R.py[row];
+      double acc = 0.0;
+      for (int dv = -r; dv <= r; ++dv) {
+        const int sy = y - dv;
+        if (sy < 0 || sy >= g.h) continue;
+        const float* krow = k2 + (dv + r) * ks;
+        for (int du = -r; du <= r; ++du) {
+          const int sx = x - du;
+          if (sx < 0 || sx >= g.w) continue;
+          const size_t idx = static_cast<size_t>(sy) * g.w + sx;
+          if (rm && rm[idx] != 0) continue;
+          const float v = vr[idx];
+          if (!(v > 0.0f) || !isfinite(v)) continue;
+          acc = fma(static_cast<double>(krow[du + r]), static_cast<double>(v), acc);
+        }
+      }
+      const double rv = R.vt[row] + acc;
+      if (rv > 0.0) R.w[row] = 1.0 / rv;
+    } else {
+      if (R.vt[row] > 0.0) R.w[row] = 1.0 / R.vt[row];
+    }
+  }
+}
+
+void launch_reweight(cudaStream_t st, const StampGeom& g, int n_stamps, const TpsDev& t, const int* sx,
+                     const int* sy, const FitRows& R, const uint8_t* accepted, const int* cnt,
+                     const double* theta, const float* phi, const float* vr, const uint8_t* rm) {
+  if (n_stamps == 0) return;
+  const size_t smem = sizeof(float) * static_cast<size_t>(g.ks) * g.ks;
+  DGPU_CUDA(cudaFuncSetAttribute(k_reweight, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  k_reweight<<<n_stamps, 256, smem, st>>>(g, t, sx, sy, R, accepted, cnt, theta, phi, vr, rm);
+  DGPU_LAUNCH("k_reweight");
+}
+
+}  // namespace dgpu

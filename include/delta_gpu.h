@@ -130,6 +130,81 @@ int dgpu_photometric_scale_at(const double* knots, int n_knots, const double* th
                               int64_t n_theta, const double* component_sums, int nc,
                               const double* points, int64_t m, double* out);
 
+/* ---- penalised GLS + stamp fit ------------------------------------------------ */
+/* Result of a GLS solve (src/../include/delta/solve.hpp:16-26) plus the
+ * fit_kernel diagnostics (include/delta/fit.hpp:16-37). Array members are
+ * caller buffers: theta[(nc+1)*k], lambda_grid / gcv_curve[n_lambda],
+ * component_sums[nc], stamp_*[n_stamps supplied]; the stamp arrays receive
+ * the n_stamps_total contributing stamps in supplied order. */
+typedef struct {
+  double* theta;
+  double* lambda_grid;
+  double* gcv_curve;
+  double* component_sums;
+  int32_t* stamp_x;
+  int32_t* stamp_y;
+  double* stamp_chi2;
+  uint8_t* stamp_accepted;
+  int n_components;
+  int n_spatial;
+  double lambda;
+  double gcv;
+  double effective_dof;
+  double rss;
+  double reduced_chi2;
+  int64_t n_pixels;
+  int n_stamps_used;
+  int n_stamps_total;
+  int n_stamps_rejected;
+  int64_t cv_exact_design_bytes;
+  int n_lambda_out; /* entries written to lambda_grid / gcv_curve (0 for a fixed-lambda solve) */
+} dgpu_gls_result;
+
+/* fit_kernel, src/bindings.cpp:643-693 -> delta::fit_kernel, src/fit.cpp:63-511
+ * (include/delta/fit.hpp:65-72). Images follow `mem`; knots, stamp lists and
+ * lambda_grid are host arrays. `precision` is a DGPU_PREC_* value selecting the
+ * normal-equation arithmetic (the solve is FP64 in every mode). */
+int dgpu_fit_kernel(dgpu_context* ctx, int mem, int64_t width, int64_t height, const float* science,
+                    const float* reference, const float* science_var, const float* reference_var,
+                    const uint8_t* science_mask, const uint8_t* reference_mask, const double* knots,
+                    int n_knots, const int32_t* stamp_x, const int32_t* stamp_y, int n_stamps,
+                    int stamp_radius, double beta, int n_max, int radius, const double* lambda_grid,
+                    int n_lambda, double clip_sigma, int clip_iterations, int min_stamps, int cv_folds,
+                    int precision, dgpu_gls_result* out);
+
+/* solve_gls / solve_gls_gcv / solve_gls_cv, src/bindings.cpp:530-566 ->
+ * src/solve.cpp:208-225, 421-431. Host arrays: points m x 2, target / weights
+ * m, bn m x nc (row-major), group m (CV). lam is used by solve_gls only. */
+int dgpu_solve_gls(dgpu_context* ctx, const double* knots, int n_knots, const double* points, int64_t m,
+                   const double* target, const double* weights, const double* bn, int nc, double lam,
+                   int precision, dgpu_gls_result* out);
+int dgpu_solve_gls_gcv(dgpu_context* ctx, const double* knots, int n_knots, const double* points, int64_t m,
+                       const double* target, const double* weights, const double* bn, int nc,
+                       const double* lambda_grid, int n_lambda, int precision, dgpu_gls_result* out);
+int dgpu_solve_gls_cv(dgpu_context* ctx, const double* knots, int n_knots, const double* points, int64_t m,
+                      const double* target, const double* weights, const double* bn, int nc,
+                      const double* lambda_grid, int n_lambda, const int32_t* group, int n_groups,
+                      int precision, dgpu_gls_result* out);
+
+/* ---- noise decorrelation (ZOGY) ------------------------------------------------ */
+/* decorrelate, src/bindings.cpp:766-792 -> delta::decorrelate, src/noise.cpp:228-483
+ * (include/delta/noise.hpp:64-68). Outputs: whitened difference and its
+ * post-whitening variance, h x w float32. */
+int dgpu_decorrelate(dgpu_context* ctx, int mem, int64_t width, int64_t height, const float* difference,
+                     const dgpu_model* model, const float* var_science, const float* var_reference, int block,
+                     int kernel_cell_blocks, float* out_difference, float* out_variance);
+/* whiten_score_psf, src/bindings.cpp:796-874 -> delta::whiten_psf,
+ * src/noise.cpp:485-533. psf / out: host, psf_size^2. */
+int dgpu_whiten_score_psf(dgpu_context* ctx, int mem, const float* psf, int psf_size, const dgpu_model* model,
+                          int64_t width, int64_t height, const float* var_science, const float* var_reference,
+                          int block, float* out);
+/* decorrelate_block, src/bindings.cpp:725-745 -> src/noise.cpp:98-137. Host arrays. */
+int dgpu_decorrelate_block(dgpu_context* ctx, const float* image, int n, const float* kernel, int ksize,
+                           double var_science, double var_reference, float* out);
+/* decorrelation_kernel, src/bindings.cpp:748-760 -> src/noise.cpp:139-161. Host arrays. */
+int dgpu_decorrelation_kernel(dgpu_context* ctx, const float* kernel, int ksize, double var_science,
+                              double var_reference, int n, float* out);
+
 /* ---- matched filter ---------------------------------------------------------- */
 /* matched_filter, src/bindings.cpp:878-898 -> src/noise.cpp:535-632
  * (include/delta/noise.hpp:88-93). out: h x w float32. */

@@ -11,6 +11,7 @@ Only tests/, __graft_entry__.smoke() and bench.py's CPU legs may import this.
 from __future__ import annotations
 
 import math
+import os
 
 import numpy as np
 
@@ -921,6 +922,12 @@ def fit_kernel(science, reference, knots, stamp_x, stamp_y, stamp_radius, beta, 
             spacing = tp.min_knot_spacing()
             stamp_width = 2.0 * stamp_radius + 1.0
             use_stamped = spacing > 0.0 and spacing >= 16.0 * stamp_width
+            env = os.environ.get("DELTA_STAMP_APPROX")  # src/fit.cpp:327-328
+            if env is not None:
+                try:
+                    use_stamped = int(env) != 0
+                except ValueError:
+                    use_stamped = False
             if use_stamped:
                 gids = g["stamp"][rows]
                 g2l = {}

@@ -1,0 +1,163 @@
+"""GPU parity of the penalised GLS (GCV / CV / fixed lambda) and the stamp fit
+(IRLS + clipping) against the FP64 oracle, plus the reference's analytic
+solver checks (tests/test_solve.py:24-85 of tkillestein/delta)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from delta_b200 import _core
+from oracle import numpy_ref as nr
+from oracle import refbuild
+
+pytestmark = pytest.mark.gpu
+
+GRID = np.logspace(-6, 6, 25)
+
+
+def _problem(seed=0, n=3000, nc=6, nk=4, noise=0.05):
+    rng = np.random.default_rng(seed)
+    knots = nr.grid_knots(0, 0, 499, 399, nk, nk)
+    pts = np.column_stack([rng.uniform(0, 500, n), rng.uniform(0, 400, n)])
+    bn = rng.standard_normal((n, nc)) * rng.uniform(0.5, 5.0, nc)
+    k = knots.shape[0]
+    theta_true = rng.standard_normal((nc + 1) * k) * 0.3
+    tp = nr.ThinPlate(knots)
+    d = tp.design(pts)
+    c = theta_true.reshape(nc + 1, k).T
+    f = d @ c
+    target = f[:, nc] + np.sum(f[:, :nc] * bn, axis=1) + noise * rng.standard_normal(n)
+    weights = rng.uniform(0.5, 2.0, n)
+    return knots, pts, target, weights, bn, theta_true
+
+
+def test_solve_gls_gcv_matches_oracle():
+    knots, pts, t, w, bn, _ = _problem()
+    got = _core.solve_gls_gcv(knots, pts, t, w, bn, GRID)
+    want = nr.solve_gls_gcv(knots, pts, t, w, bn, GRID)
+    assert got["lambda"] == want["lambda"]
+    np.testing.assert_allclose(got["theta"], want["theta"], rtol=1e-7, atol=1e-9)
+    np.testing.assert_allclose(got["gcv_curve"], want["gcv_curve"], rtol=1e-6)
+    np.testing.assert_allclose(got["effective_dof"], want["effective_dof"], rtol=1e-8)
+    np.testing.assert_allclose(got["rss"], want["rss"], rtol=1e-6)
+    assert got["n_components"] == 6 and got["n_spatial"] == 16
+
+
+def test_solve_gls_fixed_lambda_and_edf_limits():
+    knots, pts, t, w, bn, _ = _problem(1, n=2000, nc=3, nk=3)
+    for lam in (1e-8, 1e-2, 1e8):
+        got = _core.solve_gls(knots, pts, t, w, bn, lam)
+        want = nr.solve_gls(knots, pts, t, w, bn, lam)
+        np.testing.assert_allclose(got["theta"], want["theta"], rtol=1e-7, atol=1e-9)
+        np.testing.assert_allclose(got["effective_dof"], want["effective_dof"], rtol=1e-7, atol=1e-6)
+        assert got["lambda_grid"].size == 0 and got["gcv_curve"].size == 0
+    p = 4 * 9
+    assert abs(_core.solve_gls(knots, pts, t, w, bn, 1e-10)["effective_dof"] - p) < 1e-3
+    assert abs(_core.solve_gls(knots, pts, t, w, bn, 1e12)["effective_dof"] - 3 * 4) < 1e-2
+
+
+def test_solve_gls_exact_recovery():
+    knots, pts, t, w, bn, theta = _problem(2, n=2500, nc=3, nk=3, noise=0.0)
+    got = _core.solve_gls(knots, pts, t, w, bn, 1e-10)
+    np.testing.assert_allclose(got["theta"], theta, rtol=1e-5, atol=1e-6)
+
+
+def test_solve_gls_cv_matches_oracle():
+    knots, pts, t, w, bn, _ = _problem(3, n=2400, nc=4, nk=3)
+    group = np.arange(t.size) % 4
+    got = _core.solve_gls_cv(knots, pts, t, w, bn, GRID, group, 4)
+    want = nr.solve_gls_cv(knots, pts, t, w, bn, GRID, group, 4)
+    assert got["lambda"] == want["lambda"]
+    fin = np.isfinite(want["gcv_curve"])
+    assert np.array_equal(np.isfinite(got["gcv_curve"]), fin)
+    np.testing.assert_allclose(got["gcv_curve"][fin], want["gcv_curve"][fin], rtol=1e-6)
+    np.testing.assert_allclose(got["theta"], want["theta"], rtol=1e-7, atol=1e-9)
+    # n_groups < 2 degrades to GCV; bad group ids raise like the reference.
+    g1 = _core.solve_gls_cv(knots, pts, t, w, bn, GRID, group, 1)
+    assert g1["lambda"] == nr.solve_gls_gcv(knots, pts, t, w, bn, GRID)["lambda"]
+    with pytest.raises(RuntimeError):
+        _core.solve_gls_cv(knots, pts, t, w, bn, GRID, group + 10, 4)
+    with pytest.raises(RuntimeError):
+        _core.solve_gls_gcv(knots, pts, t, w, bn, np.zeros(0))
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_reduced_precision_modes_close_to_fp64(precision):
+    knots, pts, t, w, bn, _ = _problem(4, n=6000, nc=6, nk=4, noise=0.05)
+    ref = _core.solve_gls_gcv(knots, pts, t, w, bn, GRID, precision="fp64")
+    got = _core.solve_gls_gcv(knots, pts, t, w, bn, GRID, precision=precision)
+    err = np.linalg.norm(got["theta"] - ref["theta"]) / np.linalg.norm(ref["theta"])
+    assert err < (1e-3 if precision == "fp32" else 1e-6), err
+
+
+# ---------------------------------------------------------------------------- fit
+
+
+def _fit_frame(seed=0, h=220, w=240, n_star=30, stamp_radius=7):
+    rng = np.random.default_rng(seed)
+    ys, xs = np.mgrid[0:h, 0:w]
+    ref = np.full((h, w), 100.0)
+    sci = np.full((h, w), 100.0)
+    pos = []
+    while len(pos) < n_star:
+        x, y = rng.uniform(12, w - 12), rng.uniform(12, h - 12)
+        if all((x - a) ** 2 + (y - b) ** 2 > 20**2 for a, b in pos):
+            pos.append((x, y))
+    for x, y in pos:
+        f = rng.uniform(5e3, 5e4)
+        ref += f / (2 * np.pi * 1.4**2) * np.exp(-((xs - x) ** 2 + (ys - y) ** 2) / (2 * 1.4**2))
+        sg = 2.0 + 0.3 * x / w
+        sci += f / (2 * np.pi * sg**2) * np.exp(-((xs - x) ** 2 + (ys - y) ** 2) / (2 * sg**2))
+    var_r = (ref / 1.5 + 9.0).astype(np.float32)
+    var_s = (sci / 1.5 + 9.0).astype(np.float32)
+    ref = (ref + rng.normal(0, 1, (h, w)) * np.sqrt(var_r)).astype(np.float32)
+    sci = (sci + rng.normal(0, 1, (h, w)) * np.sqrt(var_s)).astype(np.float32)
+    sm = np.zeros((h, w), np.uint8)
+    rm = np.zeros((h, w), np.uint8)
+    rm[:, 57] = 1
+    sm[30:34, 100] = 1
+    sx = np.array([int(round(x)) for x, _ in pos], np.int32)
+    sy = np.array([int(round(y)) for _, y in pos], np.int32)
+    sx[0], sy[0] = 3, 5  # a stamp clipped by the frame edge
+    return sci, ref, var_s, var_r, sm, rm, sx, sy
+
+
+def _oracle_bconv(beta, n_max, r):
+    if refbuild.available():
+        return lambda patch: refbuild.basis_convolve(patch, beta, n_max, r)
+    return lambda patch: nr.basis_convolve(patch, beta, n_max, r).astype(np.float32)
+
+
+@pytest.mark.parametrize("cv_folds,stamped", [(0, False), (3, False), (3, True)])
+def test_fit_kernel_matches_oracle(cv_folds, stamped, monkeypatch):
+    sci, ref, vs, vr, sm, rm, sx, sy = _fit_frame()
+    h, w = sci.shape
+    knots = nr.grid_knots(0, 0, w - 1, h - 1, 3, 3)
+    beta, n_max, sr = 1.2, 3, 7
+    r = nr.default_radius(beta, n_max)
+    monkeypatch.setenv("DELTA_STAMP_APPROX", "1" if stamped else "0")
+    kw = dict(clip_sigma=3.0, clip_iterations=3, min_stamps=5, cv_folds=cv_folds, science_var=vs,
+              reference_var=vr, science_mask=sm, reference_mask=rm)
+    got = _core.fit_kernel(sci, ref, knots, sx, sy, sr, beta, n_max, GRID, **kw)
+    want = nr.fit_kernel(sci, ref, knots, sx, sy, sr, beta, n_max, GRID, basis_convolve_fn=_oracle_bconv(beta, n_max, r),
+                         **kw)
+    for key in ("n_pixels", "n_stamps_total", "n_stamps_used", "n_stamps_rejected", "cv_exact_design_bytes"):
+        assert got[key] == want[key], key
+    assert got["lambda"] == want["lambda"]
+    np.testing.assert_array_equal(got["stamp_x"], want["stamp_x"])
+    np.testing.assert_array_equal(got["stamp_accepted"], want["stamp_accepted"])
+    np.testing.assert_allclose(got["theta"], want["theta"], rtol=1e-6, atol=1e-8 * np.abs(want["theta"]).max())
+    np.testing.assert_allclose(got["stamp_chi2"], want["stamp_chi2"], rtol=1e-6)
+    np.testing.assert_allclose(got["reduced_chi2"], want["reduced_chi2"], rtol=1e-6)
+    np.testing.assert_allclose(got["component_sums"], want["component_sums"], rtol=1e-12, atol=1e-14)
+
+
+def test_fit_kernel_errors():
+    sci, ref, vs, vr, sm, rm, sx, sy = _fit_frame(1)
+    h, w = sci.shape
+    knots = nr.grid_knots(0, 0, w - 1, h - 1, 3, 3)
+    with pytest.raises(RuntimeError):
+        _core.fit_kernel(sci, ref, knots, sx, sy[:-1], 7, 1.2, 2, GRID)
+    with pytest.raises(RuntimeError):
+        _core.fit_kernel(sci, ref, knots, np.array([-100], np.int32), np.array([-100], np.int32), 7, 1.2, 2, GRID)
