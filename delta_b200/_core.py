@@ -407,6 +407,116 @@ def fit_kernel(science, reference, knots, stamp_x, stamp_y, stamp_radius: int, b
     return out
 
 
+# ---- stamp selection -----------------------------------------------------------------
+
+
+def _detect_params(stamp_radius, threshold_sigma, max_stamps, saturation, isolation_radius, border, fwhm_radius,
+                   match_radius):
+    return _lib.DetectParams(int(stamp_radius), float(threshold_sigma), int(max_stamps), float(saturation),
+                             int(isolation_radius), int(border), int(fwhm_radius), int(match_radius))
+
+
+def weighted_mean(data, variance, mask) -> float:
+    """Inverse-variance weighted mean over unmasked pixels."""
+    d = np.ascontiguousarray(data, np.float32)
+    v = np.ascontiguousarray(variance, np.float32)
+    m = np.ascontiguousarray(mask, np.uint8)
+    out = ctypes.c_double()
+    ctx = context()
+    check(_lib.lib().dgpu_weighted_mean(ctx.handle, _lib.MEM_HOST, ctypes.c_int64(d.size), ptr(d), ptr(v), ptr(m),
+                                        ctypes.byref(out)), ctx.handle)
+    return out.value
+
+
+def estimate_background(data, mask=None):
+    """Robust (median, MAD-sigma) background over unmasked pixels."""
+    d = _img(data, "data")
+    m = _mask_opt(mask)
+    if m is not None and m.shape != d.shape:
+        raise RuntimeError("mask shape does not match data")
+    h, w = d.shape
+    med, sig = ctypes.c_double(), ctypes.c_double()
+    ctx = context()
+    check(_lib.lib().dgpu_estimate_background(ctx.handle, _lib.MEM_HOST, ctypes.c_int64(w), ctypes.c_int64(h),
+                                              ptr(d), ptr(m), ctypes.byref(med), ctypes.byref(sig)), ctx.handle)
+    return med.value, sig.value
+
+
+def detect_stamps(data, mask=None, stamp_radius: int = 15, threshold_sigma: float = 5.0, max_stamps: int = 200,
+                  saturation: float = 0.0, isolation_radius: int = 0, border: int = 0, fwhm_radius: int = 0,
+                  match_radius: int = 2) -> dict:
+    """Detect bright, isolated, unsaturated point-source stamps."""
+    d = _img(data, "data")
+    m = _mask_opt(mask)
+    if m is not None and m.shape != d.shape:
+        raise RuntimeError("mask shape does not match data")
+    h, w = d.shape
+    p = _detect_params(stamp_radius, threshold_sigma, max_stamps, saturation, isolation_radius, border, fwhm_radius,
+                       match_radius)
+    cap = max(int(max_stamps), 1)
+    cols = {"x": np.zeros(cap, np.int32), "y": np.zeros(cap, np.int32), "flux": np.zeros(cap),
+            "snr": np.zeros(cap), "fwhm": np.zeros(cap)}
+    n = ctypes.c_int()
+    ctx = context()
+    check(_lib.lib().dgpu_detect_stamps(ctx.handle, _lib.MEM_HOST, ctypes.c_int64(w), ctypes.c_int64(h), ptr(d),
+                                        ptr(m), ctypes.byref(p), cap, *[ptr(cols[k]) for k in ("x", "y", "flux",
+                                                                                              "snr", "fwhm")],
+                                        ctypes.byref(n)), ctx.handle)
+    return {k: v[: n.value].copy() for k, v in cols.items()}
+
+
+def select_stamps(science, reference, science_mask=None, reference_mask=None, catalog_x=None, catalog_y=None,
+                  stamp_radius: int = 15, threshold_sigma: float = 5.0, max_stamps: int = 200,
+                  saturation: float = 0.0, isolation_radius: int = 0, border: int = 0, fwhm_radius: int = 0,
+                  match_radius: int = 2) -> dict:
+    """Select matched stamps across both images and the convolution direction."""
+    s = _img(science, "science")
+    r = _img(reference, "reference")
+    sm = _mask_opt(science_mask)
+    rm = _mask_opt(reference_mask)
+    h, w = s.shape
+    if r.shape != s.shape:
+        raise RuntimeError("select_stamps: science/reference shape mismatch")
+    cx = None if catalog_x is None else np.ascontiguousarray(catalog_x, np.int32).ravel()
+    cy = None if catalog_y is None else np.ascontiguousarray(catalog_y, np.int32).ravel()
+    if (cx is None) != (cy is None):
+        cx = cy = None
+    ncat = 0 if cx is None else min(cx.size, cy.size)
+    p = _detect_params(stamp_radius, threshold_sigma, max_stamps, saturation, isolation_radius, border, fwhm_radius,
+                       match_radius)
+    cap = max(int(max_stamps), ncat, 1)
+    x = np.zeros(cap, np.int32)
+    y = np.zeros(cap, np.int32)
+    fs = np.zeros(cap)
+    fr = np.zeros(cap)
+    ms, mr = ctypes.c_double(), ctypes.c_double()
+    dref, n = ctypes.c_int(), ctypes.c_int()
+    ctx = context()
+    check(_lib.lib().dgpu_select_stamps(ctx.handle, _lib.MEM_HOST, ctypes.c_int64(w), ctypes.c_int64(h), ptr(s),
+                                        ptr(r), ptr(sm), ptr(rm), ptr(cx), ptr(cy), int(ncat), ctypes.byref(p), cap,
+                                        ptr(x), ptr(y), ptr(fs), ptr(fr), ctypes.byref(ms), ctypes.byref(mr),
+                                        ctypes.byref(dref), ctypes.byref(n)), ctx.handle)
+    k = n.value
+    return {"x": x[:k].copy(), "y": y[:k].copy(), "fwhm_science": fs[:k].copy(), "fwhm_reference": fr[:k].copy(),
+            "median_fwhm_science": ms.value, "median_fwhm_reference": mr.value,
+            "direction": "reference" if dref.value else "science"}
+
+
+def estimate_psf(image, xs, ys, radius: int) -> np.ndarray:
+    """Median, unit-sum postage stamp of the listed sources (the score path's PSF);
+    not part of the reference binding (the reference computes it in NumPy)."""
+    img = _img(image, "image")
+    h, w = img.shape
+    x = np.ascontiguousarray(xs, np.int32).ravel()
+    y = np.ascontiguousarray(ys, np.int32).ravel()
+    side = 2 * int(radius) + 1
+    out = np.empty((side, side), np.float32)
+    ctx = context()
+    check(_lib.lib().dgpu_estimate_psf(ctx.handle, _lib.MEM_HOST, ctypes.c_int64(w), ctypes.c_int64(h), ptr(img),
+                                       ptr(x), ptr(y), int(min(x.size, y.size)), int(radius), ptr(out)), ctx.handle)
+    return out
+
+
 # ---- noise decorrelation -------------------------------------------------------------
 
 

@@ -73,6 +73,19 @@ class CatalogParams(ctypes.Structure):
     ]
 
 
+class DetectParams(ctypes.Structure):
+    _fields_ = [
+        ("stamp_radius", ctypes.c_int),
+        ("threshold_sigma", ctypes.c_double),
+        ("max_stamps", ctypes.c_int),
+        ("saturation", ctypes.c_double),
+        ("isolation_radius", ctypes.c_int),
+        ("border", ctypes.c_int),
+        ("fwhm_radius", ctypes.c_int),
+        ("match_radius", ctypes.c_int),
+    ]
+
+
 class GlsResult(ctypes.Structure):
     _fields_ = [
         ("theta", ctypes.c_void_p),

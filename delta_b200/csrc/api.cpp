@@ -137,8 +137,21 @@ const char* dgpu_last_error(const dgpu_context* ctx) {
   return g_free_error.c_str();
 }
 
+int dgpu_set_timing(dgpu_context* ctx, int on) {
+  return guarded(ctx, [&](Context& c) {
+    resolve_timing(c);
+    c.timing_enabled = on != 0;
+  });
+}
+
+int dgpu_launch_count(unsigned long long* count) {
+  *count = launch_count();
+  return DGPU_OK;
+}
+
 int dgpu_drain_timing(dgpu_context* ctx, char (*labels)[64], double* seconds, int cap, int* n) {
   return guarded(ctx, [&](Context& c) {
+    resolve_timing(c);
     const int cnt = static_cast<int>(c.timing.size());
     for (int i = 0; i < cnt && i < cap; ++i) {
       std::strncpy(labels[i], c.timing[i].first.c_str(), 63);
@@ -385,13 +398,13 @@ int dgpu_subtract(dgpu_context* ctx, int mem, int64_t width, int64_t height, con
       launch_strided_median(c, kSampleReference, static_cast<int64_t>(n), ref, rm, scal);
     }
     {
-      StageTimer t(c, "subtract: model convolve");
       const auto taps = b.taps();
       float* dt = static_cast<float*>(c.slot(kSlotTaps, sizeof(float) * taps.size()));
       DGPU_CUDA(cudaMemcpyAsync(dt, taps.data(), sizeof(float) * taps.size(), cudaMemcpyHostToDevice, s));
       const auto ord = orders_of(b);
       int2* dord = static_cast<int2*>(c.slot(kSlotScratch2, sizeof(int2) * ord.size()));
       DGPU_CUDA(cudaMemcpyAsync(dord, ord.data(), sizeof(int2) * ord.size(), cudaMemcpyHostToDevice, s));
+      StageTimer t(c, "subtract: model convolve");
       SubtractArgs a{};
       a.w = w;
       a.h = h;
@@ -455,6 +468,21 @@ int dgpu_photometric_scale(dgpu_context* ctx, int mem, const double* knots, int 
     launch_photometric_scale(c.stream, F, ds, nc, o);
     stage_out(c, mem, out, o, 4 * n);
     if (mem == DGPU_MEM_HOST) check_status(c);
+  });
+}
+
+int dgpu_negate(dgpu_context* ctx, int mem, float* data, int64_t n) {
+  return guarded(ctx, [&](Context& c) {
+    if (n < 0) fail(DGPU_ERR_INVALID, "negate: n must be >= 0");
+    if (n == 0) return;
+    if (!data) fail(DGPU_ERR_INVALID, "negate: missing buffer");
+    const size_t bytes = 4 * static_cast<size_t>(n);
+    float* d = mem == DGPU_MEM_DEVICE ? data : static_cast<float*>(c.slot(kSlotOutDiff, bytes));
+    if (mem != DGPU_MEM_DEVICE)
+      DGPU_CUDA(cudaMemcpyAsync(d, data, bytes, cudaMemcpyHostToDevice, c.stream));
+    launch_negate(c.stream, n, d);
+    stage_out(c, mem, data, d, bytes);
+    if (mem == DGPU_MEM_HOST) DGPU_CUDA(cudaStreamSynchronize(c.stream));
   });
 }
 

@@ -26,8 +26,11 @@ struct Failure : std::runtime_error {
 
 [[noreturn]] void fail(int code, const std::string& msg);
 void check_cuda(cudaError_t e, const char* what);
+// Every kernel launch of the library goes through DGPU_LAUNCH, which also
+// counts it (dgpu_launch_count).
+void count_launch();
 #define DGPU_CUDA(call) ::dgpu::check_cuda((call), #call)
-#define DGPU_LAUNCH(what) ::dgpu::check_cuda(cudaGetLastError(), what)
+#define DGPU_LAUNCH(what) (::dgpu::count_launch(), ::dgpu::check_cuda(cudaGetLastError(), what))
 
 // ---------------------------------------------------------------------------
 // Device status word: kernels with a data-dependent loop bound record here
@@ -64,8 +67,14 @@ struct Context {
   void* slot_ptr[kSlotCount] = {};
   size_t slot_size[kSlotCount] = {};
   std::string last_error;
-  // Host-visible timing: label -> accumulated seconds (DELTA_TIMING).
+  // Host-visible timing: label -> accumulated seconds (DELTA_TIMING). Stage
+  // events are recorded without synchronising and resolved when drained.
   std::vector<std::pair<std::string, double>> timing;
+  struct PendingStage {
+    std::string label;
+    cudaEvent_t e0, e1;
+  };
+  std::vector<PendingStage> pending;
   bool timing_enabled = false;
   // Catalog results of the last dgpu_build_catalog (host copies).
   std::vector<double> cat_d;    // 12 double columns x n
@@ -80,6 +89,10 @@ struct Context {
 // RAII: clear the status word at entry, check it (after a sync) at exit.
 void reset_status(Context& c);
 void check_status(Context& c);  // synchronises the stream
+
+// Resolve the pending stage events into `timing` (synchronises the stream).
+void resolve_timing(Context& c);
+unsigned long long launch_count();
 
 // Device-side timing scope keyed by a reference DELTA_TIMING label.
 struct StageTimer {
@@ -196,6 +209,7 @@ void launch_mask_fill(cudaStream_t s, int64_t n, const uint8_t* mask, const uint
                       const float* fill, float* diff, float* var);
 void launch_model_convolve_orders(cudaStream_t s, const SubtractArgs& a, const int2* orders, bool stack);
 void launch_photometric_scale(cudaStream_t s, const DevFields& F, const float* sums, int nc, float* out);
+void launch_negate(cudaStream_t s, int64_t n, float* v);
 
 // Upper median (element size/2 of the sorted sample) of values[7j] that pass a
 // predicate, via radix select. Result written to a device float.

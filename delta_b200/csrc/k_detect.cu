@@ -1,0 +1,593 @@
+// Stamp selection on the device (reference src/detect.cpp:84-314) and the
+// median PSF stamp of the score path (python/delta/pipeline.py:285-302).
+//
+//  * background: median and 1.4826 * MAD of a flat-index-strided sample of the
+//    finite, unmasked pixels (step n / 2^18), by exact radix select;
+//  * peaks: 3x3 strict local maxima above median + k sigma inside the border,
+//    with a fully on-frame, finite, unmasked, unsaturated stamp footprint;
+//  * per-candidate flux-weighted second-moment FWHM (FP64);
+//  * candidates sorted by flux descending (raster index ascending on ties),
+//    then brightest-first greedy isolation in one CTA, chunk by chunk.
+#include <cuda_runtime.h>
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+
+#include "dev_common.cuh"
+#include "detect_internal.h"
+
+namespace dgpu {
+
+// ---------------------------------------------------------------------------
+// Sample medians (shared radix-select machinery of k_subtract.cu is per-stride 7;
+// this variant takes any stride and an optional absolute-deviation transform).
+// ---------------------------------------------------------------------------
+struct Sel {
+  unsigned count, rank, prefix, pad;
+  unsigned hist[256];
+};
+
+__global__ void k_sample_keys(int64_t n, int64_t step, const float* __restrict__ v, const uint8_t* __restrict__ mask,
+                              uint32_t* __restrict__ keys, Sel* st) {
+  const int64_t ns = (n + step - 1) / step;
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < ns;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = j * step;
+    const float x = v[i];
+    const bool ok = isfinite(x) && (mask == nullptr || mask[i] == 0);
+    const unsigned bal = __ballot_sync(__activemask(), ok);
+    if (!bal) continue;
+    const int lane = threadIdx.x & 31, leader = __ffs(bal) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(&st->count, __popc(bal));
+    base = __shfl_sync(__activemask(), base, leader);
+    if (ok) keys[base + __popc(bal & ((1u << lane) - 1))] = float_key(x);
+  }
+}
+
+// keys <- key(|value - med|) in place (src/detect.cpp:110).
+__global__ void k_abs_dev(const Sel* st, const float* __restrict__ med, uint32_t* __restrict__ keys) {
+  const unsigned count = st->count;
+  const float m = *med;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    keys[i] = float_key(fabsf(key_float(keys[i]) - m));
+}
+
+__global__ void k_sel_init(Sel* st) {
+  st->rank = st->count / 2;
+  st->prefix = 0;
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) st->hist[i] = 0;
+}
+
+__global__ void k_sel_hist(const uint32_t* __restrict__ keys, Sel* st, int shift) {
+  __shared__ unsigned hist[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+  __syncthreads();
+  const unsigned count = st->count, prefix = st->prefix;
+  const unsigned himask = shift >= 24 ? 0u : (0xffffffffu << (shift + 8));
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const uint32_t k = keys[i];
+    if ((k & himask) == (prefix & himask)) atomicAdd(&hist[(k >> shift) & 0xffu], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 256; i += blockDim.x)
+    if (hist[i]) atomicAdd(&st->hist[i], hist[i]);
+}
+
+__global__ void k_sel_pick(Sel* st, int shift, float* result, int last) {
+  if (threadIdx.x != 0) return;
+  unsigned rank = st->rank, cum = 0;
+  int digit = 255;
+  for (int d = 0; d < 256; ++d) {
+    if (rank < cum + st->hist[d]) {
+      digit = d;
+      break;
+    }
+    cum += st->hist[d];
+  }
+  st->rank = rank - cum;
+  st->prefix |= static_cast<unsigned>(digit) << shift;
+  for (int d = 0; d < 256; ++d) st->hist[d] = 0;
+  if (last) *result = st->count ? key_float(st->prefix) : 0.0f;
+}
+
+static void select_median(cudaStream_t s, Sel* st, const uint32_t* keys, int64_t cap, float* out) {
+  k_sel_init<<<1, 256, 0, s>>>(st);
+  DGPU_LAUNCH("k_sel_init");
+  const int hb = static_cast<int>(std::min<int64_t>((std::max<int64_t>(cap, 1) + 1023) / 1024, 148 * 2));
+  for (int pass = 0; pass < 4; ++pass) {
+    k_sel_hist<<<hb, 256, 0, s>>>(keys, st, 24 - 8 * pass);
+    DGPU_LAUNCH("k_sel_hist");
+    k_sel_pick<<<1, 32, 0, s>>>(st, 24 - 8 * pass, out, pass == 3);
+    DGPU_LAUNCH("k_sel_pick");
+  }
+}
+
+// bgout[0] = median (float), bgout[1] = MAD (float)
+void launch_background(Context& c, int64_t n, const float* img, const uint8_t* mask, float* bgout, Slot sel_slot,
+                       Slot key_slot) {
+  cudaStream_t s = c.stream;
+  constexpr int64_t kTarget = 1 << 18;
+  const int64_t step = n > kTarget ? n / kTarget : 1;
+  const int64_t ns = (n + step - 1) / step;
+  Sel* st = static_cast<Sel*>(c.slot(sel_slot, sizeof(Sel)));
+  uint32_t* keys = static_cast<uint32_t*>(c.slot(key_slot, sizeof(uint32_t) * std::max<int64_t>(ns, 1)));
+  DGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(Sel), s));
+  const int blocks = static_cast<int>(std::min<int64_t>((ns + 255) / 256, 148 * 8));
+  k_sample_keys<<<std::max(blocks, 1), 256, 0, s>>>(n, step, img, mask, keys, st);
+  DGPU_LAUNCH("k_sample_keys");
+  select_median(s, st, keys, ns, bgout);
+  k_abs_dev<<<std::max(blocks, 1), 256, 0, s>>>(st, bgout, keys);
+  DGPU_LAUNCH("k_abs_dev");
+  select_median(s, st, keys, ns, bgout + 1);
+}
+
+// ---------------------------------------------------------------------------
+// Candidates
+// ---------------------------------------------------------------------------
+__device__ bool footprint_ok_dev(const float* img, const uint8_t* mask, int w, int h, int x, int y, int r,
+                                 double sat) {
+  if (x - r < 0 || x + r >= w || y - r < 0 || y + r >= h) return false;
+  for (int dy = -r; dy <= r; ++dy)
+    for (int dx = -r; dx <= r; ++dx) {
+      const size_t i = static_cast<size_t>(y + dy) * w + (x + dx);
+      const float v = img[i];
+      if (!isfinite(v)) return false;
+      if (mask && mask[i] != 0) return false;
+      if (sat > 0.0 && static_cast<double>(v) >= sat) return false;
+    }
+  return true;
+}
+
+// estimate_fwhm (src/detect.cpp:115-157), FP64.
+__device__ double fwhm_dev(const float* img, int w, int h, int x, int y, int r, double bg) {
+  double sum = 0.0, sx = 0.0, sy = 0.0;
+  for (int dy = -r; dy <= r; ++dy) {
+    const int yy = y + dy;
+    if (yy < 0 || yy >= h) continue;
+    for (int dx = -r; dx <= r; ++dx) {
+      const int xx = x + dx;
+      if (xx < 0 || xx >= w) continue;
+      const double f = static_cast<double>(img[static_cast<size_t>(yy) * w + xx]) - bg;
+      const double wt = f > 0.0 ? f : 0.0;
+      sum += wt;
+      sx += wt * dx;
+      sy += wt * dy;
+    }
+  }
+  if (sum <= 0.0) return __longlong_as_double(0x7ff8000000000000ll);
+  const double mx = sx / sum, my = sy / sum;
+  double sxx = 0.0, syy = 0.0;
+  for (int dy = -r; dy <= r; ++dy) {
+    const int yy = y + dy;
+    if (yy < 0 || yy >= h) continue;
+    for (int dx = -r; dx <= r; ++dx) {
+      const int xx = x + dx;
+      if (xx < 0 || xx >= w) continue;
+      const double f = static_cast<double>(img[static_cast<size_t>(yy) * w + xx]) - bg;
+      const double wt = f > 0.0 ? f : 0.0;
+      sxx += wt * (dx - mx) * (dx - mx);
+      syy += wt * (dy - my) * (dy - my);
+    }
+  }
+  const double var = 0.5 * (sxx / sum + syy / sum);
+  if (var <= 0.0) return __longlong_as_double(0x7ff8000000000000ll);
+  return 2.354820045030949 * sqrt(var);
+}
+
+__global__ void k_peaks(int w, int h, const float* __restrict__ img, const uint8_t* __restrict__ mask,
+                        const float* __restrict__ bg, DetectParamsDev p, unsigned* count, int cap,
+                        int* __restrict__ cand) {
+  const double med = static_cast<double>(bg[0]);
+  const double sigma = 1.4826 * static_cast<double>(bg[1]);
+  const double thr = med + p.threshold_sigma * (sigma > 0.0 ? sigma : 1.0);
+  const int b = p.border;
+  const int64_t n = static_cast<int64_t>(w) * h;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int x = static_cast<int>(i % w), y = static_cast<int>(i / w);
+    if (y < b || y >= h - b || x < b || x >= w - b) continue;
+    if (x < 1 || y < 1 || x >= w - 1 || y >= h - 1) continue;  // 3x3 window on frame
+    const double v = static_cast<double>(img[i]);
+    if (!(v > thr)) continue;
+    bool peak = true;
+    for (int dy = -1; dy <= 1 && peak; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        if (dx == 0 && dy == 0) continue;
+        if (static_cast<double>(img[i + static_cast<int64_t>(dy) * w + dx]) > v) {
+          peak = false;
+          break;
+        }
+      }
+    if (!peak) continue;
+    if (!footprint_ok_dev(img, mask, w, h, x, y, p.stamp_radius, p.saturation)) continue;
+    const unsigned slot = atomicAdd(count, 1u);
+    if (static_cast<int>(slot) < cap) cand[slot] = static_cast<int>(i);
+  }
+}
+
+// Sort keys: (flux descending, index ascending) -> ascending uint64.
+__global__ void k_cand_keys(const unsigned* count, int cap, const int* __restrict__ cand, const float* __restrict__ img,
+                            unsigned long long* __restrict__ keys, int* __restrict__ vals) {
+  const int nc = min(static_cast<int>(*count), cap);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nc; i += gridDim.x * blockDim.x) {
+    const int idx = cand[i];
+    const uint32_t fk = ~float_key(img[idx]);  // descending value
+    keys[i] = (static_cast<unsigned long long>(fk) << 32) | static_cast<unsigned>(idx);
+    vals[i] = idx;
+  }
+}
+
+// Brightest-first greedy isolation (src/detect.cpp:223-240) in one CTA.
+// Output: kept raster indices in order; *n_kept.
+__global__ void __launch_bounds__(1024)
+k_isolate(int w, const unsigned* count, int cap, const int* __restrict__ sorted_idx, long long iso2, int max_stamps,
+          int* __restrict__ kept, int* n_kept, unsigned* status) {
+  extern __shared__ int ks[];  // kept x, y interleaved (2 * max_stamps)
+  __shared__ int s_nk;
+  __shared__ unsigned char pass[1024];
+  __shared__ int cx[1024], cy[1024];
+  const int nc = min(static_cast<int>(*count), cap);
+  if (threadIdx.x == 0) s_nk = 0;
+  __syncthreads();
+  for (int base = 0; base < nc; base += blockDim.x) {
+    if (s_nk >= max_stamps) break;
+    const int i = base + threadIdx.x;
+    bool ok = false;
+    if (i < nc) {
+      const int idx = sorted_idx[i];
+      const int x = idx % w, y = idx / w;
+      cx[threadIdx.x] = x;
+      cy[threadIdx.x] = y;
+      ok = true;
+      const int nk = s_nk;
+      for (int k = 0; k < nk; ++k) {
+        const long long dx = x - ks[2 * k], dy = y - ks[2 * k + 1];
+        if (dx * dx + dy * dy < iso2) {
+          ok = false;
+          break;
+        }
+      }
+    }
+    pass[threadIdx.x] = ok ? 1 : 0;
+    __syncthreads();
+    // Sequential resolution within the chunk by warp 0.
+    if (threadIdx.x < 32) {
+      const int lim = min(static_cast<int>(blockDim.x), nc - base);
+      int nk = s_nk;
+      const int chunk_start = nk;
+      for (int t = 0; t < lim && nk < max_stamps; ++t) {
+        if (!pass[t]) continue;
+        bool iso = true;
+        for (int k = chunk_start + threadIdx.x; k < nk; k += 32) {
+          const long long dx = cx[t] - ks[2 * k], dy = cy[t] - ks[2 * k + 1];
+          if (dx * dx + dy * dy < iso2) iso = false;
+        }
+        iso = __all_sync(0xffffffffu, iso);
+        if (iso) {
+          if (threadIdx.x == 0) {
+            ks[2 * nk] = cx[t];
+            ks[2 * nk + 1] = cy[t];
+            kept[nk] = cy[t] * w + cx[t];
+          }
+          __syncwarp();
+          ++nk;
+        }
+      }
+      if (threadIdx.x == 0) s_nk = nk;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *n_kept = s_nk;
+  (void)status;
+}
+
+__global__ void k_stamp_props(int w, int h, const float* __restrict__ img, const float* __restrict__ bg,
+                              const int* __restrict__ kept, const int* __restrict__ n_kept, int fwhm_radius,
+                              double* __restrict__ flux, double* __restrict__ snr, double* __restrict__ fwhm) {
+  const int nk = *n_kept;
+  const double med = static_cast<double>(bg[0]);
+  const double sigma = 1.4826 * static_cast<double>(bg[1]);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nk; i += gridDim.x * blockDim.x) {
+    const int idx = kept[i];
+    const int x = idx % w, y = idx / w;
+    const double f = static_cast<double>(img[idx]) - med;
+    flux[i] = f;
+    snr[i] = sigma > 0.0 ? f / sigma : f;
+    fwhm[i] = fwhm_dev(img, w, h, x, y, fwhm_radius, med);
+  }
+}
+
+// Catalog positions: footprint check on both images + FWHM on both
+// (select_stamps_from_catalog, src/detect.cpp:289-314).
+__global__ void k_catalog_stamps(int w, int h, const float* __restrict__ sci, const uint8_t* __restrict__ sm,
+                                 const float* __restrict__ ref, const uint8_t* __restrict__ rm,
+                                 const float* __restrict__ bg_sci, const float* __restrict__ bg_ref,
+                                 const int* __restrict__ xs, const int* __restrict__ ys, int n, DetectParamsDev p,
+                                 int* __restrict__ ok, double* __restrict__ fs, double* __restrict__ fr) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int x = xs[i], y = ys[i];
+    const bool good = footprint_ok_dev(sci, sm, w, h, x, y, p.stamp_radius, p.saturation) &&
+                      footprint_ok_dev(ref, rm, w, h, x, y, p.stamp_radius, p.saturation);
+    ok[i] = good ? 1 : 0;
+    if (good) {
+      fs[i] = fwhm_dev(sci, w, h, x, y, p.fwhm_radius, static_cast<double>(bg_sci[0]));
+      fr[i] = fwhm_dev(ref, w, h, x, y, p.fwhm_radius, static_cast<double>(bg_ref[0]));
+    }
+  }
+}
+
+// Median unit-sum PSF of the listed stamps (python/delta/pipeline.py:285-302):
+// per stamp cut - median(cut) normalised by its positive total; per pixel the
+// median across stamps (mean of the two middle values for an even count),
+// clipped at 0 and renormalised. FP64. One CTA per stamp, then one per pixel.
+__global__ void k_psf_stamps(int w, int h, const float* __restrict__ img, const int* __restrict__ xs,
+                             const int* __restrict__ ys, int n, int radius, double* __restrict__ cuts,
+                             int* __restrict__ use) {
+  extern __shared__ double sv[];  // side^2 padded to a power of two
+  const int s = blockIdx.x;
+  const int side = 2 * radius + 1, np = side * side;
+  int cap = 1;
+  while (cap < np) cap <<= 1;
+  const int x = xs[s], y = ys[s];
+  const bool inside = !(x - radius < 0 || x + radius >= w || y - radius < 0 || y + radius >= h);
+  if (!inside) {
+    if (threadIdx.x == 0) use[s] = 0;
+    return;
+  }
+  double* srt = sv + cap;
+  for (int i = threadIdx.x; i < cap; i += blockDim.x) {
+    double v = INFINITY;
+    if (i < np) v = static_cast<double>(img[static_cast<size_t>(y - radius + i / side) * w + (x - radius + i % side)]);
+    sv[i] = v;
+    srt[i] = v;
+  }
+  __syncthreads();
+  for (int size = 2; size <= cap; size <<= 1)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < cap; i += blockDim.x) {
+        const int j = i ^ stride;
+        if (j > i) {
+          const bool up = (i & size) == 0;
+          const double a = srt[i], b = srt[j];
+          if ((a > b) == up) {
+            srt[i] = b;
+            srt[j] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  const double med = (np & 1) ? srt[np / 2] : 0.5 * (srt[np / 2 - 1] + srt[np / 2]);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int i = 0; i < np; ++i) tot += sv[i] - med;
+    use[s] = tot > 0.0 ? 1 : 0;
+    srt[0] = tot;
+  }
+  __syncthreads();
+  const double tot = srt[0];
+  for (int i = threadIdx.x; i < np; i += blockDim.x) cuts[static_cast<size_t>(s) * np + i] = (sv[i] - med) / tot;
+}
+
+__global__ void k_psf_median(int n, int np, const double* __restrict__ cuts, const int* __restrict__ use,
+                             double* __restrict__ out, unsigned* status) {
+  extern __shared__ double col[];
+  const int p = blockIdx.x;
+  __shared__ int cnt;
+  if (threadIdx.x == 0) {
+    cnt = 0;
+    for (int s = 0; s < n; ++s)
+      if (use[s]) col[cnt++] = cuts[static_cast<size_t>(s) * np + p];
+    // insertion sort (n is the stamp count, a few hundred)
+    for (int i = 1; i < cnt; ++i) {
+      const double v = col[i];
+      int j = i - 1;
+      while (j >= 0 && col[j] > v) {
+        col[j + 1] = col[j];
+        --j;
+      }
+      col[j + 1] = v;
+    }
+    double m = 0.0;
+    if (cnt > 0) m = (cnt & 1) ? col[cnt / 2] : 0.5 * (col[cnt / 2 - 1] + col[cnt / 2]);
+    out[p] = m > 0.0 ? m : 0.0;
+    if (cnt == 0) atomicOr(status, kStatusBounds);
+  }
+}
+
+void launch_psf_estimate(Context& c, int w, int h, const float* img, const int* xs, const int* ys, int n, int radius,
+                         double* out, int* n_used) {
+  cudaStream_t s = c.stream;
+  const int side = 2 * radius + 1, np = side * side;
+  int cap = 1;
+  while (cap < np) cap <<= 1;
+  double* cuts = static_cast<double*>(c.slot(kSlotScratch0, sizeof(double) * static_cast<size_t>(std::max(n, 1)) * np));
+  int* use = static_cast<int*>(c.slot(kSlotBlockCounts, sizeof(int) * std::max(n, 1)));
+  const size_t smem = sizeof(double) * 2 * cap;
+  DGPU_CUDA(cudaFuncSetAttribute(k_psf_stamps, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  k_psf_stamps<<<n, 256, smem, s>>>(w, h, img, xs, ys, n, radius, cuts, use);
+  DGPU_LAUNCH("k_psf_stamps");
+  const size_t smem2 = sizeof(double) * std::max(n, 1);
+  DGPU_CUDA(cudaFuncSetAttribute(k_psf_median, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem2)));
+  k_psf_median<<<np, 32, smem2, s>>>(n, np, cuts, use, out, c.d_status);
+  DGPU_LAUNCH("k_psf_median");
+  std::vector<int> hu(n);
+  if (n) DGPU_CUDA(cudaMemcpyAsync(hu.data(), use, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+  DGPU_CUDA(cudaStreamSynchronize(s));
+  int u = 0;
+  for (int v : hu) u += v;
+  *n_used = u;
+}
+
+// weighted_mean (src/bindings.cpp:107-124): FP64 partial sums per CTA.
+__global__ void k_weighted_mean(int64_t n, const float* __restrict__ d, const float* __restrict__ v,
+                                const uint8_t* __restrict__ m, double* __restrict__ part) {
+  __shared__ double s1[256], s2[256];
+  double a = 0.0, b = 0.0;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    if (m[i] != 0) continue;
+    if (!(v[i] > 0.0f)) continue;
+    const double wv = 1.0 / static_cast<double>(v[i]);
+    a += wv;
+    b += wv * static_cast<double>(d[i]);
+  }
+  s1[threadIdx.x] = a;
+  s2[threadIdx.x] = b;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < static_cast<unsigned>(o)) {
+      s1[threadIdx.x] += s1[threadIdx.x + o];
+      s2[threadIdx.x] += s2[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = s1[0];
+    part[2 * blockIdx.x + 1] = s2[0];
+  }
+}
+
+void launch_weighted_mean(Context& c, int64_t n, const float* d, const float* v, const uint8_t* m, double* out2) {
+  const int blocks = static_cast<int>(std::min<int64_t>((n + 255) / 256, 296));
+  double* part = static_cast<double*>(c.slot(kSlotScratch1, sizeof(double) * 2 * blocks));
+  k_weighted_mean<<<blocks, 256, 0, c.stream>>>(n, d, v, m, part);
+  DGPU_LAUNCH("k_weighted_mean");
+  std::vector<double> hp(2 * blocks);
+  DGPU_CUDA(cudaMemcpyAsync(hp.data(), part, sizeof(double) * 2 * blocks, cudaMemcpyDeviceToHost, c.stream));
+  DGPU_CUDA(cudaStreamSynchronize(c.stream));
+  double a = 0.0, b = 0.0;
+  for (int i = 0; i < blocks; ++i) {
+    a += hp[2 * i];
+    b += hp[2 * i + 1];
+  }
+  out2[0] = a;
+  out2[1] = b;
+}
+
+// Full detect pipeline for one image. Returns the kept count; host copies of
+// x, y, flux, snr, fwhm in `res`.
+int run_detect(Context& c, int w, int h, const float* img, const uint8_t* mask, const DetectParamsDev& p, int which,
+               DetectHost& res) {
+  cudaStream_t s = c.stream;
+  const int64_t n = static_cast<int64_t>(w) * h;
+  const Slot ss = which ? kSlotFit12 : kSlotFit10, ks = which ? kSlotFit13 : kSlotFit11;
+  float* bg = static_cast<float*>(c.slot(which ? kSlotFit15 : kSlotFit14, 64));
+  launch_background(c, n, img, mask, bg, ss, ks);
+  const int cap = 1 << 20;
+  char* buf = static_cast<char*>(c.slot(which ? kSlotFft1 : kSlotFft0, (sizeof(int) * 3 + 2 * sizeof(unsigned long long)) * cap + 256));
+  unsigned* count = reinterpret_cast<unsigned*>(buf);
+  int* cand = reinterpret_cast<int*>(buf + 64);
+  int* sorted = cand + cap;
+  int* kept = sorted + cap;
+  unsigned long long* keys = reinterpret_cast<unsigned long long*>(kept + cap);
+  unsigned long long* keys2 = keys + cap;
+  int* vals = reinterpret_cast<int*>(c.slot(which ? kSlotFft3 : kSlotFft2, sizeof(int) * cap + 64));
+  int* nk = vals + cap;
+  DGPU_CUDA(cudaMemsetAsync(count, 0, sizeof(unsigned), s));
+  const int blocks = static_cast<int>(std::min<int64_t>((n + 255) / 256, 148 * 16));
+  k_peaks<<<blocks, 256, 0, s>>>(w, h, img, mask, bg, p, count, cap, cand);
+  DGPU_LAUNCH("k_peaks");
+  unsigned hc = 0;
+  DGPU_CUDA(cudaMemcpyAsync(&hc, count, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  DGPU_CUDA(cudaStreamSynchronize(s));
+  if (hc > static_cast<unsigned>(cap)) fail(DGPU_ERR_RUNTIME, "detect_stamps: more than 2^20 peak candidates");
+  const int nc = static_cast<int>(hc);
+  float hbg[2];
+  DGPU_CUDA(cudaMemcpyAsync(hbg, bg, sizeof(hbg), cudaMemcpyDeviceToHost, s));
+  int nkept = 0;
+  if (nc > 0) {
+    k_cand_keys<<<(nc + 255) / 256, 256, 0, s>>>(count, cap, cand, img, keys, vals);
+    DGPU_LAUNCH("k_cand_keys");
+    size_t tmp_bytes = 0;
+    DGPU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys2, vals, sorted, nc, 0, 64, s));
+    void* tmp = c.slot(which ? kSlotFft5 : kSlotFft4, tmp_bytes + 16);
+    DGPU_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys2, vals, sorted, nc, 0, 64, s));
+    const long long iso = p.isolation_radius;
+    const size_t smem = sizeof(int) * 2 * std::max(p.max_stamps, 1);
+    if (smem > 160 * 1024) fail(DGPU_ERR_INVALID, "detect_stamps: max_stamps above 20480 is not supported");
+    DGPU_CUDA(cudaFuncSetAttribute(k_isolate, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    k_isolate<<<1, 1024, smem, s>>>(w, count, cap, sorted, iso * iso, p.max_stamps, kept, nk, c.d_status);
+    DGPU_LAUNCH("k_isolate");
+    DGPU_CUDA(cudaMemcpyAsync(&nkept, nk, sizeof(int), cudaMemcpyDeviceToHost, s));
+    DGPU_CUDA(cudaStreamSynchronize(s));
+  }
+  res.median = static_cast<double>(hbg[0]);
+  res.sigma = 1.4826 * static_cast<double>(hbg[1]);
+  res.x.assign(nkept, 0);
+  res.y.assign(nkept, 0);
+  res.flux.assign(nkept, 0);
+  res.snr.assign(nkept, 0);
+  res.fwhm.assign(nkept, 0);
+  if (nkept > 0) {
+    double* props = static_cast<double*>(c.slot(which ? kSlotCompOut : kSlotCompStats, sizeof(double) * 3 * nkept));
+    k_stamp_props<<<(nkept + 127) / 128, 128, 0, s>>>(w, h, img, bg, kept, nk, p.fwhm_radius, props, props + nkept,
+                                                      props + 2 * nkept);
+    DGPU_LAUNCH("k_stamp_props");
+    std::vector<int> hk(nkept);
+    DGPU_CUDA(cudaMemcpyAsync(hk.data(), kept, sizeof(int) * nkept, cudaMemcpyDeviceToHost, s));
+    DGPU_CUDA(cudaMemcpyAsync(res.flux.data(), props, sizeof(double) * nkept, cudaMemcpyDeviceToHost, s));
+    DGPU_CUDA(cudaMemcpyAsync(res.snr.data(), props + nkept, sizeof(double) * nkept, cudaMemcpyDeviceToHost, s));
+    DGPU_CUDA(cudaMemcpyAsync(res.fwhm.data(), props + 2 * nkept, sizeof(double) * nkept, cudaMemcpyDeviceToHost, s));
+    DGPU_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < nkept; ++i) {
+      res.x[i] = hk[i] % w;
+      res.y[i] = hk[i] / w;
+    }
+  }
+  return nkept;
+}
+
+void run_background(Context& c, int64_t n, const float* img, const uint8_t* mask, double* median, double* sigma) {
+  float* bg = static_cast<float*>(c.slot(kSlotFit14, 64));
+  launch_background(c, n, img, mask, bg, kSlotFit10, kSlotFit11);
+  float hbg[2];
+  DGPU_CUDA(cudaMemcpyAsync(hbg, bg, sizeof(hbg), cudaMemcpyDeviceToHost, c.stream));
+  DGPU_CUDA(cudaStreamSynchronize(c.stream));
+  *median = static_cast<double>(hbg[0]);
+  *sigma = 1.4826 * static_cast<double>(hbg[1]);
+}
+
+void run_catalog_stamps(Context& c, int w, int h, const float* sci, const uint8_t* sm, const float* ref,
+                        const uint8_t* rm, const int* xs_host, const int* ys_host, int n, const DetectParamsDev& p,
+                        std::vector<int>& ok, std::vector<double>& fs, std::vector<double>& fr, double* med_sci,
+                        double* med_ref) {
+  cudaStream_t s = c.stream;
+  const int64_t npx = static_cast<int64_t>(w) * h;
+  float* bgs = static_cast<float*>(c.slot(kSlotFit14, 64));
+  float* bgr = static_cast<float*>(c.slot(kSlotFit15, 64));
+  launch_background(c, npx, sci, sm, bgs, kSlotFit10, kSlotFit11);
+  launch_background(c, npx, ref, rm, bgr, kSlotFit12, kSlotFit13);
+  int* dxy = static_cast<int*>(c.slot(kSlotBright, sizeof(int) * 2 * std::max(n, 1)));
+  DGPU_CUDA(cudaMemcpyAsync(dxy, xs_host, sizeof(int) * n, cudaMemcpyHostToDevice, s));
+  DGPU_CUDA(cudaMemcpyAsync(dxy + n, ys_host, sizeof(int) * n, cudaMemcpyHostToDevice, s));
+  char* ob = static_cast<char*>(c.slot(kSlotCompStats, (sizeof(int) + 2 * sizeof(double)) * std::max(n, 1) + 64));
+  double* dfs = reinterpret_cast<double*>(ob);
+  double* dfr = dfs + std::max(n, 1);
+  int* dok = reinterpret_cast<int*>(dfr + std::max(n, 1));
+  if (n > 0) {
+    k_catalog_stamps<<<(n + 127) / 128, 128, 0, s>>>(w, h, sci, sm, ref, rm, bgs, bgr, dxy, dxy + n, n, p, dok, dfs,
+                                                     dfr);
+    DGPU_LAUNCH("k_catalog_stamps");
+  }
+  ok.assign(n, 0);
+  fs.assign(n, 0.0);
+  fr.assign(n, 0.0);
+  float hb[2];
+  if (n) {
+    DGPU_CUDA(cudaMemcpyAsync(ok.data(), dok, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+    DGPU_CUDA(cudaMemcpyAsync(fs.data(), dfs, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    DGPU_CUDA(cudaMemcpyAsync(fr.data(), dfr, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  }
+  DGPU_CUDA(cudaMemcpyAsync(hb, bgs, sizeof(float) * 2, cudaMemcpyDeviceToHost, s));
+  DGPU_CUDA(cudaStreamSynchronize(s));
+  *med_sci = hb[0];
+  DGPU_CUDA(cudaMemcpyAsync(hb, bgr, sizeof(float) * 2, cudaMemcpyDeviceToHost, s));
+  DGPU_CUDA(cudaStreamSynchronize(s));
+  *med_ref = hb[0];
+}
+
+}  // namespace dgpu

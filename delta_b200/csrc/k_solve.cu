@@ -307,6 +307,7 @@ void launch_solve_batch(Context& c, const SolveBatch& b) {
   void* args[] = {&bb, &ppv};
   DGPU_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_solve_batch), dim3(grid), dim3(256), args, smem,
                                         c.stream));
+  count_launch();
 }
 
 // out = A_s^{-1} v = Linv_s^T (Linv_s v), single CTA.

@@ -686,4 +686,29 @@ void launch_photometric_scale(cudaStream_t s, const DevFields& F, const float* s
   DGPU_LAUNCH("k_photometric_scale");
 }
 
+// Transients-positive sign flip of the difference (python/delta/pipeline.py:687-689),
+// in place: float4 body, scalar tail.
+__global__ void k_negate(int64_t n, float* __restrict__ v) {
+  const int64_t n4 = (reinterpret_cast<uintptr_t>(v) & 15) ? 0 : n / 4;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  float4* v4 = reinterpret_cast<float4*>(v);
+  for (int64_t i = t; i < n4; i += stride) {
+    float4 a = v4[i];
+    a.x = -a.x;
+    a.y = -a.y;
+    a.z = -a.z;
+    a.w = -a.w;
+    v4[i] = a;
+  }
+  for (int64_t i = 4 * n4 + t; i < n; i += stride) v[i] = -v[i];
+}
+
+void launch_negate(cudaStream_t s, int64_t n, float* v) {
+  if (n <= 0) return;
+  const int blocks = static_cast<int>(std::min<int64_t>(ceil_div(ceil_div(n, 4), 256), 148 * 8));
+  k_negate<<<blocks, 256, 0, s>>>(n, v);
+  DGPU_LAUNCH("k_negate");
+}
+
 }  // namespace dgpu

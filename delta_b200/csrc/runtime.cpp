@@ -2,6 +2,7 @@
 // device-event stage timers, device field set-up.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdlib>
 #include <stdexcept>
 
@@ -42,6 +43,10 @@ void check_status(Context& c) {
   if (st & kStatusBounds) fail(DGPU_ERR_LIMIT, "a device bounds check rejected an access");
 }
 
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
 StageTimer::StageTimer(Context& ctx, const char* l) : c(ctx), label(l) {
   if (!c.timing_enabled) return;
   cudaEventCreate(&e0);
@@ -52,17 +57,27 @@ StageTimer::StageTimer(Context& ctx, const char* l) : c(ctx), label(l) {
 StageTimer::~StageTimer() {
   if (!c.timing_enabled || !e0) return;
   cudaEventRecord(e1, c.stream);
-  cudaEventSynchronize(e1);
-  float ms = 0.0f;
-  cudaEventElapsedTime(&ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  for (auto& kv : c.timing)
-    if (kv.first == label) {
-      kv.second += ms * 1e-3;
-      return;
-    }
-  c.timing.emplace_back(label, ms * 1e-3);
+  c.pending.push_back({label, e0, e1});
+}
+
+void resolve_timing(Context& c) {
+  if (c.pending.empty()) return;
+  cudaStreamSynchronize(c.stream);
+  for (auto& p : c.pending) {
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, p.e0, p.e1);
+    cudaEventDestroy(p.e0);
+    cudaEventDestroy(p.e1);
+    bool found = false;
+    for (auto& kv : c.timing)
+      if (kv.first == p.label) {
+        kv.second += ms * 1e-3;
+        found = true;
+        break;
+      }
+    if (!found) c.timing.emplace_back(p.label, ms * 1e-3);
+  }
+  c.pending.clear();
 }
 
 const void* stage_in(Context& c, int mem, const void* p, size_t bytes, Slot s) {

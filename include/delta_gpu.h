@@ -61,6 +61,11 @@ const char* dgpu_last_error(const dgpu_context* ctx);
  * DELTA_TIMING labels, src/timing.cpp:19-46); fills up to `cap` entries and
  * returns the count through *n. Enabled by DELTA_TIMING=1. */
 int dgpu_drain_timing(dgpu_context* ctx, char (*labels)[64], double* seconds, int cap, int* n);
+/* Switch the per-stage device timers on or off for this context (overrides
+ * DELTA_TIMING); stage events are recorded without synchronising. */
+int dgpu_set_timing(dgpu_context* ctx, int on);
+/* Number of kernels this library has launched in the process so far. */
+int dgpu_launch_count(unsigned long long* count);
 
 /* ---- basis (host math) ---------------------------------------------------- */
 /* GaussHermiteBasis::default_radius, src/basis.cpp:9-12. */
@@ -125,6 +130,10 @@ int dgpu_subtract(dgpu_context* ctx, int mem, int64_t width, int64_t height,
 int dgpu_photometric_scale(dgpu_context* ctx, int mem, const double* knots, int n_knots,
                            const double* theta, int64_t n_theta, const double* component_sums,
                            int nc, int64_t height, int64_t width, float* out);
+/* In-place sign flip of an n-element float image: the transients-positive
+ * convention applied to the difference when the science frame is the one
+ * convolved (python/delta/pipeline.py:687-689, np.negative on the host there). */
+int dgpu_negate(dgpu_context* ctx, int mem, float* data, int64_t n);
 /* photometric_scale_at, src/bindings.cpp:711-719 -> src/fit.cpp:532-544. out: m. */
 int dgpu_photometric_scale_at(const double* knots, int n_knots, const double* theta,
                               int64_t n_theta, const double* component_sums, int nc,
@@ -204,6 +213,42 @@ int dgpu_decorrelate_block(dgpu_context* ctx, const float* image, int n, const f
 /* decorrelation_kernel, src/bindings.cpp:748-760 -> src/noise.cpp:139-161. Host arrays. */
 int dgpu_decorrelation_kernel(dgpu_context* ctx, const float* kernel, int ksize, double var_science,
                               double var_reference, int n, float* out);
+
+/* ---- stamp selection ------------------------------------------------------------ */
+typedef struct {
+  int stamp_radius;       /* 15 */
+  double threshold_sigma; /* 5.0 */
+  int max_stamps;         /* 200 */
+  double saturation;      /* 0.0 */
+  int isolation_radius;   /* 0 -> 2 * stamp_radius */
+  int border;             /* 0 -> stamp_radius */
+  int fwhm_radius;        /* 0 -> max(5, stamp_radius / 2) */
+  int match_radius;       /* 2 */
+} dgpu_detect_params;
+
+/* estimate_background, src/bindings.cpp:232-237 -> src/detect.cpp:84-113. */
+int dgpu_estimate_background(dgpu_context* ctx, int mem, int64_t width, int64_t height, const float* data,
+                             const uint8_t* mask, double* median, double* sigma);
+/* detect_stamps, src/bindings.cpp:240-274 -> src/detect.cpp:159-241. Host output
+ * columns hold up to `capacity` stamps; *count receives the number found. */
+int dgpu_detect_stamps(dgpu_context* ctx, int mem, int64_t width, int64_t height, const float* data,
+                       const uint8_t* mask, const dgpu_detect_params* params, int capacity, int32_t* x, int32_t* y,
+                       double* flux, double* snr, double* fwhm, int* count);
+/* select_stamps, src/bindings.cpp:278-315 -> src/detect.cpp:260-314 (catalog
+ * positions when cat_x / cat_y are given, host arrays). */
+int dgpu_select_stamps(dgpu_context* ctx, int mem, int64_t width, int64_t height, const float* science,
+                       const float* reference, const uint8_t* science_mask, const uint8_t* reference_mask,
+                       const int32_t* cat_x, const int32_t* cat_y, int n_cat, const dgpu_detect_params* params,
+                       int capacity, int32_t* x, int32_t* y, double* fwhm_science, double* fwhm_reference,
+                       double* median_fwhm_science, double* median_fwhm_reference, int* direction_is_reference,
+                       int* count);
+/* Median unit-sum PSF stamp of the listed sources (the score path's
+ * _estimate_psf, python/delta/pipeline.py:285-302). out: host (2r+1)^2. */
+int dgpu_estimate_psf(dgpu_context* ctx, int mem, int64_t width, int64_t height, const float* image,
+                      const int32_t* xs, const int32_t* ys, int n, int radius, float* out);
+/* weighted_mean, src/bindings.cpp:107-124. */
+int dgpu_weighted_mean(dgpu_context* ctx, int mem, int64_t n, const float* data, const float* variance,
+                       const uint8_t* mask, double* out);
 
 /* ---- matched filter ---------------------------------------------------------- */
 /* matched_filter, src/bindings.cpp:878-898 -> src/noise.cpp:535-632

@@ -1,0 +1,183 @@
+"""GPU stamp selection, PSF estimate and the end-to-end pipeline.
+
+Stamp selection is checked against the reference-built detect.cpp
+(oracle/_ref) and its golden fixture; the pipeline against the reference's own
+statistical assertions (tests/test_pipeline.py of tkillestein/delta) and, stage
+by stage, against the oracle chain on the same inputs."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+from conftest import load_golden
+
+import delta_b200 as delta
+from delta_b200 import _core, validation
+from oracle import cref, refbuild
+from oracle import numpy_ref as nr
+
+pytestmark = pytest.mark.gpu
+
+
+def _stars(h, w, positions, total, sigma):
+    img = np.zeros((h, w), np.float64)
+    ys, xs = np.mgrid[0:h, 0:w]
+    amp = total / (2 * np.pi * sigma**2)
+    for x, y in positions:
+        img += amp * np.exp(-((xs - x) ** 2 + (ys - y) ** 2) / (2 * sigma**2))
+    return img, amp
+
+
+def _pair(sig_ref, sig_sci, transient_xy=(60, 140), seed=0):
+    h = w = 200
+    rng = np.random.default_rng(seed)
+    grid = [(x, y) for x in (40, 80, 120, 160) for y in (40, 80, 120, 160)]
+    ref, _ = _stars(h, w, grid, total=12000.0, sigma=sig_ref)
+    sci, _ = _stars(h, w, grid, total=12000.0, sigma=sig_sci)
+    trans, amp_t = _stars(h, w, [transient_xy], total=6000.0, sigma=sig_sci)
+    sci = sci + trans
+    ref = ref + 100.0 + rng.normal(0, 3.0, (h, w))
+    sci = sci + 100.0 + rng.normal(0, 3.0, (h, w))
+    return ref.astype(np.float32), sci.astype(np.float32), amp_t
+
+
+def _window_max(img, xy, r=8):
+    x, y = xy
+    return img[y - r : y + r + 1, x - r : x + r + 1].max()
+
+
+# --------------------------------------------------------------- stamp selection
+
+
+def test_background_and_selection_match_reference_golden():
+    g = load_golden("detect")
+    med, sig = _core.estimate_background(g["sci"])
+    np.testing.assert_allclose([med, sig], g["bg_sci"], rtol=0, atol=0)
+    sel = _core.select_stamps(g["sci"], g["ref"], stamp_radius=8, threshold_sigma=5.0, max_stamps=20)
+    np.testing.assert_array_equal(sel["x"], g["sel_x"])
+    np.testing.assert_array_equal(sel["y"], g["sel_y"])
+    np.testing.assert_allclose(sel["fwhm_science"], g["sel_fwhm_science"], rtol=1e-12)
+    np.testing.assert_allclose(sel["fwhm_reference"], g["sel_fwhm_reference"], rtol=1e-12)
+    assert (sel["direction"] == "reference") == bool(g["sel_direction"])
+
+
+@pytest.mark.parametrize("seed,size,n_star,max_stamps", [(0, 512, 300, 200), (1, 1024, 2000, 200),
+                                                         (2, 700, 900, 50)])
+def test_select_stamps_matches_reference(seed, size, n_star, max_stamps):
+    if not refbuild.available():
+        pytest.skip("reference library not built")
+    p = validation.synthetic_pair(size, size, n_star, seed, mask_fraction=0.005)
+    kw = dict(stamp_radius=12, threshold_sigma=5.0, max_stamps=max_stamps, saturation=p.saturation)
+    got = _core.select_stamps(p.science, p.reference, p.science_mask, p.reference_mask, **kw)
+    want = refbuild.select_stamps(p.science, p.reference, p.science_mask, p.reference_mask, **kw)
+    np.testing.assert_array_equal(got["x"], want["x"])
+    np.testing.assert_array_equal(got["y"], want["y"])
+    np.testing.assert_allclose(got["fwhm_science"], want["fwhm_science"], rtol=1e-12)
+    assert got["direction"] == want["direction"]
+    for k in ("median_fwhm_science", "median_fwhm_reference"):
+        np.testing.assert_allclose(got[k], want[k], rtol=1e-12)
+    # catalog-supplied positions
+    cx = np.asarray(want["x"][:40], np.int32)
+    cy = np.asarray(want["y"][:40], np.int32)
+    got_c = _core.select_stamps(p.science, p.reference, p.science_mask, p.reference_mask, cx, cy, **kw)
+    want_c = refbuild.select_stamps(p.science, p.reference, p.science_mask, p.reference_mask, cx, cy, **kw)
+    np.testing.assert_array_equal(got_c["x"], want_c["x"])
+    np.testing.assert_allclose(got_c["fwhm_reference"], want_c["fwhm_reference"], rtol=1e-12)
+
+
+def _np_estimate_psf(image, xs, ys, radius):
+    # python/delta/pipeline.py:285-302 restated
+    h, w = image.shape
+    stamps = []
+    for x, y in zip(xs, ys):
+        if x - radius < 0 or x + radius >= w or y - radius < 0 or y + radius >= h:
+            continue
+        cut = image[y - radius : y + radius + 1, x - radius : x + radius + 1].astype(np.float64)
+        cut = cut - np.median(cut)
+        total = cut.sum()
+        if total > 0:
+            stamps.append(cut / total)
+    psf = np.clip(np.median(np.stack(stamps), axis=0), 0.0, None)
+    return (psf / psf.sum()).astype(np.float32)
+
+
+def test_estimate_psf_and_weighted_mean():
+    p = validation.synthetic_pair(400, 400, 120, 3)
+    sel = _core.select_stamps(p.science, p.reference, stamp_radius=10)
+    for r in (8, 5):
+        got = _core.estimate_psf(p.science, sel["x"], sel["y"], r)
+        np.testing.assert_allclose(got, _np_estimate_psf(p.science, sel["x"], sel["y"], r), rtol=1e-6, atol=1e-9)
+    with pytest.raises(ValueError):
+        _core.estimate_psf(p.science, np.array([0]), np.array([0]), 8)
+    d = p.science.astype(np.float64)
+    v = p.science_var.astype(np.float64)
+    m = p.science_mask
+    good = (m == 0) & (v > 0)
+    want = np.sum(d[good] / v[good]) / np.sum(1.0 / v[good])
+    np.testing.assert_allclose(_core.weighted_mean(p.science, p.science_var, m), want, rtol=1e-12)
+
+
+# ---------------------------------------------------------------------- pipeline
+
+
+def test_subtract_removes_statics_keeps_transient_reference_sharper():
+    ref, sci, amp_t = _pair(sig_ref=1.6, sig_sci=2.4)
+    res = delta.subtract(sci, ref, gain=1.5, read_noise=4.0, n_knots=4, stamp_radius=12)
+    assert isinstance(res, delta.DiffResult)
+    assert res.solution.direction == "reference"
+    assert np.isfinite(res.solution.gcv)
+    assert np.abs(_window_max(res.difference, (80, 80))) < 0.25 * amp_t
+    assert _window_max(res.difference, (60, 140)) > 0.4 * amp_t
+
+
+def test_direction_flips_when_science_sharper():
+    ref, sci, amp_t = _pair(sig_ref=2.4, sig_sci=1.6)
+    res = delta.subtract(sci, ref, gain=1.5, read_noise=4.0, n_knots=4, stamp_radius=12)
+    assert res.solution.direction == "science"
+    assert _window_max(res.difference, (60, 140)) > 0.3 * amp_t
+
+
+def test_score_catalog_decorrelate_and_solution_roundtrip(tmp_path):
+    ref, sci, amp_t = _pair(sig_ref=1.6, sig_sci=2.4, seed=4)
+    sub = delta.Subtractor(n_knots=3, stamp_radius=12, score=True, decorrelate=True, block=64, cv_folds=0)
+    res = sub.subtract(sci, ref, gain=1.5, read_noise=4.0)
+    assert res.score is not None and res.psf is not None
+    assert res.source_catalog is not None
+    assert np.any(np.hypot(res.source_catalog["x"] - 60, res.source_catalog["y"] - 140) < 3)
+    path = tmp_path / "sol.npz"
+    res.solution.save(str(path))
+    sol = delta.KernelSolution.load(str(path))
+    again = sub.apply(sol, sci, ref, gain=1.5, read_noise=4.0)
+    np.testing.assert_array_equal(again.difference, res.difference)
+    cat2 = res.build_catalog(threshold_sigma=4.0, polarity="both")
+    assert "sign" in cat2.dtype.names
+
+
+@pytest.mark.parametrize("cv_folds", [0, 5])
+def test_pipeline_stages_match_oracle_chain(cv_folds):
+    """Stage-by-stage: the device pipeline on one C1-like frame vs the oracle
+    fed the same stamps (fit -> subtract -> score -> catalog)."""
+    p = validation.synthetic_pair(384, 384, 220, 7, mask_fraction=0.005)
+    kw = dict(n_max=4, radius=10, n_knots=3, stamp_radius=12, cv_folds=cv_folds, score=True, decorrelate=False,
+              saturation=p.saturation)
+    res = delta.subtract(p.science, p.reference, science_var=p.science_var, reference_var=p.reference_var,
+                         science_mask=p.science_mask, reference_mask=p.reference_mask, **kw)
+    sol = res.solution
+    assert sol.direction == "reference"
+    sel = _core.select_stamps(p.science, p.reference, p.science_mask, p.reference_mask, stamp_radius=12,
+                              saturation=p.saturation)
+    knots = nr.grid_knots(0, 0, 383, 383, 3, 3)
+    bconv = (lambda patch: refbuild.basis_convolve(patch, sol.beta, 4, 10)) if refbuild.available() else None
+    fit = nr.fit_kernel(p.science, p.reference, knots, sel["x"], sel["y"], 12, sol.beta, 4, np.logspace(-6, 6, 25),
+                        radius=10, cv_folds=cv_folds, science_var=p.science_var, reference_var=p.reference_var,
+                        science_mask=p.science_mask, reference_mask=p.reference_mask, basis_convolve_fn=bconv)
+    assert fit["lambda"] == sol.lam
+    np.testing.assert_allclose(sol.theta, fit["theta"], rtol=1e-6, atol=1e-9 * np.abs(fit["theta"]).max())
+    sub = cref.subtract(p.science, p.reference, knots, sol.theta, sol.beta, 4, 10, p.saturation, p.science_var,
+                        p.reference_var, p.science_mask, p.reference_mask)
+    assert np.array_equal(res.mask, sub["mask"])
+    pos = sub["variance"] > 0
+    assert np.max(np.abs(res.difference - sub["difference"])[pos] / np.sqrt(sub["variance"][pos])) < 1e-3
+    np.testing.assert_allclose(res.psf, _np_estimate_psf(p.science, sel["x"], sel["y"], 8), rtol=1e-6, atol=1e-9)
+    score = cref.matched_filter(res.difference, res.psf, res.variance)
+    np.testing.assert_array_equal(res.score, score)
