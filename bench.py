@@ -1,0 +1,490 @@
+#!/usr/bin/env python3
+"""Throughput of delta.subtract on a 4096x4096 spatially varying field, one B200 per rank.
+
+A step is one full subtract of one frame: stamp selection -> kernel fit (GCV) ->
+subtract -> ZOGY decorrelation -> PSF estimate + matched-filter score -> CCL
+catalog. Workload: 4096x4096 float32 pair, 20000 stars (dN/dF ~ F^-2.5 on
+1e3..1e6 e-), elliptical Moffat (beta 3, q 0.85, PA 30 deg) science PSF whose
+FWHM rises 3.0 -> 4.5 px along the diagonal, Gaussian FWHM 2.5 reference, 50
+transients at S/N 5-50, 1% masked; n_max 6, 4x4 thin-plate knots, GCV,
+stamp radius 15, decorrelate + score + catalog at 5 sigma. Inputs are seeded
+synthetic frames (each rank its own seed: weak scaling, no collective on the
+data path).
+
+  value   Mpix/s of the mixed-precision path, layers resident in HBM
+  plain   the same with the plain FP32 normal equations
+  e2e     the public delta_b200.subtract() call from pinned host arrays
+          (host->device upload and device->host products inside the timing)
+
+`--impl reference` times the CPU chain of the same workload instead (the
+reference's own detect/catalog/convolve code compiled from source plus the
+C / NumPy restatements of its fit, subtract, decorrelation and score).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "subtract Mpix/s on 1 B200: mixed-prec+batched vs plain, at stated FP64 error"
+UNIT = "Mpix/s"
+WORKLOAD = ("4096x4096 spatially varying Moffat field, 20000 stars, 50 transients; n_max 6, 16 TPS knots, GCV, "
+            "decorrelate + score + CCL at 5 sigma; one frame per step per GPU")
+# Algorithmic HBM bytes per science pixel of the fused model-convolve kernel:
+# science + reference (float32), reference mask (u8), difference (float32).
+MODEL_CONVOLVE_BYTES_PER_PX = 13
+MODEL_CONVOLVE_STAGE = "subtract: model convolve"
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("delta_b200", "reference"), default="delta_b200")
+    ap.add_argument("--size", type=int, default=4096, help="frame side (default: the 4096^2 workload)")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU leg (rank 0, N=1)")
+    return ap.parse_args(argv)
+
+
+def frame_config(size: int) -> dict:
+    scale = (size / 4096.0) ** 2
+    return {"size": size, "n_stars": max(50, int(round(20000 * scale))),
+            "n_transients": max(1, int(round(50 * scale)))}
+
+
+def make_frame(size: int, seed: int):
+    from delta_b200 import validation
+
+    fc = frame_config(size)
+    return validation.config2_pair(seed=seed, size=size, n_stars=fc["n_stars"], n_transients=fc["n_transients"])
+
+
+def subtract_kwargs(pair, precision: str | None = None) -> dict:
+    kw = dict(n_max=6, n_knots=4, cv_folds=0, stamp_radius=15, threshold_sigma=5.0, decorrelate=True, score=True,
+              source_catalog=True, saturation=pair.saturation)
+    if precision is not None:
+        kw["precision"] = precision
+    return kw
+
+
+# ---------------------------------------------------------------- clocks -------
+
+_REASON_BITS = {
+    "sw_power_cap": 0x4, "hw_slowdown": 0x8, "sync_boost": 0x10, "sw_thermal_slowdown": 0x20,
+    "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80, "applications_clocks_setting": 0x2,
+}
+
+
+def summarise_clocks(samples: list[tuple[float, float, int]]) -> dict:
+    """samples: (sm_mhz, sm_max_mhz, reasons bitmask) taken while the timed loop ran."""
+    if not samples:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+    seen = 0
+    for _, _, r in samples:
+        seen |= int(r)
+    return {"sm_mhz": float(statistics.median(s[0] for s in samples)),
+            "sm_max_mhz": float(max(s[1] for s in samples)),
+            "reasons": sorted(name for name, bit in _REASON_BITS.items() if seen & bit),
+            "samples": len(samples)}
+
+
+class ClockSampler:
+    """Reads SM clock, max clock and clock-event reasons through NVML every
+    `period` seconds on a thread (read-only queries)."""
+
+    def __init__(self, device_index: int, period: float = 0.1):
+        self.period = period
+        self.samples: list[tuple[float, float, int]] = []
+        self._stop = threading.Event()
+        self._thread = None
+        self.error = None
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self._nvml = pynvml
+            self._handle = self._find_handle(pynvml, device_index)
+        except Exception as exc:  # NVML missing: report no clocks rather than fail the bench
+            self._nvml = None
+            self.error = f"nvml unavailable: {exc}"
+
+    @staticmethod
+    def _find_handle(pynvml, device_index: int):
+        import torch
+
+        try:
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            return pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            pass
+        try:
+            bus = torch.cuda.get_device_properties(device_index)
+            pci = f"{bus.pci_domain_id:08x}:{bus.pci_bus_id:02x}:{bus.pci_device_id:02x}.0"
+            return pynvml.nvmlDeviceGetHandleByPciBusId(pci)
+        except Exception:
+            pass
+        return pynvml.nvmlDeviceGetHandleByIndex(device_index)
+
+    def _read(self):
+        n = self._nvml
+        sm = n.nvmlDeviceGetClockInfo(self._handle, n.NVML_CLOCK_SM)
+        mx = n.nvmlDeviceGetMaxClockInfo(self._handle, n.NVML_CLOCK_SM)
+        try:
+            reasons = n.nvmlDeviceGetCurrentClocksEventReasons(self._handle)
+        except Exception:
+            reasons = n.nvmlDeviceGetCurrentClocksThrottleReasons(self._handle)
+        return float(sm), float(mx), int(reasons)
+
+    def _loop(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self._read())
+            except Exception as exc:
+                self.error = str(exc)
+                return
+            self._stop.wait(self.period)
+
+    def __enter__(self):
+        if self._nvml is not None:
+            self._thread = threading.Thread(target=self._loop, daemon=True)
+            self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread is not None:
+            self._thread.join()
+
+    def summary(self) -> dict:
+        out = summarise_clocks(self.samples)
+        if self.error:
+            out["error"] = self.error
+        return out
+
+
+# ---------------------------------------------------------------- ranks --------
+
+
+def rank_env() -> tuple[int, int, int]:
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def max_over_ranks(value: float, device=None) -> float:
+    """Max of a per-rank scalar over the process group (identity without one)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(device=None) -> None:
+    import torch.distributed as dist
+
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        if device is not None and device.type == "cuda":
+            dist.barrier(device_ids=[device.index])
+        else:
+            dist.barrier()
+
+
+def timed_steps(fn, steps: int, device) -> float:
+    """Device milliseconds of `steps` calls of fn, barrier + synchronize on both
+    sides, CUDA events on the current stream; max over ranks."""
+    import torch
+
+    barrier(device)
+    torch.cuda.synchronize(device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize(device)
+    barrier(device)
+    return max_over_ranks(e0.elapsed_time(e1), device)
+
+
+# ---------------------------------------------------------------- pieces -------
+
+
+def load_peaks() -> tuple[dict, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def load_traffic(stage: str, size: int):
+    """DRAM bytes per launch of the roofline kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    try:
+        rows = json.loads(p.read_text())
+    except ValueError:
+        return None
+    for row in rows:
+        if row.get("stage") == stage:
+            return float(row["bytes_per_px"]) * size * size
+    return None
+
+
+def drain_stage_seconds(ctx) -> dict:
+    import ctypes
+
+    from delta_b200 import _lib
+
+    cap = 64
+    labels = (ctypes.c_char * 64 * cap)()
+    secs = (ctypes.c_double * cap)()
+    n = ctypes.c_int()
+    _lib.check(_lib.lib().dgpu_drain_timing(ctx.handle, labels, secs, cap, ctypes.byref(n)), ctx.handle)
+    return {bytes(labels[i]).split(b"\0", 1)[0].decode(): float(secs[i]) for i in range(min(n.value, cap))}
+
+
+def launch_count() -> int:
+    import ctypes
+
+    from delta_b200 import _lib
+
+    c = ctypes.c_ulonglong()
+    _lib.check(_lib.lib().dgpu_launch_count(ctypes.byref(c)))
+    return int(c.value)
+
+
+def pinned_copy(a):
+    import torch
+
+    t = torch.empty(a.shape, dtype=torch.from_numpy(a[:1].copy()).dtype, pin_memory=True)
+    out = t.numpy()
+    out[...] = a
+    return out
+
+
+def error_vs_fp64(out, ref) -> dict:
+    """Errors of one precision's products against the FP64 normal-equation path."""
+    th, th64 = np.asarray(out["solution"].theta), np.asarray(ref["solution"].theta)
+    d = out["difference"].double().cpu().numpy()
+    d64 = ref["difference"].double().cpu().numpy()
+    v64 = ref["variance"].double().cpu().numpy()
+    m64 = ref["mask"].cpu().numpy()
+    good = (v64 > 0) & (m64 == 0) & np.isfinite(d) & np.isfinite(d64)
+    z = (d - d64)[good] / np.sqrt(v64[good])
+    s = out["score"].double().cpu().numpy()
+    s64 = ref["score"].double().cpu().numpy()
+    ok = np.isfinite(s) & np.isfinite(s64)
+    cat, cat64 = out["catalog"], ref["catalog"]
+    return {"theta_rel": float(np.linalg.norm(th - th64) / max(np.linalg.norm(th64), 1e-300)),
+            "lambda_equal": bool(out["solution"].lam == ref["solution"].lam),
+            "diff_rms_sigma": float(np.sqrt(np.mean(z * z))) if z.size else None,
+            "diff_max_sigma": float(np.max(np.abs(z))) if z.size else None,
+            "score_max_abs": float(np.max(np.abs(s - s64)[ok])) if ok.any() else None,
+            "catalog_rows": [len(cat), len(cat64)]}
+
+
+def cpu_baseline(pair, size: int) -> dict:
+    """The CPU chain on one full frame of the workload (rank 0, N=1)."""
+    from oracle import chain
+
+    if not chain.available():
+        return {"value": None, "unit": UNIT, "cores": None, "kind": "port",
+                "unavailable": "oracle/_ref (the reference sources compiled by oracle/Makefile) is not built"}
+    kw = subtract_kwargs(pair)
+    kw.pop("saturation")
+    t0 = time.perf_counter()
+    stages: dict = {}
+    chain.run(pair.science, pair.reference, pair.science_var, pair.reference_var, pair.science_mask,
+              pair.reference_mask, saturation=pair.saturation, timings=stages,
+              **{k: v for k, v in kw.items() if k not in ("precision",)})
+    dt = time.perf_counter() - t0
+    return {"value": size * size / 1e6 / dt, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": f"1 full {size}x{size} frame of the workload, one pass ({dt:.1f} s): the reference's "
+                      "detect/catalog/basis-convolve code compiled from source + C (OpenMP) restatements of "
+                      "subtract and the matched filter + NumPy FP64 restatements of the fit and decorrelation",
+            "stage_seconds": {k: round(v, 3) for k, v in stages.items()}}
+
+
+# ---------------------------------------------------------------- arms ---------
+
+
+def run_reference(args) -> int:
+    rank, world, _ = rank_env()
+    if rank != 0:
+        return 0
+    from oracle import chain
+
+    if not chain.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref is not built (make -C oracle ref)"}))
+        return 0
+    # Each step is a bounded sample: the full frame when the run fits in ~3 minutes, else a smaller frame.
+    size = args.size
+    per_step = 14.0 * (size / 4096.0) ** 2  # seconds per full frame on 8 host cores
+    while size > 1024 and per_step * (args.steps + args.warmup) > 180.0:
+        size //= 2
+        per_step /= 4.0
+    pair = make_frame(size, args.seed)
+    kw = {k: v for k, v in subtract_kwargs(pair).items() if k != "saturation"}
+
+    def step():
+        chain.run(pair.science, pair.reference, pair.science_var, pair.reference_var, pair.science_mask,
+                  pair.reference_mask, saturation=pair.saturation, **kw)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    value = args.steps * size * size / 1e6 / dt
+    sample = (f"{size}x{size} frame of the workload per step" + ("" if size == args.size else
+              f" (the {args.size}^2 frame would not finish {args.steps + args.warmup} steps in minutes)"))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, **frame_config(args.size), "sample_size": size},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_gpu(args) -> int:
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = rank_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device (the product path has no CPU fallback)")
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
+
+    import delta_b200 as delta
+    from delta_b200 import _device, _lib
+    from delta_b200.pipeline import Subtractor
+
+    pair = make_frame(args.size, args.seed + rank)
+    size = args.size
+    frame = _device.DeviceFrame.from_numpy(pair.science, pair.reference, pair.science_var, pair.reference_var,
+                                           pair.science_mask, pair.reference_mask)
+    subs = {p: Subtractor(**subtract_kwargs(pair, p)) for p in ("mixed", "fp32", "fp64")}
+    ctx = _lib.context()
+
+    for _ in range(args.warmup):
+        _device.run(subs["mixed"], frame)
+    torch.cuda.synchronize(device)
+
+    # value: mixed precision, layers resident; stage timers on for the roofline kernel.
+    _lib.lib().dgpu_set_timing(ctx.handle, 1)
+    drain_stage_seconds(ctx)
+    l0 = launch_count()
+    with ClockSampler(local) as clocks:
+        ms = timed_steps(lambda: _device.run(subs["mixed"], frame), args.steps, device)
+    launches = launch_count() - l0
+    stages = drain_stage_seconds(ctx)
+    _lib.lib().dgpu_set_timing(ctx.handle, 0)
+
+    # plain FP32 normal equations, same inputs
+    for _ in range(args.warmup):
+        _device.run(subs["fp32"], frame)
+    ms_plain = timed_steps(lambda: _device.run(subs["fp32"], frame), args.steps, device)
+
+    # end to end through the public API from pinned host arrays
+    host = {k: pinned_copy(getattr(pair, k)) for k in ("science", "reference", "science_var", "reference_var",
+                                                       "science_mask", "reference_mask")}
+    kw = subtract_kwargs(pair, "mixed")
+    h2d = sum(a.nbytes for a in host.values())
+    res_holder = {}
+
+    def e2e_step():
+        res_holder["r"] = delta.subtract(host["science"], host["reference"], science_var=host["science_var"],
+                                         reference_var=host["reference_var"], science_mask=host["science_mask"],
+                                         reference_mask=host["reference_mask"], **kw)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    ms_e2e = timed_steps(e2e_step, args.steps, device)
+    r = res_holder["r"]
+    d2h = sum(a.nbytes for a in (r.difference, r.variance, r.mask, r.score) if a is not None)
+
+    # errors of mixed and plain against the FP64 normal-equation path (outside the timing)
+    out64 = _device.run(subs["fp64"], frame)
+    errors = {"mixed": error_vs_fp64(_device.run(subs["mixed"], frame), out64),
+              "plain": error_vs_fp64(_device.run(subs["fp32"], frame), out64)}
+
+    mpix = size * size / 1e6
+    value = world * args.steps * mpix / (ms / 1e3)
+    line = None
+    if rank == 0:
+        peaks, peak_kind = load_peaks()
+        t_conv = stages.get(MODEL_CONVOLVE_STAGE)
+        roofline = None
+        if t_conv:
+            per_launch = t_conv / args.steps
+            bytes_launch = MODEL_CONVOLVE_BYTES_PER_PX * size * size
+            achieved = bytes_launch / per_launch / 1e9
+            roofline = {"bound": "hbm", "kernel": "k_model_convolve", "achieved": achieved,
+                        "peak": float(peaks["hbm_gbs"]), "unit": "GB/s", "frac": achieved / float(peaks["hbm_gbs"]),
+                        "traffic": load_traffic(MODEL_CONVOLVE_STAGE, size), "peak_source": peak_kind,
+                        "algorithmic_bytes_per_launch": bytes_launch, "ms_per_launch": 1e3 * per_launch}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline(pair, size)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator of the workload)",
+            "config": {"workload": WORKLOAD, **frame_config(size), "precision": "mixed", "frames_per_rank": 1,
+                       "l2": "inputs larger than L2 (about 300 MB of layers per frame)"},
+            "plain": {"value": world * args.steps * mpix / (ms_plain / 1e3), "ms_per_step": ms_plain / args.steps,
+                      "precision": "fp32"},
+            "error_vs_fp64": errors,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * args.steps * mpix / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "stage_ms_per_step": {k: round(1e3 * v / args.steps, 4) for k, v in sorted(stages.items())},
+        }
+    if world > 1:
+        barrier(device)
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line))
+    return 0
+
+
+def main(argv=None) -> int:
+    args = parse_args(argv)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

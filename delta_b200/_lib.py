@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import sys
 import threading
 from pathlib import Path
 
@@ -206,12 +207,27 @@ class Context:
         check(lib().dgpu_synchronize(self.handle), self.handle)
 
 
+def _default_device() -> int:
+    env = os.environ.get("DELTA_B200_DEVICE")
+    if env is not None:
+        return int(env)
+    torch = sys.modules.get("torch")  # follow torch's current device when the caller uses it
+    if torch is not None and torch.cuda.is_initialized():
+        return int(torch.cuda.current_device())
+    return 0
+
+
 def context() -> Context:
-    """The calling thread's default context on device ``DELTA_B200_DEVICE`` (default 0)."""
-    ctx = getattr(_tls, "ctx", None)
+    """The calling thread's context on device ``DELTA_B200_DEVICE``, else torch's
+    current CUDA device when torch has initialised CUDA, else device 0 (one
+    context per thread and device)."""
+    dev = _default_device()
+    ctxs = getattr(_tls, "ctxs", None)
+    if ctxs is None:
+        ctxs = _tls.ctxs = {}
+    ctx = ctxs.get(dev)
     if ctx is None:
-        ctx = Context(int(os.environ.get("DELTA_B200_DEVICE", "0")))
-        _tls.ctx = ctx
+        ctx = ctxs[dev] = Context(dev)
     return ctx
 
 

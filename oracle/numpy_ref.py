@@ -807,6 +807,24 @@ def conv_var_at(x, y, k2, ks, r, var, mask) -> float:
     return acc
 
 
+def conv_var_window(k2, r, var, mask, x0, x1, y0, y1) -> np.ndarray:
+    """conv_var_at over the window [y0..y1] x [x0..x1] at once (FP64 terms of
+    the same float32 K^2 and Var samples; invalid samples contribute 0)."""
+    h, w = var.shape
+    ey0, ey1, ex0, ex1 = y0 - r, y1 + r, x0 - r, x1 + r
+    pad = np.zeros((ey1 - ey0 + 1, ex1 - ex0 + 1), np.float64)
+    sy0, sy1, sx0, sx1 = max(ey0, 0), min(ey1, h - 1), max(ex0, 0), min(ex1, w - 1)
+    v = np.asarray(var[sy0 : sy1 + 1, sx0 : sx1 + 1], np.float64)
+    ok = (v > 0.0) & np.isfinite(v)
+    if mask is not None:
+        ok &= mask[sy0 : sy1 + 1, sx0 : sx1 + 1] == 0
+    pad[sy0 - ey0 : sy1 - ey0 + 1, sx0 - ex0 : sx1 - ex0 + 1] = np.where(ok, v, 0.0)
+    ks = 2 * r + 1
+    win = np.lib.stride_tricks.sliding_window_view(pad, (ks, ks))
+    kf = np.asarray(k2, np.float64)[::-1, ::-1]
+    return np.einsum("jiab,ab->ji", win, kf)
+
+
 def gather_stamps(science, reference, stamp_x, stamp_y, stamp_radius, b1d, n_max, r,
                   science_var, reference_var, science_mask, reference_mask, basis_convolve_fn):
     """Stamp pixel gather + per-stamp B_n.  src/fit.cpp:83-229.
@@ -980,12 +998,19 @@ def fit_kernel(science, reference, knots, stamp_x, stamp_y, stamp_radius, beta, 
                     for n in range(nc):
                         kk = (kk + np.float32(a_s[0, n]) * phi[n]).astype(np.float32)
                     stamp_k2[s] = (kk * kk).astype(np.float32)
-                for j in rows:
-                    s = g["stamp"][j]
-                    vc = conv_var_at(int(g["px"][j]), int(g["py"][j]), stamp_k2[s], ks, r, var_c_img, reference_mask)
-                    rv = g["var_t"][j] + vc
-                    if rv > 0.0:
-                        weights[j] = 1.0 / rv
+                rows_arr = np.asarray(rows)
+                row_sid = g["stamp"][rows_arr]
+                for s in stamp_k2:
+                    js = rows_arr[row_sid == s]
+                    if js.size == 0:
+                        continue
+                    pxs = g["px"][js].astype(int)
+                    pys = g["py"][js].astype(int)
+                    x0, x1, y0, y1 = pxs.min(), pxs.max(), pys.min(), pys.max()
+                    cv = conv_var_window(stamp_k2[s], r, var_c_img, reference_mask, x0, x1, y0, y1)
+                    rv = g["var_t"][js] + cv[pys - y0, pxs - x0]
+                    pos = rv > 0.0
+                    weights[js[pos]] = 1.0 / rv[pos]
             else:
                 for j in rows:
                     if g["var_t"][j] > 0.0:
@@ -1252,6 +1277,38 @@ def whiten_score_psf(psf, knots, theta, beta, n_max, var_science, var_reference,
     vs = block_variance(var_science, bx, by, block, w, h)
     vr = block_variance(var_reference, bx, by, block, w, h)
     return whiten_psf(psf, kern, vs, vr, block)
+
+
+def estimate_psf(image, xs, ys, radius: int) -> np.ndarray:
+    """Median of background-subtracted, unit-sum stamps, clipped at 0 and
+    renormalised.  python/delta/pipeline.py:285-302."""
+    image = np.asarray(image, np.float32)
+    h, w = image.shape
+    stamps = []
+    for x, y in zip(xs, ys, strict=True):
+        if x - radius < 0 or x + radius >= w or y - radius < 0 or y + radius >= h:
+            continue
+        cut = image[y - radius : y + radius + 1, x - radius : x + radius + 1].astype(np.float64)
+        cut = cut - np.median(cut)
+        total = cut.sum()
+        if total > 0:
+            stamps.append(cut / total)
+    if not stamps:
+        raise ValueError("no usable sources for PSF estimation")
+    psf = np.clip(np.median(np.stack(stamps), axis=0), 0.0, None)
+    return np.ascontiguousarray(psf / psf.sum(), dtype=np.float32)
+
+
+def default_beta(fwhm_a: float, fwhm_b: float) -> float:
+    """max(0.8 sqrt(s_broad^2 - s_narrow^2), 0.5); 2.0 without a finite FWHM.
+    python/delta/pipeline.py:267-282."""
+    fwhms = [f for f in (fwhm_a, fwhm_b) if np.isfinite(f) and f > 0]
+    if not fwhms:
+        return 2.0
+    broad, narrow = max(fwhms), min(fwhms)
+    to_sigma = 1.0 / FWHM_PER_SIGMA
+    diff = (broad * to_sigma) ** 2 - (narrow * to_sigma) ** 2
+    return float(max(0.8 * (np.sqrt(diff) if diff > 0 else 0.0), 0.5))
 
 
 def matched_filter(image, psf, variance) -> np.ndarray:

@@ -85,28 +85,12 @@ def test_select_stamps_matches_reference(seed, size, n_star, max_stamps):
     np.testing.assert_allclose(got_c["fwhm_reference"], want_c["fwhm_reference"], rtol=1e-12)
 
 
-def _np_estimate_psf(image, xs, ys, radius):
-    # python/delta/pipeline.py:285-302 restated
-    h, w = image.shape
-    stamps = []
-    for x, y in zip(xs, ys):
-        if x - radius < 0 or x + radius >= w or y - radius < 0 or y + radius >= h:
-            continue
-        cut = image[y - radius : y + radius + 1, x - radius : x + radius + 1].astype(np.float64)
-        cut = cut - np.median(cut)
-        total = cut.sum()
-        if total > 0:
-            stamps.append(cut / total)
-    psf = np.clip(np.median(np.stack(stamps), axis=0), 0.0, None)
-    return (psf / psf.sum()).astype(np.float32)
-
-
 def test_estimate_psf_and_weighted_mean():
     p = validation.synthetic_pair(400, 400, 120, 3)
     sel = _core.select_stamps(p.science, p.reference, stamp_radius=10)
     for r in (8, 5):
         got = _core.estimate_psf(p.science, sel["x"], sel["y"], r)
-        np.testing.assert_allclose(got, _np_estimate_psf(p.science, sel["x"], sel["y"], r), rtol=1e-6, atol=1e-9)
+        np.testing.assert_allclose(got, nr.estimate_psf(p.science, sel["x"], sel["y"], r), rtol=1e-6, atol=1e-9)
     with pytest.raises(ValueError):
         _core.estimate_psf(p.science, np.array([0]), np.array([0]), 8)
     d = p.science.astype(np.float64)
@@ -178,6 +162,28 @@ def test_pipeline_stages_match_oracle_chain(cv_folds):
     assert np.array_equal(res.mask, sub["mask"])
     pos = sub["variance"] > 0
     assert np.max(np.abs(res.difference - sub["difference"])[pos] / np.sqrt(sub["variance"][pos])) < 1e-3
-    np.testing.assert_allclose(res.psf, _np_estimate_psf(p.science, sel["x"], sel["y"], 8), rtol=1e-6, atol=1e-9)
+    np.testing.assert_allclose(res.psf, nr.estimate_psf(p.science, sel["x"], sel["y"], 8), rtol=1e-6, atol=1e-9)
     score = cref.matched_filter(res.difference, res.psf, res.variance)
     np.testing.assert_array_equal(res.score, score)
+
+
+@pytest.mark.parametrize("direction", [None, "science"])
+def test_device_resident_path_matches_host_staged(direction):
+    """The HBM-resident stage chain (one upload) gives the same bits as the
+    per-call host-staged chain: same kernels, same inputs."""
+    p = validation.synthetic_pair(384, 384, 220, 7, mask_fraction=0.005)
+    kw = dict(n_max=4, radius=10, n_knots=3, stamp_radius=12, cv_folds=0, score=True, decorrelate=True, block=64,
+              saturation=p.saturation, direction=direction)
+    layers = dict(science_var=p.science_var, reference_var=p.reference_var, science_mask=p.science_mask,
+                  reference_mask=p.reference_mask)
+    a = delta.subtract(p.science, p.reference, device_resident=True, **layers, **kw)
+    b = delta.subtract(p.science, p.reference, device_resident=False, **layers, **kw)
+    assert a.solution.direction == b.solution.direction
+    np.testing.assert_array_equal(a.solution.theta, b.solution.theta)
+    for name in ("difference", "variance", "mask", "score", "psf"):
+        np.testing.assert_array_equal(getattr(a, name), getattr(b, name), err_msg=name)
+    assert a.source_catalog.dtype == b.source_catalog.dtype
+    np.testing.assert_array_equal(a.source_catalog, b.source_catalog)
+    again = delta.apply(a.solution, p.science, p.reference, device_resident=True, **layers,
+                        **{k: v for k, v in kw.items() if k != "direction"})
+    np.testing.assert_array_equal(again.difference, a.difference)
