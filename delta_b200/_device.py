@@ -63,9 +63,14 @@ class DeviceFrame:
                    up(smask, np.uint8), up(rmask, np.uint8))
 
 
+_CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy: handle 0 would select the context's own stream
+
+
 def _ctx_on_torch_stream():
+    """The thread's context, ordered on torch's current stream (the layers are
+    torch tensors written there)."""
     ctx = context()
-    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream or _CUDA_STREAM_LEGACY)
     return ctx
 
 

@@ -123,8 +123,11 @@ void dgpu_destroy(dgpu_context* ctx) {
 
 int dgpu_set_stream(dgpu_context* ctx, void* stream) {
   return guarded(ctx, [&](Context& c) {
+    const cudaStream_t next = stream ? static_cast<cudaStream_t>(stream) : c.own_stream;
+    if (next == c.stream) return;
+    // Work already queued on the old stream must finish before the new one runs.
     DGPU_CUDA(cudaStreamSynchronize(c.stream));
-    c.stream = stream ? static_cast<cudaStream_t>(stream) : c.own_stream;
+    c.stream = next;
   });
 }
 

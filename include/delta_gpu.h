@@ -13,7 +13,7 @@
  * work is stream-ordered on the context's stream and the call returns without
  * a final synchronisation unless the algorithm itself needs a host decision).
  * Images are row-major float32 (index y*width + x), masks uint8 bit flags
- * (src/../include/delta/image.hpp:14-22), optional layers are NULL.
+ * (include/delta/image.hpp:14-22), optional layers are NULL.
  *
  * Threading: one context per host thread; calls on a context are serialised on
  * its stream.
@@ -53,7 +53,11 @@ int dgpu_device_count(int* count);
 int dgpu_create(int device, dgpu_context** out);
 void dgpu_destroy(dgpu_context* ctx);
 /* Run subsequent work on a caller stream (a cudaStream_t); NULL restores the
- * context's own stream. */
+ * context's own stream, which is non-blocking: it does NOT order after work on
+ * the legacy default stream. A caller whose buffers are produced on the legacy
+ * default stream passes cudaStreamLegacy ((void*)0x1) here. Switching streams
+ * waits for the work already queued on the previous one; setting the current
+ * stream again is free. */
 int dgpu_set_stream(dgpu_context* ctx, void* stream);
 int dgpu_synchronize(dgpu_context* ctx);
 const char* dgpu_last_error(const dgpu_context* ctx);
@@ -96,7 +100,7 @@ int dgpu_tps_evaluate(const double* knots, int k, const double* points, int64_t 
 
 /* ---- kernel model ---------------------------------------------------------- */
 /* A fitted solution: knots (k x 2), theta ((nc+1)*k, ordered
- * [c_0 | ... | c_{nc-1} | b], src/../include/delta/solve.hpp:12-15), basis. */
+ * [c_0 | ... | c_{nc-1} | b], include/delta/solve.hpp:12-15), basis. */
 typedef struct {
   const double* knots; /* host, k x 2 */
   int n_knots;
@@ -140,7 +144,7 @@ int dgpu_photometric_scale_at(const double* knots, int n_knots, const double* th
                               const double* points, int64_t m, double* out);
 
 /* ---- penalised GLS + stamp fit ------------------------------------------------ */
-/* Result of a GLS solve (src/../include/delta/solve.hpp:16-26) plus the
+/* Result of a GLS solve (include/delta/solve.hpp:16-26) plus the
  * fit_kernel diagnostics (include/delta/fit.hpp:16-37). Array members are
  * caller buffers: theta[(nc+1)*k], lambda_grid / gcv_curve[n_lambda],
  * component_sums[nc], stamp_*[n_stamps supplied]; the stamp arrays receive

@@ -187,3 +187,37 @@ def test_device_resident_path_matches_host_staged(direction):
     again = delta.apply(a.solution, p.science, p.reference, device_resident=True, **layers,
                         **{k: v for k, v in kw.items() if k != "direction"})
     np.testing.assert_array_equal(again.difference, a.difference)
+
+
+@pytest.mark.parametrize("size", [1024, 2048])
+def test_strided_background_and_selection_match_reference(size):
+    """Frames above 2^18 px take the strided background sample (step n / 2^18,
+    src/detect.cpp:96-106); selection must still equal the reference's."""
+    if not refbuild.available():
+        pytest.skip("oracle/_ref not built")
+    scale = (size / 4096.0) ** 2
+    p = validation.config2_pair(seed=3, size=size, n_stars=int(20000 * scale), n_transients=2)
+    for img, m in ((p.science, p.science_mask), (p.reference, p.reference_mask)):
+        assert _core.estimate_background(img, m) == refbuild.estimate_background(img, m)
+    kw = dict(stamp_radius=15, threshold_sigma=5.0, max_stamps=200, saturation=p.saturation)
+    got = _core.select_stamps(p.science, p.reference, p.science_mask, p.reference_mask, **kw)
+    want = refbuild.select_stamps(p.science, p.reference, p.science_mask, p.reference_mask, **kw)
+    np.testing.assert_array_equal(got["x"], want["x"])
+    np.testing.assert_array_equal(got["y"], want["y"])
+    np.testing.assert_allclose(got["fwhm_science"], want["fwhm_science"], rtol=1e-12)
+    assert got["direction"] == want["direction"]
+
+
+def test_device_resident_large_frame_matches_host_staged():
+    """2048^2 frame: large enough that an upload left unordered against the
+    library's stream would be caught."""
+    p = validation.config2_pair(seed=5, size=2048, n_stars=5000, n_transients=12)
+    kw = dict(n_knots=4, cv_folds=0, decorrelate=True, score=True, saturation=p.saturation, precision="mixed")
+    layers = dict(science_var=p.science_var, reference_var=p.reference_var, science_mask=p.science_mask,
+                  reference_mask=p.reference_mask)
+    a = delta.subtract(p.science, p.reference, device_resident=True, **layers, **kw)
+    b = delta.subtract(p.science, p.reference, device_resident=False, **layers, **kw)
+    np.testing.assert_array_equal(a.solution.theta, b.solution.theta)
+    for name in ("difference", "variance", "mask", "score"):
+        np.testing.assert_array_equal(getattr(a, name), getattr(b, name), err_msg=name)
+    np.testing.assert_array_equal(a.source_catalog, b.source_catalog)
