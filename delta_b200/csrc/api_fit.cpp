@@ -99,7 +99,7 @@ struct Engine {
   struct Work {
     double *A, *Linv, *theta, *edf, *raw, *rss, *gcv, *lam;
     int *ok, *midx, *ridx;
-    unsigned* barrier;
+    double* partial;
   };
   Work work(int nsys) {
     const int Pp = solve_pp(P);
@@ -119,7 +119,7 @@ struct Engine {
     w.ok = reinterpret_cast<int*>(w.lam + nsys);
     w.midx = w.ok + nsys;
     w.ridx = w.midx + nsys;
-    w.barrier = static_cast<unsigned*>(c.slot(kSlotFft2, 64));
+    w.partial = static_cast<double*>(c.slot(kSlotFft2, sizeof(double) * 8 * std::max(nsys, 1)));
     return w;
   }
 
@@ -143,7 +143,7 @@ struct Engine {
     b.edf = w.edf;
     b.ok = w.ok;
     b.status = c.d_status;
-    b.barrier = w.barrier;
+    b.partial = w.partial;
     launch_solve_batch(c, b);
   }
 

@@ -47,7 +47,8 @@ void launch_reweight(cudaStream_t st, const StampGeom& g, int n_stamps, const Tp
 // Batched penalised GLS: for each system s of a batch, A_s = M_s + lam_s P0
 // (P0 = blockdiag of the k x k penalty), Cholesky A_s = L L^T, L^{-1},
 // theta_s = A_s^{-1} rhs_s, edf_s = P - lam_s ||L^{-1} F||_F^2 and, when
-// requested, the held-out error of a CV fold. One cooperative launch.
+// requested, the held-out error of a CV fold. One cluster launch, one
+// thread-block cluster per system.
 // ---------------------------------------------------------------------------
 struct SolveBatch {
   int P = 0, k = 0, nf = 0, r = 0;  // unknowns, knots, fields, rank of the penalty
@@ -65,7 +66,7 @@ struct SolveBatch {
   double* edf = nullptr;            // nsys
   int* ok = nullptr;                // nsys: 1 if the Cholesky succeeded
   unsigned* status = nullptr;
-  unsigned* barrier = nullptr;      // 2 words, zeroed before launch
+  double* partial = nullptr;        // nsys x 8 per-rank trace partials
 };
 int solve_pp(int P);  // padded size
 void launch_solve_batch(Context& c, const SolveBatch& b);

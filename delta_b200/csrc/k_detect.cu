@@ -176,9 +176,8 @@ __device__ double fwhm_dev(const float* img, int w, int h, int x, int y, int r, 
   return 2.354820045030949 * sqrt(var);
 }
 
-__global__ void k_peaks(int w, int h, const float* __restrict__ img, const uint8_t* __restrict__ mask,
-                        const float* __restrict__ bg, DetectParamsDev p, unsigned* count, int cap,
-                        int* __restrict__ cand) {
+__global__ void k_peaks(int w, int h, const float* __restrict__ img, const float* __restrict__ bg,
+                        DetectParamsDev p, unsigned* count, int cap, int* __restrict__ cand) {
   const double med = static_cast<double>(bg[0]);
   const double sigma = 1.4826 * static_cast<double>(bg[1]);
   const double thr = med + p.threshold_sigma * (sigma > 0.0 ? sigma : 1.0);
@@ -201,9 +200,38 @@ __global__ void k_peaks(int w, int h, const float* __restrict__ img, const uint8
         }
       }
     if (!peak) continue;
-    if (!footprint_ok_dev(img, mask, w, h, x, y, p.stamp_radius, p.saturation)) continue;
     const unsigned slot = atomicAdd(count, 1u);
     if (static_cast<int>(slot) < cap) cand[slot] = static_cast<int>(i);
+  }
+}
+
+// Stamp footprint of every 3x3 peak, one warp per peak: fully on the frame,
+// finite, unmasked and below saturation (src/detect.cpp:190-214).
+__global__ void k_footprint(int w, int h, const float* __restrict__ img, const uint8_t* __restrict__ mask,
+                            DetectParamsDev p, const unsigned* __restrict__ n_peaks, int cap,
+                            const int* __restrict__ peaks, unsigned* count, int* __restrict__ cand) {
+  const int lane = threadIdx.x & 31;
+  const int nwarp = static_cast<int>((gridDim.x * blockDim.x) >> 5);
+  const int np = min(static_cast<int>(*n_peaks), cap);
+  const int r = p.stamp_radius;
+  for (int c = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5); c < np; c += nwarp) {
+    const int i = peaks[c];
+    const int x = i % w, y = i / w;
+    if (x - r < 0 || x + r >= w || y - r < 0 || y + r >= h) continue;
+    bool ok = true;
+    for (int dy = -r; dy <= r && ok; ++dy) {
+      for (int dx = lane - r; dx <= r; dx += 32) {
+        const size_t j = static_cast<size_t>(y + dy) * w + (x + dx);
+        const float v = img[j];
+        if (!isfinite(v) || (mask && mask[j] != 0) || (p.saturation > 0.0 && static_cast<double>(v) >= p.saturation))
+          ok = false;
+      }
+      ok = __all_sync(0xffffffffu, ok);
+    }
+    if (ok && lane == 0) {
+      const unsigned slot = atomicAdd(count, 1u);
+      if (static_cast<int>(slot) < cap) cand[slot] = i;
+    }
   }
 }
 
@@ -487,15 +515,19 @@ int run_detect(Context& c, int w, int h, const float* img, const uint8_t* mask, 
   unsigned long long* keys2 = keys + cap;
   int* vals = reinterpret_cast<int*>(c.slot(which ? kSlotFft3 : kSlotFft2, sizeof(int) * cap + 64));
   int* nk = vals + cap;
-  DGPU_CUDA(cudaMemsetAsync(count, 0, sizeof(unsigned), s));
+  unsigned* n_peaks = count + 1;  // 3x3 peaks before the footprint test; `sorted` holds them until the sort
+  DGPU_CUDA(cudaMemsetAsync(count, 0, 2 * sizeof(unsigned), s));
   const int blocks = static_cast<int>(std::min<int64_t>((n + 255) / 256, 148 * 16));
-  k_peaks<<<blocks, 256, 0, s>>>(w, h, img, mask, bg, p, count, cap, cand);
+  k_peaks<<<blocks, 256, 0, s>>>(w, h, img, bg, p, n_peaks, cap, sorted);
   DGPU_LAUNCH("k_peaks");
-  unsigned hc = 0;
-  DGPU_CUDA(cudaMemcpyAsync(&hc, count, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  k_footprint<<<148 * 8, 256, 0, s>>>(w, h, img, mask, p, n_peaks, cap, sorted, count, cand);
+  DGPU_LAUNCH("k_footprint");
+  unsigned hc[2] = {0, 0};
+  DGPU_CUDA(cudaMemcpyAsync(hc, count, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   DGPU_CUDA(cudaStreamSynchronize(s));
-  if (hc > static_cast<unsigned>(cap)) fail(DGPU_ERR_RUNTIME, "detect_stamps: more than 2^20 peak candidates");
-  const int nc = static_cast<int>(hc);
+  if (hc[1] > static_cast<unsigned>(cap)) fail(DGPU_ERR_RUNTIME, "detect_stamps: more than 2^20 peak candidates");
+  const unsigned nfoot = hc[0];
+  const int nc = static_cast<int>(nfoot);
   float hbg[2];
   DGPU_CUDA(cudaMemcpyAsync(hbg, bg, sizeof(hbg), cudaMemcpyDeviceToHost, s));
   int nkept = 0;
