@@ -160,7 +160,7 @@ struct Engine {
   // M, rhs, ywy, n over the rows whose unit mask is set.
   void assemble(const uint8_t* mask, double* M, double* rhs, double* ywy, long long* n) {
     launch_rhs(c, N, nc, k, SS, R, mask, nullptr, rhs, ywy, n);
-    launch_normal_equations(c, prec == DGPU_PREC_MIXED ? DGPU_PREC_FP32 : prec, N, nc, k, SS, R, mask, M);
+    launch_normal_equations(c, prec, N, nc, k, SS, R, mask, M);
   }
 
   // One FP64 refinement step of system s at lambda (theta updated in place).
@@ -288,7 +288,7 @@ struct Engine {
         DGPU_CUDA(cudaMemcpyAsync(fm, m.data(), n_units, cudaMemcpyHostToDevice, c.stream));
         long long* dummy = nall + 1;
         launch_rhs(c, N, nc, k, SS, R, fm, nullptr, rg + static_cast<size_t>(g) * P, yg + g, dummy);
-        launch_normal_equations(c, prec == DGPU_PREC_MIXED ? DGPU_PREC_FP32 : prec, N, nc, k, SS, R, fm,
+        launch_normal_equations(c, prec, N, nc, k, SS, R, fm,
                                 Mg + g * PP);
         DGPU_CUDA(cudaStreamSynchronize(c.stream));
       }

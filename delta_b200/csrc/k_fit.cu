@@ -317,20 +317,26 @@ void launch_normal_equations(Context& c, int prec, int64_t N, int nc, int k, int
   int2* dpairs = static_cast<int2*>(c.slot(kSlotFit10, sizeof(int2) * (Mu + Nv)));
   DGPU_CUDA(cudaMemcpyAsync(dpairs, up.data(), sizeof(int2) * Mu, cudaMemcpyHostToDevice, st));
   DGPU_CUDA(cudaMemcpyAsync(dpairs + Mu, vp.data(), sizeof(int2) * Nv, cudaMemcpyHostToDevice, st));
-  const int gx = (Mu + kNeT - 1) / kNeT, gy = (Nv + kNeT - 1) / kNeT;
-  // Split K (rows) so the grid covers the GPU a few times over.
-  const int64_t target_splits = std::max<int64_t>(1, (148 * 6) / (gx * gy));
-  int64_t rps = std::max<int64_t>(kNeR * 8, (N + target_splits - 1) / target_splits);
-  rps = (rps + kNeR - 1) / kNeR * kNeR;
-  const int nsplit = static_cast<int>((N + rps - 1) / rps);
-  double* gpart = static_cast<double*>(c.slot(kSlotFit11, sizeof(double) * static_cast<size_t>(nsplit) * Mu * Nv));
   double* g = static_cast<double*>(c.slot(kSlotFit12, sizeof(double) * static_cast<size_t>(Mu) * Nv));
-  dim3 grid(gx, gy, nsplit);
-  if (prec == DGPU_PREC_FP32)
-    k_normal_kron<float><<<grid, 256, 0, st>>>(N, nc, k, SS, R, accepted, dpairs, Mu, dpairs + Mu, Nv, rps, gpart);
-  else
-    k_normal_kron<double><<<grid, 256, 0, st>>>(N, nc, k, SS, R, accepted, dpairs, Mu, dpairs + Mu, Nv, rps, gpart);
-  DGPU_LAUNCH("k_normal_kron");
+  double* gpart = nullptr;
+  int nsplit = 0;
+  if (prec == DGPU_PREC_MIXED) {
+    nsplit = launch_normal_tc(c, N, nc, k, SS, R, accepted, dpairs, Mu, dpairs + Mu, Nv, kSlotFit11, &gpart);
+  } else {
+    const int gx = (Mu + kNeT - 1) / kNeT, gy = (Nv + kNeT - 1) / kNeT;
+    // Split K (rows) so the grid covers the GPU a few times over.
+    const int64_t target_splits = std::max<int64_t>(1, (148 * 6) / (gx * gy));
+    int64_t rps = std::max<int64_t>(kNeR * 8, (N + target_splits - 1) / target_splits);
+    rps = (rps + kNeR - 1) / kNeR * kNeR;
+    nsplit = static_cast<int>((N + rps - 1) / rps);
+    gpart = static_cast<double*>(c.slot(kSlotFit11, sizeof(double) * static_cast<size_t>(nsplit) * Mu * Nv));
+    dim3 grid(gx, gy, nsplit);
+    if (prec == DGPU_PREC_FP32)
+      k_normal_kron<float><<<grid, 256, 0, st>>>(N, nc, k, SS, R, accepted, dpairs, Mu, dpairs + Mu, Nv, rps, gpart);
+    else
+      k_normal_kron<double><<<grid, 256, 0, st>>>(N, nc, k, SS, R, accepted, dpairs, Mu, dpairs + Mu, Nv, rps, gpart);
+    DGPU_LAUNCH("k_normal_kron");
+  }
   k_reduce_g<<<std::min(148 * 4, (Mu * Nv + 255) / 256), 256, 0, st>>>(nsplit, Mu * Nv, gpart, g);
   DGPU_LAUNCH("k_reduce_g");
   const int P = nf * k;

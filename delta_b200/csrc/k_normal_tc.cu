@@ -1,0 +1,359 @@
+// Normal equations of the kernel fit on the 5th-generation tensor cores
+// (reference src/solve.cpp:70-145, the X^T W X rank updates), "mixed" precision.
+//
+// The Kronecker-packed contraction
+//     G[u][v] = sum_i U[i][u] V[i][v],   U[i][u] = b_a b_b (u = {a,b}, b = [bn_i, 1]),
+//                                        V[i][v] = w_i d_m d_m' (v = {m,m'}),
+// is a (Mu x N) x (N x Nv) product with the N stamp rows as the reduction
+// dimension. Each CTA owns one 128 x BN output tile and one contiguous row
+// range (split K). Per 64-row chunk the CTA stages the rows in shared memory,
+// generates U and V for its tile in FP32, splits every value into
+// x = hi + lo (two bf16), writes both into the UMMA K-major canonical layout,
+// and one elected thread issues tcgen05.mma (kind::f16, bf16 x bf16 -> FP32)
+// for hi*hi + hi*lo + lo*hi into the TMEM accumulator (BF16x3: about 16
+// significant bits per product, FP32 accumulation). Two shared-memory stages
+// let the tensor core consume chunk c while the threads generate chunk c+1;
+// tcgen05.commit on an mbarrier releases a stage. The epilogue reads TMEM
+// with tcgen05.ld and writes FP64 partials; the host-side caller reduces the
+// splits in a fixed order in FP64 and an FP64 refinement step follows the solve.
+//
+// Every mbarrier wait is bounded: on expiry the kernel sets the loop-limit
+// status bit, waits (bounded) for its own MMAs, frees its TMEM and returns.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "dev_common.cuh"
+#include "fit_internal.h"
+
+namespace dgpu {
+namespace {
+
+constexpr int kBM = 128;       // u rows per tile (UMMA M)
+constexpr int kKC = 64;        // stamp rows per chunk (4 UMMA K-steps of 16)
+constexpr int kThreads = 256;
+constexpr long long kSpinCap = 1ll << 22;
+
+struct TcArgs {
+  int64_t N;
+  int nc, k, SS;
+  FitRows R;
+  const uint8_t* accepted;
+  const int2* upairs;
+  int Mu;
+  const int2* vpairs;
+  int Nv;
+  int BN;  // N tile, multiple of 16, <= 256
+  int tmem_cols;
+  int64_t rows_per_split;
+  double* gpart;
+  unsigned* status;
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// UMMA shared-memory descriptor, no swizzle (K-major "interleaved" canonical
+// layout): start address, leading byte offset (between the two K-adjacent
+// 8x16-byte core matrices), stride byte offset (between 8-row groups),
+// descriptor version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
+  d |= static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16;
+  d |= static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32;
+  d |= static_cast<uint64_t>(1) << 46;
+  return d;
+}
+
+// kind::f16 instruction descriptor: FP32 accumulate, bf16 A and B, both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(N >> 3) << 17) |
+         (static_cast<uint32_t>(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+// Bounded wait for the phase of `bar` with the given parity; false on expiry.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  const uint32_t a = smem_addr(bar);
+  for (long long it = 0; it < kSpinCap; ++it) {
+    uint32_t done = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      :
+      : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Byte offset of element (row, kk) of a rows x kKC bf16 tile in the K-major
+// canonical layout: 8x8 core matrices of 128 contiguous bytes, the kKC/8 core
+// matrices of one 8-row group adjacent (LBO = 128 B), groups kKC*16 B apart (SBO).
+__device__ __forceinline__ uint32_t canon_off(int row, int kg) {
+  return static_cast<uint32_t>(((row >> 3) * (kKC / 8) + kg) * 128 + (row & 7) * 16);
+}
+
+__device__ __forceinline__ void split_store(unsigned char* hi_base, unsigned char* lo_base, uint32_t off,
+                                            const float (&v)[8]) {
+  __align__(16) __nv_bfloat16 h[8];
+  __align__(16) __nv_bfloat16 l[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    h[j] = __float2bfloat16_rn(v[j]);
+    l[j] = __float2bfloat16_rn(v[j] - __bfloat162float(h[j]));
+  }
+  *reinterpret_cast<uint4*>(hi_base + off) = *reinterpret_cast<const uint4*>(h);
+  *reinterpret_cast<uint4*>(lo_base + off) = *reinterpret_cast<const uint4*>(l);
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int tid = threadIdx.x;
+  const int BN = a.BN;
+  const int nf = a.nc + 1;
+  const int u0 = blockIdx.x * kBM, v0 = blockIdx.y * BN;
+  const int64_t rbeg = static_cast<int64_t>(blockIdx.z) * a.rows_per_split;
+  const int64_t rend = min(a.N, rbeg + a.rows_per_split);
+  const int nchunks = rend > rbeg ? static_cast<int>((rend - rbeg + kKC - 1) / kKC) : 0;
+
+  // Shared memory carve-up (all operand buffers 1024-byte aligned).
+  const uint32_t a_bytes = kBM * kKC * 2, b_bytes = static_cast<uint32_t>(BN) * kKC * 2;
+  // stage st: A hi at st*a_bytes, A lo at (2+st)*a_bytes; B hi / lo likewise after the A buffers
+  unsigned char* b_base = smem + 4 * a_bytes;
+  float* bn_s = reinterpret_cast<float*>(b_base + 4 * b_bytes);  // kKC x nf
+  float* d_s = bn_s + kKC * nf;                                  // kKC x k
+  float* w_s = d_s + kKC * a.k;                                  // kKC
+  int2* up_s = reinterpret_cast<int2*>(w_s + kKC);               // kBM
+  int2* vp_s = up_s + kBM;                                       // BN
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(vp_s + BN + (BN & 1));
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
+  __shared__ int s_fail;
+
+  for (int m = tid; m < kBM; m += blockDim.x) up_s[m] = (u0 + m < a.Mu) ? a.upairs[u0 + m] : make_int2(-1, -1);
+  for (int n = tid; n < BN; n += blockDim.x) vp_s[n] = (v0 + n < a.Nv) ? a.vpairs[v0 + n] : make_int2(-1, -1);
+  if (tid == 0) {
+    s_fail = 0;
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (tid < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                 "r"(a.tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t idesc = umma_idesc_bf16(kBM, BN);
+  constexpr uint32_t kLBO = 128, kSBO = (kKC / 8) * 128;
+
+  int issued = 0;  // chunks whose MMAs were issued (uniform over the CTA)
+  for (int c = 0; c < nchunks; ++c) {
+    const int st = c & 1;
+    unsigned char* ahi = smem + st * a_bytes;
+    unsigned char* alo = smem + (2 + st) * a_bytes;
+    unsigned char* bhi = b_base + st * b_bytes;
+    unsigned char* blo = b_base + (2 + st) * b_bytes;
+    const int64_t r0 = rbeg + static_cast<int64_t>(c) * kKC;
+    // Stage the chunk's rows (the previous chunk's generation finished at the last barrier).
+    for (int e = tid; e < kKC * nf; e += blockDim.x) {
+      const int r = e / nf, q = e - r * nf;
+      const int64_t row = r0 + r;
+      float v = 0.0f;
+      if (row < rend) v = q < a.nc ? static_cast<float>(a.R.bn[row * a.nc + q]) : 1.0f;
+      bn_s[e] = v;
+    }
+    for (int e = tid; e < kKC * a.k; e += blockDim.x) {
+      const int r = e / a.k, q = e - r * a.k;
+      const int64_t row = r0 + r;
+      d_s[e] = row < rend ? static_cast<float>(a.R.d[row * a.k + q]) : 0.0f;
+    }
+    for (int r = tid; r < kKC; r += blockDim.x) {
+      const int64_t row = r0 + r;
+      const bool act = row < rend && a.R.valid[row] && a.accepted[row / a.SS];
+      w_s[r] = act ? static_cast<float>(a.R.w[row]) : 0.0f;
+    }
+    // The MMAs of chunk c-2 read this stage: wait for their commit.
+    if (c >= 2 && !mbar_wait(&mbar[st], static_cast<unsigned>((c - 2) >> 1) & 1u)) s_fail = 1;
+    __syncthreads();
+    if (s_fail) break;
+    // A = U tile (kBM x kKC), 8 consecutive rows (one 16-byte store) per item;
+    // consecutive threads take consecutive tile rows (conflict-free stores).
+    for (int item = tid; item < kBM * (kKC / 8); item += blockDim.x) {
+      const int m = (item & 7) + ((item >> 3) / (kKC / 8)) * 8;
+      const int kg = (item >> 3) % (kKC / 8);
+      const int2 p = up_s[m];
+      float v[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const float* b = bn_s + (kg * 8 + j) * nf;
+        v[j] = p.x >= 0 ? b[p.x] * b[p.y] : 0.0f;
+      }
+      split_store(ahi, alo, canon_off(m, kg), v);
+    }
+    // B = V tile (BN x kKC).
+    for (int item = tid; item < BN * (kKC / 8); item += blockDim.x) {
+      const int n = (item & 7) + ((item >> 3) / (kKC / 8)) * 8;
+      const int kg = (item >> 3) % (kKC / 8);
+      const int2 q = vp_s[n];
+      float v[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int r = kg * 8 + j;
+        const float* d = d_s + r * a.k;
+        v[j] = q.x >= 0 ? (w_s[r] * d[q.x]) * d[q.y] : 0.0f;
+      }
+      split_store(bhi, blo, canon_off(n, kg), v);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t ah = smem_addr(ahi), al = smem_addr(alo);
+      const uint32_t bh = smem_addr(bhi), bl = smem_addr(blo);
+#pragma unroll
+      for (int s = 0; s < kKC / 16; ++s) {
+        const uint32_t ko = static_cast<uint32_t>(s) * 256;  // two core matrices per K-step of 16
+        const uint32_t acc0 = (c > 0 || s > 0) ? 1u : 0u;
+        umma_bf16(tmem, umma_desc(ah + ko, kLBO, kSBO), umma_desc(bh + ko, kLBO, kSBO), idesc, acc0);
+        umma_bf16(tmem, umma_desc(ah + ko, kLBO, kSBO), umma_desc(bl + ko, kLBO, kSBO), idesc, 1u);
+        umma_bf16(tmem, umma_desc(al + ko, kLBO, kSBO), umma_desc(bh + ko, kLBO, kSBO), idesc, 1u);
+      }
+      umma_commit(&mbar[st]);
+    }
+    issued = c + 1;
+  }
+
+  // Drain: wait for the most recent commit of each stage (the ones not waited
+  // in the loop); together they cover every MMA issued.
+  bool ok = !s_fail;
+  for (int c = max(0, issued - 2); c < issued; ++c)
+    if (!mbar_wait(&mbar[c & 1], static_cast<unsigned>(c >> 1) & 1u)) ok = false;
+  __syncthreads();
+  if (!ok && tid == 0) atomicOr(a.status, kStatusLoopLimit);
+  tc_fence_after();
+
+  // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (tile rows), the two
+  // warp groups split the column blocks of 16.
+  const int warp = tid >> 5, lane = tid & 31;
+  const int quarter = warp & 3, half = warp >> 2;
+  const int m = quarter * 32 + lane;
+  const int u = u0 + m;
+  const int ncb = BN / 16, mid = (ncb + 1) / 2;
+  double* out = a.gpart + static_cast<size_t>(blockIdx.z) * a.Mu * a.Nv;
+  for (int cb = half ? mid : 0; cb < (half ? ncb : mid); ++cb) {
+    uint32_t r[16];
+    if (issued > 0 && ok) {
+      tmem_ld16(tmem + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(cb * 16), r);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) r[j] = 0u;
+    }
+    if (u < a.Mu) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int v = v0 + cb * 16 + j;
+        if (v < a.Nv) out[static_cast<size_t>(u) * a.Nv + v] = static_cast<double>(__uint_as_float(r[j]));
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.tmem_cols) : "memory");
+  }
+}
+
+}  // namespace
+
+size_t normal_tc_smem(int nc, int k, int BN) {
+  const size_t a_bytes = static_cast<size_t>(kBM) * kKC * 2, b_bytes = static_cast<size_t>(BN) * kKC * 2;
+  size_t s = 4 * a_bytes + 4 * b_bytes;
+  s += sizeof(float) * (static_cast<size_t>(kKC) * (nc + 1) + static_cast<size_t>(kKC) * k + kKC);
+  s += sizeof(int2) * (kBM + BN + (BN & 1));
+  s = (s + 7) / 8 * 8 + 2 * sizeof(uint64_t) + 16;
+  return s;
+}
+
+// G partials of the mixed-precision path: gpart[z][u][v] for every split z.
+// Returns the number of splits.
+int launch_normal_tc(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, const uint8_t* accepted,
+                     const int2* upairs, int Mu, const int2* vpairs, int Nv, Slot gpart_slot, double** gpart_out) {
+  const int tiles_n = (Nv + 255) / 256;
+  int BN = (Nv + tiles_n - 1) / tiles_n;
+  BN = (BN + 15) / 16 * 16;
+  const int tiles_m = (Mu + kBM - 1) / kBM;
+  const int tmem_cols = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+  const size_t smem = normal_tc_smem(nc, k, BN);
+  if (smem > 227 * 1024) fail(DGPU_ERR_INVALID, "fit_kernel: mixed-precision tile does not fit in shared memory");
+  const int64_t chunks = (N + kKC - 1) / kKC;
+  const int64_t want = std::max<int64_t>(1, 148 / std::max(1, tiles_m * tiles_n));
+  int64_t rps = ((chunks + want - 1) / want) * kKC;
+  rps = std::max<int64_t>(rps, kKC);
+  const int nsplit = static_cast<int>(std::max<int64_t>(1, (N + rps - 1) / rps));
+  double* gpart = static_cast<double*>(c.slot(gpart_slot, sizeof(double) * static_cast<size_t>(nsplit) * Mu * Nv));
+  TcArgs a;
+  a.N = N;
+  a.nc = nc;
+  a.k = k;
+  a.SS = SS;
+  a.R = R;
+  a.accepted = accepted;
+  a.upairs = upairs;
+  a.Mu = Mu;
+  a.vpairs = vpairs;
+  a.Nv = Nv;
+  a.BN = BN;
+  a.tmem_cols = tmem_cols;
+  a.rows_per_split = rps;
+  a.gpart = gpart;
+  a.status = c.d_status;
+  DGPU_CUDA(cudaFuncSetAttribute(k_normal_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  k_normal_tc<<<dim3(tiles_m, tiles_n, nsplit), kThreads, smem, c.stream>>>(a);
+  DGPU_LAUNCH("k_normal_tc");
+  *gpart_out = gpart;
+  return nsplit;
+}
+
+}  // namespace dgpu
