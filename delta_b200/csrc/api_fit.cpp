@@ -184,7 +184,7 @@ struct Engine {
     Work w = work(nl);
     DGPU_CUDA(cudaMemcpyAsync(w.lam, grid.data(), sizeof(double) * nl, cudaMemcpyHostToDevice, c.stream));
     solve(w, nl, M, nullptr, rhs, nullptr);
-    launch_quad_err(c.stream, nl, P, w.theta, M, nullptr, rhs, nullptr, ywy, w.raw);
+    launch_quad_err(c, nl, P, w.theta, M, nullptr, rhs, nullptr, ywy, w.raw);
     launch_gcv_finish(c.stream, nl, w.raw, w.edf, w.ok, n, w.rss, w.gcv);
     GlsOut o;
     o.grid = grid;
@@ -206,7 +206,7 @@ struct Engine {
     double* th = w.theta + static_cast<size_t>(s) * P;
     if (prec == DGPU_PREC_MIXED) {
       refine(w, s, lam, mask, th);
-      launch_quad_err(c.stream, 1, P, th, M, nullptr, rhs, nullptr, ywy, w.raw + s);
+      launch_quad_err(c, 1, P, th, M, nullptr, rhs, nullptr, ywy, w.raw + s);
       launch_gcv_finish(c.stream, 1, w.raw + s, w.edf + s, w.ok + s, n, w.rss + s, w.gcv + s);
     }
     o.theta = down(c, th, P);
@@ -227,7 +227,7 @@ struct Engine {
     Work w = work(1);
     DGPU_CUDA(cudaMemcpyAsync(w.lam, &lam, sizeof(double), cudaMemcpyHostToDevice, c.stream));
     solve(w, 1, M, nullptr, rhs, nullptr);
-    launch_quad_err(c.stream, 1, P, w.theta, M, nullptr, rhs, nullptr, ywy, w.raw);
+    launch_quad_err(c, 1, P, w.theta, M, nullptr, rhs, nullptr, ywy, w.raw);
     launch_gcv_finish(c.stream, 1, w.raw, w.edf, w.ok, n, w.rss, w.gcv);
     GlsOut o;
     finish_single(w, 0, lam, M, rhs, ywy, n, mask, o);
@@ -319,7 +319,7 @@ struct Engine {
       DGPU_CUDA(cudaMemcpyAsync(w.lam, lam.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, c.stream));
       DGPU_CUDA(cudaMemcpyAsync(w.midx, mi.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, c.stream));
       solve(w, ns, Mt, w.midx, rt, w.midx);
-      launch_quad_err(c.stream, ns, P, w.theta, Mg, w.midx, rg, w.midx, yg, w.raw);
+      launch_quad_err(c, ns, P, w.theta, Mg, w.midx, rg, w.midx, yg, w.raw);
       const auto err = down(c, w.raw, ns);
       const auto ok = down(c, w.ok, ns);
       for (int ii = 0; ii < m; ++ii) {
@@ -378,7 +378,7 @@ struct Engine {
     Work w1 = work(1);
     DGPU_CUDA(cudaMemcpyAsync(w1.lam, &grid[best], sizeof(double), cudaMemcpyHostToDevice, c.stream));
     solve(w1, 1, Mall, nullptr, rall, nullptr);
-    launch_quad_err(c.stream, 1, P, w1.theta, Mall, nullptr, rall, nullptr, yall, w1.raw);
+    launch_quad_err(c, 1, P, w1.theta, Mall, nullptr, rall, nullptr, yall, w1.raw);
     launch_gcv_finish(c.stream, 1, w1.raw, w1.edf, w1.ok, nall, w1.rss, w1.gcv);
     GlsOut o;
     finish_single(w1, 0, grid[best], Mall, rall, yall, nall, mask, o);

@@ -5,7 +5,7 @@
 
 namespace dgpu {
 
-void launch_quad_err(cudaStream_t st, int nsys, int P, const double* theta, const double* M, const int* m_index,
+void launch_quad_err(Context& c, int nsys, int P, const double* theta, const double* M, const int* m_index,
                      const double* r, const int* r_index, const double* y, double* out);
 void launch_gcv_finish(cudaStream_t st, int nsys, const double* raw, const double* edf, const int* ok,
                        const long long* n, double* rss, double* gcv);

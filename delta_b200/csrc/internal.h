@@ -56,6 +56,7 @@ enum Slot : int {
   kSlotFit0, kSlotFit1, kSlotFit2, kSlotFit3, kSlotFit4, kSlotFit5, kSlotFit6, kSlotFit7,
   kSlotFit8, kSlotFit9, kSlotFit10, kSlotFit11, kSlotFit12, kSlotFit13, kSlotFit14, kSlotFit15,
   kSlotFft0, kSlotFft1, kSlotFft2, kSlotFft3, kSlotFft4, kSlotFft5,
+  kSlotGlsPart,
   kSlotCount
 };
 

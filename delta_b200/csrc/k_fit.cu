@@ -349,7 +349,41 @@ void launch_normal_equations(Context& c, int prec, int64_t N, int nc, int k, int
 // e_i = t_i - x_i . theta (FP64 refinement residual), plus ywy = sum w t^2
 // and the active-row count. One CTA per row chunk, rows staged in shared memory.
 // ---------------------------------------------------------------------------
-constexpr int kRhsRows = 32;
+constexpr int kRhsRows = 128;
+
+// model_i = sum_c b_c (d_i . theta_c) in field order (background b = 1 last),
+// with theta in shared memory and the design row in registers.
+template <int KMAX>
+__device__ __forceinline__ double row_model(const double* __restrict__ d_row, const double* __restrict__ b_row,
+                                            int nc, int k, const double* __restrict__ th) {
+  double dr[KMAX];
+#pragma unroll
+  for (int m = 0; m < KMAX; ++m) dr[m] = m < k ? d_row[m] : 0.0;
+  double model = 0.0;
+  for (int c2 = 0; c2 <= nc; ++c2) {
+    const double* tc = th + c2 * k;
+    double f = 0.0;
+#pragma unroll
+    for (int m = 0; m < KMAX; ++m)
+      if (m < k) f = fma(dr[m], tc[m], f);
+    const double b = c2 < nc ? b_row[c2] : 1.0;
+    model = fma(f, b, model);
+  }
+  return model;
+}
+
+__device__ __forceinline__ double row_model_any(const double* d_row, const double* b_row, int nc, int k,
+                                                const double* th) {
+  if (k <= 16) return row_model<16>(d_row, b_row, nc, k, th);
+  if (k <= 32) return row_model<32>(d_row, b_row, nc, k, th);
+  double model = 0.0;
+  for (int c2 = 0; c2 <= nc; ++c2) {
+    double f = 0.0;
+    for (int m = 0; m < k; ++m) f = fma(d_row[m], th[c2 * k + m], f);
+    model = fma(f, c2 < nc ? b_row[c2] : 1.0, model);
+  }
+  return model;
+}
 
 __global__ void __launch_bounds__(256)
 k_rhs(int64_t N, int nc, int k, int SS, FitRows R, const uint8_t* __restrict__ accepted,
@@ -361,38 +395,17 @@ k_rhs(int64_t N, int nc, int k, int SS, FitRows R, const uint8_t* __restrict__ a
   double* sd = sb + kRhsRows * nf;        // kRhsRows x k
   double* se = sd + kRhsRows * k;         // kRhsRows : w * e
   double* sy = se + kRhsRows;             // kRhsRows : w * t * t
-  int* sa = reinterpret_cast<int*>(sy + kRhsRows);  // active flags
+  double* sth = sy + kRhsRows;            // P (theta, when given)
+  int* sa = reinterpret_cast<int*>(sth + P);  // active flags
   const int64_t rbeg = static_cast<int64_t>(blockIdx.x) * rows_per_split;
   const int64_t rend = min(N, rbeg + rows_per_split);
   const int tid = threadIdx.x;
+  if (theta)
+    for (int p = tid; p < P; p += blockDim.x) sth[p] = theta[p];
   double acc[4] = {0.0, 0.0, 0.0, 0.0};  // p = tid + 256*j
   double yacc = 0.0;
   long long nacc = 0;
   for (int64_t r0 = rbeg; r0 < rend; r0 += kRhsRows) {
-    for (int e = tid; e < kRhsRows; e += blockDim.x) {
-      const int64_t row = r0 + e;
-      const bool act = row < rend && R.valid[row] && accepted[row / SS];
-      sa[e] = act ? 1 : 0;
-      double we = 0.0, wtt = 0.0;
-      if (act) {
-        double t = R.t[row];
-        const double wv = R.w[row];
-        wtt = wv * t * t;
-        if (theta) {
-          double model = 0.0;
-          for (int c2 = 0; c2 < nf; ++c2) {
-            double f = 0.0;
-            for (int m = 0; m < k; ++m) f = fma(R.d[row * k + m], theta[c2 * k + m], f);
-            const double b = c2 < nc ? R.bn[row * nc + c2] : 1.0;
-            model = fma(f, b, model);
-          }
-          t = t - model;
-        }
-        we = wv * t;
-      }
-      se[e] = we;
-      sy[e] = wtt;
-    }
     for (int e = tid; e < kRhsRows * nf; e += blockDim.x) {
       const int rr = e / nf, c2 = e - rr * nf;
       const int64_t row = r0 + rr;
@@ -404,6 +417,22 @@ k_rhs(int64_t N, int nc, int k, int SS, FitRows R, const uint8_t* __restrict__ a
       const int rr = e / k, m = e - rr * k;
       const int64_t row = r0 + rr;
       sd[e] = row < rend ? R.d[row * k + m] : 0.0;
+    }
+    __syncthreads();
+    for (int e = tid; e < kRhsRows; e += blockDim.x) {
+      const int64_t row = r0 + e;
+      const bool act = row < rend && R.valid[row] && accepted[row / SS];
+      sa[e] = act ? 1 : 0;
+      double we = 0.0, wtt = 0.0;
+      if (act) {
+        double t = R.t[row];
+        const double wv = R.w[row];
+        wtt = wv * t * t;
+        if (theta) t = t - row_model_any(sd + e * k, sb + e * nf, nc, k, sth);
+        we = wv * t;
+      }
+      se[e] = we;
+      sy[e] = wtt;
     }
     __syncthreads();
     for (int j = 0; j < 4; ++j) {
@@ -431,13 +460,23 @@ k_rhs(int64_t N, int nc, int k, int SS, FitRows R, const uint8_t* __restrict__ a
   }
 }
 
-__global__ void k_reduce_rhs(int nsplit, int P, const double* __restrict__ rpart, const double* __restrict__ ypart,
-                             const long long* __restrict__ npart, double* __restrict__ rhs, double* ywy,
-                             long long* n) {
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
-    double s = 0.0;
-    for (int z = 0; z < nsplit; ++z) s += rpart[static_cast<size_t>(z) * P + p];
-    rhs[p] = s;
+__global__ void __launch_bounds__(256)
+k_reduce_rhs(int nsplit, int P, const double* __restrict__ rpart, const double* __restrict__ ypart,
+             const long long* __restrict__ npart, double* __restrict__ rhs, double* ywy, long long* n) {
+  // Block: 32 consecutive unknowns (lanes) x 8 warps striding the splits; the
+  // warps' partials are then added in warp order (fixed order).
+  __shared__ double red[8][33];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int p = blockIdx.x * 32 + lane;
+  double s = 0.0;
+  if (p < P)
+    for (int z = warp; z < nsplit; z += 8) s += rpart[static_cast<size_t>(z) * P + p];
+  red[warp][lane] = s;
+  __syncthreads();
+  if (warp == 0 && p < P) {
+    double t = 0.0;
+    for (int q = 0; q < 8; ++q) t += red[q][lane];
+    rhs[p] = t;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     double y = 0.0;
@@ -456,17 +495,19 @@ void launch_rhs(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, 
   cudaStream_t st = c.stream;
   const int P = (nc + 1) * k;
   if (P > 1024) fail(DGPU_ERR_INVALID, "fit: more than 1024 unknowns is not supported");
-  int64_t rps = std::max<int64_t>(kRhsRows * 16, (N + 148 * 2 - 1) / (148 * 2));
+  int64_t rps = std::max<int64_t>(kRhsRows * 2, (N + 148 * 2 - 1) / (148 * 2));
   rps = (rps + kRhsRows - 1) / kRhsRows * kRhsRows;
   const int nsplit = static_cast<int>(std::max<int64_t>(1, (N + rps - 1) / rps));
   char* buf = static_cast<char*>(c.slot(kSlotFit13, (sizeof(double) * (P + 1) + sizeof(long long)) * nsplit + 64));
   double* rpart = reinterpret_cast<double*>(buf);
   double* ypart = rpart + static_cast<size_t>(nsplit) * P;
   long long* npart = reinterpret_cast<long long*>(ypart + nsplit);
-  const size_t smem = sizeof(double) * (kRhsRows * (nc + 1) + kRhsRows * k + 2 * kRhsRows) + sizeof(int) * kRhsRows;
+  const size_t smem =
+      sizeof(double) * (kRhsRows * (nc + 1) + kRhsRows * k + 2 * kRhsRows + P) + sizeof(int) * kRhsRows;
+  DGPU_CUDA(cudaFuncSetAttribute(k_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   k_rhs<<<nsplit, 256, smem, st>>>(N, nc, k, SS, R, accepted, theta, rps, rpart, ypart, npart);
   DGPU_LAUNCH("k_rhs");
-  k_reduce_rhs<<<(P + 255) / 256, 256, 0, st>>>(nsplit, P, rpart, ypart, npart, rhs, ywy, n);
+  k_reduce_rhs<<<(P + 31) / 32, 256, 0, st>>>(nsplit, P, rpart, ypart, npart, rhs, ywy, n);
   DGPU_LAUNCH("k_reduce_rhs");
 }
 
@@ -477,23 +518,20 @@ void launch_rhs(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, 
 __global__ void __launch_bounds__(256)
 k_stamp_chi2(int nc, int k, int SS, FitRows R, const uint8_t* __restrict__ accepted,
              const double* __restrict__ theta, double* __restrict__ chi2, int* __restrict__ cnt) {
+  extern __shared__ double cth[];  // theta, (nc + 1) * k
   __shared__ double ssum[256];
   __shared__ int scnt[256];
   const int s = blockIdx.x;
-  const int nf = nc + 1;
+  const int P = (nc + 1) * k;
   double acc = 0.0;
   int n = 0;
   if (accepted[s]) {
+    for (int p = threadIdx.x; p < P; p += blockDim.x) cth[p] = theta[p];
+    __syncthreads();
     for (int i = threadIdx.x; i < SS; i += blockDim.x) {
       const size_t row = static_cast<size_t>(s) * SS + i;
       if (!R.valid[row]) continue;
-      double model = 0.0;
-      for (int c2 = 0; c2 < nf; ++c2) {
-        double f = 0.0;
-        for (int m = 0; m < k; ++m) f = fma(R.d[row * k + m], theta[c2 * k + m], f);
-        const double b = c2 < nc ? R.bn[row * nc + c2] : 1.0;
-        model = fma(f, b, model);
-      }
+      const double model = row_model_any(R.d + row * k, R.bn + row * nc, nc, k, cth);
       const double res = R.t[row] - model;
       acc += R.w[row] * res * res;
       ++n;
@@ -518,7 +556,7 @@ k_stamp_chi2(int nc, int k, int SS, FitRows R, const uint8_t* __restrict__ accep
 void launch_stamp_chi2(cudaStream_t st, int n_stamps, int nc, int k, int SS, const FitRows& R,
                        const uint8_t* accepted, const double* theta, double* chi2, int* cnt) {
   if (n_stamps == 0) return;
-  k_stamp_chi2<<<n_stamps, 256, 0, st>>>(nc, k, SS, R, accepted, theta, chi2, cnt);
+  k_stamp_chi2<<<n_stamps, 256, sizeof(double) * (nc + 1) * k, st>>>(nc, k, SS, R, accepted, theta, chi2, cnt);
   DGPU_LAUNCH("k_stamp_chi2");
 }
 
@@ -538,7 +576,10 @@ k_reweight(StampGeom g, TpsDev t, const int* __restrict__ stamp_x, const int* __
   if (!accepted[s] || cnt[s] == 0) return;
   const int ks = g.ks, kk = ks * ks, r = g.r;
   const int nc = g.nc;
-  float* k2 = wsm;                      // kk
+  float* k2 = wsm;               // kk
+  float* win = wsm + kk;         // (S + 2r)^2 reference-variance window, invalid samples = 0
+  const int side = g.S + 2 * r;
+  const int wx0 = stamp_x[s] - g.sr - r, wy0 = stamp_y[s] - g.sr - r;
   __shared__ float an[64];
   __shared__ double dsh[64];
   if (g.have_cvar) {
@@ -549,6 +590,18 @@ k_reweight(StampGeom g, TpsDev t, const int* __restrict__ stamp_x, const int* __
         for (int m = 0; m < t.k; ++m) f = fma(dsh[m], theta[n * t.k + m], f);
         an[n] = static_cast<float>(f);
       }
+    }
+    // Off-frame, masked, non-positive and non-finite samples contribute nothing
+    // (src/fit.cpp:38-59 skips them): store 0, which leaves the FP64 sum unchanged.
+    for (int i = threadIdx.x; i < side * side; i += blockDim.x) {
+      const int yy = wy0 + i / side, xx = wx0 + i % side;
+      float v = 0.0f;
+      if (yy >= 0 && yy < g.h && xx >= 0 && xx < g.w) {
+        const size_t idx = static_cast<size_t>(yy) * g.w + xx;
+        const float x = vr[idx];
+        if (!(rm && rm[idx] != 0) && x > 0.0f && isfinite(x)) v = x;
+      }
+      win[i] = v;
     }
     __syncthreads();
     for (int i = threadIdx.x; i < kk; i += blockDim.x) {
@@ -562,21 +615,13 @@ k_reweight(StampGeom g, TpsDev t, const int* __restrict__ stamp_x, const int* __
     const size_t row = static_cast<size_t>(s) * g.SS + i;
     if (!R.valid[row]) continue;
     if (g.have_cvar) {
-      const int x = R.px[row], y = R.py[row];
+      // window coordinates of (x - du, y - dv): row y - wy0 - dv, column x - wx0 - du
+      const int lx = R.px[row] - wx0, ly = R.py[row] - wy0;
       double acc = 0.0;
       for (int dv = -r; dv <= r; ++dv) {
-        const int sy = y - dv;
-        if (sy < 0 || sy >= g.h) continue;
         const float* krow = k2 + (dv + r) * ks;
-        for (int du = -r; du <= r; ++du) {
-          const int sx = x - du;
-          if (sx < 0 || sx >= g.w) continue;
-          const size_t idx = static_cast<size_t>(sy) * g.w + sx;
-          if (rm && rm[idx] != 0) continue;
-          const float v = vr[idx];
-          if (!(v > 0.0f) || !isfinite(v)) continue;
-          acc = fma(static_cast<double>(krow[du + r]), static_cast<double>(v), acc);
-        }
+        const float* wrow = win + (ly - dv) * side + lx;
+        for (int du = -r; du <= r; ++du) acc = fma(static_cast<double>(krow[du + r]), static_cast<double>(wrow[-du]), acc);
       }
       const double rv = R.vt[row] + acc;
       if (rv > 0.0) R.w[row] = 1.0 / rv;
@@ -590,7 +635,9 @@ void launch_reweight(cudaStream_t st, const StampGeom& g, int n_stamps, const Tp
                      const int* sy, const FitRows& R, const uint8_t* accepted, const int* cnt,
                      const double* theta, const float* phi, const float* vr, const uint8_t* rm) {
   if (n_stamps == 0) return;
-  const size_t smem = sizeof(float) * static_cast<size_t>(g.ks) * g.ks;
+  const size_t side = static_cast<size_t>(g.S) + 2 * g.r;
+  const size_t smem = sizeof(float) * (static_cast<size_t>(g.ks) * g.ks + side * side);
+  if (smem > 200 * 1024) fail(DGPU_ERR_INVALID, "fit_kernel: stamp plus kernel footprint too large for the reweight");
   DGPU_CUDA(cudaFuncSetAttribute(k_reweight, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   k_reweight<<<n_stamps, 256, smem, st>>>(g, t, sx, sy, R, accepted, cnt, theta, phi, vr, rm);
   DGPU_LAUNCH("k_reweight");

@@ -29,34 +29,62 @@ __device__ double block_sum(double v, double* red) {
 }
 
 // theta^T Mq theta - 2 theta . rq + yq for system s (M/r/y chosen by index).
+// Grid (row blocks of kQRows, systems): each CTA forms the partial sums of its
+// rows (one warp per row of M, coalesced); k_quad_finish adds the row blocks
+// of each system in a fixed order.
+constexpr int kQRows = 32;
+
 __global__ void __launch_bounds__(256)
 k_quad_err(int P, const double* __restrict__ theta, const double* __restrict__ M, const int* __restrict__ m_index,
-           const double* __restrict__ r, const int* __restrict__ r_index, const double* __restrict__ y,
-           double* __restrict__ out) {
+           const double* __restrict__ r, const int* __restrict__ r_index, double* __restrict__ part) {
   __shared__ double red[256];
-  const int s = blockIdx.x;
-  const double* th = theta + static_cast<size_t>(s) * P;
+  __shared__ double th[1024];
+  const int b = blockIdx.x, s = blockIdx.y, nb = gridDim.x;
   const double* Mq = M + (m_index ? static_cast<size_t>(m_index[s]) * P * P : 0);
   const double* rq = r + (r_index ? static_cast<size_t>(r_index[s]) * P : 0);
-  const double yq = y[r_index ? r_index[s] : 0];
+  for (int p = threadIdx.x; p < P; p += blockDim.x) th[p] = theta[static_cast<size_t>(s) * P + p];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int p0 = b * kQRows, p1 = min(P, p0 + kQRows);
   double quad = 0.0, lin = 0.0;
-  for (int p = threadIdx.x; p < P; p += blockDim.x) {
-    double a = 0.0;
+  for (int p = p0 + warp; p < p1; p += nw) {
     const double* row = Mq + static_cast<size_t>(p) * P;
-    for (int q = 0; q < P; ++q) a = fma(row[q], th[q], a);
-    quad = fma(th[p], a, quad);
-    lin = fma(th[p], rq[p], lin);
+    double a = 0.0;
+    for (int q = lane; q < P; q += 32) a = fma(row[q], th[q], a);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    if (lane == 0) quad = fma(th[p], a, quad);
   }
+  for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) lin = fma(th[p], rq[p], lin);
   const double Q = block_sum(quad, red);
   const double L = block_sum(lin, red);
-  if (threadIdx.x == 0) out[s] = yq - 2.0 * L + Q;
+  if (threadIdx.x == 0) {
+    part[(static_cast<size_t>(s) * nb + b) * 2] = Q;
+    part[(static_cast<size_t>(s) * nb + b) * 2 + 1] = L;
+  }
 }
 
-void launch_quad_err(cudaStream_t st, int nsys, int P, const double* theta, const double* M, const int* m_index,
+__global__ void k_quad_finish(int nsys, int nb, const double* __restrict__ part, const double* __restrict__ y,
+                              const int* __restrict__ r_index, double* __restrict__ out) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nsys; s += gridDim.x * blockDim.x) {
+    double Q = 0.0, L = 0.0;
+    for (int b = 0; b < nb; ++b) {
+      Q += part[(static_cast<size_t>(s) * nb + b) * 2];
+      L += part[(static_cast<size_t>(s) * nb + b) * 2 + 1];
+    }
+    out[s] = y[r_index ? r_index[s] : 0] - 2.0 * L + Q;
+  }
+}
+
+void launch_quad_err(Context& c, int nsys, int P, const double* theta, const double* M, const int* m_index,
                      const double* r, const int* r_index, const double* y, double* out) {
   if (nsys == 0) return;
-  k_quad_err<<<nsys, 256, 0, st>>>(P, theta, M, m_index, r, r_index, y, out);
+  const int nb = (P + kQRows - 1) / kQRows;
+  double* part = static_cast<double*>(c.slot(kSlotGlsPart, sizeof(double) * 2 * static_cast<size_t>(nb) * nsys));
+  k_quad_err<<<dim3(nb, nsys), 256, 0, c.stream>>>(P, theta, M, m_index, r, r_index, part);
   DGPU_LAUNCH("k_quad_err");
+  k_quad_finish<<<(nsys + 127) / 128, 128, 0, c.stream>>>(nsys, nb, part, y, r_index, out);
+  DGPU_LAUNCH("k_quad_finish");
 }
 
 __global__ void k_gcv_finish(int nsys, const double* __restrict__ raw, const double* __restrict__ edf,

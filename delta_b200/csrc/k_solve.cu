@@ -332,10 +332,18 @@ void launch_solve_batch(Context& c, const SolveBatch& b) {
   DGPU_LAUNCH("k_solve_cluster");
 }
 
-// out = A_s^{-1} v = Linv_s^T (Linv_s v), single CTA.
-__global__ void k_apply_inverse(const double* __restrict__ Li, int P, int Pp, const double* __restrict__ v,
-                                double* __restrict__ out) {
-  __shared__ double y[1024];
+// out = A_s^{-1} v = Linv_s^T (Linv_s v), single CTA: y by warp-per-row dot
+// products; then every warp adds y_p Linv[p][:] over its rows p into its own
+// shared-memory accumulator (lanes over columns, coalesced), and the warps'
+// accumulators are summed in warp order.
+constexpr int kAiThreads = 512;
+
+__global__ void __launch_bounds__(kAiThreads) k_apply_inverse(const double* __restrict__ Li, int P, int Pp,
+                                                               const double* __restrict__ v,
+                                                               double* __restrict__ out) {
+  extern __shared__ double aism[];
+  double* y = aism;              // P
+  double* accw = aism + P;       // nw x P
   const int warp = threadIdx.x / 32, ln = threadIdx.x % 32, nw = blockDim.x / 32;
   for (int p = warp; p < P; p += nw) {
     const double* row = Li + static_cast<size_t>(p) * Pp;
@@ -345,17 +353,27 @@ __global__ void k_apply_inverse(const double* __restrict__ Li, int P, int Pp, co
     for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
     if (ln == 0) y[p] = a;
   }
+  for (int i = threadIdx.x; i < nw * P; i += blockDim.x) accw[i] = 0.0;
+  __syncthreads();
+  double* mine = accw + static_cast<size_t>(warp) * P;
+  for (int p = warp; p < P; p += nw) {
+    const double* row = Li + static_cast<size_t>(p) * Pp;
+    const double yp = y[p];
+    for (int q = ln; q <= p; q += 32) mine[q] = fma(row[q], yp, mine[q]);
+  }
   __syncthreads();
   for (int q = threadIdx.x; q < P; q += blockDim.x) {
     double a = 0.0;
-    for (int p = q; p < P; ++p) a = fma(Li[static_cast<size_t>(p) * Pp + q], y[p], a);
+    for (int w2 = 0; w2 < nw; ++w2) a += accw[static_cast<size_t>(w2) * P + q];
     out[q] = a;
   }
 }
 
 void launch_apply_inverse(cudaStream_t st, const SolveBatch& b, int s, const double* v, double* out) {
   const int Pp = solve_pp(b.P);
-  k_apply_inverse<<<1, 512, 0, st>>>(b.Linv + static_cast<size_t>(s) * Pp * Pp, b.P, Pp, v, out);
+  const size_t smem = sizeof(double) * static_cast<size_t>(b.P) * (1 + kAiThreads / 32);
+  DGPU_CUDA(cudaFuncSetAttribute(k_apply_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  k_apply_inverse<<<1, kAiThreads, smem, st>>>(b.Linv + static_cast<size_t>(s) * Pp * Pp, b.P, Pp, v, out);
   DGPU_LAUNCH("k_apply_inverse");
 }
 

@@ -93,8 +93,10 @@ void launch_exact_fields(cudaStream_t s, const TpsDev& t, const double* theta, i
 // the tile rows plus the y halo (each thread: 4 columns x all nx, sliding a
 // 4-wide register window so every staged value is loaded once per tap); the
 // y-pass of every component then runs out of shared memory with each thread
-// holding 8 output rows of one column in registers (again a sliding window),
-// and a_n / b are blended from the coarse lattice in registers. Per output
+// holding 8 output rows of one column in registers (taps in blocks of 8, the
+// 15 rows a block touches in registers), and a_n / b are blended from the
+// coarse lattice in registers, the corners re-read only when the coarse cell
+// row changes. Per output
 // pixel the accumulation order is the reference's: x taps j = 0..ks-1, then
 // components in basis order, each y tap j ascending, d -= a_n * bn (FMA).
 // Off-frame rows of the x-pass buffer are exact zeros, which leaves every
@@ -212,41 +214,69 @@ k_model_convolve(int w, int h, const float* __restrict__ sci, const float* __res
       fy[i] = 0.0f;
     }
   }
-  auto field = [&](int f, int i) -> float {
-    const int y = min(by + ly0 + i, h - 1);
-    if (F.exact) return __ldg(F.full + (static_cast<size_t>(f) * h + y) * w + xc);
-    const float* c0 = F.latf + (static_cast<size_t>(f) * F.ncy + jy[i]) * F.ncx + jx;
-    const float* c1 = c0 + F.ncx;
-    return cell_blend(__ldg(c0), __ldg(c0 + 1), __ldg(c1), __ldg(c1 + 1), fy[i], wxv);
+  // Field values a_f(x, y_i) of this thread's 8 rows: the four lattice corners
+  // are re-read only when the coarse cell row changes (rows of a warp share
+  // them, so the branch is warp-uniform).
+  auto fields_of = [&](int f, float (&a)[kMcRPT]) {
+    if (F.exact) {
+#pragma unroll
+      for (int i = 0; i < kMcRPT; ++i) {
+        const int y = min(by + ly0 + i, h - 1);
+        a[i] = __ldg(F.full + (static_cast<size_t>(f) * h + y) * w + xc);
+      }
+      return;
+    }
+    int cj = -1;
+    float a00 = 0.0f, a01 = 0.0f, a10 = 0.0f, a11 = 0.0f;
+#pragma unroll
+    for (int i = 0; i < kMcRPT; ++i) {
+      if (jy[i] != cj) {
+        cj = jy[i];
+        const float* c0 = F.latf + (static_cast<size_t>(f) * F.ncy + cj) * F.ncx + jx;
+        const float* c1 = c0 + F.ncx;
+        a00 = __ldg(c0);
+        a01 = __ldg(c0 + 1);
+        a10 = __ldg(c1);
+        a11 = __ldg(c1 + 1);
+      }
+      a[i] = cell_blend(a00, a01, a10, a11, fy[i], wxv);
+    }
   };
   if (!STACK) {
+    float bg[kMcRPT];
+    fields_of(nc, bg);
 #pragma unroll
     for (int i = 0; i < kMcRPT; ++i) {
       const int y = min(by + ly0 + i, h - 1);
-      d[i] = __ldg(sci + static_cast<size_t>(y) * w + xc) - field(nc, i);
+      d[i] = __ldg(sci + static_cast<size_t>(y) * w + xc) - bg[i];
     }
   }
   for (int n = 0; n < nc; ++n) {
     const int2 o = orders[n];
     const float* col = txs + static_cast<size_t>(o.x) * nrows * kMcTW + lx;
     const float* ky = ktaps + o.y * ks;
-    // output row ly0+i needs buffer row ly0 + i + 2kh - j.
+    // Output row ly0+i needs buffer row ly0 + i + 2kh - j. Taps go in blocks of
+    // 8 with the rows of a block held in registers (static indices), each
+    // output still summing its taps j = 0..ks-1 in order.
     const int base = ly0 + 2 * kh;
-    float win[kMcRPT];
-#pragma unroll
-    for (int i = 0; i < kMcRPT; ++i) win[i] = col[(base + i) * kMcTW];
     float bn[kMcRPT];
 #pragma unroll
     for (int i = 0; i < kMcRPT; ++i) bn[i] = 0.0f;
-    for (int j = 0; j < ks; ++j) {
-      if (j > 0) {
+    for (int j0 = 0; j0 < ks; j0 += 8) {
+      float v[kMcRPT + 7];  // v[t] = buffer row base - j0 - 7 + t
 #pragma unroll
-        for (int i = kMcRPT - 1; i > 0; --i) win[i] = win[i - 1];
-        win[0] = col[(base - j) * kMcTW];
+      for (int t = 0; t < kMcRPT + 7; ++t) {
+        const int rr = base - j0 - 7 + t;
+        v[t] = rr >= 0 ? col[rr * kMcTW] : 0.0f;
       }
-      const float c = ky[j];
 #pragma unroll
-      for (int i = 0; i < kMcRPT; ++i) bn[i] = __fmaf_rn(c, win[i], bn[i]);
+      for (int jj = 0; jj < 8; ++jj) {
+        if (j0 + jj < ks) {
+          const float c = ky[j0 + jj];
+#pragma unroll
+          for (int i = 0; i < kMcRPT; ++i) bn[i] = __fmaf_rn(c, v[i - jj + 7], bn[i]);
+        }
+      }
     }
     if (STACK) {
       if (xin) {
@@ -258,8 +288,10 @@ k_model_convolve(int w, int h, const float* __restrict__ sci, const float* __res
       }
       continue;
     }
+    float a[kMcRPT];
+    fields_of(n, a);
 #pragma unroll
-    for (int i = 0; i < kMcRPT; ++i) d[i] = __fmaf_rn(-field(n, i), bn[i], d[i]);
+    for (int i = 0; i < kMcRPT; ++i) d[i] = __fmaf_rn(-a[i], bn[i], d[i]);
   }
   if (STACK) return;
   if (xin) {
