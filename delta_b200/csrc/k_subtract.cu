@@ -87,7 +87,7 @@ void launch_exact_fields(cudaStream_t s, const TpsDev& t, const double* theta, i
 // ---------------------------------------------------------------------------
 // Fused model convolve (src/subtract.cpp:466-639).
 //
-// One CTA per 64 x TH output tile. The sanitised reference window (tile + kh
+// One CTA per 32 x TH output tile. The sanitised reference window (tile + kh
 // halo, masked / non-finite -> fill, off-frame -> 0) is staged in shared
 // memory; the NX = n_max+1 shared x-passes are computed into shared memory for
 // the tile rows plus the y halo (each thread: 4 columns x all nx, sliding a
@@ -103,7 +103,7 @@ void launch_exact_fields(cudaStream_t s, const TpsDev& t, const double* theta, i
 // clipped y sum bit-identical to the reference's jmin/jmax loop.
 // ---------------------------------------------------------------------------
 
-constexpr int kMcTW = 64;   // tile width (columns)
+constexpr int kMcTW = 32;   // tile width (columns)
 constexpr int kMcRPT = 8;   // output rows per thread in the y pass
 constexpr int kMcXPT = 4;   // output columns per thread in the x pass
 
@@ -125,7 +125,7 @@ k_model_convolve(int w, int h, const float* __restrict__ sci, const float* __res
   const int gbw = kMcTW + 2 * kh;
   const int gbw_pad = (gbw + 3) & ~3;
   float* rtile = smem;                                       // nrows x gbw_pad
-  float* txs = rtile + nrows * gbw_pad;                      // NX x nrows x 64
+  float* txs = rtile + nrows * gbw_pad;                      // NX x nrows x kMcTW
   float* ktaps = txs + NX * nrows * kMcTW;                   // NX x ks
   const int bx = blockIdx.x * kMcTW, by = blockIdx.y * TH;
   const float fill = STACK ? 0.0f : *fillp;
@@ -324,9 +324,15 @@ size_t model_convolve_smem(int nx, int ks, int TH) {
 
 void launch_model_convolve_orders(cudaStream_t s, const SubtractArgs& a, const int2* orders, bool stack) {
   const int nx = a.n_max + 1;
-  int TH = 32;
-  const size_t kMaxSmem = 200 * 1024;
-  while (TH > 8 && model_convolve_smem(nx, a.ks, TH) > kMaxSmem) TH /= 2;
+  // Tallest tile (least redundant x-pass halo) that still lets two CTAs share
+  // an SM; otherwise the tallest that fits at all.
+  const size_t kTwoPerSm = 112 * 1024, kMaxSmem = 200 * 1024;
+  int TH = 64;
+  while (TH > 8 && model_convolve_smem(nx, a.ks, TH) > kTwoPerSm) TH /= 2;
+  if (model_convolve_smem(nx, a.ks, TH) > kTwoPerSm) {
+    TH = 64;
+    while (TH > 8 && model_convolve_smem(nx, a.ks, TH) > kMaxSmem) TH /= 2;
+  }
   const size_t smem = model_convolve_smem(nx, a.ks, TH);
   if (smem > kMaxSmem) fail(DGPU_ERR_INVALID, "subtract: kernel footprint too large for the tile engine");
   switch (nx) {
