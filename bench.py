@@ -106,7 +106,7 @@ class ClockSampler:
     """Reads SM clock, max clock and clock-event reasons through NVML every
     `period` seconds on a thread (read-only queries)."""
 
-    def __init__(self, device_index: int, period: float = 0.1):
+    def __init__(self, device_index: int, period: float = 0.02):
         self.period = period
         self.samples: list[tuple[float, float, int]] = []
         self._stop = threading.Event()
