@@ -474,6 +474,18 @@ int dgpu_photometric_scale(dgpu_context* ctx, int mem, const double* knots, int 
   });
 }
 
+int dgpu_estimate_background_noalloc(const float* data, const uint8_t* mask, int64_t width, int64_t height,
+                                     void* stream, double* median, double* sigma) {
+  return guarded_free([&] {
+    check_dims(width, height);
+    if (!data || !median || !sigma) fail(DGPU_ERR_INVALID, "estimate_background_noalloc: missing argument");
+    float r[2] = {0.0f, 0.0f};
+    background_noalloc(width * height, data, mask, static_cast<cudaStream_t>(stream), r);
+    *median = static_cast<double>(r[0]);
+    *sigma = 1.4826 * static_cast<double>(r[1]);
+  });
+}
+
 int dgpu_negate(dgpu_context* ctx, int mem, float* data, int64_t n) {
   return guarded(ctx, [&](Context& c) {
     if (n < 0) fail(DGPU_ERR_INVALID, "negate: n must be >= 0");

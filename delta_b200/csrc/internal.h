@@ -211,6 +211,9 @@ void launch_mask_fill(cudaStream_t s, int64_t n, const uint8_t* mask, const uint
 void launch_model_convolve_orders(cudaStream_t s, const SubtractArgs& a, const int2* orders, bool stack);
 void launch_photometric_scale(cudaStream_t s, const DevFields& F, const float* sums, int nc, float* out);
 void launch_negate(cudaStream_t s, int64_t n, float* v);
+// Background median / MAD of a device image with a fixed file-scope scratch
+// (no allocation); out2 (host) = {median, MAD}. Synchronises `s`.
+void background_noalloc(int64_t n, const float* img, const uint8_t* mask, cudaStream_t s, float* out2);
 
 // Upper median (element size/2 of the sorted sample) of values[7j] that pass a
 // predicate, via radix select. Result written to a device float.

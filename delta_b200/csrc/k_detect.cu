@@ -13,6 +13,8 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
+#include <mutex>
+#include <string>
 
 #include "dev_common.cuh"
 #include "detect_internal.h"
@@ -620,6 +622,74 @@ void run_catalog_stamps(Context& c, int w, int h, const float* sci, const uint8_
   DGPU_CUDA(cudaMemcpyAsync(hb, bgr, sizeof(float) * 2, cudaMemcpyDeviceToHost, s));
   DGPU_CUDA(cudaStreamSynchronize(s));
   *med_ref = hb[0];
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free background estimate (dgpu_estimate_background_noalloc).
+//
+// Same algorithm and kernels as launch_background, with the sample keys and
+// the radix-select state in one fixed, file-scope device array instead of the
+// context's workspace. The sample has at most 2^19 entries for any frame below
+// 2^31 pixels (step = n / 2^18 gives ceil(n / step) < 2^19), so the array is
+// 2 MiB + 1 KiB per device. Each call clears the select state (its counter
+// must start at zero) on the caller's stream before use. The array is shared
+// by every call on a device: calls that overlap in time (other streams or
+// threads) race on it and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int64_t kNoAllocMaxSamples = int64_t(1) << 19;
+constexpr int kNoAllocMaxDevices = 64;
+
+struct NoAllocBackground {
+  Sel sel;          // count / rank / prefix / histogram: cleared by every call
+  float result[4];  // [0] median, [1] MAD
+  uint32_t keys[kNoAllocMaxSamples];
+};
+
+static __device__ __align__(256) NoAllocBackground g_noalloc_background;
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the array on the current device, resolved once per device.
+NoAllocBackground* noalloc_background_scratch() {
+  int dev = 0;
+  DGPU_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) fail(DGPU_ERR_INVALID, "estimate_background_noalloc: device index out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_background);
+    if (e != cudaSuccess)
+      fail(DGPU_ERR_CUDA, std::string("estimate_background_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = p;
+  }
+  return static_cast<NoAllocBackground*>(g_noalloc_ptr[dev]);
+}
+
+}  // namespace
+
+void background_noalloc(int64_t n, const float* img, const uint8_t* mask, cudaStream_t s, float* out2) {
+  constexpr int64_t kTarget = 1 << 18;
+  const int64_t step = n > kTarget ? n / kTarget : 1;
+  const int64_t ns = (n + step - 1) / step;
+  if (ns > kNoAllocMaxSamples)
+    fail(DGPU_ERR_INVALID, "estimate_background_noalloc: sample exceeds the fixed 2^19-entry scratch");
+  NoAllocBackground* sc = noalloc_background_scratch();
+  Sel* st = &sc->sel;
+  uint32_t* keys = sc->keys;
+  float* res = sc->result;
+  DGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(Sel), s));
+  const int blocks = static_cast<int>(std::min<int64_t>((ns + 255) / 256, 148 * 8));
+  k_sample_keys<<<std::max(blocks, 1), 256, 0, s>>>(n, step, img, mask, keys, st);
+  DGPU_LAUNCH("k_sample_keys");
+  select_median(s, st, keys, ns, res);
+  k_abs_dev<<<std::max(blocks, 1), 256, 0, s>>>(st, res, keys);
+  DGPU_LAUNCH("k_abs_dev");
+  select_median(s, st, keys, ns, res + 1);
+  DGPU_CUDA(cudaMemcpyAsync(out2, res, 2 * sizeof(float), cudaMemcpyDeviceToHost, s));
+  DGPU_CUDA(cudaStreamSynchronize(s));
 }
 
 }  // namespace dgpu

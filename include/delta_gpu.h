@@ -230,6 +230,24 @@ typedef struct {
   int match_radius;       /* 2 */
 } dgpu_detect_params;
 
+/* Allocation-free dgpu_estimate_background (no reference counterpart).
+ * For callers that must not allocate device memory during processing: for
+ * example a loop under a fixed memory budget, or code that cannot accept the
+ * device-wide synchronisation that cudaMalloc/cudaFree imply. It needs no
+ * context: it runs on the calling thread's current device, on `stream`
+ * (NULL = legacy default stream), with `data` (float32, width x height) and the
+ * optional `mask` (uint8) in device memory, and returns after synchronising
+ * `stream`. Its scratch is one fixed array of 2 MiB + 1 KiB per device inside
+ * the library (it holds the at most 2^19 sample keys of any frame below 2^31
+ * pixels); the select state in it is cleared at the start of every call.
+ * Limits: frames up to 2^31 - 1 pixels (larger -> DGPU_ERR_INVALID). The first
+ * call on a device resolves that array's address (cudaGetSymbolAddress); make
+ * that first call before any stream capture. Calls that overlap in time on the
+ * same device (other streams or threads) share the array and race: serialise
+ * them. Results equal dgpu_estimate_background's (median, 1.4826 * MAD).
+ * Errors: status code, text from dgpu_last_error(NULL). */
+int dgpu_estimate_background_noalloc(const float* data, const uint8_t* mask, int64_t width, int64_t height,
+                                     void* stream, double* median, double* sigma);
 /* estimate_background, src/bindings.cpp:232-237 -> src/detect.cpp:84-113. */
 int dgpu_estimate_background(dgpu_context* ctx, int mem, int64_t width, int64_t height, const float* data,
                              const uint8_t* mask, double* median, double* sigma);
