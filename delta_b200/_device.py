@@ -10,6 +10,8 @@ reference's own data flow.
 from __future__ import annotations
 
 import ctypes
+import threading
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 
 import numpy as np
@@ -331,3 +333,57 @@ def apply(sub, solution, target, conv, tvar, cvar, tmask, cmask, sign, stamp_x, 
             cat = build_catalog(score, whitened, mask, psf)
     return {"solution": solution, "difference": whitened, "variance": white_var if white_var is not None else var,
             "mask": mask, "score": score, "psf": psf, "catalog": cat, "variance_scale": variance_scale}
+
+
+# ---------------------------------------------------------------------------
+# Several frames in flight: one host thread, one library context and one CUDA
+# stream per frame, so the latency-bound phases of one frame (selection, the
+# per-lambda solves, single-CTA selects) overlap the bandwidth-bound phases of
+# another. Worker threads persist, so their contexts keep their workspace.
+# ---------------------------------------------------------------------------
+
+_runners: dict = {}
+_runners_lock = threading.Lock()
+_tls = threading.local()
+
+
+def _thread_stream():
+    s = getattr(_tls, "stream", None)
+    if s is None:
+        s = _tls.stream = torch.cuda.Stream()
+    return s
+
+
+def runner(n_workers: int) -> ThreadPoolExecutor:
+    """The persistent pool of `n_workers` frame workers (one per frame in flight)."""
+    n = max(1, int(n_workers))
+    with _runners_lock:
+        ex = _runners.get(n)
+        if ex is None:
+            ex = _runners[n] = ThreadPoolExecutor(max_workers=n, thread_name_prefix=f"delta-b200-frame{n}")
+        return ex
+
+
+def on_own_stream(fn, *args, **kwargs):
+    """Run fn on the calling worker's stream, after the work already queued on
+    the default stream (inputs uploaded there), and wait for it to finish."""
+    s = _thread_stream()
+    s.wait_stream(torch.cuda.default_stream())
+    with torch.cuda.stream(s):
+        out = fn(*args, **kwargs)
+    s.synchronize()
+    return out
+
+
+def run_batch(sub, frames, catalogs=None, directions=None, max_in_flight: int | None = None) -> list:
+    """run() over several device-resident frames with up to `max_in_flight`
+    frames processed concurrently; results in input order."""
+    frames = list(frames)
+    n = len(frames)
+    if n == 0:
+        return []
+    catalogs = list(catalogs) if catalogs is not None else [None] * n
+    directions = list(directions) if directions is not None else [None] * n
+    ex = runner(max_in_flight or min(n, 4))
+    futs = [ex.submit(on_own_stream, run, sub, f, c, d) for f, c, d in zip(frames, catalogs, directions, strict=True)]
+    return [f.result() for f in futs]

@@ -421,6 +421,25 @@ class Subtractor:
         result.elapsed = time.perf_counter() - start
         return result
 
+    def subtract_batch(self, frames, *, max_in_flight: int | None = None) -> list[DiffResult]:
+        """Subtract several frames concurrently (an extension: the reference has no
+        batch call). Each item of `frames` is a dict of subtract() keyword
+        arguments (science, reference and optionally the variance / mask layers,
+        gain, read_noise, catalog, direction). With a CUDA device visible, up to
+        `max_in_flight` frames (default: up to 4) run at once, each on its own
+        host thread, library context and CUDA stream; results are returned in
+        input order. Without a device the frames run one after another."""
+        items = [dict(f) for f in frames]
+        if not items:
+            return []
+        if not self._use_device():
+            return [self.subtract(**it) for it in items]
+        from . import _device
+
+        ex = _device.runner(max_in_flight or min(len(items), 4))
+        futs = [ex.submit(_device.on_own_stream, self.subtract, **it) for it in items]
+        return [f.result() for f in futs]
+
     def apply(self, solution: KernelSolution, science, reference, *, science_var=None, reference_var=None,
               science_mask=None, reference_mask=None, gain=None, read_noise=0.0) -> DiffResult:
         start = time.perf_counter()
@@ -445,6 +464,16 @@ def subtract(science, reference, **kwargs) -> DiffResult:
     config = {k: v for k, v in kwargs.items() if k in _CONFIG_KEYS}
     call = {k: v for k, v in kwargs.items() if k not in _CONFIG_KEYS}
     return Subtractor(**config).subtract(science, reference, **call)
+
+
+def subtract_batch(frames, *, max_in_flight: int | None = None, **kwargs) -> list[DiffResult]:
+    """Configure a Subtractor from the config keywords and subtract several frames
+    concurrently (extension). Non-config keywords (gain, read_noise, ...) apply
+    to every frame unless the frame's own dict sets them."""
+    config = {k: v for k, v in kwargs.items() if k in _CONFIG_KEYS}
+    call = {k: v for k, v in kwargs.items() if k not in _CONFIG_KEYS}
+    items = [{**call, **dict(f)} for f in frames]
+    return Subtractor(**config).subtract_batch(items, max_in_flight=max_in_flight)
 
 
 def apply(solution: KernelSolution, science, reference, **kwargs) -> DiffResult:

@@ -221,3 +221,22 @@ def test_device_resident_large_frame_matches_host_staged():
     for name in ("difference", "variance", "mask", "score"):
         np.testing.assert_array_equal(getattr(a, name), getattr(b, name), err_msg=name)
     np.testing.assert_array_equal(a.source_catalog, b.source_catalog)
+
+
+def test_subtract_batch_matches_one_at_a_time():
+    """Frames in flight on their own threads, contexts and streams give the same
+    bits as subtracting them one after another."""
+    ps = [validation.synthetic_pair(512, 512, 300, s, mask_fraction=0.005) for s in (21, 22, 23)]
+    kw = dict(n_max=4, n_knots=3, stamp_radius=12, cv_folds=0, score=True, decorrelate=True, block=64,
+              precision="mixed", saturation=ps[0].saturation)
+    items = [dict(science=p.science, reference=p.reference, science_var=p.science_var,
+                  reference_var=p.reference_var, science_mask=p.science_mask, reference_mask=p.reference_mask)
+             for p in ps]
+    batch = delta.subtract_batch(items, max_in_flight=3, **kw)
+    assert len(batch) == len(ps)
+    for it, r in zip(items, batch, strict=True):
+        one = delta.subtract(**it, **kw)
+        np.testing.assert_array_equal(r.solution.theta, one.solution.theta)
+        for name in ("difference", "variance", "mask", "score"):
+            np.testing.assert_array_equal(getattr(r, name), getattr(one, name), err_msg=name)
+        np.testing.assert_array_equal(r.source_catalog, one.source_catalog)
