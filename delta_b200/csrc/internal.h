@@ -29,6 +29,10 @@ void check_cuda(cudaError_t e, const char* what);
 // Every kernel launch of the library goes through DGPU_LAUNCH, which also
 // counts it (dgpu_launch_count).
 void count_launch();
+// Raise a kernel's dynamic shared-memory limit to at least `bytes` on the
+// current device; never lowers it, so threads launching the same kernel with
+// different sizes cannot undo each other's setting between set and launch.
+void ensure_dynamic_smem(const void* func, size_t bytes);
 #define DGPU_CUDA(call) ::dgpu::check_cuda((call), #call)
 #define DGPU_LAUNCH(what) (::dgpu::count_launch(), ::dgpu::check_cuda(cudaGetLastError(), what))
 

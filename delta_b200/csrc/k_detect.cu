@@ -437,11 +437,11 @@ void launch_psf_estimate(Context& c, int w, int h, const float* img, const int* 
   double* cuts = static_cast<double*>(c.slot(kSlotScratch0, sizeof(double) * static_cast<size_t>(std::max(n, 1)) * np));
   int* use = static_cast<int*>(c.slot(kSlotBlockCounts, sizeof(int) * std::max(n, 1)));
   const size_t smem = sizeof(double) * 2 * cap;
-  DGPU_CUDA(cudaFuncSetAttribute(k_psf_stamps, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_psf_stamps), smem);
   k_psf_stamps<<<n, 256, smem, s>>>(w, h, img, xs, ys, n, radius, cuts, use);
   DGPU_LAUNCH("k_psf_stamps");
   const size_t smem2 = sizeof(double) * std::max(n, 1);
-  DGPU_CUDA(cudaFuncSetAttribute(k_psf_median, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem2)));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_psf_median), smem2);
   k_psf_median<<<np, 32, smem2, s>>>(n, np, cuts, use, out, c.d_status);
   DGPU_LAUNCH("k_psf_median");
   std::vector<int> hu(n);
@@ -543,7 +543,7 @@ int run_detect(Context& c, int w, int h, const float* img, const uint8_t* mask, 
     const long long iso = p.isolation_radius;
     const size_t smem = sizeof(int) * 2 * std::max(p.max_stamps, 1);
     if (smem > 160 * 1024) fail(DGPU_ERR_INVALID, "detect_stamps: max_stamps above 20480 is not supported");
-    DGPU_CUDA(cudaFuncSetAttribute(k_isolate, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    ensure_dynamic_smem(reinterpret_cast<const void*>(k_isolate), smem);
     k_isolate<<<1, 1024, smem, s>>>(w, count, cap, sorted, iso * iso, p.max_stamps, kept, nk, c.d_status);
     DGPU_LAUNCH("k_isolate");
     DGPU_CUDA(cudaMemcpyAsync(&nkept, nk, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -409,7 +409,7 @@ FftGeom make_fft_geom(int n) {
 void launch_rows_fwd(cudaStream_t s, const FftGeom& g, int mode, int nitems, const float* src, int w, int h,
                      const int* oxs, const int* oys, int nox, float2* spec) {
   const size_t smem = rows_smem(g);
-  DGPU_CUDA(cudaFuncSetAttribute(k_rows_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_rows_fwd), smem);
   dim3 grid(nitems, (g.n + g.rows_per_cta - 1) / g.rows_per_cta);
   k_rows_fwd<<<grid, 256, smem, s>>>(g, mode, src, w, h, oxs, oys, nox, spec);
   DGPU_LAUNCH("k_rows_fwd");
@@ -418,7 +418,7 @@ void launch_rows_fwd(cudaStream_t s, const FftGeom& g, int mode, int nitems, con
 void launch_cols(cudaStream_t s, const FftGeom& g, int mode, int nitems, float2* spec, const double* cell_power,
                  const double* cell_sumk2, const int* block_cell, const double* vsr, double* power_out) {
   const size_t smem = cols_smem(g);
-  DGPU_CUDA(cudaFuncSetAttribute(k_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_cols), smem);
   dim3 grid(nitems, (g.n / 2 + 1 + g.cols_per_cta - 1) / g.cols_per_cta);
   k_cols<<<grid, 256, smem, s>>>(g, mode, spec, cell_power, cell_sumk2, block_cell, vsr, power_out);
   DGPU_LAUNCH("k_cols");
@@ -429,7 +429,7 @@ void launch_rows_inv(cudaStream_t s, const FftGeom& g, int mode, int nitems, con
                      const double* cell_sumk2, const int* block_cell, float* acc, float* var_acc, float* dense_out) {
   if (nitems == 0) return;
   const size_t smem = rows_smem(g);
-  DGPU_CUDA(cudaFuncSetAttribute(k_rows_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_rows_inv), smem);
   dim3 grid(nitems, (g.n + g.rows_per_cta - 1) / g.rows_per_cta);
   k_rows_inv<<<grid, 256, smem, s>>>(g, mode, spec, items, w, h, oxs, oys, nox, hwin, vsr, cell_sumk2, block_cell,
                                      acc, var_acc, dense_out);
@@ -443,7 +443,7 @@ void launch_block_var(cudaStream_t s, const FftGeom& g, int nitems, int nextra, 
   int cap = 1;
   while (cap < ns * ns) cap <<= 1;
   const size_t smem = sizeof(float) * cap;
-  DGPU_CUDA(cudaFuncSetAttribute(k_block_var, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_block_var), smem);
   dim3 grid(nitems + nextra, 2);
   k_block_var<<<grid, 512, smem, s>>>(g, vs, vr, w, h, oxs, oys, nox, nitems, vsr);
   DGPU_LAUNCH("k_block_var");
@@ -453,7 +453,7 @@ void launch_local_kernels(cudaStream_t s, const FftGeom& g, int ncell, const Tps
                           const float* phi, int ks, const double* centres, double* sumk2, float* dense,
                           float* kern_out) {
   const size_t smem = sizeof(float) * static_cast<size_t>(ks) * ks;
-  DGPU_CUDA(cudaFuncSetAttribute(k_local_kernels, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_local_kernels), smem);
   k_local_kernels<<<ncell, 256, smem, s>>>(g, t, theta, nc, phi, ks, centres, sumk2, dense, kern_out);
   DGPU_LAUNCH("k_local_kernels");
 }

@@ -159,7 +159,7 @@ static void launch_gather_t(cudaStream_t st, const StampGeom& g, size_t smem, in
                             const float* vs, const float* vr, const uint8_t* sm, const uint8_t* rm,
                             const float* taps, const int2* orders, const float* fill, const FitRows& R) {
   auto kern = k_stamp_gather<NX>;
-  DGPU_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
   kern<<<n_stamps, 256, smem, st>>>(g, sx, sy, sci, ref, vs, vr, sm, rm, taps, orders, fill, R);
   DGPU_LAUNCH("k_stamp_gather");
 }
@@ -504,7 +504,7 @@ void launch_rhs(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, 
   long long* npart = reinterpret_cast<long long*>(ypart + nsplit);
   const size_t smem =
       sizeof(double) * (kRhsRows * (nc + 1) + kRhsRows * k + 2 * kRhsRows + P) + sizeof(int) * kRhsRows;
-  DGPU_CUDA(cudaFuncSetAttribute(k_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_rhs), smem);
   k_rhs<<<nsplit, 256, smem, st>>>(N, nc, k, SS, R, accepted, theta, rps, rpart, ypart, npart);
   DGPU_LAUNCH("k_rhs");
   k_reduce_rhs<<<(P + 31) / 32, 256, 0, st>>>(nsplit, P, rpart, ypart, npart, rhs, ywy, n);
@@ -638,7 +638,7 @@ void launch_reweight(cudaStream_t st, const StampGeom& g, int n_stamps, const Tp
   const size_t side = static_cast<size_t>(g.S) + 2 * g.r;
   const size_t smem = sizeof(float) * (static_cast<size_t>(g.ks) * g.ks + side * side);
   if (smem > 200 * 1024) fail(DGPU_ERR_INVALID, "fit_kernel: stamp plus kernel footprint too large for the reweight");
-  DGPU_CUDA(cudaFuncSetAttribute(k_reweight, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_reweight), smem);
   k_reweight<<<n_stamps, 256, smem, st>>>(g, t, sx, sy, R, accepted, cnt, theta, phi, vr, rm);
   DGPU_LAUNCH("k_reweight");
 }

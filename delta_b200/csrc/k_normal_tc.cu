@@ -349,7 +349,7 @@ int launch_normal_tc(Context& c, int64_t N, int nc, int k, int SS, const FitRows
   a.rows_per_split = rps;
   a.gpart = gpart;
   a.status = c.d_status;
-  DGPU_CUDA(cudaFuncSetAttribute(k_normal_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_normal_tc), smem);
   k_normal_tc<<<dim3(tiles_m, tiles_n, nsplit), kThreads, smem, c.stream>>>(a);
   DGPU_LAUNCH("k_normal_tc");
   *gpart_out = gpart;

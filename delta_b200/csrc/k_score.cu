@@ -158,8 +158,7 @@ void launch_matched_filter(cudaStream_t s, int w, int h, const float* img, const
   const size_t smem = sizeof(float) * (static_cast<size_t>(ps) * ps +
                                        static_cast<size_t>(kMfTH + 2 * r) * (kMfTW + 2 * r));
   if (smem > 200 * 1024) fail(DGPU_ERR_INVALID, "matched_filter: psf too large");
-  DGPU_CUDA(cudaFuncSetAttribute(k_matched_filter_g, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem)));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_matched_filter_g), smem);
   dim3 grid(ceil_div(w, kMfTW), ceil_div(h, kMfTH));
   k_matched_filter_g<<<grid, 256, smem, s>>>(w, h, img, var, psf_dev, ps, sumpsf2, out);
   DGPU_LAUNCH("k_matched_filter_g");

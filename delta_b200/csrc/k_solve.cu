@@ -54,26 +54,42 @@ __device__ __forceinline__ void store_tile(double* g, double (*t)[kT + 1], int P
   for (int e = threadIdx.x; e < kT * kT; e += blockDim.x) g[static_cast<size_t>(e / kT) * Pp + e % kT] = t[e / kT][e % kT];
 }
 
-// acc (2x2 per thread) += A B^T over the 32-wide inner dimension.
+// acc += A B^T over the 32-wide inner dimension with FP64 tensor-core MMAs
+// (mma.sync m8n8k4, f64): the 32 x 32 output is 4 x 4 blocks of 8 x 8; warp w
+// owns row block w / 2 and column blocks 2 (w % 2) and 2 (w % 2) + 1, two
+// accumulators of two doubles per thread (D fragment: row lane / 4, columns
+// 2 (lane % 4) + {0, 1}). A fragment: A[row lane / 4][k + lane % 4];
+// B fragment (B^T column-major): B[col lane / 4][k + lane % 4].
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
 __device__ __forceinline__ void mma_nt(double (*A)[kT + 1], double (*B)[kT + 1], double acc[2][2]) {
-  const int ra = (threadIdx.x / 16) * 2, rb = (threadIdx.x % 16) * 2;
-#pragma unroll 8
-  for (int q = 0; q < kT; ++q) {
-    const double a0 = A[ra][q], a1 = A[ra + 1][q];
-    const double b0 = B[rb][q], b1 = B[rb + 1][q];
-    acc[0][0] = fma(a0, b0, acc[0][0]);
-    acc[0][1] = fma(a0, b1, acc[0][1]);
-    acc[1][0] = fma(a1, b0, acc[1][0]);
-    acc[1][1] = fma(a1, b1, acc[1][1]);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ra = (warp >> 1) * 8 + (lane >> 2);
+  const int cb0 = (warp & 1) * 16 + (lane >> 2);
+  const int kq = lane & 3;
+#pragma unroll
+  for (int k0 = 0; k0 < kT; k0 += 4) {
+    const double a = A[ra][k0 + kq];
+    const double b0 = B[cb0][k0 + kq];
+    const double b1 = B[cb0 + 8][k0 + kq];
+    dmma_8x8x4(acc[0], a, b0);
+    dmma_8x8x4(acc[1], a, b1);
   }
 }
 
 __device__ __forceinline__ void acc_to_tile(double (*C)[kT + 1], const double acc[2][2], double scale, bool add) {
-  const int ra = (threadIdx.x / 16) * 2, rb = (threadIdx.x % 16) * 2;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r = (warp >> 1) * 8 + (lane >> 2);
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+  for (int blk = 0; blk < 2; ++blk) {
+    const int c0 = (warp & 1) * 16 + blk * 8 + (lane & 3) * 2;
 #pragma unroll
-    for (int j = 0; j < 2; ++j) C[ra + i][rb + j] = (add ? C[ra + i][rb + j] : 0.0) + scale * acc[i][j];
+    for (int i = 0; i < 2; ++i) C[r][c0 + i] = (add ? C[r][c0 + i] : 0.0) + scale * acc[blk][i];
+  }
 }
 
 // Global writes of this CTA become visible to the cluster, then all ranks meet.
@@ -314,7 +330,7 @@ void launch_solve_batch(Context& c, const SolveBatch& b) {
   if (b.nsys <= 0) return;
   const int cn = solve_cluster_size(b.nsys);
   const size_t smem = sizeof(Tiles);
-  DGPU_CUDA(cudaFuncSetAttribute(k_solve_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_solve_cluster), smem);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(static_cast<unsigned>(b.nsys * cn));
   cfg.blockDim = dim3(kSolveThreads);
@@ -372,7 +388,7 @@ __global__ void __launch_bounds__(kAiThreads) k_apply_inverse(const double* __re
 void launch_apply_inverse(cudaStream_t st, const SolveBatch& b, int s, const double* v, double* out) {
   const int Pp = solve_pp(b.P);
   const size_t smem = sizeof(double) * static_cast<size_t>(b.P) * (1 + kAiThreads / 32);
-  DGPU_CUDA(cudaFuncSetAttribute(k_apply_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_apply_inverse), smem);
   k_apply_inverse<<<1, kAiThreads, smem, st>>>(b.Linv + static_cast<size_t>(s) * Pp * Pp, b.P, Pp, v, out);
   DGPU_LAUNCH("k_apply_inverse");
 }

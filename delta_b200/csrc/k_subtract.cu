@@ -306,7 +306,7 @@ k_model_convolve(int w, int h, const float* __restrict__ sci, const float* __res
 template <int NX, bool STACK>
 static void launch_mc(cudaStream_t s, const SubtractArgs& a, const int2* orders, int TH, size_t smem) {
   auto kern = k_model_convolve<NX, STACK>;
-  DGPU_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
   dim3 grid(ceil_div(a.w, kMcTW), ceil_div(a.h, TH));
   const int threads = kMcTW * (TH / kMcRPT);
   kern<<<grid, threads, smem, s>>>(a.w, a.h, a.sci, a.ref, a.ref_mask, a.F, a.taps, orders, a.ks,
@@ -489,7 +489,7 @@ void launch_variance(cudaStream_t s, int w, int h, const DevFields& F, const flo
   const int iw = kVarB + 2 * rk;
   const size_t smem = sizeof(float) * (2 * static_cast<size_t>(ks) * ks + static_cast<size_t>(iw) * iw + nc + 4);
   if (smem > 200 * 1024) fail(DGPU_ERR_INVALID, "subtract: kernel radius too large for the variance engine");
-  DGPU_CUDA(cudaFuncSetAttribute(k_variance, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_variance), smem);
   dim3 grid(ceil_div(w, kVarB), ceil_div(h, kVarB));
   k_variance<<<grid, 256, smem, s>>>(w, h, F, phi, rk, nc, var_s, var_r, var_out);
   DGPU_LAUNCH("k_variance");
@@ -577,7 +577,7 @@ void launch_mask(cudaStream_t s, int w, int h, const float* sci, const float* re
   const int gw = kMkT + 2 * r;
   const size_t smem = static_cast<size_t>(gw) * gw + static_cast<size_t>(gw) * kMkT;
   if (smem > 200 * 1024) fail(DGPU_ERR_INVALID, "subtract: kernel radius too large for mask growth");
-  DGPU_CUDA(cudaFuncSetAttribute(k_mask, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_mask), smem);
   dim3 grid(ceil_div(w, kMkT), ceil_div(h, kMkT));
   const int has_sat = saturation > 0.0 ? 1 : 0;
   k_mask<<<grid, 256, smem, s>>>(w, h, sci, ref, sm, rm, has_sat, static_cast<float>(saturation), r,

@@ -3,6 +3,9 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <map>
+#include <mutex>
+#include <utility>
 #include <cstdlib>
 #include <stdexcept>
 
@@ -41,6 +44,19 @@ void check_status(Context& c) {
   DGPU_CUDA(cudaStreamSynchronize(c.stream));
   if (st & kStatusLoopLimit) fail(DGPU_ERR_LIMIT, "a device loop hit its iteration cap");
   if (st & kStatusBounds) fail(DGPU_ERR_LIMIT, "a device bounds check rejected an access");
+}
+
+static std::mutex g_smem_mu;
+static std::map<std::pair<int, const void*>, size_t> g_smem_set;
+
+void ensure_dynamic_smem(const void* func, size_t bytes) {
+  int dev = 0;
+  DGPU_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_smem_mu);
+  size_t& cur = g_smem_set[{dev, func}];
+  if (bytes <= cur) return;
+  DGPU_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+  cur = bytes;
 }
 
 static std::atomic<unsigned long long> g_launches{0};
