@@ -112,7 +112,10 @@ int dgpu_decorrelate(dgpu_context* ctx, int mem, int64_t width, int64_t height, 
     const auto* vr = static_cast<const float*>(stage_in(c, mem, var_reference, 4 * npx, kSlotInVarR));
     float* acc = static_cast<float*>(out_buf(c, mem, out_difference, 4 * npx, kSlotOutDiff));
     float* vacc = static_cast<float*>(out_buf(c, mem, out_variance, 4 * npx, kSlotOutVar));
-    const FftGeom g = make_fft_geom(block);
+    FftGeom g = make_fft_geom(block);
+    float2* twtab = static_cast<float2*>(c.slot(kSlotGlsPart, sizeof(float2) * twiddle_table_len(block)));
+    launch_twiddle_table(c.stream, block, twtab);
+    g.tw_tab = twtab;
     const int n = block, nb = n / 2 + 1, stride = block / 2;
     const std::vector<int> oxs = origins(w, block, stride), oys = origins(h, block, stride);
     const int nox = static_cast<int>(oxs.size()), noy = static_cast<int>(oys.size());
@@ -199,16 +202,20 @@ int dgpu_decorrelate(dgpu_context* ctx, int mem, int64_t width, int64_t height, 
       StageTimer tm(c, "decorrelate: block filter+blend");
       launch_block_var(s, g, nblk, 0, vs, vr, w, h, d_oxs, d_oys, nox, vsr);
       launch_rows_fwd(s, g, 0, nblk, D, w, h, d_oxs, d_oys, nox, spec);
-      launch_cols(s, g, 0, nblk, spec, cell_power, cell_sumk2, d_bcell, vsr, nullptr);
-      DGPU_CUDA(cudaMemsetAsync(acc, 0, 4 * npx, s));
-      DGPU_CUDA(cudaMemsetAsync(vacc, 0, 4 * npx, s));
-      for (int q = 0; q < 9; ++q)
-        launch_rows_inv(s, g, 0, colour_off[q + 1] - colour_off[q], spec, d_citems + colour_off[q], w, h, d_oxs,
-                        d_oys, nox, d_hw, vsr, cell_sumk2, d_bcell, acc, vacc, nullptr);
+      double* bnum = static_cast<double*>(c.slot(kSlotFft2, sizeof(double) * static_cast<size_t>(nblk)));
+      launch_cols(s, g, 0, nblk, spec, cell_power, cell_sumk2, d_bcell, vsr, bnum);
+      // Raw c2r outputs of every block, then the overlap-add as a per-pixel gather
+      // in the reference's colour order (same sums as 9 colour passes).
+      float* bout = static_cast<float*>(c.slot(kSlotFft4, sizeof(float) * static_cast<size_t>(nblk) * n * n));
+      launch_rows_inv(s, g, 2, nblk, spec, nullptr, w, h, d_oxs, d_oys, nox, d_hw, vsr, cell_sumk2, d_bcell, nullptr,
+                      nullptr, bout);
     }
     {
       StageTimer tm(c, "decorrelate: normalise");
-      launch_ola_normalise(s, w, h, d_wxt, d_wyt, acc, vacc);
+      launch_ola_gather(s, w, h, n, d_oxs, nox, d_oys, noy, d_hw,
+                        static_cast<const float*>(c.slot(kSlotFft4, sizeof(float) * static_cast<size_t>(nblk) * n * n)),
+                        static_cast<const double*>(c.slot(kSlotFft2, sizeof(double) * static_cast<size_t>(nblk))),
+                        d_wxt, d_wyt, acc, vacc);
     }
     stage_out(c, mem, out_difference, acc, 4 * npx);
     stage_out(c, mem, out_variance, vacc, 4 * npx);

@@ -40,15 +40,51 @@ __device__ void make_twiddles(float2* tw, int m, int sign) {
   }
 }
 
-// In-place radix-2 DIT FFT of L lines of length m (line-major) in shared memory.
-__device__ void smem_fft(float2* x, int L, int m, int logm, const float2* tw) {
+// Twiddle table offsets (see FftGeom::tw_tab).
+__device__ __forceinline__ int tw_off_inv_n(int n) { return n / 2; }
+__device__ __forceinline__ int tw_off_fwd_hn(int n) { return n; }
+__device__ __forceinline__ int tw_off_inv_hn(int n) { return n + n / 4; }
+__device__ __forceinline__ int tw_off_split_fwd(int n) { return n + n / 2; }
+__device__ __forceinline__ int tw_off_split_inv(int n) { return n + n / 2 + n / 2 + 1; }
+
+__device__ __forceinline__ void copy_tw(float2* dst, const float2* src, int count) {
+  for (int k = threadIdx.x; k < count; k += blockDim.x) dst[k] = src[k];
+}
+
+// Same values as make_twiddles / the split factors below, once per call.
+__global__ void k_twiddle_table(int n, float2* tab) {
+  const int hn = n / 2;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n / 2; k += gridDim.x * blockDim.x) {
+    double s, c;
+    sincospi(2.0 * k / n, &s, &c);
+    tab[k] = make_float2(static_cast<float>(c), static_cast<float>(-s));
+    tab[tw_off_inv_n(n) + k] = make_float2(static_cast<float>(c), static_cast<float>(s));
+  }
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < hn / 2; k += gridDim.x * blockDim.x) {
+    double s, c;
+    sincospi(2.0 * k / hn, &s, &c);
+    tab[tw_off_fwd_hn(n) + k] = make_float2(static_cast<float>(c), static_cast<float>(-s));
+    tab[tw_off_inv_hn(n) + k] = make_float2(static_cast<float>(c), static_cast<float>(s));
+  }
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= hn; k += gridDim.x * blockDim.x) {
+    double s, c;
+    sincospi(2.0 * k / n, &s, &c);
+    tab[tw_off_split_fwd(n) + k] = make_float2(static_cast<float>(c), static_cast<float>(-s));
+    tab[tw_off_split_inv(n) + k] = make_float2(static_cast<float>(c), static_cast<float>(s));
+  }
+}
+
+// In-place radix-2 DIT FFT of L lines of length m in shared memory, line l at
+// x + l * ls (ls = m for packed rows; m + 1 for transposed column lines, which
+// keeps the strided accesses of a warp on distinct banks).
+__device__ void smem_fft(float2* x, int L, int m, int logm, const float2* tw, int ls) {
   for (int e = threadIdx.x; e < L * m; e += blockDim.x) {
     const int line = e / m, j = e - line * m;
     const int rj = static_cast<int>(__brev(static_cast<unsigned>(j)) >> (32 - logm));
     if (j < rj) {
-      const float2 t = x[line * m + j];
-      x[line * m + j] = x[line * m + rj];
-      x[line * m + rj] = t;
+      const float2 t = x[line * ls + j];
+      x[line * ls + j] = x[line * ls + rj];
+      x[line * ls + rj] = t;
     }
   }
   __syncthreads();
@@ -58,7 +94,7 @@ __device__ void smem_fft(float2* x, int L, int m, int logm, const float2* tw) {
       const int line = b / (m / 2), j = b - line * (m / 2);
       const int pos = j & (half - 1);
       const int i0 = ((j - pos) << 1) + pos, i1 = i0 + half;
-      float2* xl = x + line * m;
+      float2* xl = x + line * ls;
       const float2 a = xl[i0];
       const float2 c = cmul(xl[i1], tw[pos * tstep]);
       xl[i0] = cadd(a, c);
@@ -88,11 +124,16 @@ k_rows_fwd(FftGeom G, int mode, const float* __restrict__ src, int w, int h, con
   float2* tw = z + rows * hn;       // hn/2 (length-hn FFT)
   float2* twn = tw + hn / 2 + 1;    // hn (W^k, k < hn + 1) for the split
   const int item = blockIdx.x, r0 = blockIdx.y * rows;
-  make_twiddles(tw, hn, -1);
-  for (int k = threadIdx.x; k <= hn; k += blockDim.x) {
-    double s, c;
-    sincospi(2.0 * k / n, &s, &c);
-    twn[k] = make_float2(static_cast<float>(c), static_cast<float>(-s));
+  if (G.tw_tab) {
+    copy_tw(tw, G.tw_tab + tw_off_fwd_hn(n), hn / 2);
+    copy_tw(twn, G.tw_tab + tw_off_split_fwd(n), hn + 1);
+  } else {
+    make_twiddles(tw, hn, -1);
+    for (int k = threadIdx.x; k <= hn; k += blockDim.x) {
+      double s, c;
+      sincospi(2.0 * k / n, &s, &c);
+      twn[k] = make_float2(static_cast<float>(c), static_cast<float>(-s));
+    }
   }
   int bx = 0, by = 0;
   if (mode == 0) {
@@ -116,7 +157,7 @@ k_rows_fwd(FftGeom G, int mode, const float* __restrict__ src, int w, int h, con
     z[e] = make_float2(a, b);
   }
   __syncthreads();
-  smem_fft(z, rows, hn, G.logn - 1, tw);
+  smem_fft(z, rows, hn, G.logn - 1, tw, hn);
   for (int e = threadIdx.x; e < rows * nb; e += blockDim.x) {
     const int rr = e / nb, k = e - rr * nb;
     const float2 zk = z[rr * hn + (k % hn)];
@@ -139,28 +180,32 @@ k_cols(FftGeom G, int mode, float2* __restrict__ spec, const double* __restrict_
   extern __shared__ __align__(16) float2 fsm2[];
   const int n = G.n, nb = n / 2 + 1;
   const int C = G.cols_per_cta;
-  float2* x = fsm2;            // C x n
-  float2* tw = x + C * n;      // n/2
+  const int ls = n + 1;        // padded column-line stride (bank-conflict free transposes)
+  float2* x = fsm2;            // C x ls
+  float2* tw = x + C * ls;     // n/2
   const int item = blockIdx.x, c0 = blockIdx.y * C;
   const int ncol = min(C, nb - c0);
-  make_twiddles(tw, n, -1);
+  if (G.tw_tab)
+    copy_tw(tw, G.tw_tab, n / 2);
+  else
+    make_twiddles(tw, n, -1);
   float2* sp = spec + static_cast<size_t>(item) * n * nb;
   if (mode == 2) {
     // Spectrum = the real filter itself (decorrelation_kernel_image, src/noise.cpp:139-146).
-    for (int e = threadIdx.x; e < C * n; e += blockDim.x) x[e] = make_float2(0.f, 0.f);
+    for (int e = threadIdx.x; e < C * ls; e += blockDim.x) x[e] = make_float2(0.f, 0.f);
   } else {
     for (int e = threadIdx.x; e < C * n; e += blockDim.x) {
       const int row = e / C, cc = e - row * C;
-      x[cc * n + row] = cc < ncol ? sp[static_cast<size_t>(row) * nb + c0 + cc] : make_float2(0.f, 0.f);
+      x[cc * ls + row] = cc < ncol ? sp[static_cast<size_t>(row) * nb + c0 + cc] : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    smem_fft(x, C, n, G.logn, tw);
+    smem_fft(x, C, n, G.logn, tw, ls);
   }
   if (mode == 1) {
     for (int e = threadIdx.x; e < C * n; e += blockDim.x) {
       const int row = e / C, cc = e - row * C;
       if (cc >= ncol) continue;
-      const float2 v = x[cc * n + row];
+      const float2 v = x[cc * ls + row];
       const double re = v.x, im = v.y;
       power_out[(static_cast<size_t>(item) * n + row) * nb + c0 + cc] = re * re + im * im;
     }
@@ -170,21 +215,26 @@ k_cols(FftGeom G, int mode, float2* __restrict__ spec, const double* __restrict_
   const int cell = block_cell[item];
   const double vs = vsr[2 * item], vr = vsr[2 * item + 1];
   const double cnum = sqrt(fmax(vs + vr * cell_sumk2[cell], 0.0));
+  if (mode == 0 && blockIdx.y == 0 && threadIdx.x == 0 && power_out) power_out[item] = cnum * cnum;  // block num
   const double* pw = cell_power + static_cast<size_t>(cell) * n * nb;
   for (int e = threadIdx.x; e < C * n; e += blockDim.x) {
-    const int cc = e / n, row = e - cc * n;
+    const int row = e / C, cc = e - row * C;
     if (cc >= ncol) continue;
     const double denom = vs + vr * pw[static_cast<size_t>(row) * nb + c0 + cc];
     const float f = denom > 0.0 ? static_cast<float>(cnum / sqrt(denom)) : 0.0f;
-    x[cc * n + row] = mode == 2 ? make_float2(f, 0.0f) : make_float2(x[cc * n + row].x * f, x[cc * n + row].y * f);
+    float2& xv = x[cc * ls + row];
+    xv = mode == 2 ? make_float2(f, 0.0f) : make_float2(xv.x * f, xv.y * f);
   }
   __syncthreads();
-  make_twiddles(tw, n, +1);
+  if (G.tw_tab)
+    copy_tw(tw, G.tw_tab + tw_off_inv_n(n), n / 2);
+  else
+    make_twiddles(tw, n, +1);
   __syncthreads();
-  smem_fft(x, C, n, G.logn, tw);
+  smem_fft(x, C, n, G.logn, tw, ls);
   for (int e = threadIdx.x; e < C * n; e += blockDim.x) {
     const int row = e / C, cc = e - row * C;
-    if (cc < ncol) sp[static_cast<size_t>(row) * nb + c0 + cc] = x[cc * n + row];
+    if (cc < ncol) sp[static_cast<size_t>(row) * nb + c0 + cc] = x[cc * ls + row];
   }
 }
 
@@ -206,11 +256,16 @@ k_rows_inv(FftGeom G, int mode, const float2* __restrict__ spec, const int* __re
   float2* twn = tw + hn / 2 + 1;
   const int item = mode == 0 ? items[blockIdx.x] : blockIdx.x;
   const int r0 = blockIdx.y * rows;
-  make_twiddles(tw, hn, +1);
-  for (int k = threadIdx.x; k <= hn; k += blockDim.x) {
-    double s, c;
-    sincospi(2.0 * k / n, &s, &c);
-    twn[k] = make_float2(static_cast<float>(c), static_cast<float>(s));  // W^-k
+  if (G.tw_tab) {
+    copy_tw(tw, G.tw_tab + tw_off_inv_hn(n), hn / 2);
+    copy_tw(twn, G.tw_tab + tw_off_split_inv(n), hn + 1);  // W^-k
+  } else {
+    make_twiddles(tw, hn, +1);
+    for (int k = threadIdx.x; k <= hn; k += blockDim.x) {
+      double s, c;
+      sincospi(2.0 * k / n, &s, &c);
+      twn[k] = make_float2(static_cast<float>(c), static_cast<float>(s));  // W^-k
+    }
   }
   __syncthreads();
   const float2* sp = spec + static_cast<size_t>(item) * n * nb;
@@ -228,8 +283,16 @@ k_rows_inv(FftGeom G, int mode, const float2* __restrict__ spec, const int* __re
     z[e] = make_float2(e2.x - o2.y, e2.y + o2.x);  // 2E + i 2O
   }
   __syncthreads();
-  smem_fft(z, rows, hn, G.logn - 1, tw);
+  smem_fft(z, rows, hn, G.logn - 1, tw, hn);
   const float inv_n2 = 1.0f / static_cast<float>(static_cast<size_t>(n) * n);
+  if (mode == 2) {  // raw real block output for the overlap-add gather (dense_out: item x n x n)
+    for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
+      const int rr = e / n, m = e - rr * n;
+      const float2 v = z[rr * hn + (m >> 1)];
+      dense_out[(static_cast<size_t>(item) * n + r0 + rr) * n + m] = (m & 1) ? v.y : v.x;
+    }
+    return;
+  }
   if (mode == 1) {
     for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
       const int rr = e / n, m = e - rr * n;
@@ -259,18 +322,78 @@ k_rows_inv(FftGeom G, int mode, const float2* __restrict__ spec, const int* __re
   }
 }
 
+// Overlap-add as a gather (src/noise.cpp:430-479): every frame pixel sums the
+// Hann-weighted outputs of the (at most 3 x 3) blocks covering it in colour
+// order q = (ix % 3) * 3 + (iy % 3) -- the order of the reference's 9-colour
+// passes -- with the same float rounding after each block, then divides by the
+// separable weight sum. One thread per pixel; bout holds each block's raw
+// c2r output (item x n x n).
+__global__ void __launch_bounds__(256)
+k_ola_gather(int w, int h, int n, const int* __restrict__ oxs, int nox, const int* __restrict__ oys, int noy,
+             const double* __restrict__ hwin, const float* __restrict__ bout, const double* __restrict__ bnum,
+             const double* __restrict__ wx_total, const double* __restrict__ wy_total, float* __restrict__ acc,
+             float* __restrict__ var_acc) {
+  const int64_t npx = static_cast<int64_t>(w) * h;
+  const int s = n / 2;
+  const double inv_n2 = static_cast<double>(1.0f / static_cast<float>(static_cast<size_t>(n) * n));
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < npx;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int x = static_cast<int>(i % w), y = static_cast<int>(i / w);
+    // Largest origin index <= x (regular origins at multiples of s, then the flush origin).
+    int ixh = min(x / max(s, 1), nox - 1);
+    while (ixh + 1 < nox && oxs[ixh + 1] <= x) ++ixh;
+    while (ixh > 0 && oxs[ixh] > x) --ixh;
+    int iyh = min(y / max(s, 1), noy - 1);
+    while (iyh + 1 < noy && oys[iyh + 1] <= y) ++iyh;
+    while (iyh > 0 && oys[iyh] > y) --iyh;
+    int slot[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) slot[q] = -1;
+    for (int ix = ixh; ix >= 0 && ix > ixh - 3 && oxs[ix] + n > x; --ix)
+      for (int iy = iyh; iy >= 0 && iy > iyh - 3 && oys[iy] + n > y; --iy) slot[(ix % 3) * 3 + (iy % 3)] = iy * nox + ix;
+    float a = 0.0f, v = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const int item = slot[q];
+      if (item < 0) continue;
+      const int bx = oxs[item % nox], by = oys[item / nox];
+      const int ly = y - by, lx = x - bx;
+      const float f = bout[(static_cast<size_t>(item) * n + ly) * n + lx];
+      const double num = bnum[item];
+      const double wy_sig = hwin[ly] * inv_n2;
+      const double wy_var = hwin[ly];
+      const double wxv = hwin[lx];
+      a = static_cast<float>(static_cast<double>(a) + wy_sig * wxv * static_cast<double>(f));
+      v = static_cast<float>(static_cast<double>(v) + wy_var * wxv * num);
+    }
+    const double ws = wy_total[y] * wx_total[x];
+    if (ws > 0.0) {
+      acc[i] = static_cast<float>(static_cast<double>(a) / ws);
+      var_acc[i] = static_cast<float>(static_cast<double>(v) / ws);
+    } else {
+      acc[i] = 0.0f;
+      var_acc[i] = 0.0f;
+    }
+  }
+}
+
 // Subsampled block noise: upper median of finite positive var[y][x] over the
-// block's step-(n/64) grid (src/noise.cpp:200-224). One CTA per (block, layer).
+// block's step-(n/64) grid (src/noise.cpp:200-224). One CTA per (block, layer):
+// samples go to fixed slots (invalid ones as +inf, which rank last), the valid
+// count comes from a block reduction, and an 8-bit radix select in shared
+// memory returns the element of rank count / 2 -- the same value a sort gives.
 __global__ void __launch_bounds__(512)
 k_block_var(FftGeom G, const float* __restrict__ vs, const float* __restrict__ vr, int w, int h,
             const int* __restrict__ oxs, const int* __restrict__ oys, int nox, int nitem, double* __restrict__ vsr) {
-  extern __shared__ float vals[];
-  __shared__ int cnt;
+  extern __shared__ uint32_t keys[];
+  __shared__ unsigned hist[256];
+  __shared__ unsigned s_rank, s_prefix, s_cnt;
   const int item = blockIdx.x, layer = blockIdx.y;
   const float* var = layer == 0 ? vs : vr;
   const int n = G.n;
   const int step = max(1, n / 64);
   const int ns = (n + step - 1) / step;
+  const int m = ns * ns;
   int bx, by;
   if (item < nitem) {
     bx = oxs[item % nox];
@@ -279,36 +402,72 @@ k_block_var(FftGeom G, const float* __restrict__ vs, const float* __restrict__ v
     bx = G.extra_bx;
     by = G.extra_by;
   }
-  if (threadIdx.x == 0) cnt = 0;
-  __syncthreads();
-  int cap = 1;
-  while (cap < ns * ns) cap <<= 1;
-  for (int e = threadIdx.x; e < cap; e += blockDim.x) vals[e] = INFINITY;
-  __syncthreads();
-  for (int e = threadIdx.x; e < ns * ns; e += blockDim.x) {
+  unsigned mine = 0;
+  for (int e = threadIdx.x; e < m; e += blockDim.x) {
     const int yy = by + (e / ns) * step, xx = bx + (e % ns) * step;
-    if (yy < 0 || yy >= h || xx < 0 || xx >= w) continue;
-    const float v = var[static_cast<size_t>(yy) * w + xx];
-    if (isfinite(v) && v > 0.0f) vals[atomicAdd(&cnt, 1)] = v;
-  }
-  __syncthreads();
-  // bitonic sort ascending of `cap` values (padding +inf)
-  for (int size = 2; size <= cap; size <<= 1)
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int i = threadIdx.x; i < cap; i += blockDim.x) {
-        const int j = i ^ stride;
-        if (j > i) {
-          const bool up = (i & size) == 0;
-          const float a = vals[i], b = vals[j];
-          if ((a > b) == up) {
-            vals[i] = b;
-            vals[j] = a;
-          }
-        }
+    float v = INFINITY;
+    if (yy >= 0 && yy < h && xx >= 0 && xx < w) {
+      const float x = var[static_cast<size_t>(yy) * w + xx];
+      if (isfinite(x) && x > 0.0f) {
+        v = x;
+        ++mine;
       }
-      __syncthreads();
     }
-  if (threadIdx.x == 0) vsr[2 * item + layer] = cnt ? static_cast<double>(vals[cnt / 2]) : 0.0;
+    keys[e] = __float_as_uint(v);  // positive floats (and +inf) order as their bit patterns
+  }
+  if (threadIdx.x == 0) s_cnt = 0;
+  __syncthreads();
+  const unsigned wsum = __reduce_add_sync(0xffffffffu, mine);
+  if ((threadIdx.x & 31) == 0) atomicAdd(&s_cnt, wsum);
+  __syncthreads();
+  const unsigned cnt = s_cnt;
+  if (cnt == 0) {
+    if (threadIdx.x == 0) vsr[2 * item + layer] = 0.0;
+    return;
+  }
+  if (threadIdx.x == 0) {
+    s_rank = cnt / 2;
+    s_prefix = 0;
+  }
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    const unsigned prefix = s_prefix;
+    const unsigned himask = shift >= 24 ? 0u : (0xffffffffu << (shift + 8));
+    for (int e = threadIdx.x; e < m; e += blockDim.x) {
+      const uint32_t k = keys[e];
+      if ((k & himask) == (prefix & himask)) atomicAdd(&hist[(k >> shift) & 0xffu], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {  // one warp: 8 bins per lane, warp prefix sums, pick the digit holding the rank
+      const int lane = threadIdx.x;
+      unsigned local = 0;
+      for (int j = 0; j < 8; ++j) local += hist[lane * 8 + j];
+      unsigned incl = local;
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      const unsigned excl = incl - local;
+      const unsigned rank = s_rank;
+      const bool here = rank >= excl && rank < incl;
+      const unsigned who = __ballot_sync(0xffffffffu, here);
+      if (here) {
+        unsigned cum = excl;
+        int d = lane * 8;
+        for (int j = 0; j < 8; ++j, ++d) {
+          const unsigned c = hist[d];
+          if (rank < cum + c) break;
+          cum += c;
+        }
+        s_rank = rank - cum;
+        s_prefix = prefix | (static_cast<unsigned>(d) << shift);
+      }
+      (void)who;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) vsr[2 * item + layer] = static_cast<double>(__uint_as_float(s_prefix));
 }
 
 // Local kernel per cell: K = sum_n float(a_n(cx,cy)) phi_n (exact thin-plate
@@ -392,7 +551,14 @@ static size_t rows_smem(const FftGeom& g) {
   return sizeof(float2) * (static_cast<size_t>(g.rows_per_cta) * hn + hn / 2 + 1 + hn + 1);
 }
 static size_t cols_smem(const FftGeom& g) {
-  return sizeof(float2) * (static_cast<size_t>(g.cols_per_cta) * g.n + g.n / 2 + 1);
+  return sizeof(float2) * (static_cast<size_t>(g.cols_per_cta) * (g.n + 1) + g.n / 2 + 1);
+}
+
+size_t twiddle_table_len(int n) { return static_cast<size_t>(n) + n / 2 + 2 * (n / 2 + 1); }
+
+void launch_twiddle_table(cudaStream_t s, int n, float2* tab) {
+  k_twiddle_table<<<1, 256, 0, s>>>(n, tab);
+  DGPU_LAUNCH("k_twiddle_table");
 }
 
 FftGeom make_fft_geom(int n) {
@@ -440,9 +606,7 @@ void launch_block_var(cudaStream_t s, const FftGeom& g, int nitems, int nextra, 
                       int w, int h, const int* oxs, const int* oys, int nox, double* vsr) {
   const int step = std::max(1, g.n / 64);
   const int ns = (g.n + step - 1) / step;
-  int cap = 1;
-  while (cap < ns * ns) cap <<= 1;
-  const size_t smem = sizeof(float) * cap;
+  const size_t smem = sizeof(uint32_t) * static_cast<size_t>(ns) * ns;
   ensure_dynamic_smem(reinterpret_cast<const void*>(k_block_var), smem);
   dim3 grid(nitems + nextra, 2);
   k_block_var<<<grid, 512, smem, s>>>(g, vs, vr, w, h, oxs, oys, nox, nitems, vsr);
@@ -456,6 +620,16 @@ void launch_local_kernels(cudaStream_t s, const FftGeom& g, int ncell, const Tps
   ensure_dynamic_smem(reinterpret_cast<const void*>(k_local_kernels), smem);
   k_local_kernels<<<ncell, 256, smem, s>>>(g, t, theta, nc, phi, ks, centres, sumk2, dense, kern_out);
   DGPU_LAUNCH("k_local_kernels");
+}
+
+void launch_ola_gather(cudaStream_t s, int w, int h, int n, const int* oxs, int nox, const int* oys, int noy,
+                       const double* hwin, const float* bout, const double* bnum, const double* wx_total,
+                       const double* wy_total, float* acc, float* var_acc) {
+  const int64_t npx = static_cast<int64_t>(w) * h;
+  const int blocks = static_cast<int>(std::min<int64_t>((npx + 255) / 256, 148 * 16));
+  k_ola_gather<<<blocks, 256, 0, s>>>(w, h, n, oxs, nox, oys, noy, hwin, bout, bnum, wx_total, wy_total, acc,
+                                      var_acc);
+  DGPU_LAUNCH("k_ola_gather");
 }
 
 void launch_ola_normalise(cudaStream_t s, int w, int h, const double* wx_total, const double* wy_total, float* acc,

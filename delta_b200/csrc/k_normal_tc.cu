@@ -49,6 +49,7 @@ struct TcArgs {
   int64_t rows_per_split;
   double* gpart;
   unsigned* status;
+  int bulk;  // row arrays 16-byte aligned: full chunks arrive by cp.async.bulk
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -92,6 +93,18 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
     if (done) return true;
   }
   return false;
+}
+
+// 1-D bulk async copy global -> this CTA's shared memory, completing on `bar`
+// (no multicast). dst, src 16-byte aligned; bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
 }
 
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -162,8 +175,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
   float* w_s = d_s + kKC * a.k;                                  // kKC
   int2* up_s = reinterpret_cast<int2*>(w_s + kKC);               // kBM
   int2* vp_s = up_s + kBM;                                       // BN
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(vp_s + BN + (BN & 1));
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(vp_s + BN + (BN & 1));  // [0,1] MMA stages, [2,3] row loads
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 4);
+  // Raw rows of a chunk as stored in global memory, two buffers (16-byte aligned).
+  const uint32_t raw_bn = kKC * a.nc * 8, raw_d = kKC * a.k * 8, raw_w = kKC * 8, raw_v = kKC;
+  const uint32_t raw_bytes = raw_bn + raw_d + raw_w + raw_v;
+  unsigned char* raw_base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(tmem_slot + 4) + 15) & ~static_cast<uintptr_t>(15));
   __shared__ int s_fail;
 
   for (int m = tid; m < kBM; m += blockDim.x) up_s[m] = (u0 + m < a.Mu) ? a.upairs[u0 + m] : make_int2(-1, -1);
@@ -172,6 +190,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
     s_fail = 0;
     mbar_init(&mbar[0], 1);
     mbar_init(&mbar[1], 1);
+    mbar_init(&mbar[2], 1);
+    mbar_init(&mbar[3], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (tid < 32) {
@@ -187,6 +207,28 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
   const uint32_t idesc = umma_idesc_bf16(kBM, BN);
   constexpr uint32_t kLBO = 128, kSBO = (kKC / 8) * 128;
 
+  // Chunk c of this split is bulk-loaded when it is full and the rows are aligned.
+  auto chunk_rows = [&](int c) {
+    const int64_t left = rend - (rbeg + static_cast<int64_t>(c) * kKC);
+    return static_cast<int>(left < kKC ? left : kKC);
+  };
+  auto issue_rows = [&](int c) {  // by one thread
+    const int64_t r0 = rbeg + static_cast<int64_t>(c) * kKC;
+    unsigned char* dst = raw_base + (c & 1) * raw_bytes;
+    uint64_t* bar = &mbar[2 + (c & 1)];
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(bar, raw_bytes);
+    bulk_g2s(dst, a.R.bn + r0 * a.nc, raw_bn, bar);
+    bulk_g2s(dst + raw_bn, a.R.d + r0 * a.k, raw_d, bar);
+    bulk_g2s(dst + raw_bn + raw_d, a.R.w + r0, raw_w, bar);
+    bulk_g2s(dst + raw_bn + raw_d + raw_w, a.R.valid + r0, raw_v, bar);
+  };
+  int ld_hi = -1, ld_done = -1;  // highest chunk whose rows were bulk-requested / waited (uniform)
+  if (nchunks > 0 && a.bulk && chunk_rows(0) == kKC) {
+    ld_hi = 0;
+    if (tid == 0) issue_rows(0);
+  }
+
   int issued = 0;  // chunks whose MMAs were issued (uniform over the CTA)
   for (int c = 0; c < nchunks; ++c) {
     const int st = c & 1;
@@ -195,23 +237,50 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
     unsigned char* bhi = b_base + st * b_bytes;
     unsigned char* blo = b_base + (2 + st) * b_bytes;
     const int64_t r0 = rbeg + static_cast<int64_t>(c) * kKC;
-    // Stage the chunk's rows (the previous chunk's generation finished at the last barrier).
+    const int rows = chunk_rows(c);
+    const bool bulk_c = a.bulk && rows == kKC;
+    // Next chunk's rows fly in while this one is generated (its buffer was
+    // last read two chunks ago, before the last barrier).
+    if (c + 1 < nchunks && a.bulk && chunk_rows(c + 1) == kKC) {
+      ld_hi = c + 1;
+      if (tid == 0) issue_rows(c + 1);
+    }
+    const unsigned char* raw = raw_base + st * raw_bytes;
+    if (bulk_c) {
+      if (mbar_wait(&mbar[2 + st], static_cast<unsigned>(c >> 1) & 1u))
+        ld_done = c;
+      else
+        s_fail = 1;
+      __syncthreads();
+      if (s_fail) break;
+    }
+    const double* rbn = reinterpret_cast<const double*>(raw);
+    const double* rd = reinterpret_cast<const double*>(raw + raw_bn);
+    const double* rw = reinterpret_cast<const double*>(raw + raw_bn + raw_d);
+    const uint8_t* rv = raw + raw_bn + raw_d + raw_w;
+    // Stage the chunk's rows as FP32 (the previous chunk's generation finished at the last barrier).
     for (int e = tid; e < kKC * nf; e += blockDim.x) {
       const int r = e / nf, q = e - r * nf;
-      const int64_t row = r0 + r;
       float v = 0.0f;
-      if (row < rend) v = q < a.nc ? static_cast<float>(a.R.bn[row * a.nc + q]) : 1.0f;
+      if (r < rows) {
+        if (q < a.nc) v = static_cast<float>(bulk_c ? rbn[r * a.nc + q] : a.R.bn[(r0 + r) * a.nc + q]);
+        else v = 1.0f;
+      }
       bn_s[e] = v;
     }
     for (int e = tid; e < kKC * a.k; e += blockDim.x) {
       const int r = e / a.k, q = e - r * a.k;
-      const int64_t row = r0 + r;
-      d_s[e] = row < rend ? static_cast<float>(a.R.d[row * a.k + q]) : 0.0f;
+      d_s[e] = r < rows ? static_cast<float>(bulk_c ? rd[r * a.k + q] : a.R.d[(r0 + r) * a.k + q]) : 0.0f;
     }
     for (int r = tid; r < kKC; r += blockDim.x) {
       const int64_t row = r0 + r;
-      const bool act = row < rend && a.R.valid[row] && a.accepted[row / a.SS];
-      w_s[r] = act ? static_cast<float>(a.R.w[row]) : 0.0f;
+      bool act = false;
+      double wv = 0.0;
+      if (r < rows) {
+        act = (bulk_c ? rv[r] : a.R.valid[row]) && a.accepted[row / a.SS];
+        wv = bulk_c ? rw[r] : a.R.w[row];
+      }
+      w_s[r] = act ? static_cast<float>(wv) : 0.0f;
     }
     // The MMAs of chunk c-2 read this stage: wait for their commit.
     if (c >= 2 && !mbar_wait(&mbar[st], static_cast<unsigned>((c - 2) >> 1) & 1u)) s_fail = 1;
@@ -269,6 +338,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
   bool ok = !s_fail;
   for (int c = max(0, issued - 2); c < issued; ++c)
     if (!mbar_wait(&mbar[c & 1], static_cast<unsigned>(c >> 1) & 1u)) ok = false;
+  // Row loads still in flight (only after an early exit): wait for them too.
+  for (int c = ld_done + 1; c <= ld_hi; ++c)
+    if (!mbar_wait(&mbar[2 + (c & 1)], static_cast<unsigned>(c >> 1) & 1u)) ok = false;
   __syncthreads();
   if (!ok && tid == 0) atomicOr(a.status, kStatusLoopLimit);
   tc_fence_after();
@@ -312,7 +384,8 @@ size_t normal_tc_smem(int nc, int k, int BN) {
   size_t s = 4 * a_bytes + 4 * b_bytes;
   s += sizeof(float) * (static_cast<size_t>(kKC) * (nc + 1) + static_cast<size_t>(kKC) * k + kKC);
   s += sizeof(int2) * (kBM + BN + (BN & 1));
-  s = (s + 7) / 8 * 8 + 2 * sizeof(uint64_t) + 16;
+  s = (s + 7) / 8 * 8 + 4 * sizeof(uint64_t) + 16;
+  s += 16 + 2 * (static_cast<size_t>(kKC) * (nc + k + 1) * 8 + kKC);  // aligned raw row buffers
   return s;
 }
 
@@ -349,6 +422,9 @@ int launch_normal_tc(Context& c, int64_t N, int nc, int k, int SS, const FitRows
   a.rows_per_split = rps;
   a.gpart = gpart;
   a.status = c.d_status;
+  auto al16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+  a.bulk = al16(R.bn) && al16(R.d) && al16(R.w) && al16(R.valid) && (static_cast<size_t>(kKC) * nc * 8) % 16 == 0 &&
+           (static_cast<size_t>(kKC) * k * 8) % 16 == 0;
   ensure_dynamic_smem(reinterpret_cast<const void*>(k_normal_tc), smem);
   k_normal_tc<<<dim3(tiles_m, tiles_n, nsplit), kThreads, smem, c.stream>>>(a);
   DGPU_LAUNCH("k_normal_tc");
