@@ -104,6 +104,114 @@ __device__ void smem_fft(float2* x, int L, int m, int logm, const float2* tw, in
   }
 }
 
+// ---------------------------------------------------------------------------
+// Four-step FFT of lines of length N = 16 * N2 (N = 128 or 256): pass A does a
+// 16-point DFT in registers over the stride-N2 samples of each residue n2,
+// multiplies by W_N^(n2 k1) and writes a padded k1-major layout; pass B does the
+// N2-point DFT in registers and writes natural order. Two shared-memory round
+// trips per line instead of log2(N) + 1. tw[k] = W_N^k for k < N/2 (the sign
+// of W selects forward or inverse); lines need ls >= N + 17; 256 threads.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int bitrev_c(int i, int bits) {
+  int r = 0;
+  for (int b = 0; b < bits; ++b) r |= ((i >> b) & 1) << (bits - 1 - b);
+  return r;
+}
+
+template <int M, int LOGM>
+__device__ __forceinline__ void reg_fft(float2 (&v)[M], const float2* tw, int tstride) {
+#pragma unroll
+  for (int i = 0; i < M; ++i) {
+    const int r = bitrev_c(i, LOGM);
+    if (i < r) {
+      const float2 t = v[i];
+      v[i] = v[r];
+      v[r] = t;
+    }
+  }
+#pragma unroll
+  for (int half = 1; half < M; half <<= 1) {
+#pragma unroll
+    for (int j = 0; j < M / 2; ++j) {
+      const int pos = j & (half - 1);
+      const int i0 = ((j - pos) << 1) + pos, i1 = i0 + half;
+      const float2 w = tw[pos * (M / (2 * half)) * tstride];
+      const float2 a = v[i0];
+      const float2 c = cmul(v[i1], w);
+      v[i0] = cadd(a, c);
+      v[i1] = csub(a, c);
+    }
+  }
+}
+
+template <int N>
+__device__ void fft_lines_4step(float2* x, int L, int ls, const float2* tw) {
+  constexpr int N1 = 16, N2 = N / 16;
+  constexpr int LOGN2 = N == 256 ? 4 : 3;
+  constexpr int kLinesA = 256 / N2, kLinesB = 256 / N1;
+  for (int l0 = 0; l0 < L; l0 += kLinesA) {
+    const int line = l0 + threadIdx.x / N2, n2 = threadIdx.x % N2;
+    const bool act = line < L;
+    float2 v[N1];
+    if (act) {
+      float2* xl = x + line * ls;
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) v[n1] = xl[N2 * n1 + n2];
+      reg_fft<N1, 4>(v, tw, N2);
+#pragma unroll
+      for (int k1 = 1; k1 < N1; ++k1) {
+        const int m = n2 * k1;
+        float2 w = tw[m < N / 2 ? m : m - N / 2];
+        if (m >= N / 2) w = make_float2(-w.x, -w.y);
+        v[k1] = cmul(v[k1], w);
+      }
+    }
+    __syncthreads();
+    if (act) {
+      float2* xl = x + line * ls;
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) xl[k1 * (N2 + 1) + n2] = v[k1];
+    }
+    __syncthreads();
+  }
+  for (int l0 = 0; l0 < L; l0 += kLinesB) {
+    const int line = l0 + threadIdx.x / N1, k1 = threadIdx.x % N1;
+    const bool act = line < L;
+    float2 u[N2];
+    if (act) {
+      const float2* xl = x + line * ls;
+#pragma unroll
+      for (int n2 = 0; n2 < N2; ++n2) u[n2] = xl[k1 * (N2 + 1) + n2];
+      reg_fft<N2, LOGN2>(u, tw, N1);
+    }
+    __syncthreads();
+    if (act) {
+      float2* xl = x + line * ls;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) xl[k1 + N1 * k2] = u[k2];
+    }
+    __syncthreads();
+  }
+}
+
+// Line stride for an FFT of length m: room for the four-step layout where it
+// applies (odd in float2 units past a multiple of 16, so transposed column
+// accesses stay on distinct banks).
+__host__ __device__ __forceinline__ int fft_ls(int m, bool transposed) {
+  if (m == 128 || m == 256) return m + 17;
+  return transposed ? m + 1 : m;
+}
+
+// Dispatch: four-step for 128 / 256, radix-2 otherwise.
+__device__ __forceinline__ void fft_lines(float2* x, int L, int m, int logm, const float2* tw, int ls) {
+  if (m == 256)
+    fft_lines_4step<256>(x, L, ls, tw);
+  else if (m == 128)
+    fft_lines_4step<128>(x, L, ls, tw);
+  else
+    smem_fft(x, L, m, logm, tw, ls);
+}
+
 __device__ __forceinline__ int reflect_clamp(int s, int len) {
   if (s < 0) s = -s - 1;
   if (s >= len) s = 2 * len - s - 1;
@@ -120,8 +228,9 @@ k_rows_fwd(FftGeom G, int mode, const float* __restrict__ src, int w, int h, con
   extern __shared__ __align__(16) float2 fsm2[];
   const int n = G.n, hn = n / 2, nb = hn + 1;
   const int rows = G.rows_per_cta;
-  float2* z = fsm2;                 // rows x hn
-  float2* tw = z + rows * hn;       // hn/2 (length-hn FFT)
+  const int zl = fft_ls(hn, false);
+  float2* z = fsm2;                 // rows x zl
+  float2* tw = z + rows * zl;       // hn/2 (length-hn FFT)
   float2* twn = tw + hn / 2 + 1;    // hn (W^k, k < hn + 1) for the split
   const int item = blockIdx.x, r0 = blockIdx.y * rows;
   if (G.tw_tab) {
@@ -154,14 +263,14 @@ k_rows_fwd(FftGeom G, int mode, const float* __restrict__ src, int w, int h, con
       a = srow[2 * j];
       b = srow[2 * j + 1];
     }
-    z[e] = make_float2(a, b);
+    z[rr * zl + j] = make_float2(a, b);
   }
   __syncthreads();
-  smem_fft(z, rows, hn, G.logn - 1, tw, hn);
+  fft_lines(z, rows, hn, G.logn - 1, tw, zl);
   for (int e = threadIdx.x; e < rows * nb; e += blockDim.x) {
     const int rr = e / nb, k = e - rr * nb;
-    const float2 zk = z[rr * hn + (k % hn)];
-    const float2 zc = cconj(z[rr * hn + ((hn - k) % hn)]);
+    const float2 zk = z[rr * zl + (k % hn)];
+    const float2 zc = cconj(z[rr * zl + ((hn - k) % hn)]);
     const float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
     const float2 d = csub(zk, zc);                         // 2i O
     const float2 od = make_float2(0.5f * d.y, -0.5f * d.x);  // O = d / (2i)
@@ -180,7 +289,7 @@ k_cols(FftGeom G, int mode, float2* __restrict__ spec, const double* __restrict_
   extern __shared__ __align__(16) float2 fsm2[];
   const int n = G.n, nb = n / 2 + 1;
   const int C = G.cols_per_cta;
-  const int ls = n + 1;        // padded column-line stride (bank-conflict free transposes)
+  const int ls = fft_ls(n, true);  // padded column-line stride (bank-conflict free transposes)
   float2* x = fsm2;            // C x ls
   float2* tw = x + C * ls;     // n/2
   const int item = blockIdx.x, c0 = blockIdx.y * C;
@@ -199,7 +308,7 @@ k_cols(FftGeom G, int mode, float2* __restrict__ spec, const double* __restrict_
       x[cc * ls + row] = cc < ncol ? sp[static_cast<size_t>(row) * nb + c0 + cc] : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    smem_fft(x, C, n, G.logn, tw, ls);
+    fft_lines(x, C, n, G.logn, tw, ls);
   }
   if (mode == 1) {
     for (int e = threadIdx.x; e < C * n; e += blockDim.x) {
@@ -231,7 +340,7 @@ k_cols(FftGeom G, int mode, float2* __restrict__ spec, const double* __restrict_
   else
     make_twiddles(tw, n, +1);
   __syncthreads();
-  smem_fft(x, C, n, G.logn, tw, ls);
+  fft_lines(x, C, n, G.logn, tw, ls);
   for (int e = threadIdx.x; e < C * n; e += blockDim.x) {
     const int row = e / C, cc = e - row * C;
     if (cc < ncol) sp[static_cast<size_t>(row) * nb + c0 + cc] = x[cc * ls + row];
@@ -251,8 +360,9 @@ k_rows_inv(FftGeom G, int mode, const float2* __restrict__ spec, const int* __re
   extern __shared__ __align__(16) float2 fsm2[];
   const int n = G.n, hn = n / 2, nb = hn + 1;
   const int rows = G.rows_per_cta;
+  const int zl = fft_ls(hn, false);
   float2* z = fsm2;
-  float2* tw = z + rows * hn;
+  float2* tw = z + rows * zl;
   float2* twn = tw + hn / 2 + 1;
   const int item = mode == 0 ? items[blockIdx.x] : blockIdx.x;
   const int r0 = blockIdx.y * rows;
@@ -280,15 +390,15 @@ k_rows_inv(FftGeom G, int mode, const float2* __restrict__ spec, const int* __re
     }
     const float2 e2 = cadd(xk, xc);
     const float2 o2 = cmul(csub(xk, xc), twn[k]);
-    z[e] = make_float2(e2.x - o2.y, e2.y + o2.x);  // 2E + i 2O
+    z[rr * zl + k] = make_float2(e2.x - o2.y, e2.y + o2.x);  // 2E + i 2O
   }
   __syncthreads();
-  smem_fft(z, rows, hn, G.logn - 1, tw, hn);
+  fft_lines(z, rows, hn, G.logn - 1, tw, zl);
   const float inv_n2 = 1.0f / static_cast<float>(static_cast<size_t>(n) * n);
   if (mode == 2) {  // raw real block output for the overlap-add gather (dense_out: item x n x n)
     for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
       const int rr = e / n, m = e - rr * n;
-      const float2 v = z[rr * hn + (m >> 1)];
+      const float2 v = z[rr * zl + (m >> 1)];
       dense_out[(static_cast<size_t>(item) * n + r0 + rr) * n + m] = (m & 1) ? v.y : v.x;
     }
     return;
@@ -296,7 +406,7 @@ k_rows_inv(FftGeom G, int mode, const float2* __restrict__ spec, const int* __re
   if (mode == 1) {
     for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
       const int rr = e / n, m = e - rr * n;
-      const float2 v = z[rr * hn + (m >> 1)];
+      const float2 v = z[rr * zl + (m >> 1)];
       dense_out[(static_cast<size_t>(item) * n + r0 + rr) * n + m] = ((m & 1) ? v.y : v.x) * inv_n2;
     }
     return;
@@ -311,7 +421,7 @@ k_rows_inv(FftGeom G, int mode, const float2* __restrict__ spec, const int* __re
     const int iy = r0 + rr;
     const int y = by + iy, x = bx + m;
     if (y < 0 || y >= h || x < 0 || x >= w) continue;
-    const float2 v = z[rr * hn + (m >> 1)];
+    const float2 v = z[rr * zl + (m >> 1)];
     const float f = (m & 1) ? v.y : v.x;
     const double wy_sig = hwin[iy] * static_cast<double>(inv_n2);
     const double wy_var = hwin[iy];
@@ -346,25 +456,30 @@ k_ola_gather(int w, int h, int n, const int* __restrict__ oxs, int nox, const in
     int iyh = min(y / max(s, 1), noy - 1);
     while (iyh + 1 < noy && oys[iyh + 1] <= y) ++iyh;
     while (iyh > 0 && oys[iyh] > y) --iyh;
-    int slot[9];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) slot[q] = -1;
-    for (int ix = ixh; ix >= 0 && ix > ixh - 3 && oxs[ix] + n > x; --ix)
-      for (int iy = iyh; iy >= 0 && iy > iyh - 3 && oys[iy] + n > y; --iy) slot[(ix % 3) * 3 + (iy % 3)] = iy * nox + ix;
+    // Covering origins form the index ranges [ixl, ixh] x [iyl, iyh] (at most 3
+    // each, so at most one index per residue mod 3).
+    int ixl = ixh, iyl = iyh;
+    while (ixl > 0 && ixl > ixh - 2 && oxs[ixl - 1] + n > x) --ixl;
+    while (iyl > 0 && iyl > iyh - 2 && oys[iyl - 1] + n > y) --iyl;
     float a = 0.0f, v = 0.0f;
 #pragma unroll
-    for (int q = 0; q < 9; ++q) {
-      const int item = slot[q];
-      if (item < 0) continue;
-      const int bx = oxs[item % nox], by = oys[item / nox];
-      const int ly = y - by, lx = x - bx;
-      const float f = bout[(static_cast<size_t>(item) * n + ly) * n + lx];
-      const double num = bnum[item];
-      const double wy_sig = hwin[ly] * inv_n2;
-      const double wy_var = hwin[ly];
-      const double wxv = hwin[lx];
-      a = static_cast<float>(static_cast<double>(a) + wy_sig * wxv * static_cast<double>(f));
-      v = static_cast<float>(static_cast<double>(v) + wy_var * wxv * num);
+    for (int ca = 0; ca < 3; ++ca) {  // colour q = (ix % 3) * 3 + (iy % 3), ascending
+      const int ix = ixh - (((ixh - ca) % 3) + 3) % 3;
+      if (ix < ixl) continue;
+#pragma unroll
+      for (int cb = 0; cb < 3; ++cb) {
+        const int iy = iyh - (((iyh - cb) % 3) + 3) % 3;
+        if (iy < iyl) continue;
+        const int item = iy * nox + ix;
+        const int ly = y - oys[iy], lx = x - oxs[ix];
+        const float f = bout[(static_cast<size_t>(item) * n + ly) * n + lx];
+        const double num = bnum[item];
+        const double wy_sig = hwin[ly] * inv_n2;
+        const double wy_var = hwin[ly];
+        const double wxv = hwin[lx];
+        a = static_cast<float>(static_cast<double>(a) + wy_sig * wxv * static_cast<double>(f));
+        v = static_cast<float>(static_cast<double>(v) + wy_var * wxv * num);
+      }
     }
     const double ws = wy_total[y] * wx_total[x];
     if (ws > 0.0) {
@@ -548,10 +663,10 @@ __global__ void k_ola_normalise(int w, int h, const double* __restrict__ wx_tota
 // ---------------------------------------------------------------------------
 static size_t rows_smem(const FftGeom& g) {
   const int hn = g.n / 2;
-  return sizeof(float2) * (static_cast<size_t>(g.rows_per_cta) * hn + hn / 2 + 1 + hn + 1);
+  return sizeof(float2) * (static_cast<size_t>(g.rows_per_cta) * fft_ls(hn, false) + hn / 2 + 1 + hn + 1);
 }
 static size_t cols_smem(const FftGeom& g) {
-  return sizeof(float2) * (static_cast<size_t>(g.cols_per_cta) * (g.n + 1) + g.n / 2 + 1);
+  return sizeof(float2) * (static_cast<size_t>(g.cols_per_cta) * fft_ls(g.n, true) + g.n / 2 + 1);
 }
 
 size_t twiddle_table_len(int n) { return static_cast<size_t>(n) + n / 2 + 2 * (n / 2 + 1); }
