@@ -543,7 +543,9 @@ int dgpu_matched_filter(dgpu_context* ctx, int mem, int64_t width, int64_t heigh
     DGPU_CUDA(cudaMemcpyAsync(dpsf, psf, sizeof(float) * psf_size * psf_size, cudaMemcpyHostToDevice, c.stream));
     {
       StageTimer t(c, "score: blocked correlation");
-      launch_matched_filter(c.stream, w, h, img, var, psf, dpsf, psf_size, sumpsf2, o);
+      const size_t ntiles = static_cast<size_t>((w + 63) / 64) * ((h + 31) / 32);
+      int* nf_buf = static_cast<int*>(c.slot(kSlotScratch0, sizeof(int) * (ntiles + 1)));
+      launch_matched_filter(c.stream, w, h, img, var, psf, dpsf, psf_size, sumpsf2, o, nf_buf);
     }
     stage_out(c, mem, out, o, 4 * n);
     if (mem == DGPU_MEM_HOST) check_status(c);

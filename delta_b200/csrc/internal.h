@@ -227,7 +227,7 @@ void launch_strided_median(Context& c, int kind, int64_t n, const float* values,
 
 void launch_matched_filter(cudaStream_t s, int w, int h, const float* img, const float* var,
                            const float* psf_host, const float* psf_dev, int ps, float sumpsf2,
-                           float* out);
+                           float* out, int* nf_buf);
 
 void launch_basis_convolve(cudaStream_t s, int w, int h, const float* img, const Basis& b,
                            const float* taps, float* out);

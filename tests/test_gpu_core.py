@@ -204,6 +204,26 @@ def test_matched_filter_bit_exact(h, w, ps):
     np.testing.assert_allclose(got, nr.matched_filter(img, psf, var), atol=1e-4)
 
 
+@pytest.mark.parametrize("ps", [17, 23])
+def test_matched_filter_non_finite_tiles_bit_exact(ps):
+    """Tiles holding NaN / Inf keep the reference's zero-tap skip (a zero tap
+    never touches a non-finite pixel); all other tiles take the fast path."""
+    h, w = 300, 270
+    rng = np.random.default_rng(ps)
+    img = rng.standard_normal((h, w)).astype(np.float32) * 10
+    img[rng.integers(0, h, 25), rng.integers(0, w, 25)] = np.nan
+    img[rng.integers(0, h, 5), rng.integers(0, w, 5)] = np.inf
+    var = rng.uniform(0.5, 3.0, (h, w)).astype(np.float32)
+    r = ps // 2
+    yy, xx = np.mgrid[-r : r + 1, -r : r + 1]
+    psf = np.exp(-(xx**2 + yy**2) / (2 * 1.7**2))
+    psf = np.clip(psf / psf.sum() - 1e-4, 0, None).astype(np.float32)
+    got = _core.matched_filter(img, psf, var)
+    want = cref.matched_filter(img, psf, var)
+    assert np.array_equal(got, want, equal_nan=True)
+    assert np.isnan(got).any() and np.isfinite(got).any()
+
+
 def test_matched_filter_peak_known_answer():
     h = w = 64
     r = 6
