@@ -360,6 +360,7 @@ void launch_model_convolve_orders(cudaStream_t s, const SubtractArgs& a, const i
 // ---------------------------------------------------------------------------
 
 constexpr int kVarB = 64;
+constexpr int kVarMaxRk = 64;
 
 __global__ void __launch_bounds__(256)
 k_variance(int w, int h, DevFields F, const float* __restrict__ phi, int rk, int nc,
@@ -374,7 +375,7 @@ k_variance(int w, int h, DevFields F, const float* __restrict__ phi, int rk, int
   float* win = k1 + kk;                               // iw * iw
   float* an = win + iw * iw;                          // nc
   __shared__ double s_qsum;
-  __shared__ int s_hw;
+  __shared__ double s_box[kVarMaxRk];
   __shared__ float s_min[8], s_max[8];
   const int tid = threadIdx.x;
   const int bx = blockIdx.x * kVarB, by = blockIdx.y * kVarB;
@@ -392,39 +393,27 @@ k_variance(int w, int h, DevFields F, const float* __restrict__ phi, int rk, int
       kf[kk - 1 - i] = k2 * k2;
     }
     __syncthreads();
-    if (tid == 0) {
-      // qsum = sum_i double(K_i) * double(K_i) in index order (exact squares).
+    // Warp 1, lane 0: qsum = sum_i double(K_i)^2 in index order (the squares
+    // are exact in double). Warp 0: lane L sums the centred box of half-width
+    // L (and L + 32) in row-major order. The other warps gather the window
+    // meanwhile; every thread picks the first box reaching the target after
+    // the barrier below.
+    if (tid == 32) {
       double q = 0.0;
       for (int i = 0; i < kk; ++i) q = fma(static_cast<double>(k1[i]), static_cast<double>(k1[i]), q);
       s_qsum = q;
-    }
-    __syncthreads();
-    // Box shrink: lane L of warp 0 tests half-width L; the first box that
-    // reaches the target wins. Each box is summed in the reference's row-major
-    // order.
-    if (tid < 32) {
-      const double target = (1.0 - static_cast<double>(1e-4f)) * s_qsum;
-      int found = rk;
-      for (int base = 0; base < rk; base += 32) {
-        const int hw = base + tid;
-        bool ok = false;
-        if (hw < rk) {
-          double box = 0.0;
-          const int lo = rk - hw, hi = rk + hw;
-          for (int yy = lo; yy <= hi; ++yy)
-            for (int xx = lo; xx <= hi; ++xx) box += static_cast<double>(kf[yy * ks + xx]);
-          ok = box >= target;
-        }
-        const unsigned bal = __ballot_sync(0xffffffffu, ok);
-        if (bal) {
-          found = base + __ffs(bal) - 1;
-          break;
-        }
+    } else if (tid < 32) {
+      for (int hw = tid; hw < rk; hw += 32) {
+        double box = 0.0;
+        const int lo = rk - hw, hi = rk + hw;
+        for (int yy = lo; yy <= hi; ++yy)
+          for (int xx = lo; xx <= hi; ++xx) box += static_cast<double>(kf[yy * ks + xx]);
+        s_box[hw] = box;
       }
-      if (tid == 0) s_hw = found;
     }
-    // Gather the zero-padded window and its min / max.
+    // Gather the zero-padded window, its min / max and whether it is all finite.
     float lmin = INFINITY, lmax = -INFINITY;
+    int finite = 1;
     const int iwh = bh + 2 * rk, iww = bw + 2 * rk;
     for (int i = tid; i < iwh * iww; i += blockDim.x) {
       const int r = i / iww, c = i - r * iww;
@@ -433,6 +422,7 @@ k_variance(int w, int h, DevFields F, const float* __restrict__ phi, int rk, int
       win[r * iw + c] = v;
       lmin = fminf(lmin, v);
       lmax = fmaxf(lmax, v);
+      finite &= isfinite(v) ? 1 : 0;
     }
     for (int o = 16; o > 0; o >>= 1) {
       lmin = fminf(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
@@ -442,37 +432,76 @@ k_variance(int w, int h, DevFields F, const float* __restrict__ phi, int rk, int
       s_min[tid >> 5] = lmin;
       s_max[tid >> 5] = lmax;
     }
-    __syncthreads();
+    // A zero tap adds an exact +-0 to a sum that is never -0 when the window is
+    // finite, so the reference's zero-tap skip only matters otherwise.
+    const bool all_finite = __syncthreads_and(finite) != 0;
     float wmin = s_min[0], wmax = s_max[0];
     for (int i = 1; i < (int)(blockDim.x >> 5); ++i) {
       wmin = fminf(wmin, s_min[i]);
       wmax = fmaxf(wmax, s_max[i]);
     }
-    const int hw = s_hw;
+    int hw = rk;
+    {
+      const double target = (1.0 - static_cast<double>(1e-4f)) * s_qsum;
+      for (int b = 0; b < rk; ++b)
+        if (s_box[b] >= target) {
+          hw = b;
+          break;
+        }
+    }
     const bool flat = wmax > 0.0f && (wmax - wmin) <= 1e-3f * wmax;
     const float q = static_cast<float>(s_qsum);
     const int lo = rk - hw, hi = rk + hw;
-    for (int p = tid; p < bw * bh; p += blockDim.x) {
-      const int oy = p / bw, ox = p - oy * bw;
-      float v;
-      if (flat) {
-        v = q * win[(oy + rk) * iw + ox + rk];
-      } else {
-        float acc = 0.0f;
-        for (int ly = lo; ly <= hi; ++ly) {
-          const float* wr = win + (oy + ly) * iw + ox;
-          const float* kr = kf + ly * ks;
-          for (int lx2 = lo; lx2 <= hi; ++lx2) {
-            const float c = kr[lx2];
-            if (c == 0.0f) continue;
-            acc = __fmaf_rn(c, wr[lx2], acc);
+    // 4 x 4 outputs per thread: rows oy0 .. oy0+3, columns tx + 16 j (strided,
+    // so a warp's window loads hit distinct banks). Per output the taps are
+    // still accumulated in (ly, lx) order.
+    const int tx = tid & 15, oy0 = (tid >> 4) * 4;
+    float acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+    if (flat) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = q * win[(oy0 + i + rk) * iw + tx + 16 * j + rk];
+    } else {
+      for (int r = 0; r <= 3 + 2 * hw; ++r) {
+        const float* wrp = win + (oy0 + lo + r) * iw + tx;
+        for (int lx = lo; lx <= hi; ++lx) {
+          float v[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) v[j] = wrp[16 * j + lx];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int ly = lo + r - i;
+            if (ly < lo || ly > hi) continue;
+            const float c = kf[ly * ks + lx];
+            if (!all_finite && c == 0.0f) continue;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = __fmaf_rn(c, v[j], acc[i][j]);
           }
         }
-        v = 0.0f + acc;
       }
-      const size_t o = static_cast<size_t>(by + oy) * w + bx + ox;
-      if (var_s) v = v + __ldg(var_s + o);
-      var_out[o] = v;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f + acc[i][j];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int oy = oy0 + i;
+      if (oy >= bh) continue;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int ox = tx + 16 * j;
+        if (ox >= bw) continue;
+        const size_t o = static_cast<size_t>(by + oy) * w + bx + ox;
+        float v = acc[i][j];
+        if (var_s) v = v + __ldg(var_s + o);
+        var_out[o] = v;
+      }
     }
   } else {
     for (int p = tid; p < bw * bh; p += blockDim.x) {
@@ -488,7 +517,8 @@ void launch_variance(cudaStream_t s, int w, int h, const DevFields& F, const flo
   const int ks = 2 * rk + 1;
   const int iw = kVarB + 2 * rk;
   const size_t smem = sizeof(float) * (2 * static_cast<size_t>(ks) * ks + static_cast<size_t>(iw) * iw + nc + 4);
-  if (smem > 200 * 1024) fail(DGPU_ERR_INVALID, "subtract: kernel radius too large for the variance engine");
+  if (smem > 200 * 1024 || rk > kVarMaxRk)
+    fail(DGPU_ERR_INVALID, "subtract: kernel radius too large for the variance engine");
   ensure_dynamic_smem(reinterpret_cast<const void*>(k_variance), smem);
   dim3 grid(ceil_div(w, kVarB), ceil_div(h, kVarB));
   k_variance<<<grid, 256, smem, s>>>(w, h, F, phi, rk, nc, var_s, var_r, var_out);
