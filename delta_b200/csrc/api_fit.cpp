@@ -97,17 +97,13 @@ struct Engine {
 
   // Workspace for up to `nsys` systems sharing the solver batch.
   struct Work {
-    double *A, *Linv, *theta, *edf, *raw, *rss, *gcv, *lam;
+    double *A, *theta, *edf, *raw, *rss, *gcv, *lam;
     int *ok, *midx, *ridx;
     double* partial;
   };
   Work work(int nsys) {
-    const int Pp = solve_pp(P);
-    const size_t mat = static_cast<size_t>(Pp) * Pp;
     Work w{};
-    char* big = static_cast<char*>(c.slot(kSlotFft0, sizeof(double) * 2 * mat * nsys));
-    w.A = reinterpret_cast<double*>(big);
-    w.Linv = w.A + mat * nsys;
+    w.A = static_cast<double*>(c.slot(kSlotFft0, sizeof(double) * solve_sys_doubles(P, nf, rk) * nsys));
     const size_t small = sizeof(double) * (static_cast<size_t>(nsys) * P + 6 * nsys) + sizeof(int) * 3 * nsys + 64;
     char* sm = static_cast<char*>(c.slot(kSlotFft1, small));
     w.theta = reinterpret_cast<double*>(sm);
@@ -138,7 +134,6 @@ struct Engine {
     b.pen = d_pen;
     b.fk = d_fk;
     b.A = w.A;
-    b.Linv = w.Linv;
     b.theta = w.theta;
     b.edf = w.edf;
     b.ok = w.ok;
@@ -153,7 +148,7 @@ struct Engine {
     b.k = k;
     b.nf = nf;
     b.r = rk;
-    b.Linv = w.Linv;
+    b.A = w.A;
     return b;
   }
 

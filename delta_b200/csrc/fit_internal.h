@@ -49,10 +49,9 @@ void launch_reweight(cudaStream_t st, const StampGeom& g, int n_stamps, const Tp
 
 // ---------------------------------------------------------------------------
 // Batched penalised GLS: for each system s of a batch, A_s = M_s + lam_s P0
-// (P0 = blockdiag of the k x k penalty), Cholesky A_s = L L^T, L^{-1},
-// theta_s = A_s^{-1} rhs_s, edf_s = P - lam_s ||L^{-1} F||_F^2 and, when
-// requested, the held-out error of a CV fold. One cluster launch, one
-// thread-block cluster per system.
+// (P0 = blockdiag of the k x k penalty), Cholesky A_s = L L^T,
+// theta_s = A_s^{-1} rhs_s and edf_s = P - lam_s ||L^{-1} F||_F^2. One cluster
+// launch, one thread-block cluster per system.
 // ---------------------------------------------------------------------------
 struct SolveBatch {
   int P = 0, k = 0, nf = 0, r = 0;  // unknowns, knots, fields, rank of the penalty
@@ -64,17 +63,21 @@ struct SolveBatch {
   const double* lam = nullptr;      // nsys
   const double* pen = nullptr;      // k x k
   const double* fk = nullptr;       // k x r half factor of the penalty
-  double* A = nullptr;              // nsys x Pp x Pp workspace (L in the lower tiles)
-  double* Linv = nullptr;           // nsys x Pp x Pp
+  // nsys x solve_sys_doubles workspace: per system L in the lower tiles of a
+  // Pp x Pp matrix, the Ep x Pp appended rows [rhs^T; F^T], and the nb
+  // inverses of L's 32 x 32 diagonal tiles.
+  double* A = nullptr;
   double* theta = nullptr;          // nsys x P
   double* edf = nullptr;            // nsys
   int* ok = nullptr;                // nsys: 1 if the Cholesky succeeded
   unsigned* status = nullptr;
   double* partial = nullptr;        // nsys x 8 per-rank trace partials
 };
-int solve_pp(int P);  // padded size
+int solve_pp(int P);                               // padded size
+int solve_ep(int nf, int r);                       // appended rows, padded
+size_t solve_sys_doubles(int P, int nf, int r);    // workspace per system
 void launch_solve_batch(Context& c, const SolveBatch& b);
-// Apply a system's inverse: out = A_s^{-1} v (uses the Linv of system s).
+// Apply a system's inverse: out = A_s^{-1} v (from the factor tiles of system s).
 void launch_apply_inverse(cudaStream_t st, const SolveBatch& b, int s, const double* v, double* out);
 
 }  // namespace dgpu
