@@ -101,9 +101,9 @@ struct Engine {
     int *ok, *midx, *ridx;
     double* partial;
   };
-  Work work(int nsys) {
+  Work work(int nsys, int nm = 1) {
     Work w{};
-    w.A = static_cast<double*>(c.slot(kSlotFft0, sizeof(double) * solve_sys_doubles(P, nf, rk) * nsys));
+    w.A = static_cast<double*>(c.slot(kSlotFft0, sizeof(double) * solve_work_doubles(P, nf, rk, nsys, nm)));
     const size_t small = sizeof(double) * (static_cast<size_t>(nsys) * P + 6 * nsys) + sizeof(int) * 3 * nsys + 64;
     char* sm = static_cast<char*>(c.slot(kSlotFft1, small));
     w.theta = reinterpret_cast<double*>(sm);
@@ -119,7 +119,8 @@ struct Engine {
     return w;
   }
 
-  void solve(const Work& w, int nsys, const double* M, const int* midx, const double* rhs, const int* ridx) {
+  void solve(const Work& w, int nsys, const double* M, const int* midx, const double* rhs, const int* ridx,
+             int nm = 1) {
     SolveBatch b;
     b.P = P;
     b.k = k;
@@ -128,6 +129,7 @@ struct Engine {
     b.nsys = nsys;
     b.M = M;
     b.m_index = midx;
+    b.nm = nm;
     b.rhs = rhs;
     b.r_index = ridx;
     b.lam = w.lam;
@@ -300,7 +302,7 @@ struct Engine {
     }
     std::vector<double> curve(nl, kInf);
     std::vector<char> done(nl, 0);
-    Work w = work(std::max(nl * G, 1));
+    Work w = work(std::max(nl * G, 1), G);
     auto evaluate = [&](const std::vector<int>& idx) {
       const int m = static_cast<int>(idx.size());
       const int ns = m * G;
@@ -313,7 +315,7 @@ struct Engine {
         }
       DGPU_CUDA(cudaMemcpyAsync(w.lam, lam.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, c.stream));
       DGPU_CUDA(cudaMemcpyAsync(w.midx, mi.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, c.stream));
-      solve(w, ns, Mt, w.midx, rt, w.midx);
+      solve(w, ns, Mt, w.midx, rt, w.midx, G);
       launch_quad_err(c, ns, P, w.theta, Mg, w.midx, rg, w.midx, yg, w.raw);
       const auto err = down(c, w.raw, ns);
       const auto ok = down(c, w.ok, ns);

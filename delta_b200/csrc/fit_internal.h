@@ -58,14 +58,15 @@ struct SolveBatch {
   int nsys = 0;
   const double* M = nullptr;        // nsys_m x P x P (system s uses M + m_index[s]*P*P)
   const int* m_index = nullptr;     // per system (nullptr -> 0)
+  int nm = 1;                       // number of distinct M (m_index values 0 .. nm-1)
   const double* rhs = nullptr;      // per system rhs (rhs + r_index[s]*P)
   const int* r_index = nullptr;
   const double* lam = nullptr;      // nsys
   const double* pen = nullptr;      // k x k
   const double* fk = nullptr;       // k x r half factor of the penalty
-  // nsys x solve_sys_doubles workspace: per system L in the lower tiles of a
-  // Pp x Pp matrix, the Ep x Pp appended rows [rhs^T; F^T], and the nb
-  // inverses of L's 32 x 32 diagonal tiles.
+  // solve_work_doubles workspace (tile-major): per system L's lower tiles,
+  // the appended rows [rhs^T; F^T], the inverses of L's diagonal tiles; then
+  // each distinct M converted to tiles.
   double* A = nullptr;
   double* theta = nullptr;          // nsys x P
   double* edf = nullptr;            // nsys
@@ -76,6 +77,7 @@ struct SolveBatch {
 int solve_pp(int P);                               // padded size
 int solve_ep(int nf, int r);                       // appended rows, padded
 size_t solve_sys_doubles(int P, int nf, int r);    // workspace per system
+size_t solve_work_doubles(int P, int nf, int r, int nsys, int nm);
 void launch_solve_batch(Context& c, const SolveBatch& b);
 // Apply a system's inverse: out = A_s^{-1} v (from the factor tiles of system s).
 void launch_apply_inverse(cudaStream_t st, const SolveBatch& b, int s, const double* v, double* out);
