@@ -117,6 +117,7 @@ void dgpu_destroy(dgpu_context* ctx) {
   for (int i = 0; i < kSlotCount; ++i)
     if (c->slot_ptr[i]) cudaFree(c->slot_ptr[i]);
   if (c->d_status) cudaFree(c->d_status);
+  if (c->host_stage) cudaFreeHost(c->host_stage);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }

@@ -40,6 +40,39 @@ std::vector<T> down(Context& c, const T* dev, size_t n) {
   return h;
 }
 
+// Batched device -> host reads: every add() queues an async copy into the
+// context's pinned staging area; run() synchronises the stream once and
+// scatters the bytes to their host destinations.
+class Fetch {
+ public:
+  Fetch(Context& c, size_t max_bytes) : c_(c), cap_(max_bytes + 16 * kMaxItems), base_(c.host_staging(cap_)) {}
+  template <class T>
+  void add(T* host, const T* dev, size_t n) {
+    const size_t bytes = sizeof(T) * n;
+    off_ = (off_ + 15) & ~static_cast<size_t>(15);
+    if (off_ + bytes > cap_ || items_.size() >= kMaxItems) fail(DGPU_ERR_RUNTIME, "fetch: staging overflow");
+    if (n) DGPU_CUDA(cudaMemcpyAsync(base_ + off_, dev, bytes, cudaMemcpyDeviceToHost, c_.stream));
+    items_.push_back({host, off_, bytes});
+    off_ += bytes;
+  }
+  void run() {
+    DGPU_CUDA(cudaStreamSynchronize(c_.stream));
+    for (const Item& it : items_) std::memcpy(it.host, base_ + it.off, it.bytes);
+  }
+
+ private:
+  static constexpr size_t kMaxItems = 16;
+  struct Item {
+    void* host;
+    size_t off, bytes;
+  };
+  Context& c_;
+  size_t cap_;
+  unsigned char* base_;
+  size_t off_ = 0;
+  std::vector<Item> items_;
+};
+
 double median_copy(std::vector<double> v) {
   if (v.empty()) return kNaN;
   const size_t mid = v.size() / 2;
@@ -50,6 +83,7 @@ double median_copy(std::vector<double> v) {
 struct GlsOut {
   std::vector<double> theta;
   double lambda = 0, gcv = 0, edf = 0, rss = 0;
+  long long npix = 0;  // active rows of the fit
   std::vector<double> grid, curve;
   const double* d_theta = nullptr;  // device copy of theta
 };
@@ -206,12 +240,16 @@ struct Engine {
       launch_quad_err(c, 1, P, th, M, nullptr, rhs, nullptr, ywy, w.raw + s);
       launch_gcv_finish(c.stream, 1, w.raw + s, w.edf + s, w.ok + s, n, w.rss + s, w.gcv + s);
     }
-    o.theta = down(c, th, P);
+    o.theta.resize(P);
+    Fetch f(c, sizeof(double) * (P + 4));
+    f.add(o.theta.data(), th, P);
+    f.add(&o.edf, w.edf + s, 1);
+    f.add(&o.rss, w.rss + s, 1);
+    f.add(&o.gcv, w.gcv + s, 1);
+    f.add(&o.npix, n, 1);
+    f.run();
     o.d_theta = th;
     o.lambda = lam;
-    o.edf = down(c, w.edf + s, 1)[0];
-    o.rss = down(c, w.rss + s, 1)[0];
-    o.gcv = down(c, w.gcv + s, 1)[0];
   }
 
   // Fixed-lambda solve (src/solve.cpp:208-215).
@@ -607,26 +645,26 @@ int dgpu_fit_kernel(dgpu_context* ctx, int mem, int64_t width, int64_t height, c
 
     for (int iter = 0;; ++iter) {
       DGPU_CUDA(cudaMemcpyAsync(d_acc, accepted.data(), n_stamps, cudaMemcpyHostToDevice, st));
-      {
-        double* scratch = static_cast<double*>(c.slot(kSlotFit15, sizeof(double) * (2 * E.P + 4)));
-        long long* nn = reinterpret_cast<long long*>(scratch + 2 * E.P + 1);
-        launch_rhs(c, N, nc, k, g.SS, E.R, d_acc, nullptr, scratch, scratch + 2 * E.P, nn);
-        npix = down(c, nn, 1)[0];
-      }
-      if (npix == 0) fail(DGPU_ERR_RUNTIME, "fit_kernel: all stamp pixels clipped");
+      // The active-row count comes back with the solve (the rows are the same).
       if (cv_folds > 1) {
         std::vector<int> fold(n_stamps, -1);
         for (int s = 0; s < n_stamps; ++s)
           if (comp_of[s] >= 0) fold[s] = comp_of[s] % cv_folds;
         gls = E.cv(grid, d_acc, fold, cv_folds, warm_start, use_stamped);
-        if (!use_stamped) cv_exact_bytes = static_cast<size_t>(npix) * E.P * sizeof(double);
         warm_start = static_cast<int>(std::min_element(gls.curve.begin(), gls.curve.end()) - gls.curve.begin());
       } else {
         gls = E.gcv(grid, d_acc);
       }
+      npix = gls.npix;
+      if (npix == 0) fail(DGPU_ERR_RUNTIME, "fit_kernel: all stamp pixels clipped");
+      if (cv_folds > 1 && !use_stamped) cv_exact_bytes = static_cast<size_t>(npix) * E.P * sizeof(double);
       launch_stamp_chi2(st, n_stamps, nc, k, g.SS, E.R, d_acc, gls.d_theta, chi2_d, cnt_d);
-      stamp_chi2 = down(c, chi2_d, n_stamps);
-      cnt = down(c, cnt_d, n_stamps);
+      {
+        Fetch f(c, (sizeof(double) + sizeof(int)) * n_stamps);
+        f.add(stamp_chi2.data(), chi2_d, n_stamps);
+        f.add(cnt.data(), cnt_d, n_stamps);
+        f.run();
+      }
       const double denom = static_cast<double>(npix) - gls.edf;
       reduced = denom > 0.0 ? gls.rss / denom : kNaN;
       if (have_var) {

@@ -88,7 +88,13 @@ struct Context {
   int cat_count = 0;
   int64_t cat_npix = 0;         // label image size of the last catalog
 
+  // Pinned host staging for batched device -> host reads (grows; never
+  // shrinks).
+  unsigned char* host_stage = nullptr;
+  size_t host_stage_size = 0;
+
   void* slot(Slot s, size_t bytes);
+  unsigned char* host_staging(size_t bytes);
 };
 
 // RAII: clear the status word at entry, check it (after a sync) at exit.

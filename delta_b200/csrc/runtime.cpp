@@ -9,6 +9,8 @@
 #include <cstdlib>
 #include <stdexcept>
 
+#include <algorithm>
+
 #include "internal.h"
 
 namespace dgpu {
@@ -34,6 +36,23 @@ void* Context::slot(Slot s, size_t bytes) {
   DGPU_CUDA(cudaMalloc(&slot_ptr[s], want));
   slot_size[s] = want;
   return slot_ptr[s];
+}
+
+unsigned char* Context::host_staging(size_t bytes) {
+  if (host_stage_size >= bytes) return host_stage;
+  // Growing: copies queued on the stream may still target the old buffer.
+  if (host_stage) {
+    DGPU_CUDA(cudaStreamSynchronize(stream));
+    DGPU_CUDA(cudaFreeHost(host_stage));
+    host_stage = nullptr;
+    host_stage_size = 0;
+  }
+  const size_t want = std::max<size_t>(bytes + bytes / 8 + 256, 1 << 16);
+  void* p = nullptr;
+  DGPU_CUDA(cudaHostAlloc(&p, want, cudaHostAllocDefault));
+  host_stage = static_cast<unsigned char*>(p);
+  host_stage_size = want;
+  return host_stage;
 }
 
 void reset_status(Context& c) { DGPU_CUDA(cudaMemsetAsync(c.d_status, 0, sizeof(unsigned), c.stream)); }
