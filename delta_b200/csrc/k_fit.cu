@@ -460,6 +460,157 @@ k_rhs(int64_t N, int nc, int k, int SS, FitRows R, const uint8_t* __restrict__ a
   }
 }
 
+// The same sums on the FP64 tensor cores (mma.sync m8n8k4) for nc + 1 <= 32
+// fields and k <= 8 KT: a warp streams 32-row blocks. Refinement: the model
+// terms x_i . theta of 8 rows at a time are one product of the rows' design
+// values with theta (held in registers as B fragments), contracted with the
+// rows' b values and reduced over the 4 lanes that share a row. The sums
+// out[c][m] += sum_i (w_i e_i b_ic) d_im are a product with the rows as the
+// inner dimension, 4 rows per step. Rows that are not active contribute
+// exact zeros (their values are never multiplied). Each CTA adds its warps'
+// sums in warp order.
+__device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+template <int KT>
+__global__ void __launch_bounds__(256)
+k_rhs_mma(int64_t N, int nc, int k, int SS, FitRows R, const uint8_t* __restrict__ accepted,
+          const double* __restrict__ theta, int64_t blocks_per_cta, double* __restrict__ rpart,
+          double* __restrict__ ypart, long long* __restrict__ npart) {
+  constexpr int KS = 2 * KT;  // 4-wide steps over the design values
+  __shared__ double s_we[8][32];
+  __shared__ double s_model[8][32];
+  __shared__ double s_y[8];
+  __shared__ long long s_n[8];
+  extern __shared__ double red[];  // 8 x P
+  const int nf = nc + 1, P = nf * k;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, q = lane >> 2, kq = lane & 3;
+  double bt[4][KS];
+#pragma unroll
+  for (int n = 0; n < 4; ++n)
+#pragma unroll
+    for (int ks = 0; ks < KS; ++ks) {
+      const int c = 8 * n + q, m = 4 * ks + kq;
+      bt[n][ks] = (theta != nullptr && c < nf && m < k) ? theta[c * k + m] : 0.0;
+    }
+  double acc[4][KT][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < KT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  double yacc = 0.0;
+  long long nacc = 0;
+  const int64_t nblk = (N + 31) / 32;
+  const int64_t b0 = static_cast<int64_t>(blockIdx.x) * blocks_per_cta;
+  const int64_t b1 = min(nblk, b0 + blocks_per_cta);
+  for (int64_t blk = b0 + warp; blk < b1; blk += 8) {
+    const int64_t r0 = blk * 32;
+    const int64_t row = r0 + lane;
+    const bool act = row < N && R.valid[row] && accepted[row / SS];
+    double t = 0.0, wv = 0.0;
+    if (act) {
+      t = R.t[row];
+      wv = R.w[row];
+      yacc = fma(wv * t, t, yacc);
+      ++nacc;
+    }
+    if (theta != nullptr) {
+#pragma unroll
+      for (int rt = 0; rt < 4; ++rt) {
+        const int64_t mr = r0 + rt * 8 + q;
+        const bool in = mr < N;
+        double qa[4][2];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) qa[n][0] = qa[n][1] = 0.0;
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks) {
+          const int m = 4 * ks + kq;
+          const double a = (in && m < k) ? R.d[mr * k + m] : 0.0;
+#pragma unroll
+          for (int n = 0; n < 4; ++n) dmma_884(qa[n], a, bt[n][ks]);
+        }
+        double part = 0.0;
+#pragma unroll
+        for (int n = 0; n < 4; ++n)
+#pragma unroll
+          for (int i = 0; i < 2; ++i) {
+            const int c = 8 * n + 2 * kq + i;
+            const double b = !in ? 0.0 : (c < nc ? R.bn[mr * nc + c] : (c == nc ? 1.0 : 0.0));
+            part = fma(b, qa[n][i], part);
+          }
+        part += __shfl_xor_sync(0xffffffffu, part, 1);
+        part += __shfl_xor_sync(0xffffffffu, part, 2);
+        if (kq == 0) s_model[warp][rt * 8 + q] = part;
+      }
+      __syncwarp();
+      if (act) t = t - s_model[warp][lane];
+    }
+    s_we[warp][lane] = act ? wv * t : 0.0;
+    __syncwarp();
+#pragma unroll 2
+    for (int ks = 0; ks < 8; ++ks) {
+      const int rl = 4 * ks + kq;
+      const int64_t ar = r0 + rl;
+      const double we = s_we[warp][rl];
+      const bool live = we != 0.0;
+      double a[4], bb[KT];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int c = 8 * i + q;
+        a[i] = !live ? 0.0 : we * (c < nc ? R.bn[ar * nc + c] : (c == nc ? 1.0 : 0.0));
+      }
+#pragma unroll
+      for (int j = 0; j < KT; ++j) {
+        const int m = 8 * j + q;
+        bb[j] = (live && m < k) ? R.d[ar * k + m] : 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < KT; ++j) dmma_884(acc[i][j], a[i], bb[j]);
+    }
+    __syncwarp();
+  }
+  // Warp sums into shared memory, then added over the warps in order.
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < KT; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int c = 8 * i + q, m = 8 * j + 2 * kq + e;
+        if (c < nf && m < k) red[warp * P + c * k + m] = acc[i][j][e];
+      }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    yacc += __shfl_xor_sync(0xffffffffu, yacc, o);
+    nacc += __shfl_xor_sync(0xffffffffu, nacc, o);
+  }
+  if (lane == 0) {
+    s_y[warp] = yacc;
+    s_n[warp] = nacc;
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < P; p += blockDim.x) {
+    double v = 0.0;
+    for (int w2 = 0; w2 < 8; ++w2) v += red[w2 * P + p];
+    rpart[static_cast<size_t>(blockIdx.x) * P + p] = v;
+  }
+  if (threadIdx.x == 0) {
+    double y = 0.0;
+    long long n = 0;
+    for (int w2 = 0; w2 < 8; ++w2) {
+      y += s_y[w2];
+      n += s_n[w2];
+    }
+    ypart[blockIdx.x] = y;
+    npart[blockIdx.x] = n;
+  }
+}
+
 __global__ void __launch_bounds__(256)
 k_reduce_rhs(int nsplit, int P, const double* __restrict__ rpart, const double* __restrict__ ypart,
              const long long* __restrict__ npart, double* __restrict__ rhs, double* ywy, long long* n) {
@@ -495,18 +646,40 @@ void launch_rhs(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, 
   cudaStream_t st = c.stream;
   const int P = (nc + 1) * k;
   if (P > 1024) fail(DGPU_ERR_INVALID, "fit: more than 1024 unknowns is not supported");
-  int64_t rps = std::max<int64_t>(kRhsRows * 2, (N + 148 * 2 - 1) / (148 * 2));
-  rps = (rps + kRhsRows - 1) / kRhsRows * kRhsRows;
-  const int nsplit = static_cast<int>(std::max<int64_t>(1, (N + rps - 1) / rps));
+  const bool mma = nc + 1 <= 32 && k <= 32;
+  int nsplit;
+  int64_t rps = 0, bpc = 0;
+  if (mma) {
+    // 16 row blocks of 32 per CTA: two per warp.
+    const int64_t nblk = (N + 31) / 32;
+    bpc = 16;
+    nsplit = static_cast<int>(std::max<int64_t>(1, (nblk + bpc - 1) / bpc));
+  } else {
+    rps = std::max<int64_t>(kRhsRows * 2, (N + 148 * 2 - 1) / (148 * 2));
+    rps = (rps + kRhsRows - 1) / kRhsRows * kRhsRows;
+    nsplit = static_cast<int>(std::max<int64_t>(1, (N + rps - 1) / rps));
+  }
   char* buf = static_cast<char*>(c.slot(kSlotFit13, (sizeof(double) * (P + 1) + sizeof(long long)) * nsplit + 64));
   double* rpart = reinterpret_cast<double*>(buf);
   double* ypart = rpart + static_cast<size_t>(nsplit) * P;
   long long* npart = reinterpret_cast<long long*>(ypart + nsplit);
-  const size_t smem =
-      sizeof(double) * (kRhsRows * (nc + 1) + kRhsRows * k + 2 * kRhsRows + P) + sizeof(int) * kRhsRows;
-  ensure_dynamic_smem(reinterpret_cast<const void*>(k_rhs), smem);
-  k_rhs<<<nsplit, 256, smem, st>>>(N, nc, k, SS, R, accepted, theta, rps, rpart, ypart, npart);
-  DGPU_LAUNCH("k_rhs");
+  if (mma) {
+    const size_t smem = sizeof(double) * 8 * static_cast<size_t>(P);
+    if (k <= 16) {
+      ensure_dynamic_smem(reinterpret_cast<const void*>(k_rhs_mma<2>), smem);
+      k_rhs_mma<2><<<nsplit, 256, smem, st>>>(N, nc, k, SS, R, accepted, theta, bpc, rpart, ypart, npart);
+    } else {
+      ensure_dynamic_smem(reinterpret_cast<const void*>(k_rhs_mma<4>), smem);
+      k_rhs_mma<4><<<nsplit, 256, smem, st>>>(N, nc, k, SS, R, accepted, theta, bpc, rpart, ypart, npart);
+    }
+    DGPU_LAUNCH("k_rhs_mma");
+  } else {
+    const size_t smem =
+        sizeof(double) * (kRhsRows * (nc + 1) + kRhsRows * k + 2 * kRhsRows + P) + sizeof(int) * kRhsRows;
+    ensure_dynamic_smem(reinterpret_cast<const void*>(k_rhs), smem);
+    k_rhs<<<nsplit, 256, smem, st>>>(N, nc, k, SS, R, accepted, theta, rps, rpart, ypart, npart);
+    DGPU_LAUNCH("k_rhs");
+  }
   k_reduce_rhs<<<(P + 31) / 32, 256, 0, st>>>(nsplit, P, rpart, ypart, npart, rhs, ywy, n);
   DGPU_LAUNCH("k_reduce_rhs");
 }
