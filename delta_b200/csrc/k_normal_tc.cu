@@ -32,7 +32,8 @@ namespace {
 
 constexpr int kBM = 128;       // u rows per tile (UMMA M)
 constexpr int kKC = 64;        // stamp rows per chunk (4 UMMA K-steps of 16)
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;
+constexpr int kRS = kKC + 4;  // staged row-value stride (floats): rows contiguous, banks staggered
 constexpr long long kSpinCap = 1ll << 22;
 
 struct TcArgs {
@@ -143,14 +144,17 @@ __device__ __forceinline__ uint32_t canon_off(int row, int kg) {
   return static_cast<uint32_t>(((row >> 3) * (kKC / 8) + kg) * 128 + (row & 7) * 16);
 }
 
+// x = hi + lo, both bf16 (hi = rn(x), lo = rn(x - hi)), eight values per
+// call as packed pairs; one 16-byte store per half.
 __device__ __forceinline__ void split_store(unsigned char* hi_base, unsigned char* lo_base, uint32_t off,
                                             const float (&v)[8]) {
-  __align__(16) __nv_bfloat16 h[8];
-  __align__(16) __nv_bfloat16 l[8];
+  __align__(16) __nv_bfloat162 h[4];
+  __align__(16) __nv_bfloat162 l[4];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    h[j] = __float2bfloat16_rn(v[j]);
-    l[j] = __float2bfloat16_rn(v[j] - __bfloat162float(h[j]));
+  for (int j = 0; j < 4; ++j) {
+    h[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+    const float2 hf = __bfloat1622float2(h[j]);
+    l[j] = __floats2bfloat162_rn(v[2 * j] - hf.x, v[2 * j + 1] - hf.y);
   }
   *reinterpret_cast<uint4*>(hi_base + off) = *reinterpret_cast<const uint4*>(h);
   *reinterpret_cast<uint4*>(lo_base + off) = *reinterpret_cast<const uint4*>(l);
@@ -170,10 +174,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
   const uint32_t a_bytes = kBM * kKC * 2, b_bytes = static_cast<uint32_t>(BN) * kKC * 2;
   // stage st: A hi at st*a_bytes, A lo at (2+st)*a_bytes; B hi / lo likewise after the A buffers
   unsigned char* b_base = smem + 4 * a_bytes;
-  float* bn_s = reinterpret_cast<float*>(b_base + 4 * b_bytes);  // kKC x nf
-  float* d_s = bn_s + kKC * nf;                                  // kKC x k
-  float* w_s = d_s + kKC * a.k;                                  // kKC
-  int2* up_s = reinterpret_cast<int2*>(w_s + kKC);               // kBM
+  // Staged chunk, value-major: bnT[q][r] = b_q of row r (b_nc = 1),
+  // dT[m][r] = d_m, wdT[m][r] = w_r d_m (w_r = 0 for inactive rows).
+  float* bnT = reinterpret_cast<float*>(b_base + 4 * b_bytes);  // nf x kRS
+  float* dT = bnT + nf * kRS;                                    // k x kRS
+  float* wdT = dT + a.k * kRS;                                   // k x kRS
+  int2* up_s = reinterpret_cast<int2*>(wdT + a.k * kRS);         // kBM
   int2* vp_s = up_s + kBM;                                       // BN
   uint64_t* mbar = reinterpret_cast<uint64_t*>(vp_s + BN + (BN & 1));  // [0,1] MMA stages, [2,3] row loads
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 4);
@@ -258,29 +264,28 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
     const double* rd = reinterpret_cast<const double*>(raw + raw_bn);
     const double* rw = reinterpret_cast<const double*>(raw + raw_bn + raw_d);
     const uint8_t* rv = raw + raw_bn + raw_d + raw_w;
-    // Stage the chunk's rows as FP32 (the previous chunk's generation finished at the last barrier).
-    for (int e = tid; e < kKC * nf; e += blockDim.x) {
-      const int r = e / nf, q = e - r * nf;
-      float v = 0.0f;
-      if (r < rows) {
-        if (q < a.nc) v = static_cast<float>(bulk_c ? rbn[r * a.nc + q] : a.R.bn[(r0 + r) * a.nc + q]);
-        else v = 1.0f;
-      }
-      bn_s[e] = v;
-    }
-    for (int e = tid; e < kKC * a.k; e += blockDim.x) {
-      const int r = e / a.k, q = e - r * a.k;
-      d_s[e] = r < rows ? static_cast<float>(bulk_c ? rd[r * a.k + q] : a.R.d[(r0 + r) * a.k + q]) : 0.0f;
-    }
-    for (int r = tid; r < kKC; r += blockDim.x) {
+    // Stage the chunk's rows as FP32, value-major (the previous chunk's
+    // generation finished at the last barrier): thread (row r, group g)
+    // converts the values q = g, g + 8, ... of row r.
+    {
+      const int r = tid & (kKC - 1), g = tid >> 6, ng = blockDim.x >> 6;
       const int64_t row = r0 + r;
-      bool act = false;
-      double wv = 0.0;
-      if (r < rows) {
-        act = (bulk_c ? rv[r] : a.R.valid[row]) && a.accepted[row / a.SS];
-        wv = bulk_c ? rw[r] : a.R.w[row];
+      const bool in = r < rows;
+      float wr = 0.0f;
+      if (in) {
+        const bool act = (bulk_c ? rv[r] : a.R.valid[row]) && a.accepted[row / a.SS];
+        if (act) wr = static_cast<float>(bulk_c ? rw[r] : a.R.w[row]);
       }
-      w_s[r] = act ? static_cast<float>(wv) : 0.0f;
+      for (int q = g; q < nf; q += ng) {
+        float v = 0.0f;
+        if (in) v = q < a.nc ? static_cast<float>(bulk_c ? rbn[r * a.nc + q] : a.R.bn[row * a.nc + q]) : 1.0f;
+        bnT[q * kRS + r] = v;
+      }
+      for (int q = g; q < a.k; q += ng) {
+        const float dv = in ? static_cast<float>(bulk_c ? rd[r * a.k + q] : a.R.d[row * a.k + q]) : 0.0f;
+        dT[q * kRS + r] = dv;
+        wdT[q * kRS + r] = wr * dv;
+      }
     }
     // The MMAs of chunk c-2 read this stage: wait for their commit.
     if (c >= 2 && !mbar_wait(&mbar[st], static_cast<unsigned>((c - 2) >> 1) & 1u)) s_fail = 1;
@@ -293,24 +298,33 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
       const int kg = (item >> 3) % (kKC / 8);
       const int2 p = up_s[m];
       float v[8];
+      if (p.x >= 0) {
+        const float4* x = reinterpret_cast<const float4*>(bnT + p.x * kRS + kg * 8);
+        const float4* y = reinterpret_cast<const float4*>(bnT + p.y * kRS + kg * 8);
+        const float4 x0 = x[0], x1 = x[1], y0 = y[0], y1 = y[1];
+        v[0] = x0.x * y0.x; v[1] = x0.y * y0.y; v[2] = x0.z * y0.z; v[3] = x0.w * y0.w;
+        v[4] = x1.x * y1.x; v[5] = x1.y * y1.y; v[6] = x1.z * y1.z; v[7] = x1.w * y1.w;
+      } else {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const float* b = bn_s + (kg * 8 + j) * nf;
-        v[j] = p.x >= 0 ? b[p.x] * b[p.y] : 0.0f;
+        for (int j = 0; j < 8; ++j) v[j] = 0.0f;
       }
       split_store(ahi, alo, canon_off(m, kg), v);
     }
-    // B = V tile (BN x kKC).
+    // B = V tile (BN x kKC): (w d_m) d_m'.
     for (int item = tid; item < BN * (kKC / 8); item += blockDim.x) {
       const int n = (item & 7) + ((item >> 3) / (kKC / 8)) * 8;
       const int kg = (item >> 3) % (kKC / 8);
       const int2 q = vp_s[n];
       float v[8];
+      if (q.x >= 0) {
+        const float4* x = reinterpret_cast<const float4*>(wdT + q.x * kRS + kg * 8);
+        const float4* y = reinterpret_cast<const float4*>(dT + q.y * kRS + kg * 8);
+        const float4 x0 = x[0], x1 = x[1], y0 = y[0], y1 = y[1];
+        v[0] = x0.x * y0.x; v[1] = x0.y * y0.y; v[2] = x0.z * y0.z; v[3] = x0.w * y0.w;
+        v[4] = x1.x * y1.x; v[5] = x1.y * y1.y; v[6] = x1.z * y1.z; v[7] = x1.w * y1.w;
+      } else {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int r = kg * 8 + j;
-        const float* d = d_s + r * a.k;
-        v[j] = q.x >= 0 ? (w_s[r] * d[q.x]) * d[q.y] : 0.0f;
+        for (int j = 0; j < 8; ++j) v[j] = 0.0f;
       }
       split_store(bhi, blo, canon_off(n, kg), v);
     }
@@ -345,15 +359,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
   if (!ok && tid == 0) atomicOr(a.status, kStatusLoopLimit);
   tc_fence_after();
 
-  // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (tile rows), the two
+  // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (tile rows); the
   // warp groups split the column blocks of 16.
   const int warp = tid >> 5, lane = tid & 31;
-  const int quarter = warp & 3, half = warp >> 2;
+  const int quarter = warp & 3, grp = warp >> 2, ngrp = (blockDim.x >> 5) / 4;
   const int m = quarter * 32 + lane;
   const int u = u0 + m;
-  const int ncb = BN / 16, mid = (ncb + 1) / 2;
+  const int ncb = BN / 16;
   double* out = a.gpart + static_cast<size_t>(blockIdx.z) * a.Mu * a.Nv;
-  for (int cb = half ? mid : 0; cb < (half ? ncb : mid); ++cb) {
+  for (int cb = grp; cb < ncb; cb += ngrp) {
     uint32_t r[16];
     if (issued > 0 && ok) {
       tmem_ld16(tmem + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(cb * 16), r);
@@ -382,7 +396,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
 size_t normal_tc_smem(int nc, int k, int BN) {
   const size_t a_bytes = static_cast<size_t>(kBM) * kKC * 2, b_bytes = static_cast<size_t>(BN) * kKC * 2;
   size_t s = 4 * a_bytes + 4 * b_bytes;
-  s += sizeof(float) * (static_cast<size_t>(kKC) * (nc + 1) + static_cast<size_t>(kKC) * k + kKC);
+  s += sizeof(float) * static_cast<size_t>(kRS) * ((nc + 1) + 2 * static_cast<size_t>(k));
   s += sizeof(int2) * (kBM + BN + (BN & 1));
   s = (s + 7) / 8 * 8 + 4 * sizeof(uint64_t) + 16;
   s += 16 + 2 * (static_cast<size_t>(kKC) * (nc + k + 1) * 8 + kKC);  // aligned raw row buffers
