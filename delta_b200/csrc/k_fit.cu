@@ -470,7 +470,7 @@ k_rhs(int64_t N, int nc, int k, int SS, FitRows R, const uint8_t* __restrict__ a
 // exact zeros (their values are never multiplied). Each CTA adds its warps'
 // sums in warp order.
 __device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
                : "+d"(d[0]), "+d"(d[1])
                : "d"(a), "d"(b));
 }
@@ -522,25 +522,32 @@ k_rhs_mma(int64_t N, int nc, int k, int SS, FitRows R, const uint8_t* __restrict
       for (int rt = 0; rt < 4; ++rt) {
         const int64_t mr = r0 + rt * 8 + q;
         const bool in = mr < N;
-        double qa[4][2];
-#pragma unroll
-        for (int n = 0; n < 4; ++n) qa[n][0] = qa[n][1] = 0.0;
+        // This row's design values and b values first (all loads in flight).
+        double dv[KS], bv[8];
 #pragma unroll
         for (int ks = 0; ks < KS; ++ks) {
           const int m = 4 * ks + kq;
-          const double a = (in && m < k) ? R.d[mr * k + m] : 0.0;
-#pragma unroll
-          for (int n = 0; n < 4; ++n) dmma_884(qa[n], a, bt[n][ks]);
+          dv[ks] = (in && m < k) ? R.d[mr * k + m] : 0.0;
         }
-        double part = 0.0;
 #pragma unroll
         for (int n = 0; n < 4; ++n)
 #pragma unroll
           for (int i = 0; i < 2; ++i) {
             const int c = 8 * n + 2 * kq + i;
-            const double b = !in ? 0.0 : (c < nc ? R.bn[mr * nc + c] : (c == nc ? 1.0 : 0.0));
-            part = fma(b, qa[n][i], part);
+            bv[2 * n + i] = !in ? 0.0 : (c < nc ? R.bn[mr * nc + c] : (c == nc ? 1.0 : 0.0));
           }
+        double qa[4][2];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) qa[n][0] = qa[n][1] = 0.0;
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks)
+#pragma unroll
+          for (int n = 0; n < 4; ++n) dmma_884(qa[n], dv[ks], bt[n][ks]);
+        double part = 0.0;
+#pragma unroll
+        for (int n = 0; n < 4; ++n)
+#pragma unroll
+          for (int i = 0; i < 2; ++i) part = fma(bv[2 * n + i], qa[n][i], part);
         part += __shfl_xor_sync(0xffffffffu, part, 1);
         part += __shfl_xor_sync(0xffffffffu, part, 2);
         if (kq == 0) s_model[warp][rt * 8 + q] = part;
@@ -550,27 +557,34 @@ k_rhs_mma(int64_t N, int nc, int k, int SS, FitRows R, const uint8_t* __restrict
     }
     s_we[warp][lane] = act ? wv * t : 0.0;
     __syncwarp();
-#pragma unroll 2
-    for (int ks = 0; ks < 8; ++ks) {
-      const int rl = 4 * ks + kq;
-      const int64_t ar = r0 + rl;
-      const double we = s_we[warp][rl];
-      const bool live = we != 0.0;
-      double a[4], bb[KT];
+    // Two 4-row steps per round: all eight operand loads of a round are in
+    // flight before its products.
+#pragma unroll 1
+    for (int ks0 = 0; ks0 < 8; ks0 += 2) {
+      double a[2][4], bb[2][KT];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int c = 8 * i + q;
-        a[i] = !live ? 0.0 : we * (c < nc ? R.bn[ar * nc + c] : (c == nc ? 1.0 : 0.0));
+      for (int u = 0; u < 2; ++u) {
+        const int rl = 4 * (ks0 + u) + kq;
+        const int64_t ar = r0 + rl;
+        const double we = s_we[warp][rl];
+        const bool live = we != 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int c = 8 * i + q;
+          a[u][i] = !live ? 0.0 : we * (c < nc ? R.bn[ar * nc + c] : (c == nc ? 1.0 : 0.0));
+        }
+#pragma unroll
+        for (int j = 0; j < KT; ++j) {
+          const int m = 8 * j + q;
+          bb[u][j] = (live && m < k) ? R.d[ar * k + m] : 0.0;
+        }
       }
 #pragma unroll
-      for (int j = 0; j < KT; ++j) {
-        const int m = 8 * j + q;
-        bb[j] = (live && m < k) ? R.d[ar * k + m] : 0.0;
-      }
+      for (int u = 0; u < 2; ++u)
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < KT; ++j) dmma_884(acc[i][j], a[i], bb[j]);
+          for (int j = 0; j < KT; ++j) dmma_884(acc[i][j], a[u][i], bb[u][j]);
     }
     __syncwarp();
   }

@@ -179,7 +179,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
   float* bnT = reinterpret_cast<float*>(b_base + 4 * b_bytes);  // nf x kRS
   float* dT = bnT + nf * kRS;                                    // k x kRS
   float* wdT = dT + a.k * kRS;                                   // k x kRS
-  int2* up_s = reinterpret_cast<int2*>(wdT + a.k * kRS);         // kBM
+  float* w_s = wdT + a.k * kRS;                                  // kKC row weights
+  int2* up_s = reinterpret_cast<int2*>(w_s + kKC);               // kBM
   int2* vp_s = up_s + kBM;                                       // BN
   uint64_t* mbar = reinterpret_cast<uint64_t*>(vp_s + BN + (BN & 1));  // [0,1] MMA stages, [2,3] row loads
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 4);
@@ -265,26 +266,41 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
     const double* rw = reinterpret_cast<const double*>(raw + raw_bn + raw_d);
     const uint8_t* rv = raw + raw_bn + raw_d + raw_w;
     // Stage the chunk's rows as FP32, value-major (the previous chunk's
-    // generation finished at the last barrier): thread (row r, group g)
-    // converts the values q = g, g + 8, ... of row r.
-    {
-      const int r = tid & (kKC - 1), g = tid >> 6, ng = blockDim.x >> 6;
+    // generation finished at the last barrier). Row weights first (0 for
+    // inactive rows); then thread (value q = lane, rows 4 g .. 4 g + 3)
+    // converts four rows of one value and stores them as one float4.
+    for (int r = tid; r < kKC; r += blockDim.x) {
       const int64_t row = r0 + r;
-      const bool in = r < rows;
       float wr = 0.0f;
-      if (in) {
-        const bool act = (bulk_c ? rv[r] : a.R.valid[row]) && a.accepted[row / a.SS];
-        if (act) wr = static_cast<float>(bulk_c ? rw[r] : a.R.w[row]);
-      }
-      for (int q = g; q < nf; q += ng) {
-        float v = 0.0f;
-        if (in) v = q < a.nc ? static_cast<float>(bulk_c ? rbn[r * a.nc + q] : a.R.bn[row * a.nc + q]) : 1.0f;
-        bnT[q * kRS + r] = v;
-      }
-      for (int q = g; q < a.k; q += ng) {
-        const float dv = in ? static_cast<float>(bulk_c ? rd[r * a.k + q] : a.R.d[row * a.k + q]) : 0.0f;
-        dT[q * kRS + r] = dv;
-        wdT[q * kRS + r] = wr * dv;
+      if (r < rows && (bulk_c ? rv[r] : a.R.valid[row]) && a.accepted[row / a.SS])
+        wr = static_cast<float>(bulk_c ? rw[r] : a.R.w[row]);
+      w_s[r] = wr;
+    }
+    __syncthreads();
+    {
+      const int lane = tid & 31, qmax = nf > a.k ? nf : a.k;
+      for (int g = tid >> 5; g < kKC / 4; g += blockDim.x >> 5) {
+        for (int q = lane; q < qmax; q += 32) {
+          float bv[4], dv[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int r = 4 * g + i;
+            const int64_t row = r0 + r;
+            const bool in = r < rows;
+            bv[i] = 0.0f;
+            dv[i] = 0.0f;
+            if (in && q < nf)
+              bv[i] = q < a.nc ? static_cast<float>(bulk_c ? rbn[r * a.nc + q] : a.R.bn[row * a.nc + q]) : 1.0f;
+            if (in && q < a.k) dv[i] = static_cast<float>(bulk_c ? rd[r * a.k + q] : a.R.d[row * a.k + q]);
+          }
+          if (q < nf) *reinterpret_cast<float4*>(bnT + q * kRS + 4 * g) = make_float4(bv[0], bv[1], bv[2], bv[3]);
+          if (q < a.k) {
+            const float4 w4 = *reinterpret_cast<const float4*>(w_s + 4 * g);
+            *reinterpret_cast<float4*>(dT + q * kRS + 4 * g) = make_float4(dv[0], dv[1], dv[2], dv[3]);
+            *reinterpret_cast<float4*>(wdT + q * kRS + 4 * g) =
+                make_float4(w4.x * dv[0], w4.y * dv[1], w4.z * dv[2], w4.w * dv[3]);
+          }
+        }
       }
     }
     // The MMAs of chunk c-2 read this stage: wait for their commit.
@@ -396,7 +412,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
 size_t normal_tc_smem(int nc, int k, int BN) {
   const size_t a_bytes = static_cast<size_t>(kBM) * kKC * 2, b_bytes = static_cast<size_t>(BN) * kKC * 2;
   size_t s = 4 * a_bytes + 4 * b_bytes;
-  s += sizeof(float) * static_cast<size_t>(kRS) * ((nc + 1) + 2 * static_cast<size_t>(k));
+  s += sizeof(float) * (static_cast<size_t>(kRS) * ((nc + 1) + 2 * static_cast<size_t>(k)) + kKC);
   s += sizeof(int2) * (kBM + BN + (BN & 1));
   s = (s + 7) / 8 * 8 + 4 * sizeof(uint64_t) + 16;
   s += 16 + 2 * (static_cast<size_t>(kKC) * (nc + k + 1) * 8 + kKC);  // aligned raw row buffers

@@ -695,9 +695,12 @@ void launch_solve_batch(Context& c, const SolveBatch& b) {
   DGPU_LAUNCH("k_solve_cluster");
 }
 
-// out = A_s^{-1} v = L^-T (L^-1 v) from system s's factor tiles, one CTA:
-// forward over the column tiles (y_i = Dinv_i y_i, then y_p -= L_pi y_i for
-// the rows below, a thread per row), then the back substitution of the solver.
+// out = A_s^{-1} v = L^-T (L^-1 v) from system s's factor tiles, one CTA.
+// The tiles are first pulled into L2 (one bulk prefetch per tile; streaming
+// kernels that ran since the solve may have evicted them). Forward over the
+// column tiles: y_i = Dinv_i y_i, then y_p -= L_pi y_i for the rows below (a
+// thread per row); backward: theta_i = Dinv_i^T y_i, then y_q -= L_iq^T
+// theta_i (a thread per column).
 constexpr int kAiThreads = 512;
 
 __global__ void __launch_bounds__(kAiThreads) k_apply_inverse(const double* __restrict__ A, const double* __restrict__ Dv,
@@ -706,7 +709,11 @@ __global__ void __launch_bounds__(kAiThreads) k_apply_inverse(const double* __re
   __shared__ double y[1024];
   __shared__ double dt[kT * (kT + 1)];
   const int tid = threadIdx.x, warp = tid >> 5, ln = tid & 31;
-  const int nb = Pp / kT;
+  const int nb = Pp / kT, na = nb * (nb + 1) / 2;
+  for (int u = tid; u < na + nb; u += blockDim.x) {
+    const double* tile = u < na ? A + static_cast<size_t>(u) * kTS : Dv + static_cast<size_t>(u - na) * kTS;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(tile), "r"(static_cast<unsigned>(kTS * 8)) : "memory");
+  }
   for (int q = tid; q < Pp; q += blockDim.x) y[q] = q < P ? vin[q] : 0.0;
   for (int i = 0; i < nb; ++i) {
     const double* D = Dv + static_cast<size_t>(i) * kTS;
