@@ -201,14 +201,18 @@ int dgpu_decorrelate(dgpu_context* ctx, int mem, int64_t width, int64_t height, 
     {
       StageTimer tm(c, "decorrelate: block filter+blend");
       launch_block_var(s, g, nblk, 0, vs, vr, w, h, d_oxs, d_oys, nox, vsr);
-      launch_rows_fwd(s, g, 0, nblk, D, w, h, d_oxs, d_oys, nox, spec);
       double* bnum = static_cast<double*>(c.slot(kSlotFft2, sizeof(double) * static_cast<size_t>(nblk)));
-      launch_cols(s, g, 0, nblk, spec, cell_power, cell_sumk2, d_bcell, vsr, bnum);
       // Raw c2r outputs of every block, then the overlap-add as a per-pixel gather
       // in the reference's colour order (same sums as 9 colour passes).
       float* bout = static_cast<float*>(c.slot(kSlotFft4, sizeof(float) * static_cast<size_t>(nblk) * n * n));
-      launch_rows_inv(s, g, 2, nblk, spec, nullptr, w, h, d_oxs, d_oys, nox, d_hw, vsr, cell_sumk2, d_bcell, nullptr,
-                      nullptr, bout);
+      if (block_filter_fused(g)) {
+        launch_block_filter(s, g, nblk, D, w, h, d_oxs, d_oys, nox, cell_power, cell_sumk2, d_bcell, vsr, bnum, bout);
+      } else {
+        launch_rows_fwd(s, g, 0, nblk, D, w, h, d_oxs, d_oys, nox, spec);
+        launch_cols(s, g, 0, nblk, spec, cell_power, cell_sumk2, d_bcell, vsr, bnum);
+        launch_rows_inv(s, g, 2, nblk, spec, nullptr, w, h, d_oxs, d_oys, nox, d_hw, vsr, cell_sumk2, d_bcell,
+                        nullptr, nullptr, bout);
+      }
     }
     {
       StageTimer tm(c, "decorrelate: normalise");

@@ -27,6 +27,12 @@ void launch_cols(cudaStream_t s, const FftGeom& g, int mode, int nitems, float2*
 void launch_rows_inv(cudaStream_t s, const FftGeom& g, int mode, int nitems, const float2* spec, const int* items,
                      int w, int h, const int* oxs, const int* oys, int nox, const double* hwin, const double* vsr,
                      const double* cell_sumk2, const int* block_cell, float* acc, float* var_acc, float* dense_out);
+// The three passes of mode 0 (r2c rows, filtered columns, raw c2r rows into
+// dense_out) fused per block in one cluster launch; needs n = 256 and tw_tab.
+bool block_filter_fused(const FftGeom& g);
+void launch_block_filter(cudaStream_t s, const FftGeom& g, int nitems, const float* src, int w, int h,
+                         const int* oxs, const int* oys, int nox, const double* cell_power, const double* cell_sumk2,
+                         const int* block_cell, const double* vsr, double* bnum, float* dense_out);
 void launch_block_var(cudaStream_t s, const FftGeom& g, int nitems, int nextra, const float* vs, const float* vr,
                       int w, int h, const int* oxs, const int* oys, int nox, double* vsr);
 void launch_local_kernels(cudaStream_t s, const FftGeom& g, int ncell, const TpsDev& t, const double* theta, int nc,

@@ -14,6 +14,7 @@
 // (ix % 3, iy % 3), so every pixel accumulates its blocks in the same order on
 // every run and no two blocks of one launch touch the same pixel.
 // FFTs are unnormalised radix-2 in shared memory with FP64-derived twiddles.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -23,6 +24,8 @@
 #include "fft_internal.h"
 
 namespace dgpu {
+
+namespace cg = cooperative_groups;
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -432,6 +435,160 @@ k_rows_inv(FftGeom G, int mode, const float2* __restrict__ spec, const int* __re
   }
 }
 
+// ---------------------------------------------------------------------------
+// Fused block filter for the default 256 x 256 block (mode 0 of the three
+// passes above, in one launch): one cluster of 4 CTAs per block. Rank r keeps
+// spectrum columns [cb_r, cb_r + 33 or 32) as transposed column lines in its
+// shared memory and runs the row passes of rows 64 r .. 64 r + 63. Row pass:
+// the r2c rows are scattered into the owners' column lines (distributed
+// shared memory); column pass: forward FFT, filter, inverse FFT on local
+// lines; row inverse: every row gathers its bins from the owners, c2r, raw
+// block output (item x n x n) for the overlap-add gather. The per-line
+// arithmetic is that of k_rows_fwd / k_cols / k_rows_inv, so the output is
+// the same; the spectrum never leaves the chip.
+// ---------------------------------------------------------------------------
+constexpr int kBfRanks = 4;
+constexpr int kBfN = 256;
+constexpr int kBfBatch = 16;  // rows per row-pass batch
+constexpr int kBfCols = 33;   // column lines held by rank 0 (32 by the others)
+
+__device__ __forceinline__ int bf_owner(int k) { return k < kBfCols ? 0 : (k - 1) >> 5; }
+__device__ __forceinline__ int bf_cb(int r) { return r == 0 ? 0 : 32 * r + 1; }
+
+__global__ void __cluster_dims__(kBfRanks, 1, 1) __launch_bounds__(256)
+k_block_filter(FftGeom G, const float* __restrict__ src, int w, int h, const int* __restrict__ oxs,
+               const int* __restrict__ oys, int nox, const double* __restrict__ cell_power,
+               const double* __restrict__ cell_sumk2, const int* __restrict__ block_cell,
+               const double* __restrict__ vsr, double* __restrict__ bnum, float* __restrict__ dense_out) {
+  extern __shared__ __align__(16) float2 fsm2[];
+  constexpr int n = kBfN, hn = n / 2, nb = hn + 1;
+  const int ls = fft_ls(n, true), zl = fft_ls(hn, false);
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = static_cast<int>(cl.block_rank());
+  const int item = blockIdx.x / kBfRanks;
+  float2* x = fsm2;                      // kBfCols x ls column lines
+  float2* z = x + kBfCols * ls;          // kBfBatch x zl row lines
+  float2* tw = z + kBfBatch * zl;        // the whole twiddle table
+  copy_tw(tw, G.tw_tab, n + n / 2 + 2 * nb);
+  const float2* tw_fwd_n = tw;
+  const float2* tw_inv_n = tw + n / 2;
+  const float2* tw_fwd_hn = tw + n;
+  const float2* tw_inv_hn = tw + n + n / 4;
+  const float2* split_fwd = tw + n + n / 2;
+  const float2* split_inv = split_fwd + nb;
+  // Element (column k, row) of the block spectrum in its owner's lines.
+  auto bin = [&](int k, int row) {
+    const int q = bf_owner(k);
+    return cl.map_shared_rank(x + (k - bf_cb(q)) * ls + row, q);
+  };
+  const int bx = oxs[item % nox], by = oys[item / nox];
+  const int ncol = rank == 0 ? kBfCols : 32;
+  const int rbeg = rank * (n / kBfRanks), rend = rbeg + n / kBfRanks;
+  cl.sync();  // every rank has started before its shared memory is written
+
+  // Row pass (r2c), scattered to the column owners. 256 threads: each loop
+  // below has a fixed trip count, so its loads are all in flight together.
+  const int tid = threadIdx.x;
+  for (int b0 = rbeg; b0 < rend; b0 += kBfBatch) {
+    {
+      float2 v[kBfBatch * hn / 256];
+#pragma unroll
+      for (int i = 0; i < kBfBatch * hn / 256; ++i) {
+        const int e = tid + 256 * i, rr = e / hn, j = e - rr * hn;
+        const int sy = reflect_clamp(by + b0 + rr, h);
+        const float* srow = src + static_cast<size_t>(sy) * w;
+        v[i] = make_float2(__ldg(srow + reflect_clamp(bx + 2 * j, w)), __ldg(srow + reflect_clamp(bx + 2 * j + 1, w)));
+      }
+#pragma unroll
+      for (int i = 0; i < kBfBatch * hn / 256; ++i) {
+        const int e = tid + 256 * i, rr = e / hn, j = e - rr * hn;
+        z[rr * zl + j] = v[i];
+      }
+    }
+    __syncthreads();
+    fft_lines(z, kBfBatch, hn, G.logn - 1, tw_fwd_hn, zl);
+#pragma unroll
+    for (int i = 0; i < (kBfBatch * nb + 255) / 256; ++i) {
+      const int e = tid + 256 * i;
+      if (e >= kBfBatch * nb) break;
+      const int rr = e / nb, k = e - rr * nb;
+      const float2 zk = z[rr * zl + (k % hn)];
+      const float2 zc = cconj(z[rr * zl + ((hn - k) % hn)]);
+      const float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
+      const float2 d = csub(zk, zc);
+      const float2 od = make_float2(0.5f * d.y, -0.5f * d.x);
+      *bin(k, b0 + rr) = cadd(ev, cmul(split_fwd[k], od));
+    }
+    __syncthreads();
+  }
+  cl.sync();
+
+  // Column pass: forward, filter (src/noise.cpp:414-422), inverse. Filter:
+  // lane = column (coalesced kernel-power loads), warps over rows; rank 0's
+  // 33rd column by a thread per row.
+  fft_lines(x, ncol, n, G.logn, tw_fwd_n, ls);
+  {
+    const int cell = block_cell[item];
+    const double vs = vsr[2 * item], vr = vsr[2 * item + 1];
+    const double cnum = sqrt(fmax(vs + vr * cell_sumk2[cell], 0.0));
+    if (rank == 0 && tid == 0 && bnum) bnum[item] = cnum * cnum;
+    const double* pw = cell_power + static_cast<size_t>(cell) * n * nb + bf_cb(rank);
+    auto scale = [&](int cc, int row, double p) {
+      const double denom = vs + vr * p;
+      const float f = denom > 0.0 ? static_cast<float>(cnum / sqrt(denom)) : 0.0f;
+      float2& xv = x[cc * ls + row];
+      xv = make_float2(xv.x * f, xv.y * f);
+    };
+    const int cc = tid & 31, r0 = tid >> 5;
+    for (int rb = 0; rb < n; rb += 64) {
+      double p[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) p[i] = __ldg(pw + static_cast<size_t>(rb + r0 + 8 * i) * nb + cc);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) scale(cc, rb + r0 + 8 * i, p[i]);
+    }
+    if (ncol > 32) scale(32, tid, __ldg(pw + static_cast<size_t>(tid) * nb + 32));
+  }
+  __syncthreads();
+  fft_lines(x, ncol, n, G.logn, tw_inv_n, ls);
+  cl.sync();
+
+  // Row inverse (c2r): gather each row's bins from the owners.
+  for (int b0 = rbeg; b0 < rend; b0 += kBfBatch) {
+    {
+      float2 xk[kBfBatch * hn / 256], xc[kBfBatch * hn / 256];
+#pragma unroll
+      for (int i = 0; i < kBfBatch * hn / 256; ++i) {
+        const int e = tid + 256 * i, rr = e / hn, k = e - rr * hn;
+        xk[i] = *bin(k, b0 + rr);
+        xc[i] = cconj(*bin(hn - k, b0 + rr));
+      }
+#pragma unroll
+      for (int i = 0; i < kBfBatch * hn / 256; ++i) {
+        const int e = tid + 256 * i, rr = e / hn, k = e - rr * hn;
+        float2 a = xk[i], c = xc[i];
+        if (k == 0) {  // c2r ignores the imaginary parts of the DC and Nyquist bins
+          a.y = 0.0f;
+          c.y = 0.0f;
+        }
+        const float2 e2 = cadd(a, c);
+        const float2 o2 = cmul(csub(a, c), split_inv[k]);
+        z[rr * zl + k] = make_float2(e2.x - o2.y, e2.y + o2.x);  // 2E + i 2O
+      }
+    }
+    __syncthreads();
+    fft_lines(z, kBfBatch, hn, G.logn - 1, tw_inv_hn, zl);
+#pragma unroll 4
+    for (int i = 0; i < kBfBatch * n / 256; ++i) {
+      const int e = tid + 256 * i, rr = e / n, m = e - rr * n;
+      const float2 v = z[rr * zl + (m >> 1)];
+      dense_out[(static_cast<size_t>(item) * n + b0 + rr) * n + m] = (m & 1) ? v.y : v.x;
+    }
+    __syncthreads();
+  }
+  cl.sync();  // this CTA's lines stay alive until every rank has gathered
+}
+
 // Overlap-add as a gather (src/noise.cpp:430-479): every frame pixel sums the
 // Hann-weighted outputs of the (at most 3 x 3) blocks covering it in colour
 // order q = (ix % 3) * 3 + (iy % 3) -- the order of the reference's 9-colour
@@ -735,6 +892,21 @@ void launch_local_kernels(cudaStream_t s, const FftGeom& g, int ncell, const Tps
   ensure_dynamic_smem(reinterpret_cast<const void*>(k_local_kernels), smem);
   k_local_kernels<<<ncell, 256, smem, s>>>(g, t, theta, nc, phi, ks, centres, sumk2, dense, kern_out);
   DGPU_LAUNCH("k_local_kernels");
+}
+
+bool block_filter_fused(const FftGeom& g) { return g.n == kBfN && g.tw_tab != nullptr; }
+
+void launch_block_filter(cudaStream_t s, const FftGeom& g, int nitems, const float* src, int w, int h,
+                         const int* oxs, const int* oys, int nox, const double* cell_power, const double* cell_sumk2,
+                         const int* block_cell, const double* vsr, double* bnum, float* dense_out) {
+  if (!block_filter_fused(g)) fail(DGPU_ERR_INVALID, "decorrelate: fused block filter needs n = 256 and a twiddle table");
+  if (nitems == 0) return;
+  const size_t smem = sizeof(float2) * (static_cast<size_t>(kBfCols) * fft_ls(kBfN, true) +
+                                        static_cast<size_t>(kBfBatch) * fft_ls(kBfN / 2, false) + twiddle_table_len(kBfN));
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_block_filter), smem);
+  k_block_filter<<<nitems * kBfRanks, 256, smem, s>>>(g, src, w, h, oxs, oys, nox, cell_power, cell_sumk2, block_cell,
+                                                       vsr, bnum, dense_out);
+  DGPU_LAUNCH("k_block_filter");
 }
 
 void launch_ola_gather(cudaStream_t s, int w, int h, int n, const int* oxs, int nox, const int* oys, int noy,

@@ -625,33 +625,45 @@ k_rhs_mma(int64_t N, int nc, int k, int SS, FitRows R, const uint8_t* __restrict
   }
 }
 
+// Sum of the per-split partials: warp w of a CTA owns unknown 8 blockIdx + w,
+// its lanes stride the splits (four loads in flight), then a fixed shuffle
+// tree. Block 0's last warp also sums ywy and the row count.
 __global__ void __launch_bounds__(256)
 k_reduce_rhs(int nsplit, int P, const double* __restrict__ rpart, const double* __restrict__ ypart,
              const long long* __restrict__ npart, double* __restrict__ rhs, double* ywy, long long* n) {
-  // Block: 32 consecutive unknowns (lanes) x 8 warps striding the splits; the
-  // warps' partials are then added in warp order (fixed order).
-  __shared__ double red[8][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int p = blockIdx.x * 32 + lane;
-  double s = 0.0;
-  if (p < P)
-    for (int z = warp; z < nsplit; z += 8) s += rpart[static_cast<size_t>(z) * P + p];
-  red[warp][lane] = s;
-  __syncthreads();
-  if (warp == 0 && p < P) {
-    double t = 0.0;
-    for (int q = 0; q < 8; ++q) t += red[q][lane];
-    rhs[p] = t;
+  const int p = blockIdx.x * 8 + warp;
+  if (p < P) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    int z = lane;
+    for (; z + 96 < nsplit; z += 128) {
+      s0 += rpart[static_cast<size_t>(z) * P + p];
+      s1 += rpart[static_cast<size_t>(z + 32) * P + p];
+      s2 += rpart[static_cast<size_t>(z + 64) * P + p];
+      s3 += rpart[static_cast<size_t>(z + 96) * P + p];
+    }
+    for (; z < nsplit; z += 32) s0 += rpart[static_cast<size_t>(z) * P + p];
+    double s = (s0 + s1) + (s2 + s3);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) rhs[p] = s;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (blockIdx.x == 0 && warp == 7) {
     double y = 0.0;
     long long c = 0;
-    for (int z = 0; z < nsplit; ++z) {
+    for (int z = lane; z < nsplit; z += 32) {
       y += ypart[z];
       c += npart[z];
     }
-    if (ywy) *ywy = y;
-    if (n) *n = c;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      y += __shfl_xor_sync(0xffffffffu, y, o);
+      c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if (lane == 0) {
+      if (ywy) *ywy = y;
+      if (n) *n = c;
+    }
   }
 }
 
@@ -694,7 +706,7 @@ void launch_rhs(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, 
     k_rhs<<<nsplit, 256, smem, st>>>(N, nc, k, SS, R, accepted, theta, rps, rpart, ypart, npart);
     DGPU_LAUNCH("k_rhs");
   }
-  k_reduce_rhs<<<(P + 31) / 32, 256, 0, st>>>(nsplit, P, rpart, ypart, npart, rhs, ywy, n);
+  k_reduce_rhs<<<(P + 7) / 8, 256, 0, st>>>(nsplit, P, rpart, ypart, npart, rhs, ywy, n);
   DGPU_LAUNCH("k_reduce_rhs");
 }
 
