@@ -2,18 +2,21 @@
 //
 // Per overlap-add block (n x n, n a power of two, stride n/2, reflect padded):
 //   row pass    : n real rows -> n/2-point complex FFT of the even/odd packing
-//                 -> Hermitian split -> n/2+1 bins per row (r2c), to scratch;
+//                 -> Hermitian split -> n/2+1 bins per row (r2c);
 //   column pass : n-point complex FFT down each of the n/2+1 columns, the
 //                 decorrelation filter Phi = sqrt(vs + vr sum K^2) /
 //                 sqrt(vs + vr |Khat|^2) applied in place (|Khat|^2 from the
 //                 per-cell cache, vs / vr the block's subsampled medians), then
-//                 the inverse column FFT -- filter fused between the passes;
-//   row inverse : Hermitian merge -> n/2-point inverse FFT -> n real samples,
-//                 scaled by 1/n^2 and Hann-weighted into the frame accumulators.
-// The overlap-add runs colour by colour in the reference's 9-colour order
-// (ix % 3, iy % 3), so every pixel accumulates its blocks in the same order on
-// every run and no two blocks of one launch touch the same pixel.
-// FFTs are unnormalised radix-2 in shared memory with FP64-derived twiddles.
+//                 the inverse column FFT;
+//   row inverse : Hermitian merge -> n/2-point inverse FFT -> n real samples.
+// For n = 256 the three passes run fused in k_block_filter (one 4-CTA cluster
+// per block, the spectrum in distributed shared memory); otherwise as three
+// kernels through a scratch spectrum. The raw block outputs are then
+// overlap-added by k_ola_gather: every pixel sums its Hann-weighted blocks in
+// the reference's 9-colour order (ix % 3, iy % 3), with the float rounding of
+// the reference's colour passes, and divides by the weight sums.
+// Lines of 128 / 256 points use a four-step FFT (16-point DFTs in registers);
+// other lengths a radix-2 shared-memory FFT. Twiddles are FP64-derived.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
