@@ -402,29 +402,44 @@ __global__ void k_psf_stamps(int w, int h, const float* __restrict__ img, const 
   for (int i = threadIdx.x; i < np; i += blockDim.x) cuts[static_cast<size_t>(s) * np + i] = (sv[i] - med) / tot;
 }
 
-__global__ void k_psf_median(int n, int np, const double* __restrict__ cuts, const int* __restrict__ use,
-                             double* __restrict__ out, unsigned* status) {
+// Median over the used stamps of pixel p (a CTA per pixel): each used value's
+// rank among the used values (ties broken by stamp index) is counted in
+// parallel; the values of rank cnt/2 (and cnt/2 - 1) give the median.
+__global__ void __launch_bounds__(256) k_psf_median(int n, int np, const double* __restrict__ cuts,
+                                                     const int* __restrict__ use, double* __restrict__ out,
+                                                     unsigned* status) {
   extern __shared__ double col[];
+  int* used = reinterpret_cast<int*>(col + n);
   const int p = blockIdx.x;
   __shared__ int cnt;
+  __shared__ double lo, hi;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  int mine = 0;
+  for (int s = threadIdx.x; s < n; s += blockDim.x) {
+    const int u = use[s] != 0;
+    used[s] = u;
+    col[s] = u ? cuts[static_cast<size_t>(s) * np + p] : 0.0;
+    mine += u;
+  }
+  atomicAdd(&cnt, mine);
+  __syncthreads();
+  const int c = cnt;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    if (!used[i]) continue;
+    const double v = col[i];
+    int rank = 0;
+    for (int j = 0; j < n; ++j)
+      if (used[j] && (col[j] < v || (col[j] == v && j < i))) ++rank;
+    if (rank == c / 2) hi = v;
+    if (rank == c / 2 - 1) lo = v;
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
-    cnt = 0;
-    for (int s = 0; s < n; ++s)
-      if (use[s]) col[cnt++] = cuts[static_cast<size_t>(s) * np + p];
-    // insertion sort (n is the stamp count, a few hundred)
-    for (int i = 1; i < cnt; ++i) {
-      const double v = col[i];
-      int j = i - 1;
-      while (j >= 0 && col[j] > v) {
-        col[j + 1] = col[j];
-        --j;
-      }
-      col[j + 1] = v;
-    }
     double m = 0.0;
-    if (cnt > 0) m = (cnt & 1) ? col[cnt / 2] : 0.5 * (col[cnt / 2 - 1] + col[cnt / 2]);
+    if (c > 0) m = (c & 1) ? hi : 0.5 * (lo + hi);
     out[p] = m > 0.0 ? m : 0.0;
-    if (cnt == 0) atomicOr(status, kStatusBounds);
+    if (c == 0) atomicOr(status, kStatusBounds);
   }
 }
 
@@ -440,9 +455,9 @@ void launch_psf_estimate(Context& c, int w, int h, const float* img, const int* 
   ensure_dynamic_smem(reinterpret_cast<const void*>(k_psf_stamps), smem);
   k_psf_stamps<<<n, 256, smem, s>>>(w, h, img, xs, ys, n, radius, cuts, use);
   DGPU_LAUNCH("k_psf_stamps");
-  const size_t smem2 = sizeof(double) * std::max(n, 1);
+  const size_t smem2 = (sizeof(double) + sizeof(int)) * std::max(n, 1);
   ensure_dynamic_smem(reinterpret_cast<const void*>(k_psf_median), smem2);
-  k_psf_median<<<np, 32, smem2, s>>>(n, np, cuts, use, out, c.d_status);
+  k_psf_median<<<np, 256, smem2, s>>>(n, np, cuts, use, out, c.d_status);
   DGPU_LAUNCH("k_psf_median");
   std::vector<int> hu(n);
   if (n) DGPU_CUDA(cudaMemcpyAsync(hu.data(), use, sizeof(int) * n, cudaMemcpyDeviceToHost, s));

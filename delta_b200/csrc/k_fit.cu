@@ -196,9 +196,59 @@ __global__ void k_design_weights(int64_t N, TpsDev t, FitRows R, int have_var) {
   }
 }
 
+// The same rows with the thin-plate constants in shared memory and the
+// k - 3 null-space sums in registers (same FMA order per value), for k - 3 <= NR.
+template <int NR>
+__global__ void __launch_bounds__(256) k_design_weights_r(int64_t N, TpsDev t, FitRows R, int have_var) {
+  extern __shared__ double tsm[];
+  const int k = t.k, nr = k - 3;
+  double* kn = tsm;       // k x 2
+  double* z = tsm + 2 * k;  // k x nr
+  for (int e = threadIdx.x; e < 2 * k; e += blockDim.x) kn[e] = t.kn[e];
+  for (int e = threadIdx.x; e < k * nr; e += blockDim.x) z[e] = t.z[e];
+  __syncthreads();
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < N;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double* d = R.d + i * k;
+    if (!R.valid[i]) {
+      for (int m = 0; m < k; ++m) d[m] = 0.0;
+      R.w[i] = 0.0;
+      continue;
+    }
+    const double ux = (static_cast<double>(R.px[i]) - t.cx) / t.scale, uy = (static_cast<double>(R.py[i]) - t.cy) / t.scale;
+    double acc[NR];
+#pragma unroll
+    for (int m = 0; m < NR; ++m) acc[m] = 0.0;
+    for (int j = 0; j < k; ++j) {
+      const double dx = ux - kn[2 * j], dy = uy - kn[2 * j + 1];
+      const double sg = tps_green_dev(dx * dx + dy * dy);
+#pragma unroll
+      for (int m = 0; m < NR; ++m)
+        if (m < nr) acc[m] = fma(sg, z[j * nr + m], acc[m]);
+    }
+#pragma unroll
+    for (int m = 0; m < NR; ++m)
+      if (m < nr) d[m] = acc[m];
+    d[nr] = 1.0;
+    d[nr + 1] = ux;
+    d[nr + 2] = uy;
+    R.w[i] = have_var ? 1.0 / (R.vt[i] + R.vc[i]) : 1.0;
+  }
+}
+
 void launch_design_weights(cudaStream_t st, int64_t N, const TpsDev& t, const FitRows& R, int have_var) {
-  const int blocks = static_cast<int>(std::min<int64_t>((N + 255) / 256, 148 * 8));
-  k_design_weights<<<std::max(blocks, 1), 256, 0, st>>>(N, t, R, have_var);
+  const int blocks = std::max(1, static_cast<int>(std::min<int64_t>((N + 255) / 256, 148 * 8)));
+  const int nr = t.k - 3;
+  const size_t smem = sizeof(double) * static_cast<size_t>(t.k) * (2 + std::max(nr, 0));
+  if (nr >= 0 && nr <= 16) {
+    ensure_dynamic_smem(reinterpret_cast<const void*>(k_design_weights_r<16>), smem);
+    k_design_weights_r<16><<<blocks, 256, smem, st>>>(N, t, R, have_var);
+  } else if (nr > 16 && nr <= 32) {
+    ensure_dynamic_smem(reinterpret_cast<const void*>(k_design_weights_r<32>), smem);
+    k_design_weights_r<32><<<blocks, 256, smem, st>>>(N, t, R, have_var);
+  } else {
+    k_design_weights<<<blocks, 256, 0, st>>>(N, t, R, have_var);
+  }
   DGPU_LAUNCH("k_design_weights");
 }
 
@@ -770,13 +820,15 @@ k_reweight(StampGeom g, TpsDev t, const int* __restrict__ stamp_x, const int* __
            FitRows R, const uint8_t* __restrict__ accepted, const int* __restrict__ cnt,
            const double* __restrict__ theta, const float* __restrict__ phi, const float* __restrict__ vr,
            const uint8_t* __restrict__ rm) {
-  extern __shared__ __align__(16) float wsm[];
+  extern __shared__ __align__(16) double wsmd[];
   const int s = blockIdx.x;
   if (!accepted[s] || cnt[s] == 0) return;
   const int ks = g.ks, kk = ks * ks, r = g.r;
   const int nc = g.nc;
-  float* k2 = wsm;               // kk
-  float* win = wsm + kk;         // (S + 2r)^2 reference-variance window, invalid samples = 0
+  // K^2 and the reference-variance window as doubles (exact conversions of
+  // the float values the reference multiplies).
+  double* k2 = wsmd;             // kk
+  double* win = wsmd + kk;       // (S + 2r)^2, invalid samples = 0
   const int side = g.S + 2 * r;
   const int wx0 = stamp_x[s] - g.sr - r, wy0 = stamp_y[s] - g.sr - r;
   __shared__ float an[64];
@@ -800,32 +852,53 @@ k_reweight(StampGeom g, TpsDev t, const int* __restrict__ stamp_x, const int* __
         const float x = vr[idx];
         if (!(rm && rm[idx] != 0) && x > 0.0f && isfinite(x)) v = x;
       }
-      win[i] = v;
+      win[i] = static_cast<double>(v);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < kk; i += blockDim.x) {
       float v = 0.0f;
       for (int n = 0; n < nc; ++n) v = __fmaf_rn(an[n], phi[static_cast<size_t>(n) * kk + i], v);
-      k2[i] = v * v;
+      k2[i] = static_cast<double>(v * v);
     }
     __syncthreads();
   }
-  for (int i = threadIdx.x; i < g.SS; i += blockDim.x) {
-    const size_t row = static_cast<size_t>(s) * g.SS + i;
-    if (!R.valid[row]) continue;
+  // Four rows per thread as independent FMA chains, each in (dv, du) order.
+  constexpr int kRows = 4;
+  for (int i0 = threadIdx.x; i0 < g.SS; i0 += kRows * blockDim.x) {
+    size_t row[kRows];
+    bool live[kRows];
+    int base[kRows];
+    double acc[kRows];
+#pragma unroll
+    for (int q = 0; q < kRows; ++q) {
+      const int i = i0 + q * blockDim.x;
+      row[q] = static_cast<size_t>(s) * g.SS + i;
+      live[q] = i < g.SS && R.valid[row[q]];
+      // window index of (x - du, y - dv) at du = dv = 0 (the window centre for
+      // rows that are not live, so every tap index stays inside the window)
+      base[q] = live[q] ? (R.py[row[q]] - wy0) * side + (R.px[row[q]] - wx0) : r * side + r;
+      acc[q] = 0.0;
+    }
     if (g.have_cvar) {
-      // window coordinates of (x - du, y - dv): row y - wy0 - dv, column x - wx0 - du
-      const int lx = R.px[row] - wx0, ly = R.py[row] - wy0;
-      double acc = 0.0;
       for (int dv = -r; dv <= r; ++dv) {
-        const float* krow = k2 + (dv + r) * ks;
-        const float* wrow = win + (ly - dv) * side + lx;
-        for (int du = -r; du <= r; ++du) acc = fma(static_cast<double>(krow[du + r]), static_cast<double>(wrow[-du]), acc);
+        const double* krow = k2 + (dv + r) * ks;
+        const int off = -dv * side;
+        for (int du = -r; du <= r; ++du) {
+          const double c = krow[du + r];
+#pragma unroll
+          for (int q = 0; q < kRows; ++q) acc[q] = fma(c, win[base[q] + off - du], acc[q]);
+        }
       }
-      const double rv = R.vt[row] + acc;
-      if (rv > 0.0) R.w[row] = 1.0 / rv;
-    } else {
-      if (R.vt[row] > 0.0) R.w[row] = 1.0 / R.vt[row];
+    }
+#pragma unroll
+    for (int q = 0; q < kRows; ++q) {
+      if (!live[q]) continue;
+      if (g.have_cvar) {
+        const double rv = R.vt[row[q]] + acc[q];
+        if (rv > 0.0) R.w[row[q]] = 1.0 / rv;
+      } else {
+        if (R.vt[row[q]] > 0.0) R.w[row[q]] = 1.0 / R.vt[row[q]];
+      }
     }
   }
 }
@@ -835,7 +908,7 @@ void launch_reweight(cudaStream_t st, const StampGeom& g, int n_stamps, const Tp
                      const double* theta, const float* phi, const float* vr, const uint8_t* rm) {
   if (n_stamps == 0) return;
   const size_t side = static_cast<size_t>(g.S) + 2 * g.r;
-  const size_t smem = sizeof(float) * (static_cast<size_t>(g.ks) * g.ks + side * side);
+  const size_t smem = sizeof(double) * (static_cast<size_t>(g.ks) * g.ks + side * side);
   if (smem > 200 * 1024) fail(DGPU_ERR_INVALID, "fit_kernel: stamp plus kernel footprint too large for the reweight");
   ensure_dynamic_smem(reinterpret_cast<const void*>(k_reweight), smem);
   k_reweight<<<n_stamps, 256, smem, st>>>(g, t, sx, sy, R, accepted, cnt, theta, phi, vr, rm);
