@@ -93,10 +93,10 @@ void launch_exact_fields(cudaStream_t s, const TpsDev& t, const double* theta, i
 // the tile rows plus the y halo (each thread: 4 columns x all nx, sliding a
 // 4-wide register window so every staged value is loaded once per tap); the
 // y-pass of every component then runs out of shared memory with each thread
-// holding 8 output rows of one column in registers (taps in blocks of 8, the
-// 15 rows a block touches in registers), and a_n / b are blended from the
-// coarse lattice in registers, the corners re-read only when the coarse cell
-// row changes. Per output
+// holding 4 output rows of 2 adjacent columns in registers as float2 (taps in
+// blocks of 8, the 11 row pairs a block touches in registers, one packed FMA
+// per tap and row), and a_n / b are blended from the coarse lattice in
+// registers, the corners re-read only when the coarse cell row changes. Per output
 // pixel the accumulation order is the reference's: x taps j = 0..ks-1, then
 // components in basis order, each y tap j ascending, d -= a_n * bn (FMA).
 // Off-frame rows of the x-pass buffer are exact zeros, which leaves every
@@ -104,7 +104,7 @@ void launch_exact_fields(cudaStream_t s, const TpsDev& t, const double* theta, i
 // ---------------------------------------------------------------------------
 
 constexpr int kMcTW = 32;   // tile width (columns)
-constexpr int kMcRPT = 8;   // output rows per thread in the y pass
+constexpr int kMcYR = 4;    // output rows per thread in the y pass (2 columns each)
 constexpr int kMcXPT = 4;   // output columns per thread in the x pass
 
 struct McSmem {
@@ -186,25 +186,35 @@ k_model_convolve(int w, int h, const float* __restrict__ sci, const float* __res
   }
   __syncthreads();
 
-  // ---- y pass + field blend, 8 rows of one column per thread ----
-  const int lx = tid % kMcTW;
-  const int ly0 = (tid / kMcTW) * kMcRPT;
+  // ---- y pass + field blend: 2 adjacent columns x 4 rows per thread ----
+  // Column pairs move as float2 (one 8-byte shared load per buffer row) and
+  // every tap is one packed FMA (__ffma2_rn: an IEEE fma per lane, so each
+  // output is the same FMA chain as a scalar loop).
+  const int lx0 = 2 * (tid % (kMcTW / 2));
+  const int ly0 = (tid / (kMcTW / 2)) * kMcYR;
   if (ly0 >= TH) return;
-  const int x = bx + lx;
-  const bool xin = x < w;
-  const int xc = xin ? x : w - 1;
-  float d[kMcRPT];
-  // Coarse-cell coordinates of this column / these rows.
-  int jx = 0;
-  float wxv = 0.0f;
-  int jy[kMcRPT];
-  float fy[kMcRPT];
+  const int x0 = bx + lx0;
+  bool xin[2];
+  int xcl[2];
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    xin[u] = x0 + u < w;
+    xcl[u] = xin[u] ? x0 + u : w - 1;
+  }
+  float2 d2[kMcYR];
+  int jx[2] = {0, 0};
+  float wxv[2] = {0.0f, 0.0f};
+  int jy[kMcYR];
+  float fy[kMcYR];
   if (!STACK && !F.exact) {
-    jx = F.cellx[xc];
-    wxv = F.wx[xc];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      jx[u] = F.cellx[xcl[u]];
+      wxv[u] = F.wx[xcl[u]];
+    }
   }
 #pragma unroll
-  for (int i = 0; i < kMcRPT; ++i) {
+  for (int i = 0; i < kMcYR; ++i) {
     const int y = min(by + ly0 + i, h - 1);
     if (!STACK && !F.exact) {
       jy[i] = F.celly[y];
@@ -214,91 +224,103 @@ k_model_convolve(int w, int h, const float* __restrict__ sci, const float* __res
       fy[i] = 0.0f;
     }
   }
-  // Field values a_f(x, y_i) of this thread's 8 rows: the four lattice corners
-  // are re-read only when the coarse cell row changes (rows of a warp share
-  // them, so the branch is warp-uniform).
-  auto fields_of = [&](int f, float (&a)[kMcRPT]) {
+  // Field values a_f(x, y_i) of both columns; the lattice corners are re-read
+  // only when the coarse cell row changes.
+  auto fields_of = [&](int f, float2 (&a)[kMcYR]) {
     if (F.exact) {
 #pragma unroll
-      for (int i = 0; i < kMcRPT; ++i) {
+      for (int i = 0; i < kMcYR; ++i) {
         const int y = min(by + ly0 + i, h - 1);
-        a[i] = __ldg(F.full + (static_cast<size_t>(f) * h + y) * w + xc);
+        const float* fr = F.full + (static_cast<size_t>(f) * h + y) * w;
+        a[i] = make_float2(__ldg(fr + xcl[0]), __ldg(fr + xcl[1]));
       }
       return;
     }
-    int cj = -1;
-    float a00 = 0.0f, a01 = 0.0f, a10 = 0.0f, a11 = 0.0f;
 #pragma unroll
-    for (int i = 0; i < kMcRPT; ++i) {
-      if (jy[i] != cj) {
-        cj = jy[i];
-        const float* c0 = F.latf + (static_cast<size_t>(f) * F.ncy + cj) * F.ncx + jx;
-        const float* c1 = c0 + F.ncx;
-        a00 = __ldg(c0);
-        a01 = __ldg(c0 + 1);
-        a10 = __ldg(c1);
-        a11 = __ldg(c1 + 1);
+    for (int u = 0; u < 2; ++u) {
+      int cj = -1;
+      float a00 = 0.0f, a01 = 0.0f, a10 = 0.0f, a11 = 0.0f;
+#pragma unroll
+      for (int i = 0; i < kMcYR; ++i) {
+        if (jy[i] != cj) {
+          cj = jy[i];
+          const float* c0 = F.latf + (static_cast<size_t>(f) * F.ncy + cj) * F.ncx + jx[u];
+          const float* c1 = c0 + F.ncx;
+          a00 = __ldg(c0);
+          a01 = __ldg(c0 + 1);
+          a10 = __ldg(c1);
+          a11 = __ldg(c1 + 1);
+        }
+        const float v = cell_blend(a00, a01, a10, a11, fy[i], wxv[u]);
+        if (u == 0) a[i].x = v; else a[i].y = v;
       }
-      a[i] = cell_blend(a00, a01, a10, a11, fy[i], wxv);
     }
   };
   if (!STACK) {
-    float bg[kMcRPT];
+    float2 bg[kMcYR];
     fields_of(nc, bg);
 #pragma unroll
-    for (int i = 0; i < kMcRPT; ++i) {
+    for (int i = 0; i < kMcYR; ++i) {
       const int y = min(by + ly0 + i, h - 1);
-      d[i] = __ldg(sci + static_cast<size_t>(y) * w + xc) - bg[i];
+      const float* sr = sci + static_cast<size_t>(y) * w;
+      d2[i] = make_float2(__ldg(sr + xcl[0]) - bg[i].x, __ldg(sr + xcl[1]) - bg[i].y);
     }
   }
   for (int n = 0; n < nc; ++n) {
     const int2 o = orders[n];
-    const float* col = txs + static_cast<size_t>(o.x) * nrows * kMcTW + lx;
+    const float2* col = reinterpret_cast<const float2*>(txs + static_cast<size_t>(o.x) * nrows * kMcTW + lx0);
     const float* ky = ktaps + o.y * ks;
     // Output row ly0+i needs buffer row ly0 + i + 2kh - j. Taps go in blocks of
     // 8 with the rows of a block held in registers (static indices), each
     // output still summing its taps j = 0..ks-1 in order.
     const int base = ly0 + 2 * kh;
-    float bn[kMcRPT];
+    float2 bn[kMcYR];
 #pragma unroll
-    for (int i = 0; i < kMcRPT; ++i) bn[i] = 0.0f;
+    for (int i = 0; i < kMcYR; ++i) bn[i] = make_float2(0.0f, 0.0f);
     for (int j0 = 0; j0 < ks; j0 += 8) {
-      float v[kMcRPT + 7];  // v[t] = buffer row base - j0 - 7 + t
+      float2 v[kMcYR + 7];  // v[t] = buffer row base - j0 - 7 + t
 #pragma unroll
-      for (int t = 0; t < kMcRPT + 7; ++t) {
+      for (int t = 0; t < kMcYR + 7; ++t) {
         const int rr = base - j0 - 7 + t;
-        v[t] = rr >= 0 ? col[rr * kMcTW] : 0.0f;
+        v[t] = rr >= 0 ? col[rr * (kMcTW / 2)] : make_float2(0.0f, 0.0f);
       }
 #pragma unroll
       for (int jj = 0; jj < 8; ++jj) {
         if (j0 + jj < ks) {
           const float c = ky[j0 + jj];
+          const float2 cc = make_float2(c, c);
 #pragma unroll
-          for (int i = 0; i < kMcRPT; ++i) bn[i] = __fmaf_rn(c, v[i - jj + 7], bn[i]);
+          for (int i = 0; i < kMcYR; ++i) bn[i] = __ffma2_rn(cc, v[i - jj + 7], bn[i]);
         }
       }
     }
     if (STACK) {
-      if (xin) {
 #pragma unroll
-        for (int i = 0; i < kMcRPT; ++i) {
-          const int y = by + ly0 + i;
-          if (y < h) diff[(static_cast<size_t>(n) * h + y) * w + x] = bn[i];
-        }
+      for (int i = 0; i < kMcYR; ++i) {
+        const int y = by + ly0 + i;
+        if (y >= h) continue;
+        float* dr = diff + (static_cast<size_t>(n) * h + y) * w;
+        if (xin[0]) dr[x0] = bn[i].x;
+        if (xin[1]) dr[x0 + 1] = bn[i].y;
       }
       continue;
     }
-    float a[kMcRPT];
+    float2 a[kMcYR];
     fields_of(n, a);
 #pragma unroll
-    for (int i = 0; i < kMcRPT; ++i) d[i] = __fmaf_rn(-a[i], bn[i], d[i]);
+    for (int i = 0; i < kMcYR; ++i) d2[i] = __ffma2_rn(make_float2(-a[i].x, -a[i].y), bn[i], d2[i]);
   }
   if (STACK) return;
-  if (xin) {
 #pragma unroll
-    for (int i = 0; i < kMcRPT; ++i) {
-      const int y = by + ly0 + i;
-      if (y < h) diff[static_cast<size_t>(y) * w + x] = d[i];
+  for (int i = 0; i < kMcYR; ++i) {
+    const int y = by + ly0 + i;
+    if (y >= h) continue;
+    const size_t o = static_cast<size_t>(y) * w + x0;
+    if (xin[0] && xin[1] && (o & 1) == 0) {
+      *reinterpret_cast<float2*>(diff + o) = d2[i];
+    } else {
+      if (xin[0]) diff[o] = d2[i].x;
+      if (xin[1]) diff[o + 1] = d2[i].y;
     }
   }
 }
@@ -308,7 +330,7 @@ static void launch_mc(cudaStream_t s, const SubtractArgs& a, const int2* orders,
   auto kern = k_model_convolve<NX, STACK>;
   ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
   dim3 grid(ceil_div(a.w, kMcTW), ceil_div(a.h, TH));
-  const int threads = kMcTW * (TH / kMcRPT);
+  const int threads = (kMcTW / 2) * (TH / kMcYR);
   kern<<<grid, threads, smem, s>>>(a.w, a.h, a.sci, a.ref, a.ref_mask, a.F, a.taps, orders, a.ks,
                                    a.nc, a.fill, a.diff, TH);
   DGPU_LAUNCH("k_model_convolve");
