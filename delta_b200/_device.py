@@ -52,7 +52,12 @@ class DeviceFrame:
         return tuple(self.science.shape)
 
     @classmethod
-    def from_numpy(cls, sci, ref, svar=None, rvar=None, smask=None, rmask=None, device=None, non_blocking=False):
+    def from_numpy(cls, sci, ref, svar=None, rvar=None, smask=None, rmask=None, device=None, non_blocking=False,
+                   serialize=False):
+        """Upload the layers. With serialize, frames uploading from several host
+        threads take turns (each upload completes before the next starts), so
+        the first frame of a batch can start computing while the others are
+        still in flight instead of every frame waiting for all uploads."""
         dev = device or torch.device("cuda", torch.cuda.current_device())
 
         def up(a, dt):
@@ -61,11 +66,20 @@ class DeviceFrame:
             t = torch.from_numpy(np.ascontiguousarray(a, dtype=dt))
             return t.to(dev, non_blocking=non_blocking)
 
-        return cls(up(sci, np.float32), up(ref, np.float32), up(svar, np.float32), up(rvar, np.float32),
-                   up(smask, np.uint8), up(rmask, np.uint8))
+        def all_layers():
+            return cls(up(sci, np.float32), up(ref, np.float32), up(svar, np.float32), up(rvar, np.float32),
+                       up(smask, np.uint8), up(rmask, np.uint8))
+
+        if not serialize:
+            return all_layers()
+        with _UPLOAD_LOCK:
+            frame = all_layers()
+            torch.cuda.current_stream().synchronize()
+        return frame
 
 
 _CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy: handle 0 would select the context's own stream
+_UPLOAD_LOCK = threading.Lock()
 
 
 def _ctx_on_torch_stream():

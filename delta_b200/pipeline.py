@@ -384,7 +384,7 @@ class Subtractor:
         if rvar is None and gain is not None:
             rvar = synth_variance(ref, gain, read_noise)
         logger.info("fitting {} x {} frame (device resident)", sci.shape[1], sci.shape[0])
-        frame = _device.DeviceFrame.from_numpy(sci, ref, svar, rvar, smask, rmask, non_blocking=True)
+        frame = _device.DeviceFrame.from_numpy(sci, ref, svar, rvar, smask, rmask, non_blocking=True, serialize=True)
         if solution is None:
             out = _device.run(self, frame, catalog, direction)
         else:
