@@ -103,42 +103,106 @@ def summarise_clocks(samples: list[tuple[float, float, int]]) -> dict:
             "samples": len(samples)}
 
 
-class ClockSampler:
-    """Reads SM clock, max clock and clock-event reasons through NVML every
-    `period` seconds on a thread (read-only queries)."""
+_SAMPLER_CHILD = r"""
+import sys, time
+import pynvml
+pynvml.nvmlInit()
+uuid, period = sys.argv[1], float(sys.argv[2])
+h = pynvml.nvmlDeviceGetHandleByUUID(uuid) if uuid else pynvml.nvmlDeviceGetHandleByIndex(int(sys.argv[3]))
+while True:
+    try:
+        r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+    except Exception:
+        r = pynvml.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+    sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+    mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+    print(f"{time.time():.6f} {sm} {mx} {int(r)}", flush=True)
+    time.sleep(period)
+"""
 
-    def __init__(self, device_index: int, period: float = 0.02):
+
+class ClockSampler:
+    """SM clock, max clock and clock-event reasons (read-only NVML queries)
+    sampled every `period` seconds by a small child process, so the sampling
+    does not compete for the interpreter with the bench's worker threads. It
+    is started ahead of time (start()); the context manager marks the timed
+    window and only samples inside it are kept. Falls back to a thread when
+    the child cannot start."""
+
+    def __init__(self, device_index: int, period: float = 0.01):
         self.period = period
+        self.device_index = device_index
         self.samples: list[tuple[float, float, int]] = []
+        self.error = None
+        self._proc = None
+        self._lines: list[str] = []
+        self._reader = None
+        self._t0 = self._t1 = None
         self._stop = threading.Event()
         self._thread = None
-        self.error = None
+        self._nvml = None
+
+    @staticmethod
+    def _uuid(device_index: int) -> str:
+        try:
+            import torch
+
+            u = str(torch.cuda.get_device_properties(device_index).uuid)
+            return u if u.startswith("GPU-") else "GPU-" + u
+        except Exception:
+            return ""
+
+    def start(self):
+        import subprocess
+
+        try:
+            self._proc = subprocess.Popen(
+                [sys.executable, "-c", _SAMPLER_CHILD, self._uuid(self.device_index), str(self.period),
+                 str(self.device_index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._reader = threading.Thread(target=self._drain, daemon=True)
+            self._reader.start()
+            deadline = time.time() + 15.0
+            while not self._lines and self._proc.poll() is None and time.time() < deadline:
+                time.sleep(0.01)
+            if not self._lines:
+                raise RuntimeError("clock sampler produced no sample")
+        except Exception as exc:
+            self._stop_child()
+            self.error = f"sampler process: {exc}"
+            self._start_thread()
+        return self
+
+    def _drain(self):
+        for line in self._proc.stdout:
+            self._lines.append(line)
+
+    def _stop_child(self):
+        if self._proc is not None:
+            if self._proc.poll() is None:
+                self._proc.terminate()
+                try:
+                    self._proc.wait(timeout=5)
+                except Exception:
+                    self._proc.kill()
+            self._proc = None
+
+    # Thread fallback (NVML in-process).
+    def _start_thread(self):
         try:
             import pynvml
 
             pynvml.nvmlInit()
             self._nvml = pynvml
-            self._handle = self._find_handle(pynvml, device_index)
-        except Exception as exc:  # NVML missing: report no clocks rather than fail the bench
+            uuid = self._uuid(self.device_index)
+            self._handle = (pynvml.nvmlDeviceGetHandleByUUID(uuid) if uuid
+                            else pynvml.nvmlDeviceGetHandleByIndex(self.device_index))
+        except Exception as exc:
             self._nvml = None
             self.error = f"nvml unavailable: {exc}"
-
-    @staticmethod
-    def _find_handle(pynvml, device_index: int):
-        import torch
-
-        try:
-            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
-            return pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
-        except Exception:
-            pass
-        try:
-            bus = torch.cuda.get_device_properties(device_index)
-            pci = f"{bus.pci_domain_id:08x}:{bus.pci_bus_id:02x}:{bus.pci_device_id:02x}.0"
-            return pynvml.nvmlDeviceGetHandleByPciBusId(pci)
-        except Exception:
-            pass
-        return pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            return
+        self._thread = threading.Thread(target=self._loop, daemon=True)
+        self._thread.start()
 
     def _read(self):
         n = self._nvml
@@ -153,22 +217,32 @@ class ClockSampler:
     def _loop(self):
         while not self._stop.is_set():
             try:
-                self.samples.append(self._read())
+                self._lines.append(f"{time.time():.6f} " + " ".join(str(int(v)) for v in self._read()))
             except Exception as exc:
                 self.error = str(exc)
                 return
             self._stop.wait(self.period)
 
     def __enter__(self):
-        if self._nvml is not None:
-            self._thread = threading.Thread(target=self._loop, daemon=True)
-            self._thread.start()
+        if self._proc is None and self._thread is None:
+            self.start()
+        self._t0 = time.time()
         return self
 
     def __exit__(self, *exc):
+        self._t1 = time.time()
+        time.sleep(2 * self.period)
+        self._stop_child()
         self._stop.set()
         if self._thread is not None:
             self._thread.join()
+        for line in list(self._lines):
+            parts = line.split()
+            if len(parts) != 4:
+                continue
+            t = float(parts[0])
+            if self._t0 <= t <= self._t1:
+                self.samples.append((float(parts[1]), float(parts[2]), int(parts[3])))
 
     def summary(self) -> dict:
         out = summarise_clocks(self.samples)
@@ -409,8 +483,9 @@ def run_gpu(args) -> int:
     for _ in range(args.warmup):
         batch_step()
     torch.cuda.synchronize(device)
+    clocks = ClockSampler(local).start()
     l0 = launch_count()
-    with ClockSampler(local) as clocks:
+    with clocks:
         ms = timed_steps(batch_step, args.steps, device)
     launches = launch_count() - l0
 
