@@ -45,6 +45,18 @@ WORKLOAD = ("4096x4096 spatially varying Moffat field, 20000 stars, 50 transient
 # Algorithmic HBM bytes per science pixel of the fused model-convolve kernel:
 # science + reference (float32), reference mask (u8), difference (float32).
 MODEL_CONVOLVE_BYTES_PER_PX = 13
+# FP32 FMA peak of the part (148 SMs x 128 FMA lanes x 1.965 GHz), for the
+# compute side of the model convolve's roofline.
+FP32_FMA_PEAK_TFMA = 148 * 128 * 1.965e9 / 1e12
+
+
+def model_convolve_fma_per_px(n_max: int, radius: int, tile_h: int = 64) -> float:
+    """Algorithmic FP32 FMAs per pixel of the fused model convolve: the NX
+    shared x passes over the tile plus its y halo, the nc y passes, the blend."""
+    nx = n_max + 1
+    nc = (n_max + 1) * (n_max + 2) // 2
+    ks = 2 * radius + 1
+    return nx * ks * (tile_h + 2 * radius) / tile_h + nc * ks + nc
 MODEL_CONVOLVE_STAGE = "subtract: model convolve"
 
 
@@ -540,6 +552,17 @@ def run_gpu(args) -> int:
                         "traffic": load_traffic(MODEL_CONVOLVE_STAGE, size), "peak_source": peak_kind,
                         "algorithmic_bytes_per_launch": bytes_launch, "ms_per_launch": 1e3 * per_launch,
                         "timed_in": "the one-frame-at-a-time mixed pass"}
+            sol = out64.get("solution")
+            if sol is not None:
+                from delta_b200 import _core
+
+                radius = int(_core._resolve_radius(float(sol.beta), int(sol.n_max), int(sol.radius)))
+                fma = model_convolve_fma_per_px(int(sol.n_max), radius) * size * size
+                tfma = fma / per_launch / 1e12
+                roofline["compute"] = {"bound": "fp32_fma", "achieved_tfma_s": tfma,
+                                       "peak_tfma_s": FP32_FMA_PEAK_TFMA, "frac": tfma / FP32_FMA_PEAK_TFMA,
+                                       "fma_per_launch": fma,
+                                       "note": "the kernel is FP32-issue-bound; HBM is not its limit"}
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline(pair, size)

@@ -478,38 +478,44 @@ k_variance(int w, int h, DevFields F, const float* __restrict__ phi, int rk, int
     // so a warp's window loads hit distinct banks). Per output the taps are
     // still accumulated in (ly, lx) order.
     const int tx = tid & 15, oy0 = (tid >> 4) * 4;
-    float acc[4][4];
+    // acc[i][p] holds columns 2p and 2p + 1 of row i as a pair: one packed FMA
+    // (__ffma2_rn, an IEEE fma per lane) per tap for two columns.
+    float2 acc[4][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+      for (int p = 0; p < 2; ++p) acc[i][p] = make_float2(0.0f, 0.0f);
     if (flat) {
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = q * win[(oy0 + i + rk) * iw + tx + 16 * j + rk];
+        for (int p = 0; p < 2; ++p) {
+          const float* wp = win + (oy0 + i + rk) * iw + tx + 32 * p + rk;
+          acc[i][p] = make_float2(q * wp[0], q * wp[16]);
+        }
     } else {
       for (int r = 0; r <= 3 + 2 * hw; ++r) {
         const float* wrp = win + (oy0 + lo + r) * iw + tx;
         for (int lx = lo; lx <= hi; ++lx) {
-          float v[4];
+          float2 v[2];
 #pragma unroll
-          for (int j = 0; j < 4; ++j) v[j] = wrp[16 * j + lx];
+          for (int p = 0; p < 2; ++p) v[p] = make_float2(wrp[32 * p + lx], wrp[32 * p + 16 + lx]);
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
             const int ly = lo + r - i;
             if (ly < lo || ly > hi) continue;
             const float c = kf[ly * ks + lx];
             if (!all_finite && c == 0.0f) continue;
+            const float2 cc = make_float2(c, c);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] = __fmaf_rn(c, v[j], acc[i][j]);
+            for (int p = 0; p < 2; ++p) acc[i][p] = __ffma2_rn(cc, v[p], acc[i][p]);
           }
         }
       }
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f + acc[i][j];
+        for (int p = 0; p < 2; ++p) acc[i][p] = make_float2(0.0f + acc[i][p].x, 0.0f + acc[i][p].y);
     }
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -520,7 +526,7 @@ k_variance(int w, int h, DevFields F, const float* __restrict__ phi, int rk, int
         const int ox = tx + 16 * j;
         if (ox >= bw) continue;
         const size_t o = static_cast<size_t>(by + oy) * w + bx + ox;
-        float v = acc[i][j];
+        float v = (j & 1) ? acc[i][j >> 1].y : acc[i][j >> 1].x;
         if (var_s) v = v + __ldg(var_s + o);
         var_out[o] = v;
       }
