@@ -313,20 +313,59 @@ k_isolate(int w, const unsigned* count, int cap, const int* __restrict__ sorted_
   (void)status;
 }
 
-__global__ void k_stamp_props(int w, int h, const float* __restrict__ img, const float* __restrict__ bg,
-                              const int* __restrict__ kept, const int* __restrict__ n_kept, int fwhm_radius,
-                              double* __restrict__ flux, double* __restrict__ snr, double* __restrict__ fwhm) {
-  const int nk = *n_kept;
+// One CTA per kept stamp: the threads stage the clipped weights
+// max(f - bg, 0) of the FWHM window in shared memory (0 off the frame, which
+// adds an exact zero where the reference skips the pixel), then thread 0 runs
+// the two FP64 moment passes of fwhm_dev in the same (dy, dx) order.
+__global__ void __launch_bounds__(256) k_stamp_props(int w, int h, const float* __restrict__ img,
+                                                      const float* __restrict__ bg, const int* __restrict__ kept,
+                                                      const int* __restrict__ n_kept, int fwhm_radius,
+                                                      double* __restrict__ flux, double* __restrict__ snr,
+                                                      double* __restrict__ fwhm) {
+  extern __shared__ double wt[];  // (2r+1)^2
+  const int i = blockIdx.x;
+  if (i >= *n_kept) return;
   const double med = static_cast<double>(bg[0]);
   const double sigma = 1.4826 * static_cast<double>(bg[1]);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nk; i += gridDim.x * blockDim.x) {
-    const int idx = kept[i];
-    const int x = idx % w, y = idx / w;
-    const double f = static_cast<double>(img[idx]) - med;
-    flux[i] = f;
-    snr[i] = sigma > 0.0 ? f / sigma : f;
-    fwhm[i] = fwhm_dev(img, w, h, x, y, fwhm_radius, med);
+  const int idx = kept[i];
+  const int x = idx % w, y = idx / w;
+  const int r = fwhm_radius, side = 2 * r + 1;
+  for (int e = threadIdx.x; e < side * side; e += blockDim.x) {
+    const int yy = y - r + e / side, xx = x - r + e % side;
+    double v = 0.0;
+    if (yy >= 0 && yy < h && xx >= 0 && xx < w) {
+      const double f = static_cast<double>(img[static_cast<size_t>(yy) * w + xx]) - med;
+      v = f > 0.0 ? f : 0.0;
+    }
+    wt[e] = v;
   }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const double f0 = static_cast<double>(img[idx]) - med;
+  flux[i] = f0;
+  snr[i] = sigma > 0.0 ? f0 / sigma : f0;
+  double sum = 0.0, sx = 0.0, sy = 0.0;
+  for (int dy = -r; dy <= r; ++dy)
+    for (int dx = -r; dx <= r; ++dx) {
+      const double wv = wt[(dy + r) * side + dx + r];
+      sum += wv;
+      sx += wv * dx;
+      sy += wv * dy;
+    }
+  double out = __longlong_as_double(0x7ff8000000000000ll);
+  if (sum > 0.0) {
+    const double mx = sx / sum, my = sy / sum;
+    double sxx = 0.0, syy = 0.0;
+    for (int dy = -r; dy <= r; ++dy)
+      for (int dx = -r; dx <= r; ++dx) {
+        const double wv = wt[(dy + r) * side + dx + r];
+        sxx += wv * (dx - mx) * (dx - mx);
+        syy += wv * (dy - my) * (dy - my);
+      }
+    const double var = 0.5 * (sxx / sum + syy / sum);
+    if (var > 0.0) out = 2.354820045030949 * sqrt(var);
+  }
+  fwhm[i] = out;
 }
 
 // Catalog positions: footprint check on both images + FWHM on both
@@ -573,8 +612,11 @@ int run_detect(Context& c, int w, int h, const float* img, const uint8_t* mask, 
   res.fwhm.assign(nkept, 0);
   if (nkept > 0) {
     double* props = static_cast<double*>(c.slot(which ? kSlotCompOut : kSlotCompStats, sizeof(double) * 3 * nkept));
-    k_stamp_props<<<(nkept + 127) / 128, 128, 0, s>>>(w, h, img, bg, kept, nk, p.fwhm_radius, props, props + nkept,
-                                                      props + 2 * nkept);
+    const size_t psmem = sizeof(double) * static_cast<size_t>(2 * p.fwhm_radius + 1) * (2 * p.fwhm_radius + 1);
+    if (psmem > 200 * 1024) fail(DGPU_ERR_INVALID, "detect_stamps: fwhm_radius too large");
+    ensure_dynamic_smem(reinterpret_cast<const void*>(k_stamp_props), psmem);
+    k_stamp_props<<<nkept, 256, psmem, s>>>(w, h, img, bg, kept, nk, p.fwhm_radius, props, props + nkept,
+                                            props + 2 * nkept);
     DGPU_LAUNCH("k_stamp_props");
     std::vector<int> hk(nkept);
     DGPU_CUDA(cudaMemcpyAsync(hk.data(), kept, sizeof(int) * nkept, cudaMemcpyDeviceToHost, s));

@@ -603,51 +603,57 @@ k_ola_gather(int w, int h, int n, const int* __restrict__ oxs, int nox, const in
              const double* __restrict__ hwin, const float* __restrict__ bout, const double* __restrict__ bnum,
              const double* __restrict__ wx_total, const double* __restrict__ wy_total, float* __restrict__ acc,
              float* __restrict__ var_acc) {
-  const int64_t npx = static_cast<int64_t>(w) * h;
+  // Frame rows stride over blockIdx.y: a row's covering block rows, their
+  // Hann weights and the row weight total are the same for the whole CTA.
   const int s = n / 2;
   const double inv_n2 = static_cast<double>(1.0f / static_cast<float>(static_cast<size_t>(n) * n));
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < npx;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int x = static_cast<int>(i % w), y = static_cast<int>(i / w);
-    // Largest origin index <= x (regular origins at multiples of s, then the flush origin).
-    int ixh = min(x / max(s, 1), nox - 1);
-    while (ixh + 1 < nox && oxs[ixh + 1] <= x) ++ixh;
-    while (ixh > 0 && oxs[ixh] > x) --ixh;
+  for (int y = blockIdx.y; y < h; y += gridDim.y) {
+    // Largest origin index <= y (regular origins at multiples of s, then the flush origin).
     int iyh = min(y / max(s, 1), noy - 1);
     while (iyh + 1 < noy && oys[iyh + 1] <= y) ++iyh;
     while (iyh > 0 && oys[iyh] > y) --iyh;
-    // Covering origins form the index ranges [ixl, ixh] x [iyl, iyh] (at most 3
-    // each, so at most one index per residue mod 3).
-    int ixl = ixh, iyl = iyh;
-    while (ixl > 0 && ixl > ixh - 2 && oxs[ixl - 1] + n > x) --ixl;
+    int iyl = iyh;
     while (iyl > 0 && iyl > iyh - 2 && oys[iyl - 1] + n > y) --iyl;
-    float a = 0.0f, v = 0.0f;
+    const double wyt = wy_total[y];
+    float* arow = acc + static_cast<size_t>(y) * w;
+    float* vrow = var_acc + static_cast<size_t>(y) * w;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < w; x += gridDim.x * blockDim.x) {
+      int ixh = min(x / max(s, 1), nox - 1);
+      while (ixh + 1 < nox && oxs[ixh + 1] <= x) ++ixh;
+      while (ixh > 0 && oxs[ixh] > x) --ixh;
+      // Covering origins form the index ranges [ixl, ixh] x [iyl, iyh] (at most 3
+      // each, so at most one index per residue mod 3).
+      int ixl = ixh;
+      while (ixl > 0 && ixl > ixh - 2 && oxs[ixl - 1] + n > x) --ixl;
+      float a = 0.0f, v = 0.0f;
 #pragma unroll
-    for (int ca = 0; ca < 3; ++ca) {  // colour q = (ix % 3) * 3 + (iy % 3), ascending
-      const int ix = ixh - (((ixh - ca) % 3) + 3) % 3;
-      if (ix < ixl) continue;
-#pragma unroll
-      for (int cb = 0; cb < 3; ++cb) {
-        const int iy = iyh - (((iyh - cb) % 3) + 3) % 3;
-        if (iy < iyl) continue;
-        const int item = iy * nox + ix;
-        const int ly = y - oys[iy], lx = x - oxs[ix];
-        const float f = bout[(static_cast<size_t>(item) * n + ly) * n + lx];
-        const double num = bnum[item];
-        const double wy_sig = hwin[ly] * inv_n2;
-        const double wy_var = hwin[ly];
+      for (int ca = 0; ca < 3; ++ca) {  // colour q = (ix % 3) * 3 + (iy % 3), ascending
+        const int ix = ixh - (((ixh - ca) % 3) + 3) % 3;
+        if (ix < ixl) continue;
+        const int lx = x - oxs[ix];
         const double wxv = hwin[lx];
-        a = static_cast<float>(static_cast<double>(a) + wy_sig * wxv * static_cast<double>(f));
-        v = static_cast<float>(static_cast<double>(v) + wy_var * wxv * num);
+#pragma unroll
+        for (int cb = 0; cb < 3; ++cb) {
+          const int iy = iyh - (((iyh - cb) % 3) + 3) % 3;
+          if (iy < iyl) continue;
+          const int item = iy * nox + ix;
+          const int ly = y - oys[iy];
+          const float f = bout[(static_cast<size_t>(item) * n + ly) * n + lx];
+          const double num = bnum[item];
+          const double wy_sig = hwin[ly] * inv_n2;
+          const double wy_var = hwin[ly];
+          a = static_cast<float>(static_cast<double>(a) + wy_sig * wxv * static_cast<double>(f));
+          v = static_cast<float>(static_cast<double>(v) + wy_var * wxv * num);
+        }
       }
-    }
-    const double ws = wy_total[y] * wx_total[x];
-    if (ws > 0.0) {
-      acc[i] = static_cast<float>(static_cast<double>(a) / ws);
-      var_acc[i] = static_cast<float>(static_cast<double>(v) / ws);
-    } else {
-      acc[i] = 0.0f;
-      var_acc[i] = 0.0f;
+      const double ws = wyt * wx_total[x];
+      if (ws > 0.0) {
+        arow[x] = static_cast<float>(static_cast<double>(a) / ws);
+        vrow[x] = static_cast<float>(static_cast<double>(v) / ws);
+      } else {
+        arow[x] = 0.0f;
+        vrow[x] = 0.0f;
+      }
     }
   }
 }
@@ -915,10 +921,10 @@ void launch_block_filter(cudaStream_t s, const FftGeom& g, int nitems, const flo
 void launch_ola_gather(cudaStream_t s, int w, int h, int n, const int* oxs, int nox, const int* oys, int noy,
                        const double* hwin, const float* bout, const double* bnum, const double* wx_total,
                        const double* wy_total, float* acc, float* var_acc) {
-  const int64_t npx = static_cast<int64_t>(w) * h;
-  const int blocks = static_cast<int>(std::min<int64_t>((npx + 255) / 256, 148 * 16));
-  k_ola_gather<<<blocks, 256, 0, s>>>(w, h, n, oxs, nox, oys, noy, hwin, bout, bnum, wx_total, wy_total, acc,
-                                      var_acc);
+  if (w <= 0 || h <= 0) return;
+  const dim3 grid(static_cast<unsigned>(std::min(ceil_div(w, 256), 16)), static_cast<unsigned>(std::min(h, 65535)));
+  k_ola_gather<<<grid, 256, 0, s>>>(w, h, n, oxs, nox, oys, noy, hwin, bout, bnum, wx_total, wy_total, acc,
+                                    var_acc);
   DGPU_LAUNCH("k_ola_gather");
 }
 
