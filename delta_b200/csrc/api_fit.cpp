@@ -194,13 +194,29 @@ struct Engine {
     launch_normal_equations(c, prec, N, nc, k, SS, R, mask, M);
   }
 
-  // One FP64 refinement step of system s at lambda (theta updated in place).
-  void refine(const Work& w, int s, double lam, const uint8_t* mask, double* theta) {
-    double* r = static_cast<double*>(c.slot(kSlotFit15, sizeof(double) * 2 * P));
-    launch_rhs(c, N, nc, k, SS, R, mask, theta, r, nullptr, nullptr);
-    launch_refine_update(c.stream, P, k, d_pen, lam, theta, r);
-    launch_apply_inverse(c.stream, batch_of(w), s, r, r + P);
-    launch_axpy(c.stream, P, r + P, theta);
+  // Mixed precision: the residual of an anchor theta0 in FP64 (e0 = t - X theta0),
+  // r0 = X^T W e0 and s0 = e0^T W e0, from which the rss of any theta follows
+  // as s0 - 2 (theta - theta0) . r0 + (theta - theta0)^T M (theta - theta0).
+  // Near the anchor the BF16x3 error of M enters only through the small
+  // quadratic term, where ywy - 2 theta . rhs + theta^T M theta would carry it
+  // at the scale of ywy (the rss is often 1e-4 of ywy or less).
+  struct Anchor {
+    double *r0, *rp, *delta, *s0;
+  };
+  Anchor anchor_buffers() {
+    double* a = static_cast<double*>(c.slot(kSlotFit15, sizeof(double) * (3 * static_cast<size_t>(P) + 2)));
+    return Anchor{a, a + P, a + 2 * P, a + 3 * P};
+  }
+  void anchor_at(const Anchor& a, const double* theta, const uint8_t* mask) {
+    launch_rhs(c, N, nc, k, SS, R, mask, theta, a.r0, a.s0, nullptr);
+  }
+
+  // Mixed precision: rss / GCV of every system of the batch around the anchor.
+  std::vector<double> anchored_curve(const Work& w, int nsys, const double* M, const Anchor& a,
+                                     const double* theta0, const long long* n) {
+    launch_quad_err(c, nsys, P, w.theta, M, nullptr, a.r0, nullptr, a.s0, w.raw, theta0);
+    launch_gcv_finish(c.stream, nsys, w.raw, w.edf, w.ok, n, w.rss, w.gcv);
+    return down(c, w.gcv, nsys);
   }
 
   GlsOut gcv(const std::vector<double>& grid, const uint8_t* mask) {
@@ -220,24 +236,48 @@ struct Engine {
     GlsOut o;
     o.grid = grid;
     o.curve = down(c, w.gcv, nl);
-    int best = 0;
-    double bg = kInf;
-    for (int i = 0; i < nl; ++i)
-      if (o.curve[i] < bg) {
-        bg = o.curve[i];
-        best = i;
+    auto argmin = [&]() {
+      int b = 0;
+      double bg = kInf;
+      for (int i = 0; i < nl; ++i)
+        if (o.curve[i] < bg) {
+          bg = o.curve[i];
+          b = i;
+        }
+      return b;
+    };
+    int best = argmin();
+    int anchored = -1;
+    if (prec == DGPU_PREC_MIXED) {
+      // Re-evaluate the curve around the provisional minimum until the minimum
+      // stays put (it moves at most a grid step or two).
+      const Anchor a = anchor_buffers();
+      for (int pass = 0; pass < 3 && anchored != best; ++pass) {
+        const double* th0 = w.theta + static_cast<size_t>(best) * P;
+        anchor_at(a, th0, mask);
+        anchored = best;
+        o.curve = anchored_curve(w, nl, M, a, th0, n);
+        best = argmin();
       }
-    finish_single(w, best, grid[best], M, rhs, ywy, n, mask, o);
+    }
+    finish_single(w, best, grid[best], M, n, mask, o, anchored == best);
     return o;
   }
 
-  // Fill theta / scalars of system `s` (optionally refined) into o.
-  void finish_single(const Work& w, int s, double lam, const double* M, const double* rhs, const double* ywy,
-                     const long long* n, const uint8_t* mask, GlsOut& o) {
+  // Fill theta / scalars of system `s` into o. Mixed precision: one FP64
+  // refinement step from the anchor residual at theta_s (computed here unless
+  // `anchored`), and the rss / GCV of the refined theta around that anchor.
+  void finish_single(const Work& w, int s, double lam, const double* M, const long long* n, const uint8_t* mask,
+                     GlsOut& o, bool anchored = false) {
     double* th = w.theta + static_cast<size_t>(s) * P;
     if (prec == DGPU_PREC_MIXED) {
-      refine(w, s, lam, mask, th);
-      launch_quad_err(c, 1, P, th, M, nullptr, rhs, nullptr, ywy, w.raw + s);
+      const Anchor a = anchor_buffers();
+      if (!anchored) anchor_at(a, th, mask);
+      DGPU_CUDA(cudaMemcpyAsync(a.rp, a.r0, sizeof(double) * P, cudaMemcpyDeviceToDevice, c.stream));
+      launch_refine_update(c.stream, P, k, d_pen, lam, th, a.rp);
+      launch_apply_inverse(c.stream, batch_of(w), s, a.rp, a.delta);
+      launch_axpy(c.stream, P, a.delta, th);
+      launch_quad_err(c, 1, P, a.delta, M, nullptr, a.r0, nullptr, a.s0, w.raw + s);
       launch_gcv_finish(c.stream, 1, w.raw + s, w.edf + s, w.ok + s, n, w.rss + s, w.gcv + s);
     }
     o.theta.resize(P);
@@ -265,7 +305,7 @@ struct Engine {
     launch_quad_err(c, 1, P, w.theta, M, nullptr, rhs, nullptr, ywy, w.raw);
     launch_gcv_finish(c.stream, 1, w.raw, w.edf, w.ok, n, w.rss, w.gcv);
     GlsOut o;
-    finish_single(w, 0, lam, M, rhs, ywy, n, mask, o);
+    finish_single(w, 0, lam, M, n, mask, o);
     return o;
   }
 
@@ -341,7 +381,12 @@ struct Engine {
     std::vector<double> curve(nl, kInf);
     std::vector<char> done(nl, 0);
     Work w = work(std::max(nl * G, 1), G);
-    auto evaluate = [&](const std::vector<int>& idx) {
+    // Mixed precision, row folds: held-out errors around per-fold anchors
+    // (th0[g], with the FP64 residual sums r0[g], s0[g] over fold g's rows).
+    double* th0 = nullptr;
+    double* r0 = nullptr;
+    double* s0 = nullptr;
+    auto solve_at = [&](const std::vector<int>& idx) {
       const int m = static_cast<int>(idx.size());
       const int ns = m * G;
       std::vector<double> lam(ns);
@@ -354,7 +399,15 @@ struct Engine {
       DGPU_CUDA(cudaMemcpyAsync(w.lam, lam.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, c.stream));
       DGPU_CUDA(cudaMemcpyAsync(w.midx, mi.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, c.stream));
       solve(w, ns, Mt, w.midx, rt, w.midx, G);
-      launch_quad_err(c, ns, P, w.theta, Mg, w.midx, rg, w.midx, yg, w.raw);
+      return ns;
+    };
+    auto evaluate = [&](const std::vector<int>& idx) {
+      const int m = static_cast<int>(idx.size());
+      const int ns = solve_at(idx);
+      if (th0)
+        launch_quad_err(c, ns, P, w.theta, Mg, w.midx, r0, w.midx, s0, w.raw, th0);
+      else
+        launch_quad_err(c, ns, P, w.theta, Mg, w.midx, rg, w.midx, yg, w.raw);
       const auto err = down(c, w.raw, ns);
       const auto ok = down(c, w.ok, ns);
       for (int ii = 0; ii < m; ++ii) {
@@ -409,6 +462,44 @@ struct Engine {
         bc = curve[li];
         best = li;
       }
+    if (prec == DGPU_PREC_MIXED && !stamped) {
+      // Re-evaluate every searched lambda around the folds' solutions at the
+      // provisional minimum until the minimum stays put.
+      const size_t gp = static_cast<size_t>(G) * P;
+      char* ab = static_cast<char*>(c.slot(kSlotFit12, sizeof(double) * (2 * gp + G) + static_cast<size_t>(G) * n_units));
+      double* a_th = reinterpret_cast<double*>(ab);
+      double* a_r = a_th + gp;
+      double* a_s = a_r + gp;
+      uint8_t* fmasks = reinterpret_cast<uint8_t*>(a_s + G);
+      {
+        const auto hm = down(c, mask, n_units);
+        std::vector<uint8_t> m(static_cast<size_t>(G) * n_units, 0);
+        for (int g = 0; g < G; ++g)
+          for (int u = 0; u < n_units; ++u) m[static_cast<size_t>(g) * n_units + u] = (hm[u] && fold[u] == g) ? 1 : 0;
+        DGPU_CUDA(cudaMemcpyAsync(fmasks, m.data(), m.size(), cudaMemcpyHostToDevice, c.stream));
+      }
+      std::vector<int> searched;
+      for (int li = 0; li < nl; ++li)
+        if (done[li]) searched.push_back(li);
+      for (int pass = 0, anchored = -1; pass < 3 && anchored != best; ++pass) {
+        solve_at({best});
+        DGPU_CUDA(cudaMemcpyAsync(a_th, w.theta, sizeof(double) * gp, cudaMemcpyDeviceToDevice, c.stream));
+        for (int g = 0; g < G; ++g)
+          launch_rhs(c, N, nc, k, SS, R, fmasks + static_cast<size_t>(g) * n_units, a_th + static_cast<size_t>(g) * P,
+                     a_r + static_cast<size_t>(g) * P, a_s + g, nullptr);
+        th0 = a_th;
+        r0 = a_r;
+        s0 = a_s;
+        anchored = best;
+        evaluate(searched);
+        bc = kInf;
+        for (int li : searched)
+          if (curve[li] < bc) {
+            bc = curve[li];
+            best = li;
+          }
+      }
+    }
     // Final all-data fit at the selected lambda.
     Work w1 = work(1);
     DGPU_CUDA(cudaMemcpyAsync(w1.lam, &grid[best], sizeof(double), cudaMemcpyHostToDevice, c.stream));
@@ -416,7 +507,7 @@ struct Engine {
     launch_quad_err(c, 1, P, w1.theta, Mall, nullptr, rall, nullptr, yall, w1.raw);
     launch_gcv_finish(c.stream, 1, w1.raw, w1.edf, w1.ok, nall, w1.rss, w1.gcv);
     GlsOut o;
-    finish_single(w1, 0, grid[best], Mall, rall, yall, nall, mask, o);
+    finish_single(w1, 0, grid[best], Mall, nall, mask, o);
     o.grid = grid;
     o.curve = curve;
     return o;

@@ -35,10 +35,12 @@ void launch_stamp_gather(cudaStream_t st, const StampGeom& g, int n_stamps, cons
 void launch_design_weights(cudaStream_t st, int64_t N, const TpsDev& t, const FitRows& R, int have_var);
 void launch_normal_equations(Context& c, int prec, int64_t N, int nc, int k, int SS, const FitRows& R,
                              const uint8_t* accepted, double* M);
-// Mixed precision (BF16x3 tcgen05) partials of the Kronecker-packed normal
-// equations: gpart[z][u][v] per row split z; returns the split count.
-int launch_normal_tc(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, const uint8_t* accepted,
-                     const int2* upairs, int Mu, const int2* vpairs, int Nv, Slot gpart_slot, double** gpart_out);
+// Mixed precision (BF16x3 tcgen05) Kronecker-packed normal equations:
+// G[u][v] (row-major Mu x Nv, FP64) from per-split partials in gpart_slot.
+void launch_normal_tc(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, const uint8_t* accepted,
+                      const int2* upairs, int Mu, const int2* vpairs, int Nv, Slot gpart_slot, double* g);
+// rhs = X^T W t and ywy = t^T W t over the active rows; with theta, the same
+// sums of the residual e = t - X theta (rhs = X^T W e, ywy = e^T W e).
 void launch_rhs(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, const uint8_t* accepted,
                 const double* theta, double* rhs, double* ywy, long long* n);
 void launch_stamp_chi2(cudaStream_t st, int n_stamps, int nc, int k, int SS, const FitRows& R,

@@ -5,8 +5,11 @@
 
 namespace dgpu {
 
+// out[s] = y - 2 (theta_s - anchor) . r + (theta_s - anchor)^T M (theta_s - anchor),
+// with y, r and the anchor chosen by r_index; anchor null: theta_s itself.
 void launch_quad_err(Context& c, int nsys, int P, const double* theta, const double* M, const int* m_index,
-                     const double* r, const int* r_index, const double* y, double* out);
+                     const double* r, const int* r_index, const double* y, double* out,
+                     const double* anchor = nullptr);
 void launch_gcv_finish(cudaStream_t st, int nsys, const double* raw, const double* edf, const int* ok,
                        const long long* n, double* rss, double* gcv);
 void launch_fold_train(cudaStream_t st, int groups, size_t len, const double* part, double* all, double* train);

@@ -368,27 +368,25 @@ void launch_normal_equations(Context& c, int prec, int64_t N, int nc, int k, int
   DGPU_CUDA(cudaMemcpyAsync(dpairs, up.data(), sizeof(int2) * Mu, cudaMemcpyHostToDevice, st));
   DGPU_CUDA(cudaMemcpyAsync(dpairs + Mu, vp.data(), sizeof(int2) * Nv, cudaMemcpyHostToDevice, st));
   double* g = static_cast<double*>(c.slot(kSlotFit12, sizeof(double) * static_cast<size_t>(Mu) * Nv));
-  double* gpart = nullptr;
-  int nsplit = 0;
   if (prec == DGPU_PREC_MIXED) {
-    nsplit = launch_normal_tc(c, N, nc, k, SS, R, accepted, dpairs, Mu, dpairs + Mu, Nv, kSlotFit11, &gpart);
+    launch_normal_tc(c, N, nc, k, SS, R, accepted, dpairs, Mu, dpairs + Mu, Nv, kSlotFit11, g);
   } else {
     const int gx = (Mu + kNeT - 1) / kNeT, gy = (Nv + kNeT - 1) / kNeT;
     // Split K (rows) so the grid covers the GPU a few times over.
     const int64_t target_splits = std::max<int64_t>(1, (148 * 6) / (gx * gy));
     int64_t rps = std::max<int64_t>(kNeR * 8, (N + target_splits - 1) / target_splits);
     rps = (rps + kNeR - 1) / kNeR * kNeR;
-    nsplit = static_cast<int>((N + rps - 1) / rps);
-    gpart = static_cast<double*>(c.slot(kSlotFit11, sizeof(double) * static_cast<size_t>(nsplit) * Mu * Nv));
+    const int nsplit = static_cast<int>((N + rps - 1) / rps);
+    double* gpart = static_cast<double*>(c.slot(kSlotFit11, sizeof(double) * static_cast<size_t>(nsplit) * Mu * Nv));
     dim3 grid(gx, gy, nsplit);
     if (prec == DGPU_PREC_FP32)
       k_normal_kron<float><<<grid, 256, 0, st>>>(N, nc, k, SS, R, accepted, dpairs, Mu, dpairs + Mu, Nv, rps, gpart);
     else
       k_normal_kron<double><<<grid, 256, 0, st>>>(N, nc, k, SS, R, accepted, dpairs, Mu, dpairs + Mu, Nv, rps, gpart);
     DGPU_LAUNCH("k_normal_kron");
+    k_reduce_g<<<std::min(148 * 4, (Mu * Nv + 255) / 256), 256, 0, st>>>(nsplit, Mu * Nv, gpart, g);
+    DGPU_LAUNCH("k_reduce_g");
   }
-  k_reduce_g<<<std::min(148 * 4, (Mu * Nv + 255) / 256), 256, 0, st>>>(nsplit, Mu * Nv, gpart, g);
-  DGPU_LAUNCH("k_reduce_g");
   const int P = nf * k;
   k_expand_m<<<std::min(148 * 8, (P * P + 255) / 256), 256, 0, st>>>(nf, k, Nv, g, M);
   DGPU_LAUNCH("k_expand_m");
@@ -396,7 +394,7 @@ void launch_normal_equations(Context& c, int prec, int64_t N, int nc, int k, int
 
 // ---------------------------------------------------------------------------
 // rhs = sum_i w_i e_i (b_i (x) d_i) with e_i = t_i (plain rhs) or
-// e_i = t_i - x_i . theta (FP64 refinement residual), plus ywy = sum w t^2
+// e_i = t_i - x_i . theta (FP64 refinement residual), plus ywy = sum w e^2
 // and the active-row count. One CTA per row chunk, rows staged in shared memory.
 // ---------------------------------------------------------------------------
 constexpr int kRhsRows = 128;
@@ -477,8 +475,8 @@ k_rhs(int64_t N, int nc, int k, int SS, FitRows R, const uint8_t* __restrict__ a
       if (act) {
         double t = R.t[row];
         const double wv = R.w[row];
-        wtt = wv * t * t;
         if (theta) t = t - row_model_any(sd + e * k, sb + e * nf, nc, k, sth);
+        wtt = wv * t * t;
         we = wv * t;
       }
       se[e] = we;
@@ -564,7 +562,7 @@ k_rhs_mma(int64_t N, int nc, int k, int SS, FitRows R, const uint8_t* __restrict
     if (act) {
       t = R.t[row];
       wv = R.w[row];
-      yacc = fma(wv * t, t, yacc);
+      if (theta == nullptr) yacc = fma(wv * t, t, yacc);
       ++nacc;
     }
     if (theta != nullptr) {
@@ -603,7 +601,10 @@ k_rhs_mma(int64_t N, int nc, int k, int SS, FitRows R, const uint8_t* __restrict
         if (kq == 0) s_model[warp][rt * 8 + q] = part;
       }
       __syncwarp();
-      if (act) t = t - s_model[warp][lane];
+      if (act) {
+        t = t - s_model[warp][lane];
+        yacc = fma(wv * t, t, yacc);
+      }
     }
     s_we[warp][lane] = act ? wv * t : 0.0;
     __syncwarp();

@@ -29,6 +29,10 @@ __device__ double block_sum(double v, double* red) {
 }
 
 // theta^T Mq theta - 2 theta . rq + yq for system s (M/r/y chosen by index).
+// With an anchor theta0 (one per r index) the vector is theta - theta0: given
+// rq = X^T W e0 and yq = e0^T W e0 for the residual e0 = t - X theta0, that is
+// the rss of theta expanded around theta0, whose quadratic term is small near
+// the anchor.
 // Grid (row blocks of kQRows, systems): each CTA forms the partial sums of its
 // rows (one warp per row of M, coalesced); k_quad_finish adds the row blocks
 // of each system in a fixed order.
@@ -36,13 +40,16 @@ constexpr int kQRows = 32;
 
 __global__ void __launch_bounds__(256)
 k_quad_err(int P, const double* __restrict__ theta, const double* __restrict__ M, const int* __restrict__ m_index,
-           const double* __restrict__ r, const int* __restrict__ r_index, double* __restrict__ part) {
+           const double* __restrict__ r, const int* __restrict__ r_index, const double* __restrict__ anchor,
+           double* __restrict__ part) {
   __shared__ double red[256];
   __shared__ double th[1024];
   const int b = blockIdx.x, s = blockIdx.y, nb = gridDim.x;
   const double* Mq = M + (m_index ? static_cast<size_t>(m_index[s]) * P * P : 0);
   const double* rq = r + (r_index ? static_cast<size_t>(r_index[s]) * P : 0);
-  for (int p = threadIdx.x; p < P; p += blockDim.x) th[p] = theta[static_cast<size_t>(s) * P + p];
+  const double* aq = anchor ? anchor + (r_index ? static_cast<size_t>(r_index[s]) * P : 0) : nullptr;
+  for (int p = threadIdx.x; p < P; p += blockDim.x)
+    th[p] = theta[static_cast<size_t>(s) * P + p] - (aq ? aq[p] : 0.0);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int p0 = b * kQRows, p1 = min(P, p0 + kQRows);
@@ -77,11 +84,11 @@ __global__ void k_quad_finish(int nsys, int nb, const double* __restrict__ part,
 }
 
 void launch_quad_err(Context& c, int nsys, int P, const double* theta, const double* M, const int* m_index,
-                     const double* r, const int* r_index, const double* y, double* out) {
+                     const double* r, const int* r_index, const double* y, double* out, const double* anchor) {
   if (nsys == 0) return;
   const int nb = (P + kQRows - 1) / kQRows;
   double* part = static_cast<double*>(c.slot(kSlotGlsPart, sizeof(double) * 2 * static_cast<size_t>(nb) * nsys));
-  k_quad_err<<<dim3(nb, nsys), 256, 0, c.stream>>>(P, theta, M, m_index, r, r_index, part);
+  k_quad_err<<<dim3(nb, nsys), 256, 0, c.stream>>>(P, theta, M, m_index, r, r_index, anchor, part);
   DGPU_LAUNCH("k_quad_err");
   k_quad_finish<<<(nsys + 127) / 128, 128, 0, c.stream>>>(nsys, nb, part, y, r_index, out);
   DGPU_LAUNCH("k_quad_finish");

@@ -13,9 +13,13 @@
 // for hi*hi + hi*lo + lo*hi into the TMEM accumulator (BF16x3: about 16
 // significant bits per product, FP32 accumulation). Two shared-memory stages
 // let the tensor core consume chunk c while the threads generate chunk c+1;
-// tcgen05.commit on an mbarrier releases a stage. The epilogue reads TMEM
-// with tcgen05.ld and writes FP64 partials; the host-side caller reduces the
-// splits in a fixed order in FP64 and an FP64 refinement step follows the solve.
+// tcgen05.commit on an mbarrier releases a stage. Every kDrainChunks chunks
+// the CTA waits for its MMAs, reads the accumulator with tcgen05.ld and adds
+// it into its FP64 partial in global memory, and the next chunk starts a fresh
+// accumulation: each FP32 accumulation chain is at most 12 kDrainChunks MMAs
+// long, where a whole split (80+ chunks) would lose about 1e-4 of the sums
+// to FP32 accumulation rounding. The host-side caller reduces the splits in a
+// fixed order in FP64 and an FP64 refinement step follows the solve.
 //
 // Every mbarrier wait is bounded: on expiry the kernel sets the loop-limit
 // status bit, waits (bounded) for its own MMAs, frees its TMEM and returns.
@@ -35,6 +39,7 @@ constexpr int kKC = 64;        // stamp rows per chunk (4 UMMA K-steps of 16)
 constexpr int kThreads = 512;
 constexpr int kRS = kKC + 4;  // staged row-value stride (floats): rows contiguous, banks staggered
 constexpr long long kSpinCap = 1ll << 22;
+constexpr int kDrainChunks = 4;  // chunks per FP32 accumulation chain
 
 struct TcArgs {
   int64_t N;
@@ -48,7 +53,7 @@ struct TcArgs {
   int BN;  // N tile, multiple of 16, <= 256
   int tmem_cols;
   int64_t rows_per_split;
-  double* gpart;
+  double* gpart;  // per split: tiles x BN x kBM, (tile, column, row) order
   unsigned* status;
   int bulk;  // row arrays 16-byte aligned: full chunks arrive by cp.async.bulk
 };
@@ -236,6 +241,35 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
     if (tid == 0) issue_rows(0);
   }
 
+  // Accumulator -> FP64 partial of this split: warp w reads TMEM lanes
+  // 32 (w % 4) .. +31 (tile rows); the warp groups split the column blocks of
+  // 16. The partial is column-major within the tile, so each column of a
+  // warp's 32 rows is one contiguous 256-byte access. The first drain stores,
+  // later ones add; padding rows and columns hold zeros.
+  const int warp = tid >> 5, lane = tid & 31;
+  const int quarter = warp & 3, grp = warp >> 2, ngrp = (blockDim.x >> 5) / 4;
+  double* out = a.gpart +
+                (static_cast<size_t>(blockIdx.z) * gridDim.x * gridDim.y + blockIdx.x * gridDim.y + blockIdx.y) *
+                    static_cast<size_t>(BN) * kBM +
+                quarter * 32 + lane;
+  auto drain = [&](bool first, bool valid) {
+    for (int cb = grp; cb < BN / 16; cb += ngrp) {
+      uint32_t r[16];
+      if (valid) {
+        tmem_ld16(tmem + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(cb * 16), r);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) r[j] = 0u;
+      }
+      double* o = out + static_cast<size_t>(cb) * 16 * kBM;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const double x = static_cast<double>(__uint_as_float(r[j]));
+        o[j * kBM] = first ? x : o[j * kBM] + x;
+      }
+    }
+  };
+
   int issued = 0;  // chunks whose MMAs were issued (uniform over the CTA)
   for (int c = 0; c < nchunks; ++c) {
     const int st = c & 1;
@@ -353,7 +387,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
 #pragma unroll
       for (int s = 0; s < kKC / 16; ++s) {
         const uint32_t ko = static_cast<uint32_t>(s) * 256;  // two core matrices per K-step of 16
-        const uint32_t acc0 = (c > 0 || s > 0) ? 1u : 0u;
+        const uint32_t acc0 = (c % kDrainChunks != 0 || s > 0) ? 1u : 0u;
         umma_bf16(tmem, umma_desc(ah + ko, kLBO, kSBO), umma_desc(bh + ko, kLBO, kSBO), idesc, acc0);
         umma_bf16(tmem, umma_desc(ah + ko, kLBO, kSBO), umma_desc(bl + ko, kLBO, kSBO), idesc, 1u);
         umma_bf16(tmem, umma_desc(al + ko, kLBO, kSBO), umma_desc(bh + ko, kLBO, kSBO), idesc, 1u);
@@ -361,6 +395,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
       umma_commit(&mbar[st]);
     }
     issued = c + 1;
+    if (issued % kDrainChunks == 0 && issued < nchunks) {
+      // Chunk c's commit covers every MMA of this chain; the next chunk's
+      // MMAs overwrite the accumulator only after the barrier below.
+      if (!mbar_wait(&mbar[st], static_cast<unsigned>(c >> 1) & 1u)) s_fail = 1;
+      __syncthreads();
+      if (s_fail) break;
+      tc_fence_after();
+      drain(issued == kDrainChunks, true);
+      tc_fence_before();
+      __syncthreads();
+    }
   }
 
   // Drain: wait for the most recent commit of each stage (the ones not waited
@@ -375,30 +420,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
   if (!ok && tid == 0) atomicOr(a.status, kStatusLoopLimit);
   tc_fence_after();
 
-  // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (tile rows); the
-  // warp groups split the column blocks of 16.
-  const int warp = tid >> 5, lane = tid & 31;
-  const int quarter = warp & 3, grp = warp >> 2, ngrp = (blockDim.x >> 5) / 4;
-  const int m = quarter * 32 + lane;
-  const int u = u0 + m;
-  const int ncb = BN / 16;
-  double* out = a.gpart + static_cast<size_t>(blockIdx.z) * a.Mu * a.Nv;
-  for (int cb = grp; cb < ncb; cb += ngrp) {
-    uint32_t r[16];
-    if (issued > 0 && ok) {
-      tmem_ld16(tmem + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(cb * 16), r);
-    } else {
-#pragma unroll
-      for (int j = 0; j < 16; ++j) r[j] = 0u;
-    }
-    if (u < a.Mu) {
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int v = v0 + cb * 16 + j;
-        if (v < a.Nv) out[static_cast<size_t>(u) * a.Nv + v] = static_cast<double>(__uint_as_float(r[j]));
-      }
-    }
-  }
+  // Epilogue: the last chain (stores when it is the only one; zeros after a
+  // failure, which the status bit reports).
+  if (issued > 0 && ok)
+    drain(issued <= kDrainChunks, true);
+  else
+    drain(true, false);
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
@@ -419,23 +446,49 @@ size_t normal_tc_smem(int nc, int k, int BN) {
   return s;
 }
 
-// G partials of the mixed-precision path: gpart[z][u][v] for every split z.
-// Returns the number of splits.
-int launch_normal_tc(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, const uint8_t* accepted,
-                     const int2* upairs, int Mu, const int2* vpairs, int Nv, Slot gpart_slot, double** gpart_out) {
-  const int tiles_n = (Nv + 255) / 256;
-  int BN = (Nv + tiles_n - 1) / tiles_n;
-  BN = (BN + 15) / 16 * 16;
+namespace {
+
+// G[u][v] = sum over the splits z (in order) of the tiled partials.
+__global__ void k_reduce_tiles(int nsplit, size_t split_len, int BN, int tiles_n, int Mu, int Nv,
+                               const double* __restrict__ gpart, double* __restrict__ g) {
+  for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < split_len;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int m = static_cast<int>(i % kBM);
+    const size_t cv = i / kBM;
+    const int col = static_cast<int>(cv % BN);
+    const int tile = static_cast<int>(cv / BN);
+    const int u = (tile / tiles_n) * kBM + m, v = (tile % tiles_n) * BN + col;
+    if (u >= Mu || v >= Nv) continue;
+    double s = 0.0;
+    for (int z = 0; z < nsplit; ++z) s += gpart[static_cast<size_t>(z) * split_len + i];
+    g[static_cast<size_t>(u) * Nv + v] = s;
+  }
+}
+
+}  // namespace
+
+// G of the mixed-precision path (row-major Mu x Nv, FP64).
+void launch_normal_tc(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, const uint8_t* accepted,
+                      const int2* upairs, int Mu, const int2* vpairs, int Nv, Slot gpart_slot, double* g) {
+  // Widest N tile (<= 256) whose staging fits; wide fits (many components and
+  // knots) trade a narrower B tile for more column tiles.
+  int tiles_n = (Nv + 255) / 256, BN = 0;
+  size_t smem = 0;
+  for (;; ++tiles_n) {
+    BN = ((Nv + tiles_n - 1) / tiles_n + 15) / 16 * 16;
+    smem = normal_tc_smem(nc, k, BN);
+    if (smem <= 227 * 1024 || BN <= 16) break;
+  }
   const int tiles_m = (Mu + kBM - 1) / kBM;
   const int tmem_cols = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
-  const size_t smem = normal_tc_smem(nc, k, BN);
   if (smem > 227 * 1024) fail(DGPU_ERR_INVALID, "fit_kernel: mixed-precision tile does not fit in shared memory");
   const int64_t chunks = (N + kKC - 1) / kKC;
   const int64_t want = std::max<int64_t>(1, 148 / std::max(1, tiles_m * tiles_n));
   int64_t rps = ((chunks + want - 1) / want) * kKC;
   rps = std::max<int64_t>(rps, kKC);
   const int nsplit = static_cast<int>(std::max<int64_t>(1, (N + rps - 1) / rps));
-  double* gpart = static_cast<double*>(c.slot(gpart_slot, sizeof(double) * static_cast<size_t>(nsplit) * Mu * Nv));
+  const size_t split_len = static_cast<size_t>(tiles_m) * tiles_n * BN * kBM;
+  double* gpart = static_cast<double*>(c.slot(gpart_slot, sizeof(double) * nsplit * split_len));
   TcArgs a;
   a.N = N;
   a.nc = nc;
@@ -458,8 +511,9 @@ int launch_normal_tc(Context& c, int64_t N, int nc, int k, int SS, const FitRows
   ensure_dynamic_smem(reinterpret_cast<const void*>(k_normal_tc), smem);
   k_normal_tc<<<dim3(tiles_m, tiles_n, nsplit), kThreads, smem, c.stream>>>(a);
   DGPU_LAUNCH("k_normal_tc");
-  *gpart_out = gpart;
-  return nsplit;
+  const int rb = static_cast<int>(std::min<size_t>(148 * 4, (split_len + 255) / 256));
+  k_reduce_tiles<<<rb, 256, 0, c.stream>>>(nsplit, split_len, BN, tiles_n, Mu, Nv, gpart, g);
+  DGPU_LAUNCH("k_reduce_tiles");
 }
 
 }  // namespace dgpu
