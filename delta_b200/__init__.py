@@ -42,7 +42,7 @@ from ._core import subtract as subtract_model
 from ._inputs import as_layers, synth_variance
 from ._lib import DeviceLoopLimitError, DeviceUnavailableError
 from ._log import configure_logging
-from .pipeline import DiffResult, Subtractor, apply, subtract, subtract_batch
+from .pipeline import DiffResult, Subtractor, apply, apply_batch, subtract, subtract_batch
 from .solution import KernelSolution
 
 
@@ -71,10 +71,10 @@ def write_fits(path: str, data, variance=None, mask=None, overwrite: bool = Fals
 
 __all__ = [
     "DeviceLoopLimitError", "DeviceUnavailableError", "DiffResult", "KernelSolution", "Subtractor", "__version__",
-    "apply", "as_layers", "basis_convolve", "catalog", "configure_logging", "decorrelate", "decorrelate_block",
-    "decorrelation_kernel", "detect_stamps", "estimate_background", "fit_kernel", "gauss_hermite_basis1d",
-    "gauss_hermite_kernels", "grid_knots", "matched_filter", "photometric_scale", "photometric_scale_at",
-    "read_fits", "select_stamps", "solve_gls", "solve_gls_cv", "solve_gls_gcv", "subtract", "subtract_batch", "subtract_model",
-    "synth_variance", "tps_design", "tps_evaluate", "tps_fit", "tps_penalty", "validation", "weighted_mean",
-    "whiten_score_psf", "write_fits",
+    "apply", "apply_batch", "as_layers", "basis_convolve", "catalog", "configure_logging", "decorrelate",
+    "decorrelate_block", "decorrelation_kernel", "detect_stamps", "estimate_background", "fit_kernel",
+    "gauss_hermite_basis1d", "gauss_hermite_kernels", "grid_knots", "matched_filter", "photometric_scale",
+    "photometric_scale_at", "read_fits", "select_stamps", "solve_gls", "solve_gls_cv", "solve_gls_gcv", "subtract",
+    "subtract_batch", "subtract_model", "synth_variance", "tps_design", "tps_evaluate", "tps_fit", "tps_penalty",
+    "validation", "weighted_mean", "whiten_score_psf", "write_fits",
 ]

@@ -458,6 +458,26 @@ class Subtractor:
         result.elapsed = time.perf_counter() - start
         return result
 
+    def apply_batch(self, solution: KernelSolution, frames, *, max_in_flight: int | None = None) -> list[DiffResult]:
+        """Apply one frozen solution to several frame pairs concurrently (an
+        extension: the reference applies a solution one frame at a time, through
+        apply()). Each item of `frames` is a dict of apply() keyword arguments
+        (science, reference and optionally the variance / mask layers, gain,
+        read_noise). Runs like subtract_batch(): up to `max_in_flight` frames
+        (default: up to 4) at once, each on its own host thread, library context
+        and CUDA stream, results in input order; every result equals what apply()
+        returns for that frame alone."""
+        items = [dict(f) for f in frames]
+        if not items:
+            return []
+        if not self._use_device():
+            return [self.apply(solution, **it) for it in items]
+        from . import _device
+
+        ex = _device.runner(max_in_flight or min(len(items), 4))
+        futs = [ex.submit(_device.on_own_stream, self.apply, solution, **it) for it in items]
+        return [f.result() for f in futs]
+
 
 def subtract(science, reference, **kwargs) -> DiffResult:
     """Configure a Subtractor from the config keywords and run it once."""
@@ -481,3 +501,13 @@ def apply(solution: KernelSolution, science, reference, **kwargs) -> DiffResult:
     config = {k: v for k, v in kwargs.items() if k in _CONFIG_KEYS}
     call = {k: v for k, v in kwargs.items() if k not in _CONFIG_KEYS}
     return Subtractor(**config).apply(solution, science, reference, **call)
+
+
+def apply_batch(solution: KernelSolution, frames, *, max_in_flight: int | None = None, **kwargs) -> list[DiffResult]:
+    """Configure a Subtractor from the config keywords and apply one frozen
+    solution to several frame pairs concurrently (extension). Non-config
+    keywords apply to every frame unless the frame's own dict sets them."""
+    config = {k: v for k, v in kwargs.items() if k in _CONFIG_KEYS}
+    call = {k: v for k, v in kwargs.items() if k not in _CONFIG_KEYS}
+    items = [{**call, **dict(f)} for f in frames]
+    return Subtractor(**config).apply_batch(solution, items, max_in_flight=max_in_flight)

@@ -30,7 +30,8 @@ def _setup(h, w, seed=0, n_max=3, beta=1.3, nk=3):
 
 
 @pytest.mark.parametrize("h,w,block,cells", [(300, 420, 64, 0), (300, 420, 64, 1), (257, 190, 128, 0),
-                                             (40, 50, 64, 0), (200, 200, 32, 2)])
+                                             (40, 50, 64, 0), (200, 200, 32, 2), (600, 700, 256, 0),
+                                             (530, 520, 256, 1)])
 def test_decorrelate_matches_fp64_oracle(h, w, block, cells):
     knots, theta, beta, n_max, diff, vs, vr = _setup(h, w)
     got = _core.decorrelate(diff, knots, theta, beta, n_max, vs, vr, block=block, kernel_cell_blocks=cells)

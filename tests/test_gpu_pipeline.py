@@ -240,3 +240,23 @@ def test_subtract_batch_matches_one_at_a_time():
         for name in ("difference", "variance", "mask", "score"):
             np.testing.assert_array_equal(getattr(r, name), getattr(one, name), err_msg=name)
         np.testing.assert_array_equal(r.source_catalog, one.source_catalog)
+
+
+def test_apply_batch_matches_one_at_a_time():
+    """One frozen solution applied to several frame pairs in flight gives the
+    same bits as apply() on each pair alone."""
+    ps = [validation.synthetic_pair(512, 512, 300, s, mask_fraction=0.005) for s in (31, 32, 33)]
+    kw = dict(n_max=4, n_knots=3, stamp_radius=12, cv_folds=0, score=True, decorrelate=True, block=64,
+              precision="mixed", saturation=ps[0].saturation)
+    items = [dict(science=p.science, reference=p.reference, science_var=p.science_var,
+                  reference_var=p.reference_var, science_mask=p.science_mask, reference_mask=p.reference_mask)
+             for p in ps]
+    solution = delta.subtract(**items[0], **kw).solution
+    batch = delta.apply_batch(solution, items, max_in_flight=3, **kw)
+    assert len(batch) == len(ps)
+    for it, r in zip(items, batch, strict=True):
+        one = delta.apply(solution, **it, **kw)
+        np.testing.assert_array_equal(r.solution.theta, solution.theta)
+        for name in ("difference", "variance", "mask", "score"):
+            np.testing.assert_array_equal(getattr(r, name), getattr(one, name), err_msg=name)
+        np.testing.assert_array_equal(r.source_catalog, one.source_catalog)
