@@ -170,16 +170,26 @@ def negate(t) -> None:
 
 
 def download(out: dict) -> dict:
-    """Copy the image products of run()/apply() into pinned host memory (one
-    stream sync for all of them); returns {name: ndarray | None}."""
+    """Copy the image products of run()/apply() into pinned host memory;
+    returns {name: ndarray | None}. The copies are SM stores into the mapped
+    pinned buffers (dgpu_copy_to_host), not copy-engine transfers: frames
+    computing on other streams read small results back through the one
+    device-to-host copy engine, and a 200 MB download queued there would hold
+    each of those reads for its whole duration."""
+    ctx = _ctx_on_torch_stream()
     pinned = {}
     for key in ("difference", "variance", "mask", "score"):
         t = out.get(key)
         if t is None:
             pinned[key] = None
             continue
+        t = t.contiguous()
         hbuf = torch.empty(tuple(t.shape), dtype=t.dtype, pin_memory=True)
-        hbuf.copy_(t, non_blocking=True)
+        try:
+            check(_lib.lib().dgpu_copy_to_host(ctx.handle, ctypes.c_void_p(hbuf.data_ptr()), _p(t),
+                                               ctypes.c_int64(t.numel() * t.element_size())), ctx.handle)
+        except ValueError:  # pinned memory without a mapped address: copy-engine transfer
+            hbuf.copy_(t, non_blocking=True)
         pinned[key] = hbuf
     torch.cuda.current_stream().synchronize()
     return {k: (None if v is None else v.numpy()) for k, v in pinned.items()}

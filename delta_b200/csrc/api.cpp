@@ -342,10 +342,10 @@ int dgpu_basis_convolve(dgpu_context* ctx, int mem, const float* image, int64_t 
     float* o = static_cast<float*>(out_buf(c, mem, out, sizeof(float) * n * b.nc, kSlotOutDiff));
     const auto taps = b.taps();
     float* dt = static_cast<float*>(c.slot(kSlotTaps, sizeof(float) * taps.size()));
-    DGPU_CUDA(cudaMemcpyAsync(dt, taps.data(), sizeof(float) * taps.size(), cudaMemcpyHostToDevice, c.stream));
+    DGPU_CUDA(h2d_async(dt, taps.data(), sizeof(float) * taps.size(), c.stream));
     const auto ord = orders_of(b);
     int2* dord = static_cast<int2*>(c.slot(kSlotScratch2, sizeof(int2) * ord.size()));
-    DGPU_CUDA(cudaMemcpyAsync(dord, ord.data(), sizeof(int2) * ord.size(), cudaMemcpyHostToDevice, c.stream));
+    DGPU_CUDA(h2d_async(dord, ord.data(), sizeof(int2) * ord.size(), c.stream));
     SubtractArgs a{};
     a.w = w;
     a.h = h;
@@ -404,10 +404,10 @@ int dgpu_subtract(dgpu_context* ctx, int mem, int64_t width, int64_t height, con
     {
       const auto taps = b.taps();
       float* dt = static_cast<float*>(c.slot(kSlotTaps, sizeof(float) * taps.size()));
-      DGPU_CUDA(cudaMemcpyAsync(dt, taps.data(), sizeof(float) * taps.size(), cudaMemcpyHostToDevice, s));
+      DGPU_CUDA(h2d_async(dt, taps.data(), sizeof(float) * taps.size(), s));
       const auto ord = orders_of(b);
       int2* dord = static_cast<int2*>(c.slot(kSlotScratch2, sizeof(int2) * ord.size()));
-      DGPU_CUDA(cudaMemcpyAsync(dord, ord.data(), sizeof(int2) * ord.size(), cudaMemcpyHostToDevice, s));
+      DGPU_CUDA(h2d_async(dord, ord.data(), sizeof(int2) * ord.size(), s));
       StageTimer t(c, "subtract: model convolve");
       SubtractArgs a{};
       a.w = w;
@@ -434,7 +434,7 @@ int dgpu_subtract(dgpu_context* ctx, int mem, int64_t width, int64_t height, con
           std::copy(k2.begin(), k2.end(), ph.begin() + static_cast<size_t>(q) * b.ks * b.ks);
         }
         phi = static_cast<float*>(c.slot(kSlotPhi, sizeof(float) * ph.size()));
-        DGPU_CUDA(cudaMemcpyAsync(phi, ph.data(), sizeof(float) * ph.size(), cudaMemcpyHostToDevice, s));
+        DGPU_CUDA(h2d_async(phi, ph.data(), sizeof(float) * ph.size(), s));
       }
       launch_variance(s, w, h, F, phi, b.radius, b.nc, vs, vr, var);
     }
@@ -467,7 +467,7 @@ int dgpu_photometric_scale(dgpu_context* ctx, int mem, const double* knots, int 
     std::vector<float> sums(nc);
     for (int q = 0; q < nc; ++q) sums[q] = static_cast<float>(component_sums[q]);
     float* ds = static_cast<float*>(c.slot(kSlotScratch2, sizeof(float) * std::max(nc, 1)));
-    DGPU_CUDA(cudaMemcpyAsync(ds, sums.data(), sizeof(float) * nc, cudaMemcpyHostToDevice, c.stream));
+    DGPU_CUDA(h2d_async(ds, sums.data(), sizeof(float) * nc, c.stream));
     float* o = static_cast<float*>(out_buf(c, mem, out, 4 * n, kSlotOutDiff));
     launch_photometric_scale(c.stream, F, ds, nc, o);
     stage_out(c, mem, out, o, 4 * n);
@@ -495,10 +495,34 @@ int dgpu_negate(dgpu_context* ctx, int mem, float* data, int64_t n) {
     const size_t bytes = 4 * static_cast<size_t>(n);
     float* d = mem == DGPU_MEM_DEVICE ? data : static_cast<float*>(c.slot(kSlotOutDiff, bytes));
     if (mem != DGPU_MEM_DEVICE)
-      DGPU_CUDA(cudaMemcpyAsync(d, data, bytes, cudaMemcpyHostToDevice, c.stream));
+      DGPU_CUDA(h2d_async(d, data, bytes, c.stream));
     launch_negate(c.stream, n, d);
     stage_out(c, mem, data, d, bytes);
     if (mem == DGPU_MEM_HOST) DGPU_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int dgpu_copy_to_host(dgpu_context* ctx, void* host_dst, const void* device_src, int64_t bytes) {
+  return guarded(ctx, [&](Context& c) {
+    if (bytes < 0) fail(DGPU_ERR_INVALID, "copy_to_host: bytes must be >= 0");
+    if (bytes == 0) return;
+    if (!host_dst || !device_src) fail(DGPU_ERR_INVALID, "copy_to_host: missing buffer");
+    cudaPointerAttributes pa{};
+    DGPU_CUDA(cudaPointerGetAttributes(&pa, host_dst));
+    void* dptr = nullptr;
+    if (pa.type != cudaMemoryTypeHost || cudaHostGetDevicePointer(&dptr, host_dst, 0) != cudaSuccess || !dptr) {
+      cudaGetLastError();
+      fail(DGPU_ERR_INVALID, "copy_to_host: destination is not mapped pinned host memory");
+    }
+    cudaPointerAttributes ps{};
+    DGPU_CUDA(cudaPointerGetAttributes(&ps, device_src));
+    if (ps.type != cudaMemoryTypeDevice) fail(DGPU_ERR_INVALID, "copy_to_host: source is not device memory");
+    const auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
+    const int64_t body = (al(dptr) && al(device_src)) ? bytes / 16 * 16 : 0;
+    launch_copy_to_mapped(c.stream, body, device_src, dptr);
+    if (body < bytes)
+      DGPU_CUDA(cudaMemcpyAsync(static_cast<char*>(host_dst) + body, static_cast<const char*>(device_src) + body,
+                                static_cast<size_t>(bytes - body), cudaMemcpyDeviceToHost, c.stream));
   });
 }
 
@@ -541,7 +565,7 @@ int dgpu_matched_filter(dgpu_context* ctx, int mem, int64_t width, int64_t heigh
     const auto* var = static_cast<const float*>(stage_in(c, mem, variance, 4 * n, kSlotInVarS));
     float* o = static_cast<float*>(out_buf(c, mem, out, 4 * n, kSlotOutScore));
     float* dpsf = static_cast<float*>(c.slot(kSlotPsf, sizeof(float) * psf_size * psf_size));
-    DGPU_CUDA(cudaMemcpyAsync(dpsf, psf, sizeof(float) * psf_size * psf_size, cudaMemcpyHostToDevice, c.stream));
+    DGPU_CUDA(h2d_async(dpsf, psf, sizeof(float) * psf_size * psf_size, c.stream));
     {
       StageTimer t(c, "score: blocked correlation");
       const size_t ntiles = static_cast<size_t>((w + 63) / 64) * ((h + 31) / 32);
@@ -574,14 +598,13 @@ int dgpu_build_catalog(dgpu_context* ctx, int mem, int64_t width, int64_t height
     float* dpsf = nullptr;
     if (psf && psf_size > 0) {
       dpsf = static_cast<float*>(c.slot(kSlotPsf, sizeof(float) * psf_size * psf_size));
-      DGPU_CUDA(cudaMemcpyAsync(dpsf, psf, sizeof(float) * psf_size * psf_size, cudaMemcpyHostToDevice, c.stream));
+      DGPU_CUDA(h2d_async(dpsf, psf, sizeof(float) * psf_size * psf_size, c.stream));
     }
     double* dbx = nullptr;
     if (bright_x && n_bright > 0) {
       dbx = static_cast<double*>(c.slot(kSlotBright, sizeof(double) * 2 * n_bright));
-      DGPU_CUDA(cudaMemcpyAsync(dbx, bright_x, sizeof(double) * n_bright, cudaMemcpyHostToDevice, c.stream));
-      DGPU_CUDA(cudaMemcpyAsync(dbx + n_bright, bright_y, sizeof(double) * n_bright, cudaMemcpyHostToDevice,
-                                c.stream));
+      DGPU_CUDA(h2d_async(dbx, bright_x, sizeof(double) * n_bright, c.stream));
+      DGPU_CUDA(h2d_async(dbx + n_bright, bright_y, sizeof(double) * n_bright, c.stream));
     }
     const int cnt = run_catalog(c, w, h, sc, df, mk, *params, vr, dpsf, psf_size, dbx,
                                 dbx ? dbx + n_bright : nullptr, n_bright);

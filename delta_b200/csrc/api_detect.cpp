@@ -176,8 +176,8 @@ int dgpu_estimate_psf(dgpu_context* ctx, int mem, int64_t width, int64_t height,
     const auto* img = static_cast<const float*>(stage_in(c, mem, image, 4 * npx, kSlotInSci));
     int* dxy = static_cast<int*>(c.slot(kSlotBright, sizeof(int) * 2 * std::max(n, 1)));
     if (n) {
-      DGPU_CUDA(cudaMemcpyAsync(dxy, xs, sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
-      DGPU_CUDA(cudaMemcpyAsync(dxy + n, ys, sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
+      DGPU_CUDA(h2d_async(dxy, xs, sizeof(int) * n, c.stream));
+      DGPU_CUDA(h2d_async(dxy + n, ys, sizeof(int) * n, c.stream));
     }
     const int side = 2 * radius + 1, np = side * side;
     double* dout = static_cast<double*>(c.slot(kSlotPsf, sizeof(double) * np));

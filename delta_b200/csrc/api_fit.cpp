@@ -28,7 +28,7 @@ constexpr double kNaN = std::numeric_limits<double>::quiet_NaN();
 template <class T>
 T* up(Context& c, Slot s, const T* host, size_t n) {
   T* d = static_cast<T*>(c.slot(s, sizeof(T) * std::max<size_t>(n, 1)));
-  if (n) DGPU_CUDA(cudaMemcpyAsync(d, host, sizeof(T) * n, cudaMemcpyHostToDevice, c.stream));
+  if (n) DGPU_CUDA(h2d_async(d, host, sizeof(T) * n, c.stream));
   return d;
 }
 
@@ -229,7 +229,7 @@ struct Engine {
     long long* n = reinterpret_cast<long long*>(ywy + 1);
     assemble(mask, M, rhs, ywy, n);
     Work w = work(nl);
-    DGPU_CUDA(cudaMemcpyAsync(w.lam, grid.data(), sizeof(double) * nl, cudaMemcpyHostToDevice, c.stream));
+    DGPU_CUDA(h2d_async(w.lam, grid.data(), sizeof(double) * nl, c.stream));
     solve(w, nl, M, nullptr, rhs, nullptr);
     launch_quad_err(c, nl, P, w.theta, M, nullptr, rhs, nullptr, ywy, w.raw);
     launch_gcv_finish(c.stream, nl, w.raw, w.edf, w.ok, n, w.rss, w.gcv);
@@ -300,7 +300,7 @@ struct Engine {
     long long* n = reinterpret_cast<long long*>(ywy + 1);
     assemble(mask, M, rhs, ywy, n);
     Work w = work(1);
-    DGPU_CUDA(cudaMemcpyAsync(w.lam, &lam, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    DGPU_CUDA(h2d_async(w.lam, &lam, sizeof(double), c.stream));
     solve(w, 1, M, nullptr, rhs, nullptr);
     launch_quad_err(c, 1, P, w.theta, M, nullptr, rhs, nullptr, ywy, w.raw);
     launch_gcv_finish(c.stream, 1, w.raw, w.edf, w.ok, n, w.rss, w.gcv);
@@ -351,7 +351,7 @@ struct Engine {
       }
       double* d_dsd = up(c, kSlotFit13, dsd.data(), dsd.size());
       int* d_fold = static_cast<int*>(c.slot(kSlotBlockCounts, sizeof(int) * std::max(n_units, 1)));
-      DGPU_CUDA(cudaMemcpyAsync(d_fold, f2.data(), sizeof(int) * n_units, cudaMemcpyHostToDevice, c.stream));
+      DGPU_CUDA(h2d_async(d_fold, f2.data(), sizeof(int) * n_units, c.stream));
       launch_stamped_assemble(c.stream, G, n_units, nf, k, d_fold, As, rs, ds2, d_dsd, Mg, rg, yg);
       DGPU_CUDA(cudaStreamSynchronize(c.stream));
     } else {
@@ -360,7 +360,7 @@ struct Engine {
       for (int g = 0; g < G; ++g) {
         std::vector<uint8_t> m(n_units);
         for (int u = 0; u < n_units; ++u) m[u] = (hm[u] && fold[u] == g) ? 1 : 0;
-        DGPU_CUDA(cudaMemcpyAsync(fm, m.data(), n_units, cudaMemcpyHostToDevice, c.stream));
+        DGPU_CUDA(h2d_async(fm, m.data(), n_units, c.stream));
         long long* dummy = nall + 1;
         launch_rhs(c, N, nc, k, SS, R, fm, nullptr, rg + static_cast<size_t>(g) * P, yg + g, dummy);
         launch_normal_equations(c, prec, N, nc, k, SS, R, fm,
@@ -375,7 +375,7 @@ struct Engine {
       std::vector<double> y = down(c, yg, G);
       double ys = 0.0;
       for (double v : y) ys += v;
-      DGPU_CUDA(cudaMemcpyAsync(yall, &ys, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+      DGPU_CUDA(h2d_async(yall, &ys, sizeof(double), c.stream));
       DGPU_CUDA(cudaStreamSynchronize(c.stream));
     }
     std::vector<double> curve(nl, kInf);
@@ -396,8 +396,8 @@ struct Engine {
           lam[ii * G + g] = grid[idx[ii]];
           mi[ii * G + g] = g;
         }
-      DGPU_CUDA(cudaMemcpyAsync(w.lam, lam.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, c.stream));
-      DGPU_CUDA(cudaMemcpyAsync(w.midx, mi.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, c.stream));
+      DGPU_CUDA(h2d_async(w.lam, lam.data(), sizeof(double) * ns, c.stream));
+      DGPU_CUDA(h2d_async(w.midx, mi.data(), sizeof(int) * ns, c.stream));
       solve(w, ns, Mt, w.midx, rt, w.midx, G);
       return ns;
     };
@@ -476,7 +476,7 @@ struct Engine {
         std::vector<uint8_t> m(static_cast<size_t>(G) * n_units, 0);
         for (int g = 0; g < G; ++g)
           for (int u = 0; u < n_units; ++u) m[static_cast<size_t>(g) * n_units + u] = (hm[u] && fold[u] == g) ? 1 : 0;
-        DGPU_CUDA(cudaMemcpyAsync(fmasks, m.data(), m.size(), cudaMemcpyHostToDevice, c.stream));
+        DGPU_CUDA(h2d_async(fmasks, m.data(), m.size(), c.stream));
       }
       std::vector<int> searched;
       for (int li = 0; li < nl; ++li)
@@ -502,7 +502,7 @@ struct Engine {
     }
     // Final all-data fit at the selected lambda.
     Work w1 = work(1);
-    DGPU_CUDA(cudaMemcpyAsync(w1.lam, &grid[best], sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    DGPU_CUDA(h2d_async(w1.lam, &grid[best], sizeof(double), c.stream));
     solve(w1, 1, Mall, nullptr, rall, nullptr);
     launch_quad_err(c, 1, P, w1.theta, Mall, nullptr, rall, nullptr, yall, w1.raw);
     launch_gcv_finish(c.stream, 1, w1.raw, w1.edf, w1.ok, nall, w1.rss, w1.gcv);
@@ -554,11 +554,11 @@ void direct_rows(Engine& E, const double* points, const double* target, const do
   for (int64_t i = 0; i < m; ++i) E.tp.design_row(points[2 * i], points[2 * i + 1], d.data() + i * E.k);
   E.alloc_rows();
   Context& c = E.c;
-  DGPU_CUDA(cudaMemcpyAsync(E.R.valid, valid.data(), m, cudaMemcpyHostToDevice, c.stream));
-  DGPU_CUDA(cudaMemcpyAsync(E.R.t, target, 8 * m, cudaMemcpyHostToDevice, c.stream));
-  DGPU_CUDA(cudaMemcpyAsync(E.R.w, weights, 8 * m, cudaMemcpyHostToDevice, c.stream));
-  if (E.nc) DGPU_CUDA(cudaMemcpyAsync(E.R.bn, bn, 8 * m * E.nc, cudaMemcpyHostToDevice, c.stream));
-  DGPU_CUDA(cudaMemcpyAsync(E.R.d, d.data(), 8 * d.size(), cudaMemcpyHostToDevice, c.stream));
+  DGPU_CUDA(h2d_async(E.R.valid, valid.data(), m, c.stream));
+  DGPU_CUDA(h2d_async(E.R.t, target, 8 * m, c.stream));
+  DGPU_CUDA(h2d_async(E.R.w, weights, 8 * m, c.stream));
+  if (E.nc) DGPU_CUDA(h2d_async(E.R.bn, bn, 8 * m * E.nc, c.stream));
+  DGPU_CUDA(h2d_async(E.R.d, d.data(), 8 * d.size(), c.stream));
   DGPU_CUDA(cudaStreamSynchronize(c.stream));
 }
 
@@ -677,7 +677,7 @@ int dgpu_fit_kernel(dgpu_context* ctx, int mem, int64_t width, int64_t height, c
       launch_strided_median(c, kSampleReference, static_cast<int64_t>(npx), ref, rm, fill);
       int* dsx = up(c, kSlotBright, reinterpret_cast<const int*>(stamp_x), static_cast<size_t>(n_stamps));
       int* dsy = static_cast<int*>(c.slot(kSlotCompOut, sizeof(int) * std::max(n_stamps, 1)));
-      DGPU_CUDA(cudaMemcpyAsync(dsy, stamp_y, sizeof(int) * n_stamps, cudaMemcpyHostToDevice, st));
+      DGPU_CUDA(h2d_async(dsy, stamp_y, sizeof(int) * n_stamps, st));
       const auto taps = b.taps();
       float* dt = up(c, kSlotTaps, taps.data(), taps.size());
       std::vector<int2> ord(nc);
@@ -735,7 +735,7 @@ int dgpu_fit_kernel(dgpu_context* ctx, int mem, int64_t width, int64_t height, c
     if (const char* e = std::getenv("DELTA_STAMP_APPROX")) use_stamped = std::atoi(e) != 0;
 
     for (int iter = 0;; ++iter) {
-      DGPU_CUDA(cudaMemcpyAsync(d_acc, accepted.data(), n_stamps, cudaMemcpyHostToDevice, st));
+      DGPU_CUDA(h2d_async(d_acc, accepted.data(), n_stamps, st));
       // The active-row count comes back with the solve (the rows are the same).
       if (cv_folds > 1) {
         std::vector<int> fold(n_stamps, -1);
@@ -759,8 +759,8 @@ int dgpu_fit_kernel(dgpu_context* ctx, int mem, int64_t width, int64_t height, c
       const double denom = static_cast<double>(npix) - gls.edf;
       reduced = denom > 0.0 ? gls.rss / denom : kNaN;
       if (have_var) {
-        DGPU_CUDA(cudaMemcpyAsync(dsx, stamp_x, sizeof(int) * n_stamps, cudaMemcpyHostToDevice, st));
-        DGPU_CUDA(cudaMemcpyAsync(dsy, stamp_y, sizeof(int) * n_stamps, cudaMemcpyHostToDevice, st));
+        DGPU_CUDA(h2d_async(dsx, stamp_x, sizeof(int) * n_stamps, st));
+        DGPU_CUDA(h2d_async(dsy, stamp_y, sizeof(int) * n_stamps, st));
         launch_reweight(st, g, n_stamps, tdev, dsx, dsy, E.R, d_acc, cnt_d, gls.d_theta, phi, vr, rm);
       }
       std::vector<int> to_reject;

@@ -17,7 +17,7 @@ namespace {
 template <class T>
 T* up(Context& c, Slot s, const T* host, size_t n) {
   T* d = static_cast<T*>(c.slot(s, sizeof(T) * std::max<size_t>(n, 1)));
-  if (n) DGPU_CUDA(cudaMemcpyAsync(d, host, sizeof(T) * n, cudaMemcpyHostToDevice, c.stream));
+  if (n) DGPU_CUDA(h2d_async(d, host, sizeof(T) * n, c.stream));
   return d;
 }
 
@@ -83,7 +83,7 @@ void kernel_power_host(Context& c, const FftGeom& g, const float* kernel, int ks
   float2* spec = static_cast<float2*>(c.slot(kSlotFft4, sizeof(float2) * static_cast<size_t>(n) * nb));
   launch_rows_fwd(c.stream, g, 1, 1, dd, 0, 0, nullptr, nullptr, 1, spec);
   launch_cols(c.stream, g, 1, 1, spec, nullptr, nullptr, nullptr, nullptr, d_power);
-  DGPU_CUDA(cudaMemcpyAsync(d_sumk2, &s2, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+  DGPU_CUDA(h2d_async(d_sumk2, &s2, sizeof(double), c.stream));
   DGPU_CUDA(cudaStreamSynchronize(c.stream));
 }
 
@@ -269,8 +269,7 @@ int dgpu_whiten_score_psf(dgpu_context* ctx, int mem, const float* psf, int psf_
           const int gy = ((py - r) % n + n) % n, gx = ((px - r) % n + n) % n;
           pe[static_cast<size_t>(gy) * n + gx] = psf[py * psf_size + px];
         }
-      DGPU_CUDA(cudaMemcpyAsync(dense + static_cast<size_t>(n) * n, pe.data(), sizeof(float) * pe.size(),
-                                cudaMemcpyHostToDevice, s));
+      DGPU_CUDA(h2d_async(dense + static_cast<size_t>(n) * n, pe.data(), sizeof(float) * pe.size(), s));
       DGPU_CUDA(cudaStreamSynchronize(s));
     }
     launch_block_var(s, g, 0, 1, vs, vr, w, h, nullptr, nullptr, 1, vsr - 0);
@@ -316,7 +315,7 @@ int dgpu_decorrelate_block(dgpu_context* ctx, const float* image, int n, const f
     double* small = static_cast<double*>(c.slot(kSlotFft1, sizeof(double) * 8));
     kernel_power_host(c, g, kernel, ksize, power, small);
     const double vsr[2] = {var_science, var_reference};
-    DGPU_CUDA(cudaMemcpyAsync(small + 2, vsr, sizeof(vsr), cudaMemcpyHostToDevice, c.stream));
+    DGPU_CUDA(h2d_async(small + 2, vsr, sizeof(vsr), c.stream));
     int zero = 0;
     int* dz = up(c, kSlotCellY, &zero, 1);
     float* img = up(c, kSlotFft3, image, static_cast<size_t>(n) * n);
@@ -341,7 +340,7 @@ int dgpu_decorrelation_kernel(dgpu_context* ctx, const float* kernel, int ksize,
     double* small = static_cast<double*>(c.slot(kSlotFft1, sizeof(double) * 8));
     kernel_power_host(c, g, kernel, ksize, power, small);
     const double vsr[2] = {var_science, var_reference};
-    DGPU_CUDA(cudaMemcpyAsync(small + 2, vsr, sizeof(vsr), cudaMemcpyHostToDevice, c.stream));
+    DGPU_CUDA(h2d_async(small + 2, vsr, sizeof(vsr), c.stream));
     int zero = 0;
     int* dz = up(c, kSlotCellY, &zero, 1);
     float2* spec = static_cast<float2*>(c.slot(kSlotFft0, sizeof(float2) * static_cast<size_t>(n) * nb));

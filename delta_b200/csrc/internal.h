@@ -26,6 +26,11 @@ struct Failure : std::runtime_error {
 
 [[noreturn]] void fail(int code, const std::string& msg);
 void check_cuda(cudaError_t e, const char* what);
+// Host -> device copy on `s`. A pageable source of up to 1 MiB goes in pieces
+// of at most 32 KiB: such pieces are not queued behind large transfers of
+// other streams in the host-to-device copy engine (a 256 KB piece waits for a
+// whole 70 MB layer upload of another frame; a 32 KB one does not).
+cudaError_t h2d_async(void* dst, const void* src, size_t bytes, cudaStream_t s);
 // Every kernel launch of the library goes through DGPU_LAUNCH, which also
 // counts it (dgpu_launch_count).
 void count_launch();
@@ -221,6 +226,9 @@ void launch_mask_fill(cudaStream_t s, int64_t n, const uint8_t* mask, const uint
 void launch_model_convolve_orders(cudaStream_t s, const SubtractArgs& a, const int2* orders, bool stack);
 void launch_photometric_scale(cudaStream_t s, const DevFields& F, const float* sums, int nc, float* out);
 void launch_negate(cudaStream_t s, int64_t n, float* v);
+// bytes (a multiple of 16) from device memory to mapped pinned host memory
+// (its device-side address), both 16-byte aligned, by SM stores.
+void launch_copy_to_mapped(cudaStream_t s, int64_t bytes, const void* src, void* dst);
 // Background median / MAD of a device image with a fixed file-scope scratch
 // (no allocation); out2 (host) = {median, MAD}. Synchronises `s`.
 void background_noalloc(int64_t n, const float* img, const uint8_t* mask, cudaStream_t s, float* out2);

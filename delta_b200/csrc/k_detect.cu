@@ -653,8 +653,8 @@ void run_catalog_stamps(Context& c, int w, int h, const float* sci, const uint8_
   launch_background(c, npx, sci, sm, bgs, kSlotFit10, kSlotFit11);
   launch_background(c, npx, ref, rm, bgr, kSlotFit12, kSlotFit13);
   int* dxy = static_cast<int*>(c.slot(kSlotBright, sizeof(int) * 2 * std::max(n, 1)));
-  DGPU_CUDA(cudaMemcpyAsync(dxy, xs_host, sizeof(int) * n, cudaMemcpyHostToDevice, s));
-  DGPU_CUDA(cudaMemcpyAsync(dxy + n, ys_host, sizeof(int) * n, cudaMemcpyHostToDevice, s));
+  DGPU_CUDA(h2d_async(dxy, xs_host, sizeof(int) * n, s));
+  DGPU_CUDA(h2d_async(dxy + n, ys_host, sizeof(int) * n, s));
   char* ob = static_cast<char*>(c.slot(kSlotCompStats, (sizeof(int) + 2 * sizeof(double)) * std::max(n, 1) + 64));
   double* dfs = reinterpret_cast<double*>(ob);
   double* dfr = dfs + std::max(n, 1);

@@ -365,8 +365,8 @@ void launch_normal_equations(Context& c, int prec, int64_t N, int nc, int k, int
   for (int a = 0; a < k; ++a)
     for (int b = a; b < k; ++b) vp.push_back(make_int2(a, b));
   int2* dpairs = static_cast<int2*>(c.slot(kSlotFit10, sizeof(int2) * (Mu + Nv)));
-  DGPU_CUDA(cudaMemcpyAsync(dpairs, up.data(), sizeof(int2) * Mu, cudaMemcpyHostToDevice, st));
-  DGPU_CUDA(cudaMemcpyAsync(dpairs + Mu, vp.data(), sizeof(int2) * Nv, cudaMemcpyHostToDevice, st));
+  DGPU_CUDA(h2d_async(dpairs, up.data(), sizeof(int2) * Mu, st));
+  DGPU_CUDA(h2d_async(dpairs + Mu, vp.data(), sizeof(int2) * Nv, st));
   double* g = static_cast<double*>(c.slot(kSlotFit12, sizeof(double) * static_cast<size_t>(Mu) * Nv));
   if (prec == DGPU_PREC_MIXED) {
     launch_normal_tc(c, N, nc, k, SS, R, accepted, dpairs, Mu, dpairs + Mu, Nv, kSlotFit11, g);

@@ -807,4 +807,27 @@ void launch_negate(cudaStream_t s, int64_t n, float* v) {
   DGPU_LAUNCH("k_negate");
 }
 
+// Device memory -> mapped pinned host memory by SM stores (16 bytes each, four
+// in flight per thread); both pointers 16-byte aligned, bytes a multiple of 16.
+__global__ void __launch_bounds__(256) k_copy_to_mapped(int64_t n16, const uint4* __restrict__ src, uint4* dst) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (; i + 3 * stride < n16; i += 4 * stride) {
+    const uint4 a = src[i], b = src[i + stride], c = src[i + 2 * stride], d = src[i + 3 * stride];
+    dst[i] = a;
+    dst[i + stride] = b;
+    dst[i + 2 * stride] = c;
+    dst[i + 3 * stride] = d;
+  }
+  for (; i < n16; i += stride) dst[i] = src[i];
+}
+
+void launch_copy_to_mapped(cudaStream_t s, int64_t bytes, const void* src, void* dst) {
+  if (bytes <= 0) return;
+  // 64 CTAs keep enough stores in flight to fill the host link while leaving
+  // the other SMs to the frames still computing.
+  k_copy_to_mapped<<<64, 256, 0, s>>>(bytes / 16, static_cast<const uint4*>(src), static_cast<uint4*>(dst));
+  DGPU_LAUNCH("k_copy_to_mapped");
+}
+
 }  // namespace dgpu

@@ -22,6 +22,24 @@ void check_cuda(cudaError_t e, const char* what) {
   if (e != cudaSuccess) fail(DGPU_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+cudaError_t h2d_async(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  constexpr size_t kPiece = size_t(32) << 10, kSplitMax = size_t(1) << 20;
+  if (bytes <= kPiece || bytes > kSplitMax)
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  cudaPointerAttributes pa{};
+  if (cudaPointerGetAttributes(&pa, src) != cudaSuccess) {
+    cudaGetLastError();
+    pa.type = cudaMemoryTypeUnregistered;
+  }
+  if (pa.type != cudaMemoryTypeUnregistered) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  for (size_t off = 0; off < bytes; off += kPiece) {
+    const cudaError_t e = cudaMemcpyAsync(static_cast<char*>(dst) + off, static_cast<const char*>(src) + off,
+                                          std::min(kPiece, bytes - off), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 void* Context::slot(Slot s, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (slot_size[s] >= bytes) return slot_ptr[s];
@@ -119,7 +137,7 @@ const void* stage_in(Context& c, int mem, const void* p, size_t bytes, Slot s) {
   if (p == nullptr) return nullptr;
   if (mem == DGPU_MEM_DEVICE) return p;
   void* d = c.slot(s, bytes);
-  DGPU_CUDA(cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, c.stream));
+  DGPU_CUDA(h2d_async(d, p, bytes, c.stream));
   return d;
 }
 
@@ -142,7 +160,7 @@ TpsDev upload_tps(Context& c, const ThinPlate& tp) {
   std::copy(tp.kn.begin(), tp.kn.end(), buf.begin());
   std::copy(tp.z.begin(), tp.z.end(), buf.begin() + 2 * k);
   double* d = static_cast<double*>(c.slot(kSlotZ, sizeof(double) * buf.size()));
-  DGPU_CUDA(cudaMemcpyAsync(d, buf.data(), sizeof(double) * buf.size(), cudaMemcpyHostToDevice, c.stream));
+  DGPU_CUDA(h2d_async(d, buf.data(), sizeof(double) * buf.size(), c.stream));
   TpsDev t;
   t.kn = d;
   t.z = d + 2 * k;
@@ -182,8 +200,8 @@ DevFields build_fields_dev(Context& c, const ThinPlate& tp, const double* d_thet
   fb.insert(fb.end(), g.wy.begin(), g.wy.end());
   int* di = static_cast<int*>(c.slot(kSlotCellX, sizeof(int) * ib.size()));
   float* df = static_cast<float*>(c.slot(kSlotCellY, sizeof(float) * fb.size()));
-  DGPU_CUDA(cudaMemcpyAsync(di, ib.data(), sizeof(int) * ib.size(), cudaMemcpyHostToDevice, c.stream));
-  DGPU_CUDA(cudaMemcpyAsync(df, fb.data(), sizeof(float) * fb.size(), cudaMemcpyHostToDevice, c.stream));
+  DGPU_CUDA(h2d_async(di, ib.data(), sizeof(int) * ib.size(), c.stream));
+  DGPU_CUDA(h2d_async(df, fb.data(), sizeof(float) * fb.size(), c.stream));
   const size_t nl = static_cast<size_t>(nf) * g.ncx * g.ncy;
   double* lat = static_cast<double*>(c.slot(kSlotLattice, sizeof(double) * nl));
   float* latf = static_cast<float*>(c.slot(kSlotLatticeF, sizeof(float) * nl));
@@ -200,7 +218,7 @@ DevFields build_fields_dev(Context& c, const ThinPlate& tp, const double* d_thet
 DevFields build_fields(Context& c, const ThinPlate& tp, const double* theta, int nf, int w, int h) {
   const size_t n = static_cast<size_t>(nf) * tp.k;
   double* d = static_cast<double*>(c.slot(kSlotTheta, sizeof(double) * n));
-  DGPU_CUDA(cudaMemcpyAsync(d, theta, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
+  DGPU_CUDA(h2d_async(d, theta, sizeof(double) * n, c.stream));
   return build_fields_dev(c, tp, d, nf, w, h);
 }
 

@@ -138,6 +138,16 @@ int dgpu_photometric_scale(dgpu_context* ctx, int mem, const double* knots, int 
  * convention applied to the difference when the science frame is the one
  * convolved (python/delta/pipeline.py:687-689, np.negative on the host there). */
 int dgpu_negate(dgpu_context* ctx, int mem, float* data, int64_t n);
+/* Copy of `bytes` from device memory to pinned host memory by SM stores
+ * through the destination's mapped address, ordered on the context's stream;
+ * returns once it has completed. No counterpart in the reference, which has no
+ * device: it serves the batch layer. The device's device-to-host copies share
+ * one queue in submission order, so a frame's 200 MB result download queued
+ * there would hold every read-back of the frames still computing for its whole
+ * duration. Unaligned or partial tails go by an ordinary copy. Errors:
+ * DGPU_ERR_INVALID when host_dst is not mapped pinned host memory or
+ * device_src is not device memory. */
+int dgpu_copy_to_host(dgpu_context* ctx, void* host_dst, const void* device_src, int64_t bytes);
 /* photometric_scale_at, src/bindings.cpp:711-719 -> src/fit.cpp:532-544. out: m. */
 int dgpu_photometric_scale_at(const double* knots, int n_knots, const double* theta,
                               int64_t n_theta, const double* component_sums, int nc,

@@ -260,3 +260,28 @@ def test_apply_batch_matches_one_at_a_time():
         for name in ("difference", "variance", "mask", "score"):
             np.testing.assert_array_equal(getattr(r, name), getattr(one, name), err_msg=name)
         np.testing.assert_array_equal(r.source_catalog, one.source_catalog)
+
+
+def test_copy_to_host_by_sm_stores():
+    """dgpu_copy_to_host writes device bytes into mapped pinned host memory
+    (aligned body by SM stores, a ragged tail by an ordinary copy) and rejects
+    pageable destinations."""
+    import ctypes
+
+    import torch
+
+    from delta_b200 import _device, _lib
+
+    ctx = _device._ctx_on_torch_stream()
+    for n in (0, 16, 1000, 4 * 1024 * 1024 + 3):
+        src = torch.randint(0, 256, (n,), dtype=torch.uint8, device="cuda")
+        dst = torch.zeros(n, dtype=torch.uint8, pin_memory=True)
+        _lib.check(_lib.lib().dgpu_copy_to_host(ctx.handle, ctypes.c_void_p(dst.data_ptr()),
+                                                ctypes.c_void_p(src.data_ptr()), ctypes.c_int64(n)), ctx.handle)
+        torch.cuda.current_stream().synchronize()
+        assert torch.equal(dst, src.cpu())
+    src = torch.ones(64, dtype=torch.float32, device="cuda")
+    pageable = np.zeros(64, np.float32)
+    with pytest.raises(ValueError):
+        _lib.check(_lib.lib().dgpu_copy_to_host(ctx.handle, ctypes.c_void_p(pageable.ctypes.data),
+                                                ctypes.c_void_p(src.data_ptr()), ctypes.c_int64(256)), ctx.handle)
