@@ -107,6 +107,10 @@ constexpr int kMcTW = 32;   // tile width (columns)
 constexpr int kMcYR = 4;    // output rows per thread in the y pass (2 columns each)
 constexpr int kMcXPT = 4;   // output columns per thread in the x pass
 
+// Tap rows in shared memory are padded to a multiple of 8 floats (zeros), so
+// both passes read them as 16-byte vectors (the y pass reads 8 taps at j0 + 0..7).
+__host__ __device__ constexpr int mc_tap_stride(int ks) { return (ks + 7) & ~7; }
+
 struct McSmem {
   int nrows, gbw_pad, lat_nx, lat_ny, cx0, cy0;
 };
@@ -124,14 +128,18 @@ k_model_convolve(int w, int h, const float* __restrict__ sci, const float* __res
   const int nrows = TH + 2 * kh;
   const int gbw = kMcTW + 2 * kh;
   const int gbw_pad = (gbw + 3) & ~3;
+  const int kts = mc_tap_stride(ks);
   float* rtile = smem;                                       // nrows x gbw_pad
   float* txs = rtile + nrows * gbw_pad;                      // NX x nrows x kMcTW
-  float* ktaps = txs + NX * nrows * kMcTW;                   // NX x ks
+  float* ktaps = txs + NX * nrows * kMcTW;                   // NX x kts (zero padded, 16-byte aligned rows)
   const int bx = blockIdx.x * kMcTW, by = blockIdx.y * TH;
   const float fill = STACK ? 0.0f : *fillp;
   const int tid = threadIdx.x;
 
-  for (int i = tid; i < NX * ks; i += blockDim.x) ktaps[i] = taps[i];
+  for (int i = tid; i < NX * kts; i += blockDim.x) {
+    const int q = i / kts, j = i - q * kts;
+    ktaps[i] = j < ks ? taps[q * ks + j] : 0.0f;
+  }
   for (int i = tid; i < nrows * gbw; i += blockDim.x) {
     const int r = i / gbw, c = i - r * gbw;
     const int gy = by - kh + r, gx = bx - kh + c;
@@ -164,17 +172,26 @@ k_model_convolve(int w, int h, const float* __restrict__ sci, const float* __res
       float win[kMcXPT];
 #pragma unroll
       for (int i = 0; i < kMcXPT; ++i) win[i] = row[i];
-      for (int j = 0; j < ks; ++j) {
-        if (j > 0) {
+      // Taps in groups of 4, one 16-byte load per component per group.
+      for (int j0 = 0; j0 < ks; j0 += 4) {
+        float4 kq[NX];
 #pragma unroll
-          for (int i = kMcXPT - 1; i > 0; --i) win[i] = win[i - 1];
-          win[0] = row[-j];
-        }
+        for (int q = 0; q < NX; ++q) kq[q] = *reinterpret_cast<const float4*>(ktaps + q * kts + j0);
 #pragma unroll
-        for (int q = 0; q < NX; ++q) {
-          const float kc = ktaps[q * ks + j];
+        for (int jj = 0; jj < 4; ++jj) {
+          const int j = j0 + jj;
+          if (j >= ks) break;
+          if (j > 0) {
 #pragma unroll
-          for (int i = 0; i < kMcXPT; ++i) acc[q][i] = __fmaf_rn(kc, win[i], acc[q][i]);
+            for (int i = kMcXPT - 1; i > 0; --i) win[i] = win[i - 1];
+            win[0] = row[-j];
+          }
+#pragma unroll
+          for (int q = 0; q < NX; ++q) {
+            const float kc = jj == 0 ? kq[q].x : jj == 1 ? kq[q].y : jj == 2 ? kq[q].z : kq[q].w;
+#pragma unroll
+            for (int i = 0; i < kMcXPT; ++i) acc[q][i] = __fmaf_rn(kc, win[i], acc[q][i]);
+          }
         }
       }
     }
@@ -269,7 +286,7 @@ k_model_convolve(int w, int h, const float* __restrict__ sci, const float* __res
   for (int n = 0; n < nc; ++n) {
     const int2 o = orders[n];
     const float2* col = reinterpret_cast<const float2*>(txs + static_cast<size_t>(o.x) * nrows * kMcTW + lx0);
-    const float* ky = ktaps + o.y * ks;
+    const float* ky = ktaps + o.y * kts;
     // Output row ly0+i needs buffer row ly0 + i + 2kh - j. Taps go in blocks of
     // 8 with the rows of a block held in registers (static indices), each
     // output still summing its taps j = 0..ks-1 in order.
@@ -284,10 +301,13 @@ k_model_convolve(int w, int h, const float* __restrict__ sci, const float* __res
         const int rr = base - j0 - 7 + t;
         v[t] = rr >= 0 ? col[rr * (kMcTW / 2)] : make_float2(0.0f, 0.0f);
       }
+      const float4 ka = *reinterpret_cast<const float4*>(ky + j0);
+      const float4 kb = *reinterpret_cast<const float4*>(ky + j0 + 4);
+      const float kv[8] = {ka.x, ka.y, ka.z, ka.w, kb.x, kb.y, kb.z, kb.w};
 #pragma unroll
       for (int jj = 0; jj < 8; ++jj) {
         if (j0 + jj < ks) {
-          const float c = ky[j0 + jj];
+          const float c = kv[jj];
           const float2 cc = make_float2(c, c);
 #pragma unroll
           for (int i = 0; i < kMcYR; ++i) bn[i] = __ffma2_rn(cc, v[i - jj + 7], bn[i]);
@@ -341,7 +361,7 @@ size_t model_convolve_smem(int nx, int ks, int TH) {
   const int nrows = TH + 2 * kh;
   const int gbw_pad = ((kMcTW + 2 * kh) + 3) & ~3;
   return sizeof(float) * (static_cast<size_t>(nrows) * gbw_pad + static_cast<size_t>(nx) * nrows * kMcTW +
-                          static_cast<size_t>(nx) * ks);
+                          static_cast<size_t>(nx) * mc_tap_stride(ks));
 }
 
 void launch_model_convolve_orders(cudaStream_t s, const SubtractArgs& a, const int2* orders, bool stack) {
