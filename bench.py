@@ -19,6 +19,13 @@ data path).
 `--impl reference` times the CPU chain of the same workload instead (the
 reference's own detect/catalog/convolve code compiled from source plus the
 C / NumPy restatements of its fit, subtract, decorrelation and score).
+
+`--workload uneven` runs the batch of uneven frames instead: 64 frames of
+2048x4096, 2048x2048 and 1024x4096 (science FWHM ~ U(2, 5) px, 500-20000 stars,
+0-3% masked), 16 distinct seeded frames each queued four times in a seeded
+order, through the end-to-end API with `--batch` frames in flight; it reports
+aggregate Mpix/s and the per-frame p50 / p99 latency. Ranks take frames by
+longest-processing-time dealing (descending pixel count).
 """
 
 from __future__ import annotations
@@ -70,6 +77,8 @@ def parse_args(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--batch", type=int, default=4, help="frames in flight per GPU (each its own stream)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU leg (rank 0, N=1)")
+    ap.add_argument("--workload", choices=("frame", "uneven"), default="frame",
+                    help="frame: the 4096^2 workload (default); uneven: 64 frames of mixed sizes")
     return ap.parse_args(argv)
 
 
@@ -84,6 +93,45 @@ def make_frame(size: int, seed: int):
 
     fc = frame_config(size)
     return validation.config2_pair(seed=seed, size=size, n_stars=fc["n_stars"], n_transients=fc["n_transients"])
+
+
+UNEVEN_SHAPES = ((2048, 4096), (2048, 2048), (1024, 4096))  # (height, width)
+UNEVEN_FRAMES, UNEVEN_DISTINCT = 64, 16
+
+
+def uneven_specs(seed: int, n_distinct: int = UNEVEN_DISTINCT) -> list[dict]:
+    """Seeded parameters of the distinct frames of the uneven batch: shapes in
+    turn, science FWHM ~ U(2, 5) px, stars ~ U(500, 20000), masked ~ U(0, 3%)."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_distinct):
+        h, w = UNEVEN_SHAPES[i % len(UNEVEN_SHAPES)]
+        specs.append({"height": h, "width": w, "n_stars": int(rng.uniform(500, 20000)),
+                      "sci_fwhm": float(rng.uniform(2.0, 5.0)), "mask_fraction": float(rng.uniform(0.0, 0.03)),
+                      "seed": seed * 1000 + i})
+    return specs
+
+
+def uneven_queue(seed: int, n_distinct: int = UNEVEN_DISTINCT, n_frames: int = UNEVEN_FRAMES) -> list[int]:
+    """Distinct-frame index of every queued frame: whole seeded permutations of
+    the distinct frames, repeated until n_frames are queued."""
+    rng = np.random.default_rng(seed + 1)
+    q: list[int] = []
+    while len(q) < n_frames:
+        q.extend(int(j) for j in rng.permutation(n_distinct))
+    return q[:n_frames]
+
+
+def lpt_deal(pixels: list[int], world: int) -> list[int]:
+    """Owner rank of every item: items by descending pixel count (ties by
+    index), each to the rank with the least pixels so far (lowest rank on ties)."""
+    loads = [0] * max(1, world)
+    owner = [0] * len(pixels)
+    for i in sorted(range(len(pixels)), key=lambda i: (-pixels[i], i)):
+        r = min(range(len(loads)), key=lambda k: (loads[k], k))
+        owner[i] = r
+        loads[r] += pixels[i]
+    return owner
 
 
 def subtract_kwargs(pair, precision: str | None = None) -> dict:
@@ -594,10 +642,90 @@ def run_gpu(args) -> int:
     return 0
 
 
+def run_uneven(args) -> int:
+    """The uneven batch through delta_b200's Subtractor.subtract (the call
+    subtract_batch makes per frame) on `--batch` worker streams, from pinned
+    host arrays; wall clock with a device synchronize and barrier on both sides."""
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = rank_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device (the product path has no CPU fallback)")
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
+    from delta_b200 import _device, validation
+    from delta_b200.pipeline import Subtractor
+
+    specs = uneven_specs(args.seed)
+    queue = uneven_queue(args.seed)
+    owner = lpt_deal([specs[j]["height"] * specs[j]["width"] for j in queue], world)
+    mine = [q for q in range(len(queue)) if owner[q] == rank]
+    needed = sorted({queue[q] for q in mine})
+    names = ("science", "reference", "science_var", "reference_var", "science_mask", "reference_mask")
+    host = {}
+    first = None
+    for j in needed:
+        sp = specs[j]
+        p = validation.synthetic_pair(sp["width"], sp["height"], sp["n_stars"], sp["seed"], sci_fwhm=sp["sci_fwhm"],
+                                      mask_fraction=sp["mask_fraction"])
+        host[j] = {k: pinned_copy(getattr(p, k)) for k in names}
+        first = first or p
+    # Every frame of the generator has the same gain and saturation level.
+    sub = Subtractor(**subtract_kwargs(first, "mixed")) if first is not None else None
+    lat = {}
+
+    def one(q, record):
+        t0 = time.perf_counter()
+        sub.subtract(**host[queue[q]])
+        if record:
+            lat[q] = (time.perf_counter() - t0) * 1e3
+
+    ex = _device.runner(max(1, args.batch))
+    warm: dict[int, int] = {}
+    for q in mine:
+        warm.setdefault(queue[q], q)
+    for f in [ex.submit(_device.on_own_stream, one, q, False) for q in warm.values()]:
+        f.result()
+    barrier(device)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    for f in [ex.submit(_device.on_own_stream, one, q, True) for q in mine]:
+        f.result()
+    torch.cuda.synchronize(device)
+    wall = (time.perf_counter() - t0) * 1e3
+    barrier(device)
+    wall = max_over_ranks(wall, device)
+    total_px = sum(specs[j]["height"] * specs[j]["width"] for j in queue)
+    ls = sorted(lat.values())
+    pct = (lambda f: ls[min(len(ls) - 1, int(round(f * (len(ls) - 1))))]) if ls else (lambda f: None)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "uneven batch: aggregate Mpix/s over 64 frames of mixed sizes, end to end", "unit": UNIT,
+            "value": total_px / 1e6 / (wall / 1e3), "n_gpus": world, "frames": len(queue), "wall_ms": wall,
+            "latency_ms": {"p50": pct(0.5), "p99": pct(0.99), "max": ls[-1] if ls else None, "rank": 0},
+            "frames_in_flight": max(1, args.batch), "higher_is_better": True, "scaling": "strong",
+            "dtype": "f32", "data": "synthetic (seeded generator)",
+            "config": {"workload": "64 frames: 16 distinct seeded frames of 2048x4096, 2048x2048, 1024x4096, each "
+                                   "queued 4 times; FWHM U(2,5), 500-20000 stars, 0-3% masked; n_max 6, 4x4 knots, "
+                                   "GCV, decorrelate + score + CCL", "precision": "mixed",
+                       "timing": "wall clock, device synchronize and barrier on both sides; one untimed pass "
+                                 "over the distinct frames first"}}), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main(argv=None) -> int:
     args = parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "uneven":
+        return run_uneven(args)
     return run_gpu(args)
 
 

@@ -252,6 +252,7 @@ def photometric_scale_at(knots, theta, component_sums, points) -> np.ndarray:
 # FP64 in every mode): "fp64" (default, accuracy reference), "fp32" (plain
 # FP32 SIMT), "mixed" (tensor-core split products + one FP64 refinement step).
 PRECISIONS = {"fp64": _lib.PREC_FP64, "fp32": _lib.PREC_FP32, "mixed": _lib.PREC_MIXED}
+_PREC_NAMES = {v: k for k, v in PRECISIONS.items()}
 _default_precision = "fp64"
 
 
@@ -296,6 +297,10 @@ def _gls_dict(res, bufs) -> dict:
         "rss": float(res.rss),
         "lambda_grid": bufs["lambda_grid"][:nl].copy(),
         "gcv_curve": bufs["gcv_curve"][:nl].copy(),
+        # extensions: the arithmetic that produced theta and the last mixed
+        # refinement correction (see dgpu_gls_result)
+        "precision_used": _PREC_NAMES.get(int(res.precision_used), str(int(res.precision_used))),
+        "refine_correction": float(res.refine_correction),
     }
 
 

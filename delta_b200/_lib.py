@@ -110,6 +110,8 @@ class GlsResult(ctypes.Structure):
         ("n_stamps_rejected", ctypes.c_int),
         ("cv_exact_design_bytes", ctypes.c_int64),
         ("n_lambda_out", ctypes.c_int),
+        ("refine_correction", ctypes.c_double),
+        ("precision_used", ctypes.c_int),
     ]
 
 

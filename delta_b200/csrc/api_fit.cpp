@@ -86,6 +86,8 @@ struct GlsOut {
   long long npix = 0;  // active rows of the fit
   std::vector<double> grid, curve;
   const double* d_theta = nullptr;  // device copy of theta
+  double refine_correction = 0.0;   // ||delta|| / ||theta|| of the mixed refinement step
+  int prec_used = DGPU_PREC_FP64;
 };
 
 // Rows + normal-equation machinery shared by fit_kernel and solve_gls*.
@@ -219,7 +221,7 @@ struct Engine {
     return down(c, w.gcv, nsys);
   }
 
-  GlsOut gcv(const std::vector<double>& grid, const uint8_t* mask) {
+  GlsOut gcv_once(const std::vector<double>& grid, const uint8_t* mask) {
     if (grid.empty()) fail(DGPU_ERR_RUNTIME, "solve_gls_gcv: lambda_grid is empty");
     const int nl = static_cast<int>(grid.size());
     double* M = static_cast<double*>(c.slot(kSlotScratch1,
@@ -264,6 +266,39 @@ struct Engine {
     return o;
   }
 
+  // Mixed precision falls back to FP64 normal equations, for the rest of this
+  // fit, when its solve is non-finite or its FP64 refinement correction is
+  // above kMixedFallback of theta: one step leaves about the square of that
+  // relative error, and past it the BF16x3 system is too far from the FP64 one
+  // for the system's conditioning.
+  static constexpr double kMixedFallback = 1e-2;
+  bool mixed_failed(const GlsOut& o) const {
+    if (o.prec_used != DGPU_PREC_MIXED) return false;
+    if (!(o.refine_correction <= kMixedFallback)) return true;
+    for (double v : o.theta)
+      if (!std::isfinite(v)) return true;
+    return false;
+  }
+  template <class F>
+  GlsOut with_fallback(F&& run) {
+    GlsOut o = run();
+    if (mixed_failed(o)) {
+      prec = DGPU_PREC_FP64;
+      o = run();
+    }
+    return o;
+  }
+  GlsOut gcv(const std::vector<double>& grid, const uint8_t* mask) {
+    return with_fallback([&] { return gcv_once(grid, mask); });
+  }
+  GlsOut fixed(double lam, const uint8_t* mask) {
+    return with_fallback([&] { return fixed_once(lam, mask); });
+  }
+  GlsOut cv(const std::vector<double>& grid, const uint8_t* mask, const std::vector<int>& fold, int G, int warm_start,
+            bool stamped) {
+    return with_fallback([&] { return cv_once(grid, mask, fold, G, warm_start, stamped); });
+  }
+
   // Fill theta / scalars of system `s` into o. Mixed precision: one FP64
   // refinement step from the anchor residual at theta_s (computed here unless
   // `anchored`), and the rss / GCV of the refined theta around that anchor.
@@ -281,19 +316,31 @@ struct Engine {
       launch_gcv_finish(c.stream, 1, w.raw + s, w.edf + s, w.ok + s, n, w.rss + s, w.gcv + s);
     }
     o.theta.resize(P);
-    Fetch f(c, sizeof(double) * (P + 4));
+    std::vector<double> delta(prec == DGPU_PREC_MIXED ? P : 0);
+    Fetch f(c, sizeof(double) * (2 * P + 4));
     f.add(o.theta.data(), th, P);
     f.add(&o.edf, w.edf + s, 1);
     f.add(&o.rss, w.rss + s, 1);
     f.add(&o.gcv, w.gcv + s, 1);
     f.add(&o.npix, n, 1);
+    if (!delta.empty()) f.add(delta.data(), anchor_buffers().delta, P);
     f.run();
     o.d_theta = th;
     o.lambda = lam;
+    o.prec_used = prec;
+    if (!delta.empty()) {
+      double dd = 0.0, tt = 0.0;
+      for (int p = 0; p < P; ++p) {
+        dd += delta[p] * delta[p];
+        tt += o.theta[p] * o.theta[p];
+      }
+      o.refine_correction = tt > 0.0 ? std::sqrt(dd / tt) : (dd > 0.0 ? kInf : 0.0);
+      if (!std::isfinite(dd) || !std::isfinite(tt)) o.refine_correction = kInf;
+    }
   }
 
   // Fixed-lambda solve (src/solve.cpp:208-215).
-  GlsOut fixed(double lam, const uint8_t* mask) {
+  GlsOut fixed_once(double lam, const uint8_t* mask) {
     double* M = static_cast<double*>(c.slot(kSlotScratch1, sizeof(double) * (static_cast<size_t>(P) * P + P + 2)));
     double* rhs = M + static_cast<size_t>(P) * P;
     double* ywy = rhs + P;
@@ -311,8 +358,8 @@ struct Engine {
 
   // Group CV over per-unit folds (fold[u] in [0, G), -1 = excluded).
   // stamped: per-stamp Kronecker build with stamp designs at pixel centroids.
-  GlsOut cv(const std::vector<double>& grid, const uint8_t* mask, const std::vector<int>& fold, int G,
-            int warm_start, bool stamped) {
+  GlsOut cv_once(const std::vector<double>& grid, const uint8_t* mask, const std::vector<int>& fold, int G,
+                 int warm_start, bool stamped) {
     if (grid.empty()) fail(DGPU_ERR_RUNTIME, "solve_gls_cv: lambda_grid is empty");
     const int nl = static_cast<int>(grid.size());
     const size_t PP = static_cast<size_t>(P) * P;
@@ -523,6 +570,8 @@ void write_gls(const GlsOut& o, int nc, int k, dgpu_gls_result* out) {
   out->effective_dof = o.edf;
   out->rss = o.rss;
   out->n_lambda_out = static_cast<int>(o.grid.size());
+  out->refine_correction = o.refine_correction;
+  out->precision_used = o.prec_used;
   if (out->lambda_grid && !o.grid.empty()) std::memcpy(out->lambda_grid, o.grid.data(), sizeof(double) * o.grid.size());
   if (out->gcv_curve && !o.curve.empty()) std::memcpy(out->gcv_curve, o.curve.data(), sizeof(double) * o.curve.size());
 }

@@ -302,7 +302,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
     // Stage the chunk's rows as FP32, value-major (the previous chunk's
     // generation finished at the last barrier). Row weights first (0 for
     // inactive rows); then thread (value q = lane, rows 4 g .. 4 g + 3)
-    // converts four rows of one value and stores them as one float4.
+    // converts four rows of one value and stores them as one float4. Rows of
+    // weight 0 stage zeros: an inactive row may hold a non-finite value (a
+    // masked pixel), and 0 x NaN would reach the sums through the tensor core.
     for (int r = tid; r < kKC; r += blockDim.x) {
       const int64_t row = r0 + r;
       float wr = 0.0f;
@@ -320,7 +322,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
           for (int i = 0; i < 4; ++i) {
             const int r = 4 * g + i;
             const int64_t row = r0 + r;
-            const bool in = r < rows;
+            const bool in = r < rows && w_s[r] != 0.0f;
             bv[i] = 0.0f;
             dv[i] = 0.0f;
             if (in && q < nf)

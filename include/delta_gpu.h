@@ -181,6 +181,12 @@ typedef struct {
   int n_stamps_rejected;
   int64_t cv_exact_design_bytes;
   int n_lambda_out; /* entries written to lambda_grid / gcv_curve (0 for a fixed-lambda solve) */
+  /* Beyond the reference's fields: the normal-equation arithmetic that produced
+   * theta (DGPU_PREC_*; mixed falls back to fp64 when its FP64 refinement step
+   * shows the BF16x3 solve too inaccurate for the system's conditioning), and
+   * ||correction|| / ||theta|| of the last mixed refinement step (0 otherwise). */
+  double refine_correction;
+  int precision_used;
 } dgpu_gls_result;
 
 /* fit_kernel, src/bindings.cpp:643-693 -> delta::fit_kernel, src/fit.cpp:63-511

@@ -77,3 +77,23 @@ def test_reference_arm_other_ranks_exit_quietly(capsys, monkeypatch):
     monkeypatch.setenv("WORLD_SIZE", "2")
     assert bench.main(["--impl", "reference", "--gpus", "2"]) == 0
     assert capsys.readouterr().out == ""
+
+
+def test_uneven_batch_specs_queue_and_dealing():
+    specs = bench.uneven_specs(0)
+    assert len(specs) == bench.UNEVEN_DISTINCT
+    assert {(s["height"], s["width"]) for s in specs} == set(bench.UNEVEN_SHAPES)
+    assert all(2.0 <= s["sci_fwhm"] <= 5.0 and 500 <= s["n_stars"] <= 20000 and 0 <= s["mask_fraction"] <= 0.03
+               for s in specs)
+    assert specs == bench.uneven_specs(0) and specs != bench.uneven_specs(1)
+    q = bench.uneven_queue(0)
+    assert len(q) == bench.UNEVEN_FRAMES
+    assert all(sorted(q[i:i + 16]) == list(range(16)) for i in range(0, 64, 16))
+    px = [specs[j]["height"] * specs[j]["width"] for j in q]
+    assert bench.lpt_deal(px, 1) == [0] * len(px)
+    for world in (2, 4, 8):
+        owner = bench.lpt_deal(px, world)
+        loads = [sum(p for p, r in zip(px, owner) if r == k) for k in range(world)]
+        assert max(loads) - min(loads) <= max(px)
+    # equal items alternate ranks in index order
+    assert bench.lpt_deal([5, 5, 5, 5], 2) == [0, 1, 0, 1]

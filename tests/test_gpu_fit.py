@@ -101,6 +101,8 @@ def test_solve_gls_gcv_large_system_matches_oracle():
     np.testing.assert_allclose(got["gcv_curve"], want["gcv_curve"], rtol=1e-6)
     np.testing.assert_allclose(got["effective_dof"], want["effective_dof"], rtol=1e-7)
     mixed = _core.solve_gls_gcv(knots, pts, t, w, bn, GRID, precision="mixed")
+    # a refinement correction of 2.5e-3 keeps the mixed solve (fallback above 1e-2)
+    assert mixed["precision_used"] == "mixed" and 0.0 < mixed["refine_correction"] < 1e-2
     i = int(np.argmin(want["gcv_curve"]))
     near = slice(max(0, i - 2), i + 3)
     np.testing.assert_allclose(mixed["gcv_curve"][near], want["gcv_curve"][near], rtol=2e-4)

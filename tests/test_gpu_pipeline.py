@@ -285,3 +285,38 @@ def test_copy_to_host_by_sm_stores():
     with pytest.raises(ValueError):
         _lib.check(_lib.lib().dgpu_copy_to_host(ctx.handle, ctypes.c_void_p(pageable.ctypes.data),
                                                 ctypes.c_void_p(src.data_ptr()), ctypes.c_int64(256)), ctx.handle)
+
+
+def test_mixed_precision_falls_back_on_an_ill_conditioned_fit():
+    """A frame whose PSFs nearly match drives beta to its 0.5 floor: the fit's
+    theta then carries large cancelling terms (|theta| ~ 600 for a unit
+    kernel), and the BF16x3 normal equations cannot resolve it. The mixed fit
+    must fall back to FP64 and give the FP64 pipeline's products bit for bit."""
+    import bench
+
+    sp = bench.uneven_specs(0)[4]  # 2048 x 2048, science FWHM 2.1 px vs 2.5 px reference, 2.2% masked
+    p = validation.synthetic_pair(sp["width"], sp["height"], sp["n_stars"], sp["seed"], sci_fwhm=sp["sci_fwhm"],
+                                  mask_fraction=sp["mask_fraction"])
+    layers = dict(science_var=p.science_var, reference_var=p.reference_var, science_mask=p.science_mask,
+                  reference_mask=p.reference_mask)
+    seen = {}
+    fit_kernel = _core.fit_kernel
+
+    def spy(*a, **k):
+        r = fit_kernel(*a, **k)
+        seen[k.get("precision", "fp64")] = r["precision_used"]
+        return r
+
+    _core.fit_kernel = spy
+    try:
+        sol_mixed = delta.Subtractor(**bench.subtract_kwargs(p, "mixed")).fit(p.science, p.reference, **layers)
+    finally:
+        _core.fit_kernel = fit_kernel
+    assert seen == {"mixed": "fp64"}
+    assert sol_mixed.beta == 0.5 and np.all(np.isfinite(sol_mixed.theta))
+    a = delta.subtract(p.science, p.reference, **layers, **bench.subtract_kwargs(p, "mixed"))
+    b = delta.subtract(p.science, p.reference, **layers, **bench.subtract_kwargs(p, "fp64"))
+    np.testing.assert_array_equal(a.solution.theta, b.solution.theta)
+    for name in ("difference", "variance", "mask", "score"):
+        np.testing.assert_array_equal(getattr(a, name), getattr(b, name), err_msg=name)
+    assert float(np.max(a.psf)) > 0.0 and len(a.source_catalog) == len(b.source_catalog)
