@@ -320,3 +320,52 @@ def test_mixed_precision_falls_back_on_an_ill_conditioned_fit():
     for name in ("difference", "variance", "mask", "score"):
         np.testing.assert_array_equal(getattr(a, name), getattr(b, name), err_msg=name)
     assert float(np.max(a.psf)) > 0.0 and len(a.source_catalog) == len(b.source_catalog)
+
+
+def _uneven_vs_chain(spec_index):
+    import bench
+    from oracle import chain
+
+    if not chain.available():
+        pytest.skip("oracle/_ref is not built")
+    sp = bench.uneven_specs(0)[spec_index]
+    p = validation.synthetic_pair(sp["width"], sp["height"], sp["n_stars"], sp["seed"], sci_fwhm=sp["sci_fwhm"],
+                                  mask_fraction=sp["mask_fraction"])
+    kw = bench.subtract_kwargs(p, "fp64")
+    res = delta.subtract(p.science, p.reference, science_var=p.science_var, reference_var=p.reference_var,
+                         science_mask=p.science_mask, reference_mask=p.reference_mask, **kw)
+    kw.pop("saturation")
+    kw.pop("precision")
+    want = chain.run(p.science, p.reference, p.science_var, p.reference_var, p.science_mask, p.reference_mask,
+                     saturation=p.saturation, **kw)
+    var = np.asarray(want["variance"], np.float64)
+    pos = var > 0
+    dd = np.abs(res.difference.astype(np.float64) - want["difference"])[pos] / np.sqrt(var[pos])
+    return res, want, dd
+
+
+@pytest.mark.parametrize("spec_index", [2, 7])
+def test_uneven_frames_match_oracle_chain(spec_index):
+    """Whole pipeline (FP64 fit, decorrelation, score, catalog) on frames of the
+    uneven batch against the oracle chain on the same inputs: 1024 x 4096 and
+    2048 x 2048. Masks bit-exact, whitened difference and score within 1e-3 of
+    the local sigma, catalog sizes within one row."""
+    res, want, dd = _uneven_vs_chain(spec_index)
+    np.testing.assert_array_equal(res.mask, want["mask"])
+    assert np.max(dd) < 1e-3
+    assert np.max(np.abs(res.score.astype(np.float64) - want["score"])) < 1e-3
+    assert abs(len(res.source_catalog) - len(want["catalog"]["x"])) <= 1
+
+
+def test_beta_floor_frame_against_oracle_chain():
+    """A frame whose fit sits at the beta floor: theta is ill-determined (about
+    600 in large cancelling terms for a unit kernel), so two FP64 solvers that
+    sum in different orders agree on the lambda and on |theta| to four digits
+    but not on the model everywhere: measured, the difference moves by a median
+    1.05e-3 sigma and at most 0.49 sigma between this solver and the oracle's.
+    Masks stay bit-exact; the bounds below are 3x and 2x those figures."""
+    res, want, dd = _uneven_vs_chain(4)
+    np.testing.assert_array_equal(res.mask, want["mask"])
+    assert np.median(dd) < 3e-3 and np.max(dd) < 1.0, (np.median(dd), np.max(dd))
+    n_got, n_want = len(res.source_catalog), len(want["catalog"]["x"])
+    assert abs(n_got - n_want) <= 2, (n_got, n_want)
