@@ -104,6 +104,7 @@ void launch_exact_fields(cudaStream_t s, const TpsDev& t, const double* theta, i
 // ---------------------------------------------------------------------------
 
 constexpr int kMcTW = 32;   // tile width (columns)
+constexpr int kMcPad = 8;   // zero rows in front of each x-pass buffer (y-pass reads reach row -7)
 constexpr int kMcYR = 4;    // output rows per thread in the y pass (2 columns each)
 constexpr int kMcXPT = 4;   // output columns per thread in the x pass
 
@@ -129,9 +130,10 @@ k_model_convolve(int w, int h, const float* __restrict__ sci, const float* __res
   const int gbw = kMcTW + 2 * kh;
   const int gbw_pad = (gbw + 3) & ~3;
   const int kts = mc_tap_stride(ks);
+  const int trows = nrows + kMcPad;
   float* rtile = smem;                                       // nrows x gbw_pad
-  float* txs = rtile + nrows * gbw_pad;                      // NX x nrows x kMcTW
-  float* ktaps = txs + NX * nrows * kMcTW;                   // NX x kts (zero padded, 16-byte aligned rows)
+  float* txs = rtile + nrows * gbw_pad;                      // NX x (kMcPad zero rows + nrows) x kMcTW
+  float* ktaps = txs + NX * trows * kMcTW;                   // NX x kts (zero padded, 16-byte aligned rows)
   const int bx = blockIdx.x * kMcTW, by = blockIdx.y * TH;
   const float fill = STACK ? 0.0f : *fillp;
   const int tid = threadIdx.x;
@@ -139,6 +141,10 @@ k_model_convolve(int w, int h, const float* __restrict__ sci, const float* __res
   for (int i = tid; i < NX * kts; i += blockDim.x) {
     const int q = i / kts, j = i - q * kts;
     ktaps[i] = j < ks ? taps[q * ks + j] : 0.0f;
+  }
+  for (int i = tid; i < NX * kMcPad * kMcTW; i += blockDim.x) {
+    const int q = i / (kMcPad * kMcTW);
+    txs[q * trows * kMcTW + (i - q * kMcPad * kMcTW)] = 0.0f;
   }
   for (int i = tid; i < nrows * gbw; i += blockDim.x) {
     const int r = i / gbw, c = i - r * gbw;
@@ -198,7 +204,7 @@ k_model_convolve(int w, int h, const float* __restrict__ sci, const float* __res
 #pragma unroll
     for (int q = 0; q < NX; ++q) {
       float4 v = make_float4(acc[q][0], acc[q][1], acc[q][2], acc[q][3]);
-      *reinterpret_cast<float4*>(txs + (q * nrows + r) * kMcTW + c0) = v;
+      *reinterpret_cast<float4*>(txs + (q * trows + kMcPad + r) * kMcTW + c0) = v;
     }
   }
   __syncthreads();
@@ -285,7 +291,11 @@ k_model_convolve(int w, int h, const float* __restrict__ sci, const float* __res
   }
   for (int n = 0; n < nc; ++n) {
     const int2 o = orders[n];
-    const float2* col = reinterpret_cast<const float2*>(txs + static_cast<size_t>(o.x) * nrows * kMcTW + lx0);
+    // Row kMcPad of the component's buffer is row 0; the pad rows above are
+    // zeros, so the reads of rows -7..-1 (taps past the top of the frame) need
+    // no test.
+    const float2* col =
+        reinterpret_cast<const float2*>(txs + (static_cast<size_t>(o.x) * trows + kMcPad) * kMcTW + lx0);
     const float* ky = ktaps + o.y * kts;
     // Output row ly0+i needs buffer row ly0 + i + 2kh - j. Taps go in blocks of
     // 8 with the rows of a block held in registers (static indices), each
@@ -296,11 +306,9 @@ k_model_convolve(int w, int h, const float* __restrict__ sci, const float* __res
     for (int i = 0; i < kMcYR; ++i) bn[i] = make_float2(0.0f, 0.0f);
     for (int j0 = 0; j0 < ks; j0 += 8) {
       float2 v[kMcYR + 7];  // v[t] = buffer row base - j0 - 7 + t
+      const float2* vb = col + (base - j0 - 7) * (kMcTW / 2);
 #pragma unroll
-      for (int t = 0; t < kMcYR + 7; ++t) {
-        const int rr = base - j0 - 7 + t;
-        v[t] = rr >= 0 ? col[rr * (kMcTW / 2)] : make_float2(0.0f, 0.0f);
-      }
+      for (int t = 0; t < kMcYR + 7; ++t) v[t] = vb[t * (kMcTW / 2)];
       const float4 ka = *reinterpret_cast<const float4*>(ky + j0);
       const float4 kb = *reinterpret_cast<const float4*>(ky + j0 + 4);
       const float kv[8] = {ka.x, ka.y, ka.z, ka.w, kb.x, kb.y, kb.z, kb.w};
@@ -360,8 +368,8 @@ size_t model_convolve_smem(int nx, int ks, int TH) {
   const int kh = (ks - 1) / 2;
   const int nrows = TH + 2 * kh;
   const int gbw_pad = ((kMcTW + 2 * kh) + 3) & ~3;
-  return sizeof(float) * (static_cast<size_t>(nrows) * gbw_pad + static_cast<size_t>(nx) * nrows * kMcTW +
-                          static_cast<size_t>(nx) * mc_tap_stride(ks));
+  return sizeof(float) * (static_cast<size_t>(nrows) * gbw_pad +
+                          static_cast<size_t>(nx) * (nrows + kMcPad) * kMcTW + static_cast<size_t>(nx) * mc_tap_stride(ks));
 }
 
 void launch_model_convolve_orders(cudaStream_t s, const SubtractArgs& a, const int2* orders, bool stack) {
