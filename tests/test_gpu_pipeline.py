@@ -369,3 +369,25 @@ def test_beta_floor_frame_against_oracle_chain():
     assert np.median(dd) < 3e-3 and np.max(dd) < 1.0, (np.median(dd), np.max(dd))
     n_got, n_want = len(res.source_catalog), len(want["catalog"]["x"])
     assert abs(n_got - n_want) <= 2, (n_got, n_want)
+
+
+@pytest.mark.parametrize("spec_index", [2, 7])
+def test_mixed_pipeline_close_to_fp64_on_uneven_frames(spec_index):
+    """The mixed-precision pipeline against the FP64 one on frames of the uneven
+    batch (refinement corrections near 1e-3, so the mixed solve is kept): masks
+    bit-exact, difference within 1e-3 of the local sigma, same catalog size."""
+    import bench
+
+    sp = bench.uneven_specs(0)[spec_index]
+    p = validation.synthetic_pair(sp["width"], sp["height"], sp["n_stars"], sp["seed"], sci_fwhm=sp["sci_fwhm"],
+                                  mask_fraction=sp["mask_fraction"])
+    layers = dict(science_var=p.science_var, reference_var=p.reference_var, science_mask=p.science_mask,
+                  reference_mask=p.reference_mask)
+    a = delta.subtract(p.science, p.reference, **layers, **bench.subtract_kwargs(p, "mixed"))
+    b = delta.subtract(p.science, p.reference, **layers, **bench.subtract_kwargs(p, "fp64"))
+    assert a.solution.lam == b.solution.lam
+    np.testing.assert_array_equal(a.mask, b.mask)
+    pos = b.variance > 0
+    dd = np.abs(a.difference.astype(np.float64) - b.difference)[pos] / np.sqrt(b.variance[pos].astype(np.float64))
+    assert np.max(dd) < 1e-3, np.max(dd)
+    assert len(a.source_catalog) == len(b.source_catalog)
