@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <limits>
 #include <numeric>
 
@@ -104,6 +105,10 @@ struct Engine {
   int rk = 0;
   double* d_pen = nullptr;
   double* d_fk = nullptr;
+  // Optional extra reads joined to a solution's read-back: called with the
+  // device theta just before the fetch runs (fit_kernel's per-stamp chi^2).
+  std::function<void(const double*, Fetch&)> on_fetch;
+  size_t on_fetch_bytes = 0;
 
   Engine(Context& ctx, int precision, const ThinPlate& t, int nc_, int64_t N_, int SS_, int units)
       : c(ctx), prec(precision), tp(t), nc(nc_), nf(nc_ + 1), k(t.k), P((nc_ + 1) * t.k), N(N_), SS(SS_),
@@ -203,11 +208,13 @@ struct Engine {
   // quadratic term, where ywy - 2 theta . rhs + theta^T M theta would carry it
   // at the scale of ywy (the rss is often 1e-4 of ywy or less).
   struct Anchor {
-    double *r0, *rp, *delta, *s0;
+    double *r0, *rp, *delta, *s0, *theta0, *approx;
   };
-  Anchor anchor_buffers() {
-    double* a = static_cast<double*>(c.slot(kSlotFit15, sizeof(double) * (3 * static_cast<size_t>(P) + 2)));
-    return Anchor{a, a + P, a + 2 * P, a + 3 * P};
+  // The anchor's vectors, theta0 and room for `curve` copied curve values.
+  Anchor anchor_buffers(int curve = 0) {
+    double* a = static_cast<double*>(
+        c.slot(kSlotFit15, sizeof(double) * (4 * static_cast<size_t>(P) + 2 + static_cast<size_t>(curve))));
+    return Anchor{a, a + P, a + 2 * P, a + 3 * P, a + 3 * P + 2, a + 4 * P + 2};
   }
   void anchor_at(const Anchor& a, const double* theta, const uint8_t* mask) {
     launch_rhs(c, N, nc, k, SS, R, mask, theta, a.r0, a.s0, nullptr);
@@ -237,30 +244,47 @@ struct Engine {
     launch_gcv_finish(c.stream, nl, w.raw, w.edf, w.ok, n, w.rss, w.gcv);
     GlsOut o;
     o.grid = grid;
-    o.curve = down(c, w.gcv, nl);
-    auto argmin = [&]() {
+    auto argmin = [&](const std::vector<double>& v) {  // first minimum; NaN never wins (launch_argmin_copy)
       int b = 0;
       double bg = kInf;
       for (int i = 0; i < nl; ++i)
-        if (o.curve[i] < bg) {
-          bg = o.curve[i];
+        if (v[i] < bg) {
+          bg = v[i];
           b = i;
         }
       return b;
     };
-    int best = argmin();
-    int anchored = -1;
+    int best = 0, anchored = -1;
     if (prec == DGPU_PREC_MIXED) {
       // Re-evaluate the curve around the provisional minimum until the minimum
-      // stays put (it moves at most a grid step or two).
-      const Anchor a = anchor_buffers();
-      for (int pass = 0; pass < 3 && anchored != best; ++pass) {
+      // stays put (it moves at most a grid step or two). The first anchor is
+      // picked on the device, so both curves come back in one read.
+      const Anchor a = anchor_buffers(nl);
+      DGPU_CUDA(cudaMemcpyAsync(a.approx, w.gcv, sizeof(double) * nl, cudaMemcpyDeviceToDevice, c.stream));
+      launch_argmin_copy(c.stream, nl, w.gcv, w.theta, P, a.theta0);
+      anchor_at(a, a.theta0, mask);
+      launch_quad_err(c, nl, P, w.theta, M, nullptr, a.r0, nullptr, a.s0, w.raw, a.theta0);
+      launch_gcv_finish(c.stream, nl, w.raw, w.edf, w.ok, n, w.rss, w.gcv);
+      std::vector<double> approx(nl);
+      o.curve.resize(nl);
+      {
+        Fetch f(c, sizeof(double) * 2 * nl);
+        f.add(approx.data(), a.approx, nl);
+        f.add(o.curve.data(), w.gcv, nl);
+        f.run();
+      }
+      anchored = argmin(approx);
+      best = argmin(o.curve);
+      for (int pass = 1; pass < 3 && anchored != best; ++pass) {
         const double* th0 = w.theta + static_cast<size_t>(best) * P;
         anchor_at(a, th0, mask);
         anchored = best;
         o.curve = anchored_curve(w, nl, M, a, th0, n);
-        best = argmin();
+        best = argmin(o.curve);
       }
+    } else {
+      o.curve = down(c, w.gcv, nl);
+      best = argmin(o.curve);
     }
     finish_single(w, best, grid[best], M, n, mask, o, anchored == best);
     return o;
@@ -317,13 +341,14 @@ struct Engine {
     }
     o.theta.resize(P);
     std::vector<double> delta(prec == DGPU_PREC_MIXED ? P : 0);
-    Fetch f(c, sizeof(double) * (2 * P + 4));
+    Fetch f(c, sizeof(double) * (2 * P + 4) + on_fetch_bytes);
     f.add(o.theta.data(), th, P);
     f.add(&o.edf, w.edf + s, 1);
     f.add(&o.rss, w.rss + s, 1);
     f.add(&o.gcv, w.gcv + s, 1);
     f.add(&o.npix, n, 1);
     if (!delta.empty()) f.add(delta.data(), anchor_buffers().delta, P);
+    if (on_fetch) on_fetch(th, f);
     f.run();
     o.d_theta = th;
     o.lambda = lam;
@@ -783,6 +808,13 @@ int dgpu_fit_kernel(dgpu_context* ctx, int mem, int64_t width, int64_t height, c
     bool use_stamped = knot_spacing > 0.0 && knot_spacing >= 16.0 * (2.0 * stamp_radius + 1.0);
     if (const char* e = std::getenv("DELTA_STAMP_APPROX")) use_stamped = std::atoi(e) != 0;
 
+    // Per-stamp chi^2 of each solution rides on the solution's own read-back.
+    E.on_fetch_bytes = (sizeof(double) + sizeof(int)) * static_cast<size_t>(n_stamps) + 64;
+    E.on_fetch = [&](const double* d_theta, Fetch& f) {
+      launch_stamp_chi2(st, n_stamps, nc, k, g.SS, E.R, d_acc, d_theta, chi2_d, cnt_d);
+      f.add(stamp_chi2.data(), chi2_d, n_stamps);
+      f.add(cnt.data(), cnt_d, n_stamps);
+    };
     for (int iter = 0;; ++iter) {
       DGPU_CUDA(h2d_async(d_acc, accepted.data(), n_stamps, st));
       // The active-row count comes back with the solve (the rows are the same).
@@ -798,13 +830,6 @@ int dgpu_fit_kernel(dgpu_context* ctx, int mem, int64_t width, int64_t height, c
       npix = gls.npix;
       if (npix == 0) fail(DGPU_ERR_RUNTIME, "fit_kernel: all stamp pixels clipped");
       if (cv_folds > 1 && !use_stamped) cv_exact_bytes = static_cast<size_t>(npix) * E.P * sizeof(double);
-      launch_stamp_chi2(st, n_stamps, nc, k, g.SS, E.R, d_acc, gls.d_theta, chi2_d, cnt_d);
-      {
-        Fetch f(c, (sizeof(double) + sizeof(int)) * n_stamps);
-        f.add(stamp_chi2.data(), chi2_d, n_stamps);
-        f.add(cnt.data(), cnt_d, n_stamps);
-        f.run();
-      }
       const double denom = static_cast<double>(npix) - gls.edf;
       reduced = denom > 0.0 ? gls.rss / denom : kNaN;
       if (have_var) {

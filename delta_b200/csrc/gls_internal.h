@@ -10,6 +10,9 @@ namespace dgpu {
 void launch_quad_err(Context& c, int nsys, int P, const double* theta, const double* M, const int* m_index,
                      const double* r, const int* r_index, const double* y, double* out,
                      const double* anchor = nullptr);
+// theta0 = the row of theta (P per row) at argmin(curve), chosen on the device.
+void launch_argmin_copy(cudaStream_t st, int nsys, const double* curve, const double* theta, int P,
+                        double* theta0);
 void launch_gcv_finish(cudaStream_t st, int nsys, const double* raw, const double* edf, const int* ok,
                        const long long* n, double* rss, double* gcv);
 void launch_fold_train(cudaStream_t st, int groups, size_t len, const double* part, double* all, double* train);

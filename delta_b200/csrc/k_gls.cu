@@ -83,6 +83,32 @@ __global__ void k_quad_finish(int nsys, int nb, const double* __restrict__ part,
   }
 }
 
+// theta0 = theta of the first system with the smallest curve value (NaN never
+// wins; all-NaN picks system 0), the host's argmin rule.
+__global__ void k_argmin_copy(int nsys, const double* __restrict__ curve, const double* __restrict__ theta, int P,
+                              double* __restrict__ theta0) {
+  __shared__ int s_best;
+  if (threadIdx.x == 0) {
+    int b = 0;
+    double bg = __longlong_as_double(0x7ff0000000000000ll);
+    for (int i = 0; i < nsys; ++i)
+      if (curve[i] < bg) {
+        bg = curve[i];
+        b = i;
+      }
+    s_best = b;
+  }
+  __syncthreads();
+  const double* src = theta + static_cast<size_t>(s_best) * P;
+  for (int p = threadIdx.x; p < P; p += blockDim.x) theta0[p] = src[p];
+}
+
+void launch_argmin_copy(cudaStream_t st, int nsys, const double* curve, const double* theta, int P,
+                        double* theta0) {
+  k_argmin_copy<<<1, 256, 0, st>>>(nsys, curve, theta, P, theta0);
+  DGPU_LAUNCH("k_argmin_copy");
+}
+
 void launch_quad_err(Context& c, int nsys, int P, const double* theta, const double* M, const int* m_index,
                      const double* r, const int* r_index, const double* y, double* out, const double* anchor) {
   if (nsys == 0) return;
