@@ -1,7 +1,6 @@
 // Host driver of the ZOGY decorrelation (reference src/noise.cpp:228-533,
-// src/bindings.cpp:725-874). Block geometry, the Hann tables and the colour
-// lists are tiny host tables; all FFT, filter and overlap-add work is on the
-// device (k_fft.cu).
+// src/bindings.cpp:725-874). Block geometry and the Hann tables are tiny host
+// tables; all FFT, filter and overlap-add work is on the device (k_fft.cu).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -137,12 +136,8 @@ int dgpu_decorrelate(dgpu_context* ctx, int mem, int64_t width, int64_t height, 
       centres[2 * ci + 1] = std::clamp(oys[repy] + block / 2.0, 0.0, h - 1.0);
     }
     std::vector<int> block_cell(nblk);
-    std::vector<std::vector<int>> colours(9);
     for (int iy = 0; iy < noy; ++iy)
-      for (int ix = 0; ix < nox; ++ix) {
-        block_cell[iy * nox + ix] = (iy / kgroup) * ncellx + (ix / kgroup);
-        colours[(ix % 3) * 3 + (iy % 3)].push_back(iy * nox + ix);
-      }
+      for (int ix = 0; ix < nox; ++ix) block_cell[iy * nox + ix] = (iy / kgroup) * ncellx + (ix / kgroup);
     const std::vector<double> hw = hann(n);
     std::vector<double> wxt(w, 0.0), wyt(h, 0.0);
     for (int bx : oxs)
@@ -155,20 +150,10 @@ int dgpu_decorrelate(dgpu_context* ctx, int mem, int64_t width, int64_t height, 
     std::vector<int> itab;
     itab.insert(itab.end(), oxs.begin(), oxs.end());
     itab.insert(itab.end(), oys.begin(), oys.end());
-    itab.insert(itab.end(), block_cell.begin(), block_cell.end());
-    std::vector<int> colour_items;
-    std::vector<int> colour_off(10, 0);
-    for (int q = 0; q < 9; ++q) {
-      colour_off[q] = static_cast<int>(colour_items.size());
-      colour_items.insert(colour_items.end(), colours[q].begin(), colours[q].end());
-    }
-    colour_off[9] = static_cast<int>(colour_items.size());
-    itab.insert(itab.end(), colour_items.begin(), colour_items.end());
     int* dit = up(c, kSlotCellX, itab.data(), itab.size());
     const int* d_oxs = dit;
     const int* d_oys = dit + nox;
     const int* d_bcell = d_oys + noy;
-    const int* d_citems = d_bcell + nblk;
     std::vector<double> dtab;
     dtab.insert(dtab.end(), hw.begin(), hw.end());
     dtab.insert(dtab.end(), wxt.begin(), wxt.end());

@@ -338,17 +338,18 @@ k_model_convolve(int w, int h, const float* __restrict__ sci, const float* __res
 #pragma unroll
     for (int i = 0; i < kMcYR; ++i) d2[i] = __ffma2_rn(make_float2(-a[i].x, -a[i].y), bn[i], d2[i]);
   }
-  if (STACK) return;
+  if constexpr (!STACK) {
 #pragma unroll
-  for (int i = 0; i < kMcYR; ++i) {
-    const int y = by + ly0 + i;
-    if (y >= h) continue;
-    const size_t o = static_cast<size_t>(y) * w + x0;
-    if (xin[0] && xin[1] && (o & 1) == 0) {
-      *reinterpret_cast<float2*>(diff + o) = d2[i];
-    } else {
-      if (xin[0]) diff[o] = d2[i].x;
-      if (xin[1]) diff[o + 1] = d2[i].y;
+    for (int i = 0; i < kMcYR; ++i) {
+      const int y = by + ly0 + i;
+      if (y >= h) continue;
+      const size_t o = static_cast<size_t>(y) * w + x0;
+      if (xin[0] && xin[1] && (o & 1) == 0) {
+        *reinterpret_cast<float2*>(diff + o) = d2[i];
+      } else {
+        if (xin[0]) diff[o] = d2[i].x;
+        if (xin[1]) diff[o + 1] = d2[i].y;
+      }
     }
   }
 }
