@@ -150,6 +150,7 @@ int dgpu_decorrelate(dgpu_context* ctx, int mem, int64_t width, int64_t height, 
     std::vector<int> itab;
     itab.insert(itab.end(), oxs.begin(), oxs.end());
     itab.insert(itab.end(), oys.begin(), oys.end());
+    itab.insert(itab.end(), block_cell.begin(), block_cell.end());
     int* dit = up(c, kSlotCellX, itab.data(), itab.size());
     const int* d_oxs = dit;
     const int* d_oys = dit + nox;
