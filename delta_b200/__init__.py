@@ -38,35 +38,13 @@ from ._core import (
     weighted_mean,
     whiten_score_psf,
 )
+from ._core import read_fits, write_fits
 from ._core import subtract as subtract_model
 from ._inputs import as_layers, synth_variance
 from ._lib import DeviceLoopLimitError, DeviceUnavailableError
 from ._log import configure_logging
-from .pipeline import DiffResult, Subtractor, apply, apply_batch, subtract, subtract_batch
+from .pipeline import DiffResult, Subtractor, apply, apply_batch, subtract, subtract_batch, subtract_files
 from .solution import KernelSolution
-
-
-def read_fits(path: str):
-    """FITS input needs CFITSIO in the reference; use astropy here (not bundled)."""
-    from astropy.io import fits  # optional dependency
-
-    with fits.open(path) as hdul:
-        data = hdul[0].data if hdul[0].data is not None else hdul[1].data
-        var = hdul["VARIANCE"].data if "VARIANCE" in hdul else None
-        mask = hdul["MASK"].data if "MASK" in hdul else None
-        return {"data": data, "variance": var, "mask": mask}
-
-
-def write_fits(path: str, data, variance=None, mask=None, overwrite: bool = False) -> None:
-    """Write data plus optional variance / mask layers (astropy)."""
-    from astropy.io import fits  # optional dependency
-
-    hdus = [fits.PrimaryHDU(data)]
-    if variance is not None:
-        hdus.append(fits.ImageHDU(variance, name="VARIANCE"))
-    if mask is not None:
-        hdus.append(fits.ImageHDU(mask, name="MASK"))
-    fits.HDUList(hdus).writeto(path, overwrite=overwrite)
 
 
 __all__ = [
@@ -75,6 +53,6 @@ __all__ = [
     "decorrelate_block", "decorrelation_kernel", "detect_stamps", "estimate_background", "fit_kernel",
     "gauss_hermite_basis1d", "gauss_hermite_kernels", "grid_knots", "matched_filter", "photometric_scale",
     "photometric_scale_at", "read_fits", "select_stamps", "solve_gls", "solve_gls_cv", "solve_gls_gcv", "subtract",
-    "subtract_batch", "subtract_model", "synth_variance", "tps_design", "tps_evaluate", "tps_fit", "tps_penalty",
-    "validation", "weighted_mean", "whiten_score_psf", "write_fits",
+    "subtract_batch", "subtract_files", "subtract_model", "synth_variance", "tps_design", "tps_evaluate", "tps_fit",
+    "tps_penalty", "validation", "weighted_mean", "whiten_score_psf", "write_fits",
 ]

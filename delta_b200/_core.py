@@ -421,6 +421,56 @@ def _detect_params(stamp_radius, threshold_sigma, max_stamps, saturation, isolat
                              int(isolation_radius), int(border), int(fwhm_radius), int(match_radius))
 
 
+# ---- FITS I/O ------------------------------------------------------------------------
+
+
+def _fits_check(rc: int) -> None:
+    if rc == _lib.DGPU_OK:
+        return
+    msg = _lib.lib().dgpu_last_error(None).decode(errors="replace")
+    if rc == _lib.DGPU_ERR_INVALID:
+        raise ValueError(msg)
+    raise RuntimeError(msg)
+
+
+def read_fits(path: str, *, alloc=None) -> dict:
+    """Read a FITS file into {'data', 'variance', 'mask'} arrays (src/bindings.cpp:128-145):
+    the primary image, or the DIFFERENCE extension when the primary holds no
+    2-D image, plus the optional VARIANCE / MASK extensions (None when absent).
+
+    ``alloc(shape, dtype)`` (an extension) supplies the output arrays, e.g.
+    pinned host memory for a fast upload; the default is ``np.empty``."""
+    p = str(path).encode()
+    w, h = ctypes.c_int64(), ctypes.c_int64()
+    hv, hm = ctypes.c_int(), ctypes.c_int()
+    L = _lib.lib()
+    _fits_check(L.dgpu_fits_probe(p, ctypes.byref(w), ctypes.byref(h), ctypes.byref(hv), ctypes.byref(hm)))
+    make = alloc or (lambda shape, dtype: np.empty(shape, dtype))
+    shape = (int(h.value), int(w.value))
+    data = make(shape, np.float32)
+    var = make(shape, np.float32) if hv.value else None
+    mask = make(shape, np.uint8) if hm.value else None
+    _fits_check(L.dgpu_fits_read(p, ptr(data), ptr(var), ptr(mask)))
+    return {"data": data, "variance": var, "mask": mask}
+
+
+def write_fits(path: str, data, variance=None, mask=None, overwrite: bool = False) -> None:
+    """Write data plus optional variance / mask layers to a FITS file
+    (src/bindings.cpp:147-166); raises if the file exists unless overwrite=True."""
+    d = np.ascontiguousarray(data, dtype=np.float32)
+    if d.ndim != 2:
+        raise TypeError(f"data: expected a 2-D float32 array, got shape {d.shape}")
+    h, w = d.shape
+    v = None if variance is None else np.ascontiguousarray(variance, dtype=np.float32)
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    if v is not None and v.shape != d.shape:
+        raise RuntimeError("variance shape does not match data")
+    if m is not None and m.shape != d.shape:
+        raise RuntimeError("mask shape does not match data")
+    _fits_check(_lib.lib().dgpu_fits_write(str(path).encode(), ctypes.c_int64(w), ctypes.c_int64(h), ptr(d), ptr(v),
+                                           ptr(m), int(bool(overwrite))))
+
+
 def weighted_mean(data, variance, mask) -> float:
     """Inverse-variance weighted mean over unmasked pixels."""
     d = np.ascontiguousarray(data, np.float32)

@@ -15,9 +15,14 @@
 
 using namespace dgpu;
 
-namespace {
+namespace dgpu {
+std::string& free_error() {
+  thread_local std::string e;  // errors of context-free entry points
+  return e;
+}
+}  // namespace dgpu
 
-thread_local std::string g_free_error;  // errors of context-free entry points
+namespace {
 
 template <class F>
 int guarded(dgpu_context* ctx, F&& f) {
@@ -29,11 +34,11 @@ int guarded(dgpu_context* ctx, F&& f) {
     return DGPU_OK;
   } catch (const Failure& e) {
     if (c) c->last_error = e.what();
-    g_free_error = e.what();
+    dgpu::free_error() = e.what();
     return e.code;
   } catch (const std::exception& e) {
     if (c) c->last_error = e.what();
-    g_free_error = e.what();
+    dgpu::free_error() = e.what();
     return DGPU_ERR_RUNTIME;
   }
 }
@@ -44,10 +49,10 @@ int guarded_free(F&& f) {
     f();
     return DGPU_OK;
   } catch (const Failure& e) {
-    g_free_error = e.what();
+    dgpu::free_error() = e.what();
     return e.code;
   } catch (const std::exception& e) {
-    g_free_error = e.what();
+    dgpu::free_error() = e.what();
     return DGPU_ERR_RUNTIME;
   }
 }
@@ -84,7 +89,7 @@ int dgpu_device_count(int* count) {
   const cudaError_t e = cudaGetDeviceCount(&n);
   if (e != cudaSuccess) {
     *count = 0;
-    g_free_error = cudaGetErrorString(e);
+    dgpu::free_error() = cudaGetErrorString(e);
     return DGPU_ERR_NO_DEVICE;
   }
   *count = n;
@@ -138,7 +143,7 @@ int dgpu_synchronize(dgpu_context* ctx) {
 
 const char* dgpu_last_error(const dgpu_context* ctx) {
   if (ctx) return reinterpret_cast<const Context*>(ctx)->last_error.c_str();
-  return g_free_error.c_str();
+  return dgpu::free_error().c_str();
 }
 
 int dgpu_set_timing(dgpu_context* ctx, int on) {

@@ -25,6 +25,8 @@ struct Failure : std::runtime_error {
 };
 
 [[noreturn]] void fail(int code, const std::string& msg);
+// Last error of the calling thread's context-free entry points (dgpu_last_error(NULL)).
+std::string& free_error();
 void check_cuda(cudaError_t e, const char* what);
 // Host -> device copy on `s`. A pageable source of up to 1 MiB goes in pieces
 // of at most 32 KiB: such pieces are not queued behind large transfers of

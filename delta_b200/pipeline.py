@@ -458,6 +458,49 @@ class Subtractor:
         result.elapsed = time.perf_counter() - start
         return result
 
+    def subtract_files(self, pairs, outputs=None, *, max_in_flight: int | None = None, overwrite: bool = False,
+                       **call) -> list[DiffResult]:
+        """Subtract frame pairs stored as FITS files (an extension: the batched form
+        of the reference CLI's read -> subtract -> write, python/delta/cli.py). Each
+        item of `pairs` is (science_path, reference_path); the data, VARIANCE and
+        MASK layers of each file are its inputs. With `outputs` (one path per pair)
+        the difference, variance and mask are written as the reference's
+        write_fits lays them out. Every frame is read, subtracted and written by
+        its own worker (up to `max_in_flight`, default up to 4), so one frame's
+        file I/O overlaps the others' compute; with a device the layers are read
+        straight into pinned host memory. Results come back in input order."""
+        items = [tuple(p) for p in pairs]
+        outs = list(outputs) if outputs is not None else [None] * len(items)
+        if len(outs) != len(items):
+            raise ValueError("outputs must give one path per pair")
+        use_device = self._use_device()
+        alloc = None
+        if use_device:
+            import torch
+
+            def alloc(shape, dtype):
+                return torch.empty(shape, dtype=torch.from_numpy(np.zeros(1, dtype)).dtype, pin_memory=True).numpy()
+
+        def one(sci_path, ref_path, out_path):
+            sci = _core.read_fits(str(sci_path), alloc=alloc)
+            ref = _core.read_fits(str(ref_path), alloc=alloc)
+            result = self.subtract(sci["data"], ref["data"], science_var=sci["variance"],
+                                   reference_var=ref["variance"], science_mask=sci["mask"],
+                                   reference_mask=ref["mask"], **call)
+            if out_path is not None:
+                _core.write_fits(str(out_path), result.difference, result.variance, result.mask, overwrite=overwrite)
+            return result
+
+        if not items:
+            return []
+        if not use_device:
+            return [one(s, r, o) for (s, r), o in zip(items, outs, strict=True)]
+        from . import _device
+
+        ex = _device.runner(max_in_flight or min(len(items), 4))
+        futs = [ex.submit(_device.on_own_stream, one, s, r, o) for (s, r), o in zip(items, outs, strict=True)]
+        return [f.result() for f in futs]
+
     def apply_batch(self, solution: KernelSolution, frames, *, max_in_flight: int | None = None) -> list[DiffResult]:
         """Apply one frozen solution to several frame pairs concurrently (an
         extension: the reference applies a solution one frame at a time, through
@@ -501,6 +544,16 @@ def apply(solution: KernelSolution, science, reference, **kwargs) -> DiffResult:
     config = {k: v for k, v in kwargs.items() if k in _CONFIG_KEYS}
     call = {k: v for k, v in kwargs.items() if k not in _CONFIG_KEYS}
     return Subtractor(**config).apply(solution, science, reference, **call)
+
+
+def subtract_files(pairs, outputs=None, *, max_in_flight: int | None = None, overwrite: bool = False,
+                   **kwargs) -> list[DiffResult]:
+    """Configure a Subtractor from the config keywords and subtract FITS frame
+    pairs (extension; see Subtractor.subtract_files)."""
+    config = {k: v for k, v in kwargs.items() if k in _CONFIG_KEYS}
+    call = {k: v for k, v in kwargs.items() if k not in _CONFIG_KEYS}
+    return Subtractor(**config).subtract_files(pairs, outputs, max_in_flight=max_in_flight, overwrite=overwrite,
+                                               **call)
 
 
 def apply_batch(solution: KernelSolution, frames, *, max_in_flight: int | None = None, **kwargs) -> list[DiffResult]:

@@ -148,6 +148,22 @@ int dgpu_negate(dgpu_context* ctx, int mem, float* data, int64_t n);
  * DGPU_ERR_INVALID when host_dst is not mapped pinned host memory or
  * device_src is not device memory. */
 int dgpu_copy_to_host(dgpu_context* ctx, void* host_dst, const void* device_src, int64_t bytes);
+/* ---- FITS image layers ------------------------------------------------------------ */
+/* read_fits, src/bindings.cpp:128-145 -> delta::io::read_image, src/io.cpp:79-130.
+ * Host only (no device, no context). dgpu_fits_probe gives the data layer's
+ * size and whether VARIANCE / MASK extensions exist; dgpu_fits_read fills
+ * caller buffers of width * height values (variance / mask may be NULL to
+ * skip a layer). The data layer is the primary image, or the DIFFERENCE
+ * extension when the primary holds no 2-D image. Any BITPIX is converted with
+ * BSCALE / BZERO; tile-compressed HDUs are refused (DGPU_ERR_RUNTIME). Errors
+ * read back with dgpu_last_error(NULL). */
+int dgpu_fits_probe(const char* path, int64_t* width, int64_t* height, int* has_variance, int* has_mask);
+int dgpu_fits_read(const char* path, float* data, float* variance, uint8_t* mask);
+/* write_fits, src/bindings.cpp:147-166 -> delta::io::write_image, src/io.cpp:132-178:
+ * a float32 primary image, then VARIANCE (float32) and MASK (byte) image
+ * extensions when given. Fails if the file exists unless overwrite != 0. */
+int dgpu_fits_write(const char* path, int64_t width, int64_t height, const float* data, const float* variance,
+                    const uint8_t* mask, int overwrite);
 /* photometric_scale_at, src/bindings.cpp:711-719 -> src/fit.cpp:532-544. out: m. */
 int dgpu_photometric_scale_at(const double* knots, int n_knots, const double* theta,
                               int64_t n_theta, const double* component_sums, int nc,

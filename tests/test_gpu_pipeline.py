@@ -391,3 +391,33 @@ def test_mixed_pipeline_close_to_fp64_on_uneven_frames(spec_index):
     dd = np.abs(a.difference.astype(np.float64) - b.difference)[pos] / np.sqrt(b.variance[pos].astype(np.float64))
     assert np.max(dd) < 1e-3, np.max(dd)
     assert len(a.source_catalog) == len(b.source_catalog)
+
+
+def test_subtract_files_reads_subtracts_and_writes(tmp_path):
+    """The FITS batch path: pairs read into pinned memory by their workers,
+    subtracted, and written in the reference's write_fits layout; each result
+    bit-identical to subtract() on the arrays read back from the files."""
+    ps = [validation.synthetic_pair(384, 320, 200, s, mask_fraction=0.005) for s in (41, 42)]
+    kw = dict(n_max=4, n_knots=3, stamp_radius=12, cv_folds=0, score=True, decorrelate=True, block=64,
+              saturation=ps[0].saturation)
+    pairs, outs = [], []
+    for i, p in enumerate(ps):
+        s_path, r_path = tmp_path / f"sci{i}.fits", tmp_path / f"ref{i}.fits"
+        _core.write_fits(str(s_path), p.science, p.science_var, p.science_mask)
+        _core.write_fits(str(r_path), p.reference, p.reference_var, p.reference_mask)
+        pairs.append((s_path, r_path))
+        outs.append(tmp_path / f"diff{i}.fits")
+    got = delta.subtract_files(pairs, outs, max_in_flight=2, **kw)
+    assert len(got) == 2
+    for (s_path, r_path), o, r in zip(pairs, outs, got, strict=True):
+        sci, ref = _core.read_fits(str(s_path)), _core.read_fits(str(r_path))
+        one = delta.subtract(sci["data"], ref["data"], science_var=sci["variance"], reference_var=ref["variance"],
+                             science_mask=sci["mask"], reference_mask=ref["mask"], **kw)
+        for name in ("difference", "variance", "mask", "score"):
+            np.testing.assert_array_equal(getattr(r, name), getattr(one, name), err_msg=name)
+        back = _core.read_fits(str(o))
+        np.testing.assert_array_equal(back["data"], r.difference)
+        np.testing.assert_array_equal(back["variance"], r.variance)
+        np.testing.assert_array_equal(back["mask"], r.mask)
+    with pytest.raises(ValueError):
+        delta.subtract_files(pairs, outs[:1], **kw)
