@@ -139,7 +139,7 @@ def test_score_catalog_decorrelate_and_solution_roundtrip(tmp_path):
 
 @pytest.mark.parametrize("cv_folds", [0, 5])
 def test_pipeline_stages_match_oracle_chain(cv_folds):
-    """Stage-by-stage: the device pipeline on one C1-like frame vs the oracle
+    """Stage-by-stage: the device pipeline on one 384x384 frame (n_max 4, radius 10, 3x3 knots) vs the oracle
     fed the same stamps (fit -> subtract -> score -> catalog)."""
     p = validation.synthetic_pair(384, 384, 220, 7, mask_fraction=0.005)
     kw = dict(n_max=4, radius=10, n_knots=3, stamp_radius=12, cv_folds=cv_folds, score=True, decorrelate=False,
