@@ -72,15 +72,26 @@ class DiffResult:
         return {**self.solution.header_cards(), **self.config, **environment_cards(), "DLTELAP": self.elapsed}
 
     def write(self, path: str, overwrite: bool = False, *, compress: bool = True, extra_cards=None) -> None:
-        """Multi-extension FITS with provenance (needs astropy)."""
-        from astropy.io import fits  # optional dependency
-
+        """Multi-extension FITS with provenance (python/delta/pipeline.py:150-194;
+        astropy, as in the reference). Without astropy the uncompressed layout
+        (compress=False) is written natively with the same HDUs; the tile-
+        compressed layout still needs astropy."""
         cards = self.header_cards()
         if self.variance_scale is not None:
             cards["DLTVSCL"] = self.variance_scale
         if extra_cards:
             cards.update(extra_cards)
         layers = [("VARIANCE", self.variance), ("MASK", self.mask), ("SCORE", self.score)]
+        try:
+            from astropy.io import fits  # optional dependency
+        except ImportError:
+            if compress:
+                raise ImportError("DiffResult.write(compress=True) needs astropy; compress=False is written "
+                                  "without it") from None
+            from ._fits_products import write_products
+
+            write_products(str(path), self.difference, layers, self.source_catalog, cards, overwrite=overwrite)
+            return
         if compress:
             primary = fits.PrimaryHDU()
             for k, v in cards.items():

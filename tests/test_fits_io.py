@@ -177,3 +177,72 @@ def test_pinned_style_allocator(tmp_path):
     got = _core.read_fits(path, alloc=alloc)
     assert seen == [((4, 5), np.dtype(np.float32)), ((4, 5), np.dtype(np.float32))]
     np.testing.assert_array_equal(got["variance"], data + 1)
+
+
+def _solution():
+    from delta_b200.solution import KernelSolution
+
+    return KernelSolution(beta=1.25, n_max=2, radius=4, knots=np.zeros((9, 2)), theta=np.ones(63), n_components=6,
+                          n_spatial=9, lam=1e-6, gcv=0.5, effective_dof=12.5, rss=3.0, component_sums=np.ones(6),
+                          direction="reference", shape=(3, 4), reduced_chi2=1.01, n_stamps_used=10,
+                          n_stamps_rejected=2)
+
+
+def test_diffresult_write_uncompressed_without_astropy(tmp_path):
+    """DiffResult.write(compress=False) without astropy: the reference's
+    uncompressed layout (difference + provenance cards in the primary, VARIANCE,
+    MASK, SCORE images, CATALOG table), checked by the independent parser."""
+    try:
+        import astropy  # noqa: F401
+    except ImportError:
+        pass
+    else:
+        pytest.skip("astropy present: DiffResult.write goes through it, as in the reference")
+    from delta_b200.catalog import CATALOG_DTYPE
+    from delta_b200.pipeline import DiffResult
+
+    rng = np.random.default_rng(3)
+    d = rng.normal(size=(3, 4)).astype(np.float32)
+    cat = np.zeros(2, dtype=CATALOG_DTYPE)
+    cat["x"], cat["peak_x"], cat["quality"] = [1.5, 2.25], [1, 2], [0, 3]
+    cat["is_dipole"] = [False, True]
+    res = DiffResult(difference=d, variance=d * d, mask=np.eye(3, 4, dtype=np.uint8), score=d * 2,
+                     solution=_solution(), source_catalog=cat, config={"DLTPREC": "mixed"}, elapsed=0.25)
+    path = tmp_path / "prod.fits"
+    res.write(str(path), compress=False)
+    with pytest.raises(OSError):
+        res.write(str(path), compress=False)
+    res.write(str(path), compress=False, overwrite=True, extra_cards={"DLTNOTE": "x"})
+    with pytest.raises(ImportError, match="compress"):
+        res.write(str(path), overwrite=True)
+
+    raw = path.read_bytes()
+    pos, hdus = 0, []
+    while pos < len(raw):
+        cards = []
+        while True:
+            block = raw[pos : pos + 2880]
+            pos += 2880
+            cs = [block[i : i + 80].decode("ascii") for i in range(0, 2880, 80)]
+            cards += cs
+            if any(c.startswith("END ") for c in cs):
+                break
+        kw = {c[:8].strip(): c[10:].split("/")[0].strip().strip("'").strip() for c in cards if c[8:10] == "= "}
+        n = abs(int(kw["BITPIX"])) // 8 * int(kw["NAXIS1"]) * int(kw["NAXIS2"])
+        hdus.append((kw, raw[pos : pos + n]))
+        pos += n + (-n % 2880)
+    assert [kw.get("EXTNAME") for kw, _ in hdus] == [None, "VARIANCE", "MASK", "SCORE", "CATALOG"]
+    kw0, d0 = hdus[0]
+    assert d0 == d.astype(">f4").tobytes()
+    assert kw0["DLTBETA"] == "1.25" and kw0["DLTCONV"] == "reference" and kw0["DLTNOTE"] == "x"
+    assert kw0["DLTPREC"] == "mixed" and kw0["DLTNSTU"] == "10" and kw0["DLTELAP"] == "0.25"
+    np.testing.assert_array_equal(_core.read_fits(str(path))["data"], d)
+    kwt, rows = hdus[4]
+    assert kwt["XTENSION"] == "BINTABLE" and int(kwt["TFIELDS"]) == len(CATALOG_DTYPE.names)
+    names = [kwt[f"TTYPE{i}"] for i in range(1, len(CATALOG_DTYPE.names) + 1)]
+    assert names == list(CATALOG_DTYPE.names)
+    assert kwt["TFORM1"] == "D" and kwt["TFORM3"] == "J"
+    be = np.dtype([("x", ">f8"), ("y", ">f8"), ("peak_x", ">i4")])
+    first = np.frombuffer(rows, dtype=np.uint8).reshape(2, -1)[:, : be.itemsize].copy().view(be).ravel()
+    np.testing.assert_array_equal(first["x"], cat["x"])
+    np.testing.assert_array_equal(first["peak_x"], cat["peak_x"])
