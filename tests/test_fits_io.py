@@ -246,3 +246,20 @@ def test_diffresult_write_uncompressed_without_astropy(tmp_path):
     first = np.frombuffer(rows, dtype=np.uint8).reshape(2, -1)[:, : be.itemsize].copy().view(be).ravel()
     np.testing.assert_array_equal(first["x"], cat["x"])
     np.testing.assert_array_equal(first["peak_x"], cat["peak_x"])
+
+
+def test_product_header_cards_follow_the_fixed_format():
+    from delta_b200._fits_products import card
+
+    c = card("DLTLAM", 1e-06, "lambda")
+    assert len(c) == 80 and c[:10] == "DLTLAM  = " and c[10:30].strip() == "1E-06" and c[30:33] == " / "
+    assert card("DLTDECOR", True)[29] == "T" and card("DLTNMAX", 6)[10:30] == f"{6:>20}"
+    s = card("DLTCONV", "it's")
+    assert s[10] == "'" and "'it''s" in s
+    assert card("END") == "END".ljust(80)
+    with pytest.raises(ValueError):
+        card("TOOLONGKEY", 1)
+    with pytest.raises(ValueError):
+        card("DLTCHI2", float("nan"))
+    with pytest.raises(ValueError):
+        card("DLTNOTE", "x" * 69)
