@@ -263,3 +263,11 @@ def test_product_header_cards_follow_the_fixed_format():
         card("DLTCHI2", float("nan"))
     with pytest.raises(ValueError):
         card("DLTNOTE", "x" * 69)
+
+
+def test_subtract_files_validates_before_any_work(tmp_path):
+    import delta_b200 as delta
+
+    with pytest.raises(ValueError, match="one path per pair"):
+        delta.subtract_files([("a.fits", "b.fits")], [], device_resident=False)
+    assert delta.subtract_files([], device_resident=False) == []
