@@ -450,7 +450,7 @@ def read_fits(path: str, *, alloc=None) -> dict:
     data = make(shape, np.float32)
     var = make(shape, np.float32) if hv.value else None
     mask = make(shape, np.uint8) if hm.value else None
-    _fits_check(L.dgpu_fits_read(p, ptr(data), ptr(var), ptr(mask)))
+    _fits_check(L.dgpu_fits_read(p, w, h, ptr(data), ptr(var), ptr(mask)))
     return {"data": data, "variance": var, "mask": mask}
 
 

@@ -161,13 +161,26 @@ std::vector<Hdu> scan(std::FILE* f, const std::string& path) {
     const int64_t bytes_per = std::abs(h.bitpix) / 8;
     if (bytes_per != 1 && bytes_per != 2 && bytes_per != 4 && bytes_per != 8)
       fail(DGPU_ERR_RUNTIME, "FITS: unsupported BITPIX in " + path);
-    int64_t nax = 1;
-    for (int64_t a : h.naxes) nax *= a;
-    if (h.naxes.empty()) nax = 0;
+    // Sizes from the header are untrusted: negative axes or counts would move
+    // the next HDU's offset backwards (re-parsing earlier headers forever), and
+    // large ones could overflow the byte count. Both are refused, as CFITSIO does.
+    if (h.pcount < 0) fail(DGPU_ERR_RUNTIME, "FITS: negative PCOUNT in " + path);
+    if (h.gcount < 1) fail(DGPU_ERR_RUNTIME, "FITS: GCOUNT below 1 in " + path);
+    constexpr int64_t kMaxBytes = int64_t(1) << 60;
+    int64_t nax = h.naxes.empty() ? 0 : 1;
+    for (int64_t a : h.naxes) {
+      if (a < 0) fail(DGPU_ERR_RUNTIME, "FITS: negative NAXISn in " + path);
+      if (a > 0 && nax > kMaxBytes / a) fail(DGPU_ERR_RUNTIME, "FITS: data size overflows in " + path);
+      nax *= a;
+    }
+    if (h.pcount > kMaxBytes - nax || (h.pcount + nax) > kMaxBytes / (bytes_per * h.gcount))
+      fail(DGPU_ERR_RUNTIME, "FITS: data size overflows in " + path);
     h.data_offset = hpos;
     h.data_bytes = bytes_per * h.gcount * (h.pcount + nax);
     hdus.push_back(h);
-    pos = hpos + (h.data_bytes + kRecord - 1) / kRecord * kRecord;
+    const int64_t next = hpos + (h.data_bytes + kRecord - 1) / kRecord * kRecord;
+    if (next <= pos) fail(DGPU_ERR_RUNTIME, "FITS: HDU layout does not advance in " + path);
+    pos = next;
   }
   if (hdus.empty()) fail(DGPU_ERR_RUNTIME, "FITS: " + path + " holds no HDU");
   return hdus;
@@ -367,7 +380,7 @@ int dgpu_fits_probe(const char* path, int64_t* width, int64_t* height, int* has_
   });
 }
 
-int dgpu_fits_read(const char* path, float* data, float* variance, uint8_t* mask) {
+int dgpu_fits_read(const char* path, int64_t width, int64_t height, float* data, float* variance, uint8_t* mask) {
   return fits_guarded([&] {
     if (!path || !data) fail(DGPU_ERR_INVALID, "fits_read: missing argument");
     File file;
@@ -375,6 +388,13 @@ int dgpu_fits_read(const char* path, float* data, float* variance, uint8_t* mask
     if (!file.f) fail(DGPU_ERR_RUNTIME, std::string("read_fits: cannot open ") + path);
     const std::vector<Hdu> hdus = scan(file.f, path);
     const Hdu& d = data_hdu(hdus, path);
+    // The caller's buffers hold width x height values each; a file whose data
+    // layer is any other shape (changed since the probe, or a wrong caller
+    // size) is refused before anything is written.
+    if (d.naxes[0] != width || d.naxes[1] != height)
+      fail(DGPU_ERR_INVALID, "read_fits: " + std::string(path) + " holds a " + std::to_string(d.naxes[0]) + " x " +
+                                 std::to_string(d.naxes[1]) + " image, the buffers are " + std::to_string(width) +
+                                 " x " + std::to_string(height));
     const int64_t n = d.naxes[0] * d.naxes[1];
     read_pixels(file.f, d, n, "the data layer",
                 [&](int64_t i, double v, bool) { data[i] = static_cast<float>(v); });

@@ -13,7 +13,6 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
-#include <mutex>
 #include <string>
 
 #include "dev_common.cuh"
@@ -696,7 +695,6 @@ void run_catalog_stamps(Context& c, int w, int h, const float* sci, const uint8_
 namespace {
 
 constexpr int64_t kNoAllocMaxSamples = int64_t(1) << 19;
-constexpr int kNoAllocMaxDevices = 64;
 
 struct NoAllocBackground {
   Sel sel;          // count / rank / prefix / histogram: cleared by every call
@@ -706,23 +704,15 @@ struct NoAllocBackground {
 
 static __device__ __align__(256) NoAllocBackground g_noalloc_background;
 
-std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
-
-// Device address of the array on the current device, resolved once per device.
+// Device address of the array on the current device. Resolved on every call
+// (a cheap lookup, no allocation) rather than cached: after a device reset the
+// runtime reloads the module and the array may sit at a new address.
 NoAllocBackground* noalloc_background_scratch() {
-  int dev = 0;
-  DGPU_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kNoAllocMaxDevices) fail(DGPU_ERR_INVALID, "estimate_background_noalloc: device index out of range");
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (g_noalloc_ptr[dev] == nullptr) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_background);
-    if (e != cudaSuccess)
-      fail(DGPU_ERR_CUDA, std::string("estimate_background_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    g_noalloc_ptr[dev] = p;
-  }
-  return static_cast<NoAllocBackground*>(g_noalloc_ptr[dev]);
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_background);
+  if (e != cudaSuccess)
+    fail(DGPU_ERR_CUDA, std::string("estimate_background_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  return static_cast<NoAllocBackground*>(p);
 }
 
 }  // namespace

@@ -153,12 +153,14 @@ int dgpu_copy_to_host(dgpu_context* ctx, void* host_dst, const void* device_src,
  * Host only (no device, no context). dgpu_fits_probe gives the data layer's
  * size and whether VARIANCE / MASK extensions exist; dgpu_fits_read fills
  * caller buffers of width * height values (variance / mask may be NULL to
- * skip a layer). The data layer is the primary image, or the DIFFERENCE
+ * skip a layer), and fails with DGPU_ERR_INVALID without writing when the
+ * file's data layer is not width x height. The data layer is the primary image, or the DIFFERENCE
  * extension when the primary holds no 2-D image. Any BITPIX is converted with
  * BSCALE / BZERO; tile-compressed HDUs are refused (DGPU_ERR_RUNTIME). Errors
  * read back with dgpu_last_error(NULL). */
 int dgpu_fits_probe(const char* path, int64_t* width, int64_t* height, int* has_variance, int* has_mask);
-int dgpu_fits_read(const char* path, float* data, float* variance, uint8_t* mask);
+int dgpu_fits_read(const char* path, int64_t width, int64_t height, float* data, float* variance,
+                   uint8_t* mask);
 /* write_fits, src/bindings.cpp:147-166 -> delta::io::write_image, src/io.cpp:132-178:
  * a float32 primary image, then VARIANCE (float32) and MASK (byte) image
  * extensions when given. Fails if the file exists unless overwrite != 0. */
@@ -272,9 +274,11 @@ typedef struct {
  * `stream`. Its scratch is one fixed array of 2 MiB + 1 KiB per device inside
  * the library (it holds the at most 2^19 sample keys of any frame below 2^31
  * pixels); the select state in it is cleared at the start of every call.
- * Limits: frames up to 2^31 - 1 pixels (larger -> DGPU_ERR_INVALID). The first
- * call on a device resolves that array's address (cudaGetSymbolAddress); make
- * that first call before any stream capture. Calls that overlap in time on the
+ * Limits: frames up to 2^31 - 1 pixels (larger -> DGPU_ERR_INVALID). Every
+ * call looks up that array's address on the current device
+ * (cudaGetSymbolAddress, which allocates nothing); the first call on a device
+ * may also load the library's device code, so make it before any stream
+ * capture. Calls that overlap in time on the
  * same device (other streams or threads) share the array and race: serialise
  * them. Results equal dgpu_estimate_background's (median, 1.4826 * MAD).
  * Errors: status code, text from dgpu_last_error(NULL). */

@@ -164,6 +164,39 @@ def test_read_errors(tmp_path):
         _core.read_fits(str(notfits))
 
 
+@pytest.mark.parametrize("card,value,match", [("NAXIS1", -5760, "negative NAXISn"), ("PCOUNT", -2880, "PCOUNT"),
+                                              ("GCOUNT", 0, "GCOUNT"), ("NAXIS2", 2**62, "overflows")])
+def test_hostile_sizes_are_refused_not_looped(tmp_path, card, value, match):
+    """Header sizes are untrusted: a negative axis or count would move the next
+    HDU offset backwards onto an earlier header (parsed again forever), and a
+    huge one would overflow the byte count. Each must fail at once."""
+    a = np.zeros((2, 3), np.float32)
+    ext_cards = [_card("XTENSION", "IMAGE"), _card("BITPIX", -32), _card("NAXIS", 2), _card("NAXIS1", 3),
+                 _card("NAXIS2", 2), _card("PCOUNT", 0), _card("GCOUNT", 1), _card("EXTNAME", "VARIANCE")]
+    ext_cards = [_card(card, value) if c.startswith(card.ljust(8)) else c for c in ext_cards]
+    path = tmp_path / "hostile.fits"
+    path.write_bytes(_image(True, -32, a.astype(">f4")) + _hdu(ext_cards, bytes(24)))
+    with pytest.raises(RuntimeError, match=match):
+        _core.read_fits(str(path))
+
+
+def test_read_refuses_a_data_layer_of_another_shape(tmp_path):
+    """dgpu_fits_read takes the caller's buffer shape and writes nothing when
+    the file's data layer differs from it (e.g. the file changed after the probe)."""
+    import ctypes
+
+    from delta_b200 import _lib
+
+    path = tmp_path / "a.fits"
+    _core.write_fits(str(path), np.ones((4, 5), np.float32))
+    buf = np.zeros((3, 5), np.float32)
+    rc = _lib.lib().dgpu_fits_read(str(path).encode(), ctypes.c_int64(5), ctypes.c_int64(3),
+                                   buf.ctypes.data_as(ctypes.c_void_p), None, None)
+    assert rc == _lib.DGPU_ERR_INVALID
+    assert b"4" in _lib.lib().dgpu_last_error(None)
+    assert not buf.any()
+
+
 def test_pinned_style_allocator(tmp_path):
     data = np.arange(20, dtype=np.float32).reshape(4, 5)
     path = str(tmp_path / "a.fits")

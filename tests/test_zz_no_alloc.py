@@ -37,11 +37,21 @@ def test_noalloc_background_matches_context_entry_point(shape, with_mask):
     torch.cuda.synchronize()
     L = _lib.lib()
     h, w = shape
+    args = (L, ctypes.c_void_p(d.data_ptr()), None if m is None else ctypes.c_void_p(m.data_ptr()), w, h,
+            torch.cuda.current_stream().cuda_stream)
+    # Warm-up: the first call on a device may load the library's device code,
+    # which can take device memory once; it is not the call under test.
+    rc, _, _ = _call(*args)
+    assert rc == _lib.DGPU_OK, L.dgpu_last_error(None)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()  # cudaMemGetInfo: device-wide, not torch's cache
     for _ in range(2):  # two calls in a row: the fixed scratch is reset by each call
-        rc, med, sig = _call(L, ctypes.c_void_p(d.data_ptr()), None if m is None else ctypes.c_void_p(m.data_ptr()),
-                             w, h, torch.cuda.current_stream().cuda_stream)
+        rc, med, sig = _call(*args)
         assert rc == _lib.DGPU_OK, L.dgpu_last_error(None)
         np.testing.assert_allclose([med, sig], want, rtol=1e-12, atol=0)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, f"device free memory moved by {free0 - free1} bytes across allocation-free calls"
 
 
 def test_noalloc_background_rejects_bad_arguments():
