@@ -437,26 +437,55 @@ def error_vs_fp64(out, ref) -> dict:
             "catalog_rows": [len(cat), len(cat64)]}
 
 
-def cpu_baseline(pair, size: int) -> dict:
-    """The CPU chain on one full frame of the workload (rank 0, N=1)."""
+def error_vs_oracle(out, want) -> dict:
+    """Errors of one GPU run's products against the oracle chain's on the same
+    frame: theta, the (whitened) difference in units of the local sigma, the
+    score, mask and CCL label equality (the reference's own CCL, compiled from
+    source, run on both scores)."""
+    from oracle import numpy_ref as nr
+    from oracle import refbuild
+
+    th, th0 = np.asarray(out["solution"].theta), np.asarray(want["fit"]["theta"])
+    d = out["difference"].double().cpu().numpy()
+    d0 = np.asarray(want["difference"], np.float64)
+    v0 = np.asarray(want["variance"], np.float64)
+    ok = (v0 > 0) & np.isfinite(d) & np.isfinite(d0)
+    z = (d - d0)[ok] / np.sqrt(v0[ok])
+    mask = out["mask"].cpu().numpy()
+    s = out["score"].float().cpu().numpy()
+    s0 = np.asarray(want["score"], np.float32)
+    fin = np.isfinite(s) & np.isfinite(s0)
+    lab = refbuild.label_components(nr.seed_mask(s, 5.0, +1, mask, True))[0]
+    lab0 = refbuild.label_components(nr.seed_mask(s0, 5.0, +1, want["mask"], True))[0]
+    return {"theta_rel": float(np.linalg.norm(th - th0) / max(np.linalg.norm(th0), 1e-300)),
+            "lambda_equal": bool(out["solution"].lam == want["fit"]["lambda"]),
+            "diff_rms_sigma": float(np.sqrt(np.mean(z * z))) if z.size else None,
+            "diff_max_sigma": float(np.max(np.abs(z))) if z.size else None,
+            "score_max_abs": float(np.max(np.abs(s.astype(np.float64) - s0)[fin])) if fin.any() else None,
+            "mask_equal": bool(np.array_equal(mask, want["mask"])),
+            "labels_equal": bool(np.array_equal(lab, lab0)), "components": int(lab0.max()),
+            "catalog_rows": [len(out["catalog"]), len(want["catalog"]["x"])]}
+
+
+def cpu_baseline(pair, size: int) -> tuple[dict, dict | None]:
+    """The CPU chain on one full frame of the workload (rank 0, N=1); returns
+    the baseline entry and the chain's products (the oracle for error_vs_oracle)."""
     from oracle import chain
 
     if not chain.available():
         return {"value": None, "unit": UNIT, "cores": None, "kind": "port",
-                "unavailable": "oracle/_ref (the reference sources compiled by oracle/Makefile) is not built"}
+                "unavailable": "oracle/_ref (the reference sources compiled by oracle/Makefile) is not built"}, None
     kw = subtract_kwargs(pair)
     kw.pop("saturation")
     t0 = time.perf_counter()
     stages: dict = {}
-    chain.run(pair.science, pair.reference, pair.science_var, pair.reference_var, pair.science_mask,
-              pair.reference_mask, saturation=pair.saturation, timings=stages,
-              **{k: v for k, v in kw.items() if k not in ("precision",)})
+    want = chain.run(pair.science, pair.reference, pair.science_var, pair.reference_var, pair.science_mask,
+                     pair.reference_mask, saturation=pair.saturation, timings=stages,
+                     **{k: v for k, v in kw.items() if k not in ("precision",)})
     dt = time.perf_counter() - t0
     return {"value": size * size / 1e6 / dt, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-            "sample": f"1 full {size}x{size} frame of the workload, one pass ({dt:.1f} s): the reference's "
-                      "detect/catalog/basis-convolve code compiled from source + C (OpenMP) restatements of "
-                      "subtract and the matched filter + NumPy FP64 restatements of the fit and decorrelation",
-            "stage_seconds": {k: round(v, 3) for k, v in stages.items()}}
+            "sample": f"1 full {size}x{size} frame of the workload, one pass ({dt:.1f} s): {chain.DESCRIPTION}",
+            "stage_seconds": {k: round(v, 3) for k, v in stages.items()}}, want
 
 
 # ---------------------------------------------------------------- arms ---------
@@ -471,12 +500,9 @@ def run_reference(args) -> int:
     if not chain.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref is not built (make -C oracle ref)"}))
         return 0
-    # Each step is a bounded sample: the full frame when the run fits in ~3 minutes, else a smaller frame.
+    # Each step is one full frame of the same workload as the GPU arm (about
+    # 7 s on 16 host cores), so both arms time the same configuration.
     size = args.size
-    per_step = 14.0 * (size / 4096.0) ** 2  # seconds per full frame on 8 host cores
-    while size > 1024 and per_step * (args.steps + args.warmup) > 180.0:
-        size //= 2
-        per_step /= 4.0
     pair = make_frame(size, args.seed)
     kw = {k: v for k, v in subtract_kwargs(pair).items() if k != "saturation"}
 
@@ -491,12 +517,12 @@ def run_reference(args) -> int:
         step()
     dt = time.perf_counter() - t0
     value = args.steps * size * size / 1e6 / dt
-    sample = (f"{size}x{size} frame of the workload per step" + ("" if size == args.size else
-              f" (the {args.size}^2 frame would not finish {args.steps + args.warmup} steps in minutes)"))
+    sample = f"one full {size}x{size} frame of the workload per step: {chain.DESCRIPTION}"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, **frame_config(args.size), "sample_size": size},
+            "config": {"workload": WORKLOAD, **frame_config(args.size), "precision": "fp64 (CPU)",
+                       "frames_per_rank": 1, "frames_in_flight": 1},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -581,8 +607,9 @@ def run_gpu(args) -> int:
 
     # errors of mixed and plain against the FP64 normal-equation path (outside the timing)
     out64 = _device.run(subs["fp64"], frame)
-    errors = {"mixed": error_vs_fp64(_device.run(subs["mixed"], frame), out64),
-              "plain": error_vs_fp64(_device.run(subs["fp32"], frame), out64)}
+    out_mixed = _device.run(subs["mixed"], frame)
+    out_plain = _device.run(subs["fp32"], frame)
+    errors = {"mixed": error_vs_fp64(out_mixed, out64), "plain": error_vs_fp64(out_plain, out64)}
 
     mpix = size * size / 1e6
     value = world * args.steps * B * mpix / (ms / 1e3)
@@ -611,9 +638,13 @@ def run_gpu(args) -> int:
                                        "peak_tfma_s": FP32_FMA_PEAK_TFMA, "frac": tfma / FP32_FMA_PEAK_TFMA,
                                        "fma_per_launch": fma,
                                        "note": "the kernel is FP32-issue-bound; HBM is not its limit"}
-        cpu = None
+        cpu, oracle_errors = None, None
         if world == 1 and not args.no_cpu_baseline:
-            cpu = cpu_baseline(pair, size)
+            cpu, want = cpu_baseline(pair, size)
+            if want is not None:
+                oracle_errors = {"fp64": error_vs_oracle(out64, want),
+                                 "mixed": error_vs_oracle(out_mixed, want),
+                                 "plain": error_vs_oracle(out_plain, want)}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -625,6 +656,7 @@ def run_gpu(args) -> int:
             "plain": {"value": world * args.steps * mpix / (ms_plain / 1e3), "ms_per_step": ms_plain / args.steps,
                       "precision": "fp32", "frames_in_flight": 1},
             "error_vs_fp64": errors,
+            "error_vs_oracle": oracle_errors,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": world * args.steps * B * mpix / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,

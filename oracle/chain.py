@@ -6,8 +6,9 @@ select stamps -> direction -> fit -> subtract -> sign -> [decorrelate] ->
 oracle:
 
   stamp selection  the reference's detect.cpp compiled from source (oracle/_ref)
-  kernel fit       numpy_ref.fit_kernel (FP64 restatement of src/fit.cpp, src/solve.cpp),
-                   B_n through the reference's convolve.cpp when oracle/_ref is built
+  kernel fit       numpy_ref.fit_kernel (FP64 restatement of src/fit.cpp's IRLS), each pass's
+                   GLS assembly and lambda-grid solves in C with OpenMP (oracle/csrc/oracle_fit.c,
+                   src/solve.cpp:70-262), B_n through the reference's convolve.cpp
   subtract         cref.subtract (C restatement of src/subtract.cpp, float semantics)
   decorrelate      numpy_ref.decorrelate (src/noise.cpp)
   PSF estimate     numpy_ref.estimate_psf (python/delta/pipeline.py:285-302)
@@ -28,6 +29,10 @@ import numpy as np
 
 from . import cref, refbuild
 from . import numpy_ref as nr
+
+DESCRIPTION = ("the reference's detect/catalog/basis-convolve code compiled from source + C (OpenMP) restatements "
+               "of subtract, the matched filter and the FP64 GLS assembly / lambda-grid solves of the fit + NumPy "
+               "FP64 restatements of the IRLS control and the decorrelation")
 
 
 def available() -> bool:
@@ -67,7 +72,7 @@ def run(science, reference, science_var, reference_var, science_mask, reference_
     fit = nr.fit_kernel(target, conv, knots, sel["x"], sel["y"], stamp_radius, beta, n_max, grid, radius=r,
                         clip_sigma=clip_sigma, clip_iterations=clip_iterations, min_stamps=min_stamps,
                         cv_folds=cv_folds, science_var=tvar, reference_var=cvar, science_mask=tmask,
-                        reference_mask=cmask, basis_convolve_fn=bconv)
+                        reference_mask=cmask, basis_convolve_fn=bconv, gcv_solver=cref.gls_gcv)
     t0 = mark("kernel solve", t0)
     sub = cref.subtract(target, conv, knots, fit["theta"], beta, n_max, r, saturation, tvar, cvar, tmask, cmask)
     diff = sub["difference"]

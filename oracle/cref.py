@@ -99,3 +99,69 @@ def matched_filter(image, psf, variance) -> np.ndarray:
     out = np.zeros((h, w), np.float32)
     lib().oc_matched_filter(ptr(img), ptr(var), w, h, ptr(psf), psf.shape[0], ptr(out))
     return out
+
+
+# ---------------------------------------------------------------------------
+# Penalised GLS in C (oracle/csrc/oracle_fit.c)
+# ---------------------------------------------------------------------------
+
+
+def assemble(design, target, weights, bn):
+    """M = Xs^T Xs, rhs, ywy (src/solve.cpp:70-145) by the OpenMP rank update."""
+    d = np.ascontiguousarray(design, np.float64)
+    b = np.ascontiguousarray(bn, np.float64)
+    t = np.ascontiguousarray(target, np.float64)
+    wt = np.ascontiguousarray(weights, np.float64)
+    n, k = d.shape
+    nc = b.shape[1]
+    if t.size != n or wt.size != n or b.shape[0] != n:
+        raise RuntimeError("solve_gls: row counts of design/target/weights/bn disagree")
+    p = (nc + 1) * k
+    m = np.zeros((p, p))
+    rhs = np.zeros(p)
+    ywy = ctypes.c_double()
+    rc = lib().of_assemble(ctypes.c_int64(n), k, nc, ptr(d), ptr(b), ptr(t), ptr(wt), ptr(m), ptr(rhs),
+                           ctypes.byref(ywy))
+    if rc:
+        raise MemoryError("of_assemble")
+    return m, rhs, ywy.value
+
+
+def solve_grid(s: nr.System, lambdas) -> list[dict]:
+    """solve_at (src/solve.cpp:147-193) at every lambda, lambdas in parallel."""
+    grid = np.ascontiguousarray(lambdas, np.float64)
+    p = s.p
+    f = np.ascontiguousarray(s.pen_half, np.float64)
+    nf = f.shape[1] if f.size else 0
+    theta = np.zeros((grid.size, p))
+    edf, rss, gcv = np.zeros(grid.size), np.zeros(grid.size), np.zeros(grid.size)
+    used = np.zeros(grid.size, np.int32)
+    rc = lib().of_solve_grid(p, ptr(np.ascontiguousarray(s.m, np.float64)), ptr(np.ascontiguousarray(s.p0)),
+                             ptr(np.ascontiguousarray(s.rhs, np.float64)), ctypes.c_double(s.ywy),
+                             ctypes.c_int64(s.n), ptr(f) if nf else None, nf, ptr(grid), grid.size, ptr(theta),
+                             ptr(edf), ptr(rss), ptr(gcv), ptr(used))
+    if rc:
+        raise MemoryError("of_solve_grid")
+    return [{"theta": theta[i], "lambda": float(grid[i]), "effective_dof": float(edf[i]), "rss": float(rss[i]),
+             "gcv": float(gcv[i]), "n_components": s.nc, "n_spatial": s.k, "used_ldlt": bool(used[i])}
+            for i in range(grid.size)]
+
+
+def gls_gcv(design, target, weights, bn, penalty, lambda_grid) -> dict:
+    """solve_gls_gcv_design (src/solve.cpp:227-262) with the C assembly and solves."""
+    m, rhs, ywy = assemble(design, target, weights, bn)
+    k = np.shape(design)[1]
+    nc = np.shape(bn)[1]
+    s = nr.System.from_parts(m, rhs, ywy, int(np.shape(design)[0]), nc, k, penalty)
+    res = solve_grid(s, lambda_grid)
+    return nr.pick_gcv(res, lambda_grid)
+
+
+def ldlt_solve(a, b) -> np.ndarray:
+    """Eigen-style pivoted LDL^T solve of a symmetric system (the LLT fallback)."""
+    a = np.array(a, np.float64, order="C", copy=True)
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros_like(b)
+    if lib().of_ldlt_solve(a.shape[0], ptr(a), ptr(b), ptr(x)):
+        raise MemoryError("of_ldlt_solve")
+    return x

@@ -14,6 +14,7 @@ import math
 import os
 
 import numpy as np
+import scipy.linalg
 
 MASK_GOOD = 0
 MASK_BAD = 1
@@ -596,6 +597,53 @@ class System:
         return s
 
 
+def ldlt_factor(a):
+    """Eigen 3.4's pivoted LDL^T (the reference's LLT fallback, src/solve.cpp:177-181).
+
+    Step k swaps the remaining diagonal entry of largest magnitude (first on
+    ties, read before that step's update) to position k, forms d_k and
+    column k of the unit lower factor by the left-looking update, and divides
+    the column by d_k only when d_k != 0. An all-zero diagonal stops at once
+    with identity transpositions. Returns (factor with L below and D on the
+    diagonal, transpositions)."""
+    a = np.array(a, np.float64, copy=True)
+    p = a.shape[0]
+    perm = np.arange(p)
+    for k in range(p):
+        diag = np.abs(np.diagonal(a)[k:])
+        piv = k + int(np.argmax(diag))
+        if k == 0 and diag[piv] == 0.0:
+            return a, np.arange(p)
+        perm[k] = piv
+        if piv != k:
+            a[[k, piv], :] = a[[piv, k], :]
+            a[:, [k, piv]] = a[:, [piv, k]]
+        temp = np.diagonal(a)[:k] * a[k, :k]
+        dk = a[k, k] - float(a[k, :k] @ temp)
+        a[k, k] = dk
+        col = a[k + 1 :, k] - a[k + 1 :, :k] @ temp
+        a[k + 1 :, k] = col / dk if dk != 0.0 else col
+    return a, perm
+
+
+def ldlt_solve(fac, perm, b):
+    """Solve with an ldlt_factor result; D enters by its pseudo-inverse
+    (1/d where |d| > the smallest normal double, else 0), as Eigen's solve."""
+    x = np.array(b, np.float64, copy=True)
+    p = fac.shape[0]
+    for k in range(p):
+        x[[k, perm[k]]] = x[[perm[k], k]]
+    low = np.tril(fac, -1) + np.eye(p)
+    x = scipy.linalg.solve_triangular(low, x, lower=True, unit_diagonal=True)
+    d = np.diagonal(fac)
+    inv = np.where(np.abs(d) > np.finfo(np.float64).tiny, 1.0 / np.where(d == 0.0, 1.0, d), 0.0)
+    x = (x.T * inv).T
+    x = scipy.linalg.solve_triangular(low.T, x, lower=False, unit_diagonal=True)
+    for k in range(p - 1, -1, -1):
+        x[[k, perm[k]]] = x[[perm[k], k]]
+    return x
+
+
 def solve_at(s: System, lam: float) -> dict:
     """LLT (LDLT fallback), theta, edf, rss, gcv.  src/solve.cpp:147-193."""
     a = s.m + lam * s.p0
@@ -609,8 +657,9 @@ def solve_at(s: System, lam: float) -> dict:
         else:
             edf = float(np.trace(np.linalg.solve(a, s.m)))
     except np.linalg.LinAlgError:
-        theta = np.linalg.lstsq(a, s.rhs, rcond=None)[0]
-        edf = float(np.trace(np.linalg.lstsq(a, s.m, rcond=None)[0]))
+        fac, perm = ldlt_factor(a)
+        theta = ldlt_solve(fac, perm, s.rhs)
+        edf = float(np.trace(ldlt_solve(fac, perm, s.m)))
     rss = s.ywy - 2.0 * float(theta @ s.rhs) + float(theta @ (s.m @ theta))
     rss = max(rss, 0.0)
     denom = s.n - edf
@@ -624,7 +673,12 @@ def solve_gls_gcv_system(s: System, lambda_grid) -> dict:
     grid = [float(v) for v in lambda_grid]
     if not grid:
         raise RuntimeError("solve_gls_gcv: lambda_grid is empty")
-    res = [solve_at(s, lam) for lam in grid]
+    return pick_gcv([solve_at(s, lam) for lam in grid], grid)
+
+
+def pick_gcv(res, lambda_grid) -> dict:
+    """First minimum of the GCV curve over the grid's solutions.  src/solve.cpp:240-262."""
+    grid = [float(v) for v in lambda_grid]
     curve = np.array([r["gcv"] for r in res])
     best_i = 0
     best = math.inf
@@ -850,37 +904,38 @@ def gather_stamps(science, reference, stamp_x, stamp_y, stamp_radius, b1d, n_max
         patch = sanitized_reference(reference[ey0 : ey1 + 1, ex0 : ex1 + 1],
                                     None if reference_mask is None else reference_mask[ey0 : ey1 + 1, ex0 : ex1 + 1], fill)
         bn = basis_convolve_fn(patch)
-        used = False
         sid = len(stamp_cx)
-        for y in range(y0, y1 + 1):
-            for x in range(x0, x1 + 1):
-                if science_mask is not None and science_mask[y, x] != 0:
-                    continue
-                if reference_mask is not None and reference_mask[y, x] != 0:
-                    continue
-                sv = science[y, x]
-                if not np.isfinite(sv):
-                    continue
-                vt = float(science_var[y, x]) if science_var is not None else 0.0
-                vc = float(reference_var[y, x]) if have_cvar else 0.0
-                if have_var and not (vt + vc > 0.0):
-                    continue
-                col = bn[:, y - ey0, x - ex0]
-                if not np.all(np.isfinite(col)):
-                    continue
-                rows["px"].append(float(x))
-                rows["py"].append(float(y))
-                rows["target"].append(float(sv))
-                rows["var_t"].append(vt)
-                rows["var_c"].append(vc)
-                rows["bn"].append(col.astype(np.float64))
-                rows["stamp"].append(sid)
-                used = True
+        # The stamp's pixels in raster order (y, then x), kept by the same tests
+        # as the reference's per-pixel loop.
+        ok = np.ones((y1 - y0 + 1, x1 - x0 + 1), bool)
+        if science_mask is not None:
+            ok &= science_mask[y0 : y1 + 1, x0 : x1 + 1] == 0
+        if reference_mask is not None:
+            ok &= reference_mask[y0 : y1 + 1, x0 : x1 + 1] == 0
+        sv = science[y0 : y1 + 1, x0 : x1 + 1]
+        ok &= np.isfinite(sv)
+        vt = (np.asarray(science_var[y0 : y1 + 1, x0 : x1 + 1], np.float64) if science_var is not None
+              else np.zeros(ok.shape))
+        vc = (np.asarray(reference_var[y0 : y1 + 1, x0 : x1 + 1], np.float64) if have_cvar else np.zeros(ok.shape))
+        if have_var:
+            ok &= (vt + vc) > 0.0
+        cols = bn[:, y0 - ey0 : y1 - ey0 + 1, x0 - ex0 : x1 - ex0 + 1]
+        ok &= np.all(np.isfinite(cols), axis=0)
+        yy, xx = np.nonzero(ok)
+        used = yy.size > 0
+        rows["px"].append((xx + x0).astype(np.float64))
+        rows["py"].append((yy + y0).astype(np.float64))
+        rows["target"].append(sv[yy, xx].astype(np.float64))
+        rows["var_t"].append(vt[yy, xx])
+        rows["var_c"].append(vc[yy, xx])
+        rows["bn"].append(cols[:, yy, xx].T.astype(np.float64))
+        rows["stamp"].append(np.full(yy.size, sid, np.int64))
         if used:
             stamp_cx.append(cx)
             stamp_cy.append(cy)
-    out = {k: np.asarray(v) for k, v in rows.items()}
-    out["bn"] = out["bn"].reshape(-1, nc) if len(rows["bn"]) else np.zeros((0, nc))
+    out = {k: (np.concatenate(v) if v else np.zeros(0)) for k, v in rows.items() if k != "bn"}
+    out["stamp"] = out["stamp"].astype(np.int64)
+    out["bn"] = np.concatenate(rows["bn"]).reshape(-1, nc) if rows["bn"] else np.zeros((0, nc))
     out["stamp_cx"] = np.asarray(stamp_cx, int)
     out["stamp_cy"] = np.asarray(stamp_cy, int)
     return out
@@ -889,8 +944,12 @@ def gather_stamps(science, reference, stamp_x, stamp_y, stamp_radius, b1d, n_max
 def fit_kernel(science, reference, knots, stamp_x, stamp_y, stamp_radius, beta, n_max, lambda_grid,
                radius=0, clip_sigma=4.0, clip_iterations=5, min_stamps=5, cv_folds=0,
                science_var=None, reference_var=None, science_mask=None, reference_mask=None,
-               basis_convolve_fn=None) -> dict:
-    """delta::fit_kernel restated.  src/fit.cpp:63-511."""
+               basis_convolve_fn=None, gcv_solver=None) -> dict:
+    """delta::fit_kernel restated.  src/fit.cpp:63-511.
+
+    ``gcv_solver(design, target, weights, bn, penalty, lambda_grid)`` replaces
+    the NumPy GCV solve of each IRLS pass (the timed chain passes the C
+    restatement, oracle.cref.gls_gcv)."""
     science = np.asarray(science, np.float32)
     reference = np.asarray(reference, np.float32)
     r = resolve_radius(beta, n_max, radius)
@@ -972,6 +1031,8 @@ def fit_kernel(science, reference, knots, stamp_x, stamp_y, stamp_radius, beta, 
                 gls = solve_gls_cv_design(des, tgt, wts, bn, tp.penalty, lambda_grid, grp, cv_folds, warm_start)
                 cv_exact_design_bytes = npix * (nc + 1) * k * 8
             warm_start = int(np.argmin(gls["gcv_curve"]))
+        elif gcv_solver is not None:
+            gls = gcv_solver(des, tgt, wts, bn, tp.penalty, lambda_grid)
         else:
             gls = solve_gls_gcv_system(System(des, tgt, wts, bn, tp.penalty), lambda_grid)
         c = gls["theta"].reshape(nc + 1, k).T

@@ -194,3 +194,67 @@ def test_reference_catalog_known_answers():
     m[18:23, 20] = 1
     cat = refbuild.build_catalog(s, s, mask=m, expected_fwhm=3.0)
     assert len(cat["x"]) == 2 and np.all(cat["mask_flags"] != 0)
+
+
+def _gls_problem(seed, n=4000, nc=6, knots_side=3, rank_deficient=False):
+    rng = np.random.default_rng(seed)
+    knots = nr.grid_knots(0, 0, 500, 400, knots_side, knots_side)
+    tp = nr.ThinPlate(knots)
+    pts = np.column_stack([rng.uniform(0, 500, n), rng.uniform(0, 400, n)])
+    des = tp.design(pts)
+    bn = rng.normal(size=(n, nc))
+    if rank_deficient:
+        bn[:, 3] = bn[:, 1]  # two identical components: M is singular at lambda = 0
+    target = bn @ rng.normal(size=nc) + 0.1 * rng.normal(size=n)
+    weights = rng.uniform(0.5, 2.0, n)
+    return des, target, weights, bn, tp.penalty
+
+
+def test_c_gls_assembly_and_grid_match_numpy_oracle():
+    """The C restatement of the GLS assembly and lambda-grid solve (the timed
+    CPU chain's fit) equals the NumPy FP64 oracle (src/solve.cpp:70-262)."""
+    if not cref.available():
+        pytest.skip("oracle C library not built")
+    des, t, w, bn, pen = _gls_problem(0)
+    s = nr.System(des, t, w, bn, pen)
+    m, rhs, ywy = cref.assemble(des, t, w, bn)
+    np.testing.assert_allclose(m, s.m, rtol=1e-12, atol=1e-12 * np.abs(s.m).max())
+    np.testing.assert_allclose(rhs, s.rhs, rtol=1e-12, atol=1e-12 * np.abs(s.rhs).max())
+    assert ywy == pytest.approx(s.ywy, rel=1e-13)
+    grid = np.logspace(-6, 6, 13)
+    want = nr.solve_gls_gcv_system(s, grid)
+    got = cref.gls_gcv(des, t, w, bn, pen, grid)
+    assert got["lambda"] == want["lambda"]
+    np.testing.assert_allclose(got["gcv_curve"], want["gcv_curve"], rtol=1e-9)
+    np.testing.assert_allclose(got["theta"], want["theta"], rtol=1e-8, atol=1e-10)
+
+
+def test_ldlt_fallback_on_a_rank_deficient_system():
+    """A design with two identical components is singular: the Cholesky fails
+    and the reference falls back to Eigen's pivoted LDLT (src/solve.cpp:177-181).
+    Both restatements take that path, agree on the fit, give a minimum of the
+    weighted residual, and report edf = tr(A^+ M) = rank at lambda = 0."""
+    if not cref.available():
+        pytest.skip("oracle C library not built")
+    des, t, w, bn, pen = _gls_problem(1, rank_deficient=True)
+    s = nr.System(des, t, w, bn, pen)
+    with pytest.raises(np.linalg.LinAlgError):
+        np.linalg.cholesky(s.m)
+    got = cref.solve_grid(s, [0.0, 1.0])
+    # the penalty leaves each field's affine part free, so the duplicate stays singular at any lambda
+    assert got[0]["used_ldlt"] and got[1]["used_ldlt"]
+    want = nr.solve_at(s, 0.0)
+    # theta is not unique along M's null space (any LDLT's choice there rests on
+    # rounding), so the fitted quantities are compared: M theta, rss and edf.
+    np.testing.assert_allclose(s.m @ got[0]["theta"], s.m @ want["theta"], rtol=1e-7,
+                               atol=1e-9 * np.abs(s.rhs).max())
+    assert got[0]["rss"] == pytest.approx(want["rss"], rel=1e-8)
+    assert got[0]["effective_dof"] == pytest.approx(want["effective_dof"], abs=1e-6)
+    assert round(want["effective_dof"]) == np.linalg.matrix_rank(s.m)
+    # normal equations hold: M theta = rhs (rhs lies in the range of M)
+    np.testing.assert_allclose(s.m @ want["theta"], s.rhs, rtol=1e-7, atol=1e-7 * np.abs(s.rhs).max())
+    # on an SPD matrix the LDLT solve is the ordinary solve
+    a = s.m + np.eye(s.p)
+    fac, perm = nr.ldlt_factor(a)
+    np.testing.assert_allclose(nr.ldlt_solve(fac, perm, s.rhs), np.linalg.solve(a, s.rhs), rtol=1e-9)
+    np.testing.assert_allclose(cref.ldlt_solve(a, s.rhs), np.linalg.solve(a, s.rhs), rtol=1e-9)
