@@ -301,6 +301,7 @@ def _gls_dict(res, bufs) -> dict:
         # refinement correction (see dgpu_gls_result)
         "precision_used": _PREC_NAMES.get(int(res.precision_used), str(int(res.precision_used))),
         "refine_correction": float(res.refine_correction),
+        "used_ldlt": bool(res.used_ldlt),
     }
 
 

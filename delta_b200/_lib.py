@@ -112,6 +112,7 @@ class GlsResult(ctypes.Structure):
         ("n_lambda_out", ctypes.c_int),
         ("refine_correction", ctypes.c_double),
         ("precision_used", ctypes.c_int),
+        ("used_ldlt", ctypes.c_int),
     ]
 
 

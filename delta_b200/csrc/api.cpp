@@ -153,6 +153,10 @@ int dgpu_set_timing(dgpu_context* ctx, int on) {
   });
 }
 
+int dgpu_set_label_loop_cap(dgpu_context* ctx, int cap) {
+  return guarded(ctx, [&](Context& c) { c.label_loop_cap = cap > 0 ? cap : Context::kDefaultLabelLoopCap; });
+}
+
 int dgpu_launch_count(unsigned long long* count) {
   *count = launch_count();
   return DGPU_OK;

@@ -89,6 +89,7 @@ struct GlsOut {
   const double* d_theta = nullptr;  // device copy of theta
   double refine_correction = 0.0;   // ||delta|| / ||theta|| of the mixed refinement step
   int prec_used = DGPU_PREC_FP64;
+  int ldlt = 0;                     // 1: the chosen system's Cholesky failed, solved by the LDLT fallback
 };
 
 // Rows + normal-equation machinery shared by fit_kernel and solve_gls*.
@@ -298,6 +299,7 @@ struct Engine {
   static constexpr double kMixedFallback = 1e-2;
   bool mixed_failed(const GlsOut& o) const {
     if (o.prec_used != DGPU_PREC_MIXED) return false;
+    if (o.ldlt) return true;  // the refinement step applies a Cholesky factor the system does not have
     if (!(o.refine_correction <= kMixedFallback)) return true;
     for (double v : o.theta)
       if (!std::isfinite(v)) return true;
@@ -329,6 +331,11 @@ struct Engine {
   void finish_single(const Work& w, int s, double lam, const double* M, const long long* n, const uint8_t* mask,
                      GlsOut& o, bool anchored = false) {
     double* th = w.theta + static_cast<size_t>(s) * P;
+    // A mixed system that went through the LDLT fallback has no Cholesky
+    // factor for the refinement step below; its result is discarded once the
+    // ok flag (fetched with theta) shows it, and the fit is redone in FP64
+    // (mixed_failed).
+    int ok_s = 1;
     if (prec == DGPU_PREC_MIXED) {
       const Anchor a = anchor_buffers();
       if (!anchored) anchor_at(a, th, mask);
@@ -347,12 +354,14 @@ struct Engine {
     f.add(&o.rss, w.rss + s, 1);
     f.add(&o.gcv, w.gcv + s, 1);
     f.add(&o.npix, n, 1);
+    f.add(&ok_s, w.ok + s, 1);
     if (!delta.empty()) f.add(delta.data(), anchor_buffers().delta, P);
     if (on_fetch) on_fetch(th, f);
     f.run();
     o.d_theta = th;
     o.lambda = lam;
     o.prec_used = prec;
+    o.ldlt = ok_s == 2 ? 1 : 0;
     if (!delta.empty()) {
       double dd = 0.0, tt = 0.0;
       for (int p = 0; p < P; ++p) {
@@ -597,6 +606,7 @@ void write_gls(const GlsOut& o, int nc, int k, dgpu_gls_result* out) {
   out->n_lambda_out = static_cast<int>(o.grid.size());
   out->refine_correction = o.refine_correction;
   out->precision_used = o.prec_used;
+  out->used_ldlt = o.ldlt;
   if (out->lambda_grid && !o.grid.empty()) std::memcpy(out->lambda_grid, o.grid.data(), sizeof(double) * o.grid.size());
   if (out->gcv_curve && !o.curve.empty()) std::memcpy(out->gcv_curve, o.curve.data(), sizeof(double) * o.curve.size());
 }

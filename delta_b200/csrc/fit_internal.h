@@ -72,7 +72,7 @@ struct SolveBatch {
   double* A = nullptr;
   double* theta = nullptr;          // nsys x P
   double* edf = nullptr;            // nsys
-  int* ok = nullptr;                // nsys: 1 if the Cholesky succeeded
+  int* ok = nullptr;                // nsys: 1 Cholesky, 2 LDLT fallback, 0 failed
   unsigned* status = nullptr;
   double* partial = nullptr;        // nsys x 8 per-rank trace partials
 };
@@ -81,6 +81,9 @@ int solve_ep(int nf, int r);                       // appended rows, padded
 size_t solve_sys_doubles(int P, int nf, int r);    // workspace per system
 size_t solve_work_doubles(int P, int nf, int r, int nsys, int nm);
 void launch_solve_batch(Context& c, const SolveBatch& b);
+// Pivoted LDL^T redo of every system of the batch whose Cholesky failed
+// (ok == 0): theta, edf = tr(A^+ M), ok = 2. Launched by launch_solve_batch.
+void launch_ldlt_fallback(Context& c, const SolveBatch& b);
 // Apply a system's inverse: out = A_s^{-1} v (from the factor tiles of system s).
 void launch_apply_inverse(cudaStream_t st, const SolveBatch& b, int s, const double* v, double* out);
 

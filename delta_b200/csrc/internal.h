@@ -67,7 +67,7 @@ enum Slot : int {
   kSlotFit0, kSlotFit1, kSlotFit2, kSlotFit3, kSlotFit4, kSlotFit5, kSlotFit6, kSlotFit7,
   kSlotFit8, kSlotFit9, kSlotFit10, kSlotFit11, kSlotFit12, kSlotFit13, kSlotFit14, kSlotFit15,
   kSlotFft0, kSlotFft1, kSlotFft2, kSlotFft3, kSlotFft4, kSlotFft5,
-  kSlotGlsPart,
+  kSlotGlsPart, kSlotLdlt,
   kSlotCount
 };
 
@@ -76,6 +76,10 @@ struct Context {
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   unsigned* d_status = nullptr;  // device status word (see StatusBit)
+  // Iteration cap of each union-find search / link loop of the CCL (per
+  // thread); dgpu_set_label_loop_cap lowers it for fault-handling tests.
+  static constexpr int kDefaultLabelLoopCap = 1 << 24;
+  int label_loop_cap = kDefaultLabelLoopCap;
   void* slot_ptr[kSlotCount] = {};
   size_t slot_size[kSlotCount] = {};
   std::string last_error;

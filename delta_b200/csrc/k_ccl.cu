@@ -20,7 +20,6 @@
 
 namespace dgpu {
 
-constexpr int kFindCap = 1 << 24;
 
 __global__ void k_seed(int64_t n, const float* __restrict__ score, const uint8_t* __restrict__ mask,
                        int exclude, float thr_pos, float thr_neg, uint8_t* __restrict__ seeds) {
@@ -36,8 +35,8 @@ __global__ void k_seed(int64_t n, const float* __restrict__ score, const uint8_t
   }
 }
 
-__device__ __forceinline__ int find_root(const int* L, int i, unsigned* st) {
-  for (int it = 0; it < kFindCap; ++it) {
+__device__ __forceinline__ int find_root(const int* L, int i, unsigned* st, int cap) {
+  for (int it = 0; it < cap; ++it) {
     const int p = L[i];
     if (p == i) return i;
     i = p;
@@ -46,10 +45,10 @@ __device__ __forceinline__ int find_root(const int* L, int i, unsigned* st) {
   return i;
 }
 
-__device__ void unite(int* L, int a, int b, unsigned* st) {
-  for (int it = 0; it < kFindCap; ++it) {
-    a = find_root(L, a, st);
-    b = find_root(L, b, st);
+__device__ void unite(int* L, int a, int b, unsigned* st, int cap) {
+  for (int it = 0; it < cap; ++it) {
+    a = find_root(L, a, st, cap);
+    b = find_root(L, b, st, cap);
     if (a == b) return;
     if (a < b) {
       const int t = a;
@@ -70,27 +69,27 @@ __global__ void k_label_init(int64_t n, const uint8_t* __restrict__ seeds, uint8
 }
 
 __global__ void k_label_merge(int w, int h, const uint8_t* __restrict__ seeds, uint8_t bit, int* L,
-                              unsigned* st) {
+                              unsigned* st, int cap) {
   const int64_t n = static_cast<int64_t>(w) * h;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     if (!(seeds[i] & bit)) continue;
     const int x = static_cast<int>(i % w), y = static_cast<int>(i / w);
     const int me = static_cast<int>(i);
-    if (x > 0 && (seeds[i - 1] & bit)) unite(L, me, me - 1, st);
+    if (x > 0 && (seeds[i - 1] & bit)) unite(L, me, me - 1, st, cap);
     if (y > 0) {
       const int64_t a = i - w;
-      if (x > 0 && (seeds[a - 1] & bit)) unite(L, me, static_cast<int>(a - 1), st);
-      if (seeds[a] & bit) unite(L, me, static_cast<int>(a), st);
-      if (x + 1 < w && (seeds[a + 1] & bit)) unite(L, me, static_cast<int>(a + 1), st);
+      if (x > 0 && (seeds[a - 1] & bit)) unite(L, me, static_cast<int>(a - 1), st, cap);
+      if (seeds[a] & bit) unite(L, me, static_cast<int>(a), st, cap);
+      if (x + 1 < w && (seeds[a + 1] & bit)) unite(L, me, static_cast<int>(a + 1), st, cap);
     }
   }
 }
 
-__global__ void k_label_flatten(int64_t n, int* L, unsigned* st) {
+__global__ void k_label_flatten(int64_t n, int* L, unsigned* st, int cap) {
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    if (L[i] >= 0) L[i] = find_root(L, static_cast<int>(i), st);
+    if (L[i] >= 0) L[i] = find_root(L, static_cast<int>(i), st, cap);
   }
 }
 
@@ -154,12 +153,22 @@ __global__ void k_root_rank(int64_t n, const int* __restrict__ L, const int* __r
   if (root) rank_at[i] = offsets[blockIdx.x] + warp_tot[wid] + __popc(bal & ((1u << lane) - 1));
 }
 
+// Only a root carries a rank, so a pixel maps to a label only through a root:
+// one left pointing at a non-root (a capped search gave up) gets label 0 and
+// the bounds status, which keeps every label within [1, number of roots].
 __global__ void k_label_final(int64_t n, const int* __restrict__ L, const int* __restrict__ rank_at,
-                              int* __restrict__ labels) {
+                              int* __restrict__ labels, unsigned* st) {
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int r = L[i];
-    labels[i] = r >= 0 ? rank_at[r] + 1 : 0;
+    int lbl = 0;
+    if (r >= 0) {
+      if (L[r] == r)
+        lbl = rank_at[r] + 1;
+      else
+        set_status(st, kStatusBounds);
+    }
+    labels[i] = lbl;
   }
 }
 
@@ -414,9 +423,9 @@ static int label_polarity(Context& c, int w, int h, const uint8_t* seeds, uint8_
   int* counts = static_cast<int*>(c.slot(kSlotBlockCounts, sizeof(int) * (nb + 2)));
   k_label_init<<<grid_for(n), 256, 0, s>>>(n, seeds, bit, L);
   DGPU_LAUNCH("k_label_init");
-  k_label_merge<<<grid_for(n), 256, 0, s>>>(w, h, seeds, bit, L, c.d_status);
+  k_label_merge<<<grid_for(n), 256, 0, s>>>(w, h, seeds, bit, L, c.d_status, c.label_loop_cap);
   DGPU_LAUNCH("k_label_merge");
-  k_label_flatten<<<grid_for(n), 256, 0, s>>>(n, L, c.d_status);
+  k_label_flatten<<<grid_for(n), 256, 0, s>>>(n, L, c.d_status, c.label_loop_cap);
   DGPU_LAUNCH("k_label_flatten");
   k_root_count<<<nb, kRankBlock, 0, s>>>(n, L, counts);
   DGPU_LAUNCH("k_root_count");
@@ -424,7 +433,7 @@ static int label_polarity(Context& c, int w, int h, const uint8_t* seeds, uint8_
   DGPU_LAUNCH("k_scan_counts");
   k_root_rank<<<nb, kRankBlock, 0, s>>>(n, L, counts, rank_at);
   DGPU_LAUNCH("k_root_rank");
-  k_label_final<<<grid_for(n), 256, 0, s>>>(n, L, rank_at, labels);
+  k_label_final<<<grid_for(n), 256, 0, s>>>(n, L, rank_at, labels, c.d_status);
   DGPU_LAUNCH("k_label_final");
   int total = 0;
   DGPU_CUDA(cudaMemcpyAsync(&total, counts + nb, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -27,7 +27,8 @@
 // penalty added there; E is generated at its first touch. theta = L^-T y by back
 // substitution on rank 0. The trace is reduced per rank in a fixed order and
 // summed in rank order (deterministic). A non-positive pivot marks the system
-// failed (ok = 0): the reference then falls back to LDLT.
+// failed (ok = 0); k_ldlt.cu then redoes it by pivoted LDL^T, as the reference
+// falls back from LLT to LDLT.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -693,6 +694,9 @@ void launch_solve_batch(Context& c, const SolveBatch& b) {
   SolveBatch bb = b;
   DGPU_CUDA(cudaLaunchKernelEx(&cfg, k_solve_cluster, bb, Pp, Ep, sys_stride, static_cast<const double*>(Mt)));
   DGPU_LAUNCH("k_solve_cluster");
+  // Systems whose Cholesky met a non-positive pivot are redone by pivoted
+  // LDL^T, as the reference falls back from LLT to LDLT (src/solve.cpp:177-181).
+  launch_ldlt_fallback(c, b);
 }
 
 // out = A_s^{-1} v = L^-T (L^-1 v) from system s's factor tiles, one CTA.

@@ -70,6 +70,13 @@ int dgpu_drain_timing(dgpu_context* ctx, char (*labels)[64], double* seconds, in
 int dgpu_set_timing(dgpu_context* ctx, int on);
 /* Number of kernels this library has launched in the process so far. */
 int dgpu_launch_count(unsigned long long* count);
+/* Iteration cap of every union-find search and link loop of the catalog's
+ * labelling on this context (no reference counterpart: the reference's CPU
+ * union-find has no cap). A loop that reaches it stops, the pixels it left
+ * unresolved get label 0, and the call returns DGPU_ERR_LIMIT; the context
+ * stays usable. cap <= 0 restores the default (2^24, far above any real
+ * chain). Lowering it is how the failure path is tested. */
+int dgpu_set_label_loop_cap(dgpu_context* ctx, int cap);
 
 /* ---- basis (host math) ---------------------------------------------------- */
 /* GaussHermiteBasis::default_radius, src/basis.cpp:9-12. */
@@ -205,6 +212,10 @@ typedef struct {
    * ||correction|| / ||theta|| of the last mixed refinement step (0 otherwise). */
   double refine_correction;
   int precision_used;
+  /* 1 when the selected system's Cholesky met a non-positive pivot and theta /
+   * edf come from the pivoted LDL^T fallback (the reference's LLT -> LDLT
+   * fallback, src/solve.cpp:177-181); 0 otherwise. */
+  int used_ldlt;
 } dgpu_gls_result;
 
 /* fit_kernel, src/bindings.cpp:643-693 -> delta::fit_kernel, src/fit.cpp:63-511

@@ -728,7 +728,8 @@ def cv_finish(mf, rf, ysq, n_groups, penalty, n, nc, k, lambda_grid, warm_start=
                     chol = np.linalg.cholesky(a)
                     th = np.linalg.solve(chol.T, np.linalg.solve(chol, r_train[g]))
                 except np.linalg.LinAlgError:
-                    th = np.linalg.lstsq(a, r_train[g], rcond=None)[0]
+                    fac, perm = ldlt_factor(a)  # src/solve.cpp:328-333
+                    th = ldlt_solve(fac, perm, r_train[g])
                 e = ysq[g] - 2.0 * float(th @ rf[g]) + float(th @ (mf[g] @ th))
                 tot += e if e > 0.0 else 0.0
             curve[li] = tot

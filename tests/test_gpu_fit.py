@@ -210,3 +210,57 @@ def test_fit_kernel_errors():
         _core.fit_kernel(sci, ref, knots, sx, sy[:-1], 7, 1.2, 2, GRID)
     with pytest.raises(RuntimeError):
         _core.fit_kernel(sci, ref, knots, np.array([-100], np.int32), np.array([-100], np.int32), 7, 1.2, 2, GRID)
+
+
+def _singular_problem(seed=7, n=2500, nc=4, nk=3):
+    """A design whose component 2 is zero at every row: M's block for it is
+    exactly zero, so A = M + lambda P0 keeps that field's three affine
+    directions singular at every lambda (the penalty leaves them free). The
+    Cholesky fails on the device as in Eigen; the reference then solves by its
+    pivoted LDLT (src/solve.cpp:177-181, :328-333 in CV)."""
+    knots, pts, t, w, bn, _ = _problem(seed, n=n, nc=nc, nk=nk)
+    bn = bn.copy()
+    bn[:, 2] = 0.0
+    return knots, pts, t, w, bn
+
+
+def test_ldlt_fallback_matches_oracle_on_a_singular_system():
+    knots, pts, t, w, bn = _singular_problem()
+    want = nr.solve_gls_gcv(knots, pts, t, w, bn, GRID)
+    got = _core.solve_gls_gcv(knots, pts, t, w, bn, GRID)
+    assert got["used_ldlt"]
+    assert got["lambda"] == want["lambda"]
+    np.testing.assert_allclose(got["gcv_curve"], want["gcv_curve"], rtol=1e-6)
+    np.testing.assert_allclose(got["theta"], want["theta"], rtol=1e-7, atol=1e-9)
+    np.testing.assert_allclose(got["effective_dof"], want["effective_dof"], rtol=1e-8)
+    np.testing.assert_allclose(got["rss"], want["rss"], rtol=1e-6)
+    k = knots.shape[0]
+    # the dead field's coefficients: its bending part is zeroed by the penalty,
+    # its affine part by the pseudo-inverse of the zero pivots
+    np.testing.assert_allclose(got["theta"][2 * k : 3 * k], 0.0, atol=1e-12)
+    for lam in (1e-6, 1.0, 1e6):
+        g = _core.solve_gls(knots, pts, t, w, bn, lam)
+        s = nr.solve_gls(knots, pts, t, w, bn, lam)
+        assert g["used_ldlt"]
+        np.testing.assert_allclose(g["theta"], s["theta"], rtol=1e-7, atol=1e-9)
+        np.testing.assert_allclose(g["effective_dof"], s["effective_dof"], rtol=1e-8)
+
+
+def test_ldlt_fallback_in_cv_and_mixed_precision():
+    knots, pts, t, w, bn = _singular_problem(8, n=2400)
+    group = np.arange(t.size) % 4
+    got = _core.solve_gls_cv(knots, pts, t, w, bn, GRID, group, 4)
+    want = nr.solve_gls_cv(knots, pts, t, w, bn, GRID, group, 4)
+    assert got["lambda"] == want["lambda"] and got["used_ldlt"]
+    fin = np.isfinite(want["gcv_curve"])  # coarse-to-fine search: unvisited lambdas stay inf
+    assert np.array_equal(np.isfinite(got["gcv_curve"]), fin)
+    np.testing.assert_allclose(got["gcv_curve"][fin], want["gcv_curve"][fin], rtol=1e-6)
+    np.testing.assert_allclose(got["theta"], want["theta"], rtol=1e-7, atol=1e-9)
+    # Mixed precision has no Cholesky factor to refine with: it redoes the fit in FP64.
+    mixed = _core.solve_gls_gcv(knots, pts, t, w, bn, GRID, precision="mixed")
+    assert mixed["precision_used"] == "fp64" and mixed["used_ldlt"]
+    fp64 = _core.solve_gls_gcv(knots, pts, t, w, bn, GRID)
+    np.testing.assert_array_equal(mixed["theta"], fp64["theta"])
+    # an ordinary SPD system never takes the fallback
+    knots, pts, t, w, bn, _ = _problem()
+    assert not _core.solve_gls_gcv(knots, pts, t, w, bn, GRID)["used_ldlt"]
