@@ -221,6 +221,76 @@ def subtract(science, reference, knots, theta, beta: float, n_max: int, radius: 
             "mask": mask if hm.value else None}
 
 
+def kernel_chi2(science, reference, weights, knots, theta, beta: float, n_max: int, radius: int = 0,
+                dx: float = 0.0, dy: float = 0.0, scale: float = 1.0, reference_mask=None, grad: bool = True,
+                grad_reference: bool = False) -> dict:
+    """Weighted chi^2 of the kernel model shifted by (dx, dy) and scaled by
+    ``scale`` (include/delta_gpu.h, dgpu_kernel_chi2; no reference counterpart)
+    and, with ``grad``, its gradients with respect to theta, (dx, dy) and the
+    scale; with ``grad_reference`` also with respect to the reference image.
+    Returns {'chi2', 'grad_theta', 'grad_shift', 'grad_scale', 'grad_reference'}."""
+    sci = _img(science, "science")
+    ref = _img(reference, "reference")
+    wt = _img(weights, "weights")
+    rmask = _mask_opt(reference_mask, "reference_mask")
+    if sci.shape != ref.shape or wt.shape != sci.shape:
+        raise ValueError("kernel_chi2: science, reference and weights must share a shape")
+    _same_shape(rmask, ref, "mask shape does not match data")
+    h, w = sci.shape
+    model, keep = _model(knots, theta, beta, n_max, radius)
+    n_theta = int(np.asarray(theta).size)
+    chi2 = ctypes.c_double()
+    g_theta = np.empty(n_theta) if grad else None
+    g_shift = np.empty(2) if grad else None
+    g_scale = ctypes.c_double()
+    g_ref = np.empty((h, w), np.float32) if grad_reference else None
+    ctx = context()
+    check(_lib.lib().dgpu_kernel_chi2(ctx.handle, _lib.MEM_HOST, ctypes.c_int64(w), ctypes.c_int64(h), ptr(sci),
+                                      ptr(ref), ptr(rmask), ptr(wt), ctypes.byref(model), ctypes.c_double(dx),
+                                      ctypes.c_double(dy), ctypes.c_double(scale), ctypes.byref(chi2), ptr(g_theta),
+                                      ptr(g_shift), ctypes.byref(g_scale) if grad else None, ptr(g_ref)),
+          ctx.handle)
+    return {"chi2": chi2.value, "grad_theta": g_theta, "grad_shift": g_shift,
+            "grad_scale": g_scale.value if grad else None, "grad_reference": g_ref}
+
+
+def stamp_gcv(science, reference, knots, stamp_x, stamp_y, stamp_radius: int, beta: float, n_max: int,
+              log_lambda: float, dx: float = 0.0, dy: float = 0.0, scale: float = 1.0, radius: int = 0,
+              science_var=None, reference_var=None, science_mask=None, reference_mask=None,
+              grad: bool = True) -> dict:
+    """GCV score and weighted RSS of the stamp fit at lambda = exp(log_lambda)
+    with the basis shifted by (dx, dy) and scaled by ``scale``, and (``grad``)
+    their gradients with respect to (log_lambda, dx, dy, scale)
+    (include/delta_gpu.h, dgpu_stamp_gcv; no reference counterpart)."""
+    sci = _img(science, "science")
+    ref = _img(reference, "reference")
+    svar = _img_opt(science_var, "science_var")
+    rvar = _img_opt(reference_var, "reference_var")
+    smask = _mask_opt(science_mask, "science_mask")
+    rmask = _mask_opt(reference_mask, "reference_mask")
+    if sci.shape != ref.shape:
+        raise RuntimeError("fit_kernel: science/reference shape mismatch")
+    k = _knots(knots)
+    sx = np.ascontiguousarray(stamp_x, np.int32)
+    sy = np.ascontiguousarray(stamp_y, np.int32)
+    if sx.size != sy.size:
+        raise RuntimeError("fit_kernel: stamp_x/stamp_y length mismatch")
+    h, w = sci.shape
+    nc = (n_max + 1) * (n_max + 2) // 2
+    vals = np.zeros(4)
+    theta = np.zeros((nc + 1) * k.shape[0])
+    g_gcv = np.zeros(4) if grad else None
+    g_rss = np.zeros(4) if grad else None
+    ctx = context()
+    check(_lib.lib().dgpu_stamp_gcv(
+        ctx.handle, _lib.MEM_HOST, ctypes.c_int64(w), ctypes.c_int64(h), ptr(sci), ptr(ref), ptr(svar), ptr(rvar),
+        ptr(smask), ptr(rmask), ptr(k), k.shape[0], ptr(sx), ptr(sy), int(sx.size), int(stamp_radius),
+        ctypes.c_double(beta), int(n_max), int(radius), ctypes.c_double(log_lambda), ctypes.c_double(dx),
+        ctypes.c_double(dy), ctypes.c_double(scale), ptr(vals), ptr(theta), ptr(g_gcv), ptr(g_rss)), ctx.handle)
+    return {"gcv": float(vals[0]), "rss": float(vals[1]), "effective_dof": float(vals[2]), "n_pixels": int(vals[3]),
+            "theta": theta, "grad_gcv": g_gcv, "grad_rss": g_rss}
+
+
 def photometric_scale(knots, theta, component_sums, height: int, width: int) -> np.ndarray:
     """Per-pixel photometric scale field sum_n a_n(x,y) S_n, shape (H,W)."""
     k = _knots(knots)

@@ -17,6 +17,7 @@
 #include <numeric>
 
 #include "fit_internal.h"
+#include "gcv_grad_internal.h"
 #include "gls_internal.h"
 
 using namespace dgpu;
@@ -890,6 +891,159 @@ int dgpu_fit_kernel(dgpu_context* ctx, int mem, int64_t width, int64_t height, c
       if (out->stamp_y) out->stamp_y[i] = stamp_y[s];
       if (out->stamp_chi2) out->stamp_chi2[i] = stamp_chi2[s];
       if (out->stamp_accepted) out->stamp_accepted[i] = accepted[s];
+    }
+  });
+}
+
+// GCV score and weighted RSS of the stamp fit at one lambda with the kernel
+// basis shifted by (dx, dy) and scaled by s, and their gradients with respect
+// to (log lambda, dx, dy, s) through the adjoint of the normal-equation map
+// (k_gcv_grad.cu). First-pass weights 1 / (Var_t + Var_c), no clipping.
+int dgpu_stamp_gcv(dgpu_context* ctx, int mem, int64_t width, int64_t height, const float* science,
+                   const float* reference, const float* science_var, const float* reference_var,
+                   const uint8_t* science_mask, const uint8_t* reference_mask, const double* knots, int n_knots,
+                   const int32_t* stamp_x, const int32_t* stamp_y, int n_stamps, int stamp_radius, double beta,
+                   int n_max, int radius, double log_lambda, double dx, double dy, double scale, double* values,
+                   double* theta, double* grad_gcv, double* grad_rss) {
+  return guarded(ctx, [&](Context& c) {
+    if (width <= 0 || height <= 0) fail(DGPU_ERR_INVALID, "image must be non-empty");
+    if (width * height >= (int64_t(1) << 31)) fail(DGPU_ERR_INVALID, "image too large");
+    if (!science || !reference || !knots || !values) fail(DGPU_ERR_INVALID, "stamp_gcv: missing argument");
+    if (stamp_radius < 0) fail(DGPU_ERR_INVALID, "stamp_radius must be >= 0");
+    if (!std::isfinite(log_lambda) || !std::isfinite(dx) || !std::isfinite(dy) || !std::isfinite(scale) ||
+        scale == 0.0)
+      fail(DGPU_ERR_INVALID, "stamp_gcv: log_lambda, shift and a non-zero scale must be finite");
+    if (n_stamps <= 0 || !stamp_x || !stamp_y) fail(DGPU_ERR_RUNTIME, "fit_kernel: no usable stamp pixels");
+    const int w = static_cast<int>(width), h = static_cast<int>(height);
+    const size_t npx = static_cast<size_t>(w) * h;
+    const Basis b(beta, n_max, radius);
+    const ThinPlate tp(knots, n_knots);
+    const int nc = b.nc, k = tp.k, P = (nc + 1) * k;
+    cudaStream_t st = c.stream;
+    reset_status(c);
+    const auto* sci = static_cast<const float*>(stage_in(c, mem, science, 4 * npx, kSlotInSci));
+    const auto* ref = static_cast<const float*>(stage_in(c, mem, reference, 4 * npx, kSlotInRef));
+    const auto* vs = static_cast<const float*>(stage_in(c, mem, science_var, 4 * npx, kSlotInVarS));
+    const auto* vr = static_cast<const float*>(stage_in(c, mem, reference_var, 4 * npx, kSlotInVarR));
+    const auto* sm = static_cast<const uint8_t*>(stage_in(c, mem, science_mask, npx, kSlotInMaskS));
+    const auto* rm = static_cast<const uint8_t*>(stage_in(c, mem, reference_mask, npx, kSlotInMaskR));
+    const bool have_var = vs != nullptr || vr != nullptr;
+    StampGeom g;
+    g.w = w;
+    g.h = h;
+    g.sr = stamp_radius;
+    g.S = 2 * stamp_radius + 1;
+    g.SS = g.S * g.S;
+    g.r = b.radius;
+    g.ks = b.ks;
+    g.n_max = n_max;
+    g.nc = nc;
+    g.pmax = g.S + 2 * b.radius;
+    g.have_var = have_var ? 1 : 0;
+    g.have_cvar = vr != nullptr ? 1 : 0;
+    const int64_t N = static_cast<int64_t>(n_stamps) * g.SS;
+    Engine E(c, DGPU_PREC_FP64, tp, nc, N, g.SS, n_stamps);
+    E.alloc_rows();
+    const int rk = E.rk;
+    float* fill = static_cast<float*>(c.slot(kSlotScratch2, 64));
+    launch_strided_median(c, kSampleReference, static_cast<int64_t>(npx), ref, rm, fill);
+    int* dsx = up(c, kSlotBright, reinterpret_cast<const int*>(stamp_x), static_cast<size_t>(n_stamps));
+    int* dsy = up(c, kSlotCompOut, reinterpret_cast<const int*>(stamp_y), static_cast<size_t>(n_stamps));
+    // Taps: x tables carry the scale (u_c = s B_n), y tables do not.
+    std::vector<double> gx, dgx, gy, dgy;
+    b.shifted_taps(dx, gx, dgx);
+    b.shifted_taps(dy, gy, dgy);
+    const size_t nt = gx.size();
+    std::vector<float> taps(4 * nt);
+    for (size_t i = 0; i < nt; ++i) {
+      taps[i] = static_cast<float>(scale * gx[i]);
+      taps[nt + i] = static_cast<float>(scale * dgx[i]);
+      taps[2 * nt + i] = static_cast<float>(gy[i]);
+      taps[3 * nt + i] = static_cast<float>(dgy[i]);
+    }
+    float* dt = up(c, kSlotTaps, taps.data(), taps.size());
+    std::vector<int2> ord(nc);
+    for (int i = 0; i < nc; ++i) ord[i] = make_int2(b.orders[i].first, b.orders[i].second);
+    int2* dord = up(c, kSlotRootRank, ord.data(), ord.size());
+    FitRows Rx = E.R, Ry = E.R;
+    Rx.bn = static_cast<double*>(c.slot(kSlotGrad4, sizeof(double) * static_cast<size_t>(N) * nc));
+    Ry.bn = static_cast<double*>(c.slot(kSlotGrad5, sizeof(double) * static_cast<size_t>(N) * nc));
+    {
+      StageTimer t(c, "gradient: stamp B_n convolve");
+      // Derivative rows first: the main gather's row flags and values come last.
+      launch_stamp_gather(st, g, n_stamps, dsx, dsy, sci, ref, vs, vr, sm, rm, dt + nt, dord, fill, Rx, dt + 2 * nt);
+      launch_stamp_gather(st, g, n_stamps, dsx, dsy, sci, ref, vs, vr, sm, rm, dt, dord, fill, Ry, dt + 3 * nt);
+      launch_stamp_gather(st, g, n_stamps, dsx, dsy, sci, ref, vs, vr, sm, rm, dt, dord, fill, E.R, dt + 2 * nt);
+      launch_design_weights(st, N, upload_tps(c, tp), E.R, have_var ? 1 : 0);
+    }
+    StageTimer solve_timer(c, "gradient: GCV adjoint");
+    std::vector<uint8_t> ones(n_stamps, 1);
+    uint8_t* d_acc = up(c, kSlotSeedPos, ones.data(), ones.size());
+    double* M = static_cast<double*>(c.slot(kSlotScratch1, sizeof(double) * (static_cast<size_t>(P) * P + P + 4)));
+    double* rhs = M + static_cast<size_t>(P) * P;
+    double* ywy = rhs + P;
+    double* raw = ywy + 1;
+    long long* n = reinterpret_cast<long long*>(raw + 1);
+    E.assemble(d_acc, M, rhs, ywy, n);
+    const double lam = std::exp(log_lambda);
+    const int m = gcv_rhs_cols(P, k, rk);
+    double* B = static_cast<double*>(c.slot(kSlotGrad3, sizeof(double) * 2 * static_cast<size_t>(P) * m));
+    double* X = B + static_cast<size_t>(P) * m;
+    launch_build_rhs_f(st, P, k, rk, rhs, E.d_fk, B);
+    launch_sym_solve_many(c, P, k, M, lam, E.d_pen, B, m, X);
+    double* work = static_cast<double*>(c.slot(kSlotGrad2, sizeof(double) * gcv_stats_doubles(P, k, rk) +
+                                                   sizeof(GcvScalars) + 64));
+    GcvScalars* scal = reinterpret_cast<GcvScalars*>(work + gcv_stats_doubles(P, k, rk));
+    launch_gcv_theta(st, P, k, rk, X, E.d_fk, work);
+    launch_quad_err(c, 1, P, work, M, nullptr, rhs, nullptr, ywy, raw);
+    launch_gcv_stats(st, P, k, rk, X, E.d_fk, lam, raw, n, work, scal);
+    const int nq = m - 1;
+    double* out6 = static_cast<double*>(c.slot(kSlotGrad7, sizeof(double) * (6 * static_cast<size_t>(gcv_rows_blocks(N)) + 8)));
+    if (grad_gcv || grad_rss) {
+      GcvRowsArgs a;
+      a.N = N;
+      a.nc = nc;
+      a.k = k;
+      a.nq = nq;
+      a.valid = E.R.valid;
+      a.w = E.R.w;
+      a.t = E.R.t;
+      a.d = E.R.d;
+      a.bn = E.R.bn;
+      a.bnx = Rx.bn;
+      a.bny = Ry.bn;
+      a.theta = work;
+      a.z = work + P + nq;
+      a.X = X;
+      a.scal = scal;
+      a.scale = scale;
+      a.partial = out6 + 8;
+      launch_gcv_rows(st, a, out6);
+    }
+    GcvScalars hs{};
+    double g6[6] = {0, 0, 0, 0, 0, 0};
+    std::vector<double> th(P);
+    DGPU_CUDA(cudaMemcpyAsync(&hs, scal, sizeof(GcvScalars), cudaMemcpyDeviceToHost, st));
+    DGPU_CUDA(cudaMemcpyAsync(th.data(), work, sizeof(double) * P, cudaMemcpyDeviceToHost, st));
+    if (grad_gcv || grad_rss) DGPU_CUDA(cudaMemcpyAsync(g6, out6, sizeof(g6), cudaMemcpyDeviceToHost, st));
+    check_status(c);  // synchronises
+    if (hs.n <= 0.0) fail(DGPU_ERR_RUNTIME, "fit_kernel: no usable stamp pixels");
+    values[0] = hs.gcv;
+    values[1] = hs.rss;
+    values[2] = hs.edf;
+    values[3] = hs.n;
+    if (theta) std::copy(th.begin(), th.end(), theta);
+    if (grad_gcv) {
+      grad_gcv[0] = hs.dgcv_dloglam;
+      grad_gcv[1] = g6[0];
+      grad_gcv[2] = g6[1];
+      grad_gcv[3] = g6[2];
+    }
+    if (grad_rss) {
+      grad_rss[0] = hs.drss_dloglam;
+      grad_rss[1] = g6[3];
+      grad_rss[2] = g6[4];
+      grad_rss[3] = g6[5];
     }
   });
 }

@@ -31,7 +31,7 @@ struct FitRows {
 void launch_stamp_gather(cudaStream_t st, const StampGeom& g, int n_stamps, const int* sx, const int* sy,
                          const float* sci, const float* ref, const float* vs, const float* vr,
                          const uint8_t* sm, const uint8_t* rm, const float* taps, const int2* orders,
-                         const float* fill, const FitRows& R);
+                         const float* fill, const FitRows& R, const float* taps_y = nullptr);
 void launch_design_weights(cudaStream_t st, int64_t N, const TpsDev& t, const FitRows& R, int have_var);
 void launch_normal_equations(Context& c, int prec, int64_t N, int nc, int k, int SS, const FitRows& R,
                              const uint8_t* accepted, double* M);
@@ -84,6 +84,9 @@ void launch_solve_batch(Context& c, const SolveBatch& b);
 // Pivoted LDL^T redo of every system of the batch whose Cholesky failed
 // (ok == 0): theta, edf = tr(A^+ M), ok = 2. Launched by launch_solve_batch.
 void launch_ldlt_fallback(Context& c, const SolveBatch& b);
+// X = (M + lam P0)^+ B by the same pivoted LDL^T, one CTA; B, X: P x m row-major.
+void launch_sym_solve_many(Context& c, int P, int k, const double* M, double lam, const double* pen, const double* B,
+                           int m, double* X);
 // Apply a system's inverse: out = A_s^{-1} v (from the factor tiles of system s).
 void launch_apply_inverse(cudaStream_t st, const SolveBatch& b, int s, const double* v, double* out);
 

@@ -57,6 +57,30 @@ Basis::Basis(double beta_, int n_max_, int radius_) : beta(beta_), n_max(n_max_)
   nc = static_cast<int>(orders.size());
 }
 
+void Basis::shifted_taps(double d, std::vector<double>& g, std::vector<double>& dg) const {
+  // g_n(u - d) and g_n'(u - d) at the offsets u = -r..r, with
+  // g_n'(x) = norm_n / beta * (2 n H_{n-1}(t) - t H_n(t)) exp(-t^2 / 2), t = x / beta.
+  // At d = 0, g is bit-identical to b1d (same arithmetic).
+  const double ln2 = std::log(2.0);
+  const double half_ln_pi = 0.5 * std::log(std::acos(-1.0));
+  const double ln_beta = std::log(beta);
+  g.assign(static_cast<size_t>(n_max + 1) * ks, 0.0);
+  dg.assign(g.size(), 0.0);
+  for (int i = 0; i < ks; ++i) {
+    const double t = (static_cast<double>(i - radius) - d) / beta;
+    const double e = std::exp(-0.5 * t * t);
+    double hm1 = 0.0, hc = 1.0;  // H_{n-1}, H_n
+    for (int n = 0; n <= n_max; ++n) {
+      const double norm = std::exp(-0.5 * (n * ln2 + std::lgamma(n + 1.0) + half_ln_pi + ln_beta));
+      g[static_cast<size_t>(n) * ks + i] = norm * hc * e;
+      dg[static_cast<size_t>(n) * ks + i] = norm / beta * (2.0 * n * hm1 - t * hc) * e;
+      const double hn = 2.0 * t * hc - 2.0 * n * hm1;
+      hm1 = hc;
+      hc = hn;
+    }
+  }
+}
+
 std::vector<float> Basis::taps() const {
   std::vector<float> t(b1d.size());
   for (size_t i = 0; i < b1d.size(); ++i) t[i] = static_cast<float>(b1d[i]);

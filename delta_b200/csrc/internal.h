@@ -68,6 +68,7 @@ enum Slot : int {
   kSlotFit8, kSlotFit9, kSlotFit10, kSlotFit11, kSlotFit12, kSlotFit13, kSlotFit14, kSlotFit15,
   kSlotFft0, kSlotFft1, kSlotFft2, kSlotFft3, kSlotFft4, kSlotFft5,
   kSlotGlsPart, kSlotLdlt,
+  kSlotGrad0, kSlotGrad1, kSlotGrad2, kSlotGrad3, kSlotGrad4, kSlotGrad5, kSlotGrad6, kSlotGrad7,
   kSlotCount
 };
 
@@ -142,6 +143,9 @@ struct Basis {
   std::vector<std::pair<int, int>> orders;  // (nx, ny) per component
   Basis(double beta, int n_max, int radius);  // radius <= 0 -> default
   std::vector<float> taps() const;   // float32 (n_max+1) x ks
+  // The 1-D functions sampled at the offsets shifted by d, g_n(u - d), and
+  // their derivatives g_n'(u - d) (FP64, (n_max+1) x ks each).
+  void shifted_taps(double d, std::vector<double>& g, std::vector<double>& dg) const;
   std::vector<float> kernel2d(int c) const;
   std::vector<double> component_sums() const;
 };
@@ -186,6 +190,8 @@ struct DevFields {
   const float* wx = nullptr;     // w
   const int* celly = nullptr;    // h
   const float* wy = nullptr;     // h
+  const int* gx = nullptr;       // coarse: lattice x coordinates (ncx)
+  const int* gy = nullptr;       // coarse: lattice y coordinates (ncy)
 };
 
 // Evaluate the fields of `theta` (host) on the device.

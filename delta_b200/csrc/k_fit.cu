@@ -48,8 +48,10 @@ k_stamp_gather(StampGeom g, const int* __restrict__ stamp_x, const int* __restri
                const float* __restrict__ sci, const float* __restrict__ ref,
                const float* __restrict__ vs, const float* __restrict__ vr,
                const uint8_t* __restrict__ sm, const uint8_t* __restrict__ rm,
-               const float* __restrict__ taps, const int2* __restrict__ orders,
+               const float* __restrict__ taps, const float* __restrict__ taps_y, const int2* __restrict__ orders,
                const float* __restrict__ fillp, FitRows R) {
+  // taps_y: the y-pass table (the same as taps for the plain basis; a
+  // different one for the shifted / derivative basis of the gradients).
   extern __shared__ __align__(16) float fsm[];
   const int s = blockIdx.x;
   const int tid = threadIdx.x;
@@ -79,9 +81,13 @@ k_stamp_gather(StampGeom g, const int* __restrict__ stamp_x, const int* __restri
   const int sw = x1 - x0 + 1, shh = y1 - y0 + 1;
   float* patch = fsm;                           // ph x pw
   float* tx = patch + g.pmax * g.pmax;          // NX x ph x sw
-  float* kt = tx + NX * g.pmax * g.S;           // NX x ks
+  float* kt = tx + NX * g.pmax * g.S;           // NX x ks (x pass)
+  float* kty = kt + NX * ks;                    // NX x ks (y pass)
   const float fill = *fillp;
-  for (int i = tid; i < NX * ks; i += blockDim.x) kt[i] = taps[i];
+  for (int i = tid; i < NX * ks; i += blockDim.x) {
+    kt[i] = taps[i];
+    kty[i] = taps_y[i];
+  }
   for (int i = tid; i < ph * pw; i += blockDim.x) {
     const int yy = i / pw, xx = i - yy * pw;
     const size_t idx = static_cast<size_t>(ey0 + yy) * g.w + ex0 + xx;
@@ -125,7 +131,7 @@ k_stamp_gather(StampGeom g, const int* __restrict__ stamp_x, const int* __restri
     bool fin = true;
     for (int n = 0; n < nc; ++n) {
       const int2 o = orders[n];
-      const float* ky = kt + o.y * ks;
+      const float* ky = kty + o.y * ks;
       const float* col = tx + static_cast<size_t>(o.x) * ph * sw + lx;
       float acc = 0.0f;
       for (int j = 0; j < ks; ++j) {
@@ -157,24 +163,26 @@ template <int NX>
 static void launch_gather_t(cudaStream_t st, const StampGeom& g, size_t smem, int n_stamps,
                             const int* sx, const int* sy, const float* sci, const float* ref,
                             const float* vs, const float* vr, const uint8_t* sm, const uint8_t* rm,
-                            const float* taps, const int2* orders, const float* fill, const FitRows& R) {
+                            const float* taps, const float* taps_y, const int2* orders, const float* fill,
+                            const FitRows& R) {
   auto kern = k_stamp_gather<NX>;
   ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
-  kern<<<n_stamps, 256, smem, st>>>(g, sx, sy, sci, ref, vs, vr, sm, rm, taps, orders, fill, R);
+  kern<<<n_stamps, 256, smem, st>>>(g, sx, sy, sci, ref, vs, vr, sm, rm, taps, taps_y, orders, fill, R);
   DGPU_LAUNCH("k_stamp_gather");
 }
 
 void launch_stamp_gather(cudaStream_t st, const StampGeom& g, int n_stamps, const int* sx, const int* sy,
                          const float* sci, const float* ref, const float* vs, const float* vr,
                          const uint8_t* sm, const uint8_t* rm, const float* taps, const int2* orders,
-                         const float* fill, const FitRows& R) {
+                         const float* fill, const FitRows& R, const float* taps_y) {
   if (n_stamps == 0) return;
+  if (taps_y == nullptr) taps_y = taps;
   const int nx = g.n_max + 1;
   const size_t smem = sizeof(float) * (static_cast<size_t>(g.pmax) * g.pmax +
-                                       static_cast<size_t>(nx) * g.pmax * g.S + static_cast<size_t>(nx) * g.ks);
+                                       static_cast<size_t>(nx) * g.pmax * g.S + 2 * static_cast<size_t>(nx) * g.ks);
   if (smem > 200 * 1024) fail(DGPU_ERR_INVALID, "fit_kernel: stamp + kernel footprint too large");
   switch (nx) {
-#define DGPU_G(N) case N: launch_gather_t<N>(st, g, smem, n_stamps, sx, sy, sci, ref, vs, vr, sm, rm, taps, orders, fill, R); break;
+#define DGPU_G(N) case N: launch_gather_t<N>(st, g, smem, n_stamps, sx, sy, sci, ref, vs, vr, sm, rm, taps, taps_y, orders, fill, R); break;
     DGPU_G(1) DGPU_G(2) DGPU_G(3) DGPU_G(4) DGPU_G(5) DGPU_G(6) DGPU_G(7) DGPU_G(8) DGPU_G(9) DGPU_G(10) DGPU_G(11)
 #undef DGPU_G
     default: fail(DGPU_ERR_INVALID, "fit_kernel: n_max above 10 is not supported");

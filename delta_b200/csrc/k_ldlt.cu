@@ -67,16 +67,154 @@ __device__ double block_sum(double v, double* red) {
 
 }  // namespace
 
+// Block-shared scratch of the factorisation and solves.
+struct LdltShared {
+  double temp[1024];  // d_j L_kj of the current step; later a solve vector
+  double red[33];
+  double best[32];
+  int bidx[32];
+  int piv;
+  double dk;
+  int perm[1024];  // position -> original index
+};
+
+// A = M + lambda P0 (P0 = one k x k penalty block per field); perm = identity.
+__device__ void build_penalised(double* A, const double* M, int P, int kk, double lam, const double* pen, int* perm) {
+  const size_t PP = static_cast<size_t>(P) * P;
+  for (size_t e = threadIdx.x; e < PP; e += blockDim.x) {
+    const int i = static_cast<int>(e / P), j = static_cast<int>(e - static_cast<size_t>(i) * P);
+    double v = M[e];
+    if (i / kk == j / kk) v = fma(lam, pen[(i % kk) * kk + (j % kk)], v);
+    A[e] = v;
+  }
+  for (int i = threadIdx.x; i < P; i += blockDim.x) perm[i] = i;
+  __syncthreads();
+}
+
+// Eigen's pivoted LDL^T of A in place (L below the diagonal, D on it; S.perm
+// the composed permutation). Returns the number of steps (0 for an all-zero
+// diagonal, where nothing is factored and D counts as zero).
+__device__ int ldlt_factor_block(double* A, int P, LdltShared& S) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  for (int k = 0; k < P; ++k) {
+    // Pivot: largest |A_ii| over i >= k, first on ties.
+    double best = -1.0;
+    int bi = P;
+    for (int i = k + tid; i < P; i += blockDim.x) {
+      const double v = fabs(A[static_cast<size_t>(i) * P + i]);
+      if (v > best) {
+        best = v;
+        bi = i;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ov > best || (ov == best && oi < bi)) {
+        best = ov;
+        bi = oi;
+      }
+    }
+    if (lane == 0) {
+      S.best[warp] = best;
+      S.bidx[warp] = bi;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double bb = S.best[0];
+      int ii = S.bidx[0];
+      for (int w = 1; w < nwarp; ++w)
+        if (S.best[w] > bb || (S.best[w] == bb && S.bidx[w] < ii)) {
+          bb = S.best[w];
+          ii = S.bidx[w];
+        }
+      S.piv = (k == 0 && !(bb > 0.0)) ? -1 : (ii < P ? ii : k);
+    }
+    __syncthreads();
+    const int piv = S.piv;
+    if (piv < 0) return 0;
+    if (piv != k) {
+      for (int j = tid; j < P; j += blockDim.x) {
+        const double t = A[static_cast<size_t>(k) * P + j];
+        A[static_cast<size_t>(k) * P + j] = A[static_cast<size_t>(piv) * P + j];
+        A[static_cast<size_t>(piv) * P + j] = t;
+      }
+      __syncthreads();
+      for (int i = tid; i < P; i += blockDim.x) {
+        const double t = A[static_cast<size_t>(i) * P + k];
+        A[static_cast<size_t>(i) * P + k] = A[static_cast<size_t>(i) * P + piv];
+        A[static_cast<size_t>(i) * P + piv] = t;
+      }
+      if (tid == 0) {
+        const int t = S.perm[k];
+        S.perm[k] = S.perm[piv];
+        S.perm[piv] = t;
+      }
+      __syncthreads();
+    }
+    const double* Ak = A + static_cast<size_t>(k) * P;
+    double part = 0.0;
+    for (int j = tid; j < k; j += blockDim.x) {
+      const double t = A[static_cast<size_t>(j) * P + j] * Ak[j];
+      S.temp[j] = t;
+      part = fma(Ak[j], t, part);
+    }
+    const double red = block_sum(part, S.red);  // synchronises: temp complete
+    if (tid == 0) {
+      const double dk = Ak[k] - red;
+      A[static_cast<size_t>(k) * P + k] = dk;
+      S.dk = dk;
+    }
+    __syncthreads();
+    const double dk = S.dk;
+    for (int i = k + 1 + warp; i < P; i += nwarp) {
+      const double* Ai = A + static_cast<size_t>(i) * P;
+      double acc = 0.0;
+      for (int j = lane; j < k; j += 32) acc = fma(Ai[j], S.temp[j], acc);
+      acc = warp_sum(acc);
+      if (lane == 0) {
+        const double v = Ai[k] - acc;
+        A[static_cast<size_t>(i) * P + k] = dk != 0.0 ? v / dk : v;
+      }
+    }
+    __syncthreads();
+  }
+  return P;
+}
+
+// Pseudo-inverse of D.
+__device__ void ldlt_dinv(const double* A, int P, int n_steps, double* dinv) {
+  for (int i = threadIdx.x; i < P; i += blockDim.x) {
+    const double d = n_steps ? A[static_cast<size_t>(i) * P + i] : 0.0;
+    dinv[i] = fabs(d) > DBL_MIN ? 1.0 / d : 0.0;
+  }
+  __syncthreads();
+}
+
+// One thread's column solve: Y[:, c] = L^-T D^+ L^-1 (Pi b) in the permuted
+// order, b_i = rhs(original row i). Rows above `stop` of the backward pass are
+// left unfinished (the trace needs only Y[c][c]).
+template <class Rhs>
+__device__ void ldlt_solve_col(const double* A, int P, const int* perm, const double* dinv, Rhs rhs, double* Y,
+                               int ldy, int c, int stop) {
+  for (int i = 0; i < P; ++i) {
+    const double* Ai = A + static_cast<size_t>(i) * P;
+    double v = rhs(perm[i]);
+    for (int j = 0; j < i; ++j) v = fma(-Ai[j], Y[static_cast<size_t>(j) * ldy + c], v);
+    Y[static_cast<size_t>(i) * ldy + c] = v;
+  }
+  for (int i = 0; i < P; ++i) Y[static_cast<size_t>(i) * ldy + c] *= dinv[i];
+  for (int i = P - 1; i >= stop; --i) {
+    double v = Y[static_cast<size_t>(i) * ldy + c];
+    for (int t = i + 1; t < P; ++t) v = fma(-A[static_cast<size_t>(t) * P + i], Y[static_cast<size_t>(t) * ldy + c], v);
+    Y[static_cast<size_t>(i) * ldy + c] = v;
+  }
+}
+
 __global__ void __launch_bounds__(kLdltThreads) k_ldlt_fallback(SolveBatch b, double* __restrict__ work) {
-  __shared__ double s_temp[1024];  // d_j L_kj of the current step; later the solve vector
-  __shared__ double s_red[33];
-  __shared__ double s_best[32];
-  __shared__ int s_bidx[32];
-  __shared__ int s_piv;
-  __shared__ double s_dk;
-  __shared__ int s_perm[1024];  // position -> original index
-  const int P = b.P, kk = b.k, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int nwarp = blockDim.x >> 5;
+  __shared__ LdltShared S;
+  const int P = b.P, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const size_t PP = static_cast<size_t>(P) * P;
   double* A = work + static_cast<size_t>(blockIdx.x) * (2 * PP + P);
   double* Y = A + PP;
@@ -86,111 +224,9 @@ __global__ void __launch_bounds__(kLdltThreads) k_ldlt_fallback(SolveBatch b, do
     const double lam = b.lam[s];
     const double* M = b.M + static_cast<size_t>(b.m_index ? b.m_index[s] : 0) * PP;
     const double* rhs = b.rhs + static_cast<size_t>(b.r_index ? b.r_index[s] : 0) * P;
-    // A = M + lambda P0 (P0 = one k x k penalty block per field).
-    for (size_t e = tid; e < PP; e += blockDim.x) {
-      const int i = static_cast<int>(e / P), j = static_cast<int>(e - static_cast<size_t>(i) * P);
-      double v = M[e];
-      if (i / kk == j / kk) v = fma(lam, b.pen[(i % kk) * kk + (j % kk)], v);
-      A[e] = v;
-    }
-    for (int i = tid; i < P; i += blockDim.x) s_perm[i] = i;
-    __syncthreads();
-
-    int n_steps = P;
-    for (int k = 0; k < P; ++k) {
-      // Pivot: largest |A_ii| over i >= k, first on ties.
-      double best = -1.0;
-      int bi = P;
-      for (int i = k + tid; i < P; i += blockDim.x) {
-        const double v = fabs(A[static_cast<size_t>(i) * P + i]);
-        if (v > best) {
-          best = v;
-          bi = i;
-        }
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ov > best || (ov == best && oi < bi)) {
-          best = ov;
-          bi = oi;
-        }
-      }
-      if (lane == 0) {
-        s_best[warp] = best;
-        s_bidx[warp] = bi;
-      }
-      __syncthreads();
-      if (tid == 0) {
-        double bb = s_best[0];
-        int ii = s_bidx[0];
-        for (int w = 1; w < nwarp; ++w)
-          if (s_best[w] > bb || (s_best[w] == bb && s_bidx[w] < ii)) {
-            bb = s_best[w];
-            ii = s_bidx[w];
-          }
-        // An all-zero diagonal at the first step: nothing to factor (D = 0).
-        s_piv = (k == 0 && !(bb > 0.0)) ? -1 : (ii < P ? ii : k);
-      }
-      __syncthreads();
-      const int piv = s_piv;
-      if (piv < 0) {
-        n_steps = 0;
-        break;
-      }
-      if (piv != k) {
-        for (int j = tid; j < P; j += blockDim.x) {
-          const double t = A[static_cast<size_t>(k) * P + j];
-          A[static_cast<size_t>(k) * P + j] = A[static_cast<size_t>(piv) * P + j];
-          A[static_cast<size_t>(piv) * P + j] = t;
-        }
-        __syncthreads();
-        for (int i = tid; i < P; i += blockDim.x) {
-          const double t = A[static_cast<size_t>(i) * P + k];
-          A[static_cast<size_t>(i) * P + k] = A[static_cast<size_t>(i) * P + piv];
-          A[static_cast<size_t>(i) * P + piv] = t;
-        }
-        if (tid == 0) {
-          const int t = s_perm[k];
-          s_perm[k] = s_perm[piv];
-          s_perm[piv] = t;
-        }
-        __syncthreads();
-      }
-      const double* Ak = A + static_cast<size_t>(k) * P;
-      double part = 0.0;
-      for (int j = tid; j < k; j += blockDim.x) {
-        const double t = A[static_cast<size_t>(j) * P + j] * Ak[j];
-        s_temp[j] = t;
-        part = fma(Ak[j], t, part);
-      }
-      const double red = block_sum(part, s_red);  // synchronises: s_temp complete
-      if (tid == 0) {
-        const double dk = Ak[k] - red;
-        A[static_cast<size_t>(k) * P + k] = dk;
-        s_dk = dk;
-      }
-      __syncthreads();
-      const double dk = s_dk;
-      for (int i = k + 1 + warp; i < P; i += nwarp) {
-        const double* Ai = A + static_cast<size_t>(i) * P;
-        double acc = 0.0;
-        for (int j = lane; j < k; j += 32) acc = fma(Ai[j], s_temp[j], acc);
-        acc = warp_sum(acc);
-        if (lane == 0) {
-          const double v = Ai[k] - acc;
-          A[static_cast<size_t>(i) * P + k] = dk != 0.0 ? v / dk : v;
-        }
-      }
-      __syncthreads();
-    }
-    // Pseudo-inverse of D.
-    for (int i = tid; i < P; i += blockDim.x) {
-      const double d = n_steps ? A[static_cast<size_t>(i) * P + i] : 0.0;
-      dinv[i] = fabs(d) > DBL_MIN ? 1.0 / d : 0.0;
-    }
-    __syncthreads();
+    build_penalised(A, M, P, b.k, lam, b.pen, S.perm);
+    const int n_steps = ldlt_factor_block(A, P, S);
+    ldlt_dinv(A, P, n_steps, dinv);
 
     // theta: x = Pi rhs; forward L (unit, row-oriented, one warp); D^+;
     // backward L^T (column t of L^T = row t of L, the block over i < t).
@@ -198,53 +234,69 @@ __global__ void __launch_bounds__(kLdltThreads) k_ldlt_fallback(SolveBatch b, do
       for (int i = 0; i < P; ++i) {
         const double* Ai = A + static_cast<size_t>(i) * P;
         double acc = 0.0;
-        for (int j = lane; j < i; j += 32) acc = fma(Ai[j], s_temp[j], acc);
+        for (int j = lane; j < i; j += 32) acc = fma(Ai[j], S.temp[j], acc);
         acc = warp_sum(acc);
-        if (lane == 0) s_temp[i] = rhs[s_perm[i]] - acc;
+        if (lane == 0) S.temp[i] = rhs[S.perm[i]] - acc;
         __syncwarp();
       }
     }
     __syncthreads();
-    for (int i = tid; i < P; i += blockDim.x) s_temp[i] *= dinv[i];
+    for (int i = tid; i < P; i += blockDim.x) S.temp[i] *= dinv[i];
     __syncthreads();
     for (int t = P - 1; t > 0; --t) {
-      const double zt = s_temp[t];
+      const double zt = S.temp[t];
       const double* At = A + static_cast<size_t>(t) * P;
-      for (int i = tid; i < t; i += blockDim.x) s_temp[i] = fma(-At[i], zt, s_temp[i]);
+      for (int i = tid; i < t; i += blockDim.x) S.temp[i] = fma(-At[i], zt, S.temp[i]);
       __syncthreads();
     }
-    for (int i = tid; i < P; i += blockDim.x) b.theta[static_cast<size_t>(s) * P + s_perm[i]] = s_temp[i];
+    for (int i = tid; i < P; i += blockDim.x) b.theta[static_cast<size_t>(s) * P + S.perm[i]] = S.temp[i];
 
     // edf = tr(A^+ M) = sum_c Z_cc, Z = L^-T D^+ L^-1 B, B = Pi M Pi^T; thread c owns column c.
     double zc = 0.0;
     if (tid < P) {
-      const int c = tid, oc = s_perm[c];
-      for (int i = 0; i < P; ++i) {
-        const double* Ai = A + static_cast<size_t>(i) * P;
-        double v = M[static_cast<size_t>(s_perm[i]) * P + oc];  // B = Pi M Pi^T: the trace is of A^+ M
-        for (int j = 0; j < i; ++j) v = fma(-Ai[j], Y[static_cast<size_t>(j) * P + c], v);
-        Y[static_cast<size_t>(i) * P + c] = v;
-      }
-      for (int i = 0; i < P; ++i) Y[static_cast<size_t>(i) * P + c] *= dinv[i];
-      for (int i = P - 1; i >= c; --i) {
-        double v = Y[static_cast<size_t>(i) * P + c];
-        for (int t = i + 1; t < P; ++t) v = fma(-A[static_cast<size_t>(t) * P + i], Y[static_cast<size_t>(t) * P + c], v);
-        Y[static_cast<size_t>(i) * P + c] = v;
-      }
+      const int c = tid, oc = S.perm[c];
+      ldlt_solve_col(A, P, S.perm, dinv, [&](int io) { return M[static_cast<size_t>(io) * P + oc]; }, Y, P, c, c);
       zc = Y[static_cast<size_t>(c) * P + c];
     }
     // Fixed-order sum over the columns.
     __syncthreads();
-    s_temp[tid] = tid < P ? zc : 0.0;
+    S.temp[tid] = tid < P ? zc : 0.0;
     __syncthreads();
     if (tid == 0) {
       double e = 0.0;
-      for (int c = 0; c < P; ++c) e += s_temp[c];
+      for (int c = 0; c < P; ++c) e += S.temp[c];
       b.edf[s] = e;
       b.ok[s] = 2;
     }
     __syncthreads();
   }
+}
+
+// X = A^+ B for A = M + lambda P0 (one CTA): B and X are P x m, row-major, in
+// the original order; Y is a P x m workspace. The same factorisation as the
+// fallback; used where many right-hand sides share one system.
+__global__ void __launch_bounds__(kLdltThreads) k_sym_solve_many(int P, int kk, const double* __restrict__ M, double lam,
+                                                                 const double* __restrict__ pen, const double* __restrict__ B,
+                                                                 int m, double* __restrict__ A, double* __restrict__ Y,
+                                                                 double* __restrict__ dinv, double* __restrict__ X) {
+  __shared__ LdltShared S;
+  build_penalised(A, M, P, kk, lam, pen, S.perm);
+  const int n_steps = ldlt_factor_block(A, P, S);
+  ldlt_dinv(A, P, n_steps, dinv);
+  for (int c = threadIdx.x; c < m; c += blockDim.x) {
+    ldlt_solve_col(A, P, S.perm, dinv, [&](int io) { return B[static_cast<size_t>(io) * m + c]; }, Y, m, c, 0);
+    for (int i = 0; i < P; ++i) X[static_cast<size_t>(S.perm[i]) * m + c] = Y[static_cast<size_t>(i) * m + c];
+  }
+}
+
+void launch_sym_solve_many(Context& c, int P, int k, const double* M, double lam, const double* pen, const double* B,
+                           int m, double* X) {
+  if (P > kLdltThreads) fail(DGPU_ERR_INVALID, "solve: at most 1024 unknowns are supported");
+  double* work = static_cast<double*>(
+      c.slot(kSlotGrad6, sizeof(double) * (static_cast<size_t>(P) * P + static_cast<size_t>(P) * m + P)));
+  k_sym_solve_many<<<1, kLdltThreads, 0, c.stream>>>(P, k, M, lam, pen, B, m, work, work + static_cast<size_t>(P) * P,
+                                                     work + static_cast<size_t>(P) * P + static_cast<size_t>(P) * m, X);
+  DGPU_LAUNCH("k_sym_solve_many");
 }
 
 void launch_ldlt_fallback(Context& c, const SolveBatch& b) {

@@ -208,6 +208,8 @@ DevFields build_fields_dev(Context& c, const ThinPlate& tp, const double* d_thet
   launch_lattice(c.stream, t, d_theta, nf, di, di + g.ncx, g.ncx, g.ncy, lat, latf);
   F.lat = lat;
   F.latf = latf;
+  F.gx = di;
+  F.gy = di + g.ncx;
   F.cellx = di + g.ncx + g.ncy;
   F.celly = di + g.ncx + g.ncy + w;
   F.wx = df;

@@ -244,6 +244,44 @@ int dgpu_solve_gls_cv(dgpu_context* ctx, const double* knots, int n_knots, const
                       const double* lambda_grid, int n_lambda, const int32_t* group, int n_groups,
                       int precision, dgpu_gls_result* out);
 
+/* ---- differentiation: weighted chi^2 of the kernel model -------------------------- */
+/* No reference counterpart (the reference has no gradient code). The model is
+ * the subtraction's (src/subtract.cpp:466-639, the same sanitised reference,
+ * lattice-blended fields and basis) with the kernel shifted by (dx, dy) pixels
+ * and its convolved part scaled by `scale`:
+ *   M = scale * sum_c a_c(x) [g_nx(u - dx) g_ny(v - dy) (*) R~](x) + b(x),
+ *   chi2 = sum_x W(x) (S(x) - M(x))^2 over pixels with W > 0 and a finite S.
+ * Images follow `mem`; weights (W) is float32 h x w, 0 excluding a pixel;
+ * reference_mask may be NULL. Outputs (host): chi2; the gradients are
+ * optional (NULL skips them): grad_theta (n_theta, same layout as theta),
+ * grad_shift (2: d/ddx, d/ddy), grad_scale (1), and grad_reference (h x w
+ * float32, follows `mem`; the correlation of the field-weighted residual with
+ * the flipped kernel field, 0 where the reference was replaced by the fill
+ * value, which is held constant). The convolved basis images are recomputed
+ * per tile, never stored. n_max <= 8. */
+int dgpu_kernel_chi2(dgpu_context* ctx, int mem, int64_t width, int64_t height, const float* science,
+                     const float* reference, const uint8_t* reference_mask, const float* weights,
+                     const dgpu_model* model, double dx, double dy, double scale, double* chi2, double* grad_theta,
+                     double* grad_shift, double* grad_scale, float* grad_reference);
+
+/* GCV score of the stamp fit as a function of log lambda, the kernel shift and
+ * the scale, with its gradient through the adjoint of the normal-equation map
+ * (no reference counterpart). The stamp rows are fit_kernel's
+ * (src/fit.cpp:63-229, first-pass weights 1 / (Var_t + Var_c), no clipping)
+ * with every B_n convolved with the basis shifted by (dx, dy) and scaled by
+ * `scale`; the solve at lambda = exp(log_lambda) is the reference's solve_at
+ * (src/solve.cpp:147-193): GCV = n RSS / (n - edf)^2. Images follow `mem`;
+ * knots and stamp lists are host arrays. Outputs (host): values[4] = {gcv,
+ * rss, edf, n}; theta ((nc+1)*k, optional); grad_gcv[4] and grad_rss[4]
+ * (optional) = d/d{log lambda, dx, dy, scale} of GCV and of the weighted RSS.
+ * At most 32 knots. */
+int dgpu_stamp_gcv(dgpu_context* ctx, int mem, int64_t width, int64_t height, const float* science,
+                   const float* reference, const float* science_var, const float* reference_var,
+                   const uint8_t* science_mask, const uint8_t* reference_mask, const double* knots, int n_knots,
+                   const int32_t* stamp_x, const int32_t* stamp_y, int n_stamps, int stamp_radius, double beta,
+                   int n_max, int radius, double log_lambda, double dx, double dy, double scale, double* values,
+                   double* theta, double* grad_gcv, double* grad_rss);
+
 /* ---- noise decorrelation (ZOGY) ------------------------------------------------ */
 /* decorrelate, src/bindings.cpp:766-792 -> delta::decorrelate, src/noise.cpp:228-483
  * (include/delta/noise.hpp:64-68). Outputs: whitened difference and its
