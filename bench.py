@@ -12,9 +12,11 @@ synthetic frames (each rank its own seed: weak scaling, no collective on the
 data path).
 
   value   Mpix/s of the mixed-precision path, layers resident in HBM
-  plain   the same with the plain FP32 normal equations
+  plain   the same with the plain FP32 normal equations (one frame, and
+          the same frames in flight as `value`)
   e2e     the public delta_b200.subtract() call from pinned host arrays
           (host->device upload and device->host products inside the timing)
+  uneven  the batch of uneven frames below, mixed and plain FP32
 
 `--impl reference` times the CPU chain of the same workload instead (the
 reference's own detect/catalog/convolve code compiled from source plus the
@@ -77,8 +79,10 @@ def parse_args(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--batch", type=int, default=4, help="frames in flight per GPU (each its own stream)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU leg (rank 0, N=1)")
-    ap.add_argument("--workload", choices=("frame", "uneven"), default="frame",
-                    help="frame: the 4096^2 workload (default); uneven: 64 frames of mixed sizes")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch leg of the default run")
+    ap.add_argument("--workload", choices=("frame", "uneven", "precision"), default="frame",
+                    help="frame: the 4096^2 workload (default); uneven: 64 frames of mixed sizes; "
+                         "precision: the normal-equation precision study at 725 unknowns, ~4e6 rows")
     return ap.parse_args(argv)
 
 
@@ -557,11 +561,12 @@ def run_gpu(args) -> int:
     frame = frames[0]
     subs = {p: Subtractor(**subtract_kwargs(pair, p)) for p in ("mixed", "fp32", "fp64")}
     batch_subs = [Subtractor(**subtract_kwargs(p, "mixed")) for p in pairs]
+    plain_subs = [Subtractor(**subtract_kwargs(p, "fp32")) for p in pairs]
     ctx = _lib.context()
     ex = _device.runner(B)
 
-    def batch_step():
-        futs = [ex.submit(_device.on_own_stream, _device.run, sb, f) for sb, f in zip(batch_subs, frames, strict=True)]
+    def batch_step(subs_=batch_subs):
+        futs = [ex.submit(_device.on_own_stream, _device.run, sb, f) for sb, f in zip(subs_, frames, strict=True)]
         for f in futs:
             f.result()
 
@@ -584,10 +589,13 @@ def run_gpu(args) -> int:
     stages = drain_stage_seconds(ctx)
     _lib.lib().dgpu_set_timing(ctx.handle, 0)
 
-    # plain: FP32 normal equations, one frame at a time
+    # plain: FP32 normal equations, one frame at a time and B frames in flight
     for _ in range(args.warmup):
         _device.run(subs["fp32"], frame)
     ms_plain = timed_steps(lambda: _device.run(subs["fp32"], frame), args.steps, device)
+    for _ in range(args.warmup):
+        batch_step(plain_subs)
+    ms_plain_batched = timed_steps(lambda: batch_step(plain_subs), args.steps, device)
 
     # end to end through the public batch API from pinned host arrays
     layer_names = ("science", "reference", "science_var", "reference_var", "science_mask", "reference_mask")
@@ -611,6 +619,10 @@ def run_gpu(args) -> int:
     out_plain = _device.run(subs["fp32"], frame)
     errors = {"mixed": error_vs_fp64(out_mixed, out64), "plain": error_vs_fp64(out_plain, out64)}
 
+    uneven = None
+    if not args.no_uneven:
+        uneven = uneven_batch(args, rank, world, device, precisions=("mixed", "fp32"))
+
     mpix = size * size / 1e6
     value = world * args.steps * B * mpix / (ms / 1e3)
     line = None
@@ -618,26 +630,28 @@ def run_gpu(args) -> int:
         peaks, peak_kind = load_peaks()
         t_conv = stages.get(MODEL_CONVOLVE_STAGE)
         roofline = None
-        if t_conv:
-            per_launch = t_conv / args.steps
-            bytes_launch = MODEL_CONVOLVE_BYTES_PER_PX * size * size
-            achieved = bytes_launch / per_launch / 1e9
-            roofline = {"bound": "hbm", "kernel": "k_model_convolve", "achieved": achieved,
-                        "peak": float(peaks["hbm_gbs"]), "unit": "GB/s", "frac": achieved / float(peaks["hbm_gbs"]),
-                        "traffic": load_traffic(MODEL_CONVOLVE_STAGE, size), "peak_source": peak_kind,
-                        "algorithmic_bytes_per_launch": bytes_launch, "ms_per_launch": 1e3 * per_launch,
-                        "timed_in": "the one-frame-at-a-time mixed pass"}
-            sol = out64.get("solution")
-            if sol is not None:
-                from delta_b200 import _core
+        sol = out64.get("solution")
+        if t_conv and sol is not None:
+            from delta_b200 import _core
 
-                radius = int(_core._resolve_radius(float(sol.beta), int(sol.n_max), int(sol.radius)))
-                fma = model_convolve_fma_per_px(int(sol.n_max), radius) * size * size
-                tfma = fma / per_launch / 1e12
-                roofline["compute"] = {"bound": "fp32_fma", "achieved_tfma_s": tfma,
-                                       "peak_tfma_s": FP32_FMA_PEAK_TFMA, "frac": tfma / FP32_FMA_PEAK_TFMA,
-                                       "fma_per_launch": fma,
-                                       "note": "the kernel is FP32-issue-bound; HBM is not its limit"}
+            # The model convolve is FP32-FMA bound (about 68 FMA per HBM byte),
+            # so its FP32 rate is the primary roofline; its HBM rate sits beside it.
+            per_launch = t_conv / args.steps
+            radius = int(_core._resolve_radius(float(sol.beta), int(sol.n_max), int(sol.radius)))
+            fma = model_convolve_fma_per_px(int(sol.n_max), radius) * size * size
+            tflops = 2.0 * fma / per_launch / 1e12
+            peak_tflops = 2.0 * FP32_FMA_PEAK_TFMA
+            bytes_launch = MODEL_CONVOLVE_BYTES_PER_PX * size * size
+            gbs = bytes_launch / per_launch / 1e9
+            roofline = {"bound": "fp32", "kernel": "k_model_convolve", "achieved": tflops, "peak": peak_tflops,
+                        "unit": "TFLOP/s", "frac": tflops / peak_tflops,
+                        "traffic": load_traffic(MODEL_CONVOLVE_STAGE, size),
+                        "peak_source": "nominal FP32 (148 SMs x 128 lanes x 2 FLOP x 1.965 GHz); no measured FP32 peak",
+                        "algorithmic_flop_per_launch": 2.0 * fma, "ms_per_launch": 1e3 * per_launch,
+                        "timed_in": "the one-frame-at-a-time mixed pass",
+                        "hbm": {"achieved": gbs, "peak": float(peaks["hbm_gbs"]), "unit": "GB/s",
+                                "frac": gbs / float(peaks["hbm_gbs"]), "peak_source": peak_kind,
+                                "algorithmic_bytes_per_launch": bytes_launch}}
         cpu, oracle_errors = None, None
         if world == 1 and not args.no_cpu_baseline:
             cpu, want = cpu_baseline(pair, size)
@@ -655,6 +669,10 @@ def run_gpu(args) -> int:
                        "precision": "mixed", "frames_in_flight": 1},
             "plain": {"value": world * args.steps * mpix / (ms_plain / 1e3), "ms_per_step": ms_plain / args.steps,
                       "precision": "fp32", "frames_in_flight": 1},
+            "plain_batched": {"value": world * args.steps * B * mpix / (ms_plain_batched / 1e3),
+                              "ms_per_step": ms_plain_batched / args.steps, "precision": "fp32",
+                              "frames_in_flight": B},
+            "uneven": None if uneven is None else {"workload": UNEVEN_WORKLOAD, **uneven},
             "error_vs_fp64": errors,
             "error_vs_oracle": oracle_errors,
             "roofline": roofline,
@@ -674,22 +692,13 @@ def run_gpu(args) -> int:
     return 0
 
 
-def run_uneven(args) -> int:
+def uneven_batch(args, rank: int, world: int, device, precisions=("mixed",)) -> dict:
     """The uneven batch through delta_b200's Subtractor.subtract (the call
     subtract_batch makes per frame) on `--batch` worker streams, from pinned
-    host arrays; wall clock with a device synchronize and barrier on both sides."""
+    host arrays; wall clock with a device synchronize and barrier on both
+    sides, per precision. Returns {precision: stats} (rank 0's latencies)."""
     import torch
-    import torch.distributed as dist
 
-    rank, world, local = rank_env()
-    if not torch.cuda.is_available():
-        raise SystemExit("bench.py needs a CUDA device (the product path has no CPU fallback)")
-    torch.cuda.set_device(local)
-    device = torch.device("cuda", local)
-    if world > 1:
-        from datetime import timedelta
-
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
     from delta_b200 import _device, validation
     from delta_b200.pipeline import Subtractor
 
@@ -707,56 +716,158 @@ def run_uneven(args) -> int:
                                       mask_fraction=sp["mask_fraction"])
         host[j] = {k: pinned_copy(getattr(p, k)) for k in names}
         first = first or p
-    # Every frame of the generator has the same gain and saturation level.
-    sub = Subtractor(**subtract_kwargs(first, "mixed")) if first is not None else None
-    lat = {}
-
-    def one(q, record):
-        t0 = time.perf_counter()
-        sub.subtract(**host[queue[q]])
-        if record:
-            lat[q] = (time.perf_counter() - t0) * 1e3
-
-    ex = _device.runner(max(1, args.batch))
-    warm: dict[int, int] = {}
-    for q in mine:
-        warm.setdefault(queue[q], q)
-    # Untimed: the largest frame on every worker at once (each worker context's
-    # workspace grows to its final size, as in a long-running service), then
-    # each distinct frame once.
-    if warm:
-        big = max(warm.values(), key=lambda q: specs[queue[q]]["height"] * specs[queue[q]]["width"])
-        for f in [ex.submit(_device.on_own_stream, one, big, False) for _ in range(max(1, args.batch))]:
-            f.result()
-    for f in [ex.submit(_device.on_own_stream, one, q, False) for q in warm.values()]:
-        f.result()
-    barrier(device)
-    torch.cuda.synchronize(device)
-    t0 = time.perf_counter()
-    for f in [ex.submit(_device.on_own_stream, one, q, True) for q in mine]:
-        f.result()
-    torch.cuda.synchronize(device)
-    wall = (time.perf_counter() - t0) * 1e3
-    barrier(device)
-    wall = max_over_ranks(wall, device)
     total_px = sum(specs[j]["height"] * specs[j]["width"] for j in queue)
-    ls = sorted(lat.values())
-    pct = (lambda f: ls[min(len(ls) - 1, int(round(f * (len(ls) - 1))))]) if ls else (lambda f: None)
+    ex = _device.runner(max(1, args.batch))
+    out = {}
+    for prec in precisions:
+        # Every frame of the generator has the same gain and saturation level.
+        sub = Subtractor(**subtract_kwargs(first, prec)) if first is not None else None
+        lat = {}
+
+        def one(q, record):
+            t0 = time.perf_counter()
+            sub.subtract(**host[queue[q]])
+            if record:
+                lat[q] = (time.perf_counter() - t0) * 1e3
+
+        warm: dict[int, int] = {}
+        for q in mine:
+            warm.setdefault(queue[q], q)
+        # Untimed: each distinct frame once on the workers (workspace grows
+        # stream-ordered inside the library, so no largest-frame-first warm-up
+        # is needed to keep growth out of the timed pass).
+        for f in [ex.submit(_device.on_own_stream, one, q, False) for q in warm.values()]:
+            f.result()
+        barrier(device)
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        for f in [ex.submit(_device.on_own_stream, one, q, True) for q in mine]:
+            f.result()
+        torch.cuda.synchronize(device)
+        wall = (time.perf_counter() - t0) * 1e3
+        barrier(device)
+        wall = max_over_ranks(wall, device)
+        ls = sorted(lat.values())
+        pct = (lambda f: ls[min(len(ls) - 1, int(round(f * (len(ls) - 1))))]) if ls else (lambda f: None)
+        out[prec] = {"value": total_px / 1e6 / (wall / 1e3), "unit": UNIT, "wall_ms": wall, "frames": len(queue),
+                     "latency_ms": {"p50": pct(0.5), "p99": pct(0.99), "max": ls[-1] if ls else None},
+                     "frames_in_flight": max(1, args.batch), "precision": prec}
+    return out
+
+
+UNEVEN_WORKLOAD = ("64 frames: 16 distinct seeded frames of 2048x4096, 2048x2048, 1024x4096, each queued 4 times; "
+                   "FWHM U(2,5), 500-20000 stars, 0-3% masked; n_max 6, 4x4 knots, GCV, decorrelate + score + CCL")
+
+
+def run_uneven(args) -> int:
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = rank_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device (the product path has no CPU fallback)")
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
+    stats = uneven_batch(args, rank, world, device)["mixed"]
     if rank == 0:
         print(json.dumps({
             "metric": "uneven batch: aggregate Mpix/s over 64 frames of mixed sizes, end to end", "unit": UNIT,
-            "value": total_px / 1e6 / (wall / 1e3), "n_gpus": world, "frames": len(queue), "wall_ms": wall,
-            "latency_ms": {"p50": pct(0.5), "p99": pct(0.99), "max": ls[-1] if ls else None, "rank": 0},
-            "frames_in_flight": max(1, args.batch), "higher_is_better": True, "scaling": "strong",
-            "dtype": "f32", "data": "synthetic (seeded generator)",
-            "config": {"workload": "64 frames: 16 distinct seeded frames of 2048x4096, 2048x2048, 1024x4096, each "
-                                   "queued 4 times; FWHM U(2,5), 500-20000 stars, 0-3% masked; n_max 6, 4x4 knots, "
-                                   "GCV, decorrelate + score + CCL", "precision": "mixed",
-                       "timing": "wall clock, device synchronize and barrier on both sides; untimed first: the "
-                                 "largest frame on every worker, then one pass over the distinct frames"}}),
-              flush=True)
+            "value": stats["value"], "n_gpus": world, "frames": stats["frames"], "wall_ms": stats["wall_ms"],
+            "latency_ms": {**stats["latency_ms"], "rank": 0}, "frames_in_flight": stats["frames_in_flight"],
+            "higher_is_better": True, "scaling": "strong", "dtype": "f32", "data": "synthetic (seeded generator)",
+            "config": {"workload": UNEVEN_WORKLOAD, "precision": "mixed",
+                       "timing": "wall clock, device synchronize and barrier on both sides; untimed first: one "
+                                 "pass over the distinct frames"}}), flush=True)
     if world > 1:
         dist.destroy_process_group()
+    return 0
+
+
+def precision_study(seed: int = 0, size: int = 4096, n_stamps: int = 4200, n_max: int = 6, n_knots: int = 5,
+                    stamp_radius: int = 15) -> dict:
+    """Normal-equation arithmetic at the 725-unknown shape (n_max 6: 28
+    components, 5 x 5 knots) over about 4e6 stamp rows of the 4096^2 field:
+    FP32 SIMT, TF32 and BF16x3 tensor-core builds (the latter two with their
+    FP64 refinement step) and the device FP64 path, each against the FP64
+    oracle's fit of the same rows (oracle.numpy_ref.fit_kernel with the C GLS
+    solve, B_n through the reference's own convolve.cpp). Reported per
+    precision: ||theta - theta0|| / ||theta0||, the selected lambda, and the
+    difference image and matched-filter score of its theta against those of
+    the oracle's theta (RMS and max of dD / sigma, max |dscore|), where both
+    images come from the same device subtraction so only theta differs."""
+    import torch
+
+    from delta_b200 import _core
+    from oracle import cref, refbuild
+    from oracle import numpy_ref as nr
+
+    pair = make_frame(size, seed)
+    edge = stamp_radius + 25
+    xy, flux = pair.star_xy, pair.star_flux
+    inside = (xy[:, 0] > edge) & (xy[:, 0] < size - 1 - edge) & (xy[:, 1] > edge) & (xy[:, 1] < size - 1 - edge)
+    order = np.argsort(-flux[inside], kind="stable")
+    pick = xy[inside][order][:n_stamps]
+    sx = np.rint(pick[:, 0]).astype(np.int32)
+    sy = np.rint(pick[:, 1]).astype(np.int32)
+    sel = _core.select_stamps(pair.science, pair.reference, pair.science_mask, pair.reference_mask,
+                              stamp_radius=stamp_radius, saturation=pair.saturation)
+    beta = nr.default_beta(sel["median_fwhm_science"], sel["median_fwhm_reference"])
+    knots = nr.grid_knots(0.0, 0.0, size - 1.0, size - 1.0, n_knots, n_knots)
+    grid = np.logspace(-6.0, 6.0, 25)
+    layers = dict(science_var=pair.science_var, reference_var=pair.reference_var, science_mask=pair.science_mask,
+                  reference_mask=pair.reference_mask)
+    r = nr.resolve_radius(beta, n_max, 0)
+    t0 = time.perf_counter()
+    want = nr.fit_kernel(pair.science, pair.reference, knots, sx, sy, stamp_radius, beta, n_max, grid, radius=r,
+                         clip_iterations=0, basis_convolve_fn=lambda patch: refbuild.basis_convolve(patch, beta, n_max, r),
+                         gcv_solver=cref.gls_gcv, **layers)
+    oracle_s = time.perf_counter() - t0
+    theta0 = np.asarray(want["theta"])
+    sub0 = _core.subtract(pair.science, pair.reference, knots, theta0, beta, n_max, r, pair.saturation, **layers)
+    var0 = sub0["variance"].astype(np.float64)
+    good = (var0 > 0) & (sub0["mask"] == 0)
+    psf = _core.estimate_psf(pair.science, sel["x"], sel["y"], 8)
+    score0 = _core.matched_filter(sub0["difference"], psf, sub0["variance"]).astype(np.float64)
+    out = {"P": int(theta0.size), "n_stamps": int(sx.size), "n_rows": int(want["n_pixels"]),
+           "lambda_oracle": float(want["lambda"]), "oracle_seconds": round(oracle_s, 1), "modes": {}}
+    for prec in ("fp64", "fp32", "tf32", "mixed"):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        got = _core.fit_kernel(pair.science, pair.reference, knots, sx, sy, stamp_radius, beta, n_max, grid,
+                               radius=r, clip_iterations=0, precision=prec, **layers)
+        fit_ms = (time.perf_counter() - t1) * 1e3
+        th = np.asarray(got["theta"])
+        sub = _core.subtract(pair.science, pair.reference, knots, th, beta, n_max, r, pair.saturation, **layers)
+        z = (sub["difference"].astype(np.float64) - sub0["difference"])[good] / np.sqrt(var0[good])
+        sc = _core.matched_filter(sub["difference"], psf, sub["variance"]).astype(np.float64)
+        fin = np.isfinite(sc) & np.isfinite(score0)
+        out["modes"][prec] = {
+            "theta_rel": float(np.linalg.norm(th - theta0) / np.linalg.norm(theta0)),
+            "lambda_equal": bool(got["lambda"] == want["lambda"]), "precision_used": got["precision_used"],
+            "refine_correction": float(got["refine_correction"]),
+            "diff_rms_sigma": float(np.sqrt(np.mean(z * z))), "diff_max_sigma": float(np.max(np.abs(z))),
+            "score_max_abs": float(np.max(np.abs(sc - score0)[fin])), "fit_wall_ms": round(fit_ms, 1)}
+    return out
+
+
+def run_precision(args) -> int:
+    import torch
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device (the product path has no CPU fallback)")
+    rank, _, local = rank_env()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    study = precision_study(seed=args.seed, size=args.size)
+    print(json.dumps({"metric": "normal-equation precision study (errors against the FP64 oracle)",
+                      "config": {"workload": f"{args.size}x{args.size} spatially varying field, n_max 6, 5x5 knots, "
+                                             "stamps of radius 15 at the brightest catalogue stars, GCV, one pass"},
+                      **study}), flush=True)
     return 0
 
 
@@ -766,6 +877,8 @@ def main(argv=None) -> int:
         return run_reference(args)
     if args.workload == "uneven":
         return run_uneven(args)
+    if args.workload == "precision":
+        return run_precision(args)
     return run_gpu(args)
 
 

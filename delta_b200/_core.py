@@ -320,8 +320,9 @@ def photometric_scale_at(knots, theta, component_sums, points) -> np.ndarray:
 
 # Normal-equation arithmetic of fit_kernel / solve_gls* (the solve itself is
 # FP64 in every mode): "fp64" (default, accuracy reference), "fp32" (plain
-# FP32 SIMT), "mixed" (tensor-core split products + one FP64 refinement step).
-PRECISIONS = {"fp64": _lib.PREC_FP64, "fp32": _lib.PREC_FP32, "mixed": _lib.PREC_MIXED}
+# FP32 SIMT), "mixed" (BF16x3 tensor-core split products + one FP64 refinement step),
+# "tf32" (one TF32 tensor-core product + the same refinement step).
+PRECISIONS = {"fp64": _lib.PREC_FP64, "fp32": _lib.PREC_FP32, "mixed": _lib.PREC_MIXED, "tf32": _lib.PREC_TF32}
 _PREC_NAMES = {v: k for k, v in PRECISIONS.items()}
 _default_precision = "fp64"
 

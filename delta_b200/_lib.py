@@ -30,6 +30,7 @@ MEM_DEVICE = 1
 PREC_FP64 = 0
 PREC_FP32 = 1
 PREC_MIXED = 2
+PREC_TF32 = 3
 
 
 class DeviceUnavailableError(RuntimeError):

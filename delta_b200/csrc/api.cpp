@@ -102,6 +102,7 @@ int dgpu_create(int device, dgpu_context** out) {
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) fail(DGPU_ERR_NO_DEVICE, "no CUDA device");
     if (device < 0 || device >= n) fail(DGPU_ERR_INVALID, "device index out of range");
     DGPU_CUDA(cudaSetDevice(device));
+    keep_pool_memory(device);
     auto* c = new Context();
     c->device = device;
     DGPU_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
@@ -118,9 +119,9 @@ void dgpu_destroy(dgpu_context* ctx) {
   if (!ctx) return;
   auto* c = reinterpret_cast<Context*>(ctx);
   cudaSetDevice(c->device);
-  cudaStreamSynchronize(c->stream);
   for (int i = 0; i < kSlotCount; ++i)
-    if (c->slot_ptr[i]) cudaFree(c->slot_ptr[i]);
+    if (c->slot_ptr[i]) cudaFreeAsync(c->slot_ptr[i], c->stream);
+  cudaStreamSynchronize(c->stream);
   if (c->d_status) cudaFree(c->d_status);
   if (c->host_stage) cudaFreeHost(c->host_stage);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);

@@ -82,6 +82,11 @@ double median_copy(std::vector<double> v) {
   return v[mid];
 }
 
+// The tensor-core builds of the normal equations (BF16x3 "mixed", TF32): both
+// are refined by one FP64 step and fall back to FP64 when that step shows them
+// too inaccurate for the system.
+inline bool tensor_prec(int prec) { return prec == DGPU_PREC_MIXED || prec == DGPU_PREC_TF32; }
+
 struct GlsOut {
   std::vector<double> theta;
   double lambda = 0, gcv = 0, edf = 0, rss = 0;
@@ -257,7 +262,7 @@ struct Engine {
       return b;
     };
     int best = 0, anchored = -1;
-    if (prec == DGPU_PREC_MIXED) {
+    if (tensor_prec(prec)) {
       // Re-evaluate the curve around the provisional minimum until the minimum
       // stays put (it moves at most a grid step or two). The first anchor is
       // picked on the device, so both curves come back in one read.
@@ -299,7 +304,7 @@ struct Engine {
   // for the system's conditioning.
   static constexpr double kMixedFallback = 1e-2;
   bool mixed_failed(const GlsOut& o) const {
-    if (o.prec_used != DGPU_PREC_MIXED) return false;
+    if (!tensor_prec(o.prec_used)) return false;
     if (o.ldlt) return true;  // the refinement step applies a Cholesky factor the system does not have
     if (!(o.refine_correction <= kMixedFallback)) return true;
     for (double v : o.theta)
@@ -337,7 +342,7 @@ struct Engine {
     // ok flag (fetched with theta) shows it, and the fit is redone in FP64
     // (mixed_failed).
     int ok_s = 1;
-    if (prec == DGPU_PREC_MIXED) {
+    if (tensor_prec(prec)) {
       const Anchor a = anchor_buffers();
       if (!anchored) anchor_at(a, th, mask);
       DGPU_CUDA(cudaMemcpyAsync(a.rp, a.r0, sizeof(double) * P, cudaMemcpyDeviceToDevice, c.stream));
@@ -348,7 +353,7 @@ struct Engine {
       launch_gcv_finish(c.stream, 1, w.raw + s, w.edf + s, w.ok + s, n, w.rss + s, w.gcv + s);
     }
     o.theta.resize(P);
-    std::vector<double> delta(prec == DGPU_PREC_MIXED ? P : 0);
+    std::vector<double> delta(tensor_prec(prec) ? P : 0);
     Fetch f(c, sizeof(double) * (2 * P + 4) + on_fetch_bytes);
     f.add(o.theta.data(), th, P);
     f.add(&o.edf, w.edf + s, 1);
@@ -544,7 +549,7 @@ struct Engine {
         bc = curve[li];
         best = li;
       }
-    if (prec == DGPU_PREC_MIXED && !stamped) {
+    if (tensor_prec(prec) && !stamped) {
       // Re-evaluate every searched lambda around the folds' solutions at the
       // provisional minimum until the minimum stays put.
       const size_t gp = static_cast<size_t>(G) * P;

@@ -38,7 +38,7 @@ void launch_normal_equations(Context& c, int prec, int64_t N, int nc, int k, int
 // Mixed precision (BF16x3 tcgen05) Kronecker-packed normal equations:
 // G[u][v] (row-major Mu x Nv, FP64) from per-split partials in gpart_slot.
 void launch_normal_tc(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, const uint8_t* accepted,
-                      const int2* upairs, int Mu, const int2* vpairs, int Nv, Slot gpart_slot, double* g);
+                      const int2* upairs, int Mu, const int2* vpairs, int Nv, Slot gpart_slot, double* g, bool tf32 = false);
 // rhs = X^T W t and ywy = t^T W t over the active rows; with theta, the same
 // sums of the residual e = t - X theta (rhs = X^T W e, ywy = e^T W e).
 void launch_rhs(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, const uint8_t* accepted,

@@ -109,6 +109,10 @@ struct Context {
   unsigned char* host_staging(size_t bytes);
 };
 
+// Keep freed blocks in the device's default memory pool (the workspace slots
+// grow from it stream-ordered); once per device.
+void keep_pool_memory(int device);
+
 // RAII: clear the status word at entry, check it (after a sync) at exit.
 void reset_status(Context& c);
 void check_status(Context& c);  // synchronises the stream

@@ -376,8 +376,9 @@ void launch_normal_equations(Context& c, int prec, int64_t N, int nc, int k, int
   DGPU_CUDA(h2d_async(dpairs, up.data(), sizeof(int2) * Mu, st));
   DGPU_CUDA(h2d_async(dpairs + Mu, vp.data(), sizeof(int2) * Nv, st));
   double* g = static_cast<double*>(c.slot(kSlotFit12, sizeof(double) * static_cast<size_t>(Mu) * Nv));
-  if (prec == DGPU_PREC_MIXED) {
-    launch_normal_tc(c, N, nc, k, SS, R, accepted, dpairs, Mu, dpairs + Mu, Nv, kSlotFit11, g);
+  if (prec == DGPU_PREC_MIXED || prec == DGPU_PREC_TF32) {
+    launch_normal_tc(c, N, nc, k, SS, R, accepted, dpairs, Mu, dpairs + Mu, Nv, kSlotFit11, g,
+                     prec == DGPU_PREC_TF32);
   } else {
     const int gx = (Mu + kNeT - 1) / kNeT, gy = (Nv + kNeT - 1) / kNeT;
     // Split K (rows) so the grid covers the GPU a few times over.

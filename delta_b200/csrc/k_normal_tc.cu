@@ -127,6 +127,23 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint6
       : "memory");
 }
 
+// kind::tf32 instruction descriptor: FP32 accumulate, TF32 A and B, both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc_tf32(int M, int N) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(N >> 3) << 17) |
+         (static_cast<uint32_t>(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+      :
+      : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
                : "memory");
@@ -165,6 +182,25 @@ __device__ __forceinline__ void split_store(unsigned char* hi_base, unsigned cha
   *reinterpret_cast<uint4*>(lo_base + off) = *reinterpret_cast<const uint4*>(l);
 }
 
+// TF32 operands: 4-byte elements, so a core matrix (8 rows x 16 bytes) holds 4
+// K values; 8 values round to nearest (ties away) with cvt.rna.tf32.f32 and
+// go out as two 16-byte stores into K-adjacent core matrices (128 bytes apart).
+__device__ __forceinline__ uint32_t canon_off_tf32(int row, int kg8) {
+  return static_cast<uint32_t>(((row >> 3) * (kKC / 4) + 2 * kg8) * 128 + (row & 7) * 16);
+}
+
+__device__ __forceinline__ void tf32_store(unsigned char* base, uint32_t off, const float (&v)[8]) {
+  __align__(16) uint32_t t[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t[j]) : "f"(v[j]));
+  *reinterpret_cast<uint4*>(base + off) = *reinterpret_cast<const uint4*>(t);
+  *reinterpret_cast<uint4*>(base + off + 128) = *reinterpret_cast<const uint4*>(t + 4);
+}
+
+// kTf32: one TF32 product per K-step (kind::tf32, 8 K values per MMA) in place
+// of the three BF16 products; the two stage buffers of 32-bit operands take
+// the place of the four bf16 hi / lo buffers (same bytes).
+template <bool kTf32>
 __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int tid = threadIdx.x;
@@ -216,8 +252,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const uint32_t idesc = umma_idesc_bf16(kBM, BN);
-  constexpr uint32_t kLBO = 128, kSBO = (kKC / 8) * 128;
+  const uint32_t idesc = kTf32 ? umma_idesc_tf32(kBM, BN) : umma_idesc_bf16(kBM, BN);
+  constexpr uint32_t kLBO = 128, kSBO = kTf32 ? (kKC / 4) * 128 : (kKC / 8) * 128;
 
   // Chunk c of this split is bulk-loaded when it is full and the rows are aligned.
   auto chunk_rows = [&](int c) {
@@ -273,9 +309,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
   int issued = 0;  // chunks whose MMAs were issued (uniform over the CTA)
   for (int c = 0; c < nchunks; ++c) {
     const int st = c & 1;
-    unsigned char* ahi = smem + st * a_bytes;
+    unsigned char* ahi = smem + (kTf32 ? 2 * st : st) * a_bytes;
     unsigned char* alo = smem + (2 + st) * a_bytes;
-    unsigned char* bhi = b_base + st * b_bytes;
+    unsigned char* bhi = b_base + (kTf32 ? 2 * st : st) * b_bytes;
     unsigned char* blo = b_base + (2 + st) * b_bytes;
     const int64_t r0 = rbeg + static_cast<int64_t>(c) * kKC;
     const int rows = chunk_rows(c);
@@ -360,7 +396,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
 #pragma unroll
         for (int j = 0; j < 8; ++j) v[j] = 0.0f;
       }
-      split_store(ahi, alo, canon_off(m, kg), v);
+      if (kTf32)
+        tf32_store(ahi, canon_off_tf32(m, kg), v);
+      else
+        split_store(ahi, alo, canon_off(m, kg), v);
     }
     // B = V tile (BN x kKC): (w d_m) d_m'.
     for (int item = tid; item < BN * (kKC / 8); item += blockDim.x) {
@@ -378,7 +417,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
 #pragma unroll
         for (int j = 0; j < 8; ++j) v[j] = 0.0f;
       }
-      split_store(bhi, blo, canon_off(n, kg), v);
+      if (kTf32)
+        tf32_store(bhi, canon_off_tf32(n, kg), v);
+      else
+        split_store(bhi, blo, canon_off(n, kg), v);
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
@@ -386,13 +428,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_normal_tc(TcArgs a) {
       tc_fence_after();
       const uint32_t ah = smem_addr(ahi), al = smem_addr(alo);
       const uint32_t bh = smem_addr(bhi), bl = smem_addr(blo);
+      if (kTf32) {
+        // K-steps of 8 TF32 values: 32 bytes per row, two core matrices.
 #pragma unroll
-      for (int s = 0; s < kKC / 16; ++s) {
-        const uint32_t ko = static_cast<uint32_t>(s) * 256;  // two core matrices per K-step of 16
-        const uint32_t acc0 = (c % kDrainChunks != 0 || s > 0) ? 1u : 0u;
-        umma_bf16(tmem, umma_desc(ah + ko, kLBO, kSBO), umma_desc(bh + ko, kLBO, kSBO), idesc, acc0);
-        umma_bf16(tmem, umma_desc(ah + ko, kLBO, kSBO), umma_desc(bl + ko, kLBO, kSBO), idesc, 1u);
-        umma_bf16(tmem, umma_desc(al + ko, kLBO, kSBO), umma_desc(bh + ko, kLBO, kSBO), idesc, 1u);
+        for (int s = 0; s < kKC / 8; ++s) {
+          const uint32_t ko = static_cast<uint32_t>(s) * 256;
+          const uint32_t acc0 = (c % kDrainChunks != 0 || s > 0) ? 1u : 0u;
+          umma_tf32(tmem, umma_desc(ah + ko, kLBO, kSBO), umma_desc(bh + ko, kLBO, kSBO), idesc, acc0);
+        }
+      } else {
+#pragma unroll
+        for (int s = 0; s < kKC / 16; ++s) {
+          const uint32_t ko = static_cast<uint32_t>(s) * 256;  // two core matrices per K-step of 16
+          const uint32_t acc0 = (c % kDrainChunks != 0 || s > 0) ? 1u : 0u;
+          umma_bf16(tmem, umma_desc(ah + ko, kLBO, kSBO), umma_desc(bh + ko, kLBO, kSBO), idesc, acc0);
+          umma_bf16(tmem, umma_desc(ah + ko, kLBO, kSBO), umma_desc(bl + ko, kLBO, kSBO), idesc, 1u);
+          umma_bf16(tmem, umma_desc(al + ko, kLBO, kSBO), umma_desc(bh + ko, kLBO, kSBO), idesc, 1u);
+        }
       }
       umma_commit(&mbar[st]);
     }
@@ -469,9 +521,9 @@ __global__ void k_reduce_tiles(int nsplit, size_t split_len, int BN, int tiles_n
 
 }  // namespace
 
-// G of the mixed-precision path (row-major Mu x Nv, FP64).
+// G of the tensor-core paths (row-major Mu x Nv, FP64): BF16x3 ("mixed") or TF32.
 void launch_normal_tc(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, const uint8_t* accepted,
-                      const int2* upairs, int Mu, const int2* vpairs, int Nv, Slot gpart_slot, double* g) {
+                      const int2* upairs, int Mu, const int2* vpairs, int Nv, Slot gpart_slot, double* g, bool tf32) {
   // Widest N tile (<= 256) whose staging fits; wide fits (many components and
   // knots) trade a narrower B tile for more column tiles.
   int tiles_n = (Nv + 255) / 256, BN = 0;
@@ -510,8 +562,13 @@ void launch_normal_tc(Context& c, int64_t N, int nc, int k, int SS, const FitRow
   auto al16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
   a.bulk = al16(R.bn) && al16(R.d) && al16(R.w) && al16(R.valid) && (static_cast<size_t>(kKC) * nc * 8) % 16 == 0 &&
            (static_cast<size_t>(kKC) * k * 8) % 16 == 0;
-  ensure_dynamic_smem(reinterpret_cast<const void*>(k_normal_tc), smem);
-  k_normal_tc<<<dim3(tiles_m, tiles_n, nsplit), kThreads, smem, c.stream>>>(a);
+  if (tf32) {
+    ensure_dynamic_smem(reinterpret_cast<const void*>(k_normal_tc<true>), smem);
+    k_normal_tc<true><<<dim3(tiles_m, tiles_n, nsplit), kThreads, smem, c.stream>>>(a);
+  } else {
+    ensure_dynamic_smem(reinterpret_cast<const void*>(k_normal_tc<false>), smem);
+    k_normal_tc<false><<<dim3(tiles_m, tiles_n, nsplit), kThreads, smem, c.stream>>>(a);
+  }
   DGPU_LAUNCH("k_normal_tc");
   const int rb = static_cast<int>(std::min<size_t>(148 * 4, (split_len + 255) / 256));
   k_reduce_tiles<<<rb, 256, 0, c.stream>>>(nsplit, split_len, BN, tiles_n, Mu, Nv, gpart, g);

@@ -40,20 +40,36 @@ cudaError_t h2d_async(void* dst, const void* src, size_t bytes, cudaStream_t s) 
   return cudaSuccess;
 }
 
+// Workspace grows stream-ordered from the device's memory pool: the old buffer
+// is released after the work already queued on this context's stream (which is
+// the only stream that uses it) and the new one is valid for the work queued
+// after, so growth neither synchronises the stream nor the device (a plain
+// cudaFree waits for every stream of the device). The pool keeps freed blocks
+// for reuse (release threshold raised once per device in dgpu_create).
 void* Context::slot(Slot s, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (slot_size[s] >= bytes) return slot_ptr[s];
-  // Growing: the stream may still read the old buffer.
   if (slot_ptr[s]) {
-    DGPU_CUDA(cudaStreamSynchronize(stream));
-    DGPU_CUDA(cudaFree(slot_ptr[s]));
+    DGPU_CUDA(cudaFreeAsync(slot_ptr[s], stream));
     slot_ptr[s] = nullptr;
     slot_size[s] = 0;
   }
   const size_t want = bytes + bytes / 8 + 256;
-  DGPU_CUDA(cudaMalloc(&slot_ptr[s], want));
+  DGPU_CUDA(cudaMallocAsync(&slot_ptr[s], want, stream));
   slot_size[s] = want;
   return slot_ptr[s];
+}
+
+void keep_pool_memory(int device) {
+  static std::mutex mu;
+  static std::map<int, bool> done;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done[device]) return;
+  cudaMemPool_t pool = nullptr;
+  DGPU_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+  uint64_t keep = ~uint64_t(0);
+  DGPU_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  done[device] = true;
 }
 
 unsigned char* Context::host_staging(size_t bytes) {

@@ -167,7 +167,8 @@ def synthetic_pair(width: int, height: int, n_stars: int, seed: int = 0, *,
                    read_noise_e: float = 4.0, ref_fwhm: float = 2.5, sci_fwhm=3.5,
                    sci_kind: str = "gaussian", moffat_beta: float = 3.0, moffat_q: float = 0.85,
                    moffat_pa: float = 30.0, mask_fraction: float = 0.01, n_transients: int = 0,
-                   transient_snr=(5.0, 50.0), saturation_e: float | None = None) -> SyntheticPair:
+                   transient_snr=(5.0, 50.0), saturation_e: float | None = None, science_shift=(0.0, 0.0),
+                   science_scale: float = 1.0) -> SyntheticPair:
     """Seeded pair for the benchmark configurations.
 
     Fluxes in e- follow dN/dF ~ F^-slope on flux_range; images are rendered in
@@ -177,14 +178,18 @@ def synthetic_pair(width: int, height: int, n_stars: int, seed: int = 0, *,
     number or a callable fwhm(x, y). Masks: random bad columns (kMaskBad = 1)
     covering about ``mask_fraction`` of the pixels with saturated cores
     (kMaskSaturated = 2) flagged where a source exceeds the saturation level
-    (values clipped there).
+    (values clipped there). ``science_shift`` = (dx, dy) renders the science
+    sources displaced by that many pixels and ``science_scale`` multiplies the
+    whole science frame (sky and sources, before noise): a misregistered,
+    photometrically scaled exposure of the same field.
     """
     rng = np.random.default_rng(seed)
     shape = (height, width)
     pos, flux = sample_starfield(shape, n_stars, rng, flux_range=flux_range, slope=slope, border=8)
     fw_fn = sci_fwhm if callable(sci_fwhm) else (lambda x, y, f=float(sci_fwhm): f)
     ref_e = sky_e + render_psf_field(shape, pos, flux, lambda x, y: ref_fwhm, "gaussian")
-    sci_e = sky_e + render_psf_field(shape, pos, flux, fw_fn, sci_kind, beta=moffat_beta, q=moffat_q,
+    shift = np.asarray(science_shift, np.float64).reshape(1, 2)
+    sci_e = sky_e + render_psf_field(shape, pos + shift, flux, fw_fn, sci_kind, beta=moffat_beta, q=moffat_q,
                                      pa_deg=moffat_pa)
     t_xy = np.zeros((0, 2))
     t_flux = np.zeros(0)
@@ -202,6 +207,7 @@ def synthetic_pair(width: int, height: int, n_stars: int, seed: int = 0, *,
             t_flux[i] = snr[i] * sig_bg * np.sqrt(4.0 * np.pi) * sig
         sci_e += render_psf_field(shape, t_xy, t_flux, fw_fn, sci_kind, beta=moffat_beta, q=moffat_q,
                                   pa_deg=moffat_pa)
+    sci_e = sci_e * float(science_scale)
     ref_n = rng.poisson(np.clip(ref_e, 0, None)).astype(np.float64) + rng.normal(0, read_noise_e, shape)
     sci_n = rng.poisson(np.clip(sci_e, 0, None)).astype(np.float64) + rng.normal(0, read_noise_e, shape)
     ref_adu = ref_n / gain

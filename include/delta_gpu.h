@@ -45,6 +45,8 @@ extern "C" {
 #define DGPU_PREC_FP32 1  /* "plain": FP32 SIMT products and accumulation */
 #define DGPU_PREC_MIXED 2 /* "mixed": BF16x3 split tcgen05 products, FP32 accumulate,
                              FP64 cross-CTA reduce, Cholesky and one refinement step */
+#define DGPU_PREC_TF32 3  /* "tf32": one TF32 tcgen05 product (kind::tf32), FP32 accumulate,
+                             then as "mixed" (FP64 reduce, Cholesky, one refinement step) */
 
 typedef struct dgpu_context dgpu_context;
 
