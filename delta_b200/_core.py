@@ -291,6 +291,65 @@ def stamp_gcv(science, reference, knots, stamp_x, stamp_y, stamp_radius: int, be
             "theta": theta, "grad_gcv": g_gcv, "grad_rss": g_rss}
 
 
+def subtract_batch_native(items, *, n_max: int = 6, n_knots: int = 5, radius: int = 0, stamp_radius: int = 15,
+                          threshold_sigma: float = 5.0, max_stamps: int = 200, saturation: float = 0.0,
+                          fwhm_radius: int = 0, match_radius: int = 2, lambda_grid=None, clip_sigma: float = 4.0,
+                          clip_iterations: int = 5, min_stamps: int = 5, cv_folds: int = 5, precision: str = "fp64",
+                          decorrelate: bool = True, block: int = 256, score: bool = True, catalog: bool = True,
+                          catalog_threshold_sigma: float = 5.0, frames_in_flight: int = 4,
+                          catalog_capacity: int = 4096) -> list[dict]:
+    """dgpu_subtract_batch on host frames: ``items`` are dicts of science,
+    reference and the optional science_var / reference_var / science_mask /
+    reference_mask layers. Returns per frame {difference, variance, mask,
+    score, theta, lambda, beta, direction, n_stamps_used, catalog, seconds}."""
+    grid = np.ascontiguousarray(np.logspace(-6, 6, 25) if lambda_grid is None else lambda_grid, np.float64)
+    cfg = _lib.BatchConfig(n_max, n_knots, radius, stamp_radius, threshold_sigma, max_stamps, saturation,
+                           fwhm_radius, match_radius, grid.ctypes.data, grid.size, clip_sigma, clip_iterations,
+                           min_stamps, cv_folds, PRECISIONS[precision], int(decorrelate), block, int(score),
+                           int(catalog), catalog_threshold_sigma, frames_in_flight, 0)
+    n = len(items)
+    frames = (_lib.Frame * max(n, 1))()
+    results = (_lib.FrameResult * max(n, 1))()
+    keep, outs = [], []
+    nc = (n_max + 1) * (n_max + 2) // 2
+    for i, it in enumerate(items):
+        sci, ref = _img(it["science"], "science"), _img(it["reference"], "reference")
+        layers = [_img_opt(it.get("science_var"), "science_var"), _img_opt(it.get("reference_var"), "reference_var"),
+                  _mask_opt(it.get("science_mask"), "science_mask"),
+                  _mask_opt(it.get("reference_mask"), "reference_mask")]
+        keep.append((sci, ref, *layers))
+        h, w = sci.shape
+        frames[i] = _lib.Frame(w, h, sci.ctypes.data, ref.ctypes.data,
+                               *[None if a is None else a.ctypes.data for a in layers])
+        o = {"difference": np.empty((h, w), np.float32), "variance": np.empty((h, w), np.float32),
+             "mask": np.empty((h, w), np.uint8), "score": np.empty((h, w), np.float32) if score else None,
+             "theta": np.empty((nc + 1) * n_knots * n_knots),
+             "cols": {name: np.empty(catalog_capacity, dt) for name, dt in _lib.CATALOG_COLUMNS}}
+        outs.append(o)
+        r = results[i]
+        r.difference, r.variance, r.mask = (o["difference"].ctypes.data, o["variance"].ctypes.data,
+                                            o["mask"].ctypes.data)
+        r.score = None if o["score"] is None else o["score"].ctypes.data
+        r.theta = o["theta"].ctypes.data
+        r.catalog = _lib.CatalogColumns(*[o["cols"][name].ctypes.data for name, _ in _lib.CATALOG_COLUMNS])
+        r.catalog_capacity = catalog_capacity
+    check(_lib.lib().dgpu_subtract_batch(ctypes.byref(cfg), _lib.MEM_HOST, n, frames, results))
+    out = []
+    for i, o in enumerate(outs):
+        r = results[i]
+        cat = None
+        if catalog and score:
+            if not r.catalog_fetched:
+                raise RuntimeError(f"subtract_batch: frame {i} has {r.catalog_count} catalog rows, above the capacity")
+            cat = {name: v[: r.catalog_count].copy() for name, v in o["cols"].items()}
+        out.append({"difference": o["difference"], "variance": o["variance"] if r.has_variance else None,
+                    "mask": o["mask"] if r.has_mask else None, "score": o["score"], "theta": o["theta"],
+                    "lambda": r.lambda_, "beta": r.beta,
+                    "direction": "reference" if r.direction_is_reference else "science",
+                    "n_stamps_used": r.n_stamps_used, "catalog": cat, "seconds": r.seconds})
+    return out
+
+
 def photometric_scale(knots, theta, component_sums, height: int, width: int) -> np.ndarray:
     """Per-pixel photometric scale field sum_n a_n(x,y) S_n, shape (H,W)."""
     k = _knots(knots)

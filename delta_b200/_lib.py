@@ -132,6 +132,33 @@ class CatalogColumns(ctypes.Structure):
     _fields_ = [(name, ctypes.c_void_p) for name, _ in CATALOG_COLUMNS]
 
 
+class Frame(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int64), ("height", ctypes.c_int64), ("science", ctypes.c_void_p),
+                ("reference", ctypes.c_void_p), ("science_var", ctypes.c_void_p), ("reference_var", ctypes.c_void_p),
+                ("science_mask", ctypes.c_void_p), ("reference_mask", ctypes.c_void_p)]
+
+
+class BatchConfig(ctypes.Structure):
+    _fields_ = [("n_max", ctypes.c_int), ("n_knots", ctypes.c_int), ("radius", ctypes.c_int),
+                ("stamp_radius", ctypes.c_int), ("threshold_sigma", ctypes.c_double), ("max_stamps", ctypes.c_int),
+                ("saturation", ctypes.c_double), ("fwhm_radius", ctypes.c_int), ("match_radius", ctypes.c_int),
+                ("lambda_grid", ctypes.c_void_p), ("n_lambda", ctypes.c_int), ("clip_sigma", ctypes.c_double),
+                ("clip_iterations", ctypes.c_int), ("min_stamps", ctypes.c_int), ("cv_folds", ctypes.c_int),
+                ("precision", ctypes.c_int), ("decorrelate", ctypes.c_int), ("block", ctypes.c_int),
+                ("score", ctypes.c_int), ("catalog", ctypes.c_int), ("catalog_threshold_sigma", ctypes.c_double),
+                ("frames_in_flight", ctypes.c_int), ("device", ctypes.c_int)]
+
+
+class FrameResult(ctypes.Structure):
+    _fields_ = [("difference", ctypes.c_void_p), ("variance", ctypes.c_void_p), ("mask", ctypes.c_void_p),
+                ("score", ctypes.c_void_p), ("theta", ctypes.c_void_p), ("catalog", CatalogColumns),
+                ("catalog_capacity", ctypes.c_int), ("n_theta", ctypes.c_int64), ("lambda_", ctypes.c_double),
+                ("beta", ctypes.c_double), ("direction_is_reference", ctypes.c_int), ("n_stamps_used", ctypes.c_int),
+                ("has_variance", ctypes.c_int), ("has_mask", ctypes.c_int), ("catalog_count", ctypes.c_int),
+                ("catalog_fetched", ctypes.c_int), ("status", ctypes.c_int), ("error", ctypes.c_char * 256),
+                ("seconds", ctypes.c_double)]
+
+
 def lib():
     """The loaded C library (raises DeviceUnavailableError if it is missing)."""
     global _lib

@@ -154,6 +154,18 @@ int dgpu_set_timing(dgpu_context* ctx, int on) {
   });
 }
 
+int dgpu_autotune_table(char* out, size_t cap, size_t* needed) {
+  return guarded_free([&] {
+    const std::string t = autotuner().report();
+    if (needed) *needed = t.size() + 1;
+    if (out && cap > 0) {
+      const size_t n = std::min(cap - 1, t.size());
+      std::memcpy(out, t.data(), n);
+      out[n] = '\0';
+    }
+  });
+}
+
 int dgpu_set_label_loop_cap(dgpu_context* ctx, int cap) {
   return guarded(ctx, [&](Context& c) { c.label_loop_cap = cap > 0 ? cap : Context::kDefaultLabelLoopCap; });
 }

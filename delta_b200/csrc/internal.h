@@ -7,6 +7,8 @@
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -69,6 +71,8 @@ enum Slot : int {
   kSlotFft0, kSlotFft1, kSlotFft2, kSlotFft3, kSlotFft4, kSlotFft5,
   kSlotGlsPart, kSlotLdlt,
   kSlotGrad0, kSlotGrad1, kSlotGrad2, kSlotGrad3, kSlotGrad4, kSlotGrad5, kSlotGrad6, kSlotGrad7,
+  kSlotBatch0, kSlotBatch1, kSlotBatch2, kSlotBatch3, kSlotBatch4, kSlotBatch5, kSlotBatch6, kSlotBatch7,
+  kSlotBatch8, kSlotBatch9, kSlotBatch10, kSlotBatch11,
   kSlotCount
 };
 
@@ -112,6 +116,69 @@ struct Context {
 // Keep freed blocks in the device's default memory pool (the workspace slots
 // grow from it stream-ordered); once per device.
 void keep_pool_memory(int device);
+
+// Process-wide autotuner for launch parameters that do not change a kernel's
+// results (e.g. a tile height whose per-pixel arithmetic order is fixed): the
+// first call with a new key times every candidate on the call's own data (one
+// warm launch, then one launch between CUDA events on the stream) and keeps
+// the fastest; later calls reuse it. DELTA_AUTOTUNE=0 skips the timing and
+// takes the first candidate (the heuristic choice).
+class Autotuner {
+ public:
+  // Cached choice for key, or -1.
+  int lookup(const std::string& key);
+  void store(const std::string& key, int choice, const std::vector<std::pair<int, float>>& timings);
+  bool enabled() const { return enabled_; }
+  std::string report();
+  Autotuner();
+
+ private:
+  std::mutex mu_;
+  std::map<std::string, std::pair<int, std::vector<std::pair<int, float>>>> table_;
+  bool enabled_ = true;
+};
+Autotuner& autotuner();
+
+// Pick among `cands` (the first is the heuristic default) for `key`, launching
+// launch(candidate) on stream s; every launch must write the same outputs.
+template <class Launch>
+int autotune(cudaStream_t s, const std::string& key, const std::vector<int>& cands, Launch&& launch) {
+  Autotuner& t = autotuner();
+  const int cached = t.lookup(key);
+  if (cached >= 0) {
+    launch(cached);
+    return cached;
+  }
+  if (!t.enabled() || cands.size() == 1) {
+    launch(cands.front());
+    t.store(key, cands.front(), {});
+    return cands.front();
+  }
+  cudaEvent_t e0, e1;
+  DGPU_CUDA(cudaEventCreate(&e0));
+  DGPU_CUDA(cudaEventCreate(&e1));
+  std::vector<std::pair<int, float>> times;
+  int best = cands.front();
+  float best_ms = 0.0f;
+  for (int cand : cands) {
+    launch(cand);  // warm (first launch of a template, L2 state)
+    DGPU_CUDA(cudaEventRecord(e0, s));
+    launch(cand);
+    DGPU_CUDA(cudaEventRecord(e1, s));
+    DGPU_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    DGPU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    times.emplace_back(cand, ms);
+    if (times.size() == 1 || ms < best_ms) {
+      best_ms = ms;
+      best = cand;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  t.store(key, best, times);
+  return best;
+}
 
 // RAII: clear the status word at entry, check it (after a sync) at exit.
 void reset_status(Context& c);

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 
 #include "dev_common.cuh"
@@ -373,19 +374,9 @@ size_t model_convolve_smem(int nx, int ks, int TH) {
                           static_cast<size_t>(nx) * (nrows + kMcPad) * kMcTW + static_cast<size_t>(nx) * mc_tap_stride(ks));
 }
 
-void launch_model_convolve_orders(cudaStream_t s, const SubtractArgs& a, const int2* orders, bool stack) {
+static void launch_mc_th(cudaStream_t s, const SubtractArgs& a, const int2* orders, bool stack, int TH) {
   const int nx = a.n_max + 1;
-  // Tallest tile (least redundant x-pass halo) that still lets two CTAs share
-  // an SM; otherwise the tallest that fits at all.
-  const size_t kTwoPerSm = 112 * 1024, kMaxSmem = 200 * 1024;
-  int TH = 64;
-  while (TH > 8 && model_convolve_smem(nx, a.ks, TH) > kTwoPerSm) TH /= 2;
-  if (model_convolve_smem(nx, a.ks, TH) > kTwoPerSm) {
-    TH = 64;
-    while (TH > 8 && model_convolve_smem(nx, a.ks, TH) > kMaxSmem) TH /= 2;
-  }
   const size_t smem = model_convolve_smem(nx, a.ks, TH);
-  if (smem > kMaxSmem) fail(DGPU_ERR_INVALID, "subtract: kernel footprint too large for the tile engine");
   switch (nx) {
     case 1: stack ? launch_mc<1, true>(s, a, orders, TH, smem) : launch_mc<1, false>(s, a, orders, TH, smem); break;
     case 2: stack ? launch_mc<2, true>(s, a, orders, TH, smem) : launch_mc<2, false>(s, a, orders, TH, smem); break;
@@ -400,6 +391,41 @@ void launch_model_convolve_orders(cudaStream_t s, const SubtractArgs& a, const i
     case 11: stack ? launch_mc<11, true>(s, a, orders, TH, smem) : launch_mc<11, false>(s, a, orders, TH, smem); break;
     default: fail(DGPU_ERR_INVALID, "subtract: n_max above 10 is not supported by the tile engine");
   }
+}
+
+// The tile height is autotuned per (components, kernel size, frame size class):
+// each height gives the same bits (the per-pixel order of every sum is fixed),
+// only the redundant x-pass halo and the CTAs per SM differ. The first
+// candidate is the heuristic: the tallest tile that still lets two CTAs share
+// an SM, otherwise the tallest that fits.
+void launch_model_convolve_orders(cudaStream_t s, const SubtractArgs& a, const int2* orders, bool stack) {
+  const int nx = a.n_max + 1;
+  const size_t kTwoPerSm = 112 * 1024, kMaxSmem = 200 * 1024;
+  int TH = 64;
+  while (TH > 8 && model_convolve_smem(nx, a.ks, TH) > kTwoPerSm) TH /= 2;
+  if (model_convolve_smem(nx, a.ks, TH) > kTwoPerSm) {
+    TH = 64;
+    while (TH > 8 && model_convolve_smem(nx, a.ks, TH) > kMaxSmem) TH /= 2;
+  }
+  if (model_convolve_smem(nx, a.ks, TH) > kMaxSmem)
+    fail(DGPU_ERR_INVALID, "subtract: kernel footprint too large for the tile engine");
+  std::vector<int> cands{TH};
+  for (int t : {64, 32, 16})
+    if (t != TH && model_convolve_smem(nx, a.ks, t) <= kMaxSmem) cands.push_back(t);
+  int size_class = 0;
+  for (int64_t px = static_cast<int64_t>(a.w) * a.h; px > 1; px >>= 2) ++size_class;
+  // DELTA_MODEL_CONVOLVE_TH forces one candidate (a diagnostic: the tests
+  // check that every tile height gives the same bits).
+  if (const char* f = std::getenv("DELTA_MODEL_CONVOLVE_TH")) {
+    const int th = std::atoi(f);
+    if (std::find(cands.begin(), cands.end(), th) != cands.end()) {
+      launch_mc_th(s, a, orders, stack, th);
+      return;
+    }
+  }
+  const std::string key = std::string("model_convolve") + (stack ? "/stack" : "") + "/nx" + std::to_string(nx) +
+                          "/ks" + std::to_string(a.ks) + "/px4^" + std::to_string(size_class);
+  autotune(s, key, cands, [&](int th) { launch_mc_th(s, a, orders, stack, th); });
 }
 
 // ---------------------------------------------------------------------------

@@ -6,6 +6,7 @@
 #include <map>
 #include <mutex>
 #include <utility>
+#include <cstdio>
 #include <cstdlib>
 #include <stdexcept>
 
@@ -58,6 +59,46 @@ void* Context::slot(Slot s, size_t bytes) {
   DGPU_CUDA(cudaMallocAsync(&slot_ptr[s], want, stream));
   slot_size[s] = want;
   return slot_ptr[s];
+}
+
+Autotuner::Autotuner() {
+  const char* v = std::getenv("DELTA_AUTOTUNE");
+  enabled_ = !(v != nullptr && std::string(v) == "0");
+}
+
+int Autotuner::lookup(const std::string& key) {
+  std::lock_guard<std::mutex> lock(mu_);
+  const auto it = table_.find(key);
+  return it == table_.end() ? -1 : it->second.first;
+}
+
+void Autotuner::store(const std::string& key, int choice, const std::vector<std::pair<int, float>>& timings) {
+  std::lock_guard<std::mutex> lock(mu_);
+  table_.emplace(key, std::make_pair(choice, timings));  // the first result for a key stays
+}
+
+std::string Autotuner::report() {
+  std::lock_guard<std::mutex> lock(mu_);
+  std::string out;
+  for (const auto& [key, v] : table_) {
+    out += key + " -> " + std::to_string(v.first);
+    if (!v.second.empty()) {
+      out += " (";
+      for (size_t i = 0; i < v.second.size(); ++i) {
+        char buf[64];
+        std::snprintf(buf, sizeof(buf), "%s%d: %.4f ms", i ? ", " : "", v.second[i].first, v.second[i].second);
+        out += buf;
+      }
+      out += ")";
+    }
+    out += "\n";
+  }
+  return out;
+}
+
+Autotuner& autotuner() {
+  static Autotuner t;
+  return t;
 }
 
 void keep_pool_memory(int device) {

@@ -72,6 +72,14 @@ int dgpu_drain_timing(dgpu_context* ctx, char (*labels)[64], double* seconds, in
 int dgpu_set_timing(dgpu_context* ctx, int on);
 /* Number of kernels this library has launched in the process so far. */
 int dgpu_launch_count(unsigned long long* count);
+/* The autotuner's choices so far, as text lines "key -> choice (candidate:
+ * time, ...)". No reference counterpart: the library times the candidate
+ * launch parameters of a kernel (e.g. the model convolve's tile height) on the
+ * first call with a new shape class, keeps the fastest for the process, and
+ * every candidate gives the same results. DELTA_AUTOTUNE=0 disables the
+ * timing (the heuristic choice is used). Writes at most cap bytes (NUL
+ * terminated) and the full size through *needed. */
+int dgpu_autotune_table(char* out, size_t cap, size_t* needed);
 /* Iteration cap of every union-find search and link loop of the catalog's
  * labelling on this context (no reference counterpart: the reference's CPU
  * union-find has no cap). A loop that reaches it stops, the pixels it left
@@ -421,6 +429,87 @@ int dgpu_catalog_fetch(dgpu_context* ctx, const dgpu_catalog_columns* cols, int 
  * 0 = background, 1..n numbered by each component's first pixel in raster order
  * (the numbering of src/catalog.cpp:105-261). */
 int dgpu_catalog_labels(dgpu_context* ctx, int mem, int32_t* labels, int64_t n);
+
+/* ---- batch of frames ---------------------------------------------------------- */
+/* One frame pair: row-major layers of width x height (host or device per the
+ * call's `mem`); optional layers NULL. */
+typedef struct {
+  int64_t width, height;
+  const float* science;
+  const float* reference;
+  const float* science_var;
+  const float* reference_var;
+  const uint8_t* science_mask;
+  const uint8_t* reference_mask;
+} dgpu_frame;
+
+/* Subtractor settings of the batch (python/delta/pipeline.py:308-384; the
+ * reference's defaults in brackets). */
+typedef struct {
+  int n_max;                      /* 6 */
+  int n_knots;                    /* 5 (knots per axis) */
+  int radius;                     /* 0: default radius */
+  int stamp_radius;               /* 15 */
+  double threshold_sigma;         /* 5.0 (stamp detection) */
+  int max_stamps;                 /* 200 */
+  double saturation;              /* 0.0 */
+  int fwhm_radius;                /* 0 */
+  int match_radius;               /* 2 */
+  const double* lambda_grid;      /* NULL: logspace(-6, 6, 25) */
+  int n_lambda;
+  double clip_sigma;              /* 4.0 */
+  int clip_iterations;            /* 5 */
+  int min_stamps;                 /* 5 */
+  int cv_folds;                   /* 5 (0 or 1: GCV) */
+  int precision;                  /* DGPU_PREC_* */
+  int decorrelate;                /* 1 */
+  int block;                      /* 256 */
+  int score;                      /* 1 (needs variance layers) */
+  int catalog;                    /* 1 (with score) */
+  double catalog_threshold_sigma; /* 5.0 */
+  int frames_in_flight;           /* 4 */
+  int device;                     /* CUDA device index */
+} dgpu_batch_config;
+
+/* Products of one frame. Image buffers are caller memory of width x height
+ * (host or device per `mem`; NULL skips a product): difference (whitened
+ * when decorrelated) and its variance, mask, score. theta: (nc+1)*k host
+ * values or NULL. Catalog: columns of `catalog_capacity` entries (host); the
+ * rows are copied only when catalog_count <= catalog_capacity
+ * (catalog_fetched = 1). status / error: this frame's outcome. */
+typedef struct {
+  float* difference;
+  float* variance;
+  uint8_t* mask;
+  float* score;
+  double* theta;
+  dgpu_catalog_columns catalog;
+  int catalog_capacity;
+  /* outputs */
+  int64_t n_theta;
+  double lambda;
+  double beta;
+  int direction_is_reference;
+  int n_stamps_used;
+  int has_variance;
+  int has_mask;
+  int catalog_count;
+  int catalog_fetched;
+  int status;
+  char error[256];
+  double seconds; /* wall time of the frame on its worker */
+} dgpu_frame_result;
+
+/* subtract() over many frames of any sizes (the reference's per-frame
+ * Subtractor.subtract, python/delta/pipeline.py:430-806, applied to a list of
+ * pairs as pipeline.py:872-908 does for apply). Frames are processed longest
+ * first by frames_in_flight worker threads, each with its own context and
+ * stream from a process-wide pool (workspace kept between calls). Returns
+ * DGPU_OK when every frame succeeded, else the first failed frame's status
+ * (each frame's status / error are in its result); text via
+ * dgpu_last_error(NULL). */
+int dgpu_subtract_batch(const dgpu_batch_config* cfg, int mem, int n_frames, const dgpu_frame* frames,
+                        dgpu_frame_result* results);
 
 #ifdef __cplusplus
 }

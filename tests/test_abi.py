@@ -84,3 +84,28 @@ def test_photometric_scale_at_matches_oracle():
     pts = rng.uniform(0, 400, (50, 2))
     np.testing.assert_allclose(_core.photometric_scale_at(knots, theta, sums, pts),
                                nr.photometric_scale_at(knots, theta, sums, pts), atol=1e-12)
+
+
+def test_ctypes_struct_layouts_match_the_header(tmp_path):
+    """The ctypes mirrors of the ABI structs have the C sizes and field offsets
+    (a probe compiled against include/delta_gpu.h)."""
+    import shutil
+    import subprocess
+
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    src = tmp_path / "probe.c"
+    src.write_text(
+        "#include <stdio.h>\n#include <stddef.h>\n#include \"delta_gpu.h\"\n"
+        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu\\n\", sizeof(dgpu_frame), sizeof(dgpu_batch_config),"
+        " sizeof(dgpu_frame_result), offsetof(dgpu_frame_result, n_theta), offsetof(dgpu_frame_result, error),"
+        " offsetof(dgpu_frame_result, seconds), sizeof(dgpu_gls_result), offsetof(dgpu_gls_result, used_ldlt));"
+        "return 0;}\n")
+    exe = tmp_path / "probe"
+    inc = ROOT / "include"
+    subprocess.run(["gcc", f"-I{inc}", str(src), "-o", str(exe)], check=True)
+    want = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    fr = _lib.FrameResult
+    got = [ctypes.sizeof(_lib.Frame), ctypes.sizeof(_lib.BatchConfig), ctypes.sizeof(fr), fr.n_theta.offset,
+           fr.error.offset, fr.seconds.offset, ctypes.sizeof(_lib.GlsResult), _lib.GlsResult.used_ldlt.offset]
+    assert got == want

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 from conftest import load_golden
 
-from delta_b200 import _core
+from delta_b200 import _core, validation
 from oracle import cref, refbuild
 from oracle import numpy_ref as nr
 
@@ -314,3 +314,37 @@ def test_catalog_empty_and_all_seeded():
     o = np.full((50, 40), 7.0, np.float32)
     got = _core.build_catalog(o, o, expected_fwhm=3.0)
     assert len(got["x"]) == 1 and got["n_pix"][0] == 2000
+
+
+def test_model_convolve_tile_heights_give_identical_bits_and_autotune_records():
+    """Every tile height the autotuner may pick gives the same difference,
+    variance and mask bits (the per-pixel order of each sum does not depend on
+    the tiling), and the tuner records its timed choice."""
+    import ctypes
+    import os
+
+    from delta_b200 import _lib
+
+    p = validation.synthetic_pair(700, 530, 200, 8, mask_fraction=0.01)
+    knots = nr.grid_knots(0, 0, 699, 529, 3, 3)
+    theta = np.zeros(22 * 9)
+    theta[0:9] = 1.0
+    args = (p.science, p.reference, knots, theta, 1.3, 5, 0, p.saturation, p.science_var, p.reference_var,
+            p.science_mask, p.reference_mask)
+    outs = []
+    try:
+        for th in ("16", "32", "64"):
+            os.environ["DELTA_MODEL_CONVOLVE_TH"] = th
+            outs.append(_core.subtract(*args))
+    finally:
+        os.environ.pop("DELTA_MODEL_CONVOLVE_TH", None)
+    for o in outs[1:]:
+        for name in ("difference", "variance", "mask"):
+            np.testing.assert_array_equal(o[name], outs[0][name], err_msg=name)
+    tuned = _core.subtract(*args)
+    np.testing.assert_array_equal(tuned["difference"], outs[0]["difference"])
+    need = ctypes.c_size_t()
+    buf = ctypes.create_string_buffer(4096)
+    _lib.check(_lib.lib().dgpu_autotune_table(buf, ctypes.c_size_t(4096), ctypes.byref(need)))
+    table = buf.value.decode()
+    assert "model_convolve/nx6" in table and "ms" in table, table

@@ -421,3 +421,32 @@ def test_subtract_files_reads_subtracts_and_writes(tmp_path):
         np.testing.assert_array_equal(back["mask"], r.mask)
     with pytest.raises(ValueError):
         delta.subtract_files(pairs, outs[:1], **kw)
+
+
+def test_native_batch_matches_subtract_one_at_a_time():
+    """dgpu_subtract_batch (the C++ scheduler: frames longest first over worker
+    contexts with their own streams) gives, for frames of different sizes, the
+    same bits as delta.subtract() on each frame alone: theta, lambda, the
+    whitened difference, its variance, the mask, the score and the catalog."""
+    ps = [validation.synthetic_pair(w, h, n, s, mask_fraction=0.005)
+          for w, h, n, s in ((512, 384, 260, 61), (640, 512, 400, 62), (384, 448, 200, 63), (512, 512, 300, 64))]
+    kw = dict(n_max=4, n_knots=3, stamp_radius=12, cv_folds=0, score=True, decorrelate=True, block=64,
+              precision="mixed", saturation=ps[0].saturation)
+    items = [dict(science=p.science, reference=p.reference, science_var=p.science_var,
+                  reference_var=p.reference_var, science_mask=p.science_mask, reference_mask=p.reference_mask)
+             for p in ps]
+    native = _core.subtract_batch_native(items, frames_in_flight=3, catalog=True,
+                                         **{k: v for k, v in kw.items() if k != "score"})
+    assert len(native) == len(ps)
+    for it, nat in zip(items, native, strict=True):
+        one = delta.subtract(**it, **kw)
+        np.testing.assert_array_equal(nat["theta"], one.solution.theta)
+        assert nat["lambda"] == one.solution.lam and nat["beta"] == one.solution.beta
+        assert nat["direction"] == one.solution.direction
+        for name in ("difference", "variance", "mask", "score"):
+            np.testing.assert_array_equal(nat[name], getattr(one, name), err_msg=name)
+        for name in one.source_catalog.dtype.names:
+            np.testing.assert_array_equal(nat["catalog"][name], one.source_catalog[name], err_msg=name)
+    with pytest.raises(ValueError, match="no stamps selected"):
+        blank = np.full((128, 128), 100.0, np.float32)
+        _core.subtract_batch_native([dict(science=blank, reference=blank)], score=False, decorrelate=False)
