@@ -164,6 +164,20 @@ def subtract(target, conv, tvar, cvar, tmask, cmask, solution, saturation):
     return diff, var if hv.value else None, mask if hm.value else None
 
 
+def scale_(t, factor: float) -> None:
+    """t *= factor in place on the device (library kernel, float32 product)."""
+    ctx = _ctx_on_torch_stream()
+    check(_lib.lib().dgpu_scale(ctx.handle, MEM_DEVICE, _p(t), ctypes.c_int64(t.numel()), ctypes.c_double(factor)),
+          ctx.handle)
+
+
+def fill_(t, value: float) -> None:
+    """t[:] = value on the device (library kernel)."""
+    ctx = _ctx_on_torch_stream()
+    check(_lib.lib().dgpu_fill(ctx.handle, MEM_DEVICE, _p(t), ctypes.c_int64(t.numel()), ctypes.c_double(value)),
+          ctx.handle)
+
+
 def negate(t) -> None:
     ctx = _ctx_on_torch_stream()
     check(_lib.lib().dgpu_negate(ctx.handle, MEM_DEVICE, _p(t), ctypes.c_int64(t.numel())), ctx.handle)
@@ -334,12 +348,12 @@ def apply(sub, solution, target, conv, tvar, cvar, tmask, cmask, sign, stamp_x, 
 
         variance_scale = _variance_rescale_factor(diff.cpu().numpy(), var.cpu().numpy(),
                                                   None if mask is None else mask.cpu().numpy())
-        var = var * variance_scale
+        scale_(var, variance_scale)
     whitened, white_var = diff, None
     if sub.decorrelate and tvar is not None and cvar is not None:
         whitened, white_var = decorrelate(diff, solution, tvar, cvar, sub.block)
         if variance_scale is not None:
-            white_var *= variance_scale
+            scale_(white_var, variance_scale)
     score = psf = cat = None
     if sub.score:
         if stamp_x is None or np.asarray(stamp_x).size == 0:
@@ -351,7 +365,8 @@ def apply(sub, solution, target, conv, tvar, cvar, tmask, cmask, sign, stamp_x, 
         elif var is not None:
             score_var = var
         else:
-            score_var = torch.full_like(whitened, float(np.var(whitened.cpu().numpy())))
+            score_var = torch.empty_like(whitened)
+            fill_(score_var, float(np.var(whitened.cpu().numpy())))
         score = matched_filter(whitened, psf, score_var)
         if sub.source_catalog:
             cat = build_catalog(score, whitened, mask, psf)

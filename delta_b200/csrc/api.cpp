@@ -509,6 +509,33 @@ int dgpu_estimate_background_noalloc(const float* data, const uint8_t* mask, int
   });
 }
 
+int dgpu_scale(dgpu_context* ctx, int mem, float* data, int64_t n, double scale) {
+  return guarded(ctx, [&](Context& c) {
+    if (n < 0) fail(DGPU_ERR_INVALID, "scale: n must be >= 0");
+    if (n == 0) return;
+    if (!data) fail(DGPU_ERR_INVALID, "scale: missing buffer");
+    const size_t bytes = 4 * static_cast<size_t>(n);
+    float* d = mem == DGPU_MEM_DEVICE ? data : static_cast<float*>(c.slot(kSlotOutVar, bytes));
+    if (mem != DGPU_MEM_DEVICE) DGPU_CUDA(h2d_async(d, data, bytes, c.stream));
+    launch_scale_fill(c.stream, n, d, static_cast<float>(scale), false, 0.0f);
+    stage_out(c, mem, data, d, bytes);
+    if (mem == DGPU_MEM_HOST) DGPU_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int dgpu_fill(dgpu_context* ctx, int mem, float* data, int64_t n, double value) {
+  return guarded(ctx, [&](Context& c) {
+    if (n < 0) fail(DGPU_ERR_INVALID, "fill: n must be >= 0");
+    if (n == 0) return;
+    if (!data) fail(DGPU_ERR_INVALID, "fill: missing buffer");
+    const size_t bytes = 4 * static_cast<size_t>(n);
+    float* d = mem == DGPU_MEM_DEVICE ? data : static_cast<float*>(c.slot(kSlotOutVar, bytes));
+    launch_scale_fill(c.stream, n, d, 1.0f, true, static_cast<float>(value));
+    stage_out(c, mem, data, d, bytes);
+    if (mem == DGPU_MEM_HOST) DGPU_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
 int dgpu_negate(dgpu_context* ctx, int mem, float* data, int64_t n) {
   return guarded(ctx, [&](Context& c) {
     if (n < 0) fail(DGPU_ERR_INVALID, "negate: n must be >= 0");

@@ -308,6 +308,7 @@ void launch_mask_fill(cudaStream_t s, int64_t n, const uint8_t* mask, const uint
                       const float* fill, float* diff, float* var);
 void launch_model_convolve_orders(cudaStream_t s, const SubtractArgs& a, const int2* orders, bool stack);
 void launch_photometric_scale(cudaStream_t s, const DevFields& F, const float* sums, int nc, float* out);
+void launch_scale_fill(cudaStream_t s, int64_t n, float* v, float scale, bool fill, float value);
 void launch_negate(cudaStream_t s, int64_t n, float* v);
 // bytes (a multiple of 16) from device memory to mapped pinned host memory
 // (its device-side address), both 16-byte aligned, by SM stores.

@@ -839,6 +839,20 @@ void launch_photometric_scale(cudaStream_t s, const DevFields& F, const float* s
 
 // Transients-positive sign flip of the difference (python/delta/pipeline.py:687-689),
 // in place: float4 body, scalar tail.
+// v = v * scale (float32 product, the scalar rounded to float first), or
+// v = value everywhere when fill is set.
+__global__ void k_scale_fill(int64_t n, float* __restrict__ v, float scale, int fill, float value) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    v[i] = fill ? value : v[i] * scale;
+}
+
+void launch_scale_fill(cudaStream_t s, int64_t n, float* v, float scale, bool fill, float value) {
+  const int blocks = static_cast<int>(std::min<int64_t>((n + 255) / 256, 148 * 16));
+  k_scale_fill<<<std::max(blocks, 1), 256, 0, s>>>(n, v, scale, fill ? 1 : 0, value);
+  DGPU_LAUNCH("k_scale_fill");
+}
+
 __global__ void k_negate(int64_t n, float* __restrict__ v) {
   const int64_t n4 = (reinterpret_cast<uintptr_t>(v) & 15) ? 0 : n / 4;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;

@@ -155,6 +155,13 @@ int dgpu_photometric_scale(dgpu_context* ctx, int mem, const double* knots, int 
  * convention applied to the difference when the science frame is the one
  * convolved (python/delta/pipeline.py:687-689, np.negative on the host there). */
 int dgpu_negate(dgpu_context* ctx, int mem, float* data, int64_t n);
+/* In-place v *= scale (the scale rounded to float32 first, one float32
+ * product per element) and v = value over n float32 elements: the variance
+ * rescale of Subtractor(rescale_variance=True) (python/delta/pipeline.py:
+ * 692-698, `variance * variance_scale` on float32 there) and the constant
+ * score variance of a frame without variance layers (pipeline.py:774-779). */
+int dgpu_scale(dgpu_context* ctx, int mem, float* data, int64_t n, double scale);
+int dgpu_fill(dgpu_context* ctx, int mem, float* data, int64_t n, double value);
 /* Copy of `bytes` from device memory to pinned host memory by SM stores
  * through the destination's mapped address, ordered on the context's stream;
  * returns once it has completed. No counterpart in the reference, which has no

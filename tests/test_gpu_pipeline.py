@@ -450,3 +450,20 @@ def test_native_batch_matches_subtract_one_at_a_time():
     with pytest.raises(ValueError, match="no stamps selected"):
         blank = np.full((128, 128), 100.0, np.float32)
         _core.subtract_batch_native([dict(science=blank, reference=blank)], score=False, decorrelate=False)
+
+
+def test_variance_rescale_on_the_device_matches_host_staged():
+    """rescale_variance=True: the device-resident path scales Var(D) and the
+    whitened variance with the library's kernel (a float32 product, as the
+    reference's numpy `variance * variance_scale`), bit-identical to the
+    host-staged path."""
+    p = validation.synthetic_pair(384, 384, 220, 17, mask_fraction=0.005)
+    kw = dict(n_max=4, radius=10, n_knots=3, stamp_radius=12, cv_folds=0, score=True, decorrelate=True, block=64,
+              saturation=p.saturation, rescale_variance=True)
+    layers = dict(science_var=p.science_var, reference_var=p.reference_var, science_mask=p.science_mask,
+                  reference_mask=p.reference_mask)
+    a = delta.subtract(p.science, p.reference, device_resident=True, **layers, **kw)
+    b = delta.subtract(p.science, p.reference, device_resident=False, **layers, **kw)
+    assert a.variance_scale == b.variance_scale and a.variance_scale != 1.0
+    for name in ("difference", "variance", "score"):
+        np.testing.assert_array_equal(getattr(a, name), getattr(b, name), err_msg=name)
