@@ -80,9 +80,10 @@ def parse_args(argv=None):
     ap.add_argument("--batch", type=int, default=4, help="frames in flight per GPU (each its own stream)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU leg (rank 0, N=1)")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch leg of the default run")
-    ap.add_argument("--workload", choices=("frame", "uneven", "precision"), default="frame",
+    ap.add_argument("--workload", choices=("frame", "uneven", "precision", "grad"), default="frame",
                     help="frame: the 4096^2 workload (default); uneven: 64 frames of mixed sizes; "
-                         "precision: the normal-equation precision study at 725 unknowns, ~4e6 rows")
+                         "precision: the normal-equation precision study at 725 unknowns, ~4e6 rows; "
+                         "grad: the gradient evaluations on 8 fields of 2048^2")
     return ap.parse_args(argv)
 
 
@@ -871,6 +872,76 @@ def run_precision(args) -> int:
     return 0
 
 
+def run_grad(args) -> int:
+    """Throughput of the gradient evaluations on the differentiation workload:
+    8 fields of 2048 x 2048 (each its own seeded misregistration and scale),
+    layers resident on the device. A step evaluates, on every field, chi^2 of
+    the full-frame kernel model with its gradient in theta, (dx, dy) and the
+    scale (dgpu_kernel_chi2) and the stamp-fit GCV with its gradient in
+    (log lambda, dx, dy, scale) (dgpu_stamp_gcv). theta is the FP64 fit of
+    each field's aligned exposure (n_max 6, 4 x 4 knots)."""
+    import torch
+
+    import delta_b200 as delta
+    from delta_b200 import validation
+    from delta_b200.autograd import KernelProblem, StampProblem
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device (the product path has no CPU fallback)")
+    rank, world, local = rank_env()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    size, n_fields = min(args.size, 2048), 8
+    fields = []
+    for i in range(n_fields):
+        rng = np.random.default_rng(4000 + i)
+        dx, dy = rng.uniform(-0.5, 0.5, 2)
+        s = rng.uniform(0.8, 1.2)
+        aligned = validation.synthetic_pair(size, size, 5000, 500 + i, mask_fraction=0.01)
+        moved = validation.synthetic_pair(size, size, 5000, 500 + i, science_shift=(dx, dy), science_scale=s,
+                                          mask_fraction=0.01)
+        sol = delta.subtract(aligned.science, aligned.reference, science_var=aligned.science_var,
+                             reference_var=aligned.reference_var, science_mask=aligned.science_mask,
+                             reference_mask=aligned.reference_mask, n_max=6, n_knots=4, cv_folds=0, score=False,
+                             decorrelate=False, saturation=aligned.saturation).solution
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+        good = (moved.science_mask == 0) & (moved.reference_mask == 0)
+        wt = np.where(good, 1.0 / (moved.science_var + moved.reference_var), 0.0).astype(np.float32)
+        kp = KernelProblem(t(moved.science), t(wt), sol.knots, sol.beta, sol.n_max, sol.radius,
+                           reference_mask=t(moved.reference_mask))
+        sp = StampProblem(t(moved.science), t(moved.reference), sol.knots, sol.stamp_x, sol.stamp_y, 15, sol.beta,
+                          sol.n_max, sol.radius, target_var=t(moved.science_var), convolved_var=t(moved.reference_var),
+                          target_mask=t(moved.science_mask), convolved_mask=t(moved.reference_mask))
+        fields.append((kp, sp, t(moved.reference), torch.tensor(np.asarray(sol.theta)), float(np.log(sol.lam))))
+    z2 = torch.zeros(2, dtype=torch.float64)
+    one = torch.ones((), dtype=torch.float64)
+
+    def chi2_step():
+        for kp, _, ref, th, _ in fields:
+            kp.evaluate(th, z2, one, ref, grad=True)
+
+    def gcv_step():
+        for _, sp, _, _, ll in fields:
+            sp.evaluate(torch.tensor(ll), z2, one, grad=True)
+
+    out = {}
+    for name, fn in (("chi2_grad", chi2_step), ("gcv_grad", gcv_step)):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        ms = timed_steps(fn, args.steps, dev)
+        per_field = ms / args.steps / n_fields
+        out[name] = {"ms_per_field": per_field, "fields_per_s": 1e3 / per_field,
+                     "mpix_per_s": size * size / 1e6 / (per_field / 1e3)}
+    print(json.dumps({"metric": "gradient evaluations on 8 fields of 2048x2048 (device-resident)", "unit": "ms/field",
+                      "steps": args.steps, "warmup": args.warmup,
+                      "config": {"workload": f"{n_fields} fields of {size}x{size}, n_max 6, 4x4 knots, chi^2 "
+                                             "gradient in theta/shift/scale and GCV gradient in "
+                                             "log lambda/shift/scale"}, **out}), flush=True)
+    return 0
+
+
 def main(argv=None) -> int:
     args = parse_args(argv)
     if args.impl == "reference":
@@ -879,6 +950,8 @@ def main(argv=None) -> int:
         return run_uneven(args)
     if args.workload == "precision":
         return run_precision(args)
+    if args.workload == "grad":
+        return run_grad(args)
     return run_gpu(args)
 
 
