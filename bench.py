@@ -613,6 +613,16 @@ def run_gpu(args) -> int:
     ms_e2e = timed_steps(e2e_step, args.steps, device)
     d2h = sum(a.nbytes for r in res_holder["r"] for a in (r.difference, r.variance, r.mask, r.score)
               if a is not None)
+    # The same call from ordinary (pageable) NumPy arrays, as a caller without
+    # pinned buffers would make it.
+    page_items = [{k: np.array(getattr(p, k), copy=True) for k in layer_names} for p in pairs]
+
+    def e2e_pageable_step():
+        delta.subtract_batch([dict(it) for it in page_items], max_in_flight=B, **kw)
+
+    for _ in range(max(1, args.warmup // 2)):
+        e2e_pageable_step()
+    ms_e2e_page = timed_steps(e2e_pageable_step, args.steps, device)
 
     # errors of mixed and plain against the FP64 normal-equation path (outside the timing)
     out64 = _device.run(subs["fp64"], frame)
@@ -680,7 +690,9 @@ def run_gpu(args) -> int:
             "cpu_baseline": cpu,
             "e2e": {"value": world * args.steps * B * mpix / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps,
-                    "api": "delta_b200.subtract_batch"},
+                    "api": "delta_b200.subtract_batch", "inputs": "pinned host arrays"},
+            "e2e_pageable": {"value": world * args.steps * B * mpix / (ms_e2e_page / 1e3), "unit": UNIT,
+                             "ms_per_step": ms_e2e_page / args.steps, "inputs": "pageable NumPy arrays"},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "stage_ms_per_step": {k: round(1e3 * v / args.steps, 4) for k, v in sorted(stages.items())},
