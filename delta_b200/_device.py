@@ -164,6 +164,18 @@ def subtract(target, conv, tvar, cvar, tmask, cmask, solution, saturation):
     return diff, var if hv.value else None, mask if hm.value else None
 
 
+def variance_rescale_factor(diff, var, mask) -> float:
+    """_variance_rescale_factor (median(D^2 / Var) / median(chi2_1) over the good
+    pixels) with the median selected on the device: no frame leaves HBM."""
+    from .pipeline import _MEDIAN_CHI2_1
+
+    ctx = _ctx_on_torch_stream()
+    med, cnt = ctypes.c_double(), ctypes.c_int64()
+    check(_lib.lib().dgpu_z2_median(ctx.handle, MEM_DEVICE, ctypes.c_int64(diff.numel()), _p(diff), _p(var),
+                                    _p(mask), ctypes.byref(med), ctypes.byref(cnt)), ctx.handle)
+    return 1.0 if cnt.value == 0 else float(med.value / _MEDIAN_CHI2_1)
+
+
 def scale_(t, factor: float) -> None:
     """t *= factor in place on the device (library kernel, float32 product)."""
     ctx = _ctx_on_torch_stream()
@@ -343,11 +355,7 @@ def apply(sub, solution, target, conv, tvar, cvar, tmask, cmask, sign, stamp_x, 
         negate(diff)
     variance_scale = None
     if sub.rescale_variance and var is not None:
-        # A scalar statistic of the frame, taken on the host as the reference's glue does.
-        from .pipeline import _variance_rescale_factor
-
-        variance_scale = _variance_rescale_factor(diff.cpu().numpy(), var.cpu().numpy(),
-                                                  None if mask is None else mask.cpu().numpy())
+        variance_scale = variance_rescale_factor(diff, var, mask)
         scale_(var, variance_scale)
     whitened, white_var = diff, None
     if sub.decorrelate and tvar is not None and cvar is not None:

@@ -523,6 +523,32 @@ int dgpu_scale(dgpu_context* ctx, int mem, float* data, int64_t n, double scale)
   });
 }
 
+int dgpu_z2_median(dgpu_context* ctx, int mem, int64_t n, const float* difference, const float* variance,
+                   const uint8_t* mask, double* median, int64_t* count) {
+  return guarded(ctx, [&](Context& c) {
+    if (n < 0 || !difference || !variance || !median || !count) fail(DGPU_ERR_INVALID, "z2_median: missing argument");
+    *median = 0.0;
+    *count = 0;
+    if (n == 0) return;
+    const size_t nn = static_cast<size_t>(n);
+    const auto* d = static_cast<const float*>(stage_in(c, mem, difference, 4 * nn, kSlotOutDiff));
+    const auto* v = static_cast<const float*>(stage_in(c, mem, variance, 4 * nn, kSlotOutVar));
+    const auto* m = static_cast<const uint8_t*>(stage_in(c, mem, mask, nn, kSlotOutMask));
+    auto* keys = static_cast<unsigned long long*>(c.slot(kSlotScratch0, 8 * nn));
+    auto* st = static_cast<unsigned long long*>(c.slot(kSlotScratch2, 8 * 8 + 512 * 4));
+    launch_z2_median(c.stream, n, d, v, m, keys, st, reinterpret_cast<unsigned int*>(st + 8));
+    unsigned long long h[5];
+    DGPU_CUDA(cudaMemcpyAsync(h, st, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+    DGPU_CUDA(cudaStreamSynchronize(c.stream));
+    *count = static_cast<int64_t>(h[0]);
+    if (h[0] == 0) return;
+    double a, b;
+    std::memcpy(&a, &h[3], 8);
+    std::memcpy(&b, &h[4], 8);
+    *median = (a + b) / 2.0;
+  });
+}
+
 int dgpu_fill(dgpu_context* ctx, int mem, float* data, int64_t n, double value) {
   return guarded(ctx, [&](Context& c) {
     if (n < 0) fail(DGPU_ERR_INVALID, "fill: n must be >= 0");

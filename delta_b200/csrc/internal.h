@@ -308,6 +308,11 @@ void launch_mask_fill(cudaStream_t s, int64_t n, const uint8_t* mask, const uint
                       const float* fill, float* diff, float* var);
 void launch_model_convolve_orders(cudaStream_t s, const SubtractArgs& a, const int2* orders, bool stack);
 void launch_photometric_scale(cudaStream_t s, const DevFields& F, const float* sums, int nc, float* out);
+// Both middle ranks of z^2 = D^2 / Var (FP64) over the good pixels: after the
+// call state[3] / state[4] hold the keys (bit patterns) of ranks (m-1)/2 and
+// m/2, state[0] = m. keys: n entries; hist: 512 uints.
+void launch_z2_median(cudaStream_t s, int64_t n, const float* d, const float* v, const uint8_t* m,
+                      unsigned long long* keys, unsigned long long* state, unsigned int* hist);
 void launch_scale_fill(cudaStream_t s, int64_t n, float* v, float scale, bool fill, float value);
 void launch_negate(cudaStream_t s, int64_t n, float* v);
 // bytes (a multiple of 16) from device memory to mapped pinned host memory

@@ -900,3 +900,94 @@ void launch_copy_to_mapped(cudaStream_t s, int64_t bytes, const void* src, void*
 }
 
 }  // namespace dgpu
+
+// ---------------------------------------------------------------------------
+// Median of z^2 = D^2 / Var over the good pixels, exactly as numpy's median of
+// the FP64 values (python/delta/pipeline.py's _variance_rescale_factor): the
+// two middle ranks (lo = (m-1)/2, hi = m/2) of the FP64 keys found by one
+// 64-bit radix select (8 passes of 8-bit digits, both ranks per pass), then
+// (a + b) / 2 on the host. z^2 >= 0 and finite, so the keys order as their bit
+// patterns. Good pixels: Var > 0, D and Var finite, mask 0.
+// ---------------------------------------------------------------------------
+namespace dgpu {
+
+__global__ void k_z2_keys(int64_t n, const float* __restrict__ d, const float* __restrict__ v,
+                          const uint8_t* __restrict__ m, unsigned long long* __restrict__ keys,
+                          unsigned long long* __restrict__ count) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float dv = d[i], vv = v[i];
+    if (!(vv > 0.0f) || !isfinite(dv) || !isfinite(vv) || (m && m[i] != 0)) continue;
+    const double x = static_cast<double>(dv);
+    const double z2 = x * x / static_cast<double>(vv);
+    keys[atomicAdd(count, 1ull)] = static_cast<unsigned long long>(__double_as_longlong(z2));
+  }
+}
+
+// state: [0] count, [1] rank lo, [2] rank hi, [3] prefix lo, [4] prefix hi; hist: 2 x 256.
+__global__ void k_z2_hist(const unsigned long long* __restrict__ keys, unsigned long long* __restrict__ state,
+                          int shift, unsigned int* __restrict__ hist) {
+  __shared__ unsigned int h[2][256];
+  for (int i = threadIdx.x; i < 512; i += blockDim.x) h[i >> 8][i & 255] = 0;
+  __syncthreads();
+  const unsigned long long n = state[0];
+  const unsigned long long himask = shift >= 56 ? 0ull : (~0ull << (shift + 8));
+  const unsigned long long p0 = state[3] & himask, p1 = state[4] & himask;
+  for (unsigned long long i = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+    const unsigned long long k = keys[i];
+    const unsigned dgt = static_cast<unsigned>((k >> shift) & 0xffull);
+    if ((k & himask) == p0) atomicAdd(&h[0][dgt], 1u);
+    if ((k & himask) == p1) atomicAdd(&h[1][dgt], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 512; i += blockDim.x) {
+    const unsigned c = h[i >> 8][i & 255];
+    if (c) atomicAdd(&hist[i], c);
+  }
+}
+
+__global__ void k_z2_pick(unsigned long long* __restrict__ state, int shift, unsigned int* __restrict__ hist) {
+  if (threadIdx.x >= 2) return;
+  const int t = threadIdx.x;
+  unsigned long long rank = state[1 + t];
+  unsigned long long cum = 0;
+  int d = 0;
+  for (; d < 256; ++d) {
+    const unsigned long long c = hist[t * 256 + d];
+    if (rank < cum + c) break;
+    cum += c;
+  }
+  if (d > 255) d = 255;  // unreachable while the rank is below the count
+  state[1 + t] = rank - cum;
+  state[3 + t] |= static_cast<unsigned long long>(d) << shift;
+}
+
+__global__ void k_z2_init(unsigned long long* __restrict__ state) {
+  if (threadIdx.x == 0) {
+    const unsigned long long n = state[0];
+    state[1] = n ? (n - 1) / 2 : 0;
+    state[2] = n / 2;
+    state[3] = 0;
+    state[4] = 0;
+  }
+}
+
+void launch_z2_median(cudaStream_t s, int64_t n, const float* d, const float* v, const uint8_t* m,
+                      unsigned long long* keys, unsigned long long* state, unsigned int* hist) {
+  DGPU_CUDA(cudaMemsetAsync(state, 0, 5 * sizeof(unsigned long long), s));
+  const int blocks = static_cast<int>(std::min<int64_t>((n + 255) / 256, 148 * 8));
+  k_z2_keys<<<std::max(blocks, 1), 256, 0, s>>>(n, d, v, m, keys, state);
+  DGPU_LAUNCH("k_z2_keys");
+  k_z2_init<<<1, 32, 0, s>>>(state);
+  DGPU_LAUNCH("k_z2_init");
+  for (int shift = 56; shift >= 0; shift -= 8) {
+    DGPU_CUDA(cudaMemsetAsync(hist, 0, 512 * sizeof(unsigned int), s));
+    k_z2_hist<<<std::max(blocks, 1), 256, 0, s>>>(keys, state, shift, hist);
+    DGPU_LAUNCH("k_z2_hist");
+    k_z2_pick<<<1, 32, 0, s>>>(state, shift, hist);
+    DGPU_LAUNCH("k_z2_pick");
+  }
+}
+
+}  // namespace dgpu

@@ -161,6 +161,14 @@ int dgpu_negate(dgpu_context* ctx, int mem, float* data, int64_t n);
  * 692-698, `variance * variance_scale` on float32 there) and the constant
  * score variance of a frame without variance layers (pipeline.py:774-779). */
 int dgpu_scale(dgpu_context* ctx, int mem, float* data, int64_t n, double scale);
+/* Median of z^2 = D^2 / Var (FP64) over the pixels with Var > 0, D and Var
+ * finite and mask 0 (mask may be NULL): the statistic of the variance
+ * rescale (python/delta/pipeline.py _variance_rescale_factor, numpy's median
+ * of the FP64 values, the two middle values averaged for an even count),
+ * selected on the device. *count receives the number of good pixels (0 leaves
+ * *median = 0). */
+int dgpu_z2_median(dgpu_context* ctx, int mem, int64_t n, const float* difference, const float* variance,
+                   const uint8_t* mask, double* median, int64_t* count);
 int dgpu_fill(dgpu_context* ctx, int mem, float* data, int64_t n, double value);
 /* Copy of `bytes` from device memory to pinned host memory by SM stores
  * through the destination's mapped address, ordered on the context's stream;

@@ -348,3 +348,32 @@ def test_model_convolve_tile_heights_give_identical_bits_and_autotune_records():
     _lib.check(_lib.lib().dgpu_autotune_table(buf, ctypes.c_size_t(4096), ctypes.byref(need)))
     table = buf.value.decode()
     assert "model_convolve/nx6" in table and "ms" in table, table
+
+
+@pytest.mark.parametrize("n,seed", [(1, 0), (2, 1), (1001, 2), (1000, 3), (4_000_000, 4)])
+def test_z2_median_equals_numpy(n, seed):
+    """dgpu_z2_median: numpy's median of the FP64 z^2 = D^2 / Var over the good
+    pixels (Var > 0, both finite, mask 0), odd and even counts."""
+    import ctypes
+
+    from delta_b200 import _lib
+
+    rng = np.random.default_rng(seed)
+    d = rng.normal(0, 3, n).astype(np.float32)
+    v = rng.uniform(0.5, 20, n).astype(np.float32)
+    m = (rng.random(n) < 0.05).astype(np.uint8)
+    if n > 10:
+        d[rng.random(n) < 0.01] = np.nan
+        v[rng.random(n) < 0.01] = 0.0
+        v[rng.random(n) < 0.01] = np.inf
+    good = (v > 0) & np.isfinite(d) & np.isfinite(v) & (m == 0)
+    med, cnt = ctypes.c_double(), ctypes.c_int64()
+    ctx = _core.context()
+    _lib.check(_lib.lib().dgpu_z2_median(ctx.handle, _lib.MEM_HOST, ctypes.c_int64(n),
+                                         d.ctypes.data_as(ctypes.c_void_p), v.ctypes.data_as(ctypes.c_void_p),
+                                         m.ctypes.data_as(ctypes.c_void_p), ctypes.byref(med), ctypes.byref(cnt)),
+               ctx.handle)
+    assert cnt.value == int(good.sum())
+    if cnt.value:
+        z2 = d[good].astype(np.float64) ** 2 / v[good].astype(np.float64)
+        assert med.value == float(np.median(z2))
