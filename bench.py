@@ -705,11 +705,13 @@ def run_gpu(args) -> int:
     return 0
 
 
-def uneven_batch(args, rank: int, world: int, device, precisions=("mixed",)) -> dict:
+def uneven_batch(args, rank: int, world: int, device, precisions=("mixed",), native: bool = True) -> dict:
     """The uneven batch through delta_b200's Subtractor.subtract (the call
     subtract_batch makes per frame) on `--batch` worker streams, from pinned
     host arrays; wall clock with a device synchronize and barrier on both
-    sides, per precision. Returns {precision: stats} (rank 0's latencies)."""
+    sides, per precision; with `native`, also through the native batch
+    scheduler with graph replay ("native_graphs"). Returns {name: stats}
+    (rank 0's latencies)."""
     import torch
 
     from delta_b200 import _device, validation
@@ -765,6 +767,47 @@ def uneven_batch(args, rank: int, world: int, device, precisions=("mixed",)) -> 
         out[prec] = {"value": total_px / 1e6 / (wall / 1e3), "unit": UNIT, "wall_ms": wall, "frames": len(queue),
                      "latency_ms": {"p50": pct(0.5), "p99": pct(0.99), "max": ls[-1] if ls else None},
                      "frames_in_flight": max(1, args.batch), "precision": prec}
+    if native:
+        # The same queue through the native batch scheduler (dgpu_subtract_batch:
+        # C++ workers over pooled contexts, longest frame first, each frame's
+        # post-fit device work replayed as a recorded CUDA graph once its
+        # worker has run that shape), from the same pinned host arrays.
+        from delta_b200 import _core
+
+        nkw = dict(n_max=6, n_knots=4, cv_folds=0, stamp_radius=15, threshold_sigma=5.0, decorrelate=True, score=True,
+                   catalog=True, saturation=first.saturation if first is not None else 0.0, precision="mixed")
+        B = max(1, args.batch)
+        items = [host[queue[q]] for q in mine]
+        # Products land in pinned host memory (one arena for the whole batch,
+        # allocated before the timing; slices handed out inside it).
+        need = sum(64 + 13 * it["science"].size for it in items) + 4096
+        arena = torch.empty(need, dtype=torch.uint8, pin_memory=True).numpy()
+        off = [0]
+
+        def alloc(shape, dtype):
+            nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+            o = (off[0] + 63) & ~63
+            off[0] = o + nbytes
+            return arena[o : o + nbytes].view(dtype).reshape(shape)
+
+        _core.subtract_batch_native([host[j] for j in needed], frames_in_flight=B, graphs=True, alloc=alloc,
+                                    **nkw)  # untimed
+        off[0] = 0
+        barrier(device)
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        res = _core.subtract_batch_native(items, frames_in_flight=B, graphs=True, alloc=alloc, **nkw) if items else []
+        torch.cuda.synchronize(device)
+        wall = (time.perf_counter() - t0) * 1e3
+        barrier(device)
+        wall = max_over_ranks(wall, device)
+        ls = sorted(r["seconds"] * 1e3 for r in res)
+        pct = (lambda f: ls[min(len(ls) - 1, int(round(f * (len(ls) - 1))))]) if ls else (lambda f: None)
+        out["native_graphs"] = {"value": total_px / 1e6 / (wall / 1e3), "unit": UNIT, "wall_ms": wall,
+                                "frames": len(queue), "graph_replays": int(sum(r["graph_replayed"] for r in res)),
+                                "latency_ms": {"p50": pct(0.5), "p99": pct(0.99), "max": ls[-1] if ls else None},
+                                "frames_in_flight": B, "precision": "mixed",
+                                "api": "delta_b200._core.subtract_batch_native (dgpu_subtract_batch, graphs on)"}
     return out
 
 
@@ -785,13 +828,15 @@ def run_uneven(args) -> int:
         from datetime import timedelta
 
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
-    stats = uneven_batch(args, rank, world, device)["mixed"]
+    both = uneven_batch(args, rank, world, device)
+    stats = both["mixed"]
     if rank == 0:
         print(json.dumps({
             "metric": "uneven batch: aggregate Mpix/s over 64 frames of mixed sizes, end to end", "unit": UNIT,
             "value": stats["value"], "n_gpus": world, "frames": stats["frames"], "wall_ms": stats["wall_ms"],
             "latency_ms": {**stats["latency_ms"], "rank": 0}, "frames_in_flight": stats["frames_in_flight"],
             "higher_is_better": True, "scaling": "strong", "dtype": "f32", "data": "synthetic (seeded generator)",
+            "native_graphs": both.get("native_graphs"),
             "config": {"workload": UNEVEN_WORKLOAD, "precision": "mixed",
                        "timing": "wall clock, device synchronize and barrier on both sides; untimed first: one "
                                  "pass over the distinct frames"}}), flush=True)
@@ -805,7 +850,8 @@ def precision_study(seed: int = 0, size: int = 4096, n_stamps: int = 4200, n_max
     """Normal-equation arithmetic at the 725-unknown shape (n_max 6: 28
     components, 5 x 5 knots) over about 4e6 stamp rows of the 4096^2 field:
     FP32 SIMT, TF32 and BF16x3 tensor-core builds (the latter two with their
-    FP64 refinement step) and the device FP64 path, each against the FP64
+    FP64 refinement step, without and with the FP64 fallback) and the device
+    FP64 path, each against the FP64
     oracle's fit of the same rows (oracle.numpy_ref.fit_kernel with the C GLS
     solve, B_n through the reference's own convolve.cpp). Reported per
     precision: ||theta - theta0|| / ||theta0||, the selected lambda, and the
@@ -814,7 +860,7 @@ def precision_study(seed: int = 0, size: int = 4096, n_stamps: int = 4200, n_max
     images come from the same device subtraction so only theta differs."""
     import torch
 
-    from delta_b200 import _core
+    from delta_b200 import _core, _lib
     from oracle import cref, refbuild
     from oracle import numpy_ref as nr
 
@@ -847,18 +893,28 @@ def precision_study(seed: int = 0, size: int = 4096, n_stamps: int = 4200, n_max
     score0 = _core.matched_filter(sub0["difference"], psf, sub0["variance"]).astype(np.float64)
     out = {"P": int(theta0.size), "n_stamps": int(sx.size), "n_rows": int(want["n_pixels"]),
            "lambda_oracle": float(want["lambda"]), "oracle_seconds": round(oracle_s, 1), "modes": {}}
-    for prec in ("fp64", "fp32", "tf32", "mixed"):
+    ctx = _lib.context()
+    # Each build's own error: the reduced-precision modes run without their
+    # FP64 fallback ("tf32", "mixed"), then "mixed" once more as a fit runs by
+    # default ("mixed+fallback": redone in FP64 when its refinement step shows
+    # the BF16x3 system too far from the FP64 one).
+    for mode in ("fp64", "fp32", "tf32", "mixed", "mixed+fallback"):
+        prec = mode.split("+")[0]
+        ctx.set_precision_fallback(mode.endswith("+fallback"))
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        got = _core.fit_kernel(pair.science, pair.reference, knots, sx, sy, stamp_radius, beta, n_max, grid,
-                               radius=r, clip_iterations=0, precision=prec, **layers)
+        try:
+            got = _core.fit_kernel(pair.science, pair.reference, knots, sx, sy, stamp_radius, beta, n_max, grid,
+                                   radius=r, clip_iterations=0, precision=prec, **layers)
+        finally:
+            ctx.set_precision_fallback(True)
         fit_ms = (time.perf_counter() - t1) * 1e3
         th = np.asarray(got["theta"])
         sub = _core.subtract(pair.science, pair.reference, knots, th, beta, n_max, r, pair.saturation, **layers)
         z = (sub["difference"].astype(np.float64) - sub0["difference"])[good] / np.sqrt(var0[good])
         sc = _core.matched_filter(sub["difference"], psf, sub["variance"]).astype(np.float64)
         fin = np.isfinite(sc) & np.isfinite(score0)
-        out["modes"][prec] = {
+        out["modes"][mode] = {
             "theta_rel": float(np.linalg.norm(th - theta0) / np.linalg.norm(theta0)),
             "lambda_equal": bool(got["lambda"] == want["lambda"]), "precision_used": got["precision_used"],
             "refine_correction": float(got["refine_correction"]),

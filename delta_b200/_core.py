@@ -297,16 +297,20 @@ def subtract_batch_native(items, *, n_max: int = 6, n_knots: int = 5, radius: in
                           clip_iterations: int = 5, min_stamps: int = 5, cv_folds: int = 5, precision: str = "fp64",
                           decorrelate: bool = True, block: int = 256, score: bool = True, catalog: bool = True,
                           catalog_threshold_sigma: float = 5.0, frames_in_flight: int = 4,
-                          catalog_capacity: int = 4096) -> list[dict]:
+                          catalog_capacity: int = 4096, graphs: bool = True, alloc=None) -> list[dict]:
     """dgpu_subtract_batch on host frames: ``items`` are dicts of science,
     reference and the optional science_var / reference_var / science_mask /
     reference_mask layers. Returns per frame {difference, variance, mask,
-    score, theta, lambda, beta, direction, n_stamps_used, catalog, seconds}."""
+    score, theta, lambda, beta, direction, n_stamps_used, catalog, seconds,
+    graph_replayed}. ``graphs``: run the post-fit device work of a frame as a
+    recorded CUDA graph once its worker has seen the frame's shape and layers.
+    ``alloc(shape, dtype)``, when given, makes the image outputs (e.g. pinned
+    host memory, which the products are copied into at full link speed)."""
     grid = np.ascontiguousarray(np.logspace(-6, 6, 25) if lambda_grid is None else lambda_grid, np.float64)
     cfg = _lib.BatchConfig(n_max, n_knots, radius, stamp_radius, threshold_sigma, max_stamps, saturation,
                            fwhm_radius, match_radius, grid.ctypes.data, grid.size, clip_sigma, clip_iterations,
                            min_stamps, cv_folds, PRECISIONS[precision], int(decorrelate), block, int(score),
-                           int(catalog), catalog_threshold_sigma, frames_in_flight, 0)
+                           int(catalog), catalog_threshold_sigma, frames_in_flight, 0, int(bool(graphs)))
     n = len(items)
     frames = (_lib.Frame * max(n, 1))()
     results = (_lib.FrameResult * max(n, 1))()
@@ -321,8 +325,9 @@ def subtract_batch_native(items, *, n_max: int = 6, n_knots: int = 5, radius: in
         h, w = sci.shape
         frames[i] = _lib.Frame(w, h, sci.ctypes.data, ref.ctypes.data,
                                *[None if a is None else a.ctypes.data for a in layers])
-        o = {"difference": np.empty((h, w), np.float32), "variance": np.empty((h, w), np.float32),
-             "mask": np.empty((h, w), np.uint8), "score": np.empty((h, w), np.float32) if score else None,
+        mk = alloc or np.empty
+        o = {"difference": mk((h, w), np.float32), "variance": mk((h, w), np.float32),
+             "mask": mk((h, w), np.uint8), "score": mk((h, w), np.float32) if score else None,
              "theta": np.empty((nc + 1) * n_knots * n_knots),
              "cols": {name: np.empty(catalog_capacity, dt) for name, dt in _lib.CATALOG_COLUMNS}}
         outs.append(o)
@@ -346,7 +351,8 @@ def subtract_batch_native(items, *, n_max: int = 6, n_knots: int = 5, radius: in
                     "mask": o["mask"] if r.has_mask else None, "score": o["score"], "theta": o["theta"],
                     "lambda": r.lambda_, "beta": r.beta,
                     "direction": "reference" if r.direction_is_reference else "science",
-                    "n_stamps_used": r.n_stamps_used, "catalog": cat, "seconds": r.seconds})
+                    "n_stamps_used": r.n_stamps_used, "catalog": cat, "seconds": r.seconds,
+                    "graph_replayed": bool(r.graph_replayed)})
     return out
 
 

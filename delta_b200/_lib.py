@@ -146,7 +146,7 @@ class BatchConfig(ctypes.Structure):
                 ("clip_iterations", ctypes.c_int), ("min_stamps", ctypes.c_int), ("cv_folds", ctypes.c_int),
                 ("precision", ctypes.c_int), ("decorrelate", ctypes.c_int), ("block", ctypes.c_int),
                 ("score", ctypes.c_int), ("catalog", ctypes.c_int), ("catalog_threshold_sigma", ctypes.c_double),
-                ("frames_in_flight", ctypes.c_int), ("device", ctypes.c_int)]
+                ("frames_in_flight", ctypes.c_int), ("device", ctypes.c_int), ("graphs", ctypes.c_int)]
 
 
 class FrameResult(ctypes.Structure):
@@ -156,7 +156,7 @@ class FrameResult(ctypes.Structure):
                 ("beta", ctypes.c_double), ("direction_is_reference", ctypes.c_int), ("n_stamps_used", ctypes.c_int),
                 ("has_variance", ctypes.c_int), ("has_mask", ctypes.c_int), ("catalog_count", ctypes.c_int),
                 ("catalog_fetched", ctypes.c_int), ("status", ctypes.c_int), ("error", ctypes.c_char * 256),
-                ("seconds", ctypes.c_double)]
+                ("seconds", ctypes.c_double), ("graph_replayed", ctypes.c_int)]
 
 
 def lib():
@@ -236,6 +236,11 @@ class Context:
 
     def synchronize(self):
         check(lib().dgpu_synchronize(self.handle), self.handle)
+
+    def set_precision_fallback(self, enabled: bool):
+        """Whether a MIXED / TF32 fit that its FP64 refinement shows too
+        inaccurate is redone in FP64 (the default) or returned as it is."""
+        check(lib().dgpu_set_precision_fallback(self.handle, int(bool(enabled))), self.handle)
 
 
 def _default_device() -> int:

@@ -122,6 +122,9 @@ void dgpu_destroy(dgpu_context* ctx) {
   for (int i = 0; i < kSlotCount; ++i)
     if (c->slot_ptr[i]) cudaFreeAsync(c->slot_ptr[i], c->stream);
   cudaStreamSynchronize(c->stream);
+  for (auto& kv : c->graphs)
+    if (kv.second) cudaGraphExecDestroy(kv.second);
+  if (c->arena.base) cudaFreeHost(c->arena.base);
   if (c->d_status) cudaFree(c->d_status);
   if (c->host_stage) cudaFreeHost(c->host_stage);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -168,6 +171,10 @@ int dgpu_autotune_table(char* out, size_t cap, size_t* needed) {
 
 int dgpu_set_label_loop_cap(dgpu_context* ctx, int cap) {
   return guarded(ctx, [&](Context& c) { c.label_loop_cap = cap > 0 ? cap : Context::kDefaultLabelLoopCap; });
+}
+
+int dgpu_set_precision_fallback(dgpu_context* ctx, int enabled) {
+  return guarded(ctx, [&](Context& c) { c.precision_fallback = enabled != 0; });
 }
 
 int dgpu_launch_count(unsigned long long* count) {
@@ -645,7 +652,7 @@ int dgpu_matched_filter(dgpu_context* ctx, int mem, int64_t width, int64_t heigh
       StageTimer t(c, "score: blocked correlation");
       const size_t ntiles = static_cast<size_t>((w + 63) / 64) * ((h + 31) / 32);
       int* nf_buf = static_cast<int*>(c.slot(kSlotScratch0, sizeof(int) * (ntiles + 1)));
-      launch_matched_filter(c.stream, w, h, img, var, psf, dpsf, psf_size, sumpsf2, o, nf_buf);
+      launch_matched_filter(c.stream, w, h, img, var, dpsf, psf_size, sumpsf2, o, nf_buf);
     }
     stage_out(c, mem, out, o, 4 * n);
     if (mem == DGPU_MEM_HOST) check_status(c);

@@ -23,6 +23,7 @@
 #include <mutex>
 #include <numeric>
 #include <thread>
+#include <string>
 #include <vector>
 
 #include "internal.h"
@@ -45,27 +46,57 @@ double default_beta(double fa, double fb) {
   return std::max(0.8 * ks, 0.5);
 }
 
-// Second-moment FWHM of a PSF stamp's positive part (python/delta/catalog.py:60-74).
+// numpy's pairwise summation of a contiguous float64 vector (blocks of at
+// most 128 summed with eight interleaved partials), so the sums below round
+// exactly like the Python pipeline's `.sum()`.
+double np_sum(const double* a, size_t n) {
+  if (n < 8) {
+    double r = 0.0;
+    for (size_t i = 0; i < n; ++i) r += a[i];
+    return r;
+  }
+  if (n <= 128) {
+    double r[8];
+    for (int j = 0; j < 8; ++j) r[j] = a[j];
+    size_t i = 8;
+    for (; i < n - n % 8; i += 8)
+      for (int j = 0; j < 8; ++j) r[j] += a[i + j];
+    double res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+    for (; i < n; ++i) res += a[i];
+    return res;
+  }
+  size_t n2 = n / 2;
+  n2 -= n2 % 8;
+  return np_sum(a, n2) + np_sum(a + n2, n - n2);
+}
+
+// Second-moment FWHM of a PSF stamp's positive part (python/delta/catalog.py:
+// 60-74), with the Python pipeline's element-wise products and sums. This file
+// is compiled without floating-point contraction, so no product here is fused
+// into an FMA that numpy would round separately.
 double psf_fwhm(const std::vector<float>& psf, int side) {
-  double tot = 0.0, mx = 0.0, my = 0.0;
-  for (int y = 0; y < side; ++y)
-    for (int x = 0; x < side; ++x) {
-      const double v = std::max(0.0, static_cast<double>(psf[static_cast<size_t>(y) * side + x]));
-      tot += v;
-      mx += v * x;
-      my += v * y;
-    }
+  const size_t n = static_cast<size_t>(side) * side;
+  std::vector<double> wgt(n), t(n);
+  for (size_t i = 0; i < n; ++i) wgt[i] = std::max(static_cast<double>(psf[i]), 0.0);
+  const double tot = np_sum(wgt.data(), n);
   if (!(tot > 0.0)) fail(DGPU_ERR_RUNTIME, "PSF stamp has no positive flux");
-  mx /= tot;
-  my /= tot;
-  double vx = 0.0, vy = 0.0;
-  for (int y = 0; y < side; ++y)
-    for (int x = 0; x < side; ++x) {
-      const double v = std::max(0.0, static_cast<double>(psf[static_cast<size_t>(y) * side + x]));
-      vx += v * (x - mx) * (x - mx);
-      vy += v * (y - my) * (y - my);
-    }
-  return std::sqrt(0.5 * (vx / tot + vy / tot)) / kFwhmToSigma;
+  auto moment = [&](bool along_x, double centre, bool second) {
+    for (int y = 0; y < side; ++y)
+      for (int x = 0; x < side; ++x) {
+        const size_t i = static_cast<size_t>(y) * side + x;
+        const double c = along_x ? x : y;
+        if (second) {
+          const double d = c - centre;
+          t[i] = wgt[i] * (d * d);
+        } else {
+          t[i] = wgt[i] * c;
+        }
+      }
+    return np_sum(t.data(), n) / tot;
+  };
+  const double mx = moment(true, 0.0, false), my = moment(false, 0.0, false);
+  const double vx = moment(true, mx, true), vy = moment(false, my, true);
+  return std::sqrt(0.5 * (vx + vy)) / kFwhmToSigma;
 }
 
 void check_rc(int rc, dgpu_context* ctx) {
@@ -95,6 +126,75 @@ dgpu_context* acquire_context(int device) {
 void release_context(int device, dgpu_context* c) {
   std::lock_guard<std::mutex> lock(g_pool_mu);
   g_pool.emplace_back(device, c);
+}
+
+// Runs `body` (device work on c.stream, no host synchronisation) as a
+// recorded CUDA graph when the context has run this key before; see
+// dgpu_subtract_batch in include/delta_gpu.h. Returns true when the graph ran.
+template <class F>
+bool run_segment(Context& c, bool graphs, const std::string& key, F&& body) {
+  if (!graphs) {
+    body();
+    return false;
+  }
+  const auto it = c.graphs.find(key);
+  if (it == c.graphs.end()) {
+    body();  // first sight: sizes the workspace, settles the autotuner
+    c.graphs.emplace(key, nullptr);
+    return false;
+  }
+  CaptureArena& a = c.arena;
+  if (a.overflow || !a.base) {  // (re)size the arena; the previous frame's copies have finished
+    const size_t want = std::max<size_t>(size_t(1) << 20, 2 * a.used);
+    if (a.base) DGPU_CUDA(cudaFreeHost(a.base));
+    a.base = nullptr;
+    a.size = 0;
+    void* p = nullptr;
+    DGPU_CUDA(cudaHostAlloc(&p, want, cudaHostAllocDefault));
+    a.base = static_cast<unsigned char*>(p);
+    a.size = want;
+    a.overflow = false;
+  }
+  a.used = 0;
+  cudaGraph_t g = nullptr;
+  DGPU_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+  capture_arena() = &a;
+  bool recorded = true;
+  try {
+    body();
+  } catch (const Failure&) {
+    recorded = false;
+  }
+  capture_arena() = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c.stream, &g);
+  if (!recorded || e != cudaSuccess || g == nullptr) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    body();
+    return false;
+  }
+  cudaGraphExec_t& ex = it->second;
+  if (ex) {
+    cudaGraphExecUpdateResultInfo info{};
+    if (cudaGraphExecUpdate(ex, g, &info) != cudaSuccess) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(ex);
+      ex = nullptr;
+    }
+  }
+  if (!ex) {
+    const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+    if (ie != cudaSuccess) {
+      cudaGetLastError();
+      ex = nullptr;
+      cudaGraphDestroy(g);
+      body();
+      return false;
+    }
+  }
+  cudaGraphDestroy(g);
+  DGPU_CUDA(cudaGraphLaunch(ex, c.stream));
+  return true;
 }
 
 const void* upload(Context& c, const void* host, size_t bytes, Slot s) {
@@ -181,21 +281,28 @@ void run_frame(dgpu_context* handle, const dgpu_batch_config& cfg, int mem, cons
   float* diff = static_cast<float*>(c.slot(kSlotBatch6, 4 * n));
   float* var = static_cast<float*>(c.slot(kSlotBatch7, 4 * n));
   uint8_t* mask = static_cast<uint8_t*>(c.slot(kSlotBatch8, n));
+  const bool decor = cfg.decorrelate && tvar && cvar;
+  float* dw = decor ? static_cast<float*>(c.slot(kSlotBatch9, 4 * n)) : nullptr;
+  float* vw = decor ? static_cast<float*>(c.slot(kSlotBatch10, 4 * n)) : nullptr;
   int hv = 0, hm = 0;
-  check_rc(dgpu_subtract(handle, D, w, h, target, conv, tvar, cvar, tmask, cmask, &model, cfg.saturation, diff, var,
-                         mask, &hv, &hm),
-           handle);
-  if (sci_conv) check_rc(dgpu_negate(handle, D, diff, static_cast<int64_t>(n)), handle);
-  // 5. decorrelate
-  const float* whitened = diff;
-  const float* white_var = hv ? var : nullptr;
-  if (cfg.decorrelate && tvar && cvar) {
-    float* dw = static_cast<float*>(c.slot(kSlotBatch9, 4 * n));
-    float* vw = static_cast<float*>(c.slot(kSlotBatch10, 4 * n));
-    check_rc(dgpu_decorrelate(handle, D, w, h, diff, &model, tvar, cvar, cfg.block, 0, dw, vw), handle);
-    whitened = dw;
-    white_var = vw;
-  }
+  // 4-5. subtract, sign, decorrelate: device work only, recorded as one graph
+  // per shape and layer configuration once this context has run it. (The
+  // basis radius follows each frame's beta; a frame whose radius needs more
+  // workspace than the key's earlier frames is refused while recording and
+  // runs directly.)
+  char key[256];
+  std::snprintf(key, sizeof(key), "%lldx%lld/l%d%d%d%d/s%d/c%d/d%d/b%d/n%d/k%d", static_cast<long long>(w),
+                static_cast<long long>(h), tvar != nullptr, cvar != nullptr, tmask != nullptr, cmask != nullptr,
+                cfg.saturation > 0.0, sci_conv, decor, cfg.block, cfg.n_max, K);
+  r.graph_replayed = run_segment(c, cfg.graphs != 0, key, [&]() {
+    check_rc(dgpu_subtract(handle, D, w, h, target, conv, tvar, cvar, tmask, cmask, &model, cfg.saturation, diff,
+                           var, mask, &hv, &hm),
+             handle);
+    if (sci_conv) check_rc(dgpu_negate(handle, D, diff, static_cast<int64_t>(n)), handle);
+    if (decor) check_rc(dgpu_decorrelate(handle, D, w, h, diff, &model, tvar, cvar, cfg.block, 0, dw, vw), handle);
+  }) ? 1 : 0;
+  const float* whitened = decor ? dw : diff;
+  const float* white_var = decor ? vw : (hv ? var : nullptr);
   // 6. score and catalog
   const float* score = nullptr;
   int n_cat = 0;
@@ -285,6 +392,7 @@ int dgpu_subtract_batch(const dgpu_batch_config* cfg, int mem, int n_frames, con
       const auto t0 = std::chrono::steady_clock::now();
       r.status = DGPU_OK;
       r.error[0] = '\0';
+      r.graph_replayed = 0;
       try {
         run_frame(ctx, *cfg, mem, frames[order[i]], r);
       } catch (const Failure& e) {

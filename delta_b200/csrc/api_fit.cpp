@@ -314,7 +314,7 @@ struct Engine {
   template <class F>
   GlsOut with_fallback(F&& run) {
     GlsOut o = run();
-    if (mixed_failed(o)) {
+    if (c.precision_fallback && mixed_failed(o)) {
       prec = DGPU_PREC_FP64;
       o = run();
     }

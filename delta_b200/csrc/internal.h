@@ -35,6 +35,21 @@ void check_cuda(cudaError_t e, const char* what);
 // other streams in the host-to-device copy engine (a 256 KB piece waits for a
 // whole 70 MB layer upload of another frame; a 32 KB one does not).
 cudaError_t h2d_async(void* dst, const void* src, size_t bytes, cudaStream_t s);
+
+// Recording of a frame segment into a CUDA graph (the batch driver). While the
+// calling thread records, host -> device copies go through a pinned arena that
+// lives with the context (so the recorded copy nodes read memory that stays
+// valid and holds this frame's values), and workspace growth, autotuning,
+// stage timing and stream synchronisation are refused: the recording is then
+// dropped and the segment run directly.
+struct CaptureArena {
+  unsigned char* base = nullptr;
+  size_t size = 0;
+  size_t used = 0;
+  bool overflow = false;
+};
+CaptureArena*& capture_arena();  // this thread's; non-null while recording
+inline bool capturing() { return capture_arena() != nullptr; }
 // Every kernel launch of the library goes through DGPU_LAUNCH, which also
 // counts it (dgpu_launch_count).
 void count_launch();
@@ -85,6 +100,9 @@ struct Context {
   // thread); dgpu_set_label_loop_cap lowers it for fault-handling tests.
   static constexpr int kDefaultLabelLoopCap = 1 << 24;
   int label_loop_cap = kDefaultLabelLoopCap;
+  // Redo a reduced-precision fit in FP64 when its refinement shows it too
+  // inaccurate (dgpu_set_precision_fallback).
+  bool precision_fallback = true;
   void* slot_ptr[kSlotCount] = {};
   size_t slot_size[kSlotCount] = {};
   std::string last_error;
@@ -108,6 +126,12 @@ struct Context {
   // shrinks).
   unsigned char* host_stage = nullptr;
   size_t host_stage_size = 0;
+
+  // Recorded frame segments of the batch driver: key (shape and layer
+  // configuration) -> executable graph (nullptr: seen once, not recorded
+  // yet), and the pinned arena their copy nodes read.
+  std::map<std::string, cudaGraphExec_t> graphs;
+  CaptureArena arena;
 
   void* slot(Slot s, size_t bytes);
   unsigned char* host_staging(size_t bytes);
@@ -149,6 +173,7 @@ int autotune(cudaStream_t s, const std::string& key, const std::vector<int>& can
     launch(cached);
     return cached;
   }
+  if (capturing()) fail(DGPU_ERR_RUNTIME, "autotuning while recording a graph");
   if (!t.enabled() || cands.size() == 1) {
     launch(cands.front());
     t.store(key, cands.front(), {});
@@ -328,9 +353,8 @@ enum SampleKind { kSampleReference = 0, kSampleDifference = 1 };
 void launch_strided_median(Context& c, int kind, int64_t n, const float* values, const uint8_t* mask,
                            float* d_result);
 
-void launch_matched_filter(cudaStream_t s, int w, int h, const float* img, const float* var,
-                           const float* psf_host, const float* psf_dev, int ps, float sumpsf2,
-                           float* out, int* nf_buf);
+void launch_matched_filter(cudaStream_t s, int w, int h, const float* img, const float* var, const float* psf_dev,
+                           int ps, float sumpsf2, float* out, int* nf_buf);
 
 void launch_basis_convolve(cudaStream_t s, int w, int h, const float* img, const Basis& b,
                            const float* taps, float* out);

@@ -11,21 +11,23 @@
 // largest magnitude, read before that step's update (the left-looking variant
 // never updates the trailing diagonal early), first on ties.
 //
-// It runs after every batched solve: a block whose systems all succeeded exits
-// after reading their ok flags. Failed systems are rare (an under-constrained
-// field at lambda ~ 0), so one 1024-thread CTA takes a system at a time, with
-// the matrix in a global workspace (L2-resident):
+// It runs after every batched solve, as three launches over chunks of up to
+// kLdltChunk systems (a system whose Cholesky succeeded leaves each of them at
+// once); a failed system gets a 1024-thread CTA for the factorisation and
+// theta, then P / 128 CTAs for the trace, with its matrices in a per-system
+// global workspace (L2-resident):
 //   factor   P left-looking steps: pivot search (block argmax), symmetric
 //            swap of full rows and columns, d_k by a block reduction, column k
 //            of L by one warp per row (contiguous row reads);
 //   theta    forward substitution by one warp (row-oriented), D^+, backward
 //            substitution column-oriented by the block, inverse permutation;
 //   edf      Z = L^-T D^+ L^-1 (Pi M Pi^T) with one thread per column (no
-//            synchronisation between columns), summed down the diagonal in a
-//            fixed order.
+//            synchronisation between columns), the diagonal summed in a fixed
+//            order by the finishing launch.
 // A solved system is marked ok = 2, so callers can tell which arithmetic
-// produced it. The trace costs O(P^3) and the whole fallback a few
-// milliseconds at P ~ 500; it replaces a failed fit.
+// produced it. Failed systems are rare for a well-posed fit, but a basis far
+// narrower than the pixel scale makes every small-lambda system singular, so
+// all of a batch's failures are factored at once.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,9 +39,16 @@
 namespace dgpu {
 
 constexpr int kLdltThreads = 1024;
-constexpr int kLdltBlocks = 4;
+constexpr int kLdltChunk = 32;      // systems per round of the three launches
+constexpr int kLdltTraceThreads = 128;
 
-size_t ldlt_work_doubles(int P) { return static_cast<size_t>(kLdltBlocks) * (2 * static_cast<size_t>(P) * P + P); }
+// Per-system workspace: A (P x P, then L and D), Y (P x P), D^+ (P), the trace
+// column terms (P) as doubles; then per system the permutation (P) and a
+// factored flag as ints.
+__host__ __device__ inline size_t ldlt_sys_doubles(int P) { return 2 * static_cast<size_t>(P) * P + 2 * static_cast<size_t>(P); }
+size_t ldlt_work_bytes(int P, int nsys) {
+  return sizeof(double) * ldlt_sys_doubles(P) * nsys + sizeof(int) * (static_cast<size_t>(P) + 1) * nsys;
+}
 
 namespace {
 
@@ -212,64 +221,94 @@ __device__ void ldlt_solve_col(const double* A, int P, const int* perm, const do
   }
 }
 
-__global__ void __launch_bounds__(kLdltThreads) k_ldlt_fallback(SolveBatch b, double* __restrict__ work) {
+struct LdltWork {
+  double* d;  // chunk x ldlt_sys_doubles(P)
+  int* i;     // chunk x (P + 1): permutation, factored flag
+};
+
+// One CTA per system of the chunk [s0, s0 + gridDim.x): factor and theta of a
+// failed system; the factored flag tells the next two launches which systems
+// to finish.
+__global__ void __launch_bounds__(kLdltThreads) k_ldlt_factor(SolveBatch b, int s0, LdltWork wk) {
   __shared__ LdltShared S;
   const int P = b.P, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const size_t PP = static_cast<size_t>(P) * P;
-  double* A = work + static_cast<size_t>(blockIdx.x) * (2 * PP + P);
-  double* Y = A + PP;
-  double* dinv = Y + PP;
-  for (int s = blockIdx.x; s < b.nsys; s += gridDim.x) {
-    if (b.ok[s]) continue;  // same value for every thread of the block
-    const double lam = b.lam[s];
-    const double* M = b.M + static_cast<size_t>(b.m_index ? b.m_index[s] : 0) * PP;
-    const double* rhs = b.rhs + static_cast<size_t>(b.r_index ? b.r_index[s] : 0) * P;
-    build_penalised(A, M, P, b.k, lam, b.pen, S.perm);
-    const int n_steps = ldlt_factor_block(A, P, S);
-    ldlt_dinv(A, P, n_steps, dinv);
+  const int s = s0 + static_cast<int>(blockIdx.x);
+  double* A = wk.d + blockIdx.x * ldlt_sys_doubles(P);
+  double* dinv = A + 2 * PP;
+  int* perm = wk.i + blockIdx.x * (static_cast<size_t>(P) + 1);
+  int* factored = perm + P;
+  if (b.ok[s]) {  // same value for every thread of the block
+    if (tid == 0) *factored = 0;
+    return;
+  }
+  const double lam = b.lam[s];
+  const double* M = b.M + static_cast<size_t>(b.m_index ? b.m_index[s] : 0) * PP;
+  const double* rhs = b.rhs + static_cast<size_t>(b.r_index ? b.r_index[s] : 0) * P;
+  build_penalised(A, M, P, b.k, lam, b.pen, S.perm);
+  const int n_steps = ldlt_factor_block(A, P, S);
+  ldlt_dinv(A, P, n_steps, dinv);
 
-    // theta: x = Pi rhs; forward L (unit, row-oriented, one warp); D^+;
-    // backward L^T (column t of L^T = row t of L, the block over i < t).
-    if (warp == 0) {
-      for (int i = 0; i < P; ++i) {
-        const double* Ai = A + static_cast<size_t>(i) * P;
-        double acc = 0.0;
-        for (int j = lane; j < i; j += 32) acc = fma(Ai[j], S.temp[j], acc);
-        acc = warp_sum(acc);
-        if (lane == 0) S.temp[i] = rhs[S.perm[i]] - acc;
-        __syncwarp();
-      }
+  // theta: x = Pi rhs; forward L (unit, row-oriented, one warp); D^+;
+  // backward L^T (column t of L^T = row t of L, the block over i < t).
+  if (warp == 0) {
+    for (int i = 0; i < P; ++i) {
+      const double* Ai = A + static_cast<size_t>(i) * P;
+      double acc = 0.0;
+      for (int j = lane; j < i; j += 32) acc = fma(Ai[j], S.temp[j], acc);
+      acc = warp_sum(acc);
+      if (lane == 0) S.temp[i] = rhs[S.perm[i]] - acc;
+      __syncwarp();
     }
-    __syncthreads();
-    for (int i = tid; i < P; i += blockDim.x) S.temp[i] *= dinv[i];
-    __syncthreads();
-    for (int t = P - 1; t > 0; --t) {
-      const double zt = S.temp[t];
-      const double* At = A + static_cast<size_t>(t) * P;
-      for (int i = tid; i < t; i += blockDim.x) S.temp[i] = fma(-At[i], zt, S.temp[i]);
-      __syncthreads();
-    }
-    for (int i = tid; i < P; i += blockDim.x) b.theta[static_cast<size_t>(s) * P + S.perm[i]] = S.temp[i];
-
-    // edf = tr(A^+ M) = sum_c Z_cc, Z = L^-T D^+ L^-1 B, B = Pi M Pi^T; thread c owns column c.
-    double zc = 0.0;
-    if (tid < P) {
-      const int c = tid, oc = S.perm[c];
-      ldlt_solve_col(A, P, S.perm, dinv, [&](int io) { return M[static_cast<size_t>(io) * P + oc]; }, Y, P, c, c);
-      zc = Y[static_cast<size_t>(c) * P + c];
-    }
-    // Fixed-order sum over the columns.
-    __syncthreads();
-    S.temp[tid] = tid < P ? zc : 0.0;
-    __syncthreads();
-    if (tid == 0) {
-      double e = 0.0;
-      for (int c = 0; c < P; ++c) e += S.temp[c];
-      b.edf[s] = e;
-      b.ok[s] = 2;
-    }
+  }
+  __syncthreads();
+  for (int i = tid; i < P; i += blockDim.x) S.temp[i] *= dinv[i];
+  __syncthreads();
+  for (int t = P - 1; t > 0; --t) {
+    const double zt = S.temp[t];
+    const double* At = A + static_cast<size_t>(t) * P;
+    for (int i = tid; i < t; i += blockDim.x) S.temp[i] = fma(-At[i], zt, S.temp[i]);
     __syncthreads();
   }
+  for (int i = tid; i < P; i += blockDim.x) {
+    b.theta[static_cast<size_t>(s) * P + S.perm[i]] = S.temp[i];
+    perm[i] = S.perm[i];
+  }
+  if (tid == 0) *factored = 1;
+}
+
+// edf term of column c: Z_cc, Z = L^-T D^+ L^-1 B, B = Pi M Pi^T (thread c
+// solves column c). Grid: (chunk systems, ceil(P / 128)).
+__global__ void __launch_bounds__(kLdltTraceThreads) k_ldlt_trace(SolveBatch b, int s0, LdltWork wk) {
+  const int P = b.P;
+  const size_t PP = static_cast<size_t>(P) * P;
+  const int s = s0 + static_cast<int>(blockIdx.x);
+  double* A = wk.d + blockIdx.x * ldlt_sys_doubles(P);
+  double* Y = A + PP;
+  const double* dinv = A + 2 * PP;
+  double* zc = A + 2 * PP + P;
+  const int* perm = wk.i + blockIdx.x * (static_cast<size_t>(P) + 1);
+  if (!perm[P]) return;
+  const int c = static_cast<int>(blockIdx.y) * kLdltTraceThreads + static_cast<int>(threadIdx.x);
+  if (c >= P) return;
+  const double* M = b.M + static_cast<size_t>(b.m_index ? b.m_index[s] : 0) * PP;
+  const int oc = perm[c];
+  ldlt_solve_col(A, P, perm, dinv, [&](int io) { return M[static_cast<size_t>(io) * P + oc]; }, Y, P, c, c);
+  zc[c] = Y[static_cast<size_t>(c) * P + c];
+}
+
+// edf = sum_c Z_cc in column order; ok = 2.
+__global__ void k_ldlt_finish(SolveBatch b, int s0, LdltWork wk) {
+  const int P = b.P;
+  const size_t PP = static_cast<size_t>(P) * P;
+  const int s = s0 + static_cast<int>(blockIdx.x);
+  const int* perm = wk.i + blockIdx.x * (static_cast<size_t>(P) + 1);
+  if (threadIdx.x != 0 || !perm[P]) return;
+  const double* zc = wk.d + blockIdx.x * ldlt_sys_doubles(P) + 2 * PP + P;
+  double e = 0.0;
+  for (int c = 0; c < P; ++c) e += zc[c];
+  b.edf[s] = e;
+  b.ok[s] = 2;
 }
 
 // X = A^+ B for A = M + lambda P0 (one CTA): B and X are P x m, row-major, in
@@ -302,10 +341,21 @@ void launch_sym_solve_many(Context& c, int P, int k, const double* M, double lam
 void launch_ldlt_fallback(Context& c, const SolveBatch& b) {
   if (b.nsys <= 0) return;
   if (b.P > kLdltThreads) fail(DGPU_ERR_INVALID, "solve: the LDLT fallback supports at most 1024 unknowns");
-  double* work = static_cast<double*>(c.slot(kSlotLdlt, sizeof(double) * ldlt_work_doubles(b.P)));
-  const int blocks = std::min(b.nsys, kLdltBlocks);
-  k_ldlt_fallback<<<blocks, kLdltThreads, 0, c.stream>>>(b, work);
-  DGPU_LAUNCH("k_ldlt_fallback");
+  const int chunk = std::min(b.nsys, kLdltChunk);
+  char* work = static_cast<char*>(c.slot(kSlotLdlt, ldlt_work_bytes(b.P, chunk)));
+  LdltWork wk;
+  wk.d = reinterpret_cast<double*>(work);
+  wk.i = reinterpret_cast<int*>(work + sizeof(double) * ldlt_sys_doubles(b.P) * chunk);
+  for (int s0 = 0; s0 < b.nsys; s0 += chunk) {
+    const int m = std::min(chunk, b.nsys - s0);
+    k_ldlt_factor<<<m, kLdltThreads, 0, c.stream>>>(b, s0, wk);
+    DGPU_LAUNCH("k_ldlt_factor");
+    k_ldlt_trace<<<dim3(m, (b.P + kLdltTraceThreads - 1) / kLdltTraceThreads), kLdltTraceThreads, 0, c.stream>>>(
+        b, s0, wk);
+    DGPU_LAUNCH("k_ldlt_trace");
+    k_ldlt_finish<<<m, 32, 0, c.stream>>>(b, s0, wk);
+    DGPU_LAUNCH("k_ldlt_finish");
+  }
 }
 
 }  // namespace dgpu

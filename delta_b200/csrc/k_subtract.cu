@@ -374,8 +374,17 @@ size_t model_convolve_smem(int nx, int ks, int TH) {
                           static_cast<size_t>(nx) * (nrows + kMcPad) * kMcTW + static_cast<size_t>(nx) * mc_tap_stride(ks));
 }
 
+size_t model_convolve_fast_smem(int nx, int ks, int TH);
+bool model_convolve_fast_available(int nx, int ks);
+bool launch_model_convolve_fast(cudaStream_t s, const SubtractArgs& a, const int2* orders, int TH);
+
 static void launch_mc_th(cudaStream_t s, const SubtractArgs& a, const int2* orders, bool stack, int TH) {
   const int nx = a.n_max + 1;
+  // The common basis shapes run the compile-time-shaped kernel (same bits;
+  // DELTA_MODEL_CONVOLVE_GENERIC=1 forces this generic one, a diagnostic the
+  // tests use to compare the two).
+  const char* generic = std::getenv("DELTA_MODEL_CONVOLVE_GENERIC");
+  if (!stack && !(generic && generic[0] == '1') && launch_model_convolve_fast(s, a, orders, TH)) return;
   const size_t smem = model_convolve_smem(nx, a.ks, TH);
   switch (nx) {
     case 1: stack ? launch_mc<1, true>(s, a, orders, TH, smem) : launch_mc<1, false>(s, a, orders, TH, smem); break;
@@ -400,18 +409,19 @@ static void launch_mc_th(cudaStream_t s, const SubtractArgs& a, const int2* orde
 // an SM, otherwise the tallest that fits.
 void launch_model_convolve_orders(cudaStream_t s, const SubtractArgs& a, const int2* orders, bool stack) {
   const int nx = a.n_max + 1;
+  const bool fast = !stack && model_convolve_fast_available(nx, a.ks);
+  auto smem_of = [&](int th) { return fast ? model_convolve_fast_smem(nx, a.ks, th) : model_convolve_smem(nx, a.ks, th); };
   const size_t kTwoPerSm = 112 * 1024, kMaxSmem = 200 * 1024;
   int TH = 64;
-  while (TH > 8 && model_convolve_smem(nx, a.ks, TH) > kTwoPerSm) TH /= 2;
-  if (model_convolve_smem(nx, a.ks, TH) > kTwoPerSm) {
+  while (TH > 8 && smem_of(TH) > kTwoPerSm) TH /= 2;
+  if (smem_of(TH) > kTwoPerSm) {
     TH = 64;
-    while (TH > 8 && model_convolve_smem(nx, a.ks, TH) > kMaxSmem) TH /= 2;
+    while (TH > 8 && smem_of(TH) > kMaxSmem) TH /= 2;
   }
-  if (model_convolve_smem(nx, a.ks, TH) > kMaxSmem)
-    fail(DGPU_ERR_INVALID, "subtract: kernel footprint too large for the tile engine");
+  if (smem_of(TH) > kMaxSmem) fail(DGPU_ERR_INVALID, "subtract: kernel footprint too large for the tile engine");
   std::vector<int> cands{TH};
   for (int t : {64, 32, 16})
-    if (t != TH && model_convolve_smem(nx, a.ks, t) <= kMaxSmem) cands.push_back(t);
+    if (t != TH && smem_of(t) <= kMaxSmem) cands.push_back(t);
   int size_class = 0;
   for (int64_t px = static_cast<int64_t>(a.w) * a.h; px > 1; px >>= 2) ++size_class;
   // DELTA_MODEL_CONVOLVE_TH forces one candidate (a diagnostic: the tests
@@ -423,7 +433,8 @@ void launch_model_convolve_orders(cudaStream_t s, const SubtractArgs& a, const i
       return;
     }
   }
-  const std::string key = std::string("model_convolve") + (stack ? "/stack" : "") + "/nx" + std::to_string(nx) +
+  const std::string key = std::string("model_convolve") + (stack ? "/stack" : fast ? "/fast" : "") + "/nx" +
+                          std::to_string(nx) +
                           "/ks" + std::to_string(a.ks) + "/px4^" + std::to_string(size_class);
   autotune(s, key, cands, [&](int th) { launch_mc_th(s, a, orders, stack, th); });
 }

@@ -8,6 +8,7 @@
 #include <utility>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <stdexcept>
 
 #include <algorithm>
@@ -23,7 +24,23 @@ void check_cuda(cudaError_t e, const char* what) {
   if (e != cudaSuccess) fail(DGPU_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+CaptureArena*& capture_arena() {
+  static thread_local CaptureArena* a = nullptr;
+  return a;
+}
+
 cudaError_t h2d_async(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (CaptureArena* a = capture_arena()) {
+    const size_t off = (a->used + 15) & ~size_t(15);
+    if (off + bytes > a->size) {
+      a->used = off + bytes;
+      a->overflow = true;
+      return cudaErrorMemoryAllocation;
+    }
+    std::memcpy(a->base + off, src, bytes);
+    a->used = off + bytes;
+    return cudaMemcpyAsync(dst, a->base + off, bytes, cudaMemcpyHostToDevice, s);
+  }
   constexpr size_t kPiece = size_t(32) << 10, kSplitMax = size_t(1) << 20;
   if (bytes <= kPiece || bytes > kSplitMax)
     return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
@@ -50,6 +67,7 @@ cudaError_t h2d_async(void* dst, const void* src, size_t bytes, cudaStream_t s) 
 void* Context::slot(Slot s, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (slot_size[s] >= bytes) return slot_ptr[s];
+  if (capturing()) fail(DGPU_ERR_RUNTIME, "workspace growth while recording a graph");
   if (slot_ptr[s]) {
     DGPU_CUDA(cudaFreeAsync(slot_ptr[s], stream));
     slot_ptr[s] = nullptr;
@@ -115,6 +133,7 @@ void keep_pool_memory(int device) {
 
 unsigned char* Context::host_staging(size_t bytes) {
   if (host_stage_size >= bytes) return host_stage;
+  if (capturing()) fail(DGPU_ERR_RUNTIME, "staging growth while recording a graph");
   // Growing: copies queued on the stream may still target the old buffer.
   if (host_stage) {
     DGPU_CUDA(cudaStreamSynchronize(stream));
@@ -133,6 +152,7 @@ unsigned char* Context::host_staging(size_t bytes) {
 void reset_status(Context& c) { DGPU_CUDA(cudaMemsetAsync(c.d_status, 0, sizeof(unsigned), c.stream)); }
 
 void check_status(Context& c) {
+  if (capturing()) fail(DGPU_ERR_RUNTIME, "a synchronising check while recording a graph");
   unsigned st = 0;
   DGPU_CUDA(cudaMemcpyAsync(&st, c.d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, c.stream));
   DGPU_CUDA(cudaStreamSynchronize(c.stream));
@@ -158,7 +178,7 @@ void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 StageTimer::StageTimer(Context& ctx, const char* l) : c(ctx), label(l) {
-  if (!c.timing_enabled) return;
+  if (!c.timing_enabled || capturing()) return;  // recorded segments are not stage-timed
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, c.stream);

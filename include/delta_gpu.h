@@ -87,6 +87,15 @@ int dgpu_autotune_table(char* out, size_t cap, size_t* needed);
  * stays usable. cap <= 0 restores the default (2^24, far above any real
  * chain). Lowering it is how the failure path is tested. */
 int dgpu_set_label_loop_cap(dgpu_context* ctx, int cap);
+/* Reduced-precision fallback of the kernel fit on this context (no reference
+ * counterpart: the reference builds its normal equations in FP64 only). With
+ * enabled != 0 (the default) a DGPU_PREC_MIXED / DGPU_PREC_TF32 fit whose
+ * FP64 refinement correction exceeds 1e-2 of theta, whose solve is
+ * non-finite, or whose chosen system needed the LDLT fallback is redone with
+ * FP64 normal equations (precision_used reports which ran). With enabled == 0
+ * the tensor-core result is returned as it is, with its refine_correction:
+ * this is how the precision study measures each build's own error. */
+int dgpu_set_precision_fallback(dgpu_context* ctx, int enabled);
 
 /* ---- basis (host math) ---------------------------------------------------- */
 /* GaussHermiteBasis::default_radius, src/basis.cpp:9-12. */
@@ -484,6 +493,7 @@ typedef struct {
   double catalog_threshold_sigma; /* 5.0 */
   int frames_in_flight;           /* 4 */
   int device;                     /* CUDA device index */
+  int graphs;                     /* 1: record the post-fit segment as a CUDA graph (see below) */
 } dgpu_batch_config;
 
 /* Products of one frame. Image buffers are caller memory of width x height
@@ -512,7 +522,8 @@ typedef struct {
   int catalog_fetched;
   int status;
   char error[256];
-  double seconds; /* wall time of the frame on its worker */
+  double seconds;     /* wall time of the frame on its worker */
+  int graph_replayed; /* 1: the post-fit segment ran as a recorded graph */
 } dgpu_frame_result;
 
 /* subtract() over many frames of any sizes (the reference's per-frame
@@ -522,7 +533,18 @@ typedef struct {
  * stream from a process-wide pool (workspace kept between calls). Returns
  * DGPU_OK when every frame succeeded, else the first failed frame's status
  * (each frame's status / error are in its result); text via
- * dgpu_last_error(NULL). */
+ * dgpu_last_error(NULL).
+ *
+ * With cfg->graphs != 0 the device work after the kernel fit (subtraction,
+ * sign, decorrelation: some forty launches) runs as one CUDA graph launch.
+ * No reference counterpart. A worker context runs the first frame of each
+ * layer configuration and shape directly (that sizes its workspace and
+ * settles the autotuner); later frames of that key are recorded into a graph
+ * -- the frame's small tables go through a pinned arena of the context --
+ * and the key's executable graph is updated in place (instantiated when the
+ * update is refused) and launched. A recording that meets anything that
+ * cannot be recorded is dropped and the segment run directly. Results are the
+ * same bits either way. */
 int dgpu_subtract_batch(const dgpu_batch_config* cfg, int mem, int n_frames, const dgpu_frame* frames,
                         dgpu_frame_result* results);
 

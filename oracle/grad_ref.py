@@ -43,6 +43,31 @@ def shifted_basis1d(beta: float, n_max: int, radius: int, d: float):
     return g, dg
 
 
+def model_image(reference, knots, theta, beta, n_max, radius=0, dx=0.0, dy=0.0, scale=1.0, reference_mask=None):
+    """M = s * sum_c a_c (K_c^d (*) R~) + b in FP64, one component at a time
+    (the convolved basis images are never stacked), with the float32 lattice
+    fields of subtract.cpp. Used to synthesise an exposure whose shift and
+    scale are known in the model's own parametrisation."""
+    ref = np.asarray(reference, np.float32)
+    h, w = ref.shape
+    r = nr.resolve_radius(beta, n_max, radius)
+    orders = nr.basis_orders(n_max)
+    nc = len(orders)
+    rmask = None if reference_mask is None else np.asarray(reference_mask, np.uint8)
+    fill = nr.reference_fill_value(ref, rmask)
+    rs = nr.sanitized_reference(ref, rmask, fill).astype(np.float64)
+    fields = nr.Fields(knots, theta, nc, w, h)
+    g, _ = shifted_basis1d(beta, n_max, r, dx)
+    gy, _ = shifted_basis1d(beta, n_max, r, dy)
+    m = np.zeros((h, w))
+    for nx in range(n_max + 1):
+        xpass = nr.convolve_x(rs, g[nx])
+        for c, (ox, oy) in enumerate(orders):
+            if ox == nx:
+                m += fields.field_full(c).astype(np.float64) * nr.convolve_y(xpass, gy[oy])
+    return scale * m + fields.field_full(nc).astype(np.float64)
+
+
 class KernelModel:
     """The objective on one frame: fixed S, R, W, knots and basis; the
     parameters theta, (dx, dy), s vary."""

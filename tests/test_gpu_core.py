@@ -347,7 +347,38 @@ def test_model_convolve_tile_heights_give_identical_bits_and_autotune_records():
     buf = ctypes.create_string_buffer(4096)
     _lib.check(_lib.lib().dgpu_autotune_table(buf, ctypes.c_size_t(4096), ctypes.byref(need)))
     table = buf.value.decode()
-    assert "model_convolve/nx6" in table and "ms" in table, table
+    assert "model_convolve/fast/nx6" in table and "ms" in table, table
+
+
+@pytest.mark.parametrize("n_max,radius,beta", [(2, 0, 2.0), (3, 0, 1.5), (4, 10, 1.0), (5, 7, 1.7), (6, 11, 1.36),
+                                               (6, 16, 2.0), (6, 14, 1.8), (4, 4, 0.8)])
+def test_model_convolve_fast_kernel_equals_generic(n_max, radius, beta):
+    """The compile-time-shaped model convolve (common n_max and tap counts,
+    taps zero padded to a multiple of 8, packed field blend) gives the generic
+    tile kernel's bits on a frame with masked, non-finite and off-frame
+    reference pixels, on the coarse-lattice and the exact-field paths."""
+    import os
+
+    for (h, w, nk) in ((530, 700, 3), (90, 75, 3)):
+        rng = np.random.default_rng(n_max * 100 + radius)
+        p = validation.synthetic_pair(w, h, 120, n_max, mask_fraction=0.01)
+        ref = p.reference.copy()
+        ref[rng.integers(0, h, 6), rng.integers(0, w, 6)] = np.nan
+        ref[rng.integers(0, h, 3), rng.integers(0, w, 3)] = -np.inf
+        knots = nr.grid_knots(0, 0, w - 1, h - 1, nk, nk)
+        nc = (n_max + 1) * (n_max + 2) // 2
+        theta = _theta(rng, nc, knots.shape[0])
+        args = (p.science, ref, knots, theta, beta, n_max, radius, p.saturation, p.science_var, p.reference_var,
+                p.science_mask, p.reference_mask)
+        fast = _core.subtract(*args)
+        try:
+            os.environ["DELTA_MODEL_CONVOLVE_GENERIC"] = "1"
+            generic = _core.subtract(*args)
+        finally:
+            os.environ.pop("DELTA_MODEL_CONVOLVE_GENERIC", None)
+        for name in ("difference", "variance", "mask"):
+            assert np.array_equal(fast[name].view(np.uint32) if name != "mask" else fast[name],
+                                  generic[name].view(np.uint32) if name != "mask" else generic[name]), (name, h, w)
 
 
 @pytest.mark.parametrize("n,seed", [(1, 0), (2, 1), (1001, 2), (1000, 3), (4_000_000, 4)])

@@ -452,6 +452,32 @@ def test_native_batch_matches_subtract_one_at_a_time():
         _core.subtract_batch_native([dict(science=blank, reference=blank)], score=False, decorrelate=False)
 
 
+def test_native_batch_graph_replay_gives_the_same_bits():
+    """dgpu_subtract_batch with the post-fit device work recorded as CUDA graphs
+    (a worker runs the first frame of a shape directly, then records and
+    replays): the same bits as the direct launches, frame by frame, and the
+    repeated shapes did replay."""
+    shapes = ((320, 384, 51), (256, 320, 52), (320, 384, 53), (256, 320, 54), (320, 384, 55), (256, 320, 56))
+    ps = [validation.synthetic_pair(w, h, 180, s, mask_fraction=0.005) for w, h, s in shapes]
+    kw = dict(n_max=4, n_knots=3, stamp_radius=12, cv_folds=0, decorrelate=True, block=64, precision="mixed",
+              saturation=ps[0].saturation, catalog=True)
+    items = [dict(science=p.science, reference=p.reference, science_var=p.science_var,
+                  reference_var=p.reference_var, science_mask=p.science_mask, reference_mask=p.reference_mask)
+             for p in ps]
+    direct = _core.subtract_batch_native(items, frames_in_flight=1, graphs=False, **kw)
+    replay = _core.subtract_batch_native(items, frames_in_flight=1, graphs=True, **kw)
+    again = _core.subtract_batch_native(items, frames_in_flight=2, graphs=True, **kw)
+    assert sum(r["graph_replayed"] for r in replay) >= 2
+    assert all(not r["graph_replayed"] for r in direct)
+    for run in (replay, again):
+        for a, b in zip(direct, run, strict=True):
+            np.testing.assert_array_equal(a["theta"], b["theta"])
+            for name in ("difference", "variance", "mask", "score"):
+                np.testing.assert_array_equal(a[name], b[name], err_msg=name)
+            for name in a["catalog"]:
+                np.testing.assert_array_equal(a["catalog"][name], b["catalog"][name], err_msg=name)
+
+
 def test_variance_rescale_on_the_device_matches_host_staged():
     """rescale_variance=True: the device-resident path scales Var(D) and the
     whitened variance with the library's kernel (a float32 product, as the
