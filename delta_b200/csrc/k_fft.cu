@@ -124,8 +124,31 @@ __host__ __device__ constexpr int bitrev_c(int i, int bits) {
   return r;
 }
 
-template <int M, int LOGM>
-__device__ __forceinline__ void reg_fft(float2 (&v)[M], const float2* tw, int tstride) {
+// v * W_16^j for the unrolled (compile-time) j of a register FFT, SIGN = -1
+// forward (W = exp(-2 pi i / 16)), +1 inverse: j = 0 is the identity, j = 4
+// the exact swap by -+i, the others one complex multiply by constants equal to
+// the twiddle table's float values (cos / sin of j pi / 8 rounded from FP64).
+template <int SIGN>
+__device__ __forceinline__ float2 mul_w16(float2 v, int j) {
+  if (j == 0) return v;
+  if (j == 4) return SIGN < 0 ? make_float2(v.y, -v.x) : make_float2(-v.y, v.x);
+  float c, sn;
+  switch (j) {
+    case 1: c = 0.923879532511286738f; sn = 0.382683432365089772f; break;
+    case 2: c = 0.707106781186547524f; sn = 0.707106781186547524f; break;
+    case 3: c = 0.382683432365089772f; sn = 0.923879532511286738f; break;
+    case 5: c = -0.382683432365089772f; sn = 0.923879532511286738f; break;
+    case 6: c = -0.707106781186547524f; sn = 0.707106781186547524f; break;
+    default: c = -0.923879532511286738f; sn = 0.382683432365089772f; break;  // j == 7
+  }
+  return cmul(v, make_float2(c, SIGN < 0 ? -sn : sn));
+}
+
+// In-register radix-2 FFT of M = 8 or 16 points (a sub-FFT of a four-step
+// line of N = 128 or 256): every butterfly twiddle is a 16th root of unity,
+// W_16^(pos * 8 / half), so none is loaded.
+template <int M, int LOGM, int SIGN>
+__device__ __forceinline__ void reg_fft(float2 (&v)[M]) {
 #pragma unroll
   for (int i = 0; i < M; ++i) {
     const int r = bitrev_c(i, LOGM);
@@ -141,17 +164,16 @@ __device__ __forceinline__ void reg_fft(float2 (&v)[M], const float2* tw, int ts
     for (int j = 0; j < M / 2; ++j) {
       const int pos = j & (half - 1);
       const int i0 = ((j - pos) << 1) + pos, i1 = i0 + half;
-      const float2 w = tw[pos * (M / (2 * half)) * tstride];
       const float2 a = v[i0];
-      const float2 c = cmul(v[i1], w);
+      const float2 c = mul_w16<SIGN>(v[i1], pos * 8 / half);
       v[i0] = cadd(a, c);
       v[i1] = csub(a, c);
     }
   }
 }
 
-template <int N>
-__device__ void fft_lines_4step(float2* x, int L, int ls, const float2* tw) {
+template <int N, int SIGN>
+__device__ void fft_lines_4step_d(float2* x, int L, int ls, const float2* tw) {
   constexpr int N1 = 16, N2 = N / 16;
   constexpr int LOGN2 = N == 256 ? 4 : 3;
   constexpr int kLinesA = 256 / N2, kLinesB = 256 / N1;
@@ -163,7 +185,7 @@ __device__ void fft_lines_4step(float2* x, int L, int ls, const float2* tw) {
       float2* xl = x + line * ls;
 #pragma unroll
       for (int n1 = 0; n1 < N1; ++n1) v[n1] = xl[N2 * n1 + n2];
-      reg_fft<N1, 4>(v, tw, N2);
+      reg_fft<N1, 4, SIGN>(v);
 #pragma unroll
       for (int k1 = 1; k1 < N1; ++k1) {
         const int m = n2 * k1;
@@ -188,7 +210,7 @@ __device__ void fft_lines_4step(float2* x, int L, int ls, const float2* tw) {
       const float2* xl = x + line * ls;
 #pragma unroll
       for (int n2 = 0; n2 < N2; ++n2) u[n2] = xl[k1 * (N2 + 1) + n2];
-      reg_fft<N2, LOGN2>(u, tw, N1);
+      reg_fft<N2, LOGN2, SIGN>(u);
     }
     __syncthreads();
     if (act) {
@@ -208,12 +230,14 @@ __host__ __device__ __forceinline__ int fft_ls(int m, bool transposed) {
   return transposed ? m + 1 : m;
 }
 
-// Dispatch: four-step for 128 / 256, radix-2 otherwise.
+// Dispatch: four-step for 128 / 256, radix-2 otherwise. SIGN is the
+// direction of `tw` (-1 forward, +1 inverse), known at every call site.
+template <int SIGN>
 __device__ __forceinline__ void fft_lines(float2* x, int L, int m, int logm, const float2* tw, int ls) {
   if (m == 256)
-    fft_lines_4step<256>(x, L, ls, tw);
+    fft_lines_4step_d<256, SIGN>(x, L, ls, tw);
   else if (m == 128)
-    fft_lines_4step<128>(x, L, ls, tw);
+    fft_lines_4step_d<128, SIGN>(x, L, ls, tw);
   else
     smem_fft(x, L, m, logm, tw, ls);
 }
@@ -272,7 +296,7 @@ k_rows_fwd(FftGeom G, int mode, const float* __restrict__ src, int w, int h, con
     z[rr * zl + j] = make_float2(a, b);
   }
   __syncthreads();
-  fft_lines(z, rows, hn, G.logn - 1, tw, zl);
+  fft_lines<-1>(z, rows, hn, G.logn - 1, tw, zl);
   for (int e = threadIdx.x; e < rows * nb; e += blockDim.x) {
     const int rr = e / nb, k = e - rr * nb;
     const float2 zk = z[rr * zl + (k % hn)];
@@ -314,7 +338,7 @@ k_cols(FftGeom G, int mode, float2* __restrict__ spec, const double* __restrict_
       x[cc * ls + row] = cc < ncol ? sp[static_cast<size_t>(row) * nb + c0 + cc] : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    fft_lines(x, C, n, G.logn, tw, ls);
+    fft_lines<-1>(x, C, n, G.logn, tw, ls);
   }
   if (mode == 1) {
     for (int e = threadIdx.x; e < C * n; e += blockDim.x) {
@@ -346,7 +370,7 @@ k_cols(FftGeom G, int mode, float2* __restrict__ spec, const double* __restrict_
   else
     make_twiddles(tw, n, +1);
   __syncthreads();
-  fft_lines(x, C, n, G.logn, tw, ls);
+  fft_lines<1>(x, C, n, G.logn, tw, ls);
   for (int e = threadIdx.x; e < C * n; e += blockDim.x) {
     const int row = e / C, cc = e - row * C;
     if (cc < ncol) sp[static_cast<size_t>(row) * nb + c0 + cc] = x[cc * ls + row];
@@ -399,7 +423,7 @@ k_rows_inv(FftGeom G, int mode, const float2* __restrict__ spec, const int* __re
     z[rr * zl + k] = make_float2(e2.x - o2.y, e2.y + o2.x);  // 2E + i 2O
   }
   __syncthreads();
-  fft_lines(z, rows, hn, G.logn - 1, tw, zl);
+  fft_lines<1>(z, rows, hn, G.logn - 1, tw, zl);
   const float inv_n2 = 1.0f / static_cast<float>(static_cast<size_t>(n) * n);
   if (mode == 2) {  // raw real block output for the overlap-add gather (dense_out: item x n x n)
     for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
@@ -441,24 +465,30 @@ k_rows_inv(FftGeom G, int mode, const float2* __restrict__ spec, const int* __re
 // ---------------------------------------------------------------------------
 // Fused block filter for the default 256 x 256 block (mode 0 of the three
 // passes above, in one launch): one cluster of 4 CTAs per block. Rank r keeps
-// spectrum columns [cb_r, cb_r + 33 or 32) as transposed column lines in its
-// shared memory and runs the row passes of rows 64 r .. 64 r + 63. Row pass:
-// the r2c rows are scattered into the owners' column lines (distributed
-// shared memory); column pass: forward FFT, filter, inverse FFT on local
-// lines; row inverse: every row gathers its bins from the owners, c2r, raw
-// block output (item x n x n) for the overlap-add gather. The per-line
-// arithmetic is that of k_rows_fwd / k_cols / k_rows_inv, so the output is
-// the same; the spectrum never leaves the chip.
+// spectrum columns [32 r, 32 r + 32) as transposed column lines in its shared
+// memory (with the Nyquist column packed into rank 0's DC line, see bf_owner)
+// and runs the row passes of rows 64 r .. 64 r + 63. Row pass: the r2c rows
+// are scattered into the owners' column lines (distributed shared memory);
+// column pass: forward FFT, filter, inverse FFT on local lines; row inverse:
+// every row gathers its bins from the owners, c2r, raw block output
+// (item x n x n) for the overlap-add gather. The row and column arithmetic is
+// that of k_rows_fwd / k_cols / k_rows_inv except for the packed DC / Nyquist
+// pair (the same transforms to FP32 rounding); the spectrum never leaves the
+// chip.
 // ---------------------------------------------------------------------------
 constexpr int kBfRanks = 4;
 constexpr int kBfN = 256;
 constexpr int kBfBatch = 16;  // rows per row-pass batch
-constexpr int kBfCols = 33;   // column lines held by rank 0 (32 by the others)
+constexpr int kBfCols = 32;   // column lines per rank
 
-__device__ __forceinline__ int bf_owner(int k) { return k < kBfCols ? 0 : (k - 1) >> 5; }
-__device__ __forceinline__ int bf_cb(int r) { return r == 0 ? 0 : 32 * r + 1; }
+// Bins 1..127 of every row live in line k % 32 of rank k / 32. The DC (k = 0)
+// and Nyquist (k = 128) bins of a real row are real, so their two columns share
+// rank 0's line 0 as one complex sequence (DC in the real part, Nyquist in the
+// imaginary part): one column FFT carries both, and every rank holds 32 lines.
+__device__ __forceinline__ int bf_owner(int k) { return k >> 5; }
+__device__ __forceinline__ int bf_cb(int r) { return 32 * r; }
 
-__global__ void __cluster_dims__(kBfRanks, 1, 1) __launch_bounds__(256)
+__global__ void __cluster_dims__(kBfRanks, 1, 1) __launch_bounds__(256, 2)
 k_block_filter(FftGeom G, const float* __restrict__ src, int w, int h, const int* __restrict__ oxs,
                const int* __restrict__ oys, int nox, const double* __restrict__ cell_power,
                const double* __restrict__ cell_sumk2, const int* __restrict__ block_cell,
@@ -485,7 +515,7 @@ k_block_filter(FftGeom G, const float* __restrict__ src, int w, int h, const int
     return cl.map_shared_rank(x + (k - bf_cb(q)) * ls + row, q);
   };
   const int bx = oxs[item % nox], by = oys[item / nox];
-  const int ncol = rank == 0 ? kBfCols : 32;
+  const int ncol = kBfCols;
   const int rbeg = rank * (n / kBfRanks), rend = rbeg + n / kBfRanks;
   cl.sync();  // every rank has started before its shared memory is written
 
@@ -509,7 +539,7 @@ k_block_filter(FftGeom G, const float* __restrict__ src, int w, int h, const int
       }
     }
     __syncthreads();
-    fft_lines(z, kBfBatch, hn, G.logn - 1, tw_fwd_hn, zl);
+    fft_lines<-1>(z, kBfBatch, hn, G.logn - 1, tw_fwd_hn, zl);
 #pragma unroll
     for (int i = 0; i < (kBfBatch * nb + 255) / 256; ++i) {
       const int e = tid + 256 * i;
@@ -520,7 +550,11 @@ k_block_filter(FftGeom G, const float* __restrict__ src, int w, int h, const int
       const float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
       const float2 d = csub(zk, zc);
       const float2 od = make_float2(0.5f * d.y, -0.5f * d.x);
-      *bin(k, b0 + rr) = cadd(ev, cmul(split_fwd[k], od));
+      const float2 X = cadd(ev, cmul(split_fwd[k], od));
+      if (k == 0 || k == hn)  // real: into the packed line (separate 4-byte words)
+        reinterpret_cast<float*>(cl.map_shared_rank(x + b0 + rr, 0))[k == 0 ? 0 : 1] = X.x;
+      else
+        *bin(k, b0 + rr) = X;
     }
     __syncthreads();
   }
@@ -528,8 +562,11 @@ k_block_filter(FftGeom G, const float* __restrict__ src, int w, int h, const int
 
   // Column pass: forward, filter (src/noise.cpp:414-422), inverse. Filter:
   // lane = column (coalesced kernel-power loads), warps over rows; rank 0's
-  // 33rd column by a thread per row.
-  fft_lines(x, ncol, n, G.logn, tw_fwd_n, ls);
+  // packed line by a thread per bin pair (k, n - k): the transform Z of
+  // DC + i Nyquist splits into A = (Z_k + conj Z_-k) / 2 (the DC column's) and
+  // B = (Z_k - conj Z_-k) / 2i (the Nyquist column's), each is filtered with
+  // its own column's factor, and A + iB is put back.
+  fft_lines<-1>(x, ncol, n, G.logn, tw_fwd_n, ls);
   {
     const int cell = block_cell[item];
     const double vs = vsr[2 * item], vr = vsr[2 * item + 1];
@@ -543,17 +580,35 @@ k_block_filter(FftGeom G, const float* __restrict__ src, int w, int h, const int
       xv = make_float2(xv.x * f, xv.y * f);
     };
     const int cc = tid & 31, r0 = tid >> 5;
-    for (int rb = 0; rb < n; rb += 64) {
-      double p[8];
+    if (rank != 0 || cc != 0) {
+      for (int rb = 0; rb < n; rb += 64) {
+        double p[8];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) p[i] = __ldg(pw + static_cast<size_t>(rb + r0 + 8 * i) * nb + cc);
+        for (int i = 0; i < 8; ++i) p[i] = __ldg(pw + static_cast<size_t>(rb + r0 + 8 * i) * nb + cc);
 #pragma unroll
-      for (int i = 0; i < 8; ++i) scale(cc, rb + r0 + 8 * i, p[i]);
+        for (int i = 0; i < 8; ++i) scale(cc, rb + r0 + 8 * i, p[i]);
+      }
     }
-    if (ncol > 32) scale(32, tid, __ldg(pw + static_cast<size_t>(tid) * nb + 32));
+    if (rank == 0 && tid <= hn) {
+      auto factor = [&](int row, int col) {
+        const double denom = vs + vr * __ldg(pw + static_cast<size_t>(row) * nb + col);
+        return denom > 0.0 ? static_cast<float>(cnum / sqrt(denom)) : 0.0f;
+      };
+      const int k = tid, m = (n - k) & (n - 1);
+      const float2 zk = x[k], zmc = cconj(x[m]);
+      const float2 a = make_float2(0.5f * (zk.x + zmc.x), 0.5f * (zk.y + zmc.y));
+      const float2 dd = csub(zk, zmc);
+      const float2 b = make_float2(0.5f * dd.y, -0.5f * dd.x);
+      const float fa = factor(k, 0), fb = factor(k, hn);
+      x[k] = make_float2(a.x * fa - b.y * fb, a.y * fa + b.x * fb);
+      if (m != k) {
+        const float ga = factor(m, 0), gb = factor(m, hn);  // A_-k = conj A_k, B_-k = conj B_k
+        x[m] = make_float2(a.x * ga + b.y * gb, -a.y * ga + b.x * gb);
+      }
+    }
   }
   __syncthreads();
-  fft_lines(x, ncol, n, G.logn, tw_inv_n, ls);
+  fft_lines<1>(x, ncol, n, G.logn, tw_inv_n, ls);
   cl.sync();
 
   // Row inverse (c2r): gather each row's bins from the owners.
@@ -563,8 +618,14 @@ k_block_filter(FftGeom G, const float* __restrict__ src, int w, int h, const int
 #pragma unroll
       for (int i = 0; i < kBfBatch * hn / 256; ++i) {
         const int e = tid + 256 * i, rr = e / hn, k = e - rr * hn;
-        xk[i] = *bin(k, b0 + rr);
-        xc[i] = cconj(*bin(hn - k, b0 + rr));
+        if (k == 0) {  // the packed line: DC in the real part, Nyquist in the imaginary part
+          const float2 p = *cl.map_shared_rank(x + b0 + rr, 0);
+          xk[i] = make_float2(p.x, 0.0f);
+          xc[i] = make_float2(p.y, 0.0f);
+        } else {
+          xk[i] = *bin(k, b0 + rr);
+          xc[i] = cconj(*bin(hn - k, b0 + rr));
+        }
       }
 #pragma unroll
       for (int i = 0; i < kBfBatch * hn / 256; ++i) {
@@ -580,7 +641,7 @@ k_block_filter(FftGeom G, const float* __restrict__ src, int w, int h, const int
       }
     }
     __syncthreads();
-    fft_lines(z, kBfBatch, hn, G.logn - 1, tw_inv_hn, zl);
+    fft_lines<1>(z, kBfBatch, hn, G.logn - 1, tw_inv_hn, zl);
 #pragma unroll 4
     for (int i = 0; i < kBfBatch * n / 256; ++i) {
       const int e = tid + 256 * i, rr = e / n, m = e - rr * n;
