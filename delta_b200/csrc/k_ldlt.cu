@@ -9,16 +9,20 @@
 // pseudo-inverse of D (1/d where |d| > the smallest normal double, else 0).
 // The pivot order is Eigen's: at step k the remaining diagonal entry of
 // largest magnitude, read before that step's update (the left-looking variant
-// never updates the trailing diagonal early), first on ties.
+// never updates the trailing diagonal early), first on ties. Because that
+// order depends on the diagonal alone, it is replayed first and the permuted
+// matrix factored without pivoting by a blocked algorithm (the same factors;
+// the sums are taken in another order, so they agree to rounding).
 //
 // It runs after every batched solve, as three launches over chunks of up to
 // kLdltChunk systems (a system whose Cholesky succeeded leaves each of them at
 // once); a failed system gets a 1024-thread CTA for the factorisation and
 // theta, then P / 128 CTAs for the trace, with its matrices in a per-system
 // global workspace (L2-resident):
-//   factor   P left-looking steps: pivot search (block argmax), symmetric
-//            swap of full rows and columns, d_k by a block reduction, column k
-//            of L by one warp per row (contiguous row reads);
+//   factor   the pivot order by one warp over the diagonal, then panels of 32
+//            columns: the diagonal block by one warp, the rows below by one
+//            thread each, the trailing lower triangle minus W L^T in 4 x 4
+//            register blocks (build_pivoted, ldlt_blocked);
 //   theta    forward substitution by one warp (row-oriented), D^+, backward
 //            substitution column-oriented by the block, inverse permutation;
 //   edf      Z = L^-T D^+ L^-1 (Pi M Pi^T) with one thread per column (no
@@ -42,10 +46,15 @@ constexpr int kLdltThreads = 1024;
 constexpr int kLdltChunk = 32;      // systems per round of the three launches
 constexpr int kLdltTraceThreads = 128;
 
+constexpr int kLb = 32;  // panel width of the blocked factorisation
+
 // Per-system workspace: A (P x P, then L and D), Y (P x P), D^+ (P), the trace
-// column terms (P) as doubles; then per system the permutation (P) and a
+// column terms (P), the transposed panels W^T and L^T of the factorisation
+// (2 x kLb x P) as doubles; then per system the permutation (P) and a
 // factored flag as ints.
-__host__ __device__ inline size_t ldlt_sys_doubles(int P) { return 2 * static_cast<size_t>(P) * P + 2 * static_cast<size_t>(P); }
+__host__ __device__ inline size_t ldlt_sys_doubles(int P) {
+  return 2 * static_cast<size_t>(P) * P + 2 * static_cast<size_t>(P) + 2 * static_cast<size_t>(kLb) * P;
+}
 size_t ldlt_work_bytes(int P, int nsys) {
   return sizeof(double) * ldlt_sys_doubles(P) * nsys + sizeof(int) * (static_cast<size_t>(P) + 1) * nsys;
 }
@@ -87,109 +96,165 @@ struct LdltShared {
   int perm[1024];  // position -> original index
 };
 
-// A = M + lambda P0 (P0 = one k x k penalty block per field); perm = identity.
-__device__ void build_penalised(double* A, const double* M, int P, int kk, double lam, const double* pen, int* perm) {
+// Eigen's pivot order, from the diagonal alone: its LDLT is left-looking, so
+// the trailing diagonal is never updated before its own step and step k's
+// pivot (the largest |A_ii| over the positions not yet factored, first on
+// ties) depends only on the diagonal of A = M + lambda P0 and the swaps made
+// so far. One warp replays the P steps on the diagonal; the permuted matrix
+// B = Pi A Pi^T is then factored without pivoting. Returns false when the
+// whole diagonal is zero (Eigen then factors nothing).
+__device__ bool build_pivoted(double* B, const double* M, int P, int kk, double lam, const double* pen,
+                              LdltShared& S) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double* dg = S.temp;
+  for (int i = tid; i < P; i += blockDim.x) {
+    dg[i] = fma(lam, pen[(i % kk) * kk + (i % kk)], M[static_cast<size_t>(i) * P + i]);
+    S.perm[i] = i;
+  }
+  if (tid == 0) S.piv = 0;
+  __syncthreads();
+  if (warp == 0) {
+    for (int k = 0; k < P; ++k) {
+      double best = -1.0;
+      int bi = P;
+      for (int i = k + lane; i < P; i += 32) {
+        const double v = fabs(dg[i]);
+        if (v > best) {
+          best = v;
+          bi = i;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ov > best || (ov == best && oi < bi)) {
+          best = ov;
+          bi = oi;
+        }
+      }
+      if (k == 0 && !(best > 0.0)) {
+        if (lane == 0) S.piv = -1;
+        break;
+      }
+      if (lane == 0 && bi < P && bi != k) {
+        const double t = dg[k];
+        dg[k] = dg[bi];
+        dg[bi] = t;
+        const int q = S.perm[k];
+        S.perm[k] = S.perm[bi];
+        S.perm[bi] = q;
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  if (S.piv < 0) return false;
   const size_t PP = static_cast<size_t>(P) * P;
   for (size_t e = threadIdx.x; e < PP; e += blockDim.x) {
     const int i = static_cast<int>(e / P), j = static_cast<int>(e - static_cast<size_t>(i) * P);
-    double v = M[e];
-    if (i / kk == j / kk) v = fma(lam, pen[(i % kk) * kk + (j % kk)], v);
-    A[e] = v;
+    const int pi = S.perm[i], pj = S.perm[j];
+    double v = M[static_cast<size_t>(pi) * P + pj];
+    if (pi / kk == pj / kk) v = fma(lam, pen[(pi % kk) * kk + (pj % kk)], v);
+    B[e] = v;
   }
-  for (int i = threadIdx.x; i < P; i += blockDim.x) perm[i] = i;
   __syncthreads();
+  return true;
 }
 
-// Eigen's pivoted LDL^T of A in place (L below the diagonal, D on it; S.perm
-// the composed permutation). Returns the number of steps (0 for an all-zero
-// diagonal, where nothing is factored and D counts as zero).
-__device__ int ldlt_factor_block(double* A, int P, LdltShared& S) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
-  for (int k = 0; k < P; ++k) {
-    // Pivot: largest |A_ii| over i >= k, first on ties.
-    double best = -1.0;
-    int bi = P;
-    for (int i = k + tid; i < P; i += blockDim.x) {
-      const double v = fabs(A[static_cast<size_t>(i) * P + i]);
-      if (v > best) {
-        best = v;
-        bi = i;
-      }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      if (ov > best || (ov == best && oi < bi)) {
-        best = ov;
-        bi = oi;
-      }
-    }
-    if (lane == 0) {
-      S.best[warp] = best;
-      S.bidx[warp] = bi;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      double bb = S.best[0];
-      int ii = S.bidx[0];
-      for (int w = 1; w < nwarp; ++w)
-        if (S.best[w] > bb || (S.best[w] == bb && S.bidx[w] < ii)) {
-          bb = S.best[w];
-          ii = S.bidx[w];
+// LDL^T of B without pivoting (the lower triangle; L below the diagonal, D on
+// it), right-looking over panels of kLb columns:
+//   (a) the panel's diagonal block by one warp, left-looking inside it;
+//   (b) the panel's rows below by one thread each, against the block;
+//   (c) the trailing lower triangle minus W L^T (W = L D, both panels kept
+//       transposed so a column read is contiguous), 4 x 4 entries per thread.
+// A zero d_k leaves its column undivided, as Eigen does. Wt, Lt: kLb x P each.
+__device__ void ldlt_blocked(double* B, int P, double* Wt, double* Lt) {
+  __shared__ double blk[kLb][kLb + 1];
+  __shared__ double dblk[kLb];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int p0 = 0; p0 < P; p0 += kLb) {
+    const int nb = min(kLb, P - p0);
+    if (warp == 0) {
+      if (lane < nb)
+        for (int c = 0; c <= lane; ++c) blk[lane][c] = B[static_cast<size_t>(p0 + lane) * P + p0 + c];
+      __syncwarp();
+      for (int k = 0; k < nb; ++k) {
+        if (lane == k) {
+          double d = blk[k][k];
+          for (int j = 0; j < k; ++j) d = fma(-blk[k][j], dblk[j] * blk[k][j], d);
+          dblk[k] = d;
         }
-      S.piv = (k == 0 && !(bb > 0.0)) ? -1 : (ii < P ? ii : k);
+        __syncwarp();
+        const double dk = dblk[k];
+        if (lane > k && lane < nb) {
+          double v = blk[lane][k];
+          for (int j = 0; j < k; ++j) v = fma(-blk[lane][j], dblk[j] * blk[k][j], v);
+          blk[lane][k] = dk != 0.0 ? v / dk : v;
+        }
+        __syncwarp();
+      }
+      if (lane < nb) {
+        double* Br = B + static_cast<size_t>(p0 + lane) * P + p0;
+        for (int c = 0; c < lane; ++c) Br[c] = blk[lane][c];
+        Br[lane] = dblk[lane];
+      }
     }
     __syncthreads();
-    const int piv = S.piv;
-    if (piv < 0) return 0;
-    if (piv != k) {
-      for (int j = tid; j < P; j += blockDim.x) {
-        const double t = A[static_cast<size_t>(k) * P + j];
-        A[static_cast<size_t>(k) * P + j] = A[static_cast<size_t>(piv) * P + j];
-        A[static_cast<size_t>(piv) * P + j] = t;
+    const int r0 = p0 + nb;
+    for (int i = r0 + tid; i < P; i += blockDim.x) {
+      double* Bi = B + static_cast<size_t>(i) * P + p0;
+      for (int k = 0; k < nb; ++k) {
+        double v = Bi[k];
+        for (int j = 0; j < k; ++j) v = fma(-Bi[j], dblk[j] * blk[k][j], v);
+        const double dk = dblk[k];
+        const double l = dk != 0.0 ? v / dk : v;
+        Bi[k] = l;
+        Lt[static_cast<size_t>(k) * P + i] = l;
+        Wt[static_cast<size_t>(k) * P + i] = l * dk;
       }
-      __syncthreads();
-      for (int i = tid; i < P; i += blockDim.x) {
-        const double t = A[static_cast<size_t>(i) * P + k];
-        A[static_cast<size_t>(i) * P + k] = A[static_cast<size_t>(i) * P + piv];
-        A[static_cast<size_t>(i) * P + piv] = t;
-      }
-      if (tid == 0) {
-        const int t = S.perm[k];
-        S.perm[k] = S.perm[piv];
-        S.perm[piv] = t;
-      }
-      __syncthreads();
-    }
-    const double* Ak = A + static_cast<size_t>(k) * P;
-    double part = 0.0;
-    for (int j = tid; j < k; j += blockDim.x) {
-      const double t = A[static_cast<size_t>(j) * P + j] * Ak[j];
-      S.temp[j] = t;
-      part = fma(Ak[j], t, part);
-    }
-    const double red = block_sum(part, S.red);  // synchronises: temp complete
-    if (tid == 0) {
-      const double dk = Ak[k] - red;
-      A[static_cast<size_t>(k) * P + k] = dk;
-      S.dk = dk;
     }
     __syncthreads();
-    const double dk = S.dk;
-    for (int i = k + 1 + warp; i < P; i += nwarp) {
-      const double* Ai = A + static_cast<size_t>(i) * P;
-      double acc = 0.0;
-      for (int j = lane; j < k; j += 32) acc = fma(Ai[j], S.temp[j], acc);
-      acc = warp_sum(acc);
-      if (lane == 0) {
-        const double v = Ai[k] - acc;
-        A[static_cast<size_t>(i) * P + k] = dk != 0.0 ? v / dk : v;
+    const int T = P - r0;
+    if (T > 0) {
+      const int nt = (T + 3) / 4;
+      const int nblocks = nt * (nt + 1) / 2;
+      for (int b = tid; b < nblocks; b += blockDim.x) {
+        int bi = static_cast<int>((sqrt(8.0 * b + 1.0) - 1.0) * 0.5);
+        while ((bi + 1) * (bi + 2) / 2 <= b) ++bi;
+        while (bi * (bi + 1) / 2 > b) --bi;
+        const int bj = b - bi * (bi + 1) / 2;
+        const int i0 = r0 + 4 * bi, j0 = r0 + 4 * bj;
+        double acc[4][4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
+        for (int k = 0; k < nb; ++k) {
+          const double* wr = Wt + static_cast<size_t>(k) * P;
+          const double* lr = Lt + static_cast<size_t>(k) * P;
+          double wv[4], lv[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            wv[u] = i0 + u < P ? wr[i0 + u] : 0.0;
+            lv[u] = j0 + u < P ? lr[j0 + u] : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] = fma(wv[u], lv[v], acc[u][v]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            const int ii = i0 + u, jj = j0 + v;
+            if (ii < P && jj <= ii) B[static_cast<size_t>(ii) * P + jj] -= acc[u][v];
+          }
       }
     }
     __syncthreads();
   }
-  return P;
 }
 
 // Pseudo-inverse of D.
@@ -245,9 +310,10 @@ __global__ void __launch_bounds__(kLdltThreads) k_ldlt_factor(SolveBatch b, int 
   const double lam = b.lam[s];
   const double* M = b.M + static_cast<size_t>(b.m_index ? b.m_index[s] : 0) * PP;
   const double* rhs = b.rhs + static_cast<size_t>(b.r_index ? b.r_index[s] : 0) * P;
-  build_penalised(A, M, P, b.k, lam, b.pen, S.perm);
-  const int n_steps = ldlt_factor_block(A, P, S);
-  ldlt_dinv(A, P, n_steps, dinv);
+  double* Wt = A + 2 * PP + 2 * static_cast<size_t>(P);
+  const bool any = build_pivoted(A, M, P, b.k, lam, b.pen, S);
+  if (any) ldlt_blocked(A, P, Wt, Wt + static_cast<size_t>(kLb) * P);
+  ldlt_dinv(A, P, any ? P : 0, dinv);
 
   // theta: x = Pi rhs; forward L (unit, row-oriented, one warp); D^+;
   // backward L^T (column t of L^T = row t of L, the block over i < t).
@@ -319,9 +385,10 @@ __global__ void __launch_bounds__(kLdltThreads) k_sym_solve_many(int P, int kk, 
                                                                  int m, double* __restrict__ A, double* __restrict__ Y,
                                                                  double* __restrict__ dinv, double* __restrict__ X) {
   __shared__ LdltShared S;
-  build_penalised(A, M, P, kk, lam, pen, S.perm);
-  const int n_steps = ldlt_factor_block(A, P, S);
-  ldlt_dinv(A, P, n_steps, dinv);
+  double* Wt = dinv + P;  // 2 x kLb x P panel workspace
+  const bool any = build_pivoted(A, M, P, kk, lam, pen, S);
+  if (any) ldlt_blocked(A, P, Wt, Wt + static_cast<size_t>(kLb) * P);
+  ldlt_dinv(A, P, any ? P : 0, dinv);
   for (int c = threadIdx.x; c < m; c += blockDim.x) {
     ldlt_solve_col(A, P, S.perm, dinv, [&](int io) { return B[static_cast<size_t>(io) * m + c]; }, Y, m, c, 0);
     for (int i = 0; i < P; ++i) X[static_cast<size_t>(S.perm[i]) * m + c] = Y[static_cast<size_t>(i) * m + c];
@@ -332,7 +399,8 @@ void launch_sym_solve_many(Context& c, int P, int k, const double* M, double lam
                            int m, double* X) {
   if (P > kLdltThreads) fail(DGPU_ERR_INVALID, "solve: at most 1024 unknowns are supported");
   double* work = static_cast<double*>(
-      c.slot(kSlotGrad6, sizeof(double) * (static_cast<size_t>(P) * P + static_cast<size_t>(P) * m + P)));
+      c.slot(kSlotGrad6, sizeof(double) * (static_cast<size_t>(P) * P + static_cast<size_t>(P) * m + P +
+                                           2 * static_cast<size_t>(kLb) * P)));
   k_sym_solve_many<<<1, kLdltThreads, 0, c.stream>>>(P, k, M, lam, pen, B, m, work, work + static_cast<size_t>(P) * P,
                                                      work + static_cast<size_t>(P) * P + static_cast<size_t>(P) * m, X);
   DGPU_LAUNCH("k_sym_solve_many");
