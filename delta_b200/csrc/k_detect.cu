@@ -16,93 +16,25 @@
 #include <string>
 
 #include "dev_common.cuh"
+#include "select_internal.h"
 #include "detect_internal.h"
 
 namespace dgpu {
 
 // ---------------------------------------------------------------------------
-// Sample medians (shared radix-select machinery of k_subtract.cu is per-stride 7;
-// this variant takes any stride and an optional absolute-deviation transform).
+// Sample medians: the radix select of k_select.cu on a flat-index-strided
+// sample, and the absolute-deviation transform for the MAD.
 // ---------------------------------------------------------------------------
-struct Sel {
-  unsigned count, rank, prefix, pad;
-  unsigned hist[256];
-};
-
-__global__ void k_sample_keys(int64_t n, int64_t step, const float* __restrict__ v, const uint8_t* __restrict__ mask,
-                              uint32_t* __restrict__ keys, Sel* st) {
-  const int64_t ns = (n + step - 1) / step;
-  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < ns;
-       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t i = j * step;
-    const float x = v[i];
-    const bool ok = isfinite(x) && (mask == nullptr || mask[i] == 0);
-    const unsigned bal = __ballot_sync(__activemask(), ok);
-    if (!bal) continue;
-    const int lane = threadIdx.x & 31, leader = __ffs(bal) - 1;
-    unsigned base = 0;
-    if (lane == leader) base = atomicAdd(&st->count, __popc(bal));
-    base = __shfl_sync(__activemask(), base, leader);
-    if (ok) keys[base + __popc(bal & ((1u << lane) - 1))] = float_key(x);
-  }
-}
-
 // keys <- key(|value - med|) in place (src/detect.cpp:110).
-__global__ void k_abs_dev(const Sel* st, const float* __restrict__ med, uint32_t* __restrict__ keys) {
+__global__ void k_abs_dev(const RadixSelect* st, const float* __restrict__ med, uint32_t* __restrict__ keys) {
   const unsigned count = st->count;
   const float m = *med;
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
     keys[i] = float_key(fabsf(key_float(keys[i]) - m));
 }
 
-__global__ void k_sel_init(Sel* st) {
-  st->rank = st->count / 2;
-  st->prefix = 0;
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) st->hist[i] = 0;
-}
-
-__global__ void k_sel_hist(const uint32_t* __restrict__ keys, Sel* st, int shift) {
-  __shared__ unsigned hist[256];
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
-  __syncthreads();
-  const unsigned count = st->count, prefix = st->prefix;
-  const unsigned himask = shift >= 24 ? 0u : (0xffffffffu << (shift + 8));
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    const uint32_t k = keys[i];
-    if ((k & himask) == (prefix & himask)) atomicAdd(&hist[(k >> shift) & 0xffu], 1u);
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < 256; i += blockDim.x)
-    if (hist[i]) atomicAdd(&st->hist[i], hist[i]);
-}
-
-__global__ void k_sel_pick(Sel* st, int shift, float* result, int last) {
-  if (threadIdx.x != 0) return;
-  unsigned rank = st->rank, cum = 0;
-  int digit = 255;
-  for (int d = 0; d < 256; ++d) {
-    if (rank < cum + st->hist[d]) {
-      digit = d;
-      break;
-    }
-    cum += st->hist[d];
-  }
-  st->rank = rank - cum;
-  st->prefix |= static_cast<unsigned>(digit) << shift;
-  for (int d = 0; d < 256; ++d) st->hist[d] = 0;
-  if (last) *result = st->count ? key_float(st->prefix) : 0.0f;
-}
-
-static void select_median(cudaStream_t s, Sel* st, const uint32_t* keys, int64_t cap, float* out) {
-  k_sel_init<<<1, 256, 0, s>>>(st);
-  DGPU_LAUNCH("k_sel_init");
-  const int hb = static_cast<int>(std::min<int64_t>((std::max<int64_t>(cap, 1) + 1023) / 1024, 148 * 2));
-  for (int pass = 0; pass < 4; ++pass) {
-    k_sel_hist<<<hb, 256, 0, s>>>(keys, st, 24 - 8 * pass);
-    DGPU_LAUNCH("k_sel_hist");
-    k_sel_pick<<<1, 32, 0, s>>>(st, 24 - 8 * pass, out, pass == 3);
-    DGPU_LAUNCH("k_sel_pick");
-  }
+static void select_median(cudaStream_t s, RadixSelect* st, const uint32_t* keys, int64_t cap, float* out) {
+  launch_select_upper_median(s, st, keys, cap, out);
 }
 
 // bgout[0] = median (float), bgout[1] = MAD (float)
@@ -112,12 +44,11 @@ void launch_background(Context& c, int64_t n, const float* img, const uint8_t* m
   constexpr int64_t kTarget = 1 << 18;
   const int64_t step = n > kTarget ? n / kTarget : 1;
   const int64_t ns = (n + step - 1) / step;
-  Sel* st = static_cast<Sel*>(c.slot(sel_slot, sizeof(Sel)));
+  RadixSelect* st = static_cast<RadixSelect*>(c.slot(sel_slot, sizeof(RadixSelect)));
   uint32_t* keys = static_cast<uint32_t*>(c.slot(key_slot, sizeof(uint32_t) * std::max<int64_t>(ns, 1)));
-  DGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(Sel), s));
+  DGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(RadixSelect), s));
   const int blocks = static_cast<int>(std::min<int64_t>((ns + 255) / 256, 148 * 8));
-  k_sample_keys<<<std::max(blocks, 1), 256, 0, s>>>(n, step, img, mask, keys, st);
-  DGPU_LAUNCH("k_sample_keys");
+  launch_sample_keys(s, n, step, img, mask, keys, st);
   select_median(s, st, keys, ns, bgout);
   k_abs_dev<<<std::max(blocks, 1), 256, 0, s>>>(st, bgout, keys);
   DGPU_LAUNCH("k_abs_dev");
@@ -697,7 +628,7 @@ namespace {
 constexpr int64_t kNoAllocMaxSamples = int64_t(1) << 19;
 
 struct NoAllocBackground {
-  Sel sel;          // count / rank / prefix / histogram: cleared by every call
+  RadixSelect sel;          // count / rank / prefix / histogram: cleared by every call
   float result[4];  // [0] median, [1] MAD
   uint32_t keys[kNoAllocMaxSamples];
 };
@@ -724,13 +655,12 @@ void background_noalloc(int64_t n, const float* img, const uint8_t* mask, cudaSt
   if (ns > kNoAllocMaxSamples)
     fail(DGPU_ERR_INVALID, "estimate_background_noalloc: sample exceeds the fixed 2^19-entry scratch");
   NoAllocBackground* sc = noalloc_background_scratch();
-  Sel* st = &sc->sel;
+  RadixSelect* st = &sc->sel;
   uint32_t* keys = sc->keys;
   float* res = sc->result;
-  DGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(Sel), s));
+  DGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(RadixSelect), s));
   const int blocks = static_cast<int>(std::min<int64_t>((ns + 255) / 256, 148 * 8));
-  k_sample_keys<<<std::max(blocks, 1), 256, 0, s>>>(n, step, img, mask, keys, st);
-  DGPU_LAUNCH("k_sample_keys");
+  launch_sample_keys(s, n, step, img, mask, keys, st);
   select_median(s, st, keys, ns, res);
   k_abs_dev<<<std::max(blocks, 1), 256, 0, s>>>(st, res, keys);
   DGPU_LAUNCH("k_abs_dev");

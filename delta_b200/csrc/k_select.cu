@@ -1,0 +1,90 @@
+// Radix-select sample medians (select_internal.h): one compaction launch, then
+// per 8-bit digit a grid-wide histogram and a one-thread pick of the digit
+// holding the rank. No host synchronisation: the count, the rank and the key
+// prefix stay on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "dev_common.cuh"
+#include "select_internal.h"
+
+namespace dgpu {
+
+__global__ void k_sample_keys(int64_t n, int64_t step, const float* __restrict__ v, const uint8_t* __restrict__ mask,
+                              uint32_t* __restrict__ keys, RadixSelect* st) {
+  const int64_t ns = (n + step - 1) / step;
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < ns;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = j * step;
+    const float x = v[i];
+    const bool ok = isfinite(x) && (mask == nullptr || mask[i] == 0);
+    const unsigned bal = __ballot_sync(__activemask(), ok);
+    if (!bal) continue;
+    const int lane = threadIdx.x & 31, leader = __ffs(bal) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(&st->count, __popc(bal));
+    base = __shfl_sync(__activemask(), base, leader);
+    if (ok) keys[base + __popc(bal & ((1u << lane) - 1))] = float_key(x);
+  }
+}
+
+__global__ void k_select_init(RadixSelect* st) {
+  st->rank = st->count / 2;
+  st->prefix = 0;
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) st->hist[i] = 0;
+}
+
+__global__ void k_select_hist(const uint32_t* __restrict__ keys, RadixSelect* st, int shift) {
+  __shared__ unsigned hist[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+  __syncthreads();
+  const unsigned count = st->count, prefix = st->prefix;
+  const unsigned himask = shift >= 24 ? 0u : (0xffffffffu << (shift + 8));
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const uint32_t k = keys[i];
+    if ((k & himask) == (prefix & himask)) atomicAdd(&hist[(k >> shift) & 0xffu], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 256; i += blockDim.x)
+    if (hist[i]) atomicAdd(&st->hist[i], hist[i]);
+}
+
+__global__ void k_select_pick(RadixSelect* st, int shift, float* result, int last) {
+  if (threadIdx.x != 0) return;
+  unsigned rank = st->rank, cum = 0;
+  int digit = 255;
+  for (int d = 0; d < 256; ++d) {
+    if (rank < cum + st->hist[d]) {
+      digit = d;
+      break;
+    }
+    cum += st->hist[d];
+  }
+  st->rank = rank - cum;
+  st->prefix |= static_cast<unsigned>(digit) << shift;
+  for (int d = 0; d < 256; ++d) st->hist[d] = 0;
+  if (last) *result = st->count ? key_float(st->prefix) : 0.0f;
+}
+
+void launch_sample_keys(cudaStream_t s, int64_t n, int64_t step, const float* v, const uint8_t* mask, uint32_t* keys,
+                        RadixSelect* st) {
+  const int64_t ns = (n + step - 1) / step;
+  const int blocks = static_cast<int>(std::min<int64_t>((std::max<int64_t>(ns, 1) + 255) / 256, 148 * 8));
+  k_sample_keys<<<blocks, 256, 0, s>>>(n, step, v, mask, keys, st);
+  DGPU_LAUNCH("k_sample_keys");
+}
+
+void launch_select_upper_median(cudaStream_t s, RadixSelect* st, const uint32_t* keys, int64_t cap, float* out) {
+  k_select_init<<<1, 256, 0, s>>>(st);
+  DGPU_LAUNCH("k_select_init");
+  const int hb = static_cast<int>(std::min<int64_t>((std::max<int64_t>(cap, 1) + 1023) / 1024, 148 * 2));
+  for (int pass = 0; pass < 4; ++pass) {
+    k_select_hist<<<hb, 256, 0, s>>>(keys, st, 24 - 8 * pass);
+    DGPU_LAUNCH("k_select_hist");
+    k_select_pick<<<1, 32, 0, s>>>(st, 24 - 8 * pass, out, pass == 3);
+    DGPU_LAUNCH("k_select_pick");
+  }
+}
+
+}  // namespace dgpu

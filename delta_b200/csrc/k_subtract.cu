@@ -12,6 +12,7 @@
 #include <cmath>
 
 #include "dev_common.cuh"
+#include "select_internal.h"
 
 namespace dgpu {
 
@@ -374,7 +375,7 @@ size_t model_convolve_smem(int nx, int ks, int TH) {
                           static_cast<size_t>(nx) * (nrows + kMcPad) * kMcTW + static_cast<size_t>(nx) * mc_tap_stride(ks));
 }
 
-size_t model_convolve_fast_smem(int nx, int ks, int TH);
+size_t model_convolve_fast_smem(int nx, int ks, int TH, const DevFields& F);
 bool model_convolve_fast_available(int nx, int ks);
 bool launch_model_convolve_fast(cudaStream_t s, const SubtractArgs& a, const int2* orders, int TH);
 
@@ -410,7 +411,7 @@ static void launch_mc_th(cudaStream_t s, const SubtractArgs& a, const int2* orde
 void launch_model_convolve_orders(cudaStream_t s, const SubtractArgs& a, const int2* orders, bool stack) {
   const int nx = a.n_max + 1;
   const bool fast = !stack && model_convolve_fast_available(nx, a.ks);
-  auto smem_of = [&](int th) { return fast ? model_convolve_fast_smem(nx, a.ks, th) : model_convolve_smem(nx, a.ks, th); };
+  auto smem_of = [&](int th) { return fast ? model_convolve_fast_smem(nx, a.ks, th, a.F) : model_convolve_smem(nx, a.ks, th); };
   const size_t kTwoPerSm = 112 * 1024, kMaxSmem = 200 * 1024;
   int TH = 64;
   while (TH > 8 && smem_of(TH) > kTwoPerSm) TH /= 2;
@@ -736,95 +737,18 @@ void launch_mask_fill(cudaStream_t s, int64_t n, const uint8_t* mask, const uint
 // fill). An empty sample yields 0.
 // ---------------------------------------------------------------------------
 
-struct SelectState {
-  unsigned int count;   // sample size
-  unsigned int rank;    // remaining rank within the current prefix bucket
-  unsigned int prefix;  // key bits fixed so far
-  unsigned int hist[256];
-};
-
-__global__ void k_compact_samples(int kind, int64_t n, const float* __restrict__ v,
-                                  const uint8_t* __restrict__ mask, uint32_t* __restrict__ keys,
-                                  SelectState* st) {
-  const int64_t nsamp = (n + 6) / 7;
-  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < nsamp;
-       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t i = 7 * j;
-    const float x = v[i];
-    const bool ok = isfinite(x) && (mask == nullptr || mask[i] == 0);
-    // kind 0 (reference): good finite reference pixels; kind 1 (difference):
-    // unmasked finite difference pixels (mask is the grown output mask).
-    (void)kind;
-    const unsigned bal = __ballot_sync(__activemask(), ok);
-    if (bal == 0) continue;
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(bal) - 1;
-    unsigned base = 0;
-    if (lane == leader) base = atomicAdd(&st->count, __popc(bal));
-    base = __shfl_sync(__activemask(), base, leader);
-    if (ok) keys[base + __popc(bal & ((1u << lane) - 1))] = float_key(x);
-  }
-}
-
-__global__ void k_select_init(SelectState* st) {
-  st->rank = st->count / 2;
-  st->prefix = 0;
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) st->hist[i] = 0;
-}
-
-__global__ void k_select_hist(const uint32_t* __restrict__ keys, SelectState* st, int shift) {
-  __shared__ unsigned hist[256];
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
-  __syncthreads();
-  const unsigned count = st->count;
-  const unsigned prefix = st->prefix;
-  const unsigned himask = shift >= 24 ? 0u : (0xffffffffu << (shift + 8));
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    const uint32_t k = keys[i];
-    if ((k & himask) == (prefix & himask)) atomicAdd(&hist[(k >> shift) & 0xffu], 1u);
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < 256; i += blockDim.x)
-    if (hist[i]) atomicAdd(&st->hist[i], hist[i]);
-}
-
-__global__ void k_select_pick(SelectState* st, int shift, float* result, int last) {
-  if (threadIdx.x != 0) return;
-  unsigned rank = st->rank, cum = 0;
-  int digit = 255;
-  for (int d = 0; d < 256; ++d) {
-    if (rank < cum + st->hist[d]) {
-      digit = d;
-      break;
-    }
-    cum += st->hist[d];
-  }
-  st->rank = rank - cum;
-  st->prefix |= static_cast<unsigned>(digit) << shift;
-  for (int d = 0; d < 256; ++d) st->hist[d] = 0;
-  if (last) *result = st->count ? key_float(st->prefix) : 0.0f;
-}
-
 void launch_strided_median(Context& c, int kind, int64_t n, const float* values, const uint8_t* mask,
                            float* d_result) {
+  // kind 0 (reference): good finite reference pixels; kind 1 (difference):
+  // unmasked finite difference pixels (mask is the grown output mask).
+  (void)kind;
   cudaStream_t s = c.stream;
   const int64_t nsamp = (n + 6) / 7;
-  auto* st = static_cast<SelectState*>(c.slot(kSlotSelect, sizeof(SelectState)));
+  auto* st = static_cast<RadixSelect*>(c.slot(kSlotSelect, sizeof(RadixSelect)));
   auto* keys = static_cast<uint32_t*>(c.slot(kSlotSamples, sizeof(uint32_t) * std::max<int64_t>(nsamp, 1)));
-  DGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(SelectState), s));
-  const int blocks = static_cast<int>(std::min<int64_t>(ceil_div(std::max<int64_t>(nsamp, 1), 256), 148 * 8));
-  k_compact_samples<<<blocks, 256, 0, s>>>(kind, n, values, mask, keys, st);
-  DGPU_LAUNCH("k_compact_samples");
-  k_select_init<<<1, 256, 0, s>>>(st);
-  DGPU_LAUNCH("k_select_init");
-  const int hb = static_cast<int>(std::min<int64_t>(ceil_div(std::max<int64_t>(nsamp, 1), 1024), 148 * 2));
-  for (int pass = 0; pass < 4; ++pass) {
-    const int shift = 24 - 8 * pass;
-    k_select_hist<<<hb, 256, 0, s>>>(keys, st, shift);
-    DGPU_LAUNCH("k_select_hist");
-    k_select_pick<<<1, 32, 0, s>>>(st, shift, d_result, pass == 3);
-    DGPU_LAUNCH("k_select_pick");
-  }
+  DGPU_CUDA(cudaMemsetAsync(st, 0, sizeof(RadixSelect), s));
+  launch_sample_keys(s, n, 7, values, mask, keys, st);
+  launch_select_upper_median(s, st, keys, nsamp, d_result);
 }
 
 // photometric_scale (src/fit.cpp:513-530): out = sum_c float(S_c) * a_c in
