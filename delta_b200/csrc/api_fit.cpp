@@ -189,6 +189,7 @@ struct Engine {
     b.ok = w.ok;
     b.status = c.d_status;
     b.partial = w.partial;
+    StageTimer t(c, "fit: lambda-grid solve");
     launch_solve_batch(c, b);
   }
 
@@ -204,6 +205,7 @@ struct Engine {
 
   // M, rhs, ywy, n over the rows whose unit mask is set.
   void assemble(const uint8_t* mask, double* M, double* rhs, double* ywy, long long* n) {
+    StageTimer t(c, "fit: normal equations");
     launch_rhs(c, N, nc, k, SS, R, mask, nullptr, rhs, ywy, n);
     launch_normal_equations(c, prec, N, nc, k, SS, R, mask, M);
   }

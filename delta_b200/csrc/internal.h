@@ -282,6 +282,7 @@ struct DevFields {
   const float* latf = nullptr;   // coarse: nf*ncy*ncx, float32 copies of the FP64 lattice
   const double* lat = nullptr;   // coarse FP64 lattice
   int ncx = 0, ncy = 0;
+  int stride = 0;                // coarse: lattice spacing in pixels (cells of `stride`, the last extended)
   const int* cellx = nullptr;    // w
   const float* wx = nullptr;     // w
   const int* celly = nullptr;    // h

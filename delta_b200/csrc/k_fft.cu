@@ -657,64 +657,91 @@ k_block_filter(FftGeom G, const float* __restrict__ src, int w, int h, const int
 // Hann-weighted outputs of the (at most 3 x 3) blocks covering it in colour
 // order q = (ix % 3) * 3 + (iy % 3) -- the order of the reference's 9-colour
 // passes -- with the same float rounding after each block, then divides by the
-// separable weight sum. One thread per pixel; bout holds each block's raw
-// c2r output (item x n x n).
-__global__ void __launch_bounds__(256)
+// separable weight sum. bout holds each block's raw c2r output (item x n x n).
+// One CTA per tile of kOlaTW columns x kOlaTH rows, one thread per column: a
+// thread finds its column's covering blocks (in colour order) and their Hann
+// weights once, the CTA finds each row's once (shared memory), and every pixel
+// then reads only its block outputs.
+constexpr int kOlaTW = 128;
+constexpr int kOlaTH = 16;
+
+// Covering origins of coordinate c, in colour order (index % 3 = 0, 1, 2):
+// idx[k] (or -1) and the offset inside the block. Origins are ascending and
+// the covering ones form a run of at most 3.
+__device__ __forceinline__ void ola_cover(int c, const int* __restrict__ o, int no, int n, int (&idx)[3],
+                                          int (&off)[3]) {
+  const int s = max(n / 2, 1);
+  int hi = min(c / s, no - 1);
+  while (hi + 1 < no && o[hi + 1] <= c) ++hi;
+  while (hi > 0 && o[hi] > c) --hi;
+  int lo = hi;
+  while (lo > 0 && lo > hi - 2 && o[lo - 1] + n > c) --lo;
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const int ix = hi - (((hi - r) % 3) + 3) % 3;
+    idx[r] = ix >= lo ? ix : -1;
+    off[r] = ix >= lo ? c - o[ix] : 0;
+  }
+}
+
+__global__ void __launch_bounds__(kOlaTW)
 k_ola_gather(int w, int h, int n, const int* __restrict__ oxs, int nox, const int* __restrict__ oys, int noy,
              const double* __restrict__ hwin, const float* __restrict__ bout, const double* __restrict__ bnum,
              const double* __restrict__ wx_total, const double* __restrict__ wy_total, float* __restrict__ acc,
              float* __restrict__ var_acc) {
-  // Frame rows stride over blockIdx.y: a row's covering block rows, their
-  // Hann weights and the row weight total are the same for the whole CTA.
-  const int s = n / 2;
+  __shared__ int r_iy[kOlaTH][3], r_ly[kOlaTH][3];
+  __shared__ double r_wyt[kOlaTH];
+  const int x = blockIdx.x * kOlaTW + threadIdx.x;
+  const int y0 = blockIdx.y * kOlaTH;
+  if (threadIdx.x < kOlaTH && y0 + static_cast<int>(threadIdx.x) < h) {
+    const int y = y0 + threadIdx.x;
+    int iy[3], ly[3];
+    ola_cover(y, oys, noy, n, iy, ly);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      r_iy[threadIdx.x][r] = iy[r];
+      r_ly[threadIdx.x][r] = ly[r];
+    }
+    r_wyt[threadIdx.x] = wy_total[y];
+  }
+  __syncthreads();
+  if (x >= w) return;
+  int ix[3], lx[3];
+  ola_cover(x, oxs, nox, n, ix, lx);
+  double wxv[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) wxv[r] = ix[r] >= 0 ? hwin[lx[r]] : 0.0;
+  const double wxt = wx_total[x];
   const double inv_n2 = static_cast<double>(1.0f / static_cast<float>(static_cast<size_t>(n) * n));
-  for (int y = blockIdx.y; y < h; y += gridDim.y) {
-    // Largest origin index <= y (regular origins at multiples of s, then the flush origin).
-    int iyh = min(y / max(s, 1), noy - 1);
-    while (iyh + 1 < noy && oys[iyh + 1] <= y) ++iyh;
-    while (iyh > 0 && oys[iyh] > y) --iyh;
-    int iyl = iyh;
-    while (iyl > 0 && iyl > iyh - 2 && oys[iyl - 1] + n > y) --iyl;
-    const double wyt = wy_total[y];
-    float* arow = acc + static_cast<size_t>(y) * w;
-    float* vrow = var_acc + static_cast<size_t>(y) * w;
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < w; x += gridDim.x * blockDim.x) {
-      int ixh = min(x / max(s, 1), nox - 1);
-      while (ixh + 1 < nox && oxs[ixh + 1] <= x) ++ixh;
-      while (ixh > 0 && oxs[ixh] > x) --ixh;
-      // Covering origins form the index ranges [ixl, ixh] x [iyl, iyh] (at most 3
-      // each, so at most one index per residue mod 3).
-      int ixl = ixh;
-      while (ixl > 0 && ixl > ixh - 2 && oxs[ixl - 1] + n > x) --ixl;
-      float a = 0.0f, v = 0.0f;
+  const int rows = min(kOlaTH, h - y0);
+  for (int t = 0; t < rows; ++t) {
+    const int y = y0 + t;
+    float a = 0.0f, v = 0.0f;
 #pragma unroll
-      for (int ca = 0; ca < 3; ++ca) {  // colour q = (ix % 3) * 3 + (iy % 3), ascending
-        const int ix = ixh - (((ixh - ca) % 3) + 3) % 3;
-        if (ix < ixl) continue;
-        const int lx = x - oxs[ix];
-        const double wxv = hwin[lx];
+    for (int ca = 0; ca < 3; ++ca) {  // colour q = (ix % 3) * 3 + (iy % 3), ascending
+      if (ix[ca] < 0) continue;
 #pragma unroll
-        for (int cb = 0; cb < 3; ++cb) {
-          const int iy = iyh - (((iyh - cb) % 3) + 3) % 3;
-          if (iy < iyl) continue;
-          const int item = iy * nox + ix;
-          const int ly = y - oys[iy];
-          const float f = bout[(static_cast<size_t>(item) * n + ly) * n + lx];
-          const double num = bnum[item];
-          const double wy_sig = hwin[ly] * inv_n2;
-          const double wy_var = hwin[ly];
-          a = static_cast<float>(static_cast<double>(a) + wy_sig * wxv * static_cast<double>(f));
-          v = static_cast<float>(static_cast<double>(v) + wy_var * wxv * num);
-        }
+      for (int cb = 0; cb < 3; ++cb) {
+        const int iy = r_iy[t][cb];
+        if (iy < 0) continue;
+        const int item = iy * nox + ix[ca];
+        const int ly = r_ly[t][cb];
+        const float f = bout[(static_cast<size_t>(item) * n + ly) * n + lx[ca]];
+        const double num = bnum[item];
+        const double wy_sig = hwin[ly] * inv_n2;
+        const double wy_var = hwin[ly];
+        a = static_cast<float>(static_cast<double>(a) + wy_sig * wxv[ca] * static_cast<double>(f));
+        v = static_cast<float>(static_cast<double>(v) + wy_var * wxv[ca] * num);
       }
-      const double ws = wyt * wx_total[x];
-      if (ws > 0.0) {
-        arow[x] = static_cast<float>(static_cast<double>(a) / ws);
-        vrow[x] = static_cast<float>(static_cast<double>(v) / ws);
-      } else {
-        arow[x] = 0.0f;
-        vrow[x] = 0.0f;
-      }
+    }
+    const double ws = r_wyt[t] * wxt;
+    const size_t o = static_cast<size_t>(y) * w + x;
+    if (ws > 0.0) {
+      acc[o] = static_cast<float>(static_cast<double>(a) / ws);
+      var_acc[o] = static_cast<float>(static_cast<double>(v) / ws);
+    } else {
+      acc[o] = 0.0f;
+      var_acc[o] = 0.0f;
     }
   }
 }
@@ -983,9 +1010,9 @@ void launch_ola_gather(cudaStream_t s, int w, int h, int n, const int* oxs, int 
                        const double* hwin, const float* bout, const double* bnum, const double* wx_total,
                        const double* wy_total, float* acc, float* var_acc) {
   if (w <= 0 || h <= 0) return;
-  const dim3 grid(static_cast<unsigned>(std::min(ceil_div(w, 256), 16)), static_cast<unsigned>(std::min(h, 65535)));
-  k_ola_gather<<<grid, 256, 0, s>>>(w, h, n, oxs, nox, oys, noy, hwin, bout, bnum, wx_total, wy_total, acc,
-                                    var_acc);
+  const dim3 grid(static_cast<unsigned>(ceil_div(w, kOlaTW)), static_cast<unsigned>(ceil_div(h, kOlaTH)));
+  k_ola_gather<<<grid, kOlaTW, 0, s>>>(w, h, n, oxs, nox, oys, noy, hwin, bout, bnum, wx_total, wy_total, acc,
+                                       var_acc);
   DGPU_LAUNCH("k_ola_gather");
 }
 

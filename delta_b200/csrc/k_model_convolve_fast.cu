@@ -14,6 +14,9 @@
 //     reference's sum over j = 0..ks-1 bit for bit.
 //   * The x pass keeps its 4-wide sliding window in registers across the
 //     unrolled taps (no moves), one 16-byte tap load per component per 4 taps.
+//   * The lattice corners of the cells the tile touches (every field) are
+//     staged in shared memory once, so the blend of each component reads no
+//     global memory.
 //   * The field blend works on the two columns of a thread as one packed pair:
 //     per coarse cell row the corner differences e = a10 - a00, t = a01 - a00,
 //     g = (a11 - a10) - t, then per row base = fma(e, fy, a00),
@@ -48,7 +51,7 @@ __global__ void __launch_bounds__(256)
 k_model_convolve_f(int w, int h, const float* __restrict__ sci, const float* __restrict__ ref,
                    const uint8_t* __restrict__ rmask, DevFields F, const float* __restrict__ taps,
                    const int2* __restrict__ orders, int ks, int nc, const float* __restrict__ fillp,
-                   float* __restrict__ diff, int TH) {
+                   float* __restrict__ diff, int TH, int lat_cap) {
   constexpr int KSP = 8 * KB;
   extern __shared__ __align__(16) float smem[];
   const int kh = (ks - 1) / 2;
@@ -59,9 +62,26 @@ k_model_convolve_f(int w, int h, const float* __restrict__ sci, const float* __r
   float* rtile = smem;                          // nrows x rw; column kFLPad + c <-> frame column bx - kh + c
   float* txs = rtile + nrows * rw;              // NX x (kFPad zero rows + nrows) x kFTW
   float* ktaps = txs + NX * trows * kFTW;       // NX x KSP, zero padded
+  float* slat = ktaps + NX * KSP;               // nf x lly x llx lattice corners (lat_cap floats)
   const int bx = blockIdx.x * kFTW, by = blockIdx.y * TH;
   const float fill = *fillp;
   const int tid = threadIdx.x;
+
+  // Corners of the lattice cells this tile touches (same cells for the whole CTA).
+  int lcx0 = 0, lcy0 = 0, llx = 0, lly = 0;
+  bool staged = false;
+  if (!F.exact) {
+    lcx0 = F.cellx[bx];
+    lcy0 = F.celly[by];
+    llx = F.cellx[min(bx + kFTW - 1, w - 1)] + 2 - lcx0;
+    lly = F.celly[min(by + TH - 1, h - 1)] + 2 - lcy0;
+    staged = F.nf * llx * lly <= lat_cap;
+    if (staged)
+      for (int i = tid; i < F.nf * lly * llx; i += blockDim.x) {
+        const int f = i / (lly * llx), r = (i / llx) % lly, c = i % llx;
+        slat[i] = __ldg(F.latf + (static_cast<size_t>(f) * F.ncy + lcy0 + r) * F.ncx + lcx0 + c);
+      }
+  }
 
   for (int i = tid; i < NX * KSP; i += blockDim.x) {
     const int q = i / KSP, j = i - q * KSP;
@@ -176,12 +196,22 @@ k_model_convolve_f(int w, int h, const float* __restrict__ sci, const float* __r
     for (int i = 0; i < kFYR; ++i) {
       if (jy[i] != cj) {
         cj = jy[i];
-        const float* r0 = F.latf + (static_cast<size_t>(f) * F.ncy + cj) * F.ncx;
-        const float* r1 = r0 + F.ncx;
-        a00 = make_float2(__ldg(r0 + jx[0]), __ldg(r0 + jx[1]));
-        const float2 a01 = make_float2(__ldg(r0 + jx[0] + 1), __ldg(r0 + jx[1] + 1));
-        const float2 a10 = make_float2(__ldg(r1 + jx[0]), __ldg(r1 + jx[1]));
-        const float2 a11 = make_float2(__ldg(r1 + jx[0] + 1), __ldg(r1 + jx[1] + 1));
+        float2 a01, a10, a11;
+        if (staged) {
+          const float* r0 = slat + (f * lly + (cj - lcy0)) * llx - lcx0;
+          const float* r1 = r0 + llx;
+          a00 = make_float2(r0[jx[0]], r0[jx[1]]);
+          a01 = make_float2(r0[jx[0] + 1], r0[jx[1] + 1]);
+          a10 = make_float2(r1[jx[0]], r1[jx[1]]);
+          a11 = make_float2(r1[jx[0] + 1], r1[jx[1] + 1]);
+        } else {
+          const float* r0 = F.latf + (static_cast<size_t>(f) * F.ncy + cj) * F.ncx;
+          const float* r1 = r0 + F.ncx;
+          a00 = make_float2(__ldg(r0 + jx[0]), __ldg(r0 + jx[1]));
+          a01 = make_float2(__ldg(r0 + jx[0] + 1), __ldg(r0 + jx[1] + 1));
+          a10 = make_float2(__ldg(r1 + jx[0]), __ldg(r1 + jx[1]));
+          a11 = make_float2(__ldg(r1 + jx[0] + 1), __ldg(r1 + jx[1] + 1));
+        }
         e = fsub2(a10, a00);
         t = fsub2(a01, a00);
         g = fsub2(fsub2(a11, a10), t);
@@ -245,6 +275,13 @@ k_model_convolve_f(int w, int h, const float* __restrict__ sci, const float* __r
   }
 }
 
+// Floats of shared memory for the lattice corners a tile of TH rows touches.
+int lattice_cap(const DevFields& F, int TH) {
+  if (F.exact || F.stride <= 0) return 0;
+  const int lx = std::min(F.ncx, (kFTW - 1) / F.stride + 3), ly = std::min(F.ncy, (TH - 1) / F.stride + 3);
+  return F.nf * lx * ly;
+}
+
 template <int NX, int KB>
 void launch_f(cudaStream_t s, const SubtractArgs& a, const int2* orders, int TH, size_t smem) {
   auto kern = k_model_convolve_f<NX, KB>;
@@ -252,7 +289,7 @@ void launch_f(cudaStream_t s, const SubtractArgs& a, const int2* orders, int TH,
   dim3 grid(ceil_div(a.w, kFTW), ceil_div(a.h, TH));
   const int threads = (kFTW / 2) * (TH / kFYR);
   kern<<<grid, threads, smem, s>>>(a.w, a.h, a.sci, a.ref, a.ref_mask, a.F, a.taps, orders, a.ks, a.nc, a.fill,
-                                   a.diff, TH);
+                                   a.diff, TH, lattice_cap(a.F, TH));
   DGPU_LAUNCH("k_model_convolve_f");
 }
 
@@ -269,12 +306,12 @@ bool launch_nx(cudaStream_t s, const SubtractArgs& a, const int2* orders, int TH
 
 }  // namespace
 
-size_t model_convolve_fast_smem(int nx, int ks, int TH) {
+size_t model_convolve_fast_smem(int nx, int ks, int TH, const DevFields& F) {
   const int kh = (ks - 1) / 2;
   const int nrows = TH + 2 * kh;
   const int kb = (ks + 7) / 8;
   return sizeof(float) * (static_cast<size_t>(nrows) * fast_rw(ks) + static_cast<size_t>(nx) * (nrows + kFPad) * kFTW +
-                          static_cast<size_t>(nx) * 8 * kb);
+                          static_cast<size_t>(nx) * 8 * kb + static_cast<size_t>(lattice_cap(F, TH)));
 }
 
 bool model_convolve_fast_available(int nx, int ks) {
@@ -285,7 +322,7 @@ bool model_convolve_fast_available(int nx, int ks) {
 bool launch_model_convolve_fast(cudaStream_t s, const SubtractArgs& a, const int2* orders, int TH) {
   const int nx = a.n_max + 1;
   if (!model_convolve_fast_available(nx, a.ks)) return false;
-  const size_t smem = model_convolve_fast_smem(nx, a.ks, TH);
+  const size_t smem = model_convolve_fast_smem(nx, a.ks, TH, a.F);
   const int kb = (a.ks + 7) / 8;
   switch (nx) {
     case 3: return launch_nx<3>(s, a, orders, TH, smem, kb);

@@ -267,6 +267,7 @@ DevFields build_fields_dev(Context& c, const ThinPlate& tp, const double* d_thet
   F.exact = 0;
   F.ncx = g.ncx;
   F.ncy = g.ncy;
+  F.stride = g.stride;
   std::vector<int> ib;
   ib.insert(ib.end(), g.gx.begin(), g.gx.end());
   ib.insert(ib.end(), g.gy.begin(), g.gy.end());
