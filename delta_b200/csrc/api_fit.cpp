@@ -189,6 +189,7 @@ struct Engine {
     b.ok = w.ok;
     b.status = c.d_status;
     b.partial = w.partial;
+    b.skip_ldlt = quick_fallback() ? 1 : 0;
     StageTimer t(c, "fit: lambda-grid solve");
     launch_solve_batch(c, b);
   }
@@ -275,12 +276,19 @@ struct Engine {
       launch_quad_err(c, nl, P, w.theta, M, nullptr, a.r0, nullptr, a.s0, w.raw, a.theta0);
       launch_gcv_finish(c.stream, nl, w.raw, w.edf, w.ok, n, w.rss, w.gcv);
       std::vector<double> approx(nl);
+      std::vector<int> okv(nl);
       o.curve.resize(nl);
       {
-        Fetch f(c, sizeof(double) * 2 * nl);
+        Fetch f(c, sizeof(double) * 2 * nl + sizeof(int) * nl);
         f.add(approx.data(), a.approx, nl);
         f.add(o.curve.data(), w.gcv, nl);
+        f.add(okv.data(), w.ok, nl);
         f.run();
+      }
+      if (quick_fallback() && std::find(okv.begin(), okv.end(), 0) != okv.end()) {
+        o.prec_used = prec;  // a Cholesky failed in the reduced-precision system: redo in FP64
+        o.ldlt = 1;
+        return o;
       }
       anchored = argmin(approx);
       best = argmin(o.curve);
@@ -298,6 +306,11 @@ struct Engine {
     finish_single(w, best, grid[best], M, n, mask, o, anchored == best);
     return o;
   }
+
+  // A reduced-precision attempt that the FP64 fallback would redo: a system
+  // whose Cholesky fails is not LDLT-solved (the whole attempt is redone in
+  // FP64 instead, see mixed_failed).
+  bool quick_fallback() const { return tensor_prec(prec) && c.precision_fallback; }
 
   // Mixed precision falls back to FP64 normal equations, for the rest of this
   // fit, when its solve is non-finite or its FP64 refinement correction is
@@ -369,7 +382,7 @@ struct Engine {
     o.d_theta = th;
     o.lambda = lam;
     o.prec_used = prec;
-    o.ldlt = ok_s == 2 ? 1 : 0;
+    o.ldlt = ok_s == 1 ? 0 : 1;  // 2: LDLT fallback; 0: failed Cholesky left for the FP64 redo
     if (!delta.empty()) {
       double dd = 0.0, tt = 0.0;
       for (int p = 0; p < P; ++p) {
@@ -475,6 +488,7 @@ struct Engine {
     double* th0 = nullptr;
     double* r0 = nullptr;
     double* s0 = nullptr;
+    bool chol_failed = false;  // a reduced-precision fold system failed its Cholesky (quick_fallback)
     auto solve_at = [&](const std::vector<int>& idx) {
       const int m = static_cast<int>(idx.size());
       const int ns = m * G;
@@ -499,6 +513,8 @@ struct Engine {
         launch_quad_err(c, ns, P, w.theta, Mg, w.midx, rg, w.midx, yg, w.raw);
       const auto err = down(c, w.raw, ns);
       const auto ok = down(c, w.ok, ns);
+      if (quick_fallback())
+        for (int v : ok) chol_failed = chol_failed || v == 0;
       for (int ii = 0; ii < m; ++ii) {
         double tot = 0.0;
         for (int g = 0; g < G; ++g) {
@@ -597,6 +613,7 @@ struct Engine {
     launch_gcv_finish(c.stream, 1, w1.raw, w1.edf, w1.ok, nall, w1.rss, w1.gcv);
     GlsOut o;
     finish_single(w1, 0, grid[best], Mall, nall, mask, o);
+    if (chol_failed) o.ldlt = 1;  // redone in FP64 (mixed_failed)
     o.grid = grid;
     o.curve = curve;
     return o;

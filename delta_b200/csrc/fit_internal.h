@@ -75,6 +75,9 @@ struct SolveBatch {
   int* ok = nullptr;                // nsys: 1 Cholesky, 2 LDLT fallback, 0 failed
   unsigned* status = nullptr;
   double* partial = nullptr;        // nsys x 8 per-rank trace partials
+  // 1: leave systems whose Cholesky failed at ok = 0 (no LDLT fallback): a
+  // reduced-precision attempt that will be redone in FP64 anyway.
+  int skip_ldlt = 0;
 };
 int solve_pp(int P);                               // padded size
 int solve_ep(int nf, int r);                       // appended rows, padded

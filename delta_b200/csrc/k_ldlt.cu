@@ -343,9 +343,19 @@ __global__ void __launch_bounds__(kLdltThreads) k_ldlt_factor(SolveBatch b, int 
   if (tid == 0) *factored = 1;
 }
 
-// edf term of column c: Z_cc, Z = L^-T D^+ L^-1 B, B = Pi M Pi^T (thread c
-// solves column c). Grid: (chunk systems, ceil(P / 128)).
+// edf terms Z_cc, Z = L^-T D^+ L^-1 B, B = Pi M Pi^T: thread c solves column
+// c, the CTA's kLdltTraceThreads columns together, by panels of kLb rows. Per
+// panel the threads solve its triangular block with their panel values in
+// registers, then update the rows still to come with the panel's L read once
+// into shared memory (chunks of kTrRows rows) -- every L value is a broadcast
+// shared load, every y value one coalesced load and store. The backward
+// pass stops at the panel of the CTA's first column (x_c needs x_t, t > c
+// only). Grid: (chunk systems, ceil(P / kLdltTraceThreads)).
+constexpr int kTrRows = 64;
+
 __global__ void __launch_bounds__(kLdltTraceThreads) k_ldlt_trace(SolveBatch b, int s0, LdltWork wk) {
+  __shared__ double lp[kLb][kLb + 1];     // the panel's diagonal block
+  __shared__ double ls[kTrRows][kLb + 1];  // a chunk of the panel's other rows (forward) / columns (backward)
   const int P = b.P;
   const size_t PP = static_cast<size_t>(P) * P;
   const int s = s0 + static_cast<int>(blockIdx.x);
@@ -354,13 +364,108 @@ __global__ void __launch_bounds__(kLdltTraceThreads) k_ldlt_trace(SolveBatch b, 
   const double* dinv = A + 2 * PP;
   double* zc = A + 2 * PP + P;
   const int* perm = wk.i + blockIdx.x * (static_cast<size_t>(P) + 1);
-  if (!perm[P]) return;
-  const int c = static_cast<int>(blockIdx.y) * kLdltTraceThreads + static_cast<int>(threadIdx.x);
-  if (c >= P) return;
+  if (!perm[P]) return;  // the same for the whole CTA
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int c0 = static_cast<int>(blockIdx.y) * kLdltTraceThreads;
+  const int c = c0 + tid;
+  const bool act = c < P;
   const double* M = b.M + static_cast<size_t>(b.m_index ? b.m_index[s] : 0) * PP;
-  const int oc = perm[c];
-  ldlt_solve_col(A, P, perm, dinv, [&](int io) { return M[static_cast<size_t>(io) * P + oc]; }, Y, P, c, c);
-  zc[c] = Y[static_cast<size_t>(c) * P + c];
+  if (act) {
+    const int oc = perm[c];
+    for (int i = 0; i < P; ++i) Y[static_cast<size_t>(i) * P + c] = M[static_cast<size_t>(perm[i]) * P + oc];
+  }
+  double yp[kLb];
+  // Forward: y = L^-1 b (L unit lower).
+  for (int p0 = 0; p0 < P; p0 += kLb) {
+    const int nb = min(kLb, P - p0);
+    __syncthreads();
+    for (int e = tid; e < nb * nb; e += nt) {
+      const int r = e / nb, q = e - r * nb;
+      lp[r][q] = q < r ? A[static_cast<size_t>(p0 + r) * P + p0 + q] : 0.0;
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int k = 0; k < kLb; ++k) {
+        if (k < nb) {
+          double v = Y[static_cast<size_t>(p0 + k) * P + c];
+#pragma unroll
+          for (int j = 0; j < k; ++j) v = fma(-lp[k][j], yp[j], v);
+          yp[k] = v;
+          Y[static_cast<size_t>(p0 + k) * P + c] = v;
+        }
+      }
+    }
+    for (int r0 = p0 + nb; r0 < P; r0 += kTrRows) {
+      const int nr = min(kTrRows, P - r0);
+      __syncthreads();
+      for (int e = tid; e < nr * nb; e += nt) {
+        const int r = e / nb, q = e - r * nb;
+        ls[r][q] = A[static_cast<size_t>(r0 + r) * P + p0 + q];
+      }
+      __syncthreads();
+      if (act) {
+        for (int r = 0; r < nr; ++r) {
+          double* yr = Y + static_cast<size_t>(r0 + r) * P + c;
+          double v = *yr;
+#pragma unroll
+          for (int k = 0; k < kLb; ++k)
+            if (k < nb) v = fma(-ls[r][k], yp[k], v);
+          *yr = v;
+        }
+      }
+    }
+  }
+  // D^+.
+  if (act)
+    for (int i = 0; i < P; ++i) Y[static_cast<size_t>(i) * P + c] *= dinv[i];
+  // Backward: x = L^-T y, panels from the last down to the one holding c0.
+  const int last = ((P - 1) / kLb) * kLb;
+  for (int p0 = last; p0 + kLb > c0; p0 -= kLb) {
+    const int nb = min(kLb, P - p0);
+    __syncthreads();
+    for (int e = tid; e < nb * nb; e += nt) {
+      const int r = e / nb, q = e - r * nb;
+      lp[r][q] = q < r ? A[static_cast<size_t>(p0 + r) * P + p0 + q] : 0.0;
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int kk = kLb - 1; kk >= 0; --kk) {
+        if (kk < nb) {
+          double v = Y[static_cast<size_t>(p0 + kk) * P + c];
+#pragma unroll
+          for (int t = kk + 1; t < kLb; ++t)
+            if (t < nb) v = fma(-lp[t][kk], yp[t], v);
+          yp[kk] = v;
+          Y[static_cast<size_t>(p0 + kk) * P + c] = v;
+        }
+      }
+    }
+    // rows r in [c0, p0) above the panel: y_r -= sum_t L[p0 + t][r] x_t
+    const int rlo = min(c0, p0);
+    for (int r0 = rlo; r0 < p0; r0 += kTrRows) {
+      const int nr = min(kTrRows, p0 - r0);
+      __syncthreads();
+      for (int e = tid; e < nr * nb; e += nt) {
+        const int q = e / nr, r = e - q * nr;  // consecutive threads read consecutive columns of row p0 + q
+        ls[r][q] = A[static_cast<size_t>(p0 + q) * P + r0 + r];
+      }
+      __syncthreads();
+      if (act) {
+        for (int r = 0; r < nr; ++r) {
+          double* yr = Y + static_cast<size_t>(r0 + r) * P + c;
+          double v = *yr;
+#pragma unroll
+          for (int t = 0; t < kLb; ++t)
+            if (t < nb) v = fma(-ls[r][t], yp[t], v);
+          *yr = v;
+        }
+      }
+    }
+    if (p0 == 0) break;
+  }
+  if (act) zc[c] = Y[static_cast<size_t>(c) * P + c];
 }
 
 // edf = sum_c Z_cc in column order; ok = 2.

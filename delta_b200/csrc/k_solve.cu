@@ -696,6 +696,7 @@ void launch_solve_batch(Context& c, const SolveBatch& b) {
   DGPU_LAUNCH("k_solve_cluster");
   // Systems whose Cholesky met a non-positive pivot are redone by pivoted
   // LDL^T, as the reference falls back from LLT to LDLT (src/solve.cpp:177-181).
+  if (b.skip_ldlt) return;
   StageTimer t(c, "fit: LDLT fallback");
   launch_ldlt_fallback(c, b);
 }
