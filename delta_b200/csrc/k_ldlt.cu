@@ -67,33 +67,13 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Block-wide sum in a fixed order (warp sums, then warp 0 over the warps).
-__device__ double block_sum(double v, double* red) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  v = warp_sum(v);
-  __syncthreads();
-  if (lane == 0) red[warp] = v;
-  __syncthreads();
-  if (warp == 0) {
-    double t = lane < static_cast<int>(blockDim.x >> 5) ? red[lane] : 0.0;
-    t = warp_sum(t);
-    if (lane == 0) red[32] = t;
-  }
-  __syncthreads();
-  return red[32];
-}
-
 }  // namespace
 
 // Block-shared scratch of the factorisation and solves.
 struct LdltShared {
-  double temp[1024];  // d_j L_kj of the current step; later a solve vector
-  double red[33];
-  double best[32];
-  int bidx[32];
-  int piv;
-  double dk;
-  int perm[1024];  // position -> original index
+  double temp[1024];  // the pivot replay's diagonal; later a solve vector
+  int piv;            // -1: the whole diagonal is zero
+  int perm[1024];     // position -> original index
 };
 
 // Eigen's pivot order, from the diagonal alone: its LDLT is left-looking, so
@@ -266,26 +246,6 @@ __device__ void ldlt_dinv(const double* A, int P, int n_steps, double* dinv) {
   __syncthreads();
 }
 
-// One thread's column solve: Y[:, c] = L^-T D^+ L^-1 (Pi b) in the permuted
-// order, b_i = rhs(original row i). Rows above `stop` of the backward pass are
-// left unfinished (the trace needs only Y[c][c]).
-template <class Rhs>
-__device__ void ldlt_solve_col(const double* A, int P, const int* perm, const double* dinv, Rhs rhs, double* Y,
-                               int ldy, int c, int stop) {
-  for (int i = 0; i < P; ++i) {
-    const double* Ai = A + static_cast<size_t>(i) * P;
-    double v = rhs(perm[i]);
-    for (int j = 0; j < i; ++j) v = fma(-Ai[j], Y[static_cast<size_t>(j) * ldy + c], v);
-    Y[static_cast<size_t>(i) * ldy + c] = v;
-  }
-  for (int i = 0; i < P; ++i) Y[static_cast<size_t>(i) * ldy + c] *= dinv[i];
-  for (int i = P - 1; i >= stop; --i) {
-    double v = Y[static_cast<size_t>(i) * ldy + c];
-    for (int t = i + 1; t < P; ++t) v = fma(-A[static_cast<size_t>(t) * P + i], Y[static_cast<size_t>(t) * ldy + c], v);
-    Y[static_cast<size_t>(i) * ldy + c] = v;
-  }
-}
-
 struct LdltWork {
   double* d;  // chunk x ldlt_sys_doubles(P)
   int* i;     // chunk x (P + 1): permutation, factored flag
@@ -343,37 +303,20 @@ __global__ void __launch_bounds__(kLdltThreads) k_ldlt_factor(SolveBatch b, int 
   if (tid == 0) *factored = 1;
 }
 
-// edf terms Z_cc, Z = L^-T D^+ L^-1 B, B = Pi M Pi^T: thread c solves column
-// c, the CTA's kLdltTraceThreads columns together, by panels of kLb rows. Per
-// panel the threads solve its triangular block with their panel values in
-// registers, then update the rows still to come with the panel's L read once
-// into shared memory (chunks of kTrRows rows) -- every L value is a broadcast
-// shared load, every y value one coalesced load and store. The backward
-// pass stops at the panel of the CTA's first column (x_c needs x_t, t > c
-// only). Grid: (chunk systems, ceil(P / kLdltTraceThreads)).
+// Y[:, c] <- L^-T D^+ L^-1 Y[:, c] for the thread's column c (Y is P rows of
+// stride ldy), the CTA's columns together, by panels of kLb rows. Per panel the
+// threads solve its triangular block with their panel values in registers,
+// then update the rows still to come with the panel's L read once into shared
+// memory (chunks of kTrRows rows): every L value is a broadcast shared load,
+// every y value one coalesced load and store. The backward pass stops at the
+// panel holding row `stop` (rows above it are left unfinished).
 constexpr int kTrRows = 64;
 
-__global__ void __launch_bounds__(kLdltTraceThreads) k_ldlt_trace(SolveBatch b, int s0, LdltWork wk) {
-  __shared__ double lp[kLb][kLb + 1];     // the panel's diagonal block
+__device__ void panel_solve(const double* A, int P, const double* dinv, double* Y, size_t ldy, int c, bool act,
+                            int stop) {
+  __shared__ double lp[kLb][kLb + 1];      // the panel's diagonal block
   __shared__ double ls[kTrRows][kLb + 1];  // a chunk of the panel's other rows (forward) / columns (backward)
-  const int P = b.P;
-  const size_t PP = static_cast<size_t>(P) * P;
-  const int s = s0 + static_cast<int>(blockIdx.x);
-  double* A = wk.d + blockIdx.x * ldlt_sys_doubles(P);
-  double* Y = A + PP;
-  const double* dinv = A + 2 * PP;
-  double* zc = A + 2 * PP + P;
-  const int* perm = wk.i + blockIdx.x * (static_cast<size_t>(P) + 1);
-  if (!perm[P]) return;  // the same for the whole CTA
   const int tid = threadIdx.x, nt = blockDim.x;
-  const int c0 = static_cast<int>(blockIdx.y) * kLdltTraceThreads;
-  const int c = c0 + tid;
-  const bool act = c < P;
-  const double* M = b.M + static_cast<size_t>(b.m_index ? b.m_index[s] : 0) * PP;
-  if (act) {
-    const int oc = perm[c];
-    for (int i = 0; i < P; ++i) Y[static_cast<size_t>(i) * P + c] = M[static_cast<size_t>(perm[i]) * P + oc];
-  }
   double yp[kLb];
   // Forward: y = L^-1 b (L unit lower).
   for (int p0 = 0; p0 < P; p0 += kLb) {
@@ -388,11 +331,11 @@ __global__ void __launch_bounds__(kLdltTraceThreads) k_ldlt_trace(SolveBatch b, 
 #pragma unroll
       for (int k = 0; k < kLb; ++k) {
         if (k < nb) {
-          double v = Y[static_cast<size_t>(p0 + k) * P + c];
+          double v = Y[static_cast<size_t>(p0 + k) * ldy + c];
 #pragma unroll
           for (int j = 0; j < k; ++j) v = fma(-lp[k][j], yp[j], v);
           yp[k] = v;
-          Y[static_cast<size_t>(p0 + k) * P + c] = v;
+          Y[static_cast<size_t>(p0 + k) * ldy + c] = v;
         }
       }
     }
@@ -406,7 +349,7 @@ __global__ void __launch_bounds__(kLdltTraceThreads) k_ldlt_trace(SolveBatch b, 
       __syncthreads();
       if (act) {
         for (int r = 0; r < nr; ++r) {
-          double* yr = Y + static_cast<size_t>(r0 + r) * P + c;
+          double* yr = Y + static_cast<size_t>(r0 + r) * ldy + c;
           double v = *yr;
 #pragma unroll
           for (int k = 0; k < kLb; ++k)
@@ -418,10 +361,10 @@ __global__ void __launch_bounds__(kLdltTraceThreads) k_ldlt_trace(SolveBatch b, 
   }
   // D^+.
   if (act)
-    for (int i = 0; i < P; ++i) Y[static_cast<size_t>(i) * P + c] *= dinv[i];
-  // Backward: x = L^-T y, panels from the last down to the one holding c0.
+    for (int i = 0; i < P; ++i) Y[static_cast<size_t>(i) * ldy + c] *= dinv[i];
+  // Backward: x = L^-T y, panels from the last down to the one holding `stop`.
   const int last = ((P - 1) / kLb) * kLb;
-  for (int p0 = last; p0 + kLb > c0; p0 -= kLb) {
+  for (int p0 = last; p0 + kLb > stop; p0 -= kLb) {
     const int nb = min(kLb, P - p0);
     __syncthreads();
     for (int e = tid; e < nb * nb; e += nt) {
@@ -433,17 +376,17 @@ __global__ void __launch_bounds__(kLdltTraceThreads) k_ldlt_trace(SolveBatch b, 
 #pragma unroll
       for (int kk = kLb - 1; kk >= 0; --kk) {
         if (kk < nb) {
-          double v = Y[static_cast<size_t>(p0 + kk) * P + c];
+          double v = Y[static_cast<size_t>(p0 + kk) * ldy + c];
 #pragma unroll
           for (int t = kk + 1; t < kLb; ++t)
             if (t < nb) v = fma(-lp[t][kk], yp[t], v);
           yp[kk] = v;
-          Y[static_cast<size_t>(p0 + kk) * P + c] = v;
+          Y[static_cast<size_t>(p0 + kk) * ldy + c] = v;
         }
       }
     }
-    // rows r in [c0, p0) above the panel: y_r -= sum_t L[p0 + t][r] x_t
-    const int rlo = min(c0, p0);
+    // rows r in [stop, p0) above the panel: y_r -= sum_t L[p0 + t][r] x_t
+    const int rlo = min(stop, p0);
     for (int r0 = rlo; r0 < p0; r0 += kTrRows) {
       const int nr = min(kTrRows, p0 - r0);
       __syncthreads();
@@ -454,7 +397,7 @@ __global__ void __launch_bounds__(kLdltTraceThreads) k_ldlt_trace(SolveBatch b, 
       __syncthreads();
       if (act) {
         for (int r = 0; r < nr; ++r) {
-          double* yr = Y + static_cast<size_t>(r0 + r) * P + c;
+          double* yr = Y + static_cast<size_t>(r0 + r) * ldy + c;
           double v = *yr;
 #pragma unroll
           for (int t = 0; t < kLb; ++t)
@@ -465,6 +408,30 @@ __global__ void __launch_bounds__(kLdltTraceThreads) k_ldlt_trace(SolveBatch b, 
     }
     if (p0 == 0) break;
   }
+}
+
+// edf terms Z_cc, Z = L^-T D^+ L^-1 B, B = Pi M Pi^T: thread c solves column c
+// (x_c needs x_t, t > c only, so the backward pass stops at the CTA's first
+// column). Grid: (chunk systems, ceil(P / kLdltTraceThreads)).
+__global__ void __launch_bounds__(kLdltTraceThreads) k_ldlt_trace(SolveBatch b, int s0, LdltWork wk) {
+  const int P = b.P;
+  const size_t PP = static_cast<size_t>(P) * P;
+  const int s = s0 + static_cast<int>(blockIdx.x);
+  double* A = wk.d + blockIdx.x * ldlt_sys_doubles(P);
+  double* Y = A + PP;
+  const double* dinv = A + 2 * PP;
+  double* zc = A + 2 * PP + P;
+  const int* perm = wk.i + blockIdx.x * (static_cast<size_t>(P) + 1);
+  if (!perm[P]) return;  // the same for the whole CTA
+  const int c0 = static_cast<int>(blockIdx.y) * kLdltTraceThreads;
+  const int c = c0 + static_cast<int>(threadIdx.x);
+  const bool act = c < P;
+  const double* M = b.M + static_cast<size_t>(b.m_index ? b.m_index[s] : 0) * PP;
+  if (act) {
+    const int oc = perm[c];
+    for (int i = 0; i < P; ++i) Y[static_cast<size_t>(i) * P + c] = M[static_cast<size_t>(perm[i]) * P + oc];
+  }
+  panel_solve(A, P, dinv, Y, P, c, act, c0);
   if (act) zc[c] = Y[static_cast<size_t>(c) * P + c];
 }
 
@@ -482,33 +449,52 @@ __global__ void k_ldlt_finish(SolveBatch b, int s0, LdltWork wk) {
   b.ok[s] = 2;
 }
 
-// X = A^+ B for A = M + lambda P0 (one CTA): B and X are P x m, row-major, in
-// the original order; Y is a P x m workspace. The same factorisation as the
-// fallback; used where many right-hand sides share one system.
-__global__ void __launch_bounds__(kLdltThreads) k_sym_solve_many(int P, int kk, const double* __restrict__ M, double lam,
-                                                                 const double* __restrict__ pen, const double* __restrict__ B,
-                                                                 int m, double* __restrict__ A, double* __restrict__ Y,
-                                                                 double* __restrict__ dinv, double* __restrict__ X) {
+// X = A^+ B for A = M + lambda P0: B and X are P x m, row-major, in the
+// original order. The same factorisation as the fallback (one CTA), then the
+// columns of B by the panel solve (m / kLdltTraceThreads CTAs); used where
+// many right-hand sides share one system. Workspace: A (P x P), Y (P x m),
+// D^+ (P), the factorisation's panels (2 kLb P), the permutation (P ints).
+__global__ void __launch_bounds__(kLdltThreads) k_sym_factor(int P, int kk, const double* __restrict__ M, double lam,
+                                                             const double* __restrict__ pen, double* __restrict__ A,
+                                                             double* __restrict__ dinv, int* __restrict__ perm) {
   __shared__ LdltShared S;
   double* Wt = dinv + P;  // 2 x kLb x P panel workspace
   const bool any = build_pivoted(A, M, P, kk, lam, pen, S);
   if (any) ldlt_blocked(A, P, Wt, Wt + static_cast<size_t>(kLb) * P);
   ldlt_dinv(A, P, any ? P : 0, dinv);
-  for (int c = threadIdx.x; c < m; c += blockDim.x) {
-    ldlt_solve_col(A, P, S.perm, dinv, [&](int io) { return B[static_cast<size_t>(io) * m + c]; }, Y, m, c, 0);
-    for (int i = 0; i < P; ++i) X[static_cast<size_t>(S.perm[i]) * m + c] = Y[static_cast<size_t>(i) * m + c];
-  }
+  for (int i = threadIdx.x; i < P; i += blockDim.x) perm[i] = S.perm[i];
+}
+
+__global__ void __launch_bounds__(kLdltTraceThreads) k_sym_solve_cols(int P, const double* __restrict__ A,
+                                                                      const double* __restrict__ dinv,
+                                                                      const int* __restrict__ perm,
+                                                                      const double* __restrict__ B, int m,
+                                                                      double* __restrict__ Y, double* __restrict__ X) {
+  const int c = static_cast<int>(blockIdx.x) * kLdltTraceThreads + static_cast<int>(threadIdx.x);
+  const bool act = c < m;
+  if (act)
+    for (int i = 0; i < P; ++i) Y[static_cast<size_t>(i) * m + c] = B[static_cast<size_t>(perm[i]) * m + c];
+  panel_solve(A, P, dinv, Y, m, c, act, 0);
+  if (act)
+    for (int i = 0; i < P; ++i) X[static_cast<size_t>(perm[i]) * m + c] = Y[static_cast<size_t>(i) * m + c];
 }
 
 void launch_sym_solve_many(Context& c, int P, int k, const double* M, double lam, const double* pen, const double* B,
                            int m, double* X) {
   if (P > kLdltThreads) fail(DGPU_ERR_INVALID, "solve: at most 1024 unknowns are supported");
-  double* work = static_cast<double*>(
-      c.slot(kSlotGrad6, sizeof(double) * (static_cast<size_t>(P) * P + static_cast<size_t>(P) * m + P +
-                                           2 * static_cast<size_t>(kLb) * P)));
-  k_sym_solve_many<<<1, kLdltThreads, 0, c.stream>>>(P, k, M, lam, pen, B, m, work, work + static_cast<size_t>(P) * P,
-                                                     work + static_cast<size_t>(P) * P + static_cast<size_t>(P) * m, X);
-  DGPU_LAUNCH("k_sym_solve_many");
+  const size_t PP = static_cast<size_t>(P) * P, Pm = static_cast<size_t>(P) * m;
+  char* work = static_cast<char*>(c.slot(
+      kSlotGrad6, sizeof(double) * (PP + Pm + P + 2 * static_cast<size_t>(kLb) * P) + sizeof(int) * P + 16));
+  double* A = reinterpret_cast<double*>(work);
+  double* Y = A + PP;
+  double* dinv = Y + Pm;
+  int* perm = reinterpret_cast<int*>(dinv + P + 2 * static_cast<size_t>(kLb) * P);
+  k_sym_factor<<<1, kLdltThreads, 0, c.stream>>>(P, k, M, lam, pen, A, dinv, perm);
+  DGPU_LAUNCH("k_sym_factor");
+  if (m <= 0) return;
+  k_sym_solve_cols<<<(m + kLdltTraceThreads - 1) / kLdltTraceThreads, kLdltTraceThreads, 0, c.stream>>>(
+      P, A, dinv, perm, B, m, Y, X);
+  DGPU_LAUNCH("k_sym_solve_cols");
 }
 
 void launch_ldlt_fallback(Context& c, const SolveBatch& b) {
