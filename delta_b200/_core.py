@@ -310,7 +310,8 @@ def subtract_batch_native(items, *, n_max: int = 6, n_knots: int = 5, radius: in
     cfg = _lib.BatchConfig(n_max, n_knots, radius, stamp_radius, threshold_sigma, max_stamps, saturation,
                            fwhm_radius, match_radius, grid.ctypes.data, grid.size, clip_sigma, clip_iterations,
                            min_stamps, cv_folds, PRECISIONS[precision], int(decorrelate), block, int(score),
-                           int(catalog), catalog_threshold_sigma, frames_in_flight, 0, int(bool(graphs)))
+                           int(catalog), catalog_threshold_sigma, frames_in_flight, _lib._default_device(),
+                           int(bool(graphs)))
     n = len(items)
     frames = (_lib.Frame * max(n, 1))()
     results = (_lib.FrameResult * max(n, 1))()

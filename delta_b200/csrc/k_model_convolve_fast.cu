@@ -12,8 +12,13 @@
 //     stay finite for any image below ~1e37) a zero tap adds an exact +-0 to a
 //     sum that starts at +0 and is never -0, so each output keeps the
 //     reference's sum over j = 0..ks-1 bit for bit.
-//   * The x pass keeps its 4-wide sliding window in registers across the
-//     unrolled taps (no moves), one 16-byte tap load per component per 4 taps.
+//   * The x pass works on row pairs: the reference window is staged with
+//     rows 2p and 2p + 1 interleaved, so one 8-byte load gives both rows'
+//     sample and one packed FMA (an IEEE fma per lane) applies a tap to both;
+//     each thread holds 2 columns x 2 rows x NX components, its 2-wide
+//     sliding window in registers across the unrolled taps, and reads the taps
+//     duplicated (k, k) two at a time with 16-byte loads. Off-frame rows are
+//     staged as zeros, so their x sums are exact +0 without a row test.
 //   * The lattice corners of the cells the tile touches (every field) are
 //     staged in shared memory once, so the blend of each component reads no
 //     global memory.
@@ -39,7 +44,6 @@ constexpr int kFTW = 32;   // tile width (columns)
 constexpr int kFPad = 8;   // zero rows in front of each x-pass buffer
 constexpr int kFLPad = 8;  // zero columns left of the reference window
 constexpr int kFYR = 4;    // output rows per thread in the y pass (2 columns each)
-constexpr int kFXPT = 4;   // output columns per thread in the x pass
 
 __host__ __device__ constexpr int fast_rw(int ks) { return (kFLPad + kFTW + (ks - 1) + 3) & ~3; }
 
@@ -59,10 +63,12 @@ k_model_convolve_f(int w, int h, const float* __restrict__ sci, const float* __r
   const int gbw = kFTW + 2 * kh;
   const int rw = fast_rw(ks);
   const int trows = nrows + kFPad;
-  float* rtile = smem;                          // nrows x rw; column kFLPad + c <-> frame column bx - kh + c
-  float* txs = rtile + nrows * rw;              // NX x (kFPad zero rows + nrows) x kFTW
+  const int npair = (nrows + 1) / 2;
+  float* rtile = smem;                          // npair x rw row pairs; column kFLPad + c <-> frame column bx - kh + c
+  float* txs = rtile + 2 * npair * rw;          // NX x (kFPad zero rows + nrows) x kFTW
   float* ktaps = txs + NX * trows * kFTW;       // NX x KSP, zero padded
-  float* slat = ktaps + NX * KSP;               // nf x lly x llx lattice corners (lat_cap floats)
+  float2* ktaps2 = reinterpret_cast<float2*>(ktaps + NX * KSP);  // the same taps duplicated (k, k)
+  float* slat = ktaps + 3 * NX * KSP;           // nf x lly x llx lattice corners (lat_cap floats)
   const int bx = blockIdx.x * kFTW, by = blockIdx.y * TH;
   const float fill = *fillp;
   const int tid = threadIdx.x;
@@ -85,68 +91,66 @@ k_model_convolve_f(int w, int h, const float* __restrict__ sci, const float* __r
 
   for (int i = tid; i < NX * KSP; i += blockDim.x) {
     const int q = i / KSP, j = i - q * KSP;
-    ktaps[i] = j < ks ? taps[q * ks + j] : 0.0f;
+    const float k = j < ks ? taps[q * ks + j] : 0.0f;
+    ktaps[i] = k;
+    ktaps2[i] = make_float2(k, k);
   }
   for (int i = tid; i < NX * kFPad * kFTW; i += blockDim.x) {
     const int q = i / (kFPad * kFTW);
     txs[q * trows * kFTW + (i - q * kFPad * kFTW)] = 0.0f;
   }
-  for (int i = tid; i < nrows * rw; i += blockDim.x) {
+  for (int i = tid; i < 2 * npair * rw; i += blockDim.x) {
     const int r = i / rw, cc = i - r * rw, c = cc - kFLPad;
     const int gy = by - kh + r, gx = bx - kh + c;
     float v = 0.0f;
-    if (c >= 0 && c < gbw && gy >= 0 && gy < h && gx >= 0 && gx < w) {
+    if (r < nrows && c >= 0 && c < gbw && gy >= 0 && gy < h && gx >= 0 && gx < w) {
       const size_t idx = static_cast<size_t>(gy) * w + gx;
       v = __ldg(ref + idx);
       const bool bad = (rmask && __ldg(rmask + idx) != 0) || !isfinite(v);
       if (bad) v = fill;
     }
-    rtile[i] = v;
+    rtile[((r >> 1) * rw + cc) * 2 + (r & 1)] = v;
   }
   __syncthreads();
 
-  // ---- x pass: txs[nx][r][lx] = sum_j k[nx][j] * R~[y][x + kh - j] ----
-  constexpr int ngrp = kFTW / kFXPT;
-  for (int it = tid; it < nrows * ngrp; it += blockDim.x) {
-    const int r = it / ngrp, cg = it - r * ngrp;
-    const int gy = by - kh + r;
-    const int c0 = cg * kFXPT;
-    float acc[NX][kFXPT];
+  // ---- x pass: txs[nx][r][lx] = sum_j k[nx][j] * R~[y][x + kh - j], rows in pairs ----
+  constexpr int ngrp = kFTW / 2;
+  const float2* rt2 = reinterpret_cast<const float2*>(rtile);
+  for (int it = tid; it < npair * ngrp; it += blockDim.x) {
+    const int rp = it / ngrp, cg = it - rp * ngrp;
+    const int c0 = cg * 2;
+    const float2* row = rt2 + rp * rw + kFLPad + c0 + 2 * kh;  // column of tap j=0, output 0
+    float2 acc[NX][2];
 #pragma unroll
-    for (int q = 0; q < NX; ++q)
+    for (int q = 0; q < NX; ++q) acc[q][0] = acc[q][1] = make_float2(0.0f, 0.0f);
+    float2 win[2] = {row[0], row[1]};
 #pragma unroll
-      for (int i = 0; i < kFXPT; ++i) acc[q][i] = 0.0f;
-    if (gy >= 0 && gy < h) {
-      const float* row = rtile + r * rw + kFLPad + c0 + 2 * kh;  // column of tap j=0, output 0
-      float win[kFXPT];
+    for (int j0 = 0; j0 < KSP; j0 += 2) {
+      float4 kq[NX];
 #pragma unroll
-      for (int i = 0; i < kFXPT; ++i) win[i] = row[i];
+      for (int q = 0; q < NX; ++q) kq[q] = *reinterpret_cast<const float4*>(ktaps2 + q * KSP + j0);
 #pragma unroll
-      for (int j0 = 0; j0 < KSP; j0 += 4) {
-        float4 kq[NX];
+      for (int jj = 0; jj < 2; ++jj) {
+        const int j = j0 + jj;
+        if (j > 0) {
+          win[1] = win[0];
+          win[0] = row[-j];
+        }
 #pragma unroll
-        for (int q = 0; q < NX; ++q) kq[q] = *reinterpret_cast<const float4*>(ktaps + q * KSP + j0);
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj) {
-          const int j = j0 + jj;
-          if (j > 0) {
-#pragma unroll
-            for (int i = kFXPT - 1; i > 0; --i) win[i] = win[i - 1];
-            win[0] = row[-j];
-          }
-#pragma unroll
-          for (int q = 0; q < NX; ++q) {
-            const float kc = jj == 0 ? kq[q].x : jj == 1 ? kq[q].y : jj == 2 ? kq[q].z : kq[q].w;
-#pragma unroll
-            for (int i = 0; i < kFXPT; ++i) acc[q][i] = __fmaf_rn(kc, win[i], acc[q][i]);
-          }
+        for (int q = 0; q < NX; ++q) {
+          const float2 kc = jj == 0 ? make_float2(kq[q].x, kq[q].y) : make_float2(kq[q].z, kq[q].w);
+          acc[q][0] = __ffma2_rn(kc, win[0], acc[q][0]);
+          acc[q][1] = __ffma2_rn(kc, win[1], acc[q][1]);
         }
       }
     }
+    const int r = 2 * rp;
 #pragma unroll
     for (int q = 0; q < NX; ++q) {
-      const float4 v = make_float4(acc[q][0], acc[q][1], acc[q][2], acc[q][3]);
-      *reinterpret_cast<float4*>(txs + (q * trows + kFPad + r) * kFTW + c0) = v;
+      *reinterpret_cast<float2*>(txs + (q * trows + kFPad + r) * kFTW + c0) = make_float2(acc[q][0].x, acc[q][1].x);
+      if (r + 1 < nrows)
+        *reinterpret_cast<float2*>(txs + (q * trows + kFPad + r + 1) * kFTW + c0) =
+            make_float2(acc[q][0].y, acc[q][1].y);
     }
   }
   __syncthreads();
@@ -310,8 +314,9 @@ size_t model_convolve_fast_smem(int nx, int ks, int TH, const DevFields& F) {
   const int kh = (ks - 1) / 2;
   const int nrows = TH + 2 * kh;
   const int kb = (ks + 7) / 8;
-  return sizeof(float) * (static_cast<size_t>(nrows) * fast_rw(ks) + static_cast<size_t>(nx) * (nrows + kFPad) * kFTW +
-                          static_cast<size_t>(nx) * 8 * kb + static_cast<size_t>(lattice_cap(F, TH)));
+  return sizeof(float) * (2 * static_cast<size_t>((nrows + 1) / 2) * fast_rw(ks) +
+                          static_cast<size_t>(nx) * (nrows + kFPad) * kFTW + static_cast<size_t>(nx) * 3 * 8 * kb +
+                          static_cast<size_t>(lattice_cap(F, TH)));
 }
 
 bool model_convolve_fast_available(int nx, int ks) {

@@ -50,21 +50,48 @@ __global__ void k_select_hist(const uint32_t* __restrict__ keys, RadixSelect* st
     if (hist[i]) atomicAdd(&st->hist[i], hist[i]);
 }
 
+// One warp: each lane sums 8 bins, a warp prefix sum finds the lane whose
+// bins hold the rank, that lane walks its 8, and the histogram is cleared.
 __global__ void k_select_pick(RadixSelect* st, int shift, float* result, int last) {
-  if (threadIdx.x != 0) return;
-  unsigned rank = st->rank, cum = 0;
-  int digit = 255;
-  for (int d = 0; d < 256; ++d) {
-    if (rank < cum + st->hist[d]) {
-      digit = d;
-      break;
-    }
-    cum += st->hist[d];
+  const int lane = threadIdx.x;
+  if (lane >= 32) return;
+  unsigned h[8];
+  unsigned local = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    h[j] = st->hist[lane * 8 + j];
+    local += h[j];
   }
-  st->rank = rank - cum;
-  st->prefix |= static_cast<unsigned>(digit) << shift;
-  for (int d = 0; d < 256; ++d) st->hist[d] = 0;
-  if (last) *result = st->count ? key_float(st->prefix) : 0.0f;
+  unsigned incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const unsigned excl = incl - local;
+  const unsigned rank = st->rank;
+  // The lane holding the rank (the last lane when the rank is past every bin,
+  // which leaves digit 255 as a sequential scan would).
+  const bool here = (rank >= excl && rank < incl) || (lane == 31 && rank >= incl);
+  const unsigned who = __ballot_sync(0xffffffffu, here);
+  __syncwarp();
+  if (lane == __ffs(who) - 1) {
+    unsigned cum = excl;
+    int digit = lane * 8 + 7;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      if (rank < cum + h[j]) {
+        digit = lane * 8 + j;
+        break;
+      }
+      cum += h[j];
+    }
+    st->rank = rank - cum;
+    st->prefix |= static_cast<unsigned>(digit) << shift;
+    if (last) *result = st->count ? key_float(st->prefix) : 0.0f;
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) st->hist[lane * 8 + j] = 0;
 }
 
 void launch_sample_keys(cudaStream_t s, int64_t n, int64_t step, const float* v, const uint8_t* mask, uint32_t* keys,
