@@ -522,22 +522,26 @@ k_block_filter(FftGeom G, const float* __restrict__ src, int w, int h, const int
   // Row pass (r2c), scattered to the column owners. 256 threads: each loop
   // below has a fixed trip count, so its loads are all in flight together.
   const int tid = threadIdx.x;
-  for (int b0 = rbeg; b0 < rend; b0 += kBfBatch) {
-    {
-      float2 v[kBfBatch * hn / 256];
+  // The next batch's samples are loaded while this batch transforms.
+  constexpr int kPer = kBfBatch * hn / 256;
+  float2 v[kPer];
+  auto load_batch = [&](int b) {
 #pragma unroll
-      for (int i = 0; i < kBfBatch * hn / 256; ++i) {
-        const int e = tid + 256 * i, rr = e / hn, j = e - rr * hn;
-        const int sy = reflect_clamp(by + b0 + rr, h);
-        const float* srow = src + static_cast<size_t>(sy) * w;
-        v[i] = make_float2(__ldg(srow + reflect_clamp(bx + 2 * j, w)), __ldg(srow + reflect_clamp(bx + 2 * j + 1, w)));
-      }
-#pragma unroll
-      for (int i = 0; i < kBfBatch * hn / 256; ++i) {
-        const int e = tid + 256 * i, rr = e / hn, j = e - rr * hn;
-        z[rr * zl + j] = v[i];
-      }
+    for (int i = 0; i < kPer; ++i) {
+      const int e = tid + 256 * i, rr = e / hn, j = e - rr * hn;
+      const int sy = reflect_clamp(by + b + rr, h);
+      const float* srow = src + static_cast<size_t>(sy) * w;
+      v[i] = make_float2(__ldg(srow + reflect_clamp(bx + 2 * j, w)), __ldg(srow + reflect_clamp(bx + 2 * j + 1, w)));
     }
+  };
+  load_batch(rbeg);
+  for (int b0 = rbeg; b0 < rend; b0 += kBfBatch) {
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int e = tid + 256 * i, rr = e / hn, j = e - rr * hn;
+      z[rr * zl + j] = v[i];
+    }
+    if (b0 + kBfBatch < rend) load_batch(b0 + kBfBatch);
     __syncthreads();
     fft_lines<-1>(z, kBfBatch, hn, G.logn - 1, tw_fwd_hn, zl);
 #pragma unroll
@@ -611,35 +615,38 @@ k_block_filter(FftGeom G, const float* __restrict__ src, int w, int h, const int
   fft_lines<1>(x, ncol, n, G.logn, tw_inv_n, ls);
   cl.sync();
 
-  // Row inverse (c2r): gather each row's bins from the owners.
-  for (int b0 = rbeg; b0 < rend; b0 += kBfBatch) {
-    {
-      float2 xk[kBfBatch * hn / 256], xc[kBfBatch * hn / 256];
+  // Row inverse (c2r): gather each row's bins from the owners; the next
+  // batch's bins are requested while this batch transforms.
+  float2 xk[kPer], xc[kPer];
+  auto gather_batch = [&](int b) {
 #pragma unroll
-      for (int i = 0; i < kBfBatch * hn / 256; ++i) {
-        const int e = tid + 256 * i, rr = e / hn, k = e - rr * hn;
-        if (k == 0) {  // the packed line: DC in the real part, Nyquist in the imaginary part
-          const float2 p = *cl.map_shared_rank(x + b0 + rr, 0);
-          xk[i] = make_float2(p.x, 0.0f);
-          xc[i] = make_float2(p.y, 0.0f);
-        } else {
-          xk[i] = *bin(k, b0 + rr);
-          xc[i] = cconj(*bin(hn - k, b0 + rr));
-        }
-      }
-#pragma unroll
-      for (int i = 0; i < kBfBatch * hn / 256; ++i) {
-        const int e = tid + 256 * i, rr = e / hn, k = e - rr * hn;
-        float2 a = xk[i], c = xc[i];
-        if (k == 0) {  // c2r ignores the imaginary parts of the DC and Nyquist bins
-          a.y = 0.0f;
-          c.y = 0.0f;
-        }
-        const float2 e2 = cadd(a, c);
-        const float2 o2 = cmul(csub(a, c), split_inv[k]);
-        z[rr * zl + k] = make_float2(e2.x - o2.y, e2.y + o2.x);  // 2E + i 2O
+    for (int i = 0; i < kPer; ++i) {
+      const int e = tid + 256 * i, rr = e / hn, k = e - rr * hn;
+      if (k == 0) {  // the packed line: DC in the real part, Nyquist in the imaginary part
+        const float2 p = *cl.map_shared_rank(x + b + rr, 0);
+        xk[i] = make_float2(p.x, 0.0f);
+        xc[i] = make_float2(p.y, 0.0f);
+      } else {
+        xk[i] = *bin(k, b + rr);
+        xc[i] = cconj(*bin(hn - k, b + rr));
       }
     }
+  };
+  gather_batch(rbeg);
+  for (int b0 = rbeg; b0 < rend; b0 += kBfBatch) {
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int e = tid + 256 * i, rr = e / hn, k = e - rr * hn;
+      float2 a = xk[i], c = xc[i];
+      if (k == 0) {  // c2r ignores the imaginary parts of the DC and Nyquist bins
+        a.y = 0.0f;
+        c.y = 0.0f;
+      }
+      const float2 e2 = cadd(a, c);
+      const float2 o2 = cmul(csub(a, c), split_inv[k]);
+      z[rr * zl + k] = make_float2(e2.x - o2.y, e2.y + o2.x);  // 2E + i 2O
+    }
+    if (b0 + kBfBatch < rend) gather_batch(b0 + kBfBatch);
     __syncthreads();
     fft_lines<1>(z, kBfBatch, hn, G.logn - 1, tw_inv_hn, zl);
 #pragma unroll 4
