@@ -197,11 +197,10 @@ def negate(t) -> None:
 
 def download(out: dict) -> dict:
     """Copy the image products of run()/apply() into pinned host memory;
-    returns {name: ndarray | None}. The copies are SM stores into the mapped
-    pinned buffers (dgpu_copy_to_host), not copy-engine transfers: frames
-    computing on other streams read small results back through the one
-    device-to-host copy engine, and a 200 MB download queued there would hold
-    each of those reads for its whole duration."""
+    returns {name: ndarray | None}. The copies go through the copy engine
+    (dgpu_copy_to_host); the library's own small read-backs reach the host by
+    SM stores, so frames computing on other streams do not wait behind a
+    200 MB download."""
     ctx = _ctx_on_torch_stream()
     pinned = {}
     for key in ("difference", "variance", "mask", "score"):
@@ -211,11 +210,8 @@ def download(out: dict) -> dict:
             continue
         t = t.contiguous()
         hbuf = torch.empty(tuple(t.shape), dtype=t.dtype, pin_memory=True)
-        try:
-            check(_lib.lib().dgpu_copy_to_host(ctx.handle, ctypes.c_void_p(hbuf.data_ptr()), _p(t),
-                                               ctypes.c_int64(t.numel() * t.element_size())), ctx.handle)
-        except ValueError:  # pinned memory without a mapped address: copy-engine transfer
-            hbuf.copy_(t, non_blocking=True)
+        check(_lib.lib().dgpu_copy_to_host(ctx.handle, ctypes.c_void_p(hbuf.data_ptr()), _p(t),
+                                           ctypes.c_int64(t.numel() * t.element_size())), ctx.handle)
         pinned[key] = hbuf
     torch.cuda.current_stream().synchronize()
     return {k: (None if v is None else v.numpy()) for k, v in pinned.items()}

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -30,6 +31,7 @@ int guarded(dgpu_context* ctx, F&& f) {
   try {
     if (ctx == nullptr) fail(DGPU_ERR_INVALID, "null context");
     DGPU_CUDA(cudaSetDevice(c->device));
+    drop_reads(*c);
     f(*c);
     return DGPU_OK;
   } catch (const Failure& e) {
@@ -126,7 +128,7 @@ void dgpu_destroy(dgpu_context* ctx) {
     if (kv.second) cudaGraphExecDestroy(kv.second);
   if (c->arena.base) cudaFreeHost(c->arena.base);
   if (c->d_status) cudaFree(c->d_status);
-  if (c->host_stage) cudaFreeHost(c->host_stage);
+  if (c->rb_host) cudaFreeHost(c->rb_host);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }
@@ -545,8 +547,8 @@ int dgpu_z2_median(dgpu_context* ctx, int mem, int64_t n, const float* differenc
     auto* st = static_cast<unsigned long long*>(c.slot(kSlotScratch2, 8 * 8 + 512 * 4));
     launch_z2_median(c.stream, n, d, v, m, keys, st, reinterpret_cast<unsigned int*>(st + 8));
     unsigned long long h[5];
-    DGPU_CUDA(cudaMemcpyAsync(h, st, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
-    DGPU_CUDA(cudaStreamSynchronize(c.stream));
+    read_back(c, h, st, sizeof(h));
+    sync_reads(c);
     *count = static_cast<int64_t>(h[0]);
     if (h[0] == 0) return;
     double a, b;
@@ -591,20 +593,11 @@ int dgpu_copy_to_host(dgpu_context* ctx, void* host_dst, const void* device_src,
     if (!host_dst || !device_src) fail(DGPU_ERR_INVALID, "copy_to_host: missing buffer");
     cudaPointerAttributes pa{};
     DGPU_CUDA(cudaPointerGetAttributes(&pa, host_dst));
-    void* dptr = nullptr;
-    if (pa.type != cudaMemoryTypeHost || cudaHostGetDevicePointer(&dptr, host_dst, 0) != cudaSuccess || !dptr) {
-      cudaGetLastError();
-      fail(DGPU_ERR_INVALID, "copy_to_host: destination is not mapped pinned host memory");
-    }
+    if (pa.type != cudaMemoryTypeHost) fail(DGPU_ERR_INVALID, "copy_to_host: destination is not pinned host memory");
     cudaPointerAttributes ps{};
     DGPU_CUDA(cudaPointerGetAttributes(&ps, device_src));
     if (ps.type != cudaMemoryTypeDevice) fail(DGPU_ERR_INVALID, "copy_to_host: source is not device memory");
-    const auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
-    const int64_t body = (al(dptr) && al(device_src)) ? bytes / 16 * 16 : 0;
-    launch_copy_to_mapped(c.stream, body, device_src, dptr);
-    if (body < bytes)
-      DGPU_CUDA(cudaMemcpyAsync(static_cast<char*>(host_dst) + body, static_cast<const char*>(device_src) + body,
-                                static_cast<size_t>(bytes - body), cudaMemcpyDeviceToHost, c.stream));
+    DGPU_CUDA(cudaMemcpyAsync(host_dst, device_src, static_cast<size_t>(bytes), cudaMemcpyDeviceToHost, c.stream));
   });
 }
 

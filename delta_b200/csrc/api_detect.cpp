@@ -21,6 +21,7 @@ int guarded(dgpu_context* ctx, F&& f) {
   try {
     if (!ctx) fail(DGPU_ERR_INVALID, "null context");
     DGPU_CUDA(cudaSetDevice(c->device));
+    drop_reads(*c);
     reset_status(*c);
     f(*c);
     return DGPU_OK;
@@ -185,8 +186,8 @@ int dgpu_estimate_psf(dgpu_context* ctx, int mem, int64_t width, int64_t height,
     if (n > 0) launch_psf_estimate(c, w, h, img, dxy, dxy + n, n, radius, dout, &used);
     if (used == 0) fail(DGPU_ERR_INVALID, "no usable sources for PSF estimation");
     std::vector<double> psf(np);
-    DGPU_CUDA(cudaMemcpyAsync(psf.data(), dout, sizeof(double) * np, cudaMemcpyDeviceToHost, c.stream));
-    DGPU_CUDA(cudaStreamSynchronize(c.stream));
+    read_back(c, psf.data(), dout, sizeof(double) * np);
+    sync_reads(c);
     double s = 0.0;
     for (double v : psf) s += v;
     for (int i = 0; i < np; ++i) out[i] = static_cast<float>(psf[i] / s);

@@ -37,42 +37,25 @@ T* up(Context& c, Slot s, const T* host, size_t n) {
 template <class T>
 std::vector<T> down(Context& c, const T* dev, size_t n) {
   std::vector<T> h(n);
-  if (n) DGPU_CUDA(cudaMemcpyAsync(h.data(), dev, sizeof(T) * n, cudaMemcpyDeviceToHost, c.stream));
-  DGPU_CUDA(cudaStreamSynchronize(c.stream));
+  if (n) read_back(c, h.data(), dev, sizeof(T) * n);
+  sync_reads(c);
   return h;
 }
 
-// Batched device -> host reads: every add() queues an async copy into the
-// context's pinned staging area; run() synchronises the stream once and
-// scatters the bytes to their host destinations.
+// Batched device -> host reads: every add() queues a read-back; run()
+// synchronises the stream once and scatters the bytes to their host
+// destinations.
 class Fetch {
  public:
-  Fetch(Context& c, size_t max_bytes) : c_(c), cap_(max_bytes + 16 * kMaxItems), base_(c.host_staging(cap_)) {}
+  Fetch(Context& c, size_t /*max_bytes*/) : c_(c) {}
   template <class T>
   void add(T* host, const T* dev, size_t n) {
-    const size_t bytes = sizeof(T) * n;
-    off_ = (off_ + 15) & ~static_cast<size_t>(15);
-    if (off_ + bytes > cap_ || items_.size() >= kMaxItems) fail(DGPU_ERR_RUNTIME, "fetch: staging overflow");
-    if (n) DGPU_CUDA(cudaMemcpyAsync(base_ + off_, dev, bytes, cudaMemcpyDeviceToHost, c_.stream));
-    items_.push_back({host, off_, bytes});
-    off_ += bytes;
+    if (n) read_back(c_, host, dev, sizeof(T) * n);
   }
-  void run() {
-    DGPU_CUDA(cudaStreamSynchronize(c_.stream));
-    for (const Item& it : items_) std::memcpy(it.host, base_ + it.off, it.bytes);
-  }
+  void run() { sync_reads(c_); }
 
  private:
-  static constexpr size_t kMaxItems = 16;
-  struct Item {
-    void* host;
-    size_t off, bytes;
-  };
   Context& c_;
-  size_t cap_;
-  unsigned char* base_;
-  size_t off_ = 0;
-  std::vector<Item> items_;
 };
 
 double median_copy(std::vector<double> v) {
@@ -642,6 +625,7 @@ int guarded(dgpu_context* ctx, F&& f) {
   try {
     if (!ctx) fail(DGPU_ERR_INVALID, "null context");
     DGPU_CUDA(cudaSetDevice(c->device));
+    drop_reads(*c);
     reset_status(*c);
     f(*c);
     check_status(*c);
@@ -1047,9 +1031,9 @@ int dgpu_stamp_gcv(dgpu_context* ctx, int mem, int64_t width, int64_t height, co
     GcvScalars hs{};
     double g6[6] = {0, 0, 0, 0, 0, 0};
     std::vector<double> th(P);
-    DGPU_CUDA(cudaMemcpyAsync(&hs, scal, sizeof(GcvScalars), cudaMemcpyDeviceToHost, st));
-    DGPU_CUDA(cudaMemcpyAsync(th.data(), work, sizeof(double) * P, cudaMemcpyDeviceToHost, st));
-    if (grad_gcv || grad_rss) DGPU_CUDA(cudaMemcpyAsync(g6, out6, sizeof(g6), cudaMemcpyDeviceToHost, st));
+    read_back(c, &hs, scal, sizeof(GcvScalars));
+    read_back(c, th.data(), work, sizeof(double) * P);
+    if (grad_gcv || grad_rss) read_back(c, g6, out6, sizeof(g6));
     check_status(c);  // synchronises
     if (hs.n <= 0.0) fail(DGPU_ERR_RUNTIME, "fit_kernel: no usable stamp pixels");
     values[0] = hs.gcv;

@@ -18,6 +18,7 @@ int guarded(dgpu_context* ctx, F&& f) {
   try {
     if (ctx == nullptr) fail(DGPU_ERR_INVALID, "null context");
     DGPU_CUDA(cudaSetDevice(c->device));
+    drop_reads(*c);
     f(*c);
     return DGPU_OK;
   } catch (const Failure& e) {
@@ -174,8 +175,8 @@ int dgpu_kernel_chi2(dgpu_context* ctx, int mem, int64_t width, int64_t height, 
       stage_out(c, mem, grad_reference, r.out, 4 * n);
     }
     double hs[4];
-    DGPU_CUDA(cudaMemcpyAsync(hs, sums, sizeof(hs), cudaMemcpyDeviceToHost, s));
-    if (want_theta) DGPU_CUDA(cudaMemcpyAsync(gth.data(), d_gth, sizeof(double) * gth.size(), cudaMemcpyDeviceToHost, s));
+    read_back(c, hs, sums, sizeof(hs));
+    if (want_theta) read_back(c, gth.data(), d_gth, sizeof(double) * gth.size());
     check_status(c);  // synchronises
     *chi2 = hs[0];
     if (grad_scale) *grad_scale = hs[1];

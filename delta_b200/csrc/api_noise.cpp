@@ -26,6 +26,7 @@ int guarded(dgpu_context* ctx, F&& f) {
   try {
     if (!ctx) fail(DGPU_ERR_INVALID, "null context");
     DGPU_CUDA(cudaSetDevice(c->device));
+    drop_reads(*c);
     reset_status(*c);
     f(*c);
     return DGPU_OK;
@@ -271,8 +272,8 @@ int dgpu_whiten_score_psf(dgpu_context* ctx, int mem, const float* psf, int psf_
     launch_rows_inv(s, g, 1, 1, spec_psf, nullptr, 0, 0, nullptr, nullptr, 1, nullptr, nullptr, nullptr, nullptr,
                     nullptr, nullptr, outd);
     std::vector<float> full(static_cast<size_t>(n) * n);
-    DGPU_CUDA(cudaMemcpyAsync(full.data(), outd, sizeof(float) * full.size(), cudaMemcpyDeviceToHost, s));
-    DGPU_CUDA(cudaStreamSynchronize(s));
+    read_back(c, full.data(), outd, sizeof(float) * full.size());
+    sync_reads(c);
     // Centre crop and unit-sum renormalisation (src/noise.cpp:515-531).
     const int r = psf_size / 2;
     double sum = 0.0;
@@ -311,7 +312,7 @@ int dgpu_decorrelate_block(dgpu_context* ctx, const float* image, int n, const f
     float* outd = static_cast<float*>(c.slot(kSlotFft4, sizeof(float) * static_cast<size_t>(n) * n));
     launch_rows_inv(c.stream, g, 1, 1, spec, nullptr, 0, 0, nullptr, nullptr, 1, nullptr, nullptr, nullptr, nullptr,
                     nullptr, nullptr, outd);
-    DGPU_CUDA(cudaMemcpyAsync(out, outd, sizeof(float) * static_cast<size_t>(n) * n, cudaMemcpyDeviceToHost, c.stream));
+    read_back(c, out, outd, sizeof(float) * static_cast<size_t>(n) * n);
     check_status(c);
   });
 }
@@ -335,8 +336,8 @@ int dgpu_decorrelation_kernel(dgpu_context* ctx, const float* kernel, int ksize,
     launch_rows_inv(c.stream, g, 1, 1, spec, nullptr, 0, 0, nullptr, nullptr, 1, nullptr, nullptr, nullptr, nullptr,
                     nullptr, nullptr, outd);
     std::vector<float> full(static_cast<size_t>(n) * n);
-    DGPU_CUDA(cudaMemcpyAsync(full.data(), outd, sizeof(float) * full.size(), cudaMemcpyDeviceToHost, c.stream));
-    DGPU_CUDA(cudaStreamSynchronize(c.stream));
+    read_back(c, full.data(), outd, sizeof(float) * full.size());
+    sync_reads(c);
     const int half = n / 2;
     for (int y = 0; y < n; ++y)
       for (int x = 0; x < n; ++x)

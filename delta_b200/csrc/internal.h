@@ -122,10 +122,17 @@ struct Context {
   int cat_count = 0;
   int64_t cat_npix = 0;         // label image size of the last catalog
 
-  // Pinned host staging for batched device -> host reads (grows; never
-  // shrinks).
-  unsigned char* host_stage = nullptr;
-  size_t host_stage_size = 0;
+  // Read-backs (read_back / sync_reads): a mapped pinned area that the host
+  // logic's small device -> host copies reach by SM stores, and the copies
+  // still to be scattered to their destinations at the next sync_reads.
+  struct ReadBack {
+    void* host;
+    size_t off, bytes;
+  };
+  unsigned char* rb_host = nullptr;
+  unsigned char* rb_dev = nullptr;  // rb_host's device address
+  size_t rb_used = 0;
+  std::vector<ReadBack> rb_items;
 
   // Recorded frame segments of the batch driver: key (shape and layer
   // configuration) -> executable graph (nullptr: seen once, not recorded
@@ -134,7 +141,6 @@ struct Context {
   CaptureArena arena;
 
   void* slot(Slot s, size_t bytes);
-  unsigned char* host_staging(size_t bytes);
 };
 
 // Keep freed blocks in the device's default memory pool (the workspace slots
@@ -208,6 +214,20 @@ int autotune(cudaStream_t s, const std::string& key, const std::vector<int>& can
 // RAII: clear the status word at entry, check it (after a sync) at exit.
 void reset_status(Context& c);
 void check_status(Context& c);  // synchronises the stream
+
+// Device -> host read-backs of the host logic. read_back queues a copy of
+// `bytes` from device memory, ordered on the context's stream; `host` holds
+// the bytes only after the next sync_reads, which synchronises the stream and
+// scatters them (so `host` must stay valid until then). Up to 1 MiB per sync
+// goes by SM stores into the context's mapped pinned area: every stream's
+// device-to-host copy-engine transfers share one queue in submission order,
+// and a read-back queued there behind another frame's 200 MB download waits
+// for all of it. Larger reads, and reads while a graph is recorded, use that
+// queue. Entry points drop read-backs that an error left unscattered.
+void read_back(Context& c, void* host, const void* dev, size_t bytes);
+void sync_reads(Context& c);
+void drop_reads(Context& c);
+void launch_read_back(cudaStream_t s, const void* src, void* dst, size_t bytes);
 
 // Resolve the pending stage events into `timing` (synchronises the stream).
 void resolve_timing(Context& c);
@@ -343,7 +363,6 @@ void launch_scale_fill(cudaStream_t s, int64_t n, float* v, float scale, bool fi
 void launch_negate(cudaStream_t s, int64_t n, float* v);
 // bytes (a multiple of 16) from device memory to mapped pinned host memory
 // (its device-side address), both 16-byte aligned, by SM stores.
-void launch_copy_to_mapped(cudaStream_t s, int64_t bytes, const void* src, void* dst);
 // Background median / MAD of a device image with a fixed file-scope scratch
 // (no allocation); out2 (host) = {median, MAD}. Synchronises `s`.
 void background_noalloc(int64_t n, const float* img, const uint8_t* mask, cudaStream_t s, float* out2);

@@ -436,8 +436,8 @@ static int label_polarity(Context& c, int w, int h, const uint8_t* seeds, uint8_
   k_label_final<<<grid_for(n), 256, 0, s>>>(n, L, rank_at, labels, c.d_status);
   DGPU_LAUNCH("k_label_final");
   int total = 0;
-  DGPU_CUDA(cudaMemcpyAsync(&total, counts + nb, sizeof(int), cudaMemcpyDeviceToHost, s));
-  DGPU_CUDA(cudaStreamSynchronize(s));
+  read_back(c, &total, counts + nb, sizeof(int));
+  sync_reads(c);
   return total;
 }
 
@@ -543,8 +543,8 @@ int run_catalog(Context& c, int w, int h, const float* score, const float* diff,
   DGPU_LAUNCH("k_comp_finish");
   // Bring the columns back into the context (host).
   std::vector<char> host(out_bytes);
-  DGPU_CUDA(cudaMemcpyAsync(host.data(), ob, nc * (12 * 8 + 4 * 4 + 8), cudaMemcpyDeviceToHost, s));
-  DGPU_CUDA(cudaStreamSynchronize(s));
+  read_back(c, host.data(), ob, nc * (12 * 8 + 4 * 4 + 8));
+  sync_reads(c);
   std::memcpy(c.cat_d.data(), host.data(), nc * 12 * 8);
   std::memcpy(c.cat_i.data(), host.data() + nc * 12 * 8, nc * 4 * 4);
   std::memcpy(c.cat_u8.data(), host.data() + nc * (12 * 8 + 4 * 4), nc * 8);

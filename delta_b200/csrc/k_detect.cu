@@ -429,8 +429,8 @@ void launch_psf_estimate(Context& c, int w, int h, const float* img, const int* 
   k_psf_median<<<np, 256, smem2, s>>>(n, np, cuts, use, out, c.d_status);
   DGPU_LAUNCH("k_psf_median");
   std::vector<int> hu(n);
-  if (n) DGPU_CUDA(cudaMemcpyAsync(hu.data(), use, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
-  DGPU_CUDA(cudaStreamSynchronize(s));
+  if (n) read_back(c, hu.data(), use, sizeof(int) * n);
+  sync_reads(c);
   int u = 0;
   for (int v : hu) u += v;
   *n_used = u;
@@ -471,8 +471,8 @@ void launch_weighted_mean(Context& c, int64_t n, const float* d, const float* v,
   k_weighted_mean<<<blocks, 256, 0, c.stream>>>(n, d, v, m, part);
   DGPU_LAUNCH("k_weighted_mean");
   std::vector<double> hp(2 * blocks);
-  DGPU_CUDA(cudaMemcpyAsync(hp.data(), part, sizeof(double) * 2 * blocks, cudaMemcpyDeviceToHost, c.stream));
-  DGPU_CUDA(cudaStreamSynchronize(c.stream));
+  read_back(c, hp.data(), part, sizeof(double) * 2 * blocks);
+  sync_reads(c);
   double a = 0.0, b = 0.0;
   for (int i = 0; i < blocks; ++i) {
     a += hp[2 * i];
@@ -509,13 +509,13 @@ int run_detect(Context& c, int w, int h, const float* img, const uint8_t* mask, 
   k_footprint<<<148 * 8, 256, 0, s>>>(w, h, img, mask, p, n_peaks, cap, sorted, count, cand);
   DGPU_LAUNCH("k_footprint");
   unsigned hc[2] = {0, 0};
-  DGPU_CUDA(cudaMemcpyAsync(hc, count, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-  DGPU_CUDA(cudaStreamSynchronize(s));
+  float hbg[2];
+  read_back(c, hc, count, 2 * sizeof(unsigned));
+  read_back(c, hbg, bg, sizeof(hbg));
+  sync_reads(c);
   if (hc[1] > static_cast<unsigned>(cap)) fail(DGPU_ERR_RUNTIME, "detect_stamps: more than 2^20 peak candidates");
   const unsigned nfoot = hc[0];
   const int nc = static_cast<int>(nfoot);
-  float hbg[2];
-  DGPU_CUDA(cudaMemcpyAsync(hbg, bg, sizeof(hbg), cudaMemcpyDeviceToHost, s));
   int nkept = 0;
   if (nc > 0) {
     k_cand_keys<<<(nc + 255) / 256, 256, 0, s>>>(count, cap, cand, img, keys, vals);
@@ -530,8 +530,8 @@ int run_detect(Context& c, int w, int h, const float* img, const uint8_t* mask, 
     ensure_dynamic_smem(reinterpret_cast<const void*>(k_isolate), smem);
     k_isolate<<<1, 1024, smem, s>>>(w, count, cap, sorted, iso * iso, p.max_stamps, kept, nk, c.d_status);
     DGPU_LAUNCH("k_isolate");
-    DGPU_CUDA(cudaMemcpyAsync(&nkept, nk, sizeof(int), cudaMemcpyDeviceToHost, s));
-    DGPU_CUDA(cudaStreamSynchronize(s));
+    read_back(c, &nkept, nk, sizeof(int));
+    sync_reads(c);
   }
   res.median = static_cast<double>(hbg[0]);
   res.sigma = 1.4826 * static_cast<double>(hbg[1]);
@@ -549,11 +549,11 @@ int run_detect(Context& c, int w, int h, const float* img, const uint8_t* mask, 
                                             props + 2 * nkept);
     DGPU_LAUNCH("k_stamp_props");
     std::vector<int> hk(nkept);
-    DGPU_CUDA(cudaMemcpyAsync(hk.data(), kept, sizeof(int) * nkept, cudaMemcpyDeviceToHost, s));
-    DGPU_CUDA(cudaMemcpyAsync(res.flux.data(), props, sizeof(double) * nkept, cudaMemcpyDeviceToHost, s));
-    DGPU_CUDA(cudaMemcpyAsync(res.snr.data(), props + nkept, sizeof(double) * nkept, cudaMemcpyDeviceToHost, s));
-    DGPU_CUDA(cudaMemcpyAsync(res.fwhm.data(), props + 2 * nkept, sizeof(double) * nkept, cudaMemcpyDeviceToHost, s));
-    DGPU_CUDA(cudaStreamSynchronize(s));
+    read_back(c, hk.data(), kept, sizeof(int) * nkept);
+    read_back(c, res.flux.data(), props, sizeof(double) * nkept);
+    read_back(c, res.snr.data(), props + nkept, sizeof(double) * nkept);
+    read_back(c, res.fwhm.data(), props + 2 * nkept, sizeof(double) * nkept);
+    sync_reads(c);
     for (int i = 0; i < nkept; ++i) {
       res.x[i] = hk[i] % w;
       res.y[i] = hk[i] / w;
@@ -566,8 +566,8 @@ void run_background(Context& c, int64_t n, const float* img, const uint8_t* mask
   float* bg = static_cast<float*>(c.slot(kSlotFit14, 64));
   launch_background(c, n, img, mask, bg, kSlotFit10, kSlotFit11);
   float hbg[2];
-  DGPU_CUDA(cudaMemcpyAsync(hbg, bg, sizeof(hbg), cudaMemcpyDeviceToHost, c.stream));
-  DGPU_CUDA(cudaStreamSynchronize(c.stream));
+  read_back(c, hbg, bg, sizeof(hbg));
+  sync_reads(c);
   *median = static_cast<double>(hbg[0]);
   *sigma = 1.4826 * static_cast<double>(hbg[1]);
 }
@@ -599,15 +599,15 @@ void run_catalog_stamps(Context& c, int w, int h, const float* sci, const uint8_
   fr.assign(n, 0.0);
   float hb[2];
   if (n) {
-    DGPU_CUDA(cudaMemcpyAsync(ok.data(), dok, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
-    DGPU_CUDA(cudaMemcpyAsync(fs.data(), dfs, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
-    DGPU_CUDA(cudaMemcpyAsync(fr.data(), dfr, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    read_back(c, ok.data(), dok, sizeof(int) * n);
+    read_back(c, fs.data(), dfs, sizeof(double) * n);
+    read_back(c, fr.data(), dfr, sizeof(double) * n);
   }
-  DGPU_CUDA(cudaMemcpyAsync(hb, bgs, sizeof(float) * 2, cudaMemcpyDeviceToHost, s));
-  DGPU_CUDA(cudaStreamSynchronize(s));
+  read_back(c, hb, bgs, sizeof(float) * 2);
+  sync_reads(c);
   *med_sci = hb[0];
-  DGPU_CUDA(cudaMemcpyAsync(hb, bgr, sizeof(float) * 2, cudaMemcpyDeviceToHost, s));
-  DGPU_CUDA(cudaStreamSynchronize(s));
+  read_back(c, hb, bgr, sizeof(float) * 2);
+  sync_reads(c);
   *med_ref = hb[0];
 }
 

@@ -811,27 +811,26 @@ void launch_negate(cudaStream_t s, int64_t n, float* v) {
   DGPU_LAUNCH("k_negate");
 }
 
-// Device memory -> mapped pinned host memory by SM stores (16 bytes each, four
-// in flight per thread); both pointers 16-byte aligned, bytes a multiple of 16.
-__global__ void __launch_bounds__(256) k_copy_to_mapped(int64_t n16, const uint4* __restrict__ src, uint4* dst) {
-  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  for (; i + 3 * stride < n16; i += 4 * stride) {
-    const uint4 a = src[i], b = src[i + stride], c = src[i + 2 * stride], d = src[i + 3 * stride];
-    dst[i] = a;
-    dst[i + stride] = b;
-    dst[i + 2 * stride] = c;
-    dst[i + 3 * stride] = d;
+// Device memory -> the context's mapped pinned read-back area by SM stores
+// (16 bytes at a time when both ends are 16-byte aligned).
+__global__ void k_read_back(const unsigned char* __restrict__ src, unsigned char* dst, size_t n) {
+  const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+  size_t head = 0;
+  if (((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15u) == 0) {
+    const size_t n16 = n / 16;
+    for (size_t i = t; i < n16; i += stride)
+      reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
+    head = n16 * 16;
   }
-  for (; i < n16; i += stride) dst[i] = src[i];
+  for (size_t i = head + t; i < n; i += stride) dst[i] = src[i];
 }
 
-void launch_copy_to_mapped(cudaStream_t s, int64_t bytes, const void* src, void* dst) {
-  if (bytes <= 0) return;
-  // 64 CTAs keep enough stores in flight to fill the host link while leaving
-  // the other SMs to the frames still computing.
-  k_copy_to_mapped<<<64, 256, 0, s>>>(bytes / 16, static_cast<const uint4*>(src), static_cast<uint4*>(dst));
-  DGPU_LAUNCH("k_copy_to_mapped");
+void launch_read_back(cudaStream_t s, const void* src, void* dst, size_t bytes) {
+  if (bytes == 0) return;
+  const int blocks = static_cast<int>(std::min<size_t>((bytes + 4095) / 4096, 32));
+  k_read_back<<<blocks, 256, 0, s>>>(static_cast<const unsigned char*>(src), static_cast<unsigned char*>(dst), bytes);
+  DGPU_LAUNCH("k_read_back");
 }
 
 }  // namespace dgpu

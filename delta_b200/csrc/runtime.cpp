@@ -131,33 +131,53 @@ void keep_pool_memory(int device) {
   done[device] = true;
 }
 
-unsigned char* Context::host_staging(size_t bytes) {
-  if (host_stage_size >= bytes) return host_stage;
-  if (capturing()) fail(DGPU_ERR_RUNTIME, "staging growth while recording a graph");
-  // Growing: copies queued on the stream may still target the old buffer.
-  if (host_stage) {
-    DGPU_CUDA(cudaStreamSynchronize(stream));
-    DGPU_CUDA(cudaFreeHost(host_stage));
-    host_stage = nullptr;
-    host_stage_size = 0;
-  }
-  const size_t want = std::max<size_t>(bytes + bytes / 8 + 256, 1 << 16);
-  void* p = nullptr;
-  DGPU_CUDA(cudaHostAlloc(&p, want, cudaHostAllocDefault));
-  host_stage = static_cast<unsigned char*>(p);
-  host_stage_size = want;
-  return host_stage;
-}
-
 void reset_status(Context& c) { DGPU_CUDA(cudaMemsetAsync(c.d_status, 0, sizeof(unsigned), c.stream)); }
 
 void check_status(Context& c) {
   if (capturing()) fail(DGPU_ERR_RUNTIME, "a synchronising check while recording a graph");
   unsigned st = 0;
-  DGPU_CUDA(cudaMemcpyAsync(&st, c.d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, c.stream));
-  DGPU_CUDA(cudaStreamSynchronize(c.stream));
+  read_back(c, &st, c.d_status, sizeof(unsigned));
+  sync_reads(c);
   if (st & kStatusLoopLimit) fail(DGPU_ERR_LIMIT, "a device loop hit its iteration cap");
   if (st & kStatusBounds) fail(DGPU_ERR_LIMIT, "a device bounds check rejected an access");
+}
+
+constexpr size_t kReadBackBytes = size_t(1) << 20;
+
+void read_back(Context& c, void* host, const void* dev, size_t bytes) {
+  if (bytes == 0) return;
+  if (!capturing() && c.rb_host == nullptr) {
+    void* p = nullptr;
+    DGPU_CUDA(cudaHostAlloc(&p, kReadBackBytes, cudaHostAllocMapped));
+    void* d = nullptr;
+    if (cudaHostGetDevicePointer(&d, p, 0) != cudaSuccess || d == nullptr) {
+      cudaFreeHost(p);
+      fail(DGPU_ERR_CUDA, "read-back area: no device address for mapped pinned memory");
+    }
+    c.rb_host = static_cast<unsigned char*>(p);
+    c.rb_dev = static_cast<unsigned char*>(d);
+    c.rb_used = 0;
+  }
+  const size_t off = (c.rb_used + 15) & ~size_t(15);
+  if (capturing() || off + bytes > kReadBackBytes) {
+    DGPU_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, c.stream));
+    return;
+  }
+  launch_read_back(c.stream, dev, c.rb_dev + off, bytes);
+  c.rb_items.push_back({host, off, bytes});
+  c.rb_used = off + bytes;
+}
+
+void sync_reads(Context& c) {
+  DGPU_CUDA(cudaStreamSynchronize(c.stream));
+  for (const auto& it : c.rb_items) std::memcpy(it.host, c.rb_host + it.off, it.bytes);
+  c.rb_items.clear();
+  c.rb_used = 0;
+}
+
+void drop_reads(Context& c) {
+  c.rb_items.clear();
+  c.rb_used = 0;
 }
 
 static std::mutex g_smem_mu;

@@ -179,15 +179,16 @@ int dgpu_scale(dgpu_context* ctx, int mem, float* data, int64_t n, double scale)
 int dgpu_z2_median(dgpu_context* ctx, int mem, int64_t n, const float* difference, const float* variance,
                    const uint8_t* mask, double* median, int64_t* count);
 int dgpu_fill(dgpu_context* ctx, int mem, float* data, int64_t n, double value);
-/* Copy of `bytes` from device memory to pinned host memory by SM stores
- * through the destination's mapped address, ordered on the context's stream;
- * returns once it has completed. No counterpart in the reference, which has no
- * device: it serves the batch layer. The device's device-to-host copies share
- * one queue in submission order, so a frame's 200 MB result download queued
- * there would hold every read-back of the frames still computing for its whole
- * duration. Unaligned or partial tails go by an ordinary copy. Errors:
- * DGPU_ERR_INVALID when host_dst is not mapped pinned host memory or
- * device_src is not device memory. */
+/* Copy of `bytes` from device memory to pinned host memory, ordered on the
+ * context's stream through the copy engine (asynchronous: synchronize that
+ * stream before reading host_dst). No counterpart in the reference, which has
+ * no device: it serves the batch layer. Every stream's device-to-host
+ * copy-engine transfers share one queue in submission order, so the library
+ * keeps its own small read-backs (status words, counts, stamp lists, theta,
+ * catalog rows) out of that queue: they go by SM stores into a mapped pinned
+ * area of the context, and a frame's 200 MB download queued here does not
+ * hold the frames still computing. Errors: DGPU_ERR_INVALID when host_dst is
+ * not pinned host memory or device_src is not device memory. */
 int dgpu_copy_to_host(dgpu_context* ctx, void* host_dst, const void* device_src, int64_t bytes);
 /* ---- FITS image layers ------------------------------------------------------------ */
 /* read_fits, src/bindings.cpp:128-145 -> delta::io::read_image, src/io.cpp:79-130.

@@ -262,10 +262,10 @@ def test_apply_batch_matches_one_at_a_time():
         np.testing.assert_array_equal(r.source_catalog, one.source_catalog)
 
 
-def test_copy_to_host_by_sm_stores():
-    """dgpu_copy_to_host writes device bytes into mapped pinned host memory
-    (aligned body by SM stores, a ragged tail by an ordinary copy) and rejects
-    pageable destinations."""
+def test_copy_to_host_orders_on_the_stream():
+    """dgpu_copy_to_host copies device bytes into pinned host memory after the
+    stream's queued work (ragged sizes included) and rejects pageable
+    destinations."""
     import ctypes
 
     import torch
@@ -273,8 +273,9 @@ def test_copy_to_host_by_sm_stores():
     from delta_b200 import _device, _lib
 
     ctx = _device._ctx_on_torch_stream()
-    for n in (0, 16, 1000, 4 * 1024 * 1024 + 3):
+    for n in (0, 16, 1000, 4 * 1024 * 1024 + 3, 3 * (4 << 20) + 5):
         src = torch.randint(0, 256, (n,), dtype=torch.uint8, device="cuda")
+        src.add_(1)  # queued on the stream just before the copy, which must see it
         dst = torch.zeros(n, dtype=torch.uint8, pin_memory=True)
         _lib.check(_lib.lib().dgpu_copy_to_host(ctx.handle, ctypes.c_void_p(dst.data_ptr()),
                                                 ctypes.c_void_p(src.data_ptr()), ctypes.c_int64(n)), ctx.handle)
