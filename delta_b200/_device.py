@@ -47,17 +47,34 @@ class DeviceFrame:
     science_mask: object = None
     reference_mask: object = None
 
+    # Upload of the variance layers still in flight (serialized uploads only):
+    # wait_variances() orders the current stream after it.
+    variances_ready: object = None
+
     @property
     def shape(self):
         return tuple(self.science.shape)
 
+    def wait_variances(self) -> None:
+        if self.variances_ready is not None:
+            torch.cuda.current_stream().wait_event(self.variances_ready)
+
+    def finish_upload(self) -> None:
+        """Block until every layer has arrived (the host arrays may then go)."""
+        if self.variances_ready is not None:
+            self.variances_ready.synchronize()
+
     @classmethod
     def from_numpy(cls, sci, ref, svar=None, rvar=None, smask=None, rmask=None, device=None, non_blocking=False,
                    serialize=False):
-        """Upload the layers. With serialize, frames uploading from several host
-        threads take turns (each upload completes before the next starts), so
-        the first frame of a batch can start computing while the others are
-        still in flight instead of every frame waiting for all uploads."""
+        """Upload the layers. With serialize, the copies of frames uploading from
+        several host threads go in call order through one upload stream of the
+        device, so each frame's layers arrive at the full host-link rate instead
+        of every frame's upload sharing the link with the others. The current
+        stream then waits for the science, reference and mask layers (stamp
+        selection needs no more), and wait_variances() for the rest; the host
+        arrays must stay unchanged until finish_upload() or the frame's work has
+        run."""
         dev = device or torch.device("cuda", torch.cuda.current_device())
 
         def up(a, dt):
@@ -66,20 +83,39 @@ class DeviceFrame:
             t = torch.from_numpy(np.ascontiguousarray(a, dtype=dt))
             return t.to(dev, non_blocking=non_blocking)
 
-        def all_layers():
+        if not serialize:
             return cls(up(sci, np.float32), up(ref, np.float32), up(svar, np.float32), up(rvar, np.float32),
                        up(smask, np.uint8), up(rmask, np.uint8))
-
-        if not serialize:
-            return all_layers()
-        with _UPLOAD_LOCK:
-            frame = all_layers()
-            torch.cuda.current_stream().synchronize()
-        return frame
+        cur = torch.cuda.current_stream(dev)
+        up_s = _upload_stream(dev)
+        with _UPLOAD_LOCK:  # one frame's copies stay together on the shared stream
+            up_s.wait_stream(cur)
+            with torch.cuda.stream(up_s):
+                s_, r_, sm_, rm_ = up(sci, np.float32), up(ref, np.float32), up(smask, np.uint8), up(rmask, np.uint8)
+                first = torch.cuda.Event()
+                first.record(up_s)
+                sv_, rv_ = up(svar, np.float32), up(rvar, np.float32)
+                rest = torch.cuda.Event()
+                rest.record(up_s)
+        cur.wait_event(first)
+        for t in (s_, r_, sv_, rv_, sm_, rm_):
+            if t is not None:  # the frame's work runs on cur: no reuse of the memory before it has
+                t.record_stream(cur)
+        return cls(s_, r_, sv_, rv_, sm_, rm_, variances_ready=rest)
 
 
 _CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy: handle 0 would select the context's own stream
 _UPLOAD_LOCK = threading.Lock()
+_XFER_STREAMS: dict = {}
+
+
+def _upload_stream(dev):
+    """The device's one stream for serialized frame uploads."""
+    with _UPLOAD_LOCK:
+        s = _XFER_STREAMS.get(dev.index)
+        if s is None:
+            s = _XFER_STREAMS[dev.index] = torch.cuda.Stream(device=dev)
+        return s
 
 
 def _ctx_on_torch_stream():
@@ -320,6 +356,7 @@ def run(sub, frame: DeviceFrame, catalog=None, direction=None) -> dict:
         nkx = int(np.clip(round((w - 1) / sub.spatial_scale) + 1, 3, sub.n_knots))
         nky = int(np.clip(round((h - 1) / sub.spatial_scale) + 1, 3, sub.n_knots))
     knots = _core.grid_knots(0.0, 0.0, w - 1.0, h - 1.0, nkx, nky)
+    frame.wait_variances()
     fit = fit_kernel(target, conv, tvar, cvar, tmask, cmask, knots, sel["x"], sel["y"], sub, beta)
     logger.info("kernel fit: lambda={:.3g}, eff.dof={:.1f}, reduced chi2={:.3f} ({} stamps used, {} rejected of {}, "
                 "{} px)", fit["lambda"], fit["effective_dof"], fit["reduced_chi2"], fit["n_stamps_used"],
@@ -336,6 +373,7 @@ def run(sub, frame: DeviceFrame, catalog=None, direction=None) -> dict:
 
 def apply_solution(sub, solution, frame: DeviceFrame) -> dict:
     """Subtractor.apply on device-resident layers: a frozen solution, no re-fit."""
+    frame.wait_variances()
     if solution.direction == "science":
         return apply(sub, solution, frame.reference, frame.science, frame.reference_var, frame.science_var,
                      frame.reference_mask, frame.science_mask, -1.0, solution.stamp_x, solution.stamp_y)

@@ -396,10 +396,14 @@ class Subtractor:
             rvar = synth_variance(ref, gain, read_noise)
         logger.info("fitting {} x {} frame (device resident)", sci.shape[1], sci.shape[0])
         frame = _device.DeviceFrame.from_numpy(sci, ref, svar, rvar, smask, rmask, non_blocking=True, serialize=True)
-        if solution is None:
-            out = _device.run(self, frame, catalog, direction)
-        else:
-            out = _device.apply_solution(self, solution, frame)
+        try:
+            if solution is None:
+                out = _device.run(self, frame, catalog, direction)
+            else:
+                out = _device.apply_solution(self, solution, frame)
+        except BaseException:
+            frame.finish_upload()  # the host layers must outlive their copies
+            raise
         host = _device.download(out)
         return DiffResult(difference=host["difference"], variance=host["variance"], mask=host["mask"],
                           score=host["score"], solution=out["solution"], psf=out["psf"],
