@@ -11,21 +11,42 @@
 
 namespace dgpu {
 
-__global__ void k_sample_keys(int64_t n, int64_t step, const float* __restrict__ v, const uint8_t* __restrict__ mask,
-                              uint32_t* __restrict__ keys, RadixSelect* st) {
+// One reservation per block and sweep (a block-wide count of its finite,
+// unmasked samples, then one atomicAdd): a reservation per warp put up to
+// 8192 atomics on the one counter. The keys' order within the sample is free:
+// only their multiset decides the median.
+__global__ void __launch_bounds__(256) k_sample_keys(int64_t n, int64_t step, const float* __restrict__ v,
+                                                     const uint8_t* __restrict__ mask, uint32_t* __restrict__ keys,
+                                                     RadixSelect* st) {
+  __shared__ unsigned warp_n[8];
+  __shared__ unsigned block_base;
   const int64_t ns = (n + step - 1) / step;
-  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < ns;
-       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t i = j * step;
-    const float x = v[i];
-    const bool ok = isfinite(x) && (mask == nullptr || mask[i] == 0);
-    const unsigned bal = __ballot_sync(__activemask(), ok);
-    if (!bal) continue;
-    const int lane = threadIdx.x & 31, leader = __ffs(bal) - 1;
-    unsigned base = 0;
-    if (lane == leader) base = atomicAdd(&st->count, __popc(bal));
-    base = __shfl_sync(__activemask(), base, leader);
-    if (ok) keys[base + __popc(bal & ((1u << lane) - 1))] = float_key(x);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int64_t j0 = static_cast<int64_t>(blockIdx.x) * blockDim.x; j0 < ns;
+       j0 += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t j = j0 + threadIdx.x;
+    bool ok = false;
+    float x = 0.0f;
+    if (j < ns) {
+      const int64_t i = j * step;
+      x = v[i];
+      ok = isfinite(x) && (mask == nullptr || mask[i] == 0);
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, ok);
+    if (lane == 0) warp_n[warp] = __popc(bal);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned tot = 0;
+      for (int w = 0; w < 8; ++w) {
+        const unsigned c = warp_n[w];
+        warp_n[w] = tot;
+        tot += c;
+      }
+      block_base = tot ? atomicAdd(&st->count, tot) : 0u;
+    }
+    __syncthreads();
+    if (ok) keys[block_base + warp_n[warp] + __popc(bal & ((1u << lane) - 1))] = float_key(x);
+    __syncthreads();  // warp_n and block_base are rewritten by the next sweep
   }
 }
 
@@ -41,9 +62,20 @@ __global__ void k_select_hist(const uint32_t* __restrict__ keys, RadixSelect* st
   __syncthreads();
   const unsigned count = st->count, prefix = st->prefix;
   const unsigned himask = shift >= 24 ? 0u : (0xffffffffu << (shift + 8));
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    const uint32_t k = keys[i];
-    if ((k & himask) == (prefix & himask)) atomicAdd(&hist[(k >> shift) & 0xffu], 1u);
+  // Warp-aggregated: the lanes holding the same digit add once through their
+  // lowest lane (the top digits of a sky image's samples are nearly all equal,
+  // and per-lane shared atomics on one bin serialise).
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned span = gridDim.x * blockDim.x;
+  for (unsigned i0 = blockIdx.x * blockDim.x; i0 < count; i0 += span) {
+    const unsigned i = i0 + threadIdx.x;
+    unsigned tag = 256u + lane;  // unmatched: a tag of its own
+    if (i < count) {
+      const uint32_t k = keys[i];
+      if ((k & himask) == (prefix & himask)) tag = (k >> shift) & 0xffu;
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, tag);  // the loop bound is uniform per block
+    if (tag < 256u && lane == static_cast<unsigned>(__ffs(peers) - 1)) atomicAdd(&hist[tag], __popc(peers));
   }
   __syncthreads();
   for (int i = threadIdx.x; i < 256; i += blockDim.x)
