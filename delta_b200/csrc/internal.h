@@ -127,6 +127,7 @@ struct Context {
   // still to be scattered to their destinations at the next sync_reads.
   struct ReadBack {
     void* host;
+    const void* dev;  // copied into the area at the next sync_reads
     size_t off, bytes;
   };
   unsigned char* rb_host = nullptr;
@@ -215,19 +216,29 @@ int autotune(cudaStream_t s, const std::string& key, const std::vector<int>& can
 void reset_status(Context& c);
 void check_status(Context& c);  // synchronises the stream
 
-// Device -> host read-backs of the host logic. read_back queues a copy of
-// `bytes` from device memory, ordered on the context's stream; `host` holds
-// the bytes only after the next sync_reads, which synchronises the stream and
-// scatters them (so `host` must stay valid until then). Up to 1 MiB per sync
-// goes by SM stores into the context's mapped pinned area: every stream's
-// device-to-host copy-engine transfers share one queue in submission order,
-// and a read-back queued there behind another frame's 200 MB download waits
-// for all of it. Larger reads, and reads while a graph is recorded, use that
-// queue. Entry points drop read-backs that an error left unscattered.
+// Device -> host read-backs of the host logic. read_back(c, host, dev, bytes)
+// names `bytes` of device memory to bring back; `host` holds them only after
+// the next sync_reads, which copies every named range (as it is once the work
+// queued before the sync has run, so no work queued between read_back and
+// sync_reads may change a named range), synchronises the stream and scatters
+// the bytes (so `host` must stay valid until then). Up to 1 MiB per sync goes
+// by SM stores into the context's mapped pinned area, all ranges in one
+// launch: every stream's device-to-host copy-engine transfers share one queue
+// in submission order, and a read-back queued there behind another frame's
+// 200 MB download waits for all of it. Larger reads, and reads while a graph
+// is recorded, take that queue at once. Entry points drop read-backs that an
+// error left unscattered.
 void read_back(Context& c, void* host, const void* dev, size_t bytes);
 void sync_reads(Context& c);
 void drop_reads(Context& c);
-void launch_read_back(cudaStream_t s, const void* src, void* dst, size_t bytes);
+constexpr int kReadBackList = 16;  // ranges per gather launch
+struct ReadBackList {
+  const unsigned char* src[kReadBackList];
+  unsigned char* dst[kReadBackList];
+  unsigned long long bytes[kReadBackList];
+  int n;
+};
+void launch_read_back(cudaStream_t s, const ReadBackList& l);
 
 // Resolve the pending stage events into `timing` (synchronises the stream).
 void resolve_timing(Context& c);

@@ -811,9 +811,15 @@ void launch_negate(cudaStream_t s, int64_t n, float* v) {
   DGPU_LAUNCH("k_negate");
 }
 
-// Device memory -> the context's mapped pinned read-back area by SM stores
-// (16 bytes at a time when both ends are 16-byte aligned).
-__global__ void k_read_back(const unsigned char* __restrict__ src, unsigned char* dst, size_t n) {
+// Device memory -> the context's mapped pinned read-back area by SM stores:
+// range blockIdx.y of the list (16 bytes at a time when both ends are 16-byte
+// aligned).
+__global__ void k_read_back(ReadBackList l) {
+  const int it = blockIdx.y;
+  if (it >= l.n) return;
+  const unsigned char* __restrict__ src = l.src[it];
+  unsigned char* dst = l.dst[it];
+  const size_t n = l.bytes[it];
   const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
   size_t head = 0;
@@ -826,10 +832,12 @@ __global__ void k_read_back(const unsigned char* __restrict__ src, unsigned char
   for (size_t i = head + t; i < n; i += stride) dst[i] = src[i];
 }
 
-void launch_read_back(cudaStream_t s, const void* src, void* dst, size_t bytes) {
-  if (bytes == 0) return;
-  const int blocks = static_cast<int>(std::min<size_t>((bytes + 4095) / 4096, 32));
-  k_read_back<<<blocks, 256, 0, s>>>(static_cast<const unsigned char*>(src), static_cast<unsigned char*>(dst), bytes);
+void launch_read_back(cudaStream_t s, const ReadBackList& l) {
+  if (l.n <= 0) return;
+  unsigned long long most = 0;
+  for (int i = 0; i < l.n; ++i) most = std::max(most, l.bytes[i]);
+  const unsigned bx = static_cast<unsigned>(std::min<unsigned long long>((most + 4095) / 4096, 32));
+  k_read_back<<<dim3(std::max(bx, 1u), static_cast<unsigned>(l.n)), 256, 0, s>>>(l);
   DGPU_LAUNCH("k_read_back");
 }
 

@@ -64,11 +64,14 @@ cudaError_t h2d_async(void* dst, const void* src, size_t bytes, cudaStream_t s) 
 // after, so growth neither synchronises the stream nor the device (a plain
 // cudaFree waits for every stream of the device). The pool keeps freed blocks
 // for reuse (release threshold raised once per device in dgpu_create).
+static void flush_reads(Context& c);
+
 void* Context::slot(Slot s, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (slot_size[s] >= bytes) return slot_ptr[s];
   if (capturing()) fail(DGPU_ERR_RUNTIME, "workspace growth while recording a graph");
   if (slot_ptr[s]) {
+    flush_reads(*this);  // a named read-back range may lie in the buffer freed here
     DGPU_CUDA(cudaFreeAsync(slot_ptr[s], stream));
     slot_ptr[s] = nullptr;
     slot_size[s] = 0;
@@ -163,12 +166,29 @@ void read_back(Context& c, void* host, const void* dev, size_t bytes) {
     DGPU_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, c.stream));
     return;
   }
-  launch_read_back(c.stream, dev, c.rb_dev + off, bytes);
-  c.rb_items.push_back({host, off, bytes});
+  c.rb_items.push_back({host, dev, off, bytes});
   c.rb_used = off + bytes;
 }
 
+// Queue the copies of the named ranges not yet copied (one launch per 16).
+static void flush_reads(Context& c) {
+  ReadBackList l{};
+  for (auto& it : c.rb_items) {
+    if (!it.dev) continue;
+    l.src[l.n] = static_cast<const unsigned char*>(it.dev);
+    l.dst[l.n] = c.rb_dev + it.off;
+    l.bytes[l.n] = it.bytes;
+    it.dev = nullptr;
+    if (++l.n == kReadBackList) {
+      launch_read_back(c.stream, l);
+      l.n = 0;
+    }
+  }
+  if (l.n) launch_read_back(c.stream, l);
+}
+
 void sync_reads(Context& c) {
+  flush_reads(c);
   DGPU_CUDA(cudaStreamSynchronize(c.stream));
   for (const auto& it : c.rb_items) std::memcpy(it.host, c.rb_host + it.off, it.bytes);
   c.rb_items.clear();
