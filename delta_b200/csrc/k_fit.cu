@@ -854,10 +854,10 @@ k_reweight(StampGeom g, TpsDev t, const int* __restrict__ stamp_x, const int* __
     }
     // Off-frame, masked, non-positive and non-finite samples contribute nothing
     // (src/fit.cpp:38-59 skips them): store 0, which leaves the FP64 sum unchanged.
-    for (int i = threadIdx.x; i < side * side; i += blockDim.x) {
+    for (int i = threadIdx.x; i < side * side + 4; i += blockDim.x) {
       const int yy = wy0 + i / side, xx = wx0 + i % side;
       float v = 0.0f;
-      if (yy >= 0 && yy < g.h && xx >= 0 && xx < g.w) {
+      if (i < side * side && yy >= 0 && yy < g.h && xx >= 0 && xx < g.w) {
         const size_t idx = static_cast<size_t>(yy) * g.w + xx;
         const float x = vr[idx];
         if (!(rm && rm[idx] != 0) && x > 0.0f && isfinite(x)) v = x;
@@ -872,43 +872,48 @@ k_reweight(StampGeom g, TpsDev t, const int* __restrict__ stamp_x, const int* __
     }
     __syncthreads();
   }
-  // Four rows per thread as independent FMA chains, each in (dv, du) order.
-  constexpr int kRows = 4;
-  for (int i0 = threadIdx.x; i0 < g.SS; i0 += kRows * blockDim.x) {
-    size_t row[kRows];
-    bool live[kRows];
-    int base[kRows];
-    double acc[kRows];
-#pragma unroll
-    for (int q = 0; q < kRows; ++q) {
-      const int i = i0 + q * blockDim.x;
-      row[q] = static_cast<size_t>(s) * g.SS + i;
-      live[q] = i < g.SS && R.valid[row[q]];
-      // window index of (x - du, y - dv) at du = dv = 0 (the window centre for
-      // rows that are not live, so every tap index stays inside the window)
-      base[q] = live[q] ? (R.py[row[q]] - wy0) * side + (R.px[row[q]] - wx0) : r * side + r;
-      acc[q] = 0.0;
+  if (!g.have_cvar) {
+    for (int i = threadIdx.x; i < g.SS; i += blockDim.x) {
+      const size_t row = static_cast<size_t>(s) * g.SS + i;
+      if (R.valid[row] && R.vt[row] > 0.0) R.w[row] = 1.0 / R.vt[row];
     }
-    if (g.have_cvar) {
-      for (int dv = -r; dv <= r; ++dv) {
-        const double* krow = k2 + (dv + r) * ks;
-        const int off = -dv * side;
-        for (int du = -r; du <= r; ++du) {
-          const double c = krow[du + r];
-#pragma unroll
-          for (int q = 0; q < kRows; ++q) acc[q] = fma(c, win[base[q] + off - du], acc[q]);
+    return;
+  }
+  // Four horizontally adjacent rows of the stamp per thread, each an FMA
+  // chain in (dv, du) order. For a fixed dv the four share one sliding run of
+  // window values: one shared load per du step feeds four FMAs. Row (ly, lx)
+  // of the stamp sits at window offset (ly + r) * side + lx + r.
+  const int S = g.S, strips = (S + 3) / 4;
+  for (int t = threadIdx.x; t < strips * S; t += blockDim.x) {
+    const int ly = t / strips, lx0 = 4 * (t - ly * strips);
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int dv = -r; dv <= r; ++dv) {
+      const double* krow = k2 + (dv + r) * ks;
+      // window row of (y - dv); column of output q at du: lx0 + q + r - du
+      const double* wrow = win + (ly + r - dv) * side + lx0;
+      double w0 = wrow[2 * r], w1 = wrow[2 * r + 1], w2 = wrow[2 * r + 2], w3 = wrow[2 * r + 3];
+      for (int du = -r; du <= r; ++du) {
+        const double c = krow[du + r];
+        acc[0] = fma(c, w0, acc[0]);
+        acc[1] = fma(c, w1, acc[1]);
+        acc[2] = fma(c, w2, acc[2]);
+        acc[3] = fma(c, w3, acc[3]);
+        if (du < r) {
+          w3 = w2;
+          w2 = w1;
+          w1 = w0;
+          w0 = wrow[r - du - 1];
         }
       }
     }
 #pragma unroll
-    for (int q = 0; q < kRows; ++q) {
-      if (!live[q]) continue;
-      if (g.have_cvar) {
-        const double rv = R.vt[row[q]] + acc[q];
-        if (rv > 0.0) R.w[row[q]] = 1.0 / rv;
-      } else {
-        if (R.vt[row[q]] > 0.0) R.w[row[q]] = 1.0 / R.vt[row[q]];
-      }
+    for (int q = 0; q < 4; ++q) {
+      const int lx = lx0 + q;
+      if (lx >= S) break;
+      const size_t row = static_cast<size_t>(s) * g.SS + static_cast<size_t>(ly) * S + lx;
+      if (!R.valid[row]) continue;
+      const double rv = R.vt[row] + acc[q];
+      if (rv > 0.0) R.w[row] = 1.0 / rv;
     }
   }
 }
@@ -918,7 +923,9 @@ void launch_reweight(cudaStream_t st, const StampGeom& g, int n_stamps, const Tp
                      const double* theta, const float* phi, const float* vr, const uint8_t* rm) {
   if (n_stamps == 0) return;
   const size_t side = static_cast<size_t>(g.S) + 2 * g.r;
-  const size_t smem = sizeof(double) * (static_cast<size_t>(g.ks) * g.ks + side * side);
+  // (+4: the last window row's sliding runs of the four-row strips read up to
+  // three values past it, for outputs beyond the stamp that are never stored)
+  const size_t smem = sizeof(double) * (static_cast<size_t>(g.ks) * g.ks + side * side + 4);
   if (smem > 200 * 1024) fail(DGPU_ERR_INVALID, "fit_kernel: stamp plus kernel footprint too large for the reweight");
   ensure_dynamic_smem(reinterpret_cast<const void*>(k_reweight), smem);
   k_reweight<<<n_stamps, 256, smem, st>>>(g, t, sx, sy, R, accepted, cnt, theta, phi, vr, rm);

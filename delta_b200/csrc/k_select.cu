@@ -62,20 +62,9 @@ __global__ void k_select_hist(const uint32_t* __restrict__ keys, RadixSelect* st
   __syncthreads();
   const unsigned count = st->count, prefix = st->prefix;
   const unsigned himask = shift >= 24 ? 0u : (0xffffffffu << (shift + 8));
-  // Warp-aggregated: the lanes holding the same digit add once through their
-  // lowest lane (the top digits of a sky image's samples are nearly all equal,
-  // and per-lane shared atomics on one bin serialise).
-  const unsigned lane = threadIdx.x & 31u;
-  const unsigned span = gridDim.x * blockDim.x;
-  for (unsigned i0 = blockIdx.x * blockDim.x; i0 < count; i0 += span) {
-    const unsigned i = i0 + threadIdx.x;
-    unsigned tag = 256u + lane;  // unmatched: a tag of its own
-    if (i < count) {
-      const uint32_t k = keys[i];
-      if ((k & himask) == (prefix & himask)) tag = (k >> shift) & 0xffu;
-    }
-    const unsigned peers = __match_any_sync(0xffffffffu, tag);  // the loop bound is uniform per block
-    if (tag < 256u && lane == static_cast<unsigned>(__ffs(peers) - 1)) atomicAdd(&hist[tag], __popc(peers));
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const uint32_t k = keys[i];
+    if ((k & himask) == (prefix & himask)) atomicAdd(&hist[(k >> shift) & 0xffu], 1u);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < 256; i += blockDim.x)
