@@ -10,6 +10,7 @@ reference's own data flow.
 from __future__ import annotations
 
 import ctypes
+import os
 import threading
 from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
@@ -86,15 +87,24 @@ class DeviceFrame:
         if not serialize:
             return cls(up(sci, np.float32), up(ref, np.float32), up(svar, np.float32), up(rvar, np.float32),
                        up(smask, np.uint8), up(rmask, np.uint8))
+        # Pageable layers are first copied into pinned buffers by several host
+        # threads (outside the lock, so while another frame's layers cross the
+        # link): the driver's own pageable path stages them through one thread.
+        host = [_pinned_layer(a, dt) for a, dt in ((sci, np.float32), (ref, np.float32), (smask, np.uint8),
+                                                   (rmask, np.uint8), (svar, np.float32), (rvar, np.float32))]
+
+        def send(t):
+            return None if t is None else t.to(dev, non_blocking=True)
+
         cur = torch.cuda.current_stream(dev)
         up_s = _upload_stream(dev)
         with _UPLOAD_LOCK:  # one frame's copies stay together on the shared stream
             up_s.wait_stream(cur)
             with torch.cuda.stream(up_s):
-                s_, r_, sm_, rm_ = up(sci, np.float32), up(ref, np.float32), up(smask, np.uint8), up(rmask, np.uint8)
+                s_, r_, sm_, rm_ = (send(t) for t in host[:4])
                 first = torch.cuda.Event()
                 first.record(up_s)
-                sv_, rv_ = up(svar, np.float32), up(rvar, np.float32)
+                sv_, rv_ = (send(t) for t in host[4:])
                 rest = torch.cuda.Event()
                 rest.record(up_s)
         cur.wait_event(first)
@@ -107,6 +117,39 @@ class DeviceFrame:
 _CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy: handle 0 would select the context's own stream
 _UPLOAD_LOCK = threading.Lock()
 _XFER_STREAMS: dict = {}
+_STAGE_CHUNK = 8 << 20
+_STAGE_MIN = 1 << 20
+_stage_pool: list = []
+_stage_lock = threading.Lock()
+
+
+def _stage_threads() -> ThreadPoolExecutor:
+    with _stage_lock:
+        if not _stage_pool:
+            n = max(2, min(8, (os.cpu_count() or 2) // 2))
+            _stage_pool.append(ThreadPoolExecutor(max_workers=n, thread_name_prefix="delta-b200-stage"))
+        return _stage_pool[0]
+
+
+def _pinned_layer(a, dt):
+    """A CPU tensor of layer `a` (as dtype dt) in pinned memory: `a` itself when
+    it already is (or is small), else a pinned copy made in 8 MB pieces by the
+    staging threads. The pinned copy comes from torch's caching host
+    allocator, which reuses it only after the transfers queued from it have
+    run."""
+    if a is None:
+        return None
+    h = np.ascontiguousarray(a, dtype=dt)
+    t = torch.from_numpy(h)
+    if h.nbytes < _STAGE_MIN or t.is_pinned():
+        return t
+    buf = torch.empty(h.shape, dtype=t.dtype, pin_memory=True)
+    dst, src = buf.numpy().reshape(-1), h.reshape(-1)
+    step = max(1, _STAGE_CHUNK // h.itemsize)
+    futs = [_stage_threads().submit(np.copyto, dst[o:o + step], src[o:o + step]) for o in range(0, src.size, step)]
+    for f in futs:
+        f.result()
+    return buf
 
 
 def _upload_stream(dev):
