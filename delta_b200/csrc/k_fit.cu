@@ -533,7 +533,7 @@ __device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
 }
 
 template <int KT>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, KT == 2 ? 2 : 1)
 k_rhs_mma(int64_t N, int nc, int k, int SS, FitRows R, const uint8_t* __restrict__ accepted,
           const double* __restrict__ theta, int64_t blocks_per_cta, double* __restrict__ rpart,
           double* __restrict__ ypart, long long* __restrict__ npart) {
@@ -736,9 +736,11 @@ void launch_rhs(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, 
   int nsplit;
   int64_t rps = 0, bpc = 0;
   if (mma) {
-    // 16 row blocks of 32 per CTA: two per warp.
+    // Row blocks of 32 spread over one wave of CTAs (two per SM with the
+    // 16-wide design, one with the 32-wide), at least one block per warp.
     const int64_t nblk = (N + 31) / 32;
-    bpc = 16;
+    const int64_t wave = 148 * (k <= 16 ? 2 : 1);
+    bpc = std::max<int64_t>(8, (nblk + wave - 1) / wave);
     nsplit = static_cast<int>(std::max<int64_t>(1, (nblk + bpc - 1) / bpc));
   } else {
     rps = std::max<int64_t>(kRhsRows * 2, (N + 148 * 2 - 1) / (148 * 2));
