@@ -703,76 +703,150 @@ void launch_solve_batch(Context& c, const SolveBatch& b) {
 
 // out = A_s^{-1} v = L^-T (L^-1 v) from system s's factor tiles, one CTA.
 // The tiles are first pulled into L2 (one bulk prefetch per tile; streaming
-// kernels that ran since the solve may have evicted them). Forward over the
-// column tiles: y_i = Dinv_i y_i, then y_p -= L_pi y_i for the rows below (a
-// thread per row); backward: theta_i = Dinv_i^T y_i, then y_q -= L_iq^T
-// theta_i (a thread per column).
+// kernels that ran since the solve may have evicted them) and, up to 24 tile
+// columns, every Dinv tile into shared memory. Forward over the column tiles:
+// y_i = Dinv_i y_i (warp 0), then y_p -= L_pi y_i for the rows below (a thread
+// per row); backward: theta_i = Dinv_i^T y_i, then y_q -= L_iq^T theta_i (a
+// thread per column). Each thread's first row (column) of the next step is
+// loaded into registers while the current step finishes, so the L2 latency
+// overlaps the step's barriers and the diagonal solve.
 constexpr int kAiThreads = 512;
+constexpr int kDs = kT * (kT + 1);  // one Dinv tile in shared memory, padded rows
+constexpr int kAiPreloadTiles = 24;
+
+int apply_inverse_smem(int nb) { return static_cast<int>(sizeof(double)) * kDs * (nb <= kAiPreloadTiles ? nb : 1); }
+
+__device__ __forceinline__ void ai_row(const double* __restrict__ A, int tile, int rr, double (&v)[kT]) {
+  const double2* src = reinterpret_cast<const double2*>(A + static_cast<size_t>(tile) * kTS + rr * kLd);
+#pragma unroll
+  for (int c = 0; c < kT / 2; ++c) {
+    const double2 t = __ldg(src + c);
+    v[2 * c] = t.x;
+    v[2 * c + 1] = t.y;
+  }
+}
+
+__device__ __forceinline__ void ai_col(const double* __restrict__ A, int tile, int cc, double (&v)[kT]) {
+  const double* src = A + static_cast<size_t>(tile) * kTS + cc;
+#pragma unroll
+  for (int r = 0; r < kT; ++r) v[r] = __ldg(src + r * kLd);
+}
 
 __global__ void __launch_bounds__(kAiThreads) k_apply_inverse(const double* __restrict__ A, const double* __restrict__ Dv,
                                                                int P, int Pp, const double* __restrict__ vin,
                                                                double* __restrict__ out) {
+  extern __shared__ double dsm[];  // Dinv tiles (all, or the current one)
   __shared__ double y[1024];
-  __shared__ double dt[kT * (kT + 1)];
   const int tid = threadIdx.x, warp = tid >> 5, ln = tid & 31;
   const int nb = Pp / kT, na = nb * (nb + 1) / 2;
+  const bool all = nb <= kAiPreloadTiles;
   for (int u = tid; u < na + nb; u += blockDim.x) {
     const double* tile = u < na ? A + static_cast<size_t>(u) * kTS : Dv + static_cast<size_t>(u - na) * kTS;
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(tile), "r"(static_cast<unsigned>(kTS * 8)) : "memory");
   }
   for (int q = tid; q < Pp; q += blockDim.x) y[q] = q < P ? vin[q] : 0.0;
+  if (all)
+    for (int e = tid; e < nb * kT * kT; e += blockDim.x) {
+      const int t = e / (kT * kT), rc = e - t * (kT * kT);
+      dsm[t * kDs + (rc >> 5) * (kT + 1) + (rc & 31)] = Dv[static_cast<size_t>(t) * kTS + (rc >> 5) * kLd + (rc & 31)];
+    }
+  double lv[kT];
+  {
+    const int p = kT + tid;
+    if (p < Pp) ai_row(A, tri_index(p >> 5, 0), p & 31, lv);
+  }
+  __syncthreads();
   for (int i = 0; i < nb; ++i) {
-    const double* D = Dv + static_cast<size_t>(i) * kTS;
-    for (int e = tid; e < kT * kT; e += blockDim.x) dt[(e >> 5) * (kT + 1) + (e & 31)] = D[(e >> 5) * kLd + (e & 31)];
-    __syncthreads();
+    const double* D = dsm + (all ? i * kDs : 0);
+    if (!all) {
+      const double* Dg = Dv + static_cast<size_t>(i) * kTS;
+      for (int e = tid; e < kT * kT; e += blockDim.x) dsm[(e >> 5) * (kT + 1) + (e & 31)] = Dg[(e >> 5) * kLd + (e & 31)];
+      __syncthreads();
+    }
     if (warp == 0) {
       double t0 = 0.0, t1 = 0.0;
 #pragma unroll
       for (int c = 0; c < kT; c += 2) {
-        t0 = fma(dt[ln * (kT + 1) + c], y[i * kT + c], t0);
-        t1 = fma(dt[ln * (kT + 1) + c + 1], y[i * kT + c + 1], t1);
+        t0 = fma(D[ln * (kT + 1) + c], y[i * kT + c], t0);
+        t1 = fma(D[ln * (kT + 1) + c + 1], y[i * kT + c + 1], t1);
       }
       __syncwarp();
       y[i * kT + ln] = t0 + t1;
     }
     __syncthreads();
-    for (int p = (i + 1) * kT + tid; p < Pp; p += blockDim.x) {
-      const double2* Lr =
-          reinterpret_cast<const double2*>(A + static_cast<size_t>(tri_index(p >> 5, i)) * kTS + (p & 31) * kLd);
+    const int p = (i + 1) * kT + tid;
+    if (p < Pp) {
       double a0 = y[p], a1 = 0.0;
 #pragma unroll
       for (int c = 0; c < kT / 2; ++c) {
-        const double2 l2 = __ldg(Lr + c);
-        a0 = fma(-l2.x, y[i * kT + 2 * c], a0);
-        a1 = fma(-l2.y, y[i * kT + 2 * c + 1], a1);
+        a0 = fma(-lv[2 * c], y[i * kT + 2 * c], a0);
+        a1 = fma(-lv[2 * c + 1], y[i * kT + 2 * c + 1], a1);
       }
       y[p] = a0 + a1;
     }
+    for (int p2 = p + kAiThreads; p2 < Pp; p2 += kAiThreads) {
+      double l2[kT];
+      ai_row(A, tri_index(p2 >> 5, i), p2 & 31, l2);
+      double a0 = y[p2], a1 = 0.0;
+#pragma unroll
+      for (int c = 0; c < kT / 2; ++c) {
+        a0 = fma(-l2[2 * c], y[i * kT + 2 * c], a0);
+        a1 = fma(-l2[2 * c + 1], y[i * kT + 2 * c + 1], a1);
+      }
+      y[p2] = a0 + a1;
+    }
+    const int pn = (i + 2) * kT + tid;  // this thread's first row of the next step
+    if (i + 1 < nb && pn < Pp) ai_row(A, tri_index(pn >> 5, i + 1), pn & 31, lv);
     __syncthreads();
+  }
+  {
+    const int q = tid;
+    if (nb > 1 && q < (nb - 1) * kT) ai_col(A, tri_index(nb - 1, q >> 5), q & 31, lv);
   }
   for (int i = nb - 1; i >= 0; --i) {
     if (warp == 0) {
-      const double* D = Dv + static_cast<size_t>(i) * kTS;
       double t0 = 0.0, t1 = 0.0;
+      if (all) {
+        const double* D = dsm + i * kDs;
 #pragma unroll
-      for (int r = 0; r < kT; r += 2) {
-        t0 = fma(D[r * kLd + ln], y[i * kT + r], t0);
-        t1 = fma(D[(r + 1) * kLd + ln], y[i * kT + r + 1], t1);
+        for (int r = 0; r < kT; r += 2) {
+          t0 = fma(D[r * (kT + 1) + ln], y[i * kT + r], t0);
+          t1 = fma(D[(r + 1) * (kT + 1) + ln], y[i * kT + r + 1], t1);
+        }
+      } else {
+        const double* D = Dv + static_cast<size_t>(i) * kTS;
+#pragma unroll
+        for (int r = 0; r < kT; r += 2) {
+          t0 = fma(D[r * kLd + ln], y[i * kT + r], t0);
+          t1 = fma(D[(r + 1) * kLd + ln], y[i * kT + r + 1], t1);
+        }
       }
       __syncwarp();
       y[i * kT + ln] = t0 + t1;
     }
     __syncthreads();
-    for (int q = tid; q < i * kT; q += blockDim.x) {
-      const double* Lc = A + static_cast<size_t>(tri_index(i, q >> 5)) * kTS + (q & 31);
+    const int q = tid;
+    if (q < i * kT) {
       double a0 = y[q], a1 = 0.0;
 #pragma unroll
       for (int r = 0; r < kT; r += 2) {
-        a0 = fma(-Lc[r * kLd], y[i * kT + r], a0);
-        a1 = fma(-Lc[(r + 1) * kLd], y[i * kT + r + 1], a1);
+        a0 = fma(-lv[r], y[i * kT + r], a0);
+        a1 = fma(-lv[r + 1], y[i * kT + r + 1], a1);
       }
       y[q] = a0 + a1;
     }
+    for (int q2 = q + kAiThreads; q2 < i * kT; q2 += kAiThreads) {
+      double c2[kT];
+      ai_col(A, tri_index(i, q2 >> 5), q2 & 31, c2);
+      double a0 = y[q2], a1 = 0.0;
+#pragma unroll
+      for (int r = 0; r < kT; r += 2) {
+        a0 = fma(-c2[r], y[i * kT + r], a0);
+        a1 = fma(-c2[r + 1], y[i * kT + r + 1], a1);
+      }
+      y[q2] = a0 + a1;
+    }
+    if (i >= 1 && q < (i - 1) * kT) ai_col(A, tri_index(i - 1, q >> 5), q & 31, lv);
     __syncthreads();
   }
   for (int q = tid; q < P; q += blockDim.x) out[q] = y[q];
@@ -782,7 +856,9 @@ void launch_apply_inverse(cudaStream_t st, const SolveBatch& b, int s, const dou
   const int Pp = solve_pp(b.P), nb = Pp / kT, ne = solve_ep(b.nf, b.r) / kT;
   const double* A = b.A + static_cast<size_t>(s) * solve_sys_doubles(b.P, b.nf, b.r);
   const double* Dv = A + static_cast<size_t>(nb * (nb + 1) / 2 + ne * nb) * kTS;
-  k_apply_inverse<<<1, kAiThreads, 0, st>>>(A, Dv, b.P, Pp, v, out);
+  const int smem = apply_inverse_smem(nb);
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_apply_inverse), smem);
+  k_apply_inverse<<<1, kAiThreads, smem, st>>>(A, Dv, b.P, Pp, v, out);
   DGPU_LAUNCH("k_apply_inverse");
 }
 
