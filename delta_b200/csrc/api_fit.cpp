@@ -807,8 +807,12 @@ int dgpu_fit_kernel(dgpu_context* ctx, int mem, int64_t width, int64_t height, c
     const TpsDev tdev = upload_tps(c, tp);
     int* dsx = static_cast<int*>(c.slot(kSlotBright, sizeof(int) * std::max(n_stamps, 1)));
     int* dsy = static_cast<int*>(c.slot(kSlotCompOut, sizeof(int) * std::max(n_stamps, 1)));
-    double* chi2_d = static_cast<double*>(c.slot(kSlotCompStats, sizeof(double) * std::max(n_stamps, 1) + 4 * std::max(n_stamps, 1) + 64));
-    int* cnt_d = reinterpret_cast<int*>(chi2_d + std::max(n_stamps, 1));
+    const size_t ns1 = static_cast<size_t>(std::max(n_stamps, 1));
+    double* chi2_d = static_cast<double*>(
+        c.slot(kSlotCompStats, sizeof(double) * ns1 + sizeof(int) * ns1 + 16 + stamp_chi2_scratch_bytes(n_stamps)));
+    int* cnt_d = reinterpret_cast<int*>(chi2_d + ns1);
+    void* chi2_scratch = reinterpret_cast<void*>(
+        (reinterpret_cast<uintptr_t>(cnt_d + ns1) + 15) & ~static_cast<uintptr_t>(15));  // 16-aligned past cnt_d
 
     const int clip_passes = (clip_sigma > 0.0 && clip_iterations > 0) ? clip_iterations : 0;
     const int do_iterate = clip_iterations > 0 ? 1 : 0;
@@ -830,7 +834,7 @@ int dgpu_fit_kernel(dgpu_context* ctx, int mem, int64_t width, int64_t height, c
     // Per-stamp chi^2 of each solution rides on the solution's own read-back.
     E.on_fetch_bytes = (sizeof(double) + sizeof(int)) * static_cast<size_t>(n_stamps) + 64;
     E.on_fetch = [&](const double* d_theta, Fetch& f) {
-      launch_stamp_chi2(st, n_stamps, nc, k, g.SS, E.R, d_acc, d_theta, chi2_d, cnt_d);
+      launch_stamp_chi2(st, n_stamps, nc, k, g.SS, E.R, d_acc, d_theta, chi2_d, cnt_d, chi2_scratch);
       f.add(stamp_chi2.data(), chi2_d, n_stamps);
       f.add(cnt.data(), cnt_d, n_stamps);
     };

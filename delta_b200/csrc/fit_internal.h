@@ -43,8 +43,10 @@ void launch_normal_tc(Context& c, int64_t N, int nc, int k, int SS, const FitRow
 // sums of the residual e = t - X theta (rhs = X^T W e, ywy = e^T W e).
 void launch_rhs(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, const uint8_t* accepted,
                 const double* theta, double* rhs, double* ywy, long long* n);
+// scratch: stamp_chi2_scratch_bytes(n_stamps) of device memory (8-aligned).
+size_t stamp_chi2_scratch_bytes(int n_stamps);
 void launch_stamp_chi2(cudaStream_t st, int n_stamps, int nc, int k, int SS, const FitRows& R,
-                       const uint8_t* accepted, const double* theta, double* chi2, int* cnt);
+                       const uint8_t* accepted, const double* theta, double* chi2, int* cnt, void* scratch);
 void launch_reweight(cudaStream_t st, const StampGeom& g, int n_stamps, const TpsDev& t, const int* sx,
                      const int* sy, const FitRows& R, const uint8_t* accepted, const int* cnt,
                      const double* theta, const float* phi, const float* vr, const uint8_t* rm);

@@ -217,22 +217,27 @@ k_isolate(int w, const unsigned* count, int cap, const int* __restrict__ sorted_
       const int lim = min(static_cast<int>(blockDim.x), nc - base);
       int nk = s_nk;
       const int chunk_start = nk;
-      for (int t = 0; t < lim && nk < max_stamps; ++t) {
-        if (!pass[t]) continue;
-        bool iso = true;
-        for (int k = chunk_start + threadIdx.x; k < nk; k += 32) {
-          const long long dx = cx[t] - ks[2 * k], dy = cy[t] - ks[2 * k + 1];
-          if (dx * dx + dy * dy < iso2) iso = false;
-        }
-        iso = __all_sync(0xffffffffu, iso);
-        if (iso) {
-          if (threadIdx.x == 0) {
-            ks[2 * nk] = cx[t];
-            ks[2 * nk + 1] = cy[t];
-            kept[nk] = cy[t] * w + cx[t];
+      // The candidates that passed, in order, 32 flags per ballot.
+      for (int t0 = 0; t0 < lim && nk < max_stamps; t0 += 32) {
+        unsigned todo = __ballot_sync(0xffffffffu, t0 + static_cast<int>(threadIdx.x) < lim && pass[t0 + threadIdx.x]);
+        while (todo && nk < max_stamps) {
+          const int t = t0 + __ffs(todo) - 1;
+          todo &= todo - 1;
+          bool iso = true;
+          for (int k = chunk_start + threadIdx.x; k < nk; k += 32) {
+            const long long dx = cx[t] - ks[2 * k], dy = cy[t] - ks[2 * k + 1];
+            if (dx * dx + dy * dy < iso2) iso = false;
           }
-          __syncwarp();
-          ++nk;
+          iso = __all_sync(0xffffffffu, iso);
+          if (iso) {
+            if (threadIdx.x == 0) {
+              ks[2 * nk] = cx[t];
+              ks[2 * nk + 1] = cy[t];
+              kept[nk] = cy[t] * w + cx[t];
+            }
+            __syncwarp();
+            ++nk;
+          }
         }
       }
       if (threadIdx.x == 0) s_nk = nk;

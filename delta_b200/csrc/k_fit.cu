@@ -774,22 +774,28 @@ void launch_rhs(Context& c, int64_t N, int nc, int k, int SS, const FitRows& R, 
 
 // ---------------------------------------------------------------------------
 // Per-stamp chi^2 (src/fit.cpp:389-406): sum of w r^2 over the stamp's active
-// rows / count; NaN for stamps without active rows.
+// rows / count; NaN for stamps without active rows. Each stamp's rows are split
+// into kChi2Parts contiguous parts, one CTA each (partial sums in a fixed
+// order), and k_stamp_chi2_finish adds the parts in part order.
 // ---------------------------------------------------------------------------
+constexpr int kChi2Parts = 4;
+
 __global__ void __launch_bounds__(256)
 k_stamp_chi2(int nc, int k, int SS, FitRows R, const uint8_t* __restrict__ accepted,
-             const double* __restrict__ theta, double* __restrict__ chi2, int* __restrict__ cnt) {
+             const double* __restrict__ theta, double* __restrict__ psum, int* __restrict__ pcnt) {
   extern __shared__ double cth[];  // theta, (nc + 1) * k
   __shared__ double ssum[256];
   __shared__ int scnt[256];
-  const int s = blockIdx.x;
+  const int s = blockIdx.x, part = blockIdx.y;
   const int P = (nc + 1) * k;
+  const int per = (SS + kChi2Parts - 1) / kChi2Parts;
+  const int i0 = part * per, i1 = min(SS, i0 + per);
   double acc = 0.0;
   int n = 0;
   if (accepted[s]) {
     for (int p = threadIdx.x; p < P; p += blockDim.x) cth[p] = theta[p];
     __syncthreads();
-    for (int i = threadIdx.x; i < SS; i += blockDim.x) {
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
       const size_t row = static_cast<size_t>(s) * SS + i;
       if (!R.valid[row]) continue;
       const double model = row_model_any(R.d + row * k, R.bn + row * nc, nc, k, cth);
@@ -809,16 +815,40 @@ k_stamp_chi2(int nc, int k, int SS, FitRows R, const uint8_t* __restrict__ accep
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    cnt[s] = scnt[0];
-    chi2[s] = scnt[0] > 0 ? ssum[0] / scnt[0] : __longlong_as_double(0x7ff8000000000000ll);
+    psum[s * kChi2Parts + part] = ssum[0];
+    pcnt[s * kChi2Parts + part] = scnt[0];
   }
 }
 
+__global__ void k_stamp_chi2_finish(int n_stamps, const double* __restrict__ psum, const int* __restrict__ pcnt,
+                                    double* __restrict__ chi2, int* __restrict__ cnt) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_stamps) return;
+  double a = 0.0;
+  int n = 0;
+#pragma unroll
+  for (int g = 0; g < kChi2Parts; ++g) {
+    a += psum[s * kChi2Parts + g];
+    n += pcnt[s * kChi2Parts + g];
+  }
+  cnt[s] = n;
+  chi2[s] = n > 0 ? a / n : __longlong_as_double(0x7ff8000000000000ll);
+}
+
+size_t stamp_chi2_scratch_bytes(int n_stamps) {
+  return (sizeof(double) + sizeof(int)) * kChi2Parts * static_cast<size_t>(std::max(n_stamps, 1)) + 16;
+}
+
 void launch_stamp_chi2(cudaStream_t st, int n_stamps, int nc, int k, int SS, const FitRows& R,
-                       const uint8_t* accepted, const double* theta, double* chi2, int* cnt) {
+                       const uint8_t* accepted, const double* theta, double* chi2, int* cnt, void* scratch) {
   if (n_stamps == 0) return;
-  k_stamp_chi2<<<n_stamps, 256, sizeof(double) * (nc + 1) * k, st>>>(nc, k, SS, R, accepted, theta, chi2, cnt);
+  double* psum = static_cast<double*>(scratch);
+  int* pcnt = reinterpret_cast<int*>(psum + static_cast<size_t>(kChi2Parts) * n_stamps);
+  k_stamp_chi2<<<dim3(n_stamps, kChi2Parts), 256, sizeof(double) * (nc + 1) * k, st>>>(nc, k, SS, R, accepted, theta,
+                                                                                       psum, pcnt);
   DGPU_LAUNCH("k_stamp_chi2");
+  k_stamp_chi2_finish<<<(n_stamps + 127) / 128, 128, 0, st>>>(n_stamps, psum, pcnt, chi2, cnt);
+  DGPU_LAUNCH("k_stamp_chi2_finish");
 }
 
 // ---------------------------------------------------------------------------
