@@ -274,15 +274,41 @@ def negate(t) -> None:
     check(_lib.lib().dgpu_negate(ctx.handle, MEM_DEVICE, _p(t), ctypes.c_int64(t.numel())), ctx.handle)
 
 
-def download(out: dict) -> dict:
+class EarlyDownload:
+    """Device-to-host copies of some final products, started on the calling
+    thread's download stream while the frame's remaining stages compute."""
+
+    def __init__(self, products: dict):
+        cur = torch.cuda.current_stream()
+        s = _thread_download_stream()
+        s.wait_stream(cur)
+        self.host = {}
+        with torch.cuda.stream(s):
+            for key, t in products.items():
+                if t is None:
+                    self.host[key] = None
+                    continue
+                t = t.contiguous()
+                h = torch.empty(tuple(t.shape), dtype=t.dtype, pin_memory=True)
+                h.copy_(t, non_blocking=True)
+                t.record_stream(s)
+                self.host[key] = h
+        self.done = torch.cuda.Event()
+        self.done.record(s)
+
+
+def download(out: dict, early: EarlyDownload | None = None) -> dict:
     """Copy the image products of run()/apply() into pinned host memory;
     returns {name: ndarray | None}. The copies go through the copy engine
-    (dgpu_copy_to_host); the library's own small read-backs reach the host by
-    SM stores, so frames computing on other streams do not wait behind a
-    200 MB download."""
+    (dgpu_copy_to_host, or `early`'s copies for the products it holds); the
+    library's own small read-backs reach the host by SM stores, so frames
+    computing on other streams do not wait behind a 200 MB download."""
     ctx = _ctx_on_torch_stream()
     pinned = {}
     for key in ("difference", "variance", "mask", "score"):
+        if early is not None and key in early.host:
+            pinned[key] = early.host[key]
+            continue
         t = out.get(key)
         if t is None:
             pinned[key] = None
@@ -293,6 +319,8 @@ def download(out: dict) -> dict:
                                            ctypes.c_int64(t.numel() * t.element_size())), ctx.handle)
         pinned[key] = hbuf
     torch.cuda.current_stream().synchronize()
+    if early is not None:
+        early.done.synchronize()
     return {k: (None if v is None else v.numpy()) for k, v in pinned.items()}
 
 
@@ -366,7 +394,7 @@ def build_catalog(score, difference, mask, psf, threshold_sigma=5.0, threshold_s
     return _pack(cols)
 
 
-def run(sub, frame: DeviceFrame, catalog=None, direction=None) -> dict:
+def run(sub, frame: DeviceFrame, catalog=None, direction=None, early=None) -> dict:
     """One Subtractor.subtract pass on device-resident layers (fit -> subtract ->
     [decorrelate] -> [score + catalog]). Returns device tensors for the images
     and host values for the solution / PSF / catalog."""
@@ -411,20 +439,23 @@ def run(sub, frame: DeviceFrame, catalog=None, direction=None) -> dict:
         direction=direction, shape=(h, w), reduced_chi2=fit["reduced_chi2"], n_stamps_used=fit["n_stamps_used"],
         n_stamps_rejected=fit["n_stamps_rejected"], stamp_x=fit["stamp_x"], stamp_y=fit["stamp_y"],
         stamp_chi2=fit["stamp_chi2"], stamp_accepted=fit["stamp_accepted"])
-    return apply(sub, solution, target, conv, tvar, cvar, tmask, cmask, sign, sel["x"], sel["y"])
+    return apply(sub, solution, target, conv, tvar, cvar, tmask, cmask, sign, sel["x"], sel["y"], early)
 
 
-def apply_solution(sub, solution, frame: DeviceFrame) -> dict:
+def apply_solution(sub, solution, frame: DeviceFrame, early=None) -> dict:
     """Subtractor.apply on device-resident layers: a frozen solution, no re-fit."""
     frame.wait_variances()
     if solution.direction == "science":
         return apply(sub, solution, frame.reference, frame.science, frame.reference_var, frame.science_var,
-                     frame.reference_mask, frame.science_mask, -1.0, solution.stamp_x, solution.stamp_y)
+                     frame.reference_mask, frame.science_mask, -1.0, solution.stamp_x, solution.stamp_y, early)
     return apply(sub, solution, frame.science, frame.reference, frame.science_var, frame.reference_var,
-                 frame.science_mask, frame.reference_mask, 1.0, solution.stamp_x, solution.stamp_y)
+                 frame.science_mask, frame.reference_mask, 1.0, solution.stamp_x, solution.stamp_y, early)
 
 
-def apply(sub, solution, target, conv, tvar, cvar, tmask, cmask, sign, stamp_x, stamp_y) -> dict:
+def apply(sub, solution, target, conv, tvar, cvar, tmask, cmask, sign, stamp_x, stamp_y, early=None) -> dict:
+    """The stages after the fit. `early(products)`, when given, receives the
+    difference, variance and mask as soon as they are final (before the score
+    and catalog), e.g. to start their download."""
     out_levels = [v for v in (sub.saturation, sub.bright_mask) if v and v > 0]
     out_saturation = min(out_levels) if out_levels else 0.0
     diff, var, mask = subtract(target, conv, tvar, cvar, tmask, cmask, solution, out_saturation)
@@ -439,6 +470,8 @@ def apply(sub, solution, target, conv, tvar, cvar, tmask, cmask, sign, stamp_x, 
         whitened, white_var = decorrelate(diff, solution, tvar, cvar, sub.block)
         if variance_scale is not None:
             scale_(white_var, variance_scale)
+    if early is not None:  # these three are final from here on
+        early({"difference": whitened, "variance": white_var if white_var is not None else var, "mask": mask})
     score = psf = cat = None
     if sub.score:
         if stamp_x is None or np.asarray(stamp_x).size == 0:
@@ -475,6 +508,13 @@ def _thread_stream():
     s = getattr(_tls, "stream", None)
     if s is None:
         s = _tls.stream = torch.cuda.Stream()
+    return s
+
+
+def _thread_download_stream():
+    s = getattr(_tls, "dl_stream", None)
+    if s is None:
+        s = _tls.dl_stream = torch.cuda.Stream()
     return s
 
 

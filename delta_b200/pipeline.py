@@ -396,15 +396,20 @@ class Subtractor:
             rvar = synth_variance(ref, gain, read_noise)
         logger.info("fitting {} x {} frame (device resident)", sci.shape[1], sci.shape[0])
         frame = _device.DeviceFrame.from_numpy(sci, ref, svar, rvar, smask, rmask, non_blocking=True, serialize=True)
+        started = {}
+
+        def early(products):  # final before the score and catalog: start their download
+            started["dl"] = _device.EarlyDownload(products)
+
         try:
             if solution is None:
-                out = _device.run(self, frame, catalog, direction)
+                out = _device.run(self, frame, catalog, direction, early=early)
             else:
-                out = _device.apply_solution(self, solution, frame)
+                out = _device.apply_solution(self, solution, frame, early=early)
         except BaseException:
             frame.finish_upload()  # the host layers must outlive their copies
             raise
-        host = _device.download(out)
+        host = _device.download(out, started.get("dl"))
         return DiffResult(difference=host["difference"], variance=host["variance"], mask=host["mask"],
                           score=host["score"], solution=out["solution"], psf=out["psf"],
                           source_catalog=out["catalog"], variance_scale=out["variance_scale"])
