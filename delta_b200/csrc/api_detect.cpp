@@ -130,8 +130,7 @@ int dgpu_select_stamps(dgpu_context* ctx, int mem, int64_t width, int64_t height
         }
     } else {
       DetectHost ds, dr;
-      run_detect(c, w, h, s, sm, p, 0, ds);
-      run_detect(c, w, h, r, rm, p, 1, dr);
+      run_detect_pair(c, w, h, s, sm, r, rm, p, ds, dr);
       const long tol2 = static_cast<long>(p.match_radius) * p.match_radius;
       for (size_t i = 0; i < dr.x.size(); ++i) {
         int best = -1;

@@ -24,6 +24,9 @@ struct DetectHost {
 
 int run_detect(Context& c, int w, int h, const float* img, const uint8_t* mask, const DetectParamsDev& p, int which,
                DetectHost& res);
+// run_detect of two images (workspace slots 0 and 1) sharing each synchronisation.
+void run_detect_pair(Context& c, int w, int h, const float* img0, const uint8_t* mask0, const float* img1,
+                     const uint8_t* mask1, const DetectParamsDev& p, DetectHost& res0, DetectHost& res1);
 void run_background(Context& c, int64_t n, const float* img, const uint8_t* mask, double* median, double* sigma);
 void run_catalog_stamps(Context& c, int w, int h, const float* sci, const uint8_t* sm, const float* ref,
                         const uint8_t* rm, const int* xs_host, const int* ys_host, int n, const DetectParamsDev& p,

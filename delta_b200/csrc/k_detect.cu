@@ -487,84 +487,156 @@ void launch_weighted_mean(Context& c, int64_t n, const float* d, const float* v,
   out2[1] = b;
 }
 
-// Full detect pipeline for one image. Returns the kept count; host copies of
-// x, y, flux, snr, fwhm in `res`.
-int run_detect(Context& c, int w, int h, const float* img, const uint8_t* mask, const DetectParamsDev& p, int which,
-               DetectHost& res) {
+// The detect pipeline of one image in three phases, each ending in read-backs
+// that the caller's sync_reads completes: (1) background, 3x3 peaks and the
+// footprint test -> candidate counts; (2) brightest-first sort and greedy
+// isolation -> kept count; (3) the kept stamps' flux, S/N and FWHM. Two
+// images (their own workspace slots, `which` 0 and 1) can run phase by phase
+// so that they share each synchronisation.
+struct DetectJob {
+  const float* img;
+  const uint8_t* mask;
+  int which;
+  DetectHost* res;
+  float* bg;
+  unsigned* count;
+  int *cand, *sorted, *kept, *vals, *nk;
+  unsigned long long *keys, *keys2;
+  unsigned hc[2] = {0, 0};
+  float hbg[2] = {0.0f, 0.0f};
+  int nkept = 0;
+  std::vector<int> hk;
+};
+constexpr int kDetectCap = 1 << 20;
+
+static void detect_phase1(Context& c, int w, int h, const DetectParamsDev& p, DetectJob& j) {
   cudaStream_t s = c.stream;
   const int64_t n = static_cast<int64_t>(w) * h;
-  const Slot ss = which ? kSlotFit12 : kSlotFit10, ks = which ? kSlotFit13 : kSlotFit11;
-  float* bg = static_cast<float*>(c.slot(which ? kSlotFit15 : kSlotFit14, 64));
-  launch_background(c, n, img, mask, bg, ss, ks);
-  const int cap = 1 << 20;
-  char* buf = static_cast<char*>(c.slot(which ? kSlotFft1 : kSlotFft0, (sizeof(int) * 3 + 2 * sizeof(unsigned long long)) * cap + 256));
-  unsigned* count = reinterpret_cast<unsigned*>(buf);
-  int* cand = reinterpret_cast<int*>(buf + 64);
-  int* sorted = cand + cap;
-  int* kept = sorted + cap;
-  unsigned long long* keys = reinterpret_cast<unsigned long long*>(kept + cap);
-  unsigned long long* keys2 = keys + cap;
-  int* vals = reinterpret_cast<int*>(c.slot(which ? kSlotFft3 : kSlotFft2, sizeof(int) * cap + 64));
-  int* nk = vals + cap;
-  unsigned* n_peaks = count + 1;  // 3x3 peaks before the footprint test; `sorted` holds them until the sort
-  DGPU_CUDA(cudaMemsetAsync(count, 0, 2 * sizeof(unsigned), s));
+  const Slot ss = j.which ? kSlotFit12 : kSlotFit10, ks = j.which ? kSlotFit13 : kSlotFit11;
+  j.bg = static_cast<float*>(c.slot(j.which ? kSlotFit15 : kSlotFit14, 64));
+  launch_background(c, n, j.img, j.mask, j.bg, ss, ks);
+  const int cap = kDetectCap;
+  char* buf = static_cast<char*>(
+      c.slot(j.which ? kSlotFft1 : kSlotFft0, (sizeof(int) * 3 + 2 * sizeof(unsigned long long)) * cap + 256));
+  j.count = reinterpret_cast<unsigned*>(buf);
+  j.cand = reinterpret_cast<int*>(buf + 64);
+  j.sorted = j.cand + cap;
+  j.kept = j.sorted + cap;
+  j.keys = reinterpret_cast<unsigned long long*>(j.kept + cap);
+  j.keys2 = j.keys + cap;
+  j.vals = static_cast<int*>(c.slot(j.which ? kSlotFft3 : kSlotFft2, sizeof(int) * cap + 64));
+  j.nk = j.vals + cap;
+  unsigned* n_peaks = j.count + 1;  // 3x3 peaks before the footprint test; `sorted` holds them until the sort
+  DGPU_CUDA(cudaMemsetAsync(j.count, 0, 2 * sizeof(unsigned), s));
   const int blocks = static_cast<int>(std::min<int64_t>((n + 255) / 256, 148 * 16));
-  k_peaks<<<blocks, 256, 0, s>>>(w, h, img, bg, p, n_peaks, cap, sorted);
+  k_peaks<<<blocks, 256, 0, s>>>(w, h, j.img, j.bg, p, n_peaks, cap, j.sorted);
   DGPU_LAUNCH("k_peaks");
-  k_footprint<<<148 * 8, 256, 0, s>>>(w, h, img, mask, p, n_peaks, cap, sorted, count, cand);
+  k_footprint<<<148 * 8, 256, 0, s>>>(w, h, j.img, j.mask, p, n_peaks, cap, j.sorted, j.count, j.cand);
   DGPU_LAUNCH("k_footprint");
-  unsigned hc[2] = {0, 0};
-  float hbg[2];
-  read_back(c, hc, count, 2 * sizeof(unsigned));
-  read_back(c, hbg, bg, sizeof(hbg));
-  sync_reads(c);
-  if (hc[1] > static_cast<unsigned>(cap)) fail(DGPU_ERR_RUNTIME, "detect_stamps: more than 2^20 peak candidates");
-  const unsigned nfoot = hc[0];
-  const int nc = static_cast<int>(nfoot);
-  int nkept = 0;
-  if (nc > 0) {
-    k_cand_keys<<<(nc + 255) / 256, 256, 0, s>>>(count, cap, cand, img, keys, vals);
-    DGPU_LAUNCH("k_cand_keys");
-    size_t tmp_bytes = 0;
-    DGPU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys2, vals, sorted, nc, 0, 64, s));
-    void* tmp = c.slot(which ? kSlotFft5 : kSlotFft4, tmp_bytes + 16);
-    DGPU_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys2, vals, sorted, nc, 0, 64, s));
-    const long long iso = p.isolation_radius;
-    const size_t smem = sizeof(int) * 2 * std::max(p.max_stamps, 1);
-    if (smem > 160 * 1024) fail(DGPU_ERR_INVALID, "detect_stamps: max_stamps above 20480 is not supported");
-    ensure_dynamic_smem(reinterpret_cast<const void*>(k_isolate), smem);
-    k_isolate<<<1, 1024, smem, s>>>(w, count, cap, sorted, iso * iso, p.max_stamps, kept, nk, c.d_status);
-    DGPU_LAUNCH("k_isolate");
-    read_back(c, &nkept, nk, sizeof(int));
-    sync_reads(c);
-  }
-  res.median = static_cast<double>(hbg[0]);
-  res.sigma = 1.4826 * static_cast<double>(hbg[1]);
+  read_back(c, j.hc, j.count, 2 * sizeof(unsigned));
+  read_back(c, j.hbg, j.bg, sizeof(j.hbg));
+}
+
+// After phase 1's sync. Returns whether a read-back was queued.
+static bool detect_phase2(Context& c, int w, const DetectParamsDev& p, DetectJob& j) {
+  cudaStream_t s = c.stream;
+  const int cap = kDetectCap;
+  if (j.hc[1] > static_cast<unsigned>(cap)) fail(DGPU_ERR_RUNTIME, "detect_stamps: more than 2^20 peak candidates");
+  const int nc = static_cast<int>(j.hc[0]);
+  j.nkept = 0;
+  if (nc <= 0) return false;
+  k_cand_keys<<<(nc + 255) / 256, 256, 0, s>>>(j.count, cap, j.cand, j.img, j.keys, j.vals);
+  DGPU_LAUNCH("k_cand_keys");
+  size_t tmp_bytes = 0;
+  DGPU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, j.keys, j.keys2, j.vals, j.sorted, nc, 0, 64, s));
+  void* tmp = c.slot(j.which ? kSlotFft5 : kSlotFft4, tmp_bytes + 16);
+  DGPU_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, j.keys, j.keys2, j.vals, j.sorted, nc, 0, 64, s));
+  const long long iso = p.isolation_radius;
+  const size_t smem = sizeof(int) * 2 * std::max(p.max_stamps, 1);
+  if (smem > 160 * 1024) fail(DGPU_ERR_INVALID, "detect_stamps: max_stamps above 20480 is not supported");
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_isolate), smem);
+  k_isolate<<<1, 1024, smem, s>>>(w, j.count, cap, j.sorted, iso * iso, p.max_stamps, j.kept, j.nk, c.d_status);
+  DGPU_LAUNCH("k_isolate");
+  read_back(c, &j.nkept, j.nk, sizeof(int));
+  return true;
+}
+
+// After phase 2's sync. Returns whether a read-back was queued.
+static bool detect_phase3(Context& c, int w, int h, const DetectParamsDev& p, DetectJob& j) {
+  cudaStream_t s = c.stream;
+  DetectHost& res = *j.res;
+  res.median = static_cast<double>(j.hbg[0]);
+  res.sigma = 1.4826 * static_cast<double>(j.hbg[1]);
+  const int nkept = j.nkept;
   res.x.assign(nkept, 0);
   res.y.assign(nkept, 0);
   res.flux.assign(nkept, 0);
   res.snr.assign(nkept, 0);
   res.fwhm.assign(nkept, 0);
-  if (nkept > 0) {
-    double* props = static_cast<double*>(c.slot(which ? kSlotCompOut : kSlotCompStats, sizeof(double) * 3 * nkept));
-    const size_t psmem = sizeof(double) * static_cast<size_t>(2 * p.fwhm_radius + 1) * (2 * p.fwhm_radius + 1);
-    if (psmem > 200 * 1024) fail(DGPU_ERR_INVALID, "detect_stamps: fwhm_radius too large");
-    ensure_dynamic_smem(reinterpret_cast<const void*>(k_stamp_props), psmem);
-    k_stamp_props<<<nkept, 256, psmem, s>>>(w, h, img, bg, kept, nk, p.fwhm_radius, props, props + nkept,
-                                            props + 2 * nkept);
-    DGPU_LAUNCH("k_stamp_props");
-    std::vector<int> hk(nkept);
-    read_back(c, hk.data(), kept, sizeof(int) * nkept);
-    read_back(c, res.flux.data(), props, sizeof(double) * nkept);
-    read_back(c, res.snr.data(), props + nkept, sizeof(double) * nkept);
-    read_back(c, res.fwhm.data(), props + 2 * nkept, sizeof(double) * nkept);
-    sync_reads(c);
-    for (int i = 0; i < nkept; ++i) {
-      res.x[i] = hk[i] % w;
-      res.y[i] = hk[i] / w;
-    }
+  if (nkept <= 0) return false;
+  double* props =
+      static_cast<double*>(c.slot(j.which ? kSlotCompOut : kSlotCompStats, sizeof(double) * 3 * nkept));
+  const size_t psmem = sizeof(double) * static_cast<size_t>(2 * p.fwhm_radius + 1) * (2 * p.fwhm_radius + 1);
+  if (psmem > 200 * 1024) fail(DGPU_ERR_INVALID, "detect_stamps: fwhm_radius too large");
+  ensure_dynamic_smem(reinterpret_cast<const void*>(k_stamp_props), psmem);
+  k_stamp_props<<<nkept, 256, psmem, s>>>(w, h, j.img, j.bg, j.kept, j.nk, p.fwhm_radius, props, props + nkept,
+                                          props + 2 * nkept);
+  DGPU_LAUNCH("k_stamp_props");
+  j.hk.assign(nkept, 0);
+  read_back(c, j.hk.data(), j.kept, sizeof(int) * nkept);
+  read_back(c, res.flux.data(), props, sizeof(double) * nkept);
+  read_back(c, res.snr.data(), props + nkept, sizeof(double) * nkept);
+  read_back(c, res.fwhm.data(), props + 2 * nkept, sizeof(double) * nkept);
+  return true;
+}
+
+static void detect_finish(int w, DetectJob& j) {
+  for (int i = 0; i < j.nkept; ++i) {
+    j.res->x[i] = j.hk[i] % w;
+    j.res->y[i] = j.hk[i] / w;
   }
-  return nkept;
+}
+
+// Full detect pipeline for one image. Returns the kept count; host copies of
+// x, y, flux, snr, fwhm in `res`.
+int run_detect(Context& c, int w, int h, const float* img, const uint8_t* mask, const DetectParamsDev& p, int which,
+               DetectHost& res) {
+  DetectJob j;
+  j.img = img;
+  j.mask = mask;
+  j.which = which;
+  j.res = &res;
+  detect_phase1(c, w, h, p, j);
+  sync_reads(c);
+  if (detect_phase2(c, w, p, j)) sync_reads(c);
+  if (detect_phase3(c, w, h, p, j)) sync_reads(c);
+  detect_finish(w, j);
+  return j.nkept;
+}
+
+// Both images of a pair, phase by phase: three synchronisations, not six.
+void run_detect_pair(Context& c, int w, int h, const float* img0, const uint8_t* mask0, const float* img1,
+                     const uint8_t* mask1, const DetectParamsDev& p, DetectHost& res0, DetectHost& res1) {
+  DetectJob j[2];
+  j[0].img = img0;
+  j[0].mask = mask0;
+  j[0].which = 0;
+  j[0].res = &res0;
+  j[1].img = img1;
+  j[1].mask = mask1;
+  j[1].which = 1;
+  j[1].res = &res1;
+  detect_phase1(c, w, h, p, j[0]);
+  detect_phase1(c, w, h, p, j[1]);
+  sync_reads(c);
+  bool q = detect_phase2(c, w, p, j[0]);
+  q = detect_phase2(c, w, p, j[1]) || q;
+  if (q) sync_reads(c);
+  q = detect_phase3(c, w, h, p, j[0]);
+  q = detect_phase3(c, w, h, p, j[1]) || q;
+  if (q) sync_reads(c);
+  detect_finish(w, j[0]);
+  detect_finish(w, j[1]);
 }
 
 void run_background(Context& c, int64_t n, const float* img, const uint8_t* mask, double* median, double* sigma) {
