@@ -372,8 +372,6 @@ void launch_z2_median(cudaStream_t s, int64_t n, const float* d, const float* v,
                       unsigned long long* keys, unsigned long long* state, unsigned int* hist);
 void launch_scale_fill(cudaStream_t s, int64_t n, float* v, float scale, bool fill, float value);
 void launch_negate(cudaStream_t s, int64_t n, float* v);
-// bytes (a multiple of 16) from device memory to mapped pinned host memory
-// (its device-side address), both 16-byte aligned, by SM stores.
 // Background median / MAD of a device image with a fixed file-scope scratch
 // (no allocation); out2 (host) = {median, MAD}. Synchronises `s`.
 void background_noalloc(int64_t n, const float* img, const uint8_t* mask, cudaStream_t s, float* out2);
