@@ -242,6 +242,36 @@ def test_subtract_batch_matches_one_at_a_time():
         np.testing.assert_array_equal(r.source_catalog, one.source_catalog)
 
 
+def test_batch_from_pageable_and_pinned_arrays_gives_the_same_bits():
+    """Pageable layers of 1 MB or more are staged into pinned memory by several
+    host threads before their ordered upload; pinned layers go as they are. Both
+    give the same bits, and the layers' host arrays may be dropped as soon as
+    the call returns."""
+    import torch
+
+    ps = [validation.synthetic_pair(1024, 1024, 1500, s, mask_fraction=0.005) for s in (31, 32)]
+    kw = dict(n_max=4, n_knots=3, stamp_radius=12, cv_folds=0, score=True, decorrelate=True, block=256,
+              precision="mixed", saturation=ps[0].saturation)
+    names = ("science", "reference", "science_var", "reference_var", "science_mask", "reference_mask")
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.from_numpy(a[:1].copy()).dtype, pin_memory=True)
+        out = t.numpy()
+        out[...] = a
+        return out
+
+    page = [{k: np.array(getattr(p, k), copy=True) for k in names} for p in ps]
+    pin = [{k: pinned(getattr(p, k)) for k in names} for p in ps]
+    a = delta.subtract_batch(page, max_in_flight=2, **kw)
+    del page
+    b = delta.subtract_batch(pin, max_in_flight=2, **kw)
+    for ra, rb in zip(a, b, strict=True):
+        np.testing.assert_array_equal(ra.solution.theta, rb.solution.theta)
+        for name in ("difference", "variance", "mask", "score"):
+            np.testing.assert_array_equal(getattr(ra, name), getattr(rb, name), err_msg=name)
+        np.testing.assert_array_equal(ra.source_catalog, rb.source_catalog)
+
+
 def test_apply_batch_matches_one_at_a_time():
     """One frozen solution applied to several frame pairs in flight gives the
     same bits as apply() on each pair alone."""
