@@ -1,5 +1,5 @@
 // Radix-select sample medians (select_internal.h): one compaction launch, then
-// per 8-bit digit a grid-wide histogram and a one-thread pick of the digit
+// per 8-bit digit a grid-wide histogram whose last block picks the digit
 // holding the rank. No host synchronisation: the count, the rank and the key
 // prefix stay on the device.
 #include <cuda_runtime.h>
@@ -53,34 +53,20 @@ __global__ void __launch_bounds__(256) k_sample_keys(int64_t n, int64_t step, co
 __global__ void k_select_init(RadixSelect* st) {
   st->rank = st->count / 2;
   st->prefix = 0;
+  st->arrived = 0;
   for (int i = threadIdx.x; i < 256; i += blockDim.x) st->hist[i] = 0;
 }
 
-__global__ void k_select_hist(const uint32_t* __restrict__ keys, RadixSelect* st, int shift) {
-  __shared__ unsigned hist[256];
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
-  __syncthreads();
-  const unsigned count = st->count, prefix = st->prefix;
-  const unsigned himask = shift >= 24 ? 0u : (0xffffffffu << (shift + 8));
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    const uint32_t k = keys[i];
-    if ((k & himask) == (prefix & himask)) atomicAdd(&hist[(k >> shift) & 0xffu], 1u);
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < 256; i += blockDim.x)
-    if (hist[i]) atomicAdd(&st->hist[i], hist[i]);
-}
-
-// One warp: each lane sums 8 bins, a warp prefix sum finds the lane whose
-// bins hold the rank, that lane walks its 8, and the histogram is cleared.
-__global__ void k_select_pick(RadixSelect* st, int shift, float* result, int last) {
-  const int lane = threadIdx.x;
-  if (lane >= 32) return;
+// One warp of the last block to finish a histogram pass: each lane sums 8
+// bins, a warp prefix sum finds the lane whose bins hold the rank, that lane
+// walks its 8, and the histogram is cleared for the next pass.
+__device__ void select_pick_warp(RadixSelect* st, int shift, float* result, int last) {
+  const int lane = threadIdx.x & 31;
   unsigned h[8];
   unsigned local = 0;
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
-    h[j] = st->hist[lane * 8 + j];
+    h[j] = __ldcg(&st->hist[lane * 8 + j]);  // every block's atomics, past the fence
     local += h[j];
   }
   unsigned incl = local;
@@ -113,6 +99,33 @@ __global__ void k_select_pick(RadixSelect* st, int shift, float* result, int las
   }
 #pragma unroll
   for (int j = 0; j < 8; ++j) st->hist[lane * 8 + j] = 0;
+  if (lane == 0) st->arrived = 0;
+}
+
+// One radix pass: per-block histograms added into st->hist; the last block to
+// arrive (after a fence, so it sees every block's additions) picks the digit.
+__global__ void k_select_hist(const uint32_t* __restrict__ keys, RadixSelect* st, int shift, float* result, int last) {
+  __shared__ unsigned hist[256];
+  __shared__ bool is_last;
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+  __syncthreads();
+  const unsigned count = st->count, prefix = st->prefix;
+  const unsigned himask = shift >= 24 ? 0u : (0xffffffffu << (shift + 8));
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const uint32_t k = keys[i];
+    if ((k & himask) == (prefix & himask)) atomicAdd(&hist[(k >> shift) & 0xffu], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 256; i += blockDim.x)
+    if (hist[i]) atomicAdd(&st->hist[i], hist[i]);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) is_last = atomicAdd(&st->arrived, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (is_last && threadIdx.x < 32) {
+    __threadfence();
+    select_pick_warp(st, shift, result, last);
+  }
 }
 
 void launch_sample_keys(cudaStream_t s, int64_t n, int64_t step, const float* v, const uint8_t* mask, uint32_t* keys,
@@ -128,10 +141,8 @@ void launch_select_upper_median(cudaStream_t s, RadixSelect* st, const uint32_t*
   DGPU_LAUNCH("k_select_init");
   const int hb = static_cast<int>(std::min<int64_t>((std::max<int64_t>(cap, 1) + 1023) / 1024, 148 * 2));
   for (int pass = 0; pass < 4; ++pass) {
-    k_select_hist<<<hb, 256, 0, s>>>(keys, st, 24 - 8 * pass);
+    k_select_hist<<<hb, 256, 0, s>>>(keys, st, 24 - 8 * pass, out, pass == 3);
     DGPU_LAUNCH("k_select_hist");
-    k_select_pick<<<1, 32, 0, s>>>(st, 24 - 8 * pass, out, pass == 3);
-    DGPU_LAUNCH("k_select_pick");
   }
 }
 

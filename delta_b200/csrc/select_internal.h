@@ -15,7 +15,7 @@ struct RadixSelect {
   unsigned count;   // keys in the sample
   unsigned rank;    // remaining rank within the current prefix bucket
   unsigned prefix;  // key bits fixed so far
-  unsigned pad;
+  unsigned arrived;  // blocks done with the current histogram pass
   unsigned hist[256];
 };
 
