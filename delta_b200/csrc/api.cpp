@@ -12,6 +12,8 @@
 #include <cstring>
 #include <stdexcept>
 
+#include <utility>
+
 #include "internal.h"
 
 using namespace dgpu;
@@ -27,22 +29,7 @@ namespace {
 
 template <class F>
 int guarded(dgpu_context* ctx, F&& f) {
-  auto* c = reinterpret_cast<Context*>(ctx);
-  try {
-    if (ctx == nullptr) fail(DGPU_ERR_INVALID, "null context");
-    DGPU_CUDA(cudaSetDevice(c->device));
-    drop_reads(*c);
-    f(*c);
-    return DGPU_OK;
-  } catch (const Failure& e) {
-    if (c) c->last_error = e.what();
-    dgpu::free_error() = e.what();
-    return e.code;
-  } catch (const std::exception& e) {
-    if (c) c->last_error = e.what();
-    dgpu::free_error() = e.what();
-    return DGPU_ERR_RUNTIME;
-  }
+  return run_entry(ctx, false, false, std::forward<F>(f));
 }
 
 template <class F>

@@ -17,21 +17,7 @@ namespace {
 
 template <class F>
 int guarded(dgpu_context* ctx, F&& f) {
-  auto* c = reinterpret_cast<Context*>(ctx);
-  try {
-    if (!ctx) fail(DGPU_ERR_INVALID, "null context");
-    DGPU_CUDA(cudaSetDevice(c->device));
-    drop_reads(*c);
-    reset_status(*c);
-    f(*c);
-    return DGPU_OK;
-  } catch (const Failure& e) {
-    if (c) c->last_error = e.what();
-    return e.code;
-  } catch (const std::exception& e) {
-    if (c) c->last_error = e.what();
-    return DGPU_ERR_RUNTIME;
-  }
+  return run_entry(ctx, true, false, std::forward<F>(f));
 }
 
 DetectParamsDev resolve(const dgpu_detect_params* p) {

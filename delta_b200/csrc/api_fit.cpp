@@ -621,22 +621,7 @@ void write_gls(const GlsOut& o, int nc, int k, dgpu_gls_result* out) {
 
 template <class F>
 int guarded(dgpu_context* ctx, F&& f) {
-  auto* c = reinterpret_cast<Context*>(ctx);
-  try {
-    if (!ctx) fail(DGPU_ERR_INVALID, "null context");
-    DGPU_CUDA(cudaSetDevice(c->device));
-    drop_reads(*c);
-    reset_status(*c);
-    f(*c);
-    check_status(*c);
-    return DGPU_OK;
-  } catch (const Failure& e) {
-    if (c) c->last_error = e.what();
-    return e.code;
-  } catch (const std::exception& e) {
-    if (c) c->last_error = e.what();
-    return DGPU_ERR_RUNTIME;
-  }
+  return run_entry(ctx, true, true, std::forward<F>(f));
 }
 
 // Rows for the direct solver entry points: one unit per row.

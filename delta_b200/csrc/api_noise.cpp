@@ -22,21 +22,7 @@ T* up(Context& c, Slot s, const T* host, size_t n) {
 
 template <class F>
 int guarded(dgpu_context* ctx, F&& f) {
-  auto* c = reinterpret_cast<Context*>(ctx);
-  try {
-    if (!ctx) fail(DGPU_ERR_INVALID, "null context");
-    DGPU_CUDA(cudaSetDevice(c->device));
-    drop_reads(*c);
-    reset_status(*c);
-    f(*c);
-    return DGPU_OK;
-  } catch (const Failure& e) {
-    if (c) c->last_error = e.what();
-    return e.code;
-  } catch (const std::exception& e) {
-    if (c) c->last_error = e.what();
-    return DGPU_ERR_RUNTIME;
-  }
+  return run_entry(ctx, true, false, std::forward<F>(f));
 }
 
 bool pow2(int n) { return n >= 8 && (n & (n - 1)) == 0; }

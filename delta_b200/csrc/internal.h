@@ -10,6 +10,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "delta_gpu.h"
@@ -231,6 +232,33 @@ void check_status(Context& c);  // synchronises the stream
 void read_back(Context& c, void* host, const void* dev, size_t bytes);
 void sync_reads(Context& c);
 void drop_reads(Context& c);
+
+// The body of a context entry point: selects the context's device, drops the
+// read-backs an earlier error left unscattered, optionally clears the device
+// status word before the body (`reset`) and checks it after (`check`), and maps
+// a Failure to its code (anything else to DGPU_ERR_RUNTIME), recording the
+// message on the context and as the last context-free error.
+template <class F>
+int run_entry(dgpu_context* ctx, bool reset, bool check, F&& f) {
+  auto* c = reinterpret_cast<Context*>(ctx);
+  try {
+    if (ctx == nullptr) fail(DGPU_ERR_INVALID, "null context");
+    DGPU_CUDA(cudaSetDevice(c->device));
+    drop_reads(*c);
+    if (reset) reset_status(*c);
+    f(*c);
+    if (check) check_status(*c);
+    return DGPU_OK;
+  } catch (const Failure& e) {
+    if (c) c->last_error = e.what();
+    free_error() = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    if (c) c->last_error = e.what();
+    free_error() = e.what();
+    return DGPU_ERR_RUNTIME;
+  }
+}
 constexpr int kReadBackList = 16;  // ranges per gather launch
 struct ReadBackList {
   const unsigned char* src[kReadBackList];
